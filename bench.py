@@ -1,0 +1,347 @@
+#!/usr/bin/env python
+"""Benchmark of the CCpol23+(2025) force-evaluation hot path on B200.
+
+A step is one evaluation of the hot path of the 512-water FS2+FS3 box (L = 24.84 A,
+seeded synthetic configuration): Ewald self/intramolecular, real and reciprocal sums,
+the induced-dipole solve with induction forces, FS2 and FS3 (SR/LR/blend).  The 2-body
+term and the integrator are outside this path.  ns/day = steps/s x 0.0005 ps x 86400 / 1000
+(dt = 0.5 fs).  The headline value is the mixed-precision form when its relative force
+error against the FP64 form is <= 1e-5, else the FP64 form; both are reported.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+With --impl reference the CPU oracle (the reference's algorithm restated in C, the reference
+itself being Fortran/MPI with no compiler on this image) runs the same step on all host
+cores.  Multi-GPU runs are independent replicas (the path does not shard here): one seeded
+box per rank, no collectives in the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ns/day @512 H2O FS2+FS3: mixed vs FP64 GPU at rel force err <=1e-5; triples/s"
+DT_PS = 0.0005
+CONFIG = "c2_512"
+# Algorithmic work of one FS3 site-triple evaluation (energy + gradient, one SR or LR
+# representation), as the reference computes it: ~130 FLOP + 15 MUFU-class operations
+# (6 exp, 3 sqrt, 6 reciprocals).  Counted as 145 floating-point operations.
+FS3_FLOP_PER_SITE_TRIPLE = 145.0
+
+
+def ns_per_day(steps_per_s: float) -> float:
+    return steps_per_s * DT_PS * 86400.0 / 1000.0
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = []
+        for ln in Path(self.file.name).read_text().splitlines():
+            t = [x.strip() for x in ln.split(",")]
+            if len(t) >= 9:
+                rows.append(t)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def build_inputs(rank: int):
+    from ccpol23_plus_2025_mbmd_b200 import Model, data_dir
+    from ccpol23_plus_2025_mbmd_b200.generator import CONFIGS, water_box
+    cfg = CONFIGS[CONFIG]
+    model = Model(data_dir(cfg["variant"]))
+    box = water_box(model, cfg["nm"], cfg["box"], cfg["seed"] + rank)
+    return model, box, cfg
+
+
+def time_device(ctx, box, steps, warmup, flush, torch):
+    """Device-resident steps: inputs already in HBM, per-step CUDA events on the context's
+    (torch's current) stream, L2 flushed between steps outside the events."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    x, y, z, xs, ys, zs = (T(a) for a in (box.x, box.y, box.z, box.xs, box.ys, box.zs))
+    f = [torch.zeros_like(xs) for _ in range(3)]
+    c2 = [torch.zeros_like(x) for _ in range(3)]
+    c3 = [torch.zeros_like(x) for _ in range(3)]
+    mu = [torch.zeros_like(xs) for _ in range(3)]
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_timing(True)
+    for _ in range(warmup):
+        e = ctx.hot_path_device(x, y, z, xs, ys, zs, box.box, *f, *c2, *c3, *mu)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    phases = []
+    launches = 0
+    t0 = time.perf_counter()
+    for k in range(steps):
+        flush.add_(1.0)
+        ev[k][0].record(stream)
+        e = ctx.hot_path_device(x, y, z, xs, ys, zs, box.box, *f, *c2, *c3, *mu)
+        ev[k][1].record(stream)
+        phases.append(ctx.phase_ms())
+        launches += ctx.last_launches()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    ms = [a.elapsed_time(b) for a, b in ev]
+    forces = np.stack([t.cpu().numpy() for t in f])
+    return {"ms": ms, "phases": np.array(phases), "energies": e, "launches": launches,
+            "wall_s": wall, "forces": forces,
+            "com3": np.stack([t.cpu().numpy() for t in c3]),
+            "com2": np.stack([t.cpu().numpy() for t in c2])}
+
+
+def time_e2e(ctx, box, steps, warmup, flush, torch):
+    """Through the public host-buffer entry point: H2D of the step's inputs and D2H of its
+    forces, COM forces, dipoles and energies inside the timed region."""
+    ctx.set_stream(None)
+    ctx.set_timing(False)
+    for _ in range(warmup):
+        ctx.hot_path(box.x, box.y, box.z, box.xs, box.ys, box.zs, box.box)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(steps):
+        flush.add_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.hot_path(box.x, box.y, box.z, box.xs, box.ys, box.zs, box.box)
+        times.append(time.perf_counter() - t0)
+    nm, ld = box.xs.shape
+    ns = ctx.model.ns
+    npol = ctx.model.npol
+    h2d = 8 * (3 * nm + 3 * nm * ld)
+    d2h = 8 * (3 * nm * ns + 6 * nm + 3 * nm * npol) + 8 * 16 + 4 * 5
+    return times, h2d, d2h
+
+
+def cpu_baseline(box, cfg, max_seconds=60.0):
+    """The oracle's hot path on all host cores for one full step of the same box."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from ccpol23_plus_2025_mbmd_b200 import data_dir
+    O.build()
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    M = O.make_model(O.read_inputs(data_dir(cfg["variant"])), box.nm, box.box)
+    t0 = time.perf_counter()
+    e, st = O.hot_path(M, box.x, box.y, box.z, box.xs, box.ys, box.zs, box.box)
+    dt = time.perf_counter() - t0
+    return dt, cores, e, st
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    model, box, cfg = build_inputs(0)
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    from ccpol23_plus_2025_mbmd_b200 import data_dir
+    O.build()
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    M = O.make_model(O.read_inputs(data_dir(cfg["variant"])), box.nm, box.box)
+    # no warm-up steps: a CPU step has nothing to warm and each one takes tens of seconds
+    times = []
+    budget = 240.0
+    t_start = time.perf_counter()
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        O.hot_path(M, box.x, box.y, box.z, box.xs, box.ys, box.zs, box.box)
+        times.append(time.perf_counter() - t0)
+        if time.perf_counter() - t_start > budget:
+            break
+    s = float(np.mean(times))
+    val = ns_per_day(1.0 / s)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": "ns/day",
+        "n_gpus": world, "steps": len(times), "warmup": 0, "ms_per_step": s * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded jittered-lattice water box)",
+        "config": {"workload": "512 H2O FS2+FS3 hot-path force evaluation", "nm": box.nm,
+                   "box_A": box.box, "variant": cfg["variant"], "seed": cfg["seed"]},
+        "cpu_baseline": {"value": val, "unit": "ns/day", "cores": cores, "kind": "port",
+                         "sample": f"{len(times)} of {args.steps} requested full hot-path "
+                                   f"evaluations of the 512-water box (time-capped at {budget:.0f} s)"},
+        "e2e": {"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from ccpol23_plus_2025_mbmd_b200 import Context
+    from ccpol23_plus_2025_mbmd_b200.api import fma_peak_tflops
+
+    model, box, cfg = build_inputs(rank)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    results = {}
+    with ClockSampler(local) as clk:
+        for prec in ("fp64", "mixed"):
+            with Context(model, box.nm, box.box, device=local, precision=prec) as ctx:
+                if world > 1:
+                    dist.barrier()
+                torch.cuda.synchronize()
+                r = time_device(ctx, box, args.steps, args.warmup, flush, torch)
+                torch.cuda.synchronize()
+                if world > 1:
+                    dist.barrier()
+                t, h2d, d2h = time_e2e(ctx, box, args.steps, args.warmup, flush, torch)
+                r["e2e_s"] = t
+                r["h2d"], r["d2h"] = h2d, d2h
+                results[prec] = r
+    clocks = clk.summary()
+    peak64 = fma_peak_tflops(local, "fp64")
+    peak32 = fma_peak_tflops(local, "mixed")
+
+    def agg(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    out = {}
+    for prec, r in results.items():
+        ms = agg(float(np.mean(r["ms"])))
+        e2e = agg(float(np.mean(r["e2e_s"])))
+        e = r["energies"]
+        out[prec] = {"ms_per_step": ms, "ns_day": world * ns_per_day(1e3 / ms),
+                     "e2e_ns_day": world * ns_per_day(1.0 / e2e), "e2e_ms": e2e * 1e3,
+                     "triples_per_s": world * e["n_fs3_triples"] / (ms * 1e-3),
+                     "fs3_ms": float(np.mean(r["phases"][:, 6])),
+                     "phase_ms": [float(v) for v in r["phases"].mean(0)],
+                     "ind_iters": e["ind_iters"], "n_fs3_triples": e["n_fs3_triples"],
+                     "n_fs3_blend": e["n_fs3_blend"], "n_fs2_triples": e["n_fs2_triples"],
+                     "launches_per_step": r["launches"] / args.steps}
+    # mixed vs FP64 relative errors on the same box (three-body terms change, the rest is
+    # FP64 in both forms)
+    f64, fmx = results["fp64"], results["mixed"]
+    ferr = float(np.linalg.norm(fmx["forces"] - f64["forces"]) / np.linalg.norm(f64["forces"]))
+    c3err = float(np.linalg.norm(fmx["com3"] - f64["com3"]) / np.linalg.norm(f64["com3"]))
+    eerr = abs(fmx["energies"]["fs3pe"] - f64["energies"]["fs3pe"]) / abs(f64["energies"]["fs3pe"])
+    head = "mixed" if max(ferr, c3err) <= 1e-5 else "fp64"
+    H = out[head]
+    # roofline of the dominant kernel (FS3) of the headline form
+    e = results[head]["energies"]
+    site_triples = (e["n_fs3_triples"] + e["n_fs3_blend"]) * 17 ** 3
+    fs3_s = H["fs3_ms"] * 1e-3
+    achieved = FS3_FLOP_PER_SITE_TRIPLE * site_triples / fs3_s / 1e12
+    peak = peak32 if head == "mixed" else peak64
+    line = {
+        "metric": METRIC, "value": out[head]["ns_day"], "unit": "ns/day", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": H["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if head == "mixed" else "f64",
+        "data": "synthetic (seeded jittered-lattice water box, 298 K)",
+        "config": {"workload": "512 H2O FS2+FS3 hot-path force evaluation (Ewald self/real/"
+                               "recip + induced-dipole solve + induction forces + FS2 + FS3)",
+                   "nm": box.nm, "box_A": box.box, "variant": cfg["variant"], "seed": cfg["seed"],
+                   "form": head, "l2": "flushed between timed steps (256 MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "triples_per_s": H["triples_per_s"],
+        "fp64": out["fp64"], "mixed": out["mixed"],
+        "mixed_vs_fp64": {"rel_site_force_err": ferr, "rel_fs3_com_force_err": c3err,
+                          "rel_fs3_energy_err": eerr},
+        "e2e": {"value": H["e2e_ns_day"], "unit": "ns/day",
+                "h2d_bytes_per_step": results[head]["h2d"], "d2h_bytes_per_step": results[head]["d2h"]},
+        "roofline": {"bound": "fp32_pipe" if head == "mixed" else "fp64_pipe",
+                     "kernel": "k_fs3<float>" if head == "mixed" else "k_fs3<double>",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "peak_source": "measured in this run by an FMA-chain microbenchmark "
+                                    "(MEASURED_PEAKS.json has no FP32/FP64 figure)",
+                     "work": f"{FS3_FLOP_PER_SITE_TRIPLE:.0f} flop per site-triple evaluation x "
+                             f"{site_triples} site triples per launch",
+                     "traffic": None},
+        "gpu_launches": int(results[head]["launches"]),
+        "clocks": clocks,
+        "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dt, cores, eo, st = cpu_baseline(box, cfg)
+        line["cpu_baseline"] = {"value": ns_per_day(1.0 / dt), "unit": "ns/day", "cores": cores,
+                                "kind": "port",
+                                "sample": "1 full hot-path evaluation of the same 512-water box "
+                                          f"({dt:.1f} s on {cores} threads)"}
+        Fo = np.stack([st.fxs, st.fys, st.fzs])
+        line["parity_vs_oracle"] = {
+            "fp64_rel_force_err": float(np.linalg.norm(f64["forces"] - Fo) / np.linalg.norm(Fo)),
+            "mixed_rel_force_err": float(np.linalg.norm(fmx["forces"] - Fo) / np.linalg.norm(Fo))}
+    if world > 1:
+        torch.cuda.synchronize()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,273 @@
+"""Python mirror of the reference's hot-path entry points, over the C ABI.
+
+Names, argument meaning, units and side effects follow the Fortran module procedures of
+ommair/CCpol23_plus_2025_MBMD (ewald.f90, nb_induction_model.f90,
+threebody_potential.f90): positions in Angstrom; energies returned in kcal/mol; site forces
+accumulate into ``fxs/fys/fzs`` (internal units, 10 J/mol/A); 3-body COM forces are
+overwritten; the virial accumulates into ``vir`` (a 1-element float64 array, standing in
+for the module global).  Site arrays are ``(nm, ld)`` float64, site index fastest.
+Errors raise :class:`CcpError` where the reference would ``stop``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+from ._lib import CcpEnergies, check, ptr
+
+DATA = Path(__file__).resolve().parent / "data"
+
+
+def data_dir(variant: str) -> Path:
+    """Parameter directory shipped with the package: "fs3" or "fs2fs3"."""
+    return DATA / variant
+
+
+class Model:
+    """Parameters read from CONTROL, FIELD, data3b_full, data3b_full_LR_4p5."""
+
+    def __init__(self, directory):
+        L = _lib.lib()
+        h = C.c_void_p()
+        check(L.ccp_model_load(str(directory).encode(), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            _lib.lib().ccp_model_free(self._h)
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_int(self, name):
+        v = C.c_int()
+        check(_lib.lib().ccp_model_get_int(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def get_double(self, name):
+        v = C.c_double()
+        check(_lib.lib().ccp_model_get_double(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def set(self, name, value):
+        L = _lib.lib()
+        if isinstance(value, (bool, int, np.integer)) and name not in ("rcut", "rcut3", "alpha3", "delta33"):
+            check(L.ccp_model_set_int(self._h, name.encode(), int(value)))
+        else:
+            check(L.ccp_model_set_double(self._h, name.encode(), float(value)))
+
+    def array(self, name, n):
+        out = np.zeros(n)
+        check(_lib.lib().ccp_model_get_array(self._h, name.encode(), out.ctypes.data, n))
+        return out
+
+    @property
+    def ns(self):
+        return self.get_int("ns")
+
+    @property
+    def npol(self):
+        return self.get_int("npol")
+
+    @property
+    def charge(self):
+        return self.array("charge", self.ns)
+
+    @property
+    def polarizability(self):
+        return self.array("polarizability", self.ns)
+
+    @property
+    def mass(self):
+        return self.array("mass", self.ns)
+
+    @property
+    def pcoord(self):
+        return self.array("pcoord", self.ns * 3).reshape(self.ns, 3)
+
+    @property
+    def pmi(self):
+        return self.array("pmi", 3)
+
+    def sites(self, q: np.ndarray, ld: int | None = None):
+        """Site offsets from the COM for quaternions q (nm, 4) (molecular_sites.f90:14-47)."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        nm = q.shape[0]
+        ld = ld or self.ns
+        xs, ys, zs = (np.zeros((nm, ld)) for _ in range(3))
+        check(_lib.lib().ccp_sites(self._h, nm, q.ctypes.data, ld, xs.ctypes.data, ys.ctypes.data,
+                                   zs.ctypes.data))
+        return xs, ys, zs
+
+
+def fma_peak_tflops(device: int = 0, precision: str = "fp64") -> float:
+    """Measured FMA-pipe peak of the device (TFLOP/s)."""
+    v = C.c_double()
+    prec = {"fp64": _lib.CCP_FP64, "mixed": _lib.CCP_MIXED}[precision]
+    check(_lib.lib().ccp_device_fma_peak(device, prec, C.byref(v)))
+    return v.value
+
+
+def ewald_setup(ewps: float, rcut: float, box: float):
+    """ewald.f90:17-43 -> (alpha, kmax1, kmax2, kmax3)."""
+    a = C.c_double()
+    k1, k2, k3 = C.c_int(), C.c_int(), C.c_int()
+    check(_lib.lib().ccp_ewald_setup(ewps, rcut, box, C.byref(a), C.byref(k1), C.byref(k2),
+                                     C.byref(k3)))
+    return a.value, k1.value, k2.value, k3.value
+
+
+@dataclass
+class HotPathResult:
+    energies: dict
+    fxs: np.ndarray
+    fys: np.ndarray
+    fzs: np.ndarray
+    fxfs2: np.ndarray
+    fyfs2: np.ndarray
+    fzfs2: np.ndarray
+    fxfs3: np.ndarray
+    fyfs3: np.ndarray
+    fzfs3: np.ndarray
+    idmx: np.ndarray
+    idmy: np.ndarray
+    idmz: np.ndarray
+
+
+def _energies(e: CcpEnergies) -> dict:
+    return {k: getattr(e, k) for k, _ in CcpEnergies._fields_}
+
+
+class Context:
+    """Device-resident state for boxes of ``nm`` molecules on one GPU."""
+
+    def __init__(self, model: Model, nm: int, box0: float, device: int = 0,
+                 precision: str = "fp64"):
+        prec = {"fp64": _lib.CCP_FP64, "mixed": _lib.CCP_MIXED}[precision]
+        h = C.c_void_p()
+        check(_lib.lib().ccp_context_create(model.handle, nm, box0, device, prec, C.byref(h)))
+        self._h = h
+        self.model = model
+        self.nm = nm
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().ccp_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_ewald(self, alpha, k1, k2, k3):
+        check(_lib.lib().ccp_context_set_ewald(self._h, alpha, k1, k2, k3))
+
+    def set_maxit(self, maxit):
+        check(_lib.lib().ccp_context_set_maxit(self._h, maxit))
+
+    def set_stream(self, stream_ptr: int | None):
+        check(_lib.lib().ccp_context_set_stream(self._h, stream_ptr))
+
+    def set_timing(self, on: bool = True):
+        check(_lib.lib().ccp_context_set_timing(self._h, int(on)))
+
+    def phase_ms(self) -> np.ndarray:
+        out = np.zeros(7)
+        check(_lib.lib().ccp_context_phase_ms(self._h, out.ctypes.data, 7))
+        return out
+
+    def last_launches(self) -> int:
+        v = C.c_int()
+        check(_lib.lib().ccp_context_last_launches(self._h, C.byref(v)))
+        return v.value
+
+    # -- reference entry points -------------------------------------------------------
+    def ewald_self_correction(self, alp, box, x, y, z, xs, ys, zs, fxs, fys, fzs, vir):
+        q = C.c_double()
+        v = C.c_double(float(vir[0]))
+        check(_lib.lib().ccp_ewald_self_correction(self._h, alp, box, ptr(x), ptr(y), ptr(z),
+                                                   ptr(xs), ptr(ys), ptr(zs), xs.shape[1],
+                                                   C.byref(q), ptr(fxs), ptr(fys), ptr(fzs),
+                                                   C.byref(v)))
+        vir[0] = v.value
+        return q.value
+
+    def rspace_ewald(self, x, y, z, xs, ys, zs, box, alp, fxs, fys, fzs, vir):
+        q = C.c_double()
+        v = C.c_double(float(vir[0]))
+        check(_lib.lib().ccp_rspace_ewald(self._h, ptr(x), ptr(y), ptr(z), ptr(xs), ptr(ys),
+                                          ptr(zs), xs.shape[1], box, alp, C.byref(q), ptr(fxs),
+                                          ptr(fys), ptr(fzs), C.byref(v)))
+        vir[0] = v.value
+        return q.value
+
+    def kspace_ewald(self, x, y, z, xs, ys, zs, lmax, mmax, nmax, alp, box, fxs, fys, fzs, vir):
+        q = C.c_double()
+        v = C.c_double(float(vir[0]))
+        check(_lib.lib().ccp_kspace_ewald(self._h, ptr(x), ptr(y), ptr(z), ptr(xs), ptr(ys),
+                                          ptr(zs), xs.shape[1], lmax, mmax, nmax, alp, box,
+                                          C.byref(q), ptr(fxs), ptr(fys), ptr(fzs), C.byref(v)))
+        vir[0] = v.value
+        return q.value
+
+    def nb_induction(self, x, y, z, xs, ys, zs, box, idmx, idmy, idmz, fxs, fys, fzs, vir):
+        q = C.c_double()
+        v = C.c_double(float(vir[0]))
+        it = C.c_int()
+        check(_lib.lib().ccp_nb_induction(self._h, ptr(x), ptr(y), ptr(z), ptr(xs), ptr(ys),
+                                          ptr(zs), xs.shape[1], box, C.byref(q), ptr(idmx),
+                                          ptr(idmy), ptr(idmz), ptr(fxs), ptr(fys), ptr(fzs),
+                                          C.byref(v), C.byref(it)))
+        vir[0] = v.value
+        return q.value, it.value
+
+    def threebody_term(self, x, y, z, xs, ys, zs, box, fxs, fys, fzs, fxfs2, fyfs2, fzfs2,
+                       fxfs3, fyfs3, fzfs3, vir):
+        q2, q3 = C.c_double(), C.c_double()
+        v = C.c_double(float(vir[0]))
+        check(_lib.lib().ccp_threebody_term(self._h, ptr(x), ptr(y), ptr(z), ptr(xs), ptr(ys),
+                                            ptr(zs), xs.shape[1], box, C.byref(q2), C.byref(q3),
+                                            ptr(fxs), ptr(fys), ptr(fzs), ptr(fxfs2), ptr(fyfs2),
+                                            ptr(fzfs2), ptr(fxfs3), ptr(fyfs3), ptr(fzfs3),
+                                            C.byref(v)))
+        vir[0] = v.value
+        return q2.value, q3.value
+
+    def hot_path(self, x, y, z, xs, ys, zs, box) -> HotPathResult:
+        nm, ld = xs.shape
+        out = [np.zeros((nm, ld)) for _ in range(3)] + [np.zeros(nm) for _ in range(6)] + \
+              [np.zeros((nm, ld)) for _ in range(3)]
+        e = CcpEnergies()
+        check(_lib.lib().ccp_hot_path(self._h, ptr(x), ptr(y), ptr(z), ptr(xs), ptr(ys), ptr(zs),
+                                      ld, box, C.byref(e), *[ptr(a) for a in out]))
+        return HotPathResult(_energies(e), *out)
+
+    def hot_path_device(self, x, y, z, xs, ys, zs, box, fxs=None, fys=None, fzs=None,
+                        fxfs2=None, fyfs2=None, fzfs2=None, fxfs3=None, fyfs3=None,
+                        fzfs3=None, idmx=None, idmy=None, idmz=None) -> dict:
+        """All arrays are torch CUDA float64 tensors (or None); nothing crosses PCIe."""
+        def dp(t):
+            return None if t is None else t.data_ptr()
+        ld = xs.shape[1]
+        e = CcpEnergies()
+        check(_lib.lib().ccp_hot_path_device(
+            self._h, dp(x), dp(y), dp(z), dp(xs), dp(ys), dp(zs), ld, box, C.byref(e),
+            dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
+            dp(fzfs3), dp(idmx), dp(idmy), dp(idmz)))
+        return _energies(e)

@@ -1,0 +1,974 @@
+// ccp_context.cu -- device-resident state and the C-ABI entry points of the hot path.
+//
+// A context owns, on one GPU, the packed site arrays, neighbour/pair/triple lists,
+// reciprocal-space tables, dipoles and force accumulators for boxes of nm molecules.
+// The reference entry points (threebody_term, nb_induction, rspace_ewald, kspace_ewald,
+// ewald_self_correction) map onto one evaluation with a subset of terms enabled.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ccp_device.cuh"
+#include "ccp_internal.h"
+
+using namespace ccp;
+
+namespace {
+
+enum TermMask : unsigned {
+  T_SELF = 1u,
+  T_RSPACE = 2u,
+  T_KSPACE = 4u,
+  T_INDUCTION = 8u,
+  T_FS2 = 16u,
+  T_FS3 = 32u,
+};
+
+bool cuda_ok(cudaError_t e, const char *what) {
+  if (e == cudaSuccess) return true;
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return false;
+}
+
+#define CK(call)                               \
+  do {                                         \
+    if (!cuda_ok((call), #call)) return CCP_ERR_CUDA; \
+  } while (0)
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t n) {
+  *p = nullptr;
+  if (n == 0) n = 1;
+  return cudaMalloc((void **)p, n * sizeof(T));
+}
+
+}  // namespace
+
+struct ccp_context {
+  int device = 0, precision = CCP_FP64, nm = 0, ns = 0, npol = 0, nsm = 148;
+  cudaStream_t own = nullptr, stream = nullptr;
+  // model-derived constants
+  SiteSets S{};
+  double charge[kNsiteMax] = {0};
+  double rcut = 0, rcutsd = 0, rcut3 = 0, rcutsd3 = 0, alpha3 = 0, delta33 = 0;
+  bool s2 = false, s3 = false, induction = false, three_body = false, damped = false;
+  bool have_fs3 = false;
+  double alpha = 0;
+  int kmax[3] = {0, 0, 0};
+  int maxit = 500;
+  int launches = 0;
+  // inputs in the caller's layout (device copies)
+  int ld_cap = 0;
+  double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;
+  double *d_xs = nullptr, *d_ys = nullptr, *d_zs = nullptr;
+  // packed
+  double4 *d_com = nullptr, *d_act = nullptr, *d_comb = nullptr, *d_s17 = nullptr;
+  // accumulators
+  double *d_f = nullptr, *d_fc2 = nullptr, *d_fc3 = nullptr;
+  double *d_scal = nullptr;
+  int *d_icnt = nullptr;
+  // induction
+  double *d_mu = nullptr, *d_e0r = nullptr, *d_e0k = nullptr, *d_e0slf = nullptr, *d_e0s = nullptr;
+  double *d_eir = nullptr, *d_eik = nullptr, *d_eislf = nullptr, *d_eis = nullptr;
+  // lists
+  int cap = 0, tri_cap = 0, pair_cap = 0;
+  int *d_nbr = nullptr, *d_ncnt = nullptr;
+  double4 *d_nbrv = nullptr;
+  int4 *d_tri = nullptr;
+  int2 *d_pairs = nullptr;
+  // reciprocal space
+  KVec *d_kv = nullptr;
+  int nk = 0, nk_cap = 0;
+  double kv_box = -1, kv_alpha = -1;
+  int kv_kmax[3] = {-1, -1, -1};
+  double2 *d_tab = nullptr;
+  size_t tab_cap = 0;
+  double *d_sk = nullptr;
+  // FS3 tables
+  double *d_coef = nullptr, *d_bgr = nullptr;
+  int *d_types = nullptr;
+  // host staging (pinned)
+  double *h_scal = nullptr;
+  int *h_icnt = nullptr;
+  double *h_io = nullptr;
+  size_t h_io_cap = 0;
+  // constants for the Ewald self energy
+  double sumq = 0, sumq2 = 0;
+  // phase timing (diagnostics)
+  bool timing = false;
+  cudaEvent_t ev[CCP_NPHASE + 1] = {};
+  double phase_ms[CCP_NPHASE] = {0};
+};
+
+namespace {
+
+void free_ctx(ccp_context *c) {
+  cudaSetDevice(c->device);
+  void *dp[] = {c->d_x,   c->d_y,   c->d_z,     c->d_xs,    c->d_ys,   c->d_zs,    c->d_com,
+                c->d_act, c->d_comb, c->d_s17,  c->d_f,     c->d_fc2,  c->d_fc3,   c->d_scal,
+                c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
+                c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
+                c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types};
+  for (void *p : dp)
+    if (p) cudaFree(p);
+  if (c->h_scal) cudaFreeHost(c->h_scal);
+  if (c->h_icnt) cudaFreeHost(c->h_icnt);
+  if (c->h_io) cudaFreeHost(c->h_io);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->own) cudaStreamDestroy(c->own);
+}
+
+int ensure_inputs(ccp_context *c, int ld) {
+  if (ld <= c->ld_cap) return CCP_OK;
+  double **bufs[] = {&c->d_xs, &c->d_ys, &c->d_zs};
+  for (double **b : bufs) {
+    if (*b) cudaFree(*b);
+    CK(dalloc(b, (size_t)c->nm * ld));
+  }
+  c->ld_cap = ld;
+  return CCP_OK;
+}
+
+int ensure_lists(ccp_context *c, int cap, int tri_cap, int pair_cap) {
+  if (cap > c->cap) {
+    if (c->d_nbr) cudaFree(c->d_nbr);
+    if (c->d_nbrv) cudaFree(c->d_nbrv);
+    CK(dalloc(&c->d_nbr, (size_t)c->nm * cap));
+    CK(dalloc(&c->d_nbrv, (size_t)c->nm * cap));
+    c->cap = cap;
+  }
+  if (tri_cap > c->tri_cap) {
+    if (c->d_tri) cudaFree(c->d_tri);
+    CK(dalloc(&c->d_tri, (size_t)tri_cap));
+    c->tri_cap = tri_cap;
+  }
+  if (pair_cap > c->pair_cap) {
+    if (c->d_pairs) cudaFree(c->d_pairs);
+    CK(dalloc(&c->d_pairs, (size_t)pair_cap));
+    c->pair_cap = pair_cap;
+  }
+  return CCP_OK;
+}
+
+// Half-space k-vectors with the spherical cut-off, in the reference's loop order
+// (ewald.f90:933-1082): ll = 0..lmax; mm from 0 (ll = 0) or -mmax; nn from 1 (first mm
+// of ll = 0) or -nmax; keep ll^2 + mm^2 + nn^2 <= min(lmax,mmax,nmax)^2.
+std::vector<KVec> build_kvecs(int lmax, int mmax, int nmax, double alp, double box) {
+  std::vector<KVec> out;
+  const double twopi = 2.0 * kPi;
+  const int klm = std::min(lmax, std::min(mmax, nmax));
+  const int klmsq = klm * klm;
+  const double volmi = box * box * box;
+  int mmin = 0, nmin = 1;
+  for (int ll = 0; ll <= lmax; ll++) {
+    const double rl = twopi * ll / box;
+    if (ll > 0) mmin = -mmax;
+    for (int mm = mmin; mm <= mmax; mm++) {
+      const double rm = twopi * mm / box;
+      for (int nn = nmin; nn <= nmax; nn++) {
+        const double rn = twopi * nn / box;
+        const int kk = ll * ll + mm * mm + nn * nn;
+        if (kk <= klmsq) {
+          const double rksq = rl * rl + rm * rm + rn * rn;
+          KVec k;
+          k.rl = rl;
+          k.rm = rm;
+          k.rn = rn;
+          k.ak = twopi / volmi * std::exp(-0.25 * rksq / (alp * alp)) / rksq;
+          k.l = ll;
+          k.m = mm;
+          k.n = nn;
+          k.pad = 0;
+          out.push_back(k);
+        }
+      }
+      nmin = -nmax;
+    }
+  }
+  return out;
+}
+
+int ensure_kspace(ccp_context *c, double box) {
+  if (box == c->kv_box && c->alpha == c->kv_alpha && c->kmax[0] == c->kv_kmax[0] &&
+      c->kmax[1] == c->kv_kmax[1] && c->kmax[2] == c->kv_kmax[2])
+    return CCP_OK;
+  std::vector<KVec> kv = build_kvecs(c->kmax[0], c->kmax[1], c->kmax[2], c->alpha, box);
+  c->nk = (int)kv.size();
+  if (c->nk > c->nk_cap) {
+    if (c->d_kv) cudaFree(c->d_kv);
+    if (c->d_sk) cudaFree(c->d_sk);
+    CK(dalloc(&c->d_kv, (size_t)c->nk));
+    CK(dalloc(&c->d_sk, (size_t)c->nk * 4));
+    c->nk_cap = c->nk;
+  }
+  if (c->nk) CK(cudaMemcpyAsync(c->d_kv, kv.data(), sizeof(KVec) * c->nk, cudaMemcpyHostToDevice, c->stream));
+  int k1 = std::max(c->kmax[0], std::max(c->kmax[1], c->kmax[2])) + 1;
+  k1 = std::max(k1, 2);
+  const size_t tab = (size_t)3 * k1 * c->nm * c->S.na;
+  if (tab > c->tab_cap) {
+    if (c->d_tab) cudaFree(c->d_tab);
+    CK(dalloc(&c->d_tab, tab));
+    c->tab_cap = tab;
+  }
+  c->kv_box = box;
+  c->kv_alpha = c->alpha;
+  for (int a = 0; a < 3; a++) c->kv_kmax[a] = c->kmax[a];
+  return CCP_OK;
+}
+
+int ensure_host_io(ccp_context *c, size_t n) {
+  if (n <= c->h_io_cap) return CCP_OK;
+  if (c->h_io) cudaFreeHost(c->h_io);
+  c->h_io = nullptr;
+  CK(cudaMallocHost((void **)&c->h_io, n * sizeof(double)));
+  c->h_io_cap = n;
+  return CCP_OK;
+}
+
+struct EvalOut {
+  double sumff = 0, self_vir = 0, rc_e = 0, rc_vir = 0, kc_e = 0, kc_vir = 0;
+  double ind_e = 0, ind_vir = 0, fs2_e = 0, fs2_vir = 0, fs3_e = 0, fs3_vir = 0;
+  int iters = 0, ntri = 0, nblend = 0, nfs2 = 0;
+  bool converged = true;
+};
+
+#define LK(call)                                        \
+  do {                                                  \
+    c->launches++;                                      \
+    if (!cuda_ok((call), #call)) return CCP_ERR_CUDA;   \
+  } while (0)
+
+// Runs the enabled terms on inputs already in the context's device buffers
+// (x, y, z at px.., sites at pxs.. with leading dimension ld).
+int evaluate(ccp_context *c, const double *px, const double *py, const double *pz,
+             const double *pxs, const double *pys, const double *pzs, int ld, double box,
+             unsigned mask, EvalOut &o) {
+  cudaStream_t st = c->stream;
+  const int nm = c->nm, ns = c->ns;
+  const SiteSets &S = c->S;
+  if ((mask & (T_FS2 | T_FS3)) && !c->three_body) mask &= ~(T_FS2 | T_FS3);
+  if ((mask & T_FS2) && !c->s2) mask &= ~T_FS2;
+  if ((mask & T_FS3) && (!c->s3 || !c->have_fs3)) mask &= ~T_FS3;
+  if ((mask & T_FS3) && ns < kNs3) {
+    set_error("FS3 needs 17 sites per molecule");
+    return CCP_ERR_BAD_INPUT;
+  }
+  if ((mask & T_FS2) && ns < 5) {
+    set_error("FS2 needs 5 sites per molecule");
+    return CCP_ERR_BAD_INPUT;
+  }
+  EwaldParams P;
+  P.alpha = c->alpha;
+  P.rcutsd = c->rcutsd;
+  P.box = box;
+  P.twosqpi = 2.0 / std::sqrt(kPi);
+  P.delta2 = 1.65 / kBohr2a;
+  P.delta3 = 1.55 / kBohr2a;
+  P.damped = c->damped ? 1 : 0;
+  const double boxb = box / kBohr2a;
+  Fs3Params F3;
+  F3.boxb = boxb;
+  F3.rc2 = std::pow(6.3, 2.0) * std::pow(kBohr2a, -2.0);
+  F3.alp3 = c->alpha3 * kBohr2a;
+  F3.r0dmp = 6.20446 / kBohr2a;
+  F3.delta33 = c->delta33;
+  F3.rmin = 4.5 / kBohr2a;
+  F3.rmax = 5.5 / kBohr2a;
+  Fs2Params F2;
+  F2.boxb = boxb;
+  F2.rc2 = c->rcutsd3 * std::pow(kBohr2a, -2.0);
+  F2.alp3 = c->alpha3 * kBohr2a;
+  F2.r0dmp = 7.40446 / kBohr2a;
+  F2.delta33 = c->delta33;
+  if (mask & T_KSPACE || mask & T_INDUCTION) {
+    int r = ensure_kspace(c, box);
+    if (r) return r;
+  }
+  // neighbour-list radius covering every consumer (each re-tests with its exact cut-off)
+  double rl = c->rcut;
+  if (mask & T_FS3) rl = std::max(rl, 6.3);
+  if (mask & T_FS2) rl = std::max(rl, c->rcut3);
+  rl += 0.05;
+
+  auto mark = [&](int k) {
+    if (c->timing) cudaEventRecord(c->ev[k], st);
+  };
+  for (int attempt = 0; attempt < 3; attempt++) {
+    c->launches = 0;
+    mark(0);
+    LK(launch_prep(px, py, pz, pxs, pys, pzs, nm, ld, S, c->d_com, c->d_act, c->d_comb, c->d_s17,
+                   std::min(ns, kNs3), c->d_f, 3 * nm * ns, c->d_fc2, c->d_fc3, c->d_scal,
+                   c->d_icnt, st));
+    const bool need_nbr = mask & (T_RSPACE | T_INDUCTION | T_FS2 | T_FS3);
+    if (need_nbr)
+      LK(launch_neighbors(c->d_com, nm, box, rl * rl, c->cap, c->d_nbr, c->d_nbrv, c->d_ncnt,
+                          c->d_icnt, st));
+    mark(1);
+    if (mask & T_SELF)
+      LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_f, c->d_e0slf,
+                            c->d_scal, st));
+    if (mask & (T_RSPACE | T_INDUCTION)) {
+      // the real-space kernel produces Ewald forces and the static field together; when
+      // only one of the two is wanted the other output is discarded by zeroing below.
+      LK(launch_pair_static(c->d_com, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt, c->cap, nm, S, P,
+                            (mask & T_RSPACE) ? c->d_f : c->d_eir, c->d_e0r, c->d_e0s, c->d_scal,
+                            st));
+    }
+    mark(2);
+    if (mask & (T_KSPACE | T_INDUCTION))
+      LK(launch_ktab(c->d_com, c->d_act, nm, S, box, c->kmax[0], c->kmax[1], c->kmax[2], c->d_tab,
+                     st));
+    if (mask & T_KSPACE) {
+      LK(launch_kspace_sums(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
+                            c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+      LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                              c->kmax[2], c->d_mu, c->d_sk, c->alpha, nullptr, c->d_f, c->d_scal,
+                              st));
+    }
+    mark(3);
+    if (mask & T_INDUCTION) {
+      if (!(mask & T_SELF))
+        LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_eir, c->d_e0slf,
+                              c->d_scal, st));
+      LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
+                            c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+      LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                              c->kmax[2], c->d_mu, c->d_sk, c->alpha, c->d_e0k, c->d_f, c->d_scal,
+                              st));
+      if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, st));
+      CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * nm * S.np * 3, st));
+      int it = 0;
+      double change = 10.0;
+      while (change > 1.0e-20 && it < c->maxit) {
+        CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
+        LK(launch_pair_dipfield(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
+                                c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_eir, c->d_eis,
+                                c->d_eislf, st));
+        LK(launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                              c->kmax[2], c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+        LK(launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                                c->kmax[2], c->d_mu, c->d_sk, c->alpha, c->d_eik, c->d_f,
+                                c->d_scal, st));
+        LK(launch_dip_update(nm, S, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_eir, c->d_eik,
+                             c->d_eislf, c->d_eis, c->d_mu, c->d_scal, st));
+        CK(cudaMemcpyAsync(c->h_scal + S_IND_CHANGE, c->d_scal + S_IND_CHANGE, 2 * sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        change = c->h_scal[S_IND_CHANGE];
+        o.ind_e = c->h_scal[S_IND_ENERGY];
+        it++;
+      }
+      o.iters = it;
+      o.converged = it < c->maxit;
+      if (!o.converged) {
+        set_error("No convergence in the induced-dipole iteration (maxit reached)");
+        return CCP_ERR_NOT_CONVERGED;
+      }
+      LK(launch_pair_indforce(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
+                              c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_f, c->d_scal, st));
+      LK(launch_kspace_sums(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
+                            c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+      LK(launch_kspace_gather(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                              c->kmax[2], c->d_mu, c->d_sk, c->alpha, nullptr, c->d_f, c->d_scal,
+                              st));
+    }
+    mark(4);
+    if (mask & T_FS2) {
+      LK(launch_fs2_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F2, c->d_pairs, c->pair_cap,
+                         c->d_icnt, st));
+      LK(launch_fs2(c->precision, c->d_pairs, c->d_icnt, c->pair_cap, c->d_comb, c->d_s17, c->d_nbr,
+                    c->d_ncnt, c->cap, F2, nm, ns, c->d_f, c->d_fc2, c->d_scal, st));
+    }
+    mark(5);
+    if (mask & T_FS3)
+      LK(launch_fs3_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F3, c->d_tri, c->tri_cap,
+                         c->d_icnt, st));
+    mark(6);
+    if (mask & T_FS3) {
+      LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_comb, c->d_s17, F3,
+                    c->d_coef, c->d_bgr, c->d_types, nm, ns, c->d_f, c->d_fc3, c->d_scal, c->nsm,
+                    st));
+    }
+    mark(7);
+    CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_icnt, c->d_icnt, sizeof(int) * C_COUNT, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int *ic = c->h_icnt;
+    bool grow = false;
+    int ncap = c->cap, ntcap = c->tri_cap, npcap = c->pair_cap;
+    if (ic[C_OVERFLOW] > 0) {
+      ncap = std::min(nm, ic[C_OVERFLOW] + 32);
+      grow = true;
+    }
+    if (ic[C_NTRI_FS3] > c->tri_cap) {
+      ntcap = ic[C_NTRI_FS3] + ic[C_NTRI_FS3] / 4 + 64;
+      grow = true;
+    }
+    if (ic[C_NPAIR_FS2] > c->pair_cap) {
+      npcap = ic[C_NPAIR_FS2] + ic[C_NPAIR_FS2] / 4 + 64;
+      grow = true;
+    }
+    if (grow) {
+      int r = ensure_lists(c, ncap, ntcap, npcap);
+      if (r) return r;
+      continue;
+    }
+    if (c->timing)
+      for (int k = 0; k < CCP_NPHASE; k++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
+        c->phase_ms[k] = ms;
+      }
+    const double *h = c->h_scal;
+    o.sumff = h[S_SELF_SUMFF];
+    o.self_vir = h[S_SELF_VIR];
+    o.rc_e = h[S_RC_E];
+    o.rc_vir = h[S_RC_VIR];
+    o.kc_e = h[S_KC_E];
+    o.kc_vir = h[S_KC_VIR];
+    o.ind_vir = h[S_IND_VIR_R] + 2.0 * kR4pie0 * h[S_IND_VIR_K];
+    o.fs2_e = h[S_FS2_E];
+    o.fs2_vir = h[S_FS2_VIR];
+    o.fs3_e = h[S_FS3_E];
+    o.fs3_vir = h[S_FS3_VIR];
+    o.ntri = ic[C_NTRI_FS3];
+    o.nblend = ic[C_NBLEND_FS3];
+    o.nfs2 = ic[C_NTRI_FS2];
+    return CCP_OK;
+  }
+  set_error("internal list capacity kept overflowing");
+  return CCP_ERR_CAPACITY;
+}
+
+int check_args(ccp_context *c, const void *const *ptrs, int n, int ld) {
+  if (!c) {
+    set_error("null context");
+    return CCP_ERR_BAD_INPUT;
+  }
+  for (int k = 0; k < n; k++)
+    if (!ptrs[k]) {
+      set_error("null array argument");
+      return CCP_ERR_BAD_INPUT;
+    }
+  if (ld < c->ns) {
+    set_error("leading dimension ld is smaller than the number of sites");
+    return CCP_ERR_BAD_INPUT;
+  }
+  return CCP_OK;
+}
+
+// Upload the caller's host arrays (through pinned staging) into the context buffers.
+int upload(ccp_context *c, const double *x, const double *y, const double *z, const double *xs,
+           const double *ys, const double *zs, int ld) {
+  int r = ensure_inputs(c, ld);
+  if (r) return r;
+  const size_t nm = c->nm, ns = (size_t)nm * ld;
+  r = ensure_host_io(c, 3 * nm + 3 * ns);
+  if (r) return r;
+  double *h = c->h_io;
+  std::memcpy(h, x, nm * sizeof(double));
+  std::memcpy(h + nm, y, nm * sizeof(double));
+  std::memcpy(h + 2 * nm, z, nm * sizeof(double));
+  std::memcpy(h + 3 * nm, xs, ns * sizeof(double));
+  std::memcpy(h + 3 * nm + ns, ys, ns * sizeof(double));
+  std::memcpy(h + 3 * nm + 2 * ns, zs, ns * sizeof(double));
+  cudaStream_t st = c->stream;
+  CK(cudaMemcpyAsync(c->d_x, h, nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_y, h + nm, nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_z, h + 2 * nm, nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_xs, h + 3 * nm, ns * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_ys, h + 3 * nm + ns, ns * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_zs, h + 3 * nm + 2 * ns, ns * sizeof(double), cudaMemcpyHostToDevice, st));
+  return CCP_OK;
+}
+
+// Download the compact site forces and add them into the caller's (ld-layout) arrays.
+int download_forces(ccp_context *c, int ld, double *fxs, double *fys, double *fzs) {
+  if (!fxs && !fys && !fzs) return CCP_OK;
+  const size_t n = (size_t)c->nm * c->ns;
+  int r = ensure_host_io(c, 3 * n);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->h_io, c->d_f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double *out[3] = {fxs, fys, fzs};
+  for (int a = 0; a < 3; a++) {
+    if (!out[a]) continue;
+    const double *src = c->h_io + a * n;
+    for (int i = 0; i < c->nm; i++)
+      for (int s = 0; s < c->ns; s++) out[a][(size_t)i * ld + s] += src[(size_t)i * c->ns + s];
+  }
+  return CCP_OK;
+}
+
+int download_com(ccp_context *c, const double *d, double *fx, double *fy, double *fz) {
+  if (!fx && !fy && !fz) return CCP_OK;
+  const size_t nm = c->nm;
+  int r = ensure_host_io(c, 3 * nm);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->h_io, d, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (fx) std::memcpy(fx, c->h_io, nm * sizeof(double));
+  if (fy) std::memcpy(fy, c->h_io + nm, nm * sizeof(double));
+  if (fz) std::memcpy(fz, c->h_io + 2 * nm, nm * sizeof(double));
+  return CCP_OK;
+}
+
+int download_dipoles(ccp_context *c, int ld, double *mx, double *my, double *mz) {
+  if (!mx && !my && !mz) return CCP_OK;
+  const size_t n = (size_t)c->nm * c->S.np * 3;
+  int r = ensure_host_io(c, n);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->h_io, c->d_mu, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double *out[3] = {mx, my, mz};
+  for (int a = 0; a < 3; a++) {
+    if (!out[a]) continue;
+    for (int i = 0; i < c->nm; i++) {
+      for (int s = 0; s < c->ns; s++) out[a][(size_t)i * ld + s] = 0.0;
+      for (int p = 0; p < c->S.np; p++)
+        out[a][(size_t)i * ld + c->S.psite[p]] = c->h_io[((size_t)i * c->S.np + p) * 3 + a];
+    }
+  }
+  return CCP_OK;
+}
+
+double self_point_energy(const ccp_context *c, double alp, double box) {
+  // ewald.f90:79-88: -pi (sum q / alpha)^2 / (2 V) - alpha sum q^2 / sqrt(pi)
+  const double t = c->sumq / alp;
+  double e = -kPi * (t * t) / (2.0 * box * box * box);
+  e = e - alp * c->sumq2 / std::sqrt(kPi);
+  return e;
+}
+
+void fill_energies(ccp_context *c, const EvalOut &o, double box, ccp_energies *e) {
+  e->scpe = kR4pie0 * (self_point_energy(c, c->alpha, box) - o.sumff) / 418.4;
+  e->rcpe = o.rc_e / 418.4;
+  e->kcpe = 2.0 * kR4pie0 * o.kc_e / 418.4;
+  e->indpe = kR4pie0 * o.ind_e / 418.4;
+  e->fs2pe = o.fs2_e * kH2kcal;
+  e->fs3pe = o.fs3_e * kH2kcal;
+  e->vir = o.self_vir + o.rc_vir + 2.0 * kR4pie0 * o.kc_vir + o.ind_vir +
+           o.fs2_vir * kH2kcal * 418.4 + o.fs3_vir * kH2kcal * 418.4;
+  e->ind_iters = o.iters;
+  e->n_fs3_triples = o.ntri;
+  e->n_fs3_blend = o.nblend;
+  e->n_fs2_triples = o.nfs2;
+}
+
+unsigned hot_mask(const ccp_context *c) {
+  unsigned m = T_SELF | T_RSPACE | T_KSPACE;
+  if (c->induction) m |= T_INDUCTION;
+  if (c->three_body) m |= T_FS2 | T_FS3;
+  return m;
+}
+
+__global__ void k_scatter_out(const double *__restrict__ f, int nm, int ns, int ld, double *fx,
+                              double *fy, double *fz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = nm * ns;
+  if (t >= n) return;
+  const int i = t / ns, s = t % ns;
+  const size_t o = (size_t)i * ld + s;
+  if (fx) fx[o] += f[t];
+  if (fy) fy[o] += f[(size_t)n + t];
+  if (fz) fz[o] += f[2 * (size_t)n + t];
+}
+
+__global__ void k_scatter_dip(const double *__restrict__ mu, int nm, int ns, int np, int p0,
+                              int ld, double *mx, double *my, double *mz) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nm * ns) return;
+  const int i = t / ns, s = t % ns;
+  const int p = s - p0;
+  const size_t o = (size_t)i * ld + s;
+  double v[3] = {0, 0, 0};
+  if (p >= 0 && p < np)
+    for (int a = 0; a < 3; a++) v[a] = mu[((size_t)i * np + p) * 3 + a];
+  if (mx) mx[o] = v[0];
+  if (my) my[o] = v[1];
+  if (mz) mz[o] = v[2];
+}
+
+}  // namespace
+
+extern "C" {
+
+int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int precision,
+                       ccp_context **out) {
+  if (!m || !out || nm < 3 || !(box0 > 0.0) || (precision != CCP_FP64 && precision != CCP_MIXED)) {
+    set_error("ccp_context_create: bad argument");
+    return CCP_ERR_BAD_INPUT;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("no CUDA device");
+    return CCP_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("device ordinal out of range");
+    return CCP_ERR_BAD_INPUT;
+  }
+  auto *c = new ccp_context();
+  c->device = device;
+  c->precision = precision;
+  c->nm = nm;
+  c->ns = m->ns;
+  c->npol = m->npol;
+  if (!cuda_ok(cudaSetDevice(device), "cudaSetDevice")) {
+    delete c;
+    return CCP_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->nsm = prop.multiProcessorCount;
+  // site sets from the model's charges and polarisabilities
+  SiteSets &S = c->S;
+  std::memset(&S, 0, sizeof(S));
+  S.ns = m->ns;
+  const int p0 = m->ns - m->npol;
+  for (int s = 0; s < m->ns; s++) c->charge[s] = m->charge[s];
+  for (int s = 0; s < m->ns; s++) {
+    const bool q = m->charge[s] != 0.0;
+    const bool pol = s >= p0;
+    if (!q && !pol) continue;
+    if (S.na >= ccpd::kMaxA || (q && S.nq >= ccpd::kMaxQ) || (pol && S.np >= ccpd::kMaxP)) {
+      set_error("too many charged/polarisable sites per molecule");
+      delete c;
+      return CCP_ERR_BAD_INPUT;
+    }
+    const int a = S.na++;
+    S.asite[a] = s;
+    S.q[a] = m->charge[s];
+    S.p_of_a[a] = -1;
+    if (q) {
+      S.qsite[S.nq] = s;
+      S.a_of_q[S.nq] = a;
+      if (s < p0) S.self_q[S.nself_q++] = S.nq;
+      S.nq++;
+    }
+    if (pol) {
+      S.psite[S.np] = s;
+      S.a_of_p[S.np] = a;
+      S.apol[S.np] = m->polarizability[s] * std::pow(kBohr2a, 3.0);
+      S.p_of_a[a] = S.np;
+      S.np++;
+    }
+  }
+  c->sumq = 0;
+  c->sumq2 = 0;
+  for (int i = 0; i < nm; i++)
+    for (int s = 0; s < m->ns; s++) {
+      c->sumq = c->sumq + m->charge[s];
+      c->sumq2 = c->sumq2 + m->charge[s] * m->charge[s];
+    }
+  c->rcut = m->rcut;
+  c->rcutsd = m->rcut * m->rcut;
+  c->rcut3 = m->rcut3;
+  c->rcutsd3 = m->rcut3 * m->rcut3;
+  c->alpha3 = m->alpha3;
+  c->delta33 = m->delta33;
+  c->s2 = m->s2_term;
+  c->s3 = m->s3_term;
+  c->three_body = m->nonadditive_3b;
+  c->induction = m->induction && m->ind_model == "point_dipole";
+  c->damped = m->induction_type == "damped";
+  c->have_fs3 = m->have_fs3;
+  ccp_ewald_setup(kEwp, m->rcut, box0, &c->alpha, &c->kmax[0], &c->kmax[1], &c->kmax[2]);
+
+  auto fail = [&](const char *what) {
+    set_error(std::string("ccp_context_create: ") + what + ": " + cudaGetErrorString(cudaGetLastError()));
+    free_ctx(c);
+    delete c;
+    return CCP_ERR_CUDA;
+  };
+  if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) return fail("stream");
+  c->stream = c->own;
+  const size_t n = nm, nsi = (size_t)nm * m->ns, np3 = (size_t)nm * std::max(S.np, 1) * 3;
+  bool ok = dalloc(&c->d_x, n) == cudaSuccess && dalloc(&c->d_y, n) == cudaSuccess &&
+            dalloc(&c->d_z, n) == cudaSuccess && dalloc(&c->d_com, n) == cudaSuccess &&
+            dalloc(&c->d_comb, n) == cudaSuccess &&
+            dalloc(&c->d_act, n * std::max(S.na, 1)) == cudaSuccess &&
+            dalloc(&c->d_s17, n * kNs3) == cudaSuccess && dalloc(&c->d_f, 3 * nsi) == cudaSuccess &&
+            dalloc(&c->d_fc2, 3 * n) == cudaSuccess && dalloc(&c->d_fc3, 3 * n) == cudaSuccess &&
+            dalloc(&c->d_scal, (size_t)S_COUNT) == cudaSuccess &&
+            dalloc(&c->d_icnt, (size_t)C_COUNT) == cudaSuccess &&
+            dalloc(&c->d_mu, np3) == cudaSuccess && dalloc(&c->d_e0r, np3) == cudaSuccess &&
+            dalloc(&c->d_e0k, np3) == cudaSuccess && dalloc(&c->d_e0slf, np3) == cudaSuccess &&
+            dalloc(&c->d_e0s, np3) == cudaSuccess && dalloc(&c->d_eir, std::max(np3, 3 * nsi)) == cudaSuccess &&
+            dalloc(&c->d_eik, np3) == cudaSuccess && dalloc(&c->d_eislf, np3) == cudaSuccess &&
+            dalloc(&c->d_eis, np3) == cudaSuccess && dalloc(&c->d_ncnt, n) == cudaSuccess;
+  if (!ok) return fail("device allocation");
+  if (cudaMemset(c->d_e0s, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
+  if (cudaMemset(c->d_mu, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
+  if (cudaMallocHost((void **)&c->h_scal, sizeof(double) * S_COUNT) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_icnt, sizeof(int) * C_COUNT) != cudaSuccess)
+    return fail("pinned allocation");
+  if (ensure_inputs(c, m->ns) != CCP_OK) return fail("inputs");
+  const int cap0 = std::min(nm - 1, 192);
+  if (ensure_lists(c, std::max(cap0, 1), 96 * nm, 48 * nm) != CCP_OK) return fail("lists");
+  if (m->have_fs3) {
+    std::vector<double> coef(2 * m->coef_sr.size());
+    std::copy(m->coef_sr.begin(), m->coef_sr.end(), coef.begin());
+    std::copy(m->coef_lr.begin(), m->coef_lr.end(), coef.begin() + m->coef_sr.size());
+    std::vector<double> bgr(2 * 3 * 289);
+    for (int q = 0; q < 289; q++) {
+      bgr[0 * 289 + q] = m->sr.b[q];
+      bgr[1 * 289 + q] = m->sr.g[q];
+      bgr[2 * 289 + q] = m->sr.r0[q];
+      bgr[3 * 289 + q] = m->lr.b[q];
+      bgr[4 * 289 + q] = m->lr.g[q];
+      bgr[5 * 289 + q] = m->lr.r0[q];
+    }
+    if (dalloc(&c->d_coef, coef.size()) != cudaSuccess || dalloc(&c->d_bgr, bgr.size()) != cudaSuccess ||
+        dalloc(&c->d_types, (size_t)kNs3) != cudaSuccess)
+      return fail("FS3 tables");
+    if (cudaMemcpy(c->d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_bgr, bgr.data(), bgr.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_types, m->fs3_type, kNs3 * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail("FS3 upload");
+  }
+  *out = c;
+  return CCP_OK;
+}
+
+int ccp_context_destroy(ccp_context *ctx) {
+  if (!ctx) return CCP_ERR_BAD_INPUT;
+  free_ctx(ctx);
+  delete ctx;
+  return CCP_OK;
+}
+
+int ccp_context_set_ewald(ccp_context *ctx, double alpha, int k1, int k2, int k3) {
+  if (!ctx || !(alpha > 0.0) || k1 < 1 || k2 < 1 || k3 < 1) {
+    set_error("ccp_context_set_ewald: bad argument");
+    return CCP_ERR_BAD_INPUT;
+  }
+  ctx->alpha = alpha;
+  ctx->kmax[0] = k1;
+  ctx->kmax[1] = k2;
+  ctx->kmax[2] = k3;
+  return CCP_OK;
+}
+
+int ccp_context_set_maxit(ccp_context *ctx, int maxit) {
+  if (!ctx || maxit < 1) {
+    set_error("ccp_context_set_maxit: bad argument");
+    return CCP_ERR_BAD_INPUT;
+  }
+  ctx->maxit = maxit;
+  return CCP_OK;
+}
+
+int ccp_context_set_stream(ccp_context *ctx, void *stream) {
+  if (!ctx) return CCP_ERR_BAD_INPUT;
+  ctx->stream = stream ? (cudaStream_t)stream : ctx->own;
+  return CCP_OK;
+}
+
+int ccp_context_set_timing(ccp_context *ctx, int on) {
+  if (!ctx) return CCP_ERR_BAD_INPUT;
+  CK(cudaSetDevice(ctx->device));
+  if (on && !ctx->ev[0])
+    for (auto &e : ctx->ev) CK(cudaEventCreate(&e));
+  ctx->timing = on != 0;
+  return CCP_OK;
+}
+
+int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n) {
+  if (!ctx || !ms || n < 1 || n > CCP_NPHASE) return CCP_ERR_BAD_INPUT;
+  for (int k = 0; k < n; k++) ms[k] = ctx->phase_ms[k];
+  return CCP_OK;
+}
+
+int ccp_context_last_launches(const ccp_context *ctx, int *launches) {
+  if (!ctx || !launches) return CCP_ERR_BAD_INPUT;
+  *launches = ctx->launches;
+  return CCP_OK;
+}
+
+int ccp_ewald_self_correction(ccp_context *ctx, double alp, double box, const double *x,
+                              const double *y, const double *z, const double *xs,
+                              const double *ys, const double *zs, int ld, double *qscpe,
+                              double *fxs, double *fys, double *fzs, double *vir) {
+  const void *p[] = {x, y, z, xs, ys, zs, qscpe, fxs, fys, fzs, vir};
+  int r = check_args(ctx, p, 11, ld);
+  if (r) return r;
+  CK(cudaSetDevice(ctx->device));
+  const double keep = ctx->alpha;
+  ctx->alpha = alp;
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, T_SELF, o);
+  if (!r) r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r) {
+    *qscpe = kR4pie0 * (self_point_energy(ctx, alp, box) - o.sumff) / 418.4;
+    *vir += o.self_vir;
+  }
+  ctx->alpha = keep;
+  return r;
+}
+
+int ccp_rspace_ewald(ccp_context *ctx, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld, double box,
+                     double alp, double *qrcpe, double *fxs, double *fys, double *fzs,
+                     double *vir) {
+  const void *p[] = {x, y, z, xs, ys, zs, qrcpe, fxs, fys, fzs, vir};
+  int r = check_args(ctx, p, 11, ld);
+  if (r) return r;
+  CK(cudaSetDevice(ctx->device));
+  const double keep = ctx->alpha;
+  ctx->alpha = alp;
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, T_RSPACE, o);
+  if (!r) r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r) {
+    *qrcpe = o.rc_e / 418.4;
+    *vir += o.rc_vir;
+  }
+  ctx->alpha = keep;
+  return r;
+}
+
+int ccp_kspace_ewald(ccp_context *ctx, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld, int lmax,
+                     int mmax, int nmax, double alp, double box, double *qkcpe, double *fxs,
+                     double *fys, double *fzs, double *vir) {
+  const void *p[] = {x, y, z, xs, ys, zs, qkcpe, fxs, fys, fzs, vir};
+  int r = check_args(ctx, p, 11, ld);
+  if (r) return r;
+  if (lmax < 1 || mmax < 1 || nmax < 1) {
+    set_error("kspace_ewald: k-max must be >= 1");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const double keep = ctx->alpha;
+  int kk[3] = {ctx->kmax[0], ctx->kmax[1], ctx->kmax[2]};
+  ctx->alpha = alp;
+  ctx->kmax[0] = lmax;
+  ctx->kmax[1] = mmax;
+  ctx->kmax[2] = nmax;
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, T_KSPACE, o);
+  if (!r) r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r) {
+    *qkcpe = 2.0 * kR4pie0 * o.kc_e / 418.4;
+    *vir += 2.0 * kR4pie0 * o.kc_vir;
+  }
+  ctx->alpha = keep;
+  for (int a = 0; a < 3; a++) ctx->kmax[a] = kk[a];
+  return r;
+}
+
+int ccp_nb_induction(ccp_context *ctx, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld, double box,
+                     double *qindpe, double *idmx, double *idmy, double *idmz, double *fxs,
+                     double *fys, double *fzs, double *vir, int *iters) {
+  const void *p[] = {x, y, z, xs, ys, zs, qindpe, idmx, idmy, idmz, fxs, fys, fzs, vir};
+  int r = check_args(ctx, p, 14, ld);
+  if (r) return r;
+  CK(cudaSetDevice(ctx->device));
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, T_INDUCTION, o);
+  if (iters) *iters = o.iters;
+  if (r) return r;
+  r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r) r = download_dipoles(ctx, ld, idmx, idmy, idmz);
+  if (!r) {
+    *qindpe = kR4pie0 * o.ind_e / 418.4;
+    *vir += o.ind_vir;
+  }
+  return r;
+}
+
+int ccp_threebody_term(ccp_context *ctx, const double *x, const double *y, const double *z,
+                       const double *xs, const double *ys, const double *zs, int ld,
+                       double box, double *qfs2, double *qfs3, double *fxs, double *fys,
+                       double *fzs, double *fxfs2, double *fyfs2, double *fzfs2,
+                       double *fxfs3, double *fyfs3, double *fzfs3, double *vir) {
+  const void *p[] = {x, y, z, xs, ys, zs, qfs2, qfs3, fxs, fys, fzs, vir};
+  int r = check_args(ctx, p, 12, ld);
+  if (r) return r;
+  CK(cudaSetDevice(ctx->device));
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, T_FS2 | T_FS3, o);
+  if (r) return r;
+  r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r && ctx->three_body && ctx->s2) r = download_com(ctx, ctx->d_fc2, fxfs2, fyfs2, fzfs2);
+  if (!r && ctx->three_body && ctx->s3) r = download_com(ctx, ctx->d_fc3, fxfs3, fyfs3, fzfs3);
+  if (!r) {
+    if (ctx->three_body && ctx->s2) *qfs2 = o.fs2_e * kH2kcal;
+    if (ctx->three_body && ctx->s3) *qfs3 = o.fs3_e * kH2kcal;
+    *vir += (o.fs2_vir + o.fs3_vir) * kH2kcal * 418.4;
+  }
+  return r;
+}
+
+int ccp_hot_path(ccp_context *ctx, const double *x, const double *y, const double *z,
+                 const double *xs, const double *ys, const double *zs, int ld, double box,
+                 ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
+                 double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3, double *fzfs3,
+                 double *idmx, double *idmy, double *idmz) {
+  const void *p[] = {x, y, z, xs, ys, zs, e};
+  int r = check_args(ctx, p, 7, ld);
+  if (r) return r;
+  CK(cudaSetDevice(ctx->device));
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, hot_mask(ctx), o);
+  if (r) return r;
+  fill_energies(ctx, o, box, e);
+  r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r) r = download_com(ctx, ctx->d_fc2, fxfs2, fyfs2, fzfs2);
+  if (!r) r = download_com(ctx, ctx->d_fc3, fxfs3, fyfs3, fzfs3);
+  if (!r) r = download_dipoles(ctx, ld, idmx, idmy, idmz);
+  return r;
+}
+
+int ccp_hot_path_device(ccp_context *ctx, const double *x, const double *y, const double *z,
+                        const double *xs, const double *ys, const double *zs, int ld, double box,
+                        ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
+                        double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3,
+                        double *fzfs3, double *idmx, double *idmy, double *idmz) {
+  const void *p[] = {x, y, z, xs, ys, zs, e};
+  int r = check_args(ctx, p, 7, ld);
+  if (r) return r;
+  CK(cudaSetDevice(ctx->device));
+  EvalOut o;
+  r = evaluate(ctx, x, y, z, xs, ys, zs, ld, box, hot_mask(ctx), o);
+  if (r) return r;
+  fill_energies(ctx, o, box, e);
+  cudaStream_t st = ctx->stream;
+  const int n = ctx->nm * ctx->ns;
+  if (fxs || fys || fzs) {
+    k_scatter_out<<<(n + 255) / 256, 256, 0, st>>>(ctx->d_f, ctx->nm, ctx->ns, ld, fxs, fys, fzs);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
+  const size_t nb = (size_t)ctx->nm * sizeof(double);
+  double *c2[3] = {fxfs2, fyfs2, fzfs2}, *c3[3] = {fxfs3, fyfs3, fzfs3};
+  for (int a = 0; a < 3; a++) {
+    if (c2[a]) CK(cudaMemcpyAsync(c2[a], ctx->d_fc2 + (size_t)a * ctx->nm, nb, cudaMemcpyDeviceToDevice, st));
+    if (c3[a]) CK(cudaMemcpyAsync(c3[a], ctx->d_fc3 + (size_t)a * ctx->nm, nb, cudaMemcpyDeviceToDevice, st));
+  }
+  if (idmx || idmy || idmz) {
+    k_scatter_dip<<<(n + 255) / 256, 256, 0, st>>>(ctx->d_mu, ctx->nm, ctx->ns, ctx->S.np,
+                                                   ctx->ns - ctx->npol, ld, idmx, idmy, idmz);
+    ctx->launches++;
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(st));
+  return CCP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,193 @@
+// ccp_device.cuh -- device-side helpers and the kernel interface of the hot path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ccpd {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr double kR4pie0 = 138935.4835;
+constexpr double kBohr2a = 0.529177249;
+constexpr double kH2kcal = 627.510;
+constexpr int kNs3 = 17;
+constexpr int kMaxQ = 8;   // charged sites per molecule
+constexpr int kMaxP = 4;   // polarisable sites per molecule
+constexpr int kMaxA = 12;  // charged or polarisable ("active") sites per molecule
+
+// ---- exact IEEE arithmetic for the decisions that must match the reference bit for bit
+// (minimum image, COM cut-offs, R_avg branch).  __d*_rn never fuse into FMA.
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+// d - box*nint(d/box), Fortran nint rounds half away from zero like round().
+__device__ __forceinline__ double minimg(double d, double box) {
+  return xsub(d, xmul(box, round(__ddiv_rn(d, box))));
+}
+__device__ __forceinline__ double norm2x(double x, double y, double z) {
+  return xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Tang-Toennies f_n(delta r) and derivative (utility.f90:89-125), n small and fixed.
+template <int N>
+__device__ __forceinline__ double tt(double delta, double r) {
+  double dr = delta * r, term = 1.0, sum = 1.0;
+#pragma unroll
+  for (int i = 1; i <= N; i++) {
+    term = term * dr / (double)i;
+    sum += term;
+  }
+  return 1.0 - exp(-dr) * sum;
+}
+template <int N>
+__device__ __forceinline__ double dtt(double delta, double r) {
+  double f = 1.0, dr = delta * r, p = 1.0;
+#pragma unroll
+  for (int i = 1; i <= N; i++) {
+    f *= (double)i;
+    p *= dr;
+  }
+  return delta * exp(-dr) * p / f;
+}
+
+}  // namespace ccpd
+
+// Scalar accumulator slots (doubles) in ctx->d_scal.
+enum ScalSlot {
+  S_SELF_SUMFF = 0,  // ewald intramolecular sum erf(a r) q q / r
+  S_SELF_VIR,
+  S_RC_E,
+  S_RC_VIR,
+  S_KC_E,
+  S_KC_VIR,
+  S_IND_CHANGE,
+  S_IND_ENERGY,
+  S_IND_VIR_R,
+  S_IND_VIR_K,
+  S_IND_VIR_S,
+  S_IND_VIR_SHT,
+  S_FS2_E,
+  S_FS2_VIR,
+  S_FS3_E,
+  S_FS3_VIR,
+  S_COUNT
+};
+
+// Integer counters in ctx->d_icnt.
+enum CountSlot {
+  C_NPAIR_FS2 = 0,
+  C_NTRI_FS3,
+  C_NBLEND_FS3,
+  C_NTRI_FS2,
+  C_OVERFLOW,
+  C_COUNT
+};
+
+// Model constants the kernels need, passed by value.
+struct SiteSets {
+  int ns, nq, np, na;
+  int qsite[ccpd::kMaxQ];    // site index of each charged site
+  int psite[ccpd::kMaxP];    // site index of each polarisable site (last npol sites)
+  int asite[ccpd::kMaxA];    // site index of each active site
+  int a_of_q[ccpd::kMaxQ];   // active slot of each charged site
+  int a_of_p[ccpd::kMaxP];   // active slot of each polarisable site
+  int p_of_a[ccpd::kMaxA];   // polarisable slot of each active site (-1 if none)
+  double q[ccpd::kMaxA];     // charge of each active site
+  double apol[ccpd::kMaxP];  // polarizability*bohr2a^3 of each polarisable site (A^3)
+  int nself_q;               // charged sites outside the last npol (self field sources)
+  int self_q[ccpd::kMaxQ];   // their charged-slot indices
+};
+
+struct EwaldParams {
+  double alpha, rcutsd, box, twosqpi, delta2, delta3;
+  int damped;
+};
+
+struct Fs3Params {
+  double boxb, rc2, alp3, r0dmp, delta33, rmin, rmax;
+};
+
+struct Fs2Params {
+  double boxb, rc2, alp3, r0dmp, delta33;
+};
+
+// ------------------------------------------------------------------ launchers
+// All launchers enqueue on `st` and return cudaGetLastError().
+cudaError_t launch_prep(const double *x, const double *y, const double *z, const double *xs,
+                        const double *ys, const double *zs, int nm, int ld, SiteSets S,
+                        double4 *com, double4 *act, double4 *comb, double4 *s17, int ns3,
+                        double *f, int nf, double *fc2, double *fc3, double *scal,
+                        int *icnt, cudaStream_t st);
+cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
+                             int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st);
+cudaError_t launch_pair_static(const double4 *com, const double4 *act, const int *nbr,
+                               const double4 *nbrv, const int *ncnt, int cap, int nm,
+                               SiteSets S, EwaldParams P, double *f, double *e0r,
+                               double *e0s, double *scal, cudaStream_t st);
+cudaError_t launch_self_static(const double *x, const double *y, const double *z,
+                               const double *xs, const double *ys, const double *zs, int nm,
+                               int ld, SiteSets S, EwaldParams P, double *f, double *e0slf,
+                               double *scal, cudaStream_t st);
+cudaError_t launch_pair_dipfield(const double *x, const double *y, const double *z,
+                                 const double *xs, const double *ys, const double *zs,
+                                 int ld, const double4 *act, const int *nbr,
+                                 const double4 *nbrv, const int *ncnt, int cap, int nm,
+                                 SiteSets S, EwaldParams P, const double *mu, double *eir,
+                                 double *eis, double *eislf, cudaStream_t st);
+cudaError_t launch_dip_update(int nm, SiteSets S, const double *e0r, const double *e0k,
+                              const double *e0slf, const double *e0s, const double *eir,
+                              const double *eik, const double *eislf, const double *eis,
+                              double *mu, double *scal, cudaStream_t st);
+cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,
+                                 const double *xs, const double *ys, const double *zs,
+                                 int ld, const double4 *act, const int *nbr,
+                                 const double4 *nbrv, const int *ncnt, int cap, int nm,
+                                 SiteSets S, EwaldParams P, const double *mu, double *f,
+                                 double *scal, cudaStream_t st);
+
+// reciprocal space
+struct KVec {
+  double rl, rm, rn, ak;  // 2*pi*(l,m,n)/L and a(k)
+  int l, m, n, pad;
+};
+cudaError_t launch_ktab(const double4 *com, const double4 *act, int nm, SiteSets S,
+                        double box, int kmax_l, int kmax_m, int kmax_n, double2 *tab,
+                        cudaStream_t st);
+// mode: 0 Ewald (charged sites: energy, virial, forces)
+//       1 static field at polarisable sites from charges
+//       2 dipole field at polarisable sites
+//       3 induction forces at active sites
+cudaError_t launch_kspace_sums(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
+                               SiteSets S, int kl, int km, int kn, const double *mu,
+                               double *sk, double *scal, double alpha, cudaStream_t st);
+cudaError_t launch_kspace_gather(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
+                                 SiteSets S, int kl, int km, int kn, const double *mu,
+                                 const double *sk, double alpha, double *out, double *f,
+                                 double *scal, cudaStream_t st);
+
+// three-body
+cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
+                            int nm, Fs3Params P, int4 *tri, int tri_cap, int *icnt,
+                            cudaStream_t st);
+cudaError_t launch_fs3(int precision, const int4 *tri, const int *icnt, int tri_cap,
+                       const double4 *comb, const double4 *s17, Fs3Params P,
+                       const double *coef, const double *bgr, const int *types, int nm, int ns,
+                       double *f, double *fc3, double *scal, int nsm, cudaStream_t st);
+cudaError_t launch_fs2_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
+                            int nm, Fs2Params P, int2 *pairs, int pair_cap, int *icnt,
+                            cudaStream_t st);
+cudaError_t launch_fs2(int precision, const int2 *pairs, const int *icnt, int pair_cap,
+                       const double4 *comb, const double4 *s17, const int *nbr,
+                       const int *ncnt, int cap, Fs2Params P, int nm, int ns, double *f,
+                       double *fc2, double *scal, cudaStream_t st);

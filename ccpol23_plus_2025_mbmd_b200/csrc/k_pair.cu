@@ -1,0 +1,774 @@
+// k_pair.cu -- molecule-pair kernels of the hot path (sm_100a, FP64).
+//
+// One warp owns one molecule i and walks i's neighbour list; every quantity it produces
+// belongs to i's own sites, so site forces and fields are written without atomics.  Each
+// unordered pair is therefore visited from both sides; energies and virials are counted
+// on the side with j > i only, which reproduces the reference's `do j = i+1, nm` sums.
+// Only "active" sites enter (charged or polarisable): the reference loops over all 28x28
+// site pairs, but every other pair multiplies by a zero charge and a zero dipole.
+#include "ccp_device.cuh"
+
+using namespace ccpd;
+
+namespace {
+
+constexpr int kWarpsPerBlock = 4;
+
+__device__ __forceinline__ double4 ld4(const double4 *p) { return *p; }
+
+// ------------------------------------------------------------------------ prep
+__global__ void k_prep(const double *__restrict__ x, const double *__restrict__ y,
+                       const double *__restrict__ z, const double *__restrict__ xs,
+                       const double *__restrict__ ys, const double *__restrict__ zs, int nm,
+                       int ld, SiteSets S, double4 *com, double4 *act, double4 *comb,
+                       double4 *s17, int ns3, double *f, int nf, double *fc2, double *fc3,
+                       double *scal, int *icnt) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  int stride = gridDim.x * blockDim.x;
+  for (int i = t; i < nm; i += stride) {
+    com[i] = make_double4(x[i], y[i], z[i], 0.0);
+    comb[i] = make_double4(x[i] / kBohr2a, y[i] / kBohr2a, z[i] / kBohr2a, 0.0);
+    for (int a = 0; a < S.na; a++) {
+      size_t o = (size_t)i * ld + S.asite[a];
+      act[(size_t)i * S.na + a] = make_double4(xs[o], ys[o], zs[o], S.q[a]);
+    }
+    for (int s = 0; s < ns3; s++) {
+      size_t o = (size_t)i * ld + s;
+      s17[(size_t)i * kNs3 + s] =
+          make_double4(xs[o] / kBohr2a, ys[o] / kBohr2a, zs[o] / kBohr2a, 0.0);
+    }
+    fc2[i] = fc2[nm + i] = fc2[2 * nm + i] = 0.0;
+    fc3[i] = fc3[nm + i] = fc3[2 * nm + i] = 0.0;
+  }
+  for (int k = t; k < nf; k += stride) f[k] = 0.0;
+  if (t < S_COUNT) scal[t] = 0.0;
+  if (t < C_COUNT) icnt[t] = 0;
+}
+
+// ------------------------------------------------------------------- neighbours
+// One block per molecule i: candidates j != i with the reference's minimum-image COM
+// vector (computed exactly as the reference does) and |r|^2 < rlist2, written in
+// increasing j.
+__global__ void k_neighbors(const double4 *__restrict__ com, int nm, double box,
+                            double rlist2, int cap, int *nbr, double4 *nbrv, int *ncnt,
+                            int *icnt) {
+  __shared__ int warp_tot[32];
+  __shared__ int base;
+  const int i = blockIdx.x;
+  if (threadIdx.x == 0) base = 0;
+  __syncthreads();
+  const double4 ci = com[i];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int j0 = 0; j0 < nm; j0 += blockDim.x) {
+    int j = j0 + threadIdx.x;
+    bool keep = false;
+    double4 v;
+    if (j < nm && j != i) {
+      double4 cj = com[j];
+      double xcc = minimg(xsub(ci.x, cj.x), box);
+      double ycc = minimg(xsub(ci.y, cj.y), box);
+      double zcc = minimg(xsub(ci.z, cj.z), box);
+      double r2 = norm2x(xcc, ycc, zcc);
+      v = make_double4(xcc, ycc, zcc, r2);
+      keep = r2 < rlist2;
+    }
+    unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) warp_tot[wid] = __popc(bal);
+    __syncthreads();
+    int off = base;
+    for (int w = 0; w < wid; w++) off += warp_tot[w];
+    int pos = off + __popc(bal & ((1u << lane) - 1u));
+    if (keep) {
+      if (pos < cap) {
+        nbr[(size_t)i * cap + pos] = j;
+        nbrv[(size_t)i * cap + pos] = v;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int tot = 0;
+      for (int w = 0; w < nw; w++) tot += warp_tot[w];
+      base += tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    ncnt[i] = base < cap ? base : cap;
+    if (base > cap) atomicMax(&icnt[C_OVERFLOW], base);
+  }
+}
+
+// ------------------------------------------- Ewald real space + static field (real+TT)
+// rspace_ewald (ewald.f90:177-405), rspace_efield_stat (nb_induction_model.f90:128-293),
+// shortrange_efield_stat_damped (nb_induction_model.f90:5454-5629).
+template <int NQ, int NP>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_pair_static(const double4 *__restrict__ act, const int *__restrict__ nbr,
+                  const double4 *__restrict__ nbrv, const int *__restrict__ ncnt, int cap,
+                  int nm, SiteSets S, EwaldParams P, double *f, double *e0r, double *e0s,
+                  double *scal) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= nm) return;
+  const int na = S.na, ns = S.ns;
+  double4 si_q[NQ], si_p[NP];
+#pragma unroll
+  for (int a = 0; a < NQ; a++)
+    si_q[a] = a < S.nq ? ld4(&act[(size_t)i * na + S.a_of_q[a]]) : make_double4(0, 0, 0, 0);
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+    si_p[p] = p < S.np ? ld4(&act[(size_t)i * na + S.a_of_p[p]]) : make_double4(0, 0, 0, 0);
+  double F[NQ][3], E0[NP][3], Es[NP][3];
+#pragma unroll
+  for (int a = 0; a < NQ; a++) F[a][0] = F[a][1] = F[a][2] = 0.0;
+#pragma unroll
+  for (int p = 0; p < NP; p++) E0[p][0] = E0[p][1] = E0[p][2] = Es[p][0] = Es[p][1] = Es[p][2] = 0.0;
+  double e = 0.0, v = 0.0;
+  const double alp = P.alpha;
+  const int cnt = ncnt[i];
+  for (int n = lane; n < cnt; n += 32) {
+    const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
+    if (!(c.w < P.rcutsd)) continue;
+    const int j = nbr[(size_t)i * cap + n];
+    const bool half = j > i;
+    double4 sj_q[NQ];
+#pragma unroll
+    for (int b = 0; b < NQ; b++)
+      sj_q[b] = b < S.nq ? ld4(&act[(size_t)j * na + S.a_of_q[b]]) : make_double4(0, 0, 0, 0);
+#pragma unroll
+    for (int a = 0; a < NQ; a++) {
+      if (a >= S.nq) break;
+#pragma unroll
+      for (int b = 0; b < NQ; b++) {
+        if (b >= S.nq) break;
+        const double rx = (c.x + si_q[a].x) - sj_q[b].x;
+        const double ry = (c.y + si_q[a].y) - sj_q[b].y;
+        const double rz = (c.z + si_q[a].z) - sj_q[b].z;
+        const double rssq = rx * rx + ry * ry + rz * rz;
+        const double drr = sqrt(rssq);
+        const double ec = erfc(alp * drr);
+        const double qq = kR4pie0 * si_q[a].w * sj_q[b].w;
+        const double ad = alp * drr;
+        const double fc = qq * (ec / drr + P.twosqpi * alp * exp(-(ad * ad)));
+        const double cf = fc / rssq;
+        const double fx = rx * cf, fy = ry * cf, fz = rz * cf;
+        F[a][0] += fx;
+        F[a][1] += fy;
+        F[a][2] += fz;
+        if (half) {
+          e += qq * ec / drr;
+          v -= rx * fx + ry * fy + rz * fz;
+        }
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      if (p >= S.np) break;
+#pragma unroll
+      for (int b = 0; b < NQ; b++) {
+        if (b >= S.nq) break;
+        const double qj = sj_q[b].w;
+        const double dx = c.x + (si_p[p].x - sj_q[b].x);
+        const double dy = c.y + (si_p[p].y - sj_q[b].y);
+        const double dz = c.z + (si_p[p].z - sj_q[b].z);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double dist = sqrt(d2);
+        const double ad = alp * dist;
+        const double expar2 = exp(-(ad * ad));
+        const double d1i = erfc(alp * dist) / dist;
+        const double d2i = 1.0 / d2;
+        const double d3i = d2i * (d1i + P.twosqpi * alp * expar2);
+        E0[p][0] += qj * dx * d3i;
+        E0[p][1] += qj * dy * d3i;
+        E0[p][2] += qj * dz * d3i;
+        if (P.damped) {
+          const double r1 = 1.0 / dist;
+          const double r3 = r1 * r1 * r1;
+          const double g = (tt<2>(P.delta2, dist) - 1.0) * qj * r3;
+          Es[p][0] += g * dx;
+          Es[p][1] += g * dy;
+          Es[p][2] += g * dz;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NQ; a++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) F[a][k] = warp_sum(F[a][k]);
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      E0[p][k] = warp_sum(E0[p][k]);
+      Es[p][k] = warp_sum(Es[p][k]);
+    }
+  e = warp_sum(e);
+  v = warp_sum(v);
+  if (lane == 0) {
+    const size_t nfs = (size_t)nm * ns;
+#pragma unroll
+    for (int a = 0; a < NQ; a++) {
+      if (a >= S.nq) break;
+      const size_t o = (size_t)i * ns + S.qsite[a];
+      f[o] += F[a][0];
+      f[nfs + o] += F[a][1];
+      f[2 * nfs + o] += F[a][2];
+    }
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      if (p >= S.np) break;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        e0r[((size_t)i * S.np + p) * 3 + k] = E0[p][k];
+        e0s[((size_t)i * S.np + p) * 3 + k] = Es[p][k];
+      }
+    }
+    atomicAdd(&scal[S_RC_E], e);
+    atomicAdd(&scal[S_RC_VIR], v);
+  }
+}
+
+// --------------------------------------------- intramolecular static terms (per molecule)
+// ewald_self_correction intramolecular part (ewald.f90:101-147) and self_efield_stat
+// (nb_induction_model.f90:977-1115).  Both use (x + xs_a) - (x + xs_b), as the reference
+// does, so coincident sites give exactly zero and are skipped.
+__global__ void k_self_static(const double *__restrict__ x, const double *__restrict__ y,
+                              const double *__restrict__ z, const double *__restrict__ xs,
+                              const double *__restrict__ ys, const double *__restrict__ zs,
+                              int nm, int ld, SiteSets S, EwaldParams P, double *f,
+                              double *e0slf, double *scal) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double sumff = 0.0, vir = 0.0;
+  if (i < nm) {
+    const double alp = P.alpha;
+    const size_t nfs = (size_t)nm * S.ns;
+    const double xi = x[i], yi = y[i], zi = z[i];
+    for (int a = 0; a < S.nq; a++) {
+      for (int b = a + 1; b < S.nq; b++) {
+        const int sa = S.qsite[a], sb = S.qsite[b];
+        const double chg = S.q[S.a_of_q[a]] * S.q[S.a_of_q[b]];
+        const size_t oa = (size_t)i * ld + sa, ob = (size_t)i * ld + sb;
+        const double dx = (xi + xs[oa]) - (xi + xs[ob]);
+        const double dy = (yi + ys[oa]) - (yi + ys[ob]);
+        const double dz = (zi + zs[oa]) - (zi + zs[ob]);
+        const double drr = sqrt(dx * dx + dy * dy + dz * dz);
+        const double ef = erf(alp * drr);
+        sumff += ef * chg / drr;
+        const double ad = alp * drr;
+        const double fs = -kR4pie0 * chg *
+                          (ef / (drr * drr * drr) - P.twosqpi * alp * exp(-(ad * ad)) / (drr * drr));
+        const double fx = dx * fs, fy = dy * fs, fz = dz * fs;
+        const size_t ca = (size_t)i * S.ns + sa, cb = (size_t)i * S.ns + sb;
+        f[ca] += fx;
+        f[nfs + ca] += fy;
+        f[2 * nfs + ca] += fz;
+        f[cb] -= fx;
+        f[nfs + cb] -= fy;
+        f[2 * nfs + cb] -= fz;
+        vir -= dx * fx + dy * fy + dz * fz;
+      }
+    }
+    for (int p = 0; p < S.np; p++) {
+      const int sp = S.psite[p];
+      double E[3] = {0.0, 0.0, 0.0};
+      for (int u = 0; u < S.nself_q; u++) {
+        const int b = S.self_q[u];
+        const int sb = S.qsite[b];
+        const double qj = S.q[S.a_of_q[b]];
+        const size_t op = (size_t)i * ld + sp, ob = (size_t)i * ld + sb;
+        const double dx = (xi + xs[op]) - (xi + xs[ob]);
+        const double dy = (yi + ys[op]) - (yi + ys[ob]);
+        const double dz = (zi + zs[op]) - (zi + zs[ob]);
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        if (d2 == 0.0) continue;
+        const double drr = sqrt(d2);
+        const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i;
+        const double ad = alp * drr;
+        const double g = erf(alp * drr) * d3i - P.twosqpi * alp * exp(-(ad * ad)) * d2i;
+        E[0] -= qj * dx * g;
+        E[1] -= qj * dy * g;
+        E[2] -= qj * dz * g;
+      }
+      for (int k = 0; k < 3; k++) e0slf[((size_t)i * S.np + p) * 3 + k] = E[k];
+    }
+  }
+  sumff = warp_sum(sumff);
+  vir = warp_sum(vir);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&scal[S_SELF_SUMFF], sumff);
+    atomicAdd(&scal[S_SELF_VIR], vir);
+  }
+}
+
+// ------------------------------------------- dipole field (one Jacobi iteration, real)
+// rspace_efield_idm (nb_induction_model.f90:1409-1569), shortrange_efield_idm_damped
+// (:5634-5789) and self_efield_idm (:2663-2829).
+template <int NP>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_pair_dipfield(const double *__restrict__ x, const double *__restrict__ y,
+                    const double *__restrict__ z, const double *__restrict__ xs,
+                    const double *__restrict__ ys, const double *__restrict__ zs, int ld,
+                    const double4 *__restrict__ act, const int *__restrict__ nbr,
+                    const double4 *__restrict__ nbrv, const int *__restrict__ ncnt, int cap,
+                    int nm, SiteSets S, EwaldParams P, const double *__restrict__ mu,
+                    double *eir, double *eis, double *eislf) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= nm) return;
+  const int na = S.na, np = S.np;
+  const double alp = P.alpha, alp3 = alp * alp * alp;
+  double4 sp[NP];
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+    sp[p] = p < np ? ld4(&act[(size_t)i * na + S.a_of_p[p]]) : make_double4(0, 0, 0, 0);
+  double Er[NP][3], Es[NP][3];
+#pragma unroll
+  for (int p = 0; p < NP; p++) Er[p][0] = Er[p][1] = Er[p][2] = Es[p][0] = Es[p][1] = Es[p][2] = 0.0;
+  const int cnt = ncnt[i];
+  for (int n = lane; n < cnt; n += 32) {
+    const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
+    if (!(c.w < P.rcutsd)) continue;
+    const int j = nbr[(size_t)i * cap + n];
+#pragma unroll
+    for (int q = 0; q < NP; q++) {
+      if (q >= np) break;
+      const double4 sq = ld4(&act[(size_t)j * na + S.a_of_p[q]]);
+      const double mx = mu[((size_t)j * np + q) * 3 + 0];
+      const double my = mu[((size_t)j * np + q) * 3 + 1];
+      const double mz = mu[((size_t)j * np + q) * 3 + 2];
+#pragma unroll
+      for (int p = 0; p < NP; p++) {
+        if (p >= np) break;
+        const double dx = c.x + sp[p].x - sq.x;
+        const double dy = c.y + sp[p].y - sq.y;
+        const double dz = c.z + sp[p].z - sq.z;
+        const double d2 = dx * dx + dy * dy + dz * dz;
+        const double drr = sqrt(d2);
+        const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d5i = d3i * d2i;
+        const double dotj = mx * dx + my * dy + mz * dz;
+        const double ad = alp * drr;
+        const double expar2 = exp(-(ad * ad));
+        const double ec = erfc(alp * drr);
+        const double d3ii = ec * d3i + P.twosqpi * alp * expar2 * d2i;
+        const double d5ii = ec * d5i + P.twosqpi * alp * expar2 * d2i * d2i +
+                            2.0 * P.twosqpi * alp3 * expar2 * d2i / 3.0;
+        Er[p][0] += 3.0 * d5ii * dotj * dx - mx * d3ii;
+        Er[p][1] += 3.0 * d5ii * dotj * dy - my * d3ii;
+        Er[p][2] += 3.0 * d5ii * dotj * dz - mz * d3ii;
+        if (P.damped) {
+          const double g = tt<3>(P.delta3, drr) - 1.0;
+          Es[p][0] += g * (3.0 * d5i * dotj * dx - mx * d3i);
+          Es[p][1] += g * (3.0 * d5i * dotj * dy - my * d3i);
+          Es[p][2] += g * (3.0 * d5i * dotj * dz - mz * d3i);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < NP; p++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      Er[p][k] = warp_sum(Er[p][k]);
+      Es[p][k] = warp_sum(Es[p][k]);
+    }
+  // self field: point term + erf-screened intramolecular dipole-dipole (lanes 0..np-1)
+  if (lane < np) {
+    const int p = lane, s = S.psite[p];
+    const double selffac = 4.0 * alp3 / (3.0 * sqrt(kPi));
+    double E[3];
+    for (int k = 0; k < 3; k++) E[k] = selffac * mu[((size_t)i * np + p) * 3 + k];
+    double L[3] = {0.0, 0.0, 0.0};
+    const double xi = x[i], yi = y[i], zi = z[i];
+    for (int q = 0; q < np; q++) {
+      if (q == p) continue;
+      const int t = S.psite[q];
+      const size_t os = (size_t)i * ld + s, ot = (size_t)i * ld + t;
+      const double dx = (xi + xs[os]) - (xi + xs[ot]);
+      const double dy = (yi + ys[os]) - (yi + ys[ot]);
+      const double dz = (zi + zs[os]) - (zi + zs[ot]);
+      const double drr = sqrt(dx * dx + dy * dy + dz * dz);
+      const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d5i = d3i * d2i;
+      const double mx = mu[((size_t)i * np + q) * 3 + 0];
+      const double my = mu[((size_t)i * np + q) * 3 + 1];
+      const double mz = mu[((size_t)i * np + q) * 3 + 2];
+      const double dotj = mx * dx + my * dy + mz * dz;
+      const double ad = alp * drr;
+      const double expar2 = exp(-(ad * ad));
+      const double ef = erf(alp * drr);
+      const double d3ii = ef * d3i - P.twosqpi * alp * expar2 * d2i;
+      const double d5ii = ef * d5i - P.twosqpi * alp * expar2 * d2i * d2i -
+                          2.0 * P.twosqpi * alp3 * expar2 * d2i / 3.0;
+      L[0] -= 3.0 * d5ii * dotj * dx - mx * d3ii;
+      L[1] -= 3.0 * d5ii * dotj * dy - my * d3ii;
+      L[2] -= 3.0 * d5ii * dotj * dz - mz * d3ii;
+    }
+    for (int k = 0; k < 3; k++) eislf[((size_t)i * np + p) * 3 + k] = E[k] + L[k];
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int p = 0; p < NP; p++) {
+      if (p >= np) break;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        eir[((size_t)i * np + p) * 3 + k] = Er[p][k];
+        eis[((size_t)i * np + p) * 3 + k] = Es[p][k];
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------- Jacobi update (iteridm)
+// nb_induction_model.f90:1317-1359: E0 = r + k + self + short-range, same for the dipole
+// field; mu <- alpha (E0 + Eidm); change and energy use the pre-update field.
+__global__ void k_dip_update(int nm, SiteSets S, const double *__restrict__ e0r,
+                             const double *__restrict__ e0k, const double *__restrict__ e0slf,
+                             const double *__restrict__ e0s, const double *__restrict__ eir,
+                             const double *__restrict__ eik, const double *__restrict__ eislf,
+                             const double *__restrict__ eis, double *mu, double *scal) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double ch = 0.0, en = 0.0;
+  if (t < nm * S.np) {
+    const int p = t % S.np;
+    const double polr = S.apol[p];
+    double E0[3], Et[3], m[3];
+    for (int k = 0; k < 3; k++) {
+      const size_t o = (size_t)t * 3 + k;
+      E0[k] = e0r[o] + e0k[o] + e0slf[o] + e0s[o];
+      const double Ei = eir[o] + eik[o] + eislf[o] + eis[o];
+      Et[k] = Ei + E0[k];
+      m[k] = polr * Et[k];
+    }
+    const double dx = mu[(size_t)t * 3] - m[0], dy = mu[(size_t)t * 3 + 1] - m[1],
+                 dz = mu[(size_t)t * 3 + 2] - m[2];
+    ch = dx * dx + dy * dy + dz * dz;
+    for (int k = 0; k < 3; k++) mu[(size_t)t * 3 + k] = m[k];
+    en = -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
+  }
+  __shared__ double red[2][32];
+  ch = warp_sum(ch);
+  en = warp_sum(en);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][wid] = ch;
+    red[1][wid] = en;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    ch = lane < nw ? red[0][lane] : 0.0;
+    en = lane < nw ? red[1][lane] : 0.0;
+    ch = warp_sum(ch);
+    en = warp_sum(en);
+    if (lane == 0) {
+      atomicAdd(&scal[S_IND_CHANGE], ch);
+      atomicAdd(&scal[S_IND_ENERGY], en);
+    }
+  }
+}
+
+// ------------------------------------------------------------ induction forces (real)
+// real_forces (nb_induction_model.f90:3069-3631), shortrange_forces_damped (:5975-6557)
+// and self_forces (:4841-5360).  Force on active site a of i from active site b of j:
+//   F = q_a E_b(r_a) + (mu_a . grad) E_b(r_a),
+// with the field/gradient of charge q_b and dipole mu_b in the reference's screened
+// (erfc) and Tang-Toennies short-range forms, contracted as the reference contracts
+// them.  The virial of a pair is -d . F, counted from the i < j side.
+struct IndPair {
+  double fx, fy, fz;
+};
+
+__device__ __forceinline__ void ind_pair(double dx, double dy, double dz, double qa,
+                                         double max, double may, double maz, bool pa, double qb,
+                                         double mbx, double mby, double mbz, bool pb,
+                                         const EwaldParams &P, IndPair &out) {
+  const double alp = P.alpha, alp3 = alp * alp * alp, alp5 = alp3 * alp * alp;
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  const double dist = sqrt(d2);
+  const double d1i = 1.0 / dist, d2i = d1i * d1i, d3i = d2i * d1i, d4i = d2i * d2i;
+  const double d5i = d3i * d2i, d6i = d3i * d3i, d7i = d5i * d2i;
+  const double ad = alp * dist;
+  const double expar2 = exp(-(ad * ad));
+  const double ec = erfc(alp * dist);
+  const double ts = P.twosqpi;
+  const double d3ii = ec * d3i + ts * alp * expar2 * d2i;
+  const double d5ii = ec * d5i + ts * alp * expar2 * d4i + 2.0 * ts * alp3 * expar2 * d2i / 3.0;
+  const double d7ii = ec * d7i + ts * alp * expar2 * d6i + 2.0 * ts * alp3 * expar2 * d4i / 3.0 +
+                      4.0 * ts * alp5 * expar2 * d2i / 15.0;
+  const double doti = max * dx + may * dy + maz * dz;
+  const double dotj = mbx * dx + mby * dy + mbz * dz;
+  const double mm = max * mbx + may * mby + maz * mbz;
+  double fx = 0.0, fy = 0.0, fz = 0.0;
+  // screened part: q_a E_mu_b + mu_a . grad (E_q_b + E_mu_b)
+  if (pb && qa != 0.0) {
+    const double s = 3.0 * d5ii * dotj;
+    fx += qa * (s * dx - mbx * d3ii);
+    fy += qa * (s * dy - mby * d3ii);
+    fz += qa * (s * dz - mbz * d3ii);
+  }
+  if (pa) {
+    // sum_x m_x G[x][y] = qb(-3 d5 doti d_y + m_y d3) - 15 d7 doti dotj d_y
+    //                      + 3 d5 (m_y dotj + mm d_y + mb_y doti)
+    const double c1 = -3.0 * qb * d5ii * doti - 15.0 * d7ii * doti * dotj + 3.0 * d5ii * mm;
+    fx += c1 * dx + qb * max * d3ii + 3.0 * d5ii * (max * dotj + mbx * doti);
+    fy += c1 * dy + qb * may * d3ii + 3.0 * d5ii * (may * dotj + mby * doti);
+    fz += c1 * dz + qb * maz * d3ii + 3.0 * d5ii * (maz * dotj + mbz * doti);
+  }
+  if (P.damped) {
+    const double f2 = tt<2>(P.delta2, dist), f3 = tt<3>(P.delta3, dist);
+    const double df2 = dtt<2>(P.delta2, dist), df3 = dtt<3>(P.delta3, dist);
+    if (pb && qa != 0.0) {
+      const double s1 = (f2 - 1.0) * 3.0 * d5i * dotj - dotj * d3i * df2 * d1i;
+      fx += qa * (s1 * dx - (f2 - 1.0) * mbx * d3i);
+      fy += qa * (s1 * dy - (f2 - 1.0) * mby * d3i);
+      fz += qa * (s1 * dz - (f2 - 1.0) * mbz * d3i);
+    }
+    if (pa) {
+      // sum_c m_c g[x][c], g[x][c] = dE_c/dx of the short-range correction field
+      const double c1 = (f2 - 1.0) * qb * (-3.0 * d5i * doti) + qb * doti * d3i * df2 * d1i +
+                        (f3 - 1.0) * (-15.0 * dotj * d7i * doti + 3.0 * d5i * mm) +
+                        (3.0 * doti * dotj * d5i - mm * d3i) * df3 * d1i;
+      const double g2 = (f2 - 1.0) * qb * d3i;
+      const double g3 = (f3 - 1.0) * 3.0 * d5i;
+      fx += c1 * dx + g2 * max + g3 * (max * dotj + mbx * doti);
+      fy += c1 * dy + g2 * may + g3 * (may * dotj + mby * doti);
+      fz += c1 * dz + g2 * maz + g3 * (maz * dotj + mbz * doti);
+    }
+  }
+  out.fx = fx;
+  out.fy = fy;
+  out.fz = fz;
+}
+
+template <int NA>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+    k_pair_indforce(const double *__restrict__ x, const double *__restrict__ y,
+                    const double *__restrict__ z, const double *__restrict__ xs,
+                    const double *__restrict__ ys, const double *__restrict__ zs, int ld,
+                    const double4 *__restrict__ act, const int *__restrict__ nbr,
+                    const double4 *__restrict__ nbrv, const int *__restrict__ ncnt, int cap,
+                    int nm, SiteSets S, EwaldParams P, const double *__restrict__ mu,
+                    double *f, double *scal) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (i >= nm) return;
+  const int na = S.na, np = S.np;
+  double4 sa[NA];
+  double ma[NA][3];
+#pragma unroll
+  for (int a = 0; a < NA; a++) {
+    sa[a] = a < na ? ld4(&act[(size_t)i * na + a]) : make_double4(0, 0, 0, 0);
+    const int p = a < na ? S.p_of_a[a] : -1;
+    for (int k = 0; k < 3; k++) ma[a][k] = p >= 0 ? mu[((size_t)i * np + p) * 3 + k] : 0.0;
+  }
+  double F[NA][3];
+#pragma unroll
+  for (int a = 0; a < NA; a++) F[a][0] = F[a][1] = F[a][2] = 0.0;
+  double vir = 0.0;
+  const int cnt = ncnt[i];
+  for (int n = lane; n < cnt; n += 32) {
+    const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
+    if (!(c.w < P.rcutsd)) continue;
+    const int j = nbr[(size_t)i * cap + n];
+    const bool half = j > i;
+    for (int b = 0; b < na; b++) {
+      const double4 sb = ld4(&act[(size_t)j * na + b]);
+      const int pbi = S.p_of_a[b];
+      const bool pb = pbi >= 0;
+      double mbx = 0.0, mby = 0.0, mbz = 0.0;
+      if (pb) {
+        mbx = mu[((size_t)j * np + pbi) * 3 + 0];
+        mby = mu[((size_t)j * np + pbi) * 3 + 1];
+        mbz = mu[((size_t)j * np + pbi) * 3 + 2];
+      }
+#pragma unroll
+      for (int a = 0; a < NA; a++) {
+        if (a >= na) break;
+        const bool pa = S.p_of_a[a] >= 0;
+        if (!pa && !(pb && sa[a].w != 0.0)) continue;
+        const double dx = c.x + (sa[a].x - sb.x);
+        const double dy = c.y + (sa[a].y - sb.y);
+        const double dz = c.z + (sa[a].z - sb.z);
+        IndPair r;
+        ind_pair(dx, dy, dz, sa[a].w, ma[a][0], ma[a][1], ma[a][2], pa, sb.w, mbx, mby, mbz,
+                 pb, P, r);
+        F[a][0] += r.fx;
+        F[a][1] += r.fy;
+        F[a][2] += r.fz;
+        if (half) vir -= dx * r.fx + dy * r.fy + dz * r.fz;
+      }
+    }
+  }
+  // intramolecular (self_forces): lanes split the site pairs (a < b); both sides.
+  const double alp = P.alpha, alp3 = alp * alp * alp, alp5 = alp3 * alp * alp;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  for (int pr = lane; pr < na * na; pr += 32) {
+    const int a = pr / na, b = pr % na;
+    if (b <= a) continue;
+    const int s_a = S.asite[a], s_b = S.asite[b];
+    const size_t oa = (size_t)i * ld + s_a, ob = (size_t)i * ld + s_b;
+    const double dx = (xi + xs[oa]) - (xi + xs[ob]);
+    const double dy = (yi + ys[oa]) - (yi + ys[ob]);
+    const double dz = (zi + zs[oa]) - (zi + zs[ob]);
+    const double d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 == 0.0) continue;
+    const double drr = sqrt(d2);
+    const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d4i = d2i * d2i;
+    const double d5i = d3i * d2i, d6i = d3i * d3i, d7i = d6i * d1i;
+    const double ad = alp * drr;
+    const double expar2 = exp(-(ad * ad));
+    const double ef = erf(alp * drr);
+    const double ts = P.twosqpi;
+    // erf-screened kernels of the intramolecular correction (negated interactions)
+    const double d3ii = ef * d3i - ts * alp * expar2 * d2i;
+    const double d5ii = ef * d5i - ts * alp * expar2 * d4i - (2.0 / 3.0) * ts * alp3 * expar2 * d2i;
+    const double d7ii = ef * d7i - ts * alp * expar2 * d6i - (2.0 / 3.0) * ts * alp3 * expar2 * d4i -
+                        (4.0 / 15.0) * ts * alp5 * expar2 * d2i;
+    // side a (from b) with d, side b (from a) with -d
+    for (int side = 0; side < 2; side++) {
+      const int u = side == 0 ? a : b, w = side == 0 ? b : a;
+      const double sgn = side == 0 ? 1.0 : -1.0;
+      const double ex = sgn * dx, ey = sgn * dy, ez = sgn * dz;
+      const double qu = sa[u].w, qw = sa[w].w;
+      const double mux = ma[u][0], muy = ma[u][1], muz = ma[u][2];
+      const double mwx = ma[w][0], mwy = ma[w][1], mwz = ma[w][2];
+      const double doti = mux * ex + muy * ey + muz * ez;
+      const double dotj = mwx * ex + mwy * ey + mwz * ez;
+      const double mm = mux * mwx + muy * mwy + muz * mwz;
+      // field E = -(3 d5 dotj e - mw d3); gradient = -(qw(...) + dipole part)
+      const double s = 3.0 * d5ii * dotj;
+      double fx = -qu * (s * ex - mwx * d3ii), fy = -qu * (s * ey - mwy * d3ii),
+             fz = -qu * (s * ez - mwz * d3ii);
+      const double c1 = -3.0 * qw * d5ii * doti - 15.0 * d7ii * doti * dotj + 3.0 * d5ii * mm;
+      fx -= c1 * ex + qw * mux * d3ii + 3.0 * d5ii * (mux * dotj + mwx * doti);
+      fy -= c1 * ey + qw * muy * d3ii + 3.0 * d5ii * (muy * dotj + mwy * doti);
+      fz -= c1 * ez + qw * muz * d3ii + 3.0 * d5ii * (muz * dotj + mwz * doti);
+      // accumulate to a register slot: unrolled select keeps F in registers
+#pragma unroll
+      for (int t = 0; t < NA; t++)
+        if (t == u) {
+          F[t][0] += fx;
+          F[t][1] += fy;
+          F[t][2] += fz;
+        }
+      if (side == 0) vir -= ex * fx + ey * fy + ez * fz;
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < NA; a++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) F[a][k] = warp_sum(F[a][k]);
+  vir = warp_sum(vir);
+  if (lane == 0) {
+    // point self terms: field += selffac mu, gradient diagonal -= selffac q
+    const double selffac = 4.0 * alp3 / (3.0 * sqrt(kPi));
+    const size_t nfs = (size_t)nm * S.ns;
+#pragma unroll
+    for (int a = 0; a < NA; a++) {
+      if (a >= na) break;
+      const double q = sa[a].w;
+      const double px = q * selffac * ma[a][0] - selffac * q * ma[a][0];
+      const double py = q * selffac * ma[a][1] - selffac * q * ma[a][1];
+      const double pz = q * selffac * ma[a][2] - selffac * q * ma[a][2];
+      const size_t o = (size_t)i * S.ns + S.asite[a];
+      f[o] += kR4pie0 * (F[a][0] + px);
+      f[nfs + o] += kR4pie0 * (F[a][1] + py);
+      f[2 * nfs + o] += kR4pie0 * (F[a][2] + pz);
+    }
+    atomicAdd(&scal[S_IND_VIR_R], kR4pie0 * vir);
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ launchers
+cudaError_t launch_prep(const double *x, const double *y, const double *z, const double *xs,
+                        const double *ys, const double *zs, int nm, int ld, SiteSets S,
+                        double4 *com, double4 *act, double4 *comb, double4 *s17, int ns3,
+                        double *f, int nf, double *fc2, double *fc3, double *scal,
+                        int *icnt, cudaStream_t st) {
+  int threads = 256;
+  int blocks = (nf + threads - 1) / threads;
+  if (blocks < 1) blocks = 1;
+  if (blocks > 4 * 148) blocks = 4 * 148;
+  k_prep<<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, nm, ld, S, com, act, comb, s17, ns3,
+                                     f, nf, fc2, fc3, scal, icnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
+                             int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st) {
+  k_neighbors<<<nm, 128, 0, st>>>(com, nm, box, rlist2, cap, nbr, nbrv, ncnt, icnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_static(const double4 *com, const double4 *act, const int *nbr,
+                               const double4 *nbrv, const int *ncnt, int cap, int nm,
+                               SiteSets S, EwaldParams P, double *f, double *e0r,
+                               double *e0s, double *scal, cudaStream_t st) {
+  (void)com;
+  const int threads = kWarpsPerBlock * 32;
+  const int blocks = (nm + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (S.nq <= 5 && S.np <= 3)
+    k_pair_static<5, 3><<<blocks, threads, 0, st>>>(act, nbr, nbrv, ncnt, cap, nm, S, P, f, e0r,
+                                                    e0s, scal);
+  else
+    k_pair_static<kMaxQ, kMaxP><<<blocks, threads, 0, st>>>(act, nbr, nbrv, ncnt, cap, nm, S, P,
+                                                            f, e0r, e0s, scal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_self_static(const double *x, const double *y, const double *z,
+                               const double *xs, const double *ys, const double *zs, int nm,
+                               int ld, SiteSets S, EwaldParams P, double *f, double *e0slf,
+                               double *scal, cudaStream_t st) {
+  const int threads = 128;
+  k_self_static<<<(nm + threads - 1) / threads, threads, 0, st>>>(x, y, z, xs, ys, zs, nm, ld, S,
+                                                                  P, f, e0slf, scal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_dipfield(const double *x, const double *y, const double *z,
+                                 const double *xs, const double *ys, const double *zs,
+                                 int ld, const double4 *act, const int *nbr,
+                                 const double4 *nbrv, const int *ncnt, int cap, int nm,
+                                 SiteSets S, EwaldParams P, const double *mu, double *eir,
+                                 double *eis, double *eislf, cudaStream_t st) {
+  const int threads = kWarpsPerBlock * 32;
+  const int blocks = (nm + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (S.np <= 3)
+    k_pair_dipfield<3><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt,
+                                                   cap, nm, S, P, mu, eir, eis, eislf);
+  else
+    k_pair_dipfield<kMaxP><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv,
+                                                       ncnt, cap, nm, S, P, mu, eir, eis, eislf);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dip_update(int nm, SiteSets S, const double *e0r, const double *e0k,
+                              const double *e0slf, const double *e0s, const double *eir,
+                              const double *eik, const double *eislf, const double *eis,
+                              double *mu, double *scal, cudaStream_t st) {
+  const int threads = 256;
+  const int n = nm * S.np;
+  k_dip_update<<<(n + threads - 1) / threads, threads, 0, st>>>(nm, S, e0r, e0k, e0slf, e0s, eir,
+                                                                eik, eislf, eis, mu, scal);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,
+                                 const double *xs, const double *ys, const double *zs,
+                                 int ld, const double4 *act, const int *nbr,
+                                 const double4 *nbrv, const int *ncnt, int cap, int nm,
+                                 SiteSets S, EwaldParams P, const double *mu, double *f,
+                                 double *scal, cudaStream_t st) {
+  const int threads = kWarpsPerBlock * 32;
+  const int blocks = (nm + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (S.na <= 8)
+    k_pair_indforce<8><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt,
+                                                   cap, nm, S, P, mu, f, scal);
+  else
+    k_pair_indforce<kMaxA><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv,
+                                                       ncnt, cap, nm, S, P, mu, f, scal);
+  return cudaGetLastError();
+}

@@ -1,0 +1,185 @@
+/*
+ * ccpol23_b200.h -- C ABI of the B200-native CCpol23+(2025) force-evaluation hot path.
+ *
+ * The entry points below replace, one for one, the Fortran module procedures that
+ * md.f90/evolve.f90 call on the hot path of ommair/CCpol23_plus_2025_MBMD.  Each keeps
+ * the reference's argument meaning and units:
+ *   positions in Angstrom; COM arrays x[nm]; site arrays xs[i*ld + is] (site index
+ *   fastest, leading dimension ld >= ns; the reference passes its nsite=50 arrays);
+ *   energies returned in kcal/mol; site forces ACCUMULATE into fxs/fys/fzs in internal
+ *   units (10 J/mol/Angstrom); the 3-body COM forces fxfs2/fxfs3 are OVERWRITTEN;
+ *   the virial ACCUMULATES into *vir (internal units); induced dipoles are overwritten.
+ * Every entry point returns an int status (CCP_OK == 0) instead of the reference's
+ * `stop`.  All buffers in these signatures are host memory unless the name ends in
+ * _device, in which case they are device pointers on the context's GPU.
+ *
+ * Parameters that the reference reads from module globals (charges, polarisabilities,
+ * cut-offs, Ewald alpha/k-max, FS3 tables, CONTROL flags) live in a ccp_model loaded
+ * from the reference's own input files, and are copied into the context.
+ */
+#ifndef CCPOL23_B200_H
+#define CCPOL23_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status codes */
+#define CCP_OK 0
+#define CCP_ERR_BAD_INPUT 1      /* null pointer, nm/ld out of range, bad file contents */
+#define CCP_ERR_NOT_CONVERGED 2  /* dipole iteration hit maxit (reference: `stop`,
+                                    nb_induction_model.f90:1374-1379) */
+#define CCP_ERR_CUDA 3           /* a CUDA runtime call failed; see ccp_last_error() */
+#define CCP_ERR_NO_DEVICE 4      /* no CUDA device / library built without one */
+#define CCP_ERR_IO 5             /* an input file could not be opened */
+#define CCP_ERR_CAPACITY 6       /* an internal list overflowed twice (not expected) */
+
+/* precision forms of a context */
+#define CCP_FP64 0   /* plain FP64 everywhere */
+#define CCP_MIXED 1  /* FP32 three-body geometry/terms with FP64 accumulation; FP64
+                        Ewald, induction and all totals */
+
+typedef struct ccp_model ccp_model;
+typedef struct ccp_context ccp_context;
+
+/* Per-term energies (kcal/mol) and bookkeeping of one hot-path evaluation. */
+typedef struct ccp_energies {
+    double scpe;      /* Ewald self + intramolecular correction */
+    double rcpe;      /* Ewald real space */
+    double kcpe;      /* Ewald reciprocal space */
+    double indpe;     /* induction */
+    double fs2pe;     /* FS2 three-body */
+    double fs3pe;     /* FS3 three-body */
+    double vir;       /* virial added by these terms (internal units) */
+    int ind_iters;    /* Jacobi iterations taken */
+    int n_fs3_triples;    /* molecular triples inside the FS3 cut-off */
+    int n_fs3_blend;      /* of which in the SR/LR switching region */
+    int n_fs2_triples;    /* (spectator, pair) combinations inside the FS2 cut-off */
+} ccp_energies;
+
+/* Last error message of the calling thread (never NULL). */
+const char *ccp_last_error(void);
+
+/* ------------------------------------------------------------------- parameters */
+/* Reads CONTROL, FIELD, data3b_full and data3b_full_LR_4p5 from `dir`
+   (replaces control_parameters + molecule, initialization.f90:463-720), then builds the
+   principal-axis site frame (shift_to_com + principle_moment_inertia,
+   initialization.f90:728-845) and the FS3 coefficient index
+   (threebody_potential.f90:909-946, 2064-2131). */
+int ccp_model_load(const char *dir, ccp_model **out);
+void ccp_model_free(ccp_model *m);
+
+/* Scalar accessors/overrides (the reference reads these from common_arrays). */
+int ccp_model_get_int(const ccp_model *m, const char *name, int *value);
+int ccp_model_get_double(const ccp_model *m, const char *name, double *value);
+int ccp_model_set_int(ccp_model *m, const char *name, int value);
+int ccp_model_set_double(ccp_model *m, const char *name, double value);
+/* Per-site arrays: "charge", "polarizability", "mass" (ns values),
+   "pcoord" (ns*3, site-major), "pmi" (3). */
+int ccp_model_get_array(const ccp_model *m, const char *name, double *out, int n);
+
+/* sites (molecular_sites.f90:14-47): site offsets from the COM of every molecule from
+   its quaternion q[i*4 + 0..3]; writes xs/ys/zs[i*ld + is]. */
+int ccp_sites(const ccp_model *m, int nm, const double *q, int ld, double *xs, double *ys,
+              double *zs);
+
+/* ewald_setup (ewald.f90:17-43). */
+int ccp_ewald_setup(double ewps, double rcut, double box, double *alp, int *k1, int *k2,
+                    int *k3);
+
+/* --------------------------------------------------------------------- context */
+/* Allocates device-resident state for boxes of nm molecules on `device` (ordinal),
+   precision CCP_FP64 or CCP_MIXED.  Ewald alpha/k-max default to
+   ccp_ewald_setup(1e-6, rcut, box0). */
+int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int precision,
+                       ccp_context **out);
+int ccp_context_destroy(ccp_context *ctx);
+/* Override alpha and kmax1..3 (the reference's module globals alpha, kmax1-3). */
+int ccp_context_set_ewald(ccp_context *ctx, double alpha, int k1, int k2, int k3);
+/* Cap on dipole iterations (reference: maxit = 500, nb_induction_model.f90:1221). */
+int ccp_context_set_maxit(ccp_context *ctx, int maxit);
+/* Run subsequent device work on this cudaStream_t (NULL = the context's own stream). */
+int ccp_context_set_stream(ccp_context *ctx, void *stream);
+
+/* ------------------------------------------- reference entry points (host buffers) */
+/* ewald_self_correction(alp, boxi, qscpe) -- ewald.f90:45-174 (the reference reads the
+   global x, xs; here they are arguments). */
+int ccp_ewald_self_correction(ccp_context *ctx, double alp, double box, const double *x,
+                              const double *y, const double *z, const double *xs,
+                              const double *ys, const double *zs, int ld, double *qscpe,
+                              double *fxs, double *fys, double *fzs, double *vir);
+
+/* rspace_ewald(xx,yy,zz,xxs,yys,zzs,boxi,alp,qrcpe) -- ewald.f90:177-405. */
+int ccp_rspace_ewald(ccp_context *ctx, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld,
+                     double box, double alp, double *qrcpe, double *fxs, double *fys,
+                     double *fzs, double *vir);
+
+/* kspace_ewald(xx,..,lmax,mmax,nmax,alp,boxi,qkcpe) -- ewald.f90:754-1173. */
+int ccp_kspace_ewald(ccp_context *ctx, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld, int lmax,
+                     int mmax, int nmax, double alp, double box, double *qkcpe, double *fxs,
+                     double *fys, double *fzs, double *vir);
+
+/* nb_induction(xx,..,boxi,qindpe) -- nb_induction_model.f90:25-126: static field, Jacobi
+   dipole iteration (iteridm, :1193-1407), induction forces.  idm* receive the induced
+   dipoles at every site (non-polarisable sites 0).  *iters may be NULL. */
+int ccp_nb_induction(ccp_context *ctx, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld,
+                     double box, double *qindpe, double *idmx, double *idmy, double *idmz,
+                     double *fxs, double *fys, double *fzs, double *vir, int *iters);
+
+/* threebody_term(xxx,..,boxii,qfs2,qfs3) -- threebody_potential.f90:17-99: FS2 (if the
+   model's S2_term) and FS3 (if S3_term).  fxfs2/fxfs3 are overwritten only for the terms
+   that run, as in the reference. */
+int ccp_threebody_term(ccp_context *ctx, const double *x, const double *y, const double *z,
+                       const double *xs, const double *ys, const double *zs, int ld,
+                       double box, double *qfs2, double *qfs3, double *fxs, double *fys,
+                       double *fzs, double *fxfs2, double *fyfs2, double *fzfs2,
+                       double *fxfs3, double *fyfs3, double *fzfs3, double *vir);
+
+/* The whole sequence evolve.f90:842-877 runs after the 2-body term: Ewald self, real and
+   reciprocal, nb_induction (if the model's induction flag), threebody_term (if
+   nonadditive_3B), in one call with one upload and one download.  Any output pointer may
+   be NULL to skip that download. */
+int ccp_hot_path(ccp_context *ctx, const double *x, const double *y, const double *z,
+                 const double *xs, const double *ys, const double *zs, int ld, double box,
+                 ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
+                 double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3,
+                 double *fzfs3, double *idmx, double *idmy, double *idmz);
+
+/* ------------------------------------------------ device-resident form */
+/* Same as ccp_hot_path with every array already on the device (same layouts).  Nothing
+   is copied between host and device except the ccp_energies scalars. */
+int ccp_hot_path_device(ccp_context *ctx, const double *x_device, const double *y_device,
+                        const double *z_device, const double *xs_device,
+                        const double *ys_device, const double *zs_device, int ld, double box,
+                        ccp_energies *e, double *fxs_device, double *fys_device,
+                        double *fzs_device, double *fxfs2_device, double *fyfs2_device,
+                        double *fzfs2_device, double *fxfs3_device, double *fyfs3_device,
+                        double *fzfs3_device, double *idmx_device, double *idmy_device,
+                        double *idmz_device);
+
+/* ---------------------------------------------------------------- diagnostics */
+/* These have no counterpart in the reference; they serve benchmarking and profiling. */
+
+/* Launch statistics of the last evaluation: number of kernels this library launched. */
+int ccp_context_last_launches(const ccp_context *ctx, int *launches);
+
+/* When on, every evaluation records CUDA events on the launching stream between its
+   phases; ccp_context_phase_ms then returns the durations (ms) of the last evaluation:
+   [0] input packing + neighbour list, [1] Ewald real space + static field (real) +
+   intramolecular terms, [2] Ewald reciprocal space, [3] induction (static reciprocal
+   field, dipole iteration, forces), [4] FS2, [5] FS3 triple list, [6] FS3 kernel. */
+#define CCP_NPHASE 7
+int ccp_context_set_timing(ccp_context *ctx, int on);
+int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
+
+/* Measured peak of the FP64 (precision CCP_FP64) or FP32 (CCP_MIXED) fused multiply-add
+   pipe of `device`, in TFLOP/s (2 flops per FMA), from a register-resident FMA chain. */
+int ccp_device_fma_peak(int device, int precision, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,472 @@
+"""Python side of the CPU FP64 oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this
+module.  It loads ``oracle/_build/libccpol_oracle.so`` (built by ``oracle/Makefile``) and
+restates, independently of the product library:
+
+* the input readers of the reference: CONTROL (initialization.f90:463-489), FIELD and the
+  FS3 parameter files (initialization.f90:491-720);
+* the molecular frame set-up: shift_to_com (initialization.f90:728-748),
+  principle_moment_inertia with the DL_POLY Jacobi diagonaliser
+  (initialization.f90:750-845, utility.f90:458-596);
+* site placement from quaternions: sites/transform/quat_to_rot
+  (molecular_sites.f90:14-111).
+
+Arrays follow the reference layout: COM arrays ``x[nm]``; site arrays ``xs[nm, ld]`` in C
+order, i.e. site index fastest (the Fortran ``xs(nsite, nom)`` column-major layout).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+import subprocess
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "libccpol_oracle.so"
+
+BOHR2A = 0.529177249
+R4PIE0 = 138935.4835
+H2KCAL = 627.510
+EWP = 1.0e-6
+
+
+class OrcModel(C.Structure):
+    _fields_ = [
+        ("nm", C.c_int), ("ns", C.c_int), ("npol", C.c_int),
+        ("charge", C.c_double * 50), ("polarizability", C.c_double * 50),
+        ("alpha", C.c_double), ("kmax1", C.c_int), ("kmax2", C.c_int), ("kmax3", C.c_int),
+        ("rcut", C.c_double), ("rcutsd", C.c_double),
+        ("rcut3", C.c_double), ("rcutsd3", C.c_double),
+        ("alpha3", C.c_double), ("delta33", C.c_double),
+        ("s2_term", C.c_int), ("s3_term", C.c_int), ("damped", C.c_int),
+        ("bS3_s", C.c_double * 289), ("gS3_s", C.c_double * 289), ("r0S3_s", C.c_double * 289),
+        ("bS3_l", C.c_double * 289), ("gS3_l", C.c_double * 289), ("r0S3_l", C.c_double * 289),
+        ("cs3_s", C.c_double * 5000), ("cs3_l", C.c_double * 5000),
+        ("nlin", C.c_int),
+        ("ind_lin", C.c_int * (17 * 17 * 17 * 8)),
+        ("nclass", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def build():
+    """Compile the oracle with its Makefile (gcc)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = C.CDLL(str(LIB_PATH))
+        dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+        ip = C.POINTER(C.c_int)
+        mp = C.POINTER(OrcModel)
+        d = C.c_double
+        pd = C.POINTER(C.c_double)
+        L.orc_tt.restype = d
+        L.orc_tt.argtypes = [C.c_int, d, d]
+        L.orc_dtt.restype = d
+        L.orc_dtt.argtypes = [C.c_int, d, d]
+        L.orc_fill_index.restype = C.c_int
+        L.orc_fill_index.argtypes = [np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")]
+        L.orc_ewald_setup.argtypes = [d, d, d, pd, ip, ip, ip]
+        L.orc_threebody_term.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, d, pd, pd,
+                                         dp, dp, dp, dp, dp, dp, dp, dp, dp, pd]
+        L.orc_fs2_term_bohr.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, d, pd,
+                                        dp, dp, dp, dp, dp, dp, pd]
+        L.orc_ewald_self_correction.argtypes = [mp, d, d, dp, dp, dp, dp, dp, dp, C.c_int, pd,
+                                                dp, dp, dp, pd]
+        L.orc_rspace_ewald.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, d, d, pd,
+                                       dp, dp, dp, pd]
+        L.orc_kspace_ewald.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, d, d, pd, dp, dp, dp, pd]
+        L.orc_nb_induction.restype = C.c_int
+        L.orc_nb_induction.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, d, C.c_int, pd,
+                                       dp, dp, dp, dp, dp, dp, pd, ip]
+        L.orc_set_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+
+
+# --------------------------------------------------------------------------- readers
+def _fortran_logical(tok: str) -> bool:
+    t = tok.strip().strip(".").upper()
+    return t.startswith("T")
+
+
+@dataclass
+class Inputs:
+    """Values the reference reads from CONTROL, FIELD and the FS3 parameter files."""
+    control: dict
+    system_name: str
+    nm: int
+    ns: int
+    npol: int
+    names: list
+    coords: np.ndarray          # (ns, 3) as read
+    mass: np.ndarray
+    charge: np.ndarray
+    polarizability: np.ndarray
+    vdw: list = field(default_factory=list)  # (an1, an2, [14 floats]) rows
+    fs3_sr: dict | None = None
+    fs3_lr: dict | None = None
+
+
+def read_control(path) -> dict:
+    """CONTROL, 17 list-directed records (initialization.f90:463-489)."""
+    lines = Path(path).read_text().splitlines()
+    tok = [ln.split() for ln in lines]
+    c = {}
+    c["pot_name"] = tok[0][0]
+    c["ensemble"], c["taut"], c["taup"] = tok[1][0], float(tok[1][1]), float(tok[1][2])
+    c["initial_config"] = tok[2][0]
+    c["temp0"] = float(tok[3][0])
+    c["pres0"] = float(tok[4][0])
+    c["nsteps"] = int(tok[5][0])
+    c["dt"] = float(tok[6][0])
+    c["nequil"] = int(tok[7][0])
+    c["rcut"] = float(tok[8][0])
+    c["hist_freq"] = int(tok[9][0])
+    c["rand_vcom"] = _fortran_logical(tok[10][0])
+    c["rand_quat"] = _fortran_logical(tok[11][0])
+    c["induction"] = _fortran_logical(tok[12][0])
+    c["ind_model"], c["induction_type"], c["method"] = tok[12][1], tok[12][2], tok[12][3]
+    c["nonadditive_3B"] = _fortran_logical(tok[13][0])
+    c["S3_term"] = _fortran_logical(tok[13][1])
+    c["S2_term"] = _fortran_logical(tok[13][2])
+    c["rcut3"], c["alpha3"], c["r0_tilda"], c["delta33"] = (float(v) for v in tok[14][:4])
+    c["restart"] = _fortran_logical(tok[15][0])
+    c["check_forces"] = _fortran_logical(tok[16][0])
+    c["hsize"] = float(tok[16][1])
+    return c
+
+
+def read_fs3_table(path) -> dict:
+    """data3b_full / data3b_full_LR_4p5 (initialization.f90:642-701): header, 289 rows
+    `b g r0 is js` read in (is, js) order, a header, nlin, then nlin rows `idx c`; the
+    coefficients fill the array in row order."""
+    lines = Path(path).read_text().splitlines()
+    b = np.zeros(289)
+    g = np.zeros(289)
+    r0 = np.zeros(289)
+    for n in range(289):
+        t = lines[1 + n].split()
+        b[n], g[n], r0[n] = float(t[0]), float(t[1]), float(t[2])
+    nlin = int(lines[1 + 289 + 1].split()[0])
+    cs = np.zeros(5000)
+    for n in range(nlin):
+        t = lines[1 + 289 + 2 + n].split()
+        cs[n] = float(t[1])
+    return {"b": b, "g": g, "r0": r0, "cs": cs, "nlin": nlin}
+
+
+def read_inputs(directory) -> Inputs:
+    d = Path(directory)
+    control = read_control(d / "CONTROL")
+    lines = (d / "FIELD").read_text().splitlines()
+    system_name = lines[0].split()[0]
+    nm = int(lines[1].split()[0])
+    ns = int(lines[2].split()[0])
+    npol = int(lines[3].split()[0])
+    names, coords, mass, charge, pol = [], [], [], [], []
+    for s in range(ns):
+        t = lines[5 + s].split()
+        names.append(t[0])
+        coords.append([float(t[1]), float(t[2]), float(t[3])])
+        mass.append(float(t[4]))
+        charge.append(float(t[5]))
+        pol.append(float(t[6]))
+    npi = int(lines[5 + ns + 1].split()[0])
+    vdw = []
+    for k in range(npi):
+        t = lines[5 + ns + 3 + k].split()
+        vdw.append((t[0], t[1], [float(v) for v in t[2:16]]))
+    inp = Inputs(control, system_name, nm, ns, npol, names, np.array(coords), np.array(mass),
+                 np.array(charge), np.array(pol), vdw)
+    if control["nonadditive_3B"]:
+        inp.fs3_sr = read_fs3_table(d / "data3b_full")
+        inp.fs3_lr = read_fs3_table(d / "data3b_full_LR_4p5")
+    return inp
+
+
+# ------------------------------------------------------------------ molecular frame
+def jacobi(a: np.ndarray):
+    """DL_POLY cyclic Jacobi diagonaliser restated from utility.f90:458-596 (processes
+    the lower triangle; returns the rotated matrix and the eigenvector matrix)."""
+    n = a.shape[0]
+    a = a.copy()
+    v = np.eye(n)
+    rho = 1.0e-16
+    tes = 0.0
+    scl = 0.0
+    for i in range(n):
+        if abs(a[i, i]) > scl:
+            scl = abs(a[i, i])
+    for i in range(n):
+        for j in range(i + 1):
+            a[i, j] = a[i, j] / scl
+    for i in range(1, n):
+        for j in range(i):
+            tes = tes + 2.0 * a[i, j] * a[i, j]
+    tes = math.sqrt(tes)
+    while tes > rho:
+        tes = tes / float(n)
+        if tes < rho:
+            tes = rho
+        passing = True
+        while passing:
+            passing = False
+            for i in range(1, n):
+                for j in range(i):
+                    if abs(a[i, j]) >= tes:
+                        passing = True
+                        v1, v2, v3 = a[j, j], a[i, j], a[i, i]
+                        u = 0.5 * (v1 - v3)
+                        if abs(u) < rho:
+                            omg = -1.0
+                        else:
+                            omg = -v2 / math.sqrt(v2 * v2 + u * u)
+                            if u < 0.0:
+                                omg = -omg
+                        s = omg / math.sqrt(2.0 * (1.0 + math.sqrt(1.0 - omg * omg)))
+                        c = math.sqrt(1.0 - s * s)
+                        for k in range(n):
+                            if k >= i:
+                                tem = a[k, j] * c - a[k, i] * s
+                                a[k, i] = a[k, j] * s + a[k, i] * c
+                                a[k, j] = tem
+                            elif k < j:
+                                tem = a[j, k] * c - a[i, k] * s
+                                a[i, k] = a[j, k] * s + a[i, k] * c
+                                a[j, k] = tem
+                            else:
+                                tem = a[k, j] * c - a[i, k] * s
+                                a[i, k] = a[k, j] * s + a[i, k] * c
+                                a[k, j] = tem
+                            tem = v[k, j] * c - v[k, i] * s
+                            v[k, i] = v[k, j] * s + v[k, i] * c
+                            v[k, j] = tem
+                        a[j, j] = v1 * c * c + v3 * s * s - 2.0 * v2 * s * c
+                        a[i, i] = v1 * s * s + v3 * c * c + 2.0 * v2 * s * c
+                        a[i, j] = (v1 - v3) * s * c + v2 * (c * c - s * s)
+    for i in range(n):
+        for j in range(i + 1):
+            a[i, j] = scl * a[i, j]
+    return a, v
+
+
+def principal_frame(inp: Inputs):
+    """shift_to_com + principle_moment_inertia (initialization.f90:728-845).  Returns
+    (pcoord (ns,3), pmi (3,), totm)."""
+    ns = inp.ns
+    totm = 0.0
+    for s in range(ns):
+        if inp.mass[s] != 0.0:
+            totm = totm + inp.mass[s]
+    coords = inp.coords.copy()
+    r = [0.0, 0.0, 0.0]
+    for s in range(ns):
+        for a in range(3):
+            r[a] = r[a] + inp.mass[s] * coords[s, a] / totm
+    for s in range(ns):
+        for a in range(3):
+            coords[s, a] = coords[s, a] - r[a]
+    rmi = np.zeros((3, 3))
+    for i in range(3):
+        for j in range(3):
+            for s in range(ns):
+                rmi[i, j] = rmi[i, j] - inp.mass[s] * coords[s, i] * coords[s, j]
+                if i == j:
+                    rmi[i, j] = rmi[i, j] + inp.mass[s] * (
+                        coords[s, 0] ** 2 + coords[s, 1] ** 2 + coords[s, 2] ** 2)
+    rmi, rot = jacobi(rmi)
+    pmi = np.array([rmi[0, 0], rmi[1, 1], rmi[2, 2]])
+    pc = np.empty_like(coords)
+    for s in range(ns):
+        rx, ry, rz = coords[s]
+        pc[s, 0] = rx * rot[0, 0] + ry * rot[1, 0] + rz * rot[2, 0]
+        pc[s, 1] = rx * rot[0, 1] + ry * rot[1, 1] + rz * rot[2, 1]
+        pc[s, 2] = rx * rot[0, 2] + ry * rot[1, 2] + rz * rot[2, 2]
+    return pc, pmi, totm
+
+
+def quat_to_rot(q0, q1, q2, q3):
+    """molecular_sites.f90:93-111 (row-major 3x3 flattened as rott(1..9))."""
+    return np.array([
+        q0 ** 2 + q1 ** 2 - q2 ** 2 - q3 ** 2, 2.0 * (q1 * q2 - q0 * q3), 2.0 * (q1 * q3 + q0 * q2),
+        2.0 * (q1 * q2 + q0 * q3), q0 ** 2 - q1 ** 2 + q2 ** 2 - q3 ** 2, 2.0 * (q2 * q3 - q0 * q1),
+        2.0 * (q1 * q3 - q0 * q2), 2.0 * (q2 * q3 + q0 * q1), q0 ** 2 - q1 ** 2 - q2 ** 2 + q3 ** 2])
+
+
+def sites(pcoord: np.ndarray, q: np.ndarray, ld: int | None = None):
+    """sites (molecular_sites.f90:14-47): site offsets from the COM for every molecule.
+    q is (nm, 4).  Returns xs, ys, zs of shape (nm, ld)."""
+    nm = q.shape[0]
+    ns = pcoord.shape[0]
+    ld = ld or ns
+    xs = np.zeros((nm, ld))
+    ys = np.zeros((nm, ld))
+    zs = np.zeros((nm, ld))
+    for j in range(nm):
+        rott = quat_to_rot(*q[j])
+        for s in range(ns):
+            r1, r2, r3 = pcoord[s]
+            xs[j, s] = r1 * rott[0] + r2 * rott[1] + r3 * rott[2]
+            ys[j, s] = r1 * rott[3] + r2 * rott[4] + r3 * rott[5]
+            zs[j, s] = r1 * rott[6] + r2 * rott[7] + r3 * rott[8]
+    return xs, ys, zs
+
+
+def ewald_setup(rcut: float, box: float, ewps: float = EWP):
+    a = C.c_double()
+    k1, k2, k3 = C.c_int(), C.c_int(), C.c_int()
+    lib().orc_ewald_setup(ewps, rcut, box, C.byref(a), C.byref(k1), C.byref(k2), C.byref(k3))
+    return a.value, k1.value, k2.value, k3.value
+
+
+def make_model(inp: Inputs, nm: int, box: float, *, s2=None, s3=None,
+               rcut3=None, alpha3=None, delta33=None) -> OrcModel:
+    c = inp.control
+    M = OrcModel()
+    M.nm = nm
+    M.ns = inp.ns
+    M.npol = inp.npol
+    for s in range(inp.ns):
+        M.charge[s] = inp.charge[s]
+        M.polarizability[s] = inp.polarizability[s]
+    alp, k1, k2, k3 = ewald_setup(c["rcut"], box)
+    M.alpha, M.kmax1, M.kmax2, M.kmax3 = alp, k1, k2, k3
+    M.rcut = c["rcut"]
+    M.rcutsd = c["rcut"] ** 2
+    M.rcut3 = c["rcut3"] if rcut3 is None else rcut3
+    M.rcutsd3 = M.rcut3 ** 2
+    M.alpha3 = c["alpha3"] if alpha3 is None else alpha3
+    M.delta33 = c["delta33"] if delta33 is None else delta33
+    M.s2_term = int(c["S2_term"] if s2 is None else s2)
+    M.s3_term = int(c["S3_term"] if s3 is None else s3)
+    M.damped = int(c["induction_type"] == "damped")
+    if inp.fs3_sr is not None:
+        for n in range(289):
+            M.bS3_s[n], M.gS3_s[n], M.r0S3_s[n] = inp.fs3_sr["b"][n], inp.fs3_sr["g"][n], inp.fs3_sr["r0"][n]
+            M.bS3_l[n], M.gS3_l[n], M.r0S3_l[n] = inp.fs3_lr["b"][n], inp.fs3_lr["g"][n], inp.fs3_lr["r0"][n]
+        for n in range(inp.fs3_sr["nlin"]):
+            M.cs3_s[n] = inp.fs3_sr["cs"][n]
+        for n in range(inp.fs3_lr["nlin"]):
+            M.cs3_l[n] = inp.fs3_lr["cs"][n]
+        M.nlin = inp.fs3_sr["nlin"]
+    ind = np.zeros(17 * 17 * 17 * 8, dtype=np.int32)
+    M.nclass = lib().orc_fill_index(ind)
+    C.memmove(M.ind_lin, ind.ctypes.data, ind.nbytes)
+    return M
+
+
+def fill_index():
+    ind = np.zeros(17 * 17 * 17 * 8, dtype=np.int32)
+    n = lib().orc_fill_index(ind)
+    return ind, n
+
+
+# ------------------------------------------------------------------------ wrappers
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class State:
+    """Per-call outputs of the reference entry points (site forces accumulate)."""
+
+    def __init__(self, nm, ld):
+        self.fxs = np.zeros((nm, ld))
+        self.fys = np.zeros((nm, ld))
+        self.fzs = np.zeros((nm, ld))
+        self.fxfs2 = np.zeros(nm)
+        self.fyfs2 = np.zeros(nm)
+        self.fzfs2 = np.zeros(nm)
+        self.fxfs3 = np.zeros(nm)
+        self.fyfs3 = np.zeros(nm)
+        self.fzfs3 = np.zeros(nm)
+        self.idmx = np.zeros((nm, ld))
+        self.idmy = np.zeros((nm, ld))
+        self.idmz = np.zeros((nm, ld))
+        self.vir = C.c_double(0.0)
+
+
+def threebody_term(M, x, y, z, xs, ys, zs, box, st: State):
+    q2, q3 = C.c_double(0.0), C.c_double(0.0)
+    ld = xs.shape[1]
+    lib().orc_threebody_term(C.byref(M), _c(x), _c(y), _c(z), _c(xs), _c(ys), _c(zs), ld, box,
+                             C.byref(q2), C.byref(q3), st.fxs, st.fys, st.fzs,
+                             st.fxfs2, st.fyfs2, st.fzfs2, st.fxfs3, st.fyfs3, st.fzfs3,
+                             C.byref(st.vir))
+    return q2.value, q3.value
+
+
+def fs2_term_bohr(M, xx, yy, zz, xxs, yys, zzs, boxi, st: State):
+    q = C.c_double(0.0)
+    lib().orc_fs2_term_bohr(C.byref(M), _c(xx), _c(yy), _c(zz), _c(xxs), _c(yys), _c(zzs),
+                            xxs.shape[1], boxi, C.byref(q), st.fxs, st.fys, st.fzs,
+                            st.fxfs2, st.fyfs2, st.fzfs2, C.byref(st.vir))
+    return q.value
+
+
+def ewald_self_correction(M, alp, box, x, y, z, xs, ys, zs, st: State):
+    q = C.c_double(0.0)
+    lib().orc_ewald_self_correction(C.byref(M), alp, box, _c(x), _c(y), _c(z), _c(xs), _c(ys),
+                                    _c(zs), xs.shape[1], C.byref(q), st.fxs, st.fys, st.fzs,
+                                    C.byref(st.vir))
+    return q.value
+
+
+def rspace_ewald(M, x, y, z, xs, ys, zs, box, alp, st: State):
+    q = C.c_double(0.0)
+    lib().orc_rspace_ewald(C.byref(M), _c(x), _c(y), _c(z), _c(xs), _c(ys), _c(zs),
+                           xs.shape[1], box, alp, C.byref(q), st.fxs, st.fys, st.fzs,
+                           C.byref(st.vir))
+    return q.value
+
+
+def kspace_ewald(M, x, y, z, xs, ys, zs, lmax, mmax, nmax, alp, box, st: State):
+    q = C.c_double(0.0)
+    lib().orc_kspace_ewald(C.byref(M), _c(x), _c(y), _c(z), _c(xs), _c(ys), _c(zs),
+                           xs.shape[1], lmax, mmax, nmax, alp, box, C.byref(q),
+                           st.fxs, st.fys, st.fzs, C.byref(st.vir))
+    return q.value
+
+
+def nb_induction(M, x, y, z, xs, ys, zs, box, st: State, maxit: int = 500):
+    q = C.c_double(0.0)
+    it = C.c_int(0)
+    status = lib().orc_nb_induction(C.byref(M), _c(x), _c(y), _c(z), _c(xs), _c(ys), _c(zs),
+                                    xs.shape[1], box, maxit, C.byref(q), st.idmx, st.idmy,
+                                    st.idmz, st.fxs, st.fys, st.fzs, C.byref(st.vir),
+                                    C.byref(it))
+    return q.value, status, it.value
+
+
+def hot_path(M, x, y, z, xs, ys, zs, box, induction=True):
+    """The reference force-evaluation sequence after the 2-body term (evolve.f90:842-877):
+    Ewald self, real, reciprocal; induction; three-body.  Returns (energies, State)."""
+    nm, ld = xs.shape
+    st = State(nm, ld)
+    e = {}
+    e["scpe"] = ewald_self_correction(M, M.alpha, box, x, y, z, xs, ys, zs, st)
+    e["rcpe"] = rspace_ewald(M, x, y, z, xs, ys, zs, box, M.alpha, st)
+    e["kcpe"] = kspace_ewald(M, x, y, z, xs, ys, zs, M.kmax1, M.kmax2, M.kmax3, M.alpha, box, st)
+    if induction:
+        e["indpe"], status, it = nb_induction(M, x, y, z, xs, ys, zs, box, st)
+        e["ind_status"], e["ind_iters"] = status, it
+    e["fs2pe"], e["fs3pe"] = threebody_term(M, x, y, z, xs, ys, zs, box, st)
+    e["vir"] = st.vir.value
+    return e, st

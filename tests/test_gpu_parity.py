@@ -1,0 +1,195 @@
+"""GPU parity: every C-ABI entry point of the FP64 form against the CPU oracle on the same
+seeded boxes, to 1e-10 relative (energies as scalars, forces/dipoles normwise, virial as a
+scalar); the reference's own FS2 known-answer test through the GPU; mixed precision within
+its stated tolerance."""
+import numpy as np
+import pytest
+
+from ccpol23_plus_2025_mbmd_b200 import CcpError, Context, Model, data_dir
+from ccpol23_plus_2025_mbmd_b200.generator import config_box, water_box
+
+from conftest import rel
+from fs2_kat import BOHR2A, run as run_fs2_kat, site_offsets
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10          # FP64 form vs oracle
+MIXED_FTOL = 1e-5    # mixed form: relative force error of the three-body terms
+
+
+def _state(O, nm, ld):
+    return O.State(nm, ld)
+
+
+@pytest.fixture(scope="module")
+def boxes(product, oracle):
+    out = {}
+    for key, variant, nm, L, seed, ld in [("c1", "fs3", 128, 15.64, 1001, 28),
+                                          ("fs2fs3_128", "fs2fs3", 128, 15.64, 77, 50),
+                                          ("ragged_37", "fs2fs3", 37, 10.37, 9, 31)]:
+        m = Model(data_dir(variant))
+        b = water_box(m, nm, L, seed, ld=ld)
+        inp = oracle.read_inputs(data_dir(variant))
+        M = oracle.make_model(inp, nm, L)
+        out[key] = (m, b, M)
+    return out
+
+
+def _ctx(m, b, precision="fp64"):
+    return Context(m, b.nm, b.box, device=0, precision=precision)
+
+
+@pytest.mark.parametrize("key", ["c1", "ragged_37"])
+def test_ewald_terms(oracle, boxes, key):
+    O = oracle
+    m, b, M = boxes[key]
+    args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
+    with _ctx(m, b) as c:
+        for name in ("self", "rspace", "kspace"):
+            st = _state(O, b.nm, b.xs.shape[1])
+            fx, fy, fz = (np.zeros_like(b.xs) for _ in range(3))
+            vir = np.zeros(1)
+            if name == "self":
+                eo = O.ewald_self_correction(M, M.alpha, b.box, *args, st)
+                eg = c.ewald_self_correction(M.alpha, b.box, *args, fx, fy, fz, vir)
+            elif name == "rspace":
+                eo = O.rspace_ewald(M, *args, b.box, M.alpha, st)
+                eg = c.rspace_ewald(*args, b.box, M.alpha, fx, fy, fz, vir)
+            else:
+                eo = O.kspace_ewald(M, *args, M.kmax1, M.kmax2, M.kmax3, M.alpha, b.box, st)
+                eg = c.kspace_ewald(*args, M.kmax1, M.kmax2, M.kmax3, M.alpha, b.box, fx, fy, fz, vir)
+            assert abs(eg - eo) <= TOL * abs(eo), (name, eg, eo)
+            F = np.stack([fx, fy, fz])
+            Fo = np.stack([st.fxs, st.fys, st.fzs])
+            assert rel(F, Fo) <= TOL, (name, rel(F, Fo))
+            assert abs(vir[0] - st.vir.value) <= TOL * abs(st.vir.value), (name, vir[0], st.vir.value)
+
+
+@pytest.mark.parametrize("key", ["c1", "ragged_37"])
+def test_nb_induction(oracle, boxes, key):
+    O = oracle
+    m, b, M = boxes[key]
+    args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
+    st = _state(O, b.nm, b.xs.shape[1])
+    eo, status, it_o = O.nb_induction(M, *args, b.box, st)
+    assert status == 0
+    with _ctx(m, b) as c:
+        fx, fy, fz, mx, my, mz = (np.zeros_like(b.xs) for _ in range(6))
+        vir = np.zeros(1)
+        eg, it_g = c.nb_induction(*args, b.box, mx, my, mz, fx, fy, fz, vir)
+    assert it_g == it_o
+    assert abs(eg - eo) <= TOL * abs(eo), (eg, eo)
+    assert rel(np.stack([mx, my, mz]), np.stack([st.idmx, st.idmy, st.idmz])) <= TOL
+    assert rel(np.stack([fx, fy, fz]), np.stack([st.fxs, st.fys, st.fzs])) <= TOL
+    assert abs(vir[0] - st.vir.value) <= TOL * abs(st.vir.value)
+
+
+@pytest.mark.parametrize("key", ["c1", "fs2fs3_128", "ragged_37"])
+def test_threebody_term(oracle, boxes, key):
+    O = oracle
+    m, b, M = boxes[key]
+    args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
+    st = _state(O, b.nm, b.xs.shape[1])
+    e2o, e3o = O.threebody_term(M, *args, b.box, st)
+    with _ctx(m, b) as c:
+        fx, fy, fz = (np.zeros_like(b.xs) for _ in range(3))
+        c2 = [np.zeros(b.nm) for _ in range(3)]
+        c3 = [np.zeros(b.nm) for _ in range(3)]
+        vir = np.zeros(1)
+        e2g, e3g = c.threebody_term(*args, b.box, fx, fy, fz, *c2, *c3, vir)
+    assert abs(e3g - e3o) <= TOL * abs(e3o), (e3g, e3o)
+    if M.s2_term:
+        assert abs(e2g - e2o) <= TOL * abs(e2o), (e2g, e2o)
+        assert rel(np.stack(c2), np.stack([st.fxfs2, st.fyfs2, st.fzfs2])) <= TOL
+    assert rel(np.stack([fx, fy, fz]), np.stack([st.fxs, st.fys, st.fzs])) <= TOL
+    assert rel(np.stack(c3), np.stack([st.fxfs3, st.fyfs3, st.fzfs3])) <= TOL
+    assert abs(vir[0] - st.vir.value) <= TOL * abs(st.vir.value)
+
+
+@pytest.mark.parametrize("key", ["c1", "fs2fs3_128"])
+def test_hot_path(oracle, boxes, key):
+    O = oracle
+    m, b, M = boxes[key]
+    eo, st = O.hot_path(M, b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    with _ctx(m, b) as c:
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+        assert c.last_launches() > 0
+    e = r.energies
+    for k in ("scpe", "rcpe", "kcpe", "indpe", "fs3pe") + (("fs2pe",) if M.s2_term else ()):
+        assert abs(e[k] - eo[k]) <= TOL * abs(eo[k]), (k, e[k], eo[k])
+    assert abs(e["vir"] - eo["vir"]) <= TOL * abs(eo["vir"])
+    assert e["ind_iters"] == eo["ind_iters"]
+    assert rel(np.stack([r.fxs, r.fys, r.fzs]), np.stack([st.fxs, st.fys, st.fzs])) <= TOL
+    assert rel(np.stack([r.idmx, r.idmy, r.idmz]), np.stack([st.idmx, st.idmy, st.idmz])) <= TOL
+    assert rel(np.stack([r.fxfs3, r.fyfs3, r.fzfs3]), np.stack([st.fxfs3, st.fyfs3, st.fzfs3])) <= TOL
+
+
+def test_hot_path_device_matches_host(product, boxes):
+    import torch
+    m, b, M = boxes["fs2fs3_128"]
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.as_tensor(a, device=dev)
+    with _ctx(m, b) as c:
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+        f = [torch.zeros(b.xs.shape, dtype=torch.float64, device=dev) for _ in range(3)]
+        e = c.hot_path_device(T(b.x), T(b.y), T(b.z), T(b.xs), T(b.ys), T(b.zs), b.box, *f)
+    assert e["fs3pe"] == pytest.approx(r.energies["fs3pe"], rel=1e-12)
+    assert rel(np.stack([t.cpu().numpy() for t in f]), np.stack([r.fxs, r.fys, r.fzs])) <= 1e-12
+
+
+def test_fs2_known_answer_on_gpu(product):
+    """The reference's FS2 test (periodicity, finite differences, rigid virial) through the
+    C ABI: coordinates go in as Angstrom (bohr * bohr2a)."""
+    from pathlib import Path
+    m = Model(Path(__file__).parent / "golden" / "fs2_kat")
+    s = site_offsets()
+    with Context(m, 3, 40.0 * BOHR2A) as c:
+        def calc(r, box):
+            xs, ys, zs = (np.ascontiguousarray(s[a] * BOHR2A) for a in range(3))
+            fx, fy, fz = (np.zeros((3, 5)) for _ in range(3))
+            c2 = [np.zeros(3) for _ in range(3)]
+            c3 = [np.zeros(3) for _ in range(3)]
+            vir = np.zeros(1)
+            e2, _ = c.threebody_term(*(np.ascontiguousarray(r[a] * BOHR2A) for a in range(3)), xs, ys,
+                                     zs, box * BOHR2A, fx, fy, fz, *c2, *c3, vir)
+            return e2, vir[0], fx, fy, fz, c2[0], c2[1], c2[2]
+        log = run_fs2_kat(calc)
+    assert all(ok for *_, ok in log)
+
+
+def test_mixed_precision_threebody(oracle, boxes):
+    O = oracle
+    m, b, M = boxes["fs2fs3_128"]
+    args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
+    st = _state(O, b.nm, b.xs.shape[1])
+    M.s2_term, M.s3_term = 0, 1
+    try:
+        e2o, e3o = O.threebody_term(M, *args, b.box, st)
+    finally:
+        M.s2_term = 1
+    m.set("S2_term", 0)
+    try:
+        with _ctx(m, b, "mixed") as c:
+            fx, fy, fz = (np.zeros_like(b.xs) for _ in range(3))
+            c2 = [np.zeros(b.nm) for _ in range(3)]
+            c3 = [np.zeros(b.nm) for _ in range(3)]
+            vir = np.zeros(1)
+            _, e3g = c.threebody_term(*args, b.box, fx, fy, fz, *c2, *c3, vir)
+    finally:
+        m.set("S2_term", 1)
+    assert abs(e3g - e3o) <= 1e-5 * abs(e3o), (e3g, e3o)
+    Fg = np.stack([fx.sum(1), fy.sum(1), fz.sum(1)]) + np.stack(c3)
+    Fo = np.stack([st.fxs.sum(1), st.fys.sum(1), st.fzs.sum(1)]) + np.stack([st.fxfs3, st.fyfs3, st.fzfs3])
+    assert rel(Fg, Fo) <= MIXED_FTOL, rel(Fg, Fo)
+
+
+def test_maxit_reports_not_converged(product, boxes):
+    m, b, M = boxes["ragged_37"]
+    with _ctx(m, b) as c:
+        c.set_maxit(2)
+        with pytest.raises(CcpError) as e:
+            c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+        assert e.value.code == 2
+        c.set_maxit(500)
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)  # context stays usable
+        assert r.energies["ind_iters"] > 2
