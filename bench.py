@@ -123,12 +123,16 @@ def time_device(ctx, box, steps, warmup, flush, torch):
     for _ in range(warmup):
         e = ctx.hot_path_device(x, y, z, xs, ys, zs, box.box, *f, *c2, *c3, *mu)
     torch.cuda.synchronize()
+    for t in f:
+        t.zero_()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     phases = []
     launches = 0
     t0 = time.perf_counter()
     for k in range(steps):
         flush.add_(1.0)
+        for t in f:  # site forces accumulate (reference semantics): start each step at zero
+            t.zero_()
         ev[k][0].record(stream)
         e = ctx.hot_path_device(x, y, z, xs, ys, zs, box.box, *f, *c2, *c3, *mu)
         ev[k][1].record(stream)
@@ -221,6 +225,25 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_single(which):
+    import torch
+    from ccpol23_plus_2025_mbmd_b200 import Context
+    model, box, cfg = build_inputs(0)
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    args = [T(a) for a in (box.x, box.y, box.z, box.xs, box.ys, box.zs)]
+    for prec in (("fp64", "mixed") if which == "both" else (which,)):
+        with Context(model, box.nm, box.box, device=0, precision=prec) as ctx:
+            ctx.set_timing(True)
+            f = [torch.zeros_like(args[3]) for _ in range(3)]
+            e = ctx.hot_path_device(*args, box.box, *f)
+            torch.cuda.synchronize()
+            print(json.dumps({"form": prec, "phase_ms": [round(v, 4) for v in ctx.phase_ms()],
+                              "launches": ctx.last_launches(), "ind_iters": e["ind_iters"],
+                              "n_fs3_triples": e["n_fs3_triples"], "n_fs3_blend": e["n_fs3_blend"],
+                              "n_fs2_triples": e["n_fs2_triples"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -228,9 +251,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--single", choices=["fp64", "mixed", "both"],
+                    help="one device-resident evaluation per form, no timing loop (profiling)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.single:
+        run_single(args.single)
         return
     import torch
     rank, world, local = dist_env()
@@ -286,10 +314,24 @@ def main():
     # mixed vs FP64 relative errors on the same box (three-body terms change, the rest is
     # FP64 in both forms)
     f64, fmx = results["fp64"], results["mixed"]
-    ferr = float(np.linalg.norm(fmx["forces"] - f64["forces"]) / np.linalg.norm(f64["forces"]))
-    c3err = float(np.linalg.norm(fmx["com3"] - f64["com3"]) / np.linalg.norm(f64["com3"]))
+
+    def mol_force_torque(r):
+        F = r["forces"]  # (3, nm, ld) site forces of the last step
+        tot = F.sum(2) + r["com2"] + r["com3"]
+        sx, sy, sz = box.xs, box.ys, box.zs
+        tq = np.stack([(sy * F[2] - sz * F[1]).sum(1), (sz * F[0] - sx * F[2]).sum(1),
+                       (sx * F[1] - sy * F[0]).sum(1)])
+        return tot, tq
+
+    T64, Q64 = mol_force_torque(f64)
+    Tmx, Qmx = mol_force_torque(fmx)
+    rl = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    ferr = rl(fmx["forces"], f64["forces"])
+    molerr = rl(Tmx, T64)
+    tqerr = rl(Qmx, Q64)
+    c3err = rl(fmx["com3"], f64["com3"])
     eerr = abs(fmx["energies"]["fs3pe"] - f64["energies"]["fs3pe"]) / abs(f64["energies"]["fs3pe"])
-    head = "mixed" if max(ferr, c3err) <= 1e-5 else "fp64"
+    head = "mixed" if max(ferr, molerr, tqerr) <= 1e-5 else "fp64"
     H = out[head]
     # roofline of the dominant kernel (FS3) of the headline form
     e = results[head]["energies"]
@@ -310,7 +352,8 @@ def main():
                    "parallelism": f"replicas x{world}"},
         "triples_per_s": H["triples_per_s"],
         "fp64": out["fp64"], "mixed": out["mixed"],
-        "mixed_vs_fp64": {"rel_site_force_err": ferr, "rel_fs3_com_force_err": c3err,
+        "mixed_vs_fp64": {"rel_site_force_err": ferr, "rel_molecule_force_err": molerr,
+                          "rel_molecule_torque_err": tqerr, "rel_fs3_com_force_err": c3err,
                           "rel_fs3_energy_err": eerr},
         "e2e": {"value": H["e2e_ns_day"], "unit": "ns/day",
                 "h2d_bytes_per_step": results[head]["h2d"], "d2h_bytes_per_step": results[head]["d2h"]},

@@ -75,6 +75,9 @@ struct ccp_context {
   // induction
   double *d_mu = nullptr, *d_e0r = nullptr, *d_e0k = nullptr, *d_e0slf = nullptr, *d_e0s = nullptr;
   double *d_eir = nullptr, *d_eik = nullptr, *d_eislf = nullptr, *d_eis = nullptr;
+  double *d_mu2 = nullptr, *d_e0tot = nullptr, *d_eim = nullptr;
+  double4 *d_T4 = nullptr, *d_S4 = nullptr;
+  double *d_TB = nullptr, *d_SB = nullptr;
   // lists
   int cap = 0, tri_cap = 0, pair_cap = 0;
   int *d_nbr = nullptr, *d_ncnt = nullptr;
@@ -113,7 +116,8 @@ void free_ctx(ccp_context *c) {
                 c->d_act, c->d_comb, c->d_s17,  c->d_f,     c->d_fc2,  c->d_fc3,   c->d_scal,
                 c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
-                c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types};
+                c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
+                c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
   for (void *p : dp)
     if (p) cudaFree(p);
   if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -139,8 +143,13 @@ int ensure_lists(ccp_context *c, int cap, int tri_cap, int pair_cap) {
   if (cap > c->cap) {
     if (c->d_nbr) cudaFree(c->d_nbr);
     if (c->d_nbrv) cudaFree(c->d_nbrv);
+    if (c->d_T4) cudaFree(c->d_T4);
+    if (c->d_TB) cudaFree(c->d_TB);
     CK(dalloc(&c->d_nbr, (size_t)c->nm * cap));
     CK(dalloc(&c->d_nbrv, (size_t)c->nm * cap));
+    const size_t npp = (size_t)std::max(c->S.np, 1) * std::max(c->S.np, 1);
+    CK(dalloc(&c->d_T4, (size_t)c->nm * cap * npp));
+    CK(dalloc(&c->d_TB, (size_t)c->nm * cap * npp));
     c->cap = cap;
   }
   if (tri_cap > c->tri_cap) {
@@ -328,8 +337,8 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       LK(launch_kspace_sums(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
                             c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
       LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->alpha, nullptr, c->d_f, c->d_scal,
-                              st));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, nullptr, nullptr,
+                              nullptr, c->d_scal, st));
     }
     mark(3);
     if (mask & T_INDUCTION) {
@@ -339,24 +348,26 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
                             c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->alpha, c->d_e0k, c->d_f, c->d_scal,
-                              st));
+                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, nullptr, nullptr,
+                              nullptr, c->d_scal, st));
       if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, st));
+      LK(launch_dip_tensor(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt,
+                           c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, st));
+      LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
+                             st));
       CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * nm * S.np * 3, st));
       int it = 0;
       double change = 10.0;
       while (change > 1.0e-20 && it < c->maxit) {
         CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
-        LK(launch_pair_dipfield(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
-                                c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_eir, c->d_eis,
-                                c->d_eislf, st));
+        LK(launch_dip_matvec(c->d_nbr, c->d_ncnt, c->cap, nm, S.np, c->d_T4, c->d_TB, c->d_S4,
+                             c->d_SB, c->d_mu, c->d_eim, st));
         LK(launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
                               c->kmax[2], c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
         LK(launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                                c->kmax[2], c->d_mu, c->d_sk, c->alpha, c->d_eik, c->d_f,
-                                c->d_scal, st));
-        LK(launch_dip_update(nm, S, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_eir, c->d_eik,
-                             c->d_eislf, c->d_eis, c->d_mu, c->d_scal, st));
+                                c->kmax[2], c->d_mu, c->d_sk, nullptr, nullptr, c->d_e0tot,
+                                c->d_eim, c->d_mu2, c->d_scal, st));
+        std::swap(c->d_mu, c->d_mu2);
         CK(cudaMemcpyAsync(c->h_scal + S_IND_CHANGE, c->d_scal + S_IND_CHANGE, 2 * sizeof(double),
                            cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
@@ -375,8 +386,8 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       LK(launch_kspace_sums(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
                             c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
       LK(launch_kspace_gather(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->alpha, nullptr, c->d_f, c->d_scal,
-                              st));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, nullptr, nullptr,
+                              nullptr, c->d_scal, st));
     }
     mark(4);
     if (mask & T_FS2) {
@@ -703,7 +714,11 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
             dalloc(&c->d_e0k, np3) == cudaSuccess && dalloc(&c->d_e0slf, np3) == cudaSuccess &&
             dalloc(&c->d_e0s, np3) == cudaSuccess && dalloc(&c->d_eir, std::max(np3, 3 * nsi)) == cudaSuccess &&
             dalloc(&c->d_eik, np3) == cudaSuccess && dalloc(&c->d_eislf, np3) == cudaSuccess &&
-            dalloc(&c->d_eis, np3) == cudaSuccess && dalloc(&c->d_ncnt, n) == cudaSuccess;
+            dalloc(&c->d_eis, np3) == cudaSuccess && dalloc(&c->d_ncnt, n) == cudaSuccess &&
+            dalloc(&c->d_mu2, np3) == cudaSuccess && dalloc(&c->d_e0tot, np3) == cudaSuccess &&
+            dalloc(&c->d_eim, np3) == cudaSuccess &&
+            dalloc(&c->d_S4, n * std::max(S.np, 1) * std::max(S.np, 1)) == cudaSuccess &&
+            dalloc(&c->d_SB, n * std::max(S.np, 1) * std::max(S.np, 1)) == cudaSuccess;
   if (!ok) return fail("device allocation");
   if (cudaMemset(c->d_e0s, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
   if (cudaMemset(c->d_mu, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");

@@ -139,16 +139,16 @@ cudaError_t launch_self_static(const double *x, const double *y, const double *z
                                const double *xs, const double *ys, const double *zs, int nm,
                                int ld, SiteSets S, EwaldParams P, double *f, double *e0slf,
                                double *scal, cudaStream_t st);
-cudaError_t launch_pair_dipfield(const double *x, const double *y, const double *z,
-                                 const double *xs, const double *ys, const double *zs,
-                                 int ld, const double4 *act, const int *nbr,
-                                 const double4 *nbrv, const int *ncnt, int cap, int nm,
-                                 SiteSets S, EwaldParams P, const double *mu, double *eir,
-                                 double *eis, double *eislf, cudaStream_t st);
-cudaError_t launch_dip_update(int nm, SiteSets S, const double *e0r, const double *e0k,
-                              const double *e0slf, const double *e0s, const double *eir,
-                              const double *eik, const double *eislf, const double *eis,
-                              double *mu, double *scal, cudaStream_t st);
+cudaError_t launch_dip_tensor(const double *x, const double *y, const double *z,
+                              const double *xs, const double *ys, const double *zs, int ld,
+                              const double4 *act, const int *nbr, const double4 *nbrv,
+                              const int *ncnt, int cap, int nm, SiteSets S, EwaldParams P,
+                              double4 *T4, double *TB, double4 *S4, double *SB, cudaStream_t st);
+cudaError_t launch_dip_matvec(const int *nbr, const int *ncnt, int cap, int nm, int np,
+                              const double4 *T4, const double *TB, const double4 *S4,
+                              const double *SB, const double *mu, double *eim, cudaStream_t st);
+cudaError_t launch_static_total(int n, const double *a, const double *b, const double *c,
+                                const double *d, double *out, cudaStream_t st);
 cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,
                                  const double *xs, const double *ys, const double *zs,
                                  int ld, const double4 *act, const int *nbr,
@@ -171,10 +171,13 @@ cudaError_t launch_ktab(const double4 *com, const double4 *act, int nm, SiteSets
 cudaError_t launch_kspace_sums(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
                                SiteSets S, int kl, int km, int kn, const double *mu,
                                double *sk, double *scal, double alpha, cudaStream_t st);
+// MODE 2 also applies the Jacobi update: e0 = total static field, eim = real-space part of
+// the dipole field (real + short-range + self), mu read, mu_out written, change/energy into
+// scal.  out receives the field for MODE 1; f the forces for MODES 0 and 3.
 cudaError_t launch_kspace_gather(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
                                  SiteSets S, int kl, int km, int kn, const double *mu,
-                                 const double *sk, double alpha, double *out, double *f,
-                                 double *scal, cudaStream_t st);
+                                 const double *sk, double *out, double *f, const double *e0,
+                                 const double *eim, double *mu_out, double *scal, cudaStream_t st);
 
 // three-body
 cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,

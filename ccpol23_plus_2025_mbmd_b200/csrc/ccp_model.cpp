@@ -404,7 +404,9 @@ int ccp_model_load(const char *dir, ccp_model **out) {
     delete m;
     return g_err.rfind("FIELD:", 0) == 0 ? CCP_ERR_BAD_INPUT : CCP_ERR_IO;
   }
-  if (m->nonadditive_3b) {
+  // The reference opens the FS3 files whenever the 3-body term is on; they are required
+  // here only when FS3 itself is on, so an FS2-only parameter set needs no FS3 tables.
+  if (m->nonadditive_3b && m->s3_term) {
     if (!parse_fs3(d + "data3b_full", m->sr) || !parse_fs3(d + "data3b_full_LR_4p5", m->lr)) {
       if (g_err.empty()) set_error("cannot read the FS3 parameter files in " + d);
       delete m;

@@ -17,7 +17,6 @@ namespace {
 
 constexpr int kKB = 8;       // k-vectors per structure-factor block
 constexpr int kSumThreads = 256;
-constexpr int kKT = 64;      // k-vectors per shared-memory tile in the gather
 
 __global__ void k_ktab(const double4 *__restrict__ com, const double4 *__restrict__ act, int nm,
                        int na, double box, int kl, int km, int kn, int k1, double2 *tab) {
@@ -184,44 +183,64 @@ __global__ void __launch_bounds__(kSumThreads)
   }
 }
 
+// One warp per target site: the site's phase tables (3 axes x k1 entries) are staged in
+// shared memory, lanes stride over the k-vectors, and the warp reduces at the end.
+// MODE 2 also performs the Jacobi update of that site (nb_induction_model.f90:1317-1359):
+// E0 = r + k + self + short-range static fields, Eidm = real/short-range/self part (from the
+// T.mu matvec) + this reciprocal part, mu <- alpha (E0 + Eidm), with the squared change
+// and the energy -1/2 alpha (E0 + Eidm).E0 reduced into scal.
+constexpr int kGatherWarps = 8;
+
 template <int MODE>
-__global__ void k_kgather(const KVec *__restrict__ kv, int nk, const double2 *__restrict__ tab,
-                          int nm, SiteSets S, int k1, const double *__restrict__ mu,
-                          const double *__restrict__ sk, double *out, double *f) {
-  __shared__ KVec kt[kKT];
-  __shared__ double4 st4[kKT];
+__global__ void __launch_bounds__(kGatherWarps * 32)
+    k_kgather(const KVec *__restrict__ kv, int nk, const double2 *__restrict__ tab, int nm,
+              SiteSets S, int k1, const double *__restrict__ mu, const double *__restrict__ sk,
+              double *out, double *f, const double *__restrict__ e0, const double *__restrict__ eim,
+              double *mu_out, double *scal) {
+  extern __shared__ double2 stab[];
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int per = target_count(MODE, S);
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int nt = nm * per;
-  const bool live = t < nt;
-  const int i = live ? t / per : 0, r = live ? t % per : 0;
-  const int a = target_slot(MODE, S, r);
-  const int st = i * S.na + a;
-  const int N = nm * S.na;
-  const double q = S.q[a];
-  double mx = 0.0, my = 0.0, mz = 0.0;
-  const int p = S.p_of_a[a];
-  if (MODE == 3 && p >= 0 && live) {
-    mx = mu[((size_t)i * S.np + p) * 3 + 0];
-    my = mu[((size_t)i * S.np + p) * 3 + 1];
-    mz = mu[((size_t)i * S.np + p) * 3 + 2];
-  }
-  double ax = 0.0, ay = 0.0, az = 0.0;
-  for (int k0 = 0; k0 < nk; k0 += kKT) {
-    __syncthreads();
-    for (int u = threadIdx.x; u < kKT && k0 + u < nk; u += blockDim.x) {
-      kt[u] = kv[k0 + u];
-      const double *s = sk + (size_t)(k0 + u) * 4;
-      st4[u] = make_double4(s[0], s[1], s[2], s[3]);
+  const int t = blockIdx.x * kGatherWarps + wl;
+  const bool live = t < nm * per;
+  double ch = 0.0, en = 0.0;
+  if (live) {
+    const int i = t / per, r = t % per;
+    const int a = target_slot(MODE, S, r);
+    const int st = i * S.na + a;
+    const int N = nm * S.na;
+    double2 *my = stab + (size_t)wl * 3 * k1;
+    for (int u = lane; u < 3 * k1; u += 32) my[u] = tab[(size_t)u * N + st];
+    __syncwarp();
+    const double q = S.q[a];
+    double mx = 0.0, my_ = 0.0, mz = 0.0;
+    const int p = S.p_of_a[a];
+    if (MODE == 3 && p >= 0) {
+      mx = mu[((size_t)i * S.np + p) * 3 + 0];
+      my_ = mu[((size_t)i * S.np + p) * 3 + 1];
+      mz = mu[((size_t)i * S.np + p) * 3 + 2];
     }
-    __syncthreads();
-    if (!live) continue;
-    const int nkt = min(kKT, nk - k0);
-    for (int u = 0; u < nkt; u++) {
-      const KVec K = kt[u];
-      const double4 A = st4[u];
-      double c, s;
-      expikr(tab, N, k1, st, K.l, K.m, K.n, c, s);
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int k = lane; k < nk; k += 32) {
+      const KVec K = kv[k];
+      const double4 A = *reinterpret_cast<const double4 *>(sk + (size_t)k * 4);
+      const double2 el = my[K.l];
+      const double2 em = my[k1 + (K.m < 0 ? -K.m : K.m)];
+      const double2 en = my[2 * k1 + (K.n < 0 ? -K.n : K.n)];
+      double clm, slm, c, s;
+      if (K.m >= 0) {
+        clm = el.x * em.x - el.y * em.y;
+        slm = el.y * em.x + em.y * el.x;
+      } else {
+        clm = el.x * em.x + el.y * em.y;
+        slm = el.y * em.x - em.y * el.x;
+      }
+      if (K.n >= 0) {
+        c = clm * en.x - slm * en.y;
+        s = slm * en.x + clm * en.y;
+      } else {
+        c = clm * en.x + slm * en.y;
+        s = slm * en.x - clm * en.y;
+      }
       double g;
       if (MODE == 0) {
         g = 4.0 * kR4pie0 * K.ak * ((q * s) * A.x - (q * c) * A.y);
@@ -233,27 +252,62 @@ __global__ void k_kgather(const KVec *__restrict__ kv, int nk, const double2 *__
         const double mufac = -4.0 * K.ak * (c * A.z + s * A.w);
         const double qfac = -4.0 * K.ak * (-c * A.x - s * A.y);
         const double mufaci = -4.0 * K.ak * (c * A.w - s * A.z);
-        const double mk = mx * K.rl + my * K.rm + mz * K.rn;
+        const double mk = mx * K.rl + my_ * K.rm + mz * K.rn;
         g = q * mufac + mk * (qfac + mufaci);
       }
       ax += K.rl * g;
       ay += K.rm * g;
       az += K.rn * g;
     }
+    ax = warp_sum(ax);
+    ay = warp_sum(ay);
+    az = warp_sum(az);
+    if (lane == 0) {
+      if (MODE == 0 || MODE == 3) {
+        const double sc = MODE == 3 ? kR4pie0 : 1.0;
+        const size_t nfs = (size_t)nm * S.ns;
+        const size_t o = (size_t)i * S.ns + S.asite[a];
+        f[o] += sc * ax;
+        f[nfs + o] += sc * ay;
+        f[2 * nfs + o] += sc * az;
+      } else if (MODE == 1) {
+        const size_t o = ((size_t)i * S.np + r) * 3;
+        out[o] = ax;
+        out[o + 1] = ay;
+        out[o + 2] = az;
+      } else {
+        const size_t o = ((size_t)i * S.np + r) * 3;
+        const double kE[3] = {ax, ay, az};
+        const double polr = S.apol[r];
+        double Et[3], E0[3];
+        for (int c3 = 0; c3 < 3; c3++) {
+          E0[c3] = e0[o + c3];
+          Et[c3] = (eim[o + c3] + kE[c3]) + E0[c3];
+          const double m = polr * Et[c3];
+          const double d = mu[o + c3] - m;
+          ch += d * d;
+          mu_out[o + c3] = m;
+        }
+        en = -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
+      }
+    }
   }
-  if (!live) return;
-  if (MODE == 0 || MODE == 3) {
-    const double sc = MODE == 3 ? kR4pie0 : 1.0;
-    const size_t nfs = (size_t)nm * S.ns;
-    const size_t o = (size_t)i * S.ns + S.asite[a];
-    f[o] += sc * ax;
-    f[nfs + o] += sc * ay;
-    f[2 * nfs + o] += sc * az;
-  } else {
-    const size_t o = ((size_t)i * S.np + r) * 3;
-    out[o] = ax;
-    out[o + 1] = ay;
-    out[o + 2] = az;
+  if (MODE == 2) {
+    __shared__ double red[2][kGatherWarps];
+    if (lane == 0) {
+      red[0][wl] = ch;
+      red[1][wl] = en;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double c2 = 0.0, e2 = 0.0;
+      for (int w = 0; w < kGatherWarps; w++) {
+        c2 += red[0][w];
+        e2 += red[1][w];
+      }
+      atomicAdd(&scal[S_IND_CHANGE], c2);
+      atomicAdd(&scal[S_IND_ENERGY], e2);
+    }
   }
 }
 
@@ -292,20 +346,19 @@ cudaError_t launch_kspace_sums(int mode, const KVec *kv, int nk, const double2 *
 
 cudaError_t launch_kspace_gather(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
                                  SiteSets S, int kl, int km, int kn, const double *mu,
-                                 const double *sk, double alpha, double *out, double *f,
-                                 double *scal, cudaStream_t st) {
-  (void)alpha;
-  (void)scal;
+                                 const double *sk, double *out, double *f, const double *e0,
+                                 const double *eim, double *mu_out, double *scal, cudaStream_t st) {
   const int k1 = k1_of(kl, km, kn);
   const int per_t = mode == 0 ? S.nq : (mode == 3 ? S.na : S.np);
   const int n = nm * per_t;
-  const int threads = 128;
-  const int blocks = (n + threads - 1) / threads;
+  const int blocks = (n + kGatherWarps - 1) / kGatherWarps;
+  const size_t smem = sizeof(double2) * 3 * (size_t)k1 * kGatherWarps;
+  const int th = kGatherWarps * 32;
   switch (mode) {
-    case 0: k_kgather<0><<<blocks, threads, 0, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f); break;
-    case 1: k_kgather<1><<<blocks, threads, 0, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f); break;
-    case 2: k_kgather<2><<<blocks, threads, 0, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f); break;
-    default: k_kgather<3><<<blocks, threads, 0, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f); break;
+    case 0: k_kgather<0><<<blocks, th, smem, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f, e0, eim, mu_out, scal); break;
+    case 1: k_kgather<1><<<blocks, th, smem, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f, e0, eim, mu_out, scal); break;
+    case 2: k_kgather<2><<<blocks, th, smem, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f, e0, eim, mu_out, scal); break;
+    default: k_kgather<3><<<blocks, th, smem, st>>>(kv, nk, tab, nm, S, k1, mu, sk, out, f, e0, eim, mu_out, scal); break;
   }
   return cudaGetLastError();
 }

@@ -301,172 +301,6 @@ __global__ void k_self_static(const double *__restrict__ x, const double *__rest
   }
 }
 
-// ------------------------------------------- dipole field (one Jacobi iteration, real)
-// rspace_efield_idm (nb_induction_model.f90:1409-1569), shortrange_efield_idm_damped
-// (:5634-5789) and self_efield_idm (:2663-2829).
-template <int NP>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    k_pair_dipfield(const double *__restrict__ x, const double *__restrict__ y,
-                    const double *__restrict__ z, const double *__restrict__ xs,
-                    const double *__restrict__ ys, const double *__restrict__ zs, int ld,
-                    const double4 *__restrict__ act, const int *__restrict__ nbr,
-                    const double4 *__restrict__ nbrv, const int *__restrict__ ncnt, int cap,
-                    int nm, SiteSets S, EwaldParams P, const double *__restrict__ mu,
-                    double *eir, double *eis, double *eislf) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= nm) return;
-  const int na = S.na, np = S.np;
-  const double alp = P.alpha, alp3 = alp * alp * alp;
-  double4 sp[NP];
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-    sp[p] = p < np ? ld4(&act[(size_t)i * na + S.a_of_p[p]]) : make_double4(0, 0, 0, 0);
-  double Er[NP][3], Es[NP][3];
-#pragma unroll
-  for (int p = 0; p < NP; p++) Er[p][0] = Er[p][1] = Er[p][2] = Es[p][0] = Es[p][1] = Es[p][2] = 0.0;
-  const int cnt = ncnt[i];
-  for (int n = lane; n < cnt; n += 32) {
-    const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
-    if (!(c.w < P.rcutsd)) continue;
-    const int j = nbr[(size_t)i * cap + n];
-#pragma unroll
-    for (int q = 0; q < NP; q++) {
-      if (q >= np) break;
-      const double4 sq = ld4(&act[(size_t)j * na + S.a_of_p[q]]);
-      const double mx = mu[((size_t)j * np + q) * 3 + 0];
-      const double my = mu[((size_t)j * np + q) * 3 + 1];
-      const double mz = mu[((size_t)j * np + q) * 3 + 2];
-#pragma unroll
-      for (int p = 0; p < NP; p++) {
-        if (p >= np) break;
-        const double dx = c.x + sp[p].x - sq.x;
-        const double dy = c.y + sp[p].y - sq.y;
-        const double dz = c.z + sp[p].z - sq.z;
-        const double d2 = dx * dx + dy * dy + dz * dz;
-        const double drr = sqrt(d2);
-        const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d5i = d3i * d2i;
-        const double dotj = mx * dx + my * dy + mz * dz;
-        const double ad = alp * drr;
-        const double expar2 = exp(-(ad * ad));
-        const double ec = erfc(alp * drr);
-        const double d3ii = ec * d3i + P.twosqpi * alp * expar2 * d2i;
-        const double d5ii = ec * d5i + P.twosqpi * alp * expar2 * d2i * d2i +
-                            2.0 * P.twosqpi * alp3 * expar2 * d2i / 3.0;
-        Er[p][0] += 3.0 * d5ii * dotj * dx - mx * d3ii;
-        Er[p][1] += 3.0 * d5ii * dotj * dy - my * d3ii;
-        Er[p][2] += 3.0 * d5ii * dotj * dz - mz * d3ii;
-        if (P.damped) {
-          const double g = tt<3>(P.delta3, drr) - 1.0;
-          Es[p][0] += g * (3.0 * d5i * dotj * dx - mx * d3i);
-          Es[p][1] += g * (3.0 * d5i * dotj * dy - my * d3i);
-          Es[p][2] += g * (3.0 * d5i * dotj * dz - mz * d3i);
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      Er[p][k] = warp_sum(Er[p][k]);
-      Es[p][k] = warp_sum(Es[p][k]);
-    }
-  // self field: point term + erf-screened intramolecular dipole-dipole (lanes 0..np-1)
-  if (lane < np) {
-    const int p = lane, s = S.psite[p];
-    const double selffac = 4.0 * alp3 / (3.0 * sqrt(kPi));
-    double E[3];
-    for (int k = 0; k < 3; k++) E[k] = selffac * mu[((size_t)i * np + p) * 3 + k];
-    double L[3] = {0.0, 0.0, 0.0};
-    const double xi = x[i], yi = y[i], zi = z[i];
-    for (int q = 0; q < np; q++) {
-      if (q == p) continue;
-      const int t = S.psite[q];
-      const size_t os = (size_t)i * ld + s, ot = (size_t)i * ld + t;
-      const double dx = (xi + xs[os]) - (xi + xs[ot]);
-      const double dy = (yi + ys[os]) - (yi + ys[ot]);
-      const double dz = (zi + zs[os]) - (zi + zs[ot]);
-      const double drr = sqrt(dx * dx + dy * dy + dz * dz);
-      const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d5i = d3i * d2i;
-      const double mx = mu[((size_t)i * np + q) * 3 + 0];
-      const double my = mu[((size_t)i * np + q) * 3 + 1];
-      const double mz = mu[((size_t)i * np + q) * 3 + 2];
-      const double dotj = mx * dx + my * dy + mz * dz;
-      const double ad = alp * drr;
-      const double expar2 = exp(-(ad * ad));
-      const double ef = erf(alp * drr);
-      const double d3ii = ef * d3i - P.twosqpi * alp * expar2 * d2i;
-      const double d5ii = ef * d5i - P.twosqpi * alp * expar2 * d2i * d2i -
-                          2.0 * P.twosqpi * alp3 * expar2 * d2i / 3.0;
-      L[0] -= 3.0 * d5ii * dotj * dx - mx * d3ii;
-      L[1] -= 3.0 * d5ii * dotj * dy - my * d3ii;
-      L[2] -= 3.0 * d5ii * dotj * dz - mz * d3ii;
-    }
-    for (int k = 0; k < 3; k++) eislf[((size_t)i * np + p) * 3 + k] = E[k] + L[k];
-  }
-  if (lane == 0) {
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      if (p >= np) break;
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        eir[((size_t)i * np + p) * 3 + k] = Er[p][k];
-        eis[((size_t)i * np + p) * 3 + k] = Es[p][k];
-      }
-    }
-  }
-}
-
-// --------------------------------------------------------- Jacobi update (iteridm)
-// nb_induction_model.f90:1317-1359: E0 = r + k + self + short-range, same for the dipole
-// field; mu <- alpha (E0 + Eidm); change and energy use the pre-update field.
-__global__ void k_dip_update(int nm, SiteSets S, const double *__restrict__ e0r,
-                             const double *__restrict__ e0k, const double *__restrict__ e0slf,
-                             const double *__restrict__ e0s, const double *__restrict__ eir,
-                             const double *__restrict__ eik, const double *__restrict__ eislf,
-                             const double *__restrict__ eis, double *mu, double *scal) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  double ch = 0.0, en = 0.0;
-  if (t < nm * S.np) {
-    const int p = t % S.np;
-    const double polr = S.apol[p];
-    double E0[3], Et[3], m[3];
-    for (int k = 0; k < 3; k++) {
-      const size_t o = (size_t)t * 3 + k;
-      E0[k] = e0r[o] + e0k[o] + e0slf[o] + e0s[o];
-      const double Ei = eir[o] + eik[o] + eislf[o] + eis[o];
-      Et[k] = Ei + E0[k];
-      m[k] = polr * Et[k];
-    }
-    const double dx = mu[(size_t)t * 3] - m[0], dy = mu[(size_t)t * 3 + 1] - m[1],
-                 dz = mu[(size_t)t * 3 + 2] - m[2];
-    ch = dx * dx + dy * dy + dz * dz;
-    for (int k = 0; k < 3; k++) mu[(size_t)t * 3 + k] = m[k];
-    en = -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
-  }
-  __shared__ double red[2][32];
-  ch = warp_sum(ch);
-  en = warp_sum(en);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) {
-    red[0][wid] = ch;
-    red[1][wid] = en;
-  }
-  __syncthreads();
-  if (wid == 0) {
-    const int nw = blockDim.x >> 5;
-    ch = lane < nw ? red[0][lane] : 0.0;
-    en = lane < nw ? red[1][lane] : 0.0;
-    ch = warp_sum(ch);
-    en = warp_sum(en);
-    if (lane == 0) {
-      atomicAdd(&scal[S_IND_CHANGE], ch);
-      atomicAdd(&scal[S_IND_ENERGY], en);
-    }
-  }
-}
-
 // ------------------------------------------------------------ induction forces (real)
 // real_forces (nb_induction_model.f90:3069-3631), shortrange_forces_damped (:5975-6557)
 // and self_forces (:4841-5360).  Force on active site a of i from active site b of j:
@@ -725,34 +559,6 @@ cudaError_t launch_self_static(const double *x, const double *y, const double *z
   const int threads = 128;
   k_self_static<<<(nm + threads - 1) / threads, threads, 0, st>>>(x, y, z, xs, ys, zs, nm, ld, S,
                                                                   P, f, e0slf, scal);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_pair_dipfield(const double *x, const double *y, const double *z,
-                                 const double *xs, const double *ys, const double *zs,
-                                 int ld, const double4 *act, const int *nbr,
-                                 const double4 *nbrv, const int *ncnt, int cap, int nm,
-                                 SiteSets S, EwaldParams P, const double *mu, double *eir,
-                                 double *eis, double *eislf, cudaStream_t st) {
-  const int threads = kWarpsPerBlock * 32;
-  const int blocks = (nm + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  if (S.np <= 3)
-    k_pair_dipfield<3><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt,
-                                                   cap, nm, S, P, mu, eir, eis, eislf);
-  else
-    k_pair_dipfield<kMaxP><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv,
-                                                       ncnt, cap, nm, S, P, mu, eir, eis, eislf);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_dip_update(int nm, SiteSets S, const double *e0r, const double *e0k,
-                              const double *e0slf, const double *e0s, const double *eir,
-                              const double *eik, const double *eislf, const double *eis,
-                              double *mu, double *scal, cudaStream_t st) {
-  const int threads = 256;
-  const int n = nm * S.np;
-  k_dip_update<<<(n + threads - 1) / threads, threads, 0, st>>>(nm, S, e0r, e0k, e0slf, e0s, eir,
-                                                                eik, eislf, eis, mu, scal);
   return cudaGetLastError();
 }
 
