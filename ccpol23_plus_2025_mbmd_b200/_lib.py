@@ -6,11 +6,13 @@ immediately when the library is missing: there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libccpol23_b200.so"
+LIB_PATH = Path(os.environ.get("CCP_LIB_PATH") or
+                Path(__file__).resolve().parent / "lib" / "libccpol23_b200.so")
 
 CCP_OK = 0
 CCP_ERR_BAD_INPUT = 1

@@ -18,11 +18,15 @@
 // them once and its lanes then walk the spectators k (5 spectator sites each).
 #include "ccp_device.cuh"
 
+// FS3 blocks resident per SM the register allocation targets (2: <= 96 registers).
+#ifndef CCP_FS3_MINBLOCKS
+#define CCP_FS3_MINBLOCKS 2
+#endif
+
 using namespace ccpd;
 
 namespace {
 
-constexpr int kFs3Threads = 224;  // 7 warps; 3 x 289 = 867 site-pair items ~ 4 per thread
 constexpr int kPairs = 289;
 constexpr int kItems = 3 * kPairs;
 constexpr int kNt = 6;            // FS3 site types
@@ -134,17 +138,49 @@ __device__ __forceinline__ void triple_geom(double4 ci, double4 cj, double4 ck, 
   g.djk2 = norm2x(g.xjk, g.yjk, g.zjk);
 }
 
+// ---- FS3 sweep, register-blocked form --------------------------------------------
+// Sites are padded from 17 to 18 (a dummy with zero weight after site 0) so that the six
+// type blocks [0,d], [1,2], [3,4], [5..8], [9..12], [13..16] start at even padded indices.
+// With U0 = e and U1 = e d for every site pair, each gradient pass is, per type block of
+// the summed (third) site, four small matrix products
+//     M_xy(a, b) = sum_{c in block} U_x(a, c) V_y(b, c),
+// contracted with that type triple's 8 coefficients; a thread owns a 2x2 tile of outputs
+// (both rows and both columns of one type) and keeps M in registers.
+constexpr int kP = 18;       // padded sites
+constexpr int kRS = 19;      // row stride (conflict-free for 8 distinct rows of 16 B)
+constexpr int kTile = 9;     // 2x2 tiles per dimension
+constexpr int kPassThreads = 96;
+constexpr int kFs3Block = 3 * kPassThreads;
+
+__device__ __forceinline__ int pidx(int s) { return s == 0 ? 0 : s + 1; }
+__constant__ int kPType[kP] = {0, 0, 1, 1, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5};
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
 template <typename T>
 struct Fs3Smem {
-  double coef[2][kCoef];     // SR, LR coefficient by type triple
-  double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
-  double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
-  T e[kItems];               // exp(-b r) * damping of each site pair
-  T d[kItems];               // r of each site pair
-  T dl[kItems];              // d ln(e)/dr of each site pair
-  double G[kItems];          // accumulated dE/dr / r of each site pair (site-force weights)
-  double red[kFs3Threads / 32];
-  int type[kNs3];
+  using V2 = typename Vec2<T>::type;
+  double coef[2][kCoef];         // SR, LR coefficient by type triple
+  double bgr[2][3][kPairs];      // SR, LR b, g, r0 of each site pair
+  double site[3][kNs3][3];       // site offsets (bohr) of i, j, k
+  V2 uu[3][kP][kRS];             // (e, e d) of each site pair, families ij, ik, jk
+  V2 dl[3][kP][kRS];             // (d, d ln e / dr)
+  double G[3][kP][kRS];          // accumulated site-force weights
+  double red[kFs3Block / 32];
+  double cv[3][3];               // COM vectors ij, ik, jk of the current triple (bohr)
+  double rr[3];                  // their lengths
+  double sc[6];                  // fdmp, dfdmp, smfun, cf, energy, comc
+  int mol[3];
+  int branch;
 };
 
 template <typename T>
@@ -174,214 +210,316 @@ __device__ __forceinline__ void family(int p, int &m1, int &m2) {
   m2 = p == 0 ? 1 : 2;
 }
 
+// One gradient pass for the 2x2 output tile (r0, r0+1) x (c0, c0+1) of family `fam`:
+//   fam 0: outputs (is, js), sums over ks: X = U_ik(is, ks), Y = U_jk(js, ks)
+//   fam 1: outputs (is, ks), sums over js: X = U_ij(is, js), Y = U_jk(js, ks)
+//   fam 2: outputs (js, ks), sums over is: X = U_ij(is, js), Y = U_ik(is, ks)
+// q0/q1 receive the two coefficient-contracted sums; P = q0 + d q1 and dP/dd = q1 for the
+// output pair's own distance d.
+template <typename T, int fam>
+__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__restrict__ C,
+                                         int r0, int c0, T q0[4], T q1[4]) {
+  using V2 = typename Vec2<T>::type;
+  const int tr = kPType[r0], tc = kPType[c0];
+#pragma unroll
+  for (int o = 0; o < 4; o++) q0[o] = q1[o] = (T)0;
+  constexpr int kStart[7] = {0, 2, 4, 6, 10, 14, 18};
+#pragma unroll
+  for (int tb = 0; tb < 6; tb++) {
+    T M[4][4];
+#pragma unroll
+    for (int o = 0; o < 4; o++)
+#pragma unroll
+      for (int u = 0; u < 4; u++) M[o][u] = (T)0;
+#pragma unroll
+    for (int c = kStart[tb]; c < kStart[tb + 1]; c++) {
+      V2 xa, xb, ya, yb;
+      if (fam == 0) {
+        xa = S.uu[1][r0][c];
+        xb = S.uu[1][r0 + 1][c];
+        ya = S.uu[2][c0][c];
+        yb = S.uu[2][c0 + 1][c];
+      } else if (fam == 1) {
+        xa = S.uu[0][r0][c];
+        xb = S.uu[0][r0 + 1][c];
+        ya = S.uu[2][c][c0];
+        yb = S.uu[2][c][c0 + 1];
+      } else {
+        xa = S.uu[0][c][r0];
+        xb = S.uu[0][c][r0 + 1];
+        ya = S.uu[1][c][c0];
+        yb = S.uu[1][c][c0 + 1];
+      }
+      const V2 X[2] = {xa, xb}, Y[2] = {ya, yb};
+#pragma unroll
+      for (int rr = 0; rr < 2; rr++)
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+          const int o = rr * 2 + cc;
+          M[o][0] += X[rr].x * Y[cc].x;
+          M[o][1] += X[rr].x * Y[cc].y;
+          M[o][2] += X[rr].y * Y[cc].x;
+          M[o][3] += X[rr].y * Y[cc].y;
+        }
+    }
+    // coefficient c[ip*4 + jp*2 + kp] of the type triple (ti, tj, tk)
+    int ti, tj, tk;
+    if (fam == 0) {
+      ti = tr; tj = tc; tk = tb;
+    } else if (fam == 1) {
+      ti = tr; tj = tb; tk = tc;
+    } else {
+      ti = tb; tj = tr; tk = tc;
+    }
+    const double *cp = C + ((ti * kNt + tj) * kNt + tk) * 8;
+    T c[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) c[u] = (T)cp[u];
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      // M[o][x*2 + y] = sum X_x Y_y with x, y the powers carried by X and Y:
+      //  fam 0: X -> jp (d_ik), Y -> ip (d_jk); outputs carry kp (d_ij)
+      //  fam 1: X -> kp (d_ij), Y -> ip (d_jk); outputs carry jp (d_ik)
+      //  fam 2: X -> kp (d_ij), Y -> jp (d_ik); outputs carry ip (d_jk)
+      if (fam == 0) {
+        q0[o] += c[0] * M[o][0] + c[4] * M[o][1] + c[2] * M[o][2] + c[6] * M[o][3];
+        q1[o] += c[1] * M[o][0] + c[5] * M[o][1] + c[3] * M[o][2] + c[7] * M[o][3];
+      } else if (fam == 1) {
+        q0[o] += c[0] * M[o][0] + c[4] * M[o][1] + c[1] * M[o][2] + c[5] * M[o][3];
+        q1[o] += c[2] * M[o][0] + c[6] * M[o][1] + c[3] * M[o][2] + c[7] * M[o][3];
+      } else {
+        q0[o] += c[0] * M[o][0] + c[2] * M[o][1] + c[1] * M[o][2] + c[3] * M[o][3];
+        q1[o] += c[4] * M[o][0] + c[6] * M[o][1] + c[5] * M[o][2] + c[7] * M[o][3];
+      }
+    }
+  }
+}
+
 template <typename T>
-__device__ double fs3_variant(Fs3Smem<T> &S, int v, const double cv[3][3], double wsite) {
+__device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
+  using V2 = typename Vec2<T>::type;
   const int tid = threadIdx.x;
-  // ---- pair phase: e, r and d ln e / dr of the 867 site pairs
-  for (int it = tid; it < kItems; it += kFs3Threads) {
+  // ---- pair phase: e, r and d ln e / dr of the 867 site pairs (padded layout)
+#pragma unroll
+  for (int rnd = 0; rnd < (kItems + kFs3Block - 1) / kFs3Block; rnd++) {
+    const int it = tid + rnd * kFs3Block;
+    if (it >= kItems) break;
     const int p = it / kPairs, ab = it % kPairs, a = ab / kNs3, b = ab % kNs3;
     int m1, m2;
     family(p, m1, m2);
-    const double vx = cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
-    const double vy = cv[p][1] + (S.site[m1][a][1] - S.site[m2][b][1]);
-    const double vz = cv[p][2] + (S.site[m1][a][2] - S.site[m2][b][2]);
+    const double vx = S.cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
+    const double vy = S.cv[p][1] + (S.site[m1][a][1] - S.site[m2][b][1]);
+    const double vz = S.cv[p][2] + (S.site[m1][a][2] - S.site[m2][b][2]);
     const T r2 = (T)(vx * vx + vy * vy + vz * vz);
     const T r = t_sqrt<T>(r2);
     const T bb = (T)S.bgr[v][0][ab], gg = (T)S.bgr[v][1][ab], r0 = (T)S.bgr[v][2][ab];
     const T ex = t_exp<T>(-gg * (r - r0));
     const T damp = t_rcp<T>((T)1 + ex);
-    S.e[it] = t_exp<T>(-bb * r) * damp;
-    S.d[it] = r;
-    S.dl[it] = -bb + gg * ex * damp;
+    const T e = t_exp<T>(-bb * r) * damp;
+    V2 u, w;
+    u.x = e;
+    u.y = e * r;
+    w.x = r;
+    w.y = -bb + gg * ex * damp;
+    S.uu[p][pidx(a)][pidx(b)] = u;
+    S.dl[p][pidx(a)][pidx(b)] = w;
   }
   __syncthreads();
-  // ---- triple phase: per site pair, sum over the third site
+  // ---- gradient passes: warps 0-2 family ij, 3-5 ik, 6-8 jk
+  const int fam = tid / kPassThreads, lt = tid % kPassThreads;
   double esum = 0.0;
-  const double *C = S.coef[v];
-  for (int it = tid; it < kItems; it += kFs3Threads) {
-    const int p = it / kPairs, ab = it % kPairs, a = ab / kNs3, b = ab % kNs3;
-    T acc = 0, accE = 0;
-    if (p == 0) {  // (is, js) fixed, loop ks;  P = q0 + q1 d_ij
-      const T dc = S.d[it];
-      const int tij = (S.type[a] * kNt + S.type[b]) * kNt;
-      const T dl = S.dl[it];
-      for (int ks = 0; ks < kNs3; ks++) {
-        const int ik = kPairs + a * kNs3 + ks, jk = 2 * kPairs + b * kNs3 + ks;
-        const T eb = S.e[ik], db = S.d[ik], ec = S.e[jk], da = S.d[jk];
-        const double *c = C + (tij + S.type[ks]) * 8;
-        const T q0 = (T)c[0] + (T)c[2] * db + da * ((T)c[4] + (T)c[6] * db);
-        const T q1 = (T)c[1] + (T)c[3] * db + da * ((T)c[5] + (T)c[7] * db);
-        const T P = q0 + q1 * dc;
-        const T w = eb * ec;
-        accE += w * P;
-        acc += w * (dl * P + q1);
-      }
-      esum += (double)S.e[it] * (double)accE;
-      S.G[it] += wsite * (double)(S.e[it] * acc / dc);
-    } else if (p == 1) {  // (is, ks) fixed, loop js;  P = r0 + r1 d_ik
-      const T db = S.d[it];
-      const T dl = S.dl[it];
-      for (int js = 0; js < kNs3; js++) {
-        const int ij = a * kNs3 + js, jk = 2 * kPairs + js * kNs3 + b;
-        const T ea = S.e[ij], dc = S.d[ij], ec = S.e[jk], da = S.d[jk];
-        const double *c = C + ((S.type[a] * kNt + S.type[js]) * kNt + S.type[b]) * 8;
-        const T r0 = (T)c[0] + (T)c[1] * dc + da * ((T)c[4] + (T)c[5] * dc);
-        const T r1 = (T)c[2] + (T)c[3] * dc + da * ((T)c[6] + (T)c[7] * dc);
-        const T P = r0 + r1 * db;
-        acc += ea * ec * (dl * P + r1);
-      }
-      S.G[it] += wsite * (double)(S.e[it] * acc / db);
-    } else {  // (js, ks) fixed, loop is;  P = u0 + u1 d_jk
-      const T da = S.d[it];
-      const T dl = S.dl[it];
-      for (int is = 0; is < kNs3; is++) {
-        const int ij = is * kNs3 + a, ik = kPairs + is * kNs3 + b;
-        const T ea = S.e[ij], dc = S.d[ij], eb = S.e[ik], db = S.d[ik];
-        const double *c = C + ((S.type[is] * kNt + S.type[a]) * kNt + S.type[b]) * 8;
-        const T u0 = (T)c[0] + (T)c[1] * dc + db * ((T)c[2] + (T)c[3] * dc);
-        const T u1 = (T)c[4] + (T)c[5] * dc + db * ((T)c[6] + (T)c[7] * dc);
-        const T P = u0 + u1 * da;
-        acc += ea * eb * (dl * P + u1);
-      }
-      S.G[it] += wsite * (double)(S.e[it] * acc / da);
+  if (lt < kTile * kTile) {
+    const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
+    T q0[4], q1[4];
+    if (fam == 0)
+      fs3_pass<T, 0>(S, S.coef[v], r0, c0, q0, q1);
+    else if (fam == 1)
+      fs3_pass<T, 1>(S, S.coef[v], r0, c0, q0, q1);
+    else
+      fs3_pass<T, 2>(S, S.coef[v], r0, c0, q0, q1);
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      const int r = r0 + (o >> 1), c = c0 + (o & 1);
+      const V2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
+      const T P = q0[o] + w.x * q1[o];
+      if (fam == 0) esum += (double)u.x * (double)P;
+      S.G[fam][r][c] += wsite * (double)(u.x * (w.y * P + q1[o]) / w.x);
     }
   }
-  // block sum of the energy polynomial
   esum = warp_sum(esum);
   if ((tid & 31) == 0) S.red[tid >> 5] = esum;
   __syncthreads();
   double tot = 0.0;
 #pragma unroll
-  for (int w = 0; w < kFs3Threads / 32; w++) tot += S.red[w];
+  for (int w = 0; w < kFs3Block / 32; w++) tot += S.red[w];
   __syncthreads();
   return tot;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kFs3Threads)
+__global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
     k_fs3(const int4 *__restrict__ tri, const int *__restrict__ icnt, int tri_cap,
           const double4 *__restrict__ comb, const double4 *__restrict__ s17, Fs3Params P,
           const double *__restrict__ coef, const double *__restrict__ bgr,
           const int *__restrict__ types, int nm, int ns, double *f, double *fc3, double *scal) {
-  extern __shared__ unsigned char smem_raw[];
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
   const int tid = threadIdx.x;
-  for (int t = tid; t < 2 * kCoef; t += kFs3Threads) (&S.coef[0][0])[t] = coef[t];
-  for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Threads) (&S.bgr[0][0][0])[t] = bgr[t];
-  if (tid < kNs3) S.type[tid] = types[tid];
+  (void)types;
+  for (int t = tid; t < 2 * kCoef; t += kFs3Block) (&S.coef[0][0])[t] = coef[t];
+  for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&S.bgr[0][0][0])[t] = bgr[t];
+  // padded dummy site: zero weight, unit distance (keeps e / d finite)
+  for (int t = tid; t < 3 * kP; t += kFs3Block) {
+    const int p = t / kP, q = t % kP;
+    V2 z, one;
+    z.x = z.y = (T)0;
+    one.x = (T)1;
+    one.y = (T)0;
+    S.uu[p][1][q] = z;
+    S.uu[p][q][1] = z;
+    S.dl[p][1][q] = one;
+    S.dl[p][q][1] = one;
+  }
   __syncthreads();
   const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
   const double conv = kH2kcal * 418.4 / kBohr2a;
   const size_t nfs = (size_t)nm * ns;
   double e_tot = 0.0, v_tot = 0.0;
   for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
-    const int4 T4 = tri[t];
-    const int mi[3] = {T4.x, T4.y, T4.z};
-    TripleGeom g;
-    triple_geom(comb[mi[0]], comb[mi[1]], comb[mi[2]], P.boxb, g);
-    const double rij = sqrt(g.dij2), rik = sqrt(g.dik2), rjk = sqrt(g.djk2);
-    const double ravg = (rij + rjk + rik) / 3.0;
-    const double pom = exp(P.alp3 * (ravg - P.r0dmp));
-    const double ppom = 1.0 / (1.0 + pom);
-    const double fdmp = pow(ppom, P.delta33);
-    const double dfdmp = -P.alp3 * P.delta33 * pom * ppom * fdmp * (1.0 / 3.0);
-    const double cv[3][3] = {{g.xij, g.yij, g.zij}, {g.xik, g.yik, g.zik}, {g.xjk, g.yjk, g.zjk}};
-    for (int u = tid; u < 3 * kNs3; u += kFs3Threads) {
+    if (tid == 0) {
+      const int4 T4 = tri[t];
+      S.mol[0] = T4.x;
+      S.mol[1] = T4.y;
+      S.mol[2] = T4.z;
+      TripleGeom g;
+      triple_geom(comb[T4.x], comb[T4.y], comb[T4.z], P.boxb, g);
+      const double rij = sqrt(g.dij2), rik = sqrt(g.dik2), rjk = sqrt(g.djk2);
+      const double ravg = (rij + rjk + rik) / 3.0;
+      const double pom = exp(P.alp3 * (ravg - P.r0dmp));
+      const double ppom = 1.0 / (1.0 + pom);
+      const double fdmp = pow(ppom, P.delta33);
+      S.cv[0][0] = g.xij; S.cv[0][1] = g.yij; S.cv[0][2] = g.zij;
+      S.cv[1][0] = g.xik; S.cv[1][1] = g.yik; S.cv[1][2] = g.zik;
+      S.cv[2][0] = g.xjk; S.cv[2][1] = g.yjk; S.cv[2][2] = g.zjk;
+      S.rr[0] = rij; S.rr[1] = rik; S.rr[2] = rjk;
+      S.sc[0] = fdmp;
+      S.sc[1] = -P.alp3 * P.delta33 * pom * ppom * fdmp * (1.0 / 3.0);
+      S.branch = ravg <= P.rmin ? 0 : (ravg >= P.rmax ? 1 : 2);
+      const double cfact = (ravg - P.rmin) / (P.rmax - P.rmin);
+      S.sc[2] = 1.0 + 2.0 * cfact * cfact * cfact - 3.0 * cfact * cfact;
+      S.sc[3] = 2.0 / (P.rmax - P.rmin) * (cfact * cfact - cfact);
+    }
+    __syncthreads();
+    for (int u = tid; u < 3 * kNs3; u += kFs3Block) {
       const int m = u / kNs3, s = u % kNs3;
-      const double4 o = s17[(size_t)mi[m] * kNs3 + s];
+      const double4 o = s17[(size_t)S.mol[m] * kNs3 + s];
       S.site[m][s][0] = o.x;
       S.site[m][s][1] = o.y;
       S.site[m][s][2] = o.z;
     }
-    for (int u = tid; u < kItems; u += kFs3Threads) S.G[u] = 0.0;
+    for (int u = tid; u < 3 * kP * kRS; u += kFs3Block) (&S.G[0][0][0])[u] = 0.0;
     __syncthreads();
-    double energy, comc;
-    if (ravg <= P.rmin) {
-      const double Ssr = fs3_variant<T>(S, 0, cv, fdmp);
-      energy = fdmp * Ssr;
-      comc = dfdmp * Ssr;
-    } else if (ravg >= P.rmax) {
-      const double Slr = fs3_variant<T>(S, 1, cv, fdmp);
-      energy = fdmp * Slr;
-      comc = dfdmp * Slr;
-    } else {
-      const double cfact = (ravg - P.rmin) / (P.rmax - P.rmin);
-      const double smfun = 1.0 + 2.0 * cfact * cfact * cfact - 3.0 * cfact * cfact;
-      const double smfun2 = 1.0 - smfun;
-      const double cf = 2.0 / (P.rmax - P.rmin) * (cfact * cfact - cfact);
-      const double Ssr = fs3_variant<T>(S, 0, cv, fdmp * smfun);
-      const double Slr = fs3_variant<T>(S, 1, cv, fdmp * smfun2);
-      energy = fdmp * (smfun * Ssr + smfun2 * Slr);
-      comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
+    {
+      const double fdmp = S.sc[0], dfdmp = S.sc[1];
+      const int br = S.branch;
+      double energy, comc;
+      if (br != 2) {
+        const double Sv = fs3_variant<T>(S, br, fdmp);
+        energy = fdmp * Sv;
+        comc = dfdmp * Sv;
+      } else {
+        const double smfun = S.sc[2], smfun2 = 1.0 - smfun, cf = S.sc[3];
+        const double Ssr = fs3_variant<T>(S, 0, fdmp * smfun);
+        const double Slr = fs3_variant<T>(S, 1, fdmp * smfun2);
+        energy = fdmp * (smfun * Ssr + smfun2 * Slr);
+        comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
+      }
+      if (tid == 0) {
+        S.sc[4] = energy;
+        S.sc[5] = comc;
+      }
     }
-    __syncthreads();
-    // ---- site forces: F = -sum_partner G * (pair vector), 51 (molecule, site) items
+    // ---- site forces: F = -sum_partner G * (pair vector); 4 lanes per (molecule, site),
+    // each summing a quarter of the 17 partners, reduced with shuffles.
     double vsite = 0.0;
-    for (int u = tid; u < 3 * kNs3; u += kFs3Threads) {
-      const int m = u / kNs3, s = u % kNs3;
+    {
+      const int item = tid >> 2, part = tid & 3;
+      const bool act = item < 3 * kNs3;
+      const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = pidx(s);
       double fx = 0.0, fy = 0.0, fz = 0.0;
-      for (int o = 0; o < kNs3; o++) {
-        // (family, first-site, second-site, sign) of the two pair families touching m
-        if (m == 0) {
-          // i-site s: + G_ij(s,o) v_ij(s,o) + G_ik(s,o) v_ik(s,o)
-          const double g0 = S.G[s * kNs3 + o], g1 = S.G[kPairs + s * kNs3 + o];
-          const double a0 = cv[0][0] + (S.site[0][s][0] - S.site[1][o][0]);
-          const double a1 = cv[0][1] + (S.site[0][s][1] - S.site[1][o][1]);
-          const double a2 = cv[0][2] + (S.site[0][s][2] - S.site[1][o][2]);
-          const double b0 = cv[1][0] + (S.site[0][s][0] - S.site[2][o][0]);
-          const double b1 = cv[1][1] + (S.site[0][s][1] - S.site[2][o][1]);
-          const double b2 = cv[1][2] + (S.site[0][s][2] - S.site[2][o][2]);
-          fx -= g0 * a0 + g1 * b0;
-          fy -= g0 * a1 + g1 * b1;
-          fz -= g0 * a2 + g1 * b2;
-          vsite += g0 * (a0 * a0 + a1 * a1 + a2 * a2) + g1 * (b0 * b0 + b1 * b1 + b2 * b2);
-        } else if (m == 1) {
-          // j-site s: - G_ij(o,s) v_ij(o,s) + G_jk(s,o) v_jk(s,o)
-          const double g0 = S.G[o * kNs3 + s], g2 = S.G[2 * kPairs + s * kNs3 + o];
-          const double a0 = cv[0][0] + (S.site[0][o][0] - S.site[1][s][0]);
-          const double a1 = cv[0][1] + (S.site[0][o][1] - S.site[1][s][1]);
-          const double a2 = cv[0][2] + (S.site[0][o][2] - S.site[1][s][2]);
-          const double c0 = cv[2][0] + (S.site[1][s][0] - S.site[2][o][0]);
-          const double c1 = cv[2][1] + (S.site[1][s][1] - S.site[2][o][1]);
-          const double c2 = cv[2][2] + (S.site[1][s][2] - S.site[2][o][2]);
-          fx -= -g0 * a0 + g2 * c0;
-          fy -= -g0 * a1 + g2 * c1;
-          fz -= -g0 * a2 + g2 * c2;
-          vsite += g2 * (c0 * c0 + c1 * c1 + c2 * c2);
-        } else {
-          // k-site s: - G_ik(o,s) v_ik(o,s) - G_jk(o,s) v_jk(o,s)
-          const double g1 = S.G[kPairs + o * kNs3 + s], g2 = S.G[2 * kPairs + o * kNs3 + s];
-          const double b0 = cv[1][0] + (S.site[0][o][0] - S.site[2][s][0]);
-          const double b1 = cv[1][1] + (S.site[0][o][1] - S.site[2][s][1]);
-          const double b2 = cv[1][2] + (S.site[0][o][2] - S.site[2][s][2]);
-          const double c0 = cv[2][0] + (S.site[1][o][0] - S.site[2][s][0]);
-          const double c1 = cv[2][1] + (S.site[1][o][1] - S.site[2][s][1]);
-          const double c2 = cv[2][2] + (S.site[1][o][2] - S.site[2][s][2]);
-          fx -= -g1 * b0 - g2 * c0;
-          fy -= -g1 * b1 - g2 * c1;
-          fz -= -g1 * b2 - g2 * c2;
+      if (act) {
+        for (int o = part; o < kNs3; o += 4) {
+          const int po = pidx(o);
+          if (m == 0) {
+            const double g0 = S.G[0][ps][po], g1 = S.G[1][ps][po];
+            const double a0 = S.cv[0][0] + (S.site[0][s][0] - S.site[1][o][0]);
+            const double a1 = S.cv[0][1] + (S.site[0][s][1] - S.site[1][o][1]);
+            const double a2 = S.cv[0][2] + (S.site[0][s][2] - S.site[1][o][2]);
+            const double b0 = S.cv[1][0] + (S.site[0][s][0] - S.site[2][o][0]);
+            const double b1 = S.cv[1][1] + (S.site[0][s][1] - S.site[2][o][1]);
+            const double b2 = S.cv[1][2] + (S.site[0][s][2] - S.site[2][o][2]);
+            fx -= g0 * a0 + g1 * b0;
+            fy -= g0 * a1 + g1 * b1;
+            fz -= g0 * a2 + g1 * b2;
+            vsite += g0 * (a0 * a0 + a1 * a1 + a2 * a2) + g1 * (b0 * b0 + b1 * b1 + b2 * b2);
+          } else if (m == 1) {
+            const double g0 = S.G[0][po][ps], g2 = S.G[2][ps][po];
+            const double a0 = S.cv[0][0] + (S.site[0][o][0] - S.site[1][s][0]);
+            const double a1 = S.cv[0][1] + (S.site[0][o][1] - S.site[1][s][1]);
+            const double a2 = S.cv[0][2] + (S.site[0][o][2] - S.site[1][s][2]);
+            const double c0 = S.cv[2][0] + (S.site[1][s][0] - S.site[2][o][0]);
+            const double c1 = S.cv[2][1] + (S.site[1][s][1] - S.site[2][o][1]);
+            const double c2 = S.cv[2][2] + (S.site[1][s][2] - S.site[2][o][2]);
+            fx -= -g0 * a0 + g2 * c0;
+            fy -= -g0 * a1 + g2 * c1;
+            fz -= -g0 * a2 + g2 * c2;
+            vsite += g2 * (c0 * c0 + c1 * c1 + c2 * c2);
+          } else {
+            const double g1 = S.G[1][po][ps], g2 = S.G[2][po][ps];
+            const double b0 = S.cv[1][0] + (S.site[0][o][0] - S.site[2][s][0]);
+            const double b1 = S.cv[1][1] + (S.site[0][o][1] - S.site[2][s][1]);
+            const double b2 = S.cv[1][2] + (S.site[0][o][2] - S.site[2][s][2]);
+            const double c0 = S.cv[2][0] + (S.site[1][o][0] - S.site[2][s][0]);
+            const double c1 = S.cv[2][1] + (S.site[1][o][1] - S.site[2][s][1]);
+            const double c2 = S.cv[2][2] + (S.site[1][o][2] - S.site[2][s][2]);
+            fx -= -g1 * b0 - g2 * c0;
+            fy -= -g1 * b1 - g2 * c1;
+            fz -= -g1 * b2 - g2 * c2;
+          }
         }
       }
-      const size_t o = (size_t)mi[m] * ns + s;
-      atomicAdd(&f[o], fx * conv);
-      atomicAdd(&f[nfs + o], fy * conv);
-      atomicAdd(&f[2 * nfs + o], fz * conv);
+#pragma unroll
+      for (int off = 1; off < 4; off <<= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, off);
+        fy += __shfl_xor_sync(0xffffffffu, fy, off);
+        fz += __shfl_xor_sync(0xffffffffu, fz, off);
+      }
+      if (act && part == 0) {
+        const size_t o = (size_t)S.mol[m] * ns + s;
+        atomicAdd(&f[o], fx * conv);
+        atomicAdd(&f[nfs + o], fy * conv);
+        atomicAdd(&f[2 * nfs + o], fz * conv);
+      }
     }
     if (tid == 0) {
       // COM forces from the R_avg damping and switch (threebody_potential.f90:1092-1120)
-      const double ux = g.xij / rij, uy = g.yij / rij, uz = g.zij / rij;
-      const double wx = g.xik / rik, wy = g.yik / rik, wz = g.zik / rik;
-      const double sx = g.xjk / rjk, sy = g.yjk / rjk, sz = g.zjk / rjk;
-      atomicAdd(&fc3[mi[0]], -comc * (ux + wx) * conv);
-      atomicAdd(&fc3[nm + mi[0]], -comc * (uy + wy) * conv);
-      atomicAdd(&fc3[2 * nm + mi[0]], -comc * (uz + wz) * conv);
-      atomicAdd(&fc3[mi[1]], -comc * (-ux + sx) * conv);
-      atomicAdd(&fc3[nm + mi[1]], -comc * (-uy + sy) * conv);
-      atomicAdd(&fc3[2 * nm + mi[1]], -comc * (-uz + sz) * conv);
-      atomicAdd(&fc3[mi[2]], -comc * (-wx - sx) * conv);
-      atomicAdd(&fc3[nm + mi[2]], -comc * (-wy - sy) * conv);
-      atomicAdd(&fc3[2 * nm + mi[2]], -comc * (-wz - sz) * conv);
-      e_tot += energy;
+      const double comc = S.sc[5];
+      const double rij = S.rr[0], rik = S.rr[1], rjk = S.rr[2];
+      const double ux = S.cv[0][0] / rij, uy = S.cv[0][1] / rij, uz = S.cv[0][2] / rij;
+      const double wx = S.cv[1][0] / rik, wy = S.cv[1][1] / rik, wz = S.cv[1][2] / rik;
+      const double sx = S.cv[2][0] / rjk, sy = S.cv[2][1] / rjk, sz = S.cv[2][2] / rjk;
+      const int m0 = S.mol[0], m1 = S.mol[1], m2 = S.mol[2];
+      atomicAdd(&fc3[m0], -comc * (ux + wx) * conv);
+      atomicAdd(&fc3[nm + m0], -comc * (uy + wy) * conv);
+      atomicAdd(&fc3[2 * nm + m0], -comc * (uz + wz) * conv);
+      atomicAdd(&fc3[m1], -comc * (-ux + sx) * conv);
+      atomicAdd(&fc3[nm + m1], -comc * (-uy + sy) * conv);
+      atomicAdd(&fc3[2 * nm + m1], -comc * (-uz + sz) * conv);
+      atomicAdd(&fc3[m2], -comc * (-wx - sx) * conv);
+      atomicAdd(&fc3[nm + m2], -comc * (-wy - sy) * conv);
+      atomicAdd(&fc3[2 * nm + m2], -comc * (-wz - sz) * conv);
+      e_tot += S.sc[4];
       v_tot += comc * (rij + rik + rjk);
     }
     v_tot += vsite;
@@ -626,18 +764,18 @@ cudaError_t launch_fs3(int precision, const int4 *tri, const int *icnt, int tri_
     e = cudaFuncSetAttribute(k_fs3<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<double>, kFs3Threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<double>, kFs3Block, smem);
     if (per_sm < 1) per_sm = 1;
-    k_fs3<double><<<nsm * per_sm, kFs3Threads, smem, st>>>(tri, icnt, tri_cap, comb, s17, P, coef,
+    k_fs3<double><<<nsm * per_sm, kFs3Block, smem, st>>>(tri, icnt, tri_cap, comb, s17, P, coef,
                                                            bgr, types, nm, ns, f, fc3, scal);
   } else {
     const size_t smem = sizeof(Fs3Smem<float>);
     e = cudaFuncSetAttribute(k_fs3<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<float>, kFs3Threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<float>, kFs3Block, smem);
     if (per_sm < 1) per_sm = 1;
-    k_fs3<float><<<nsm * per_sm, kFs3Threads, smem, st>>>(tri, icnt, tri_cap, comb, s17, P, coef,
+    k_fs3<float><<<nsm * per_sm, kFs3Block, smem, st>>>(tri, icnt, tri_cap, comb, s17, P, coef,
                                                           bgr, types, nm, ns, f, fc3, scal);
   }
   return cudaGetLastError();
