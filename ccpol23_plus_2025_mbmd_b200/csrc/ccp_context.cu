@@ -335,10 +335,10 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
                      st));
     if (mask & T_KSPACE) {
       LK(launch_kspace_sums(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+                            c->d_mu, c->d_sk, st));
+      LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, st));
       LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, nullptr, nullptr,
-                              nullptr, c->d_scal, st));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, st));
     }
     mark(3);
     if (mask & T_INDUCTION) {
@@ -346,10 +346,9 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
         LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_eir, c->d_e0slf,
                               c->d_scal, st));
       LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+                            c->d_mu, c->d_sk, st));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, nullptr, nullptr,
-                              nullptr, c->d_scal, st));
+                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, st));
       if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, st));
       LK(launch_dip_tensor(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt,
                            c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, st));
@@ -363,10 +362,11 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
         LK(launch_dip_matvec(c->d_nbr, c->d_ncnt, c->cap, nm, S.np, c->d_T4, c->d_TB, c->d_S4,
                              c->d_SB, c->d_mu, c->d_eim, st));
         LK(launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+                              c->kmax[2], c->d_mu, c->d_sk, st));
         LK(launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                                c->kmax[2], c->d_mu, c->d_sk, nullptr, nullptr, c->d_e0tot,
-                                c->d_eim, c->d_mu2, c->d_scal, st));
+                                c->kmax[2], c->d_mu, c->d_sk, c->d_eik, nullptr, st));
+        LK(launch_dip_update(nm, S, c->d_e0tot, c->d_eim, c->d_eik, c->d_mu, c->d_mu2, c->d_scal,
+                             st));
         std::swap(c->d_mu, c->d_mu2);
         CK(cudaMemcpyAsync(c->h_scal + S_IND_CHANGE, c->d_scal + S_IND_CHANGE, 2 * sizeof(double),
                            cudaMemcpyDeviceToHost, st));
@@ -384,10 +384,10 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       LK(launch_pair_indforce(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
                               c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_f, c->d_scal, st));
       LK(launch_kspace_sums(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, c->d_scal, c->alpha, st));
+                            c->d_mu, c->d_sk, st));
+      LK(launch_kspace_energy(3, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, st));
       LK(launch_kspace_gather(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, nullptr, nullptr,
-                              nullptr, c->d_scal, st));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, st));
     }
     mark(4);
     if (mask & T_FS2) {

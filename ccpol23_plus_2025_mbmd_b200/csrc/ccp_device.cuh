@@ -168,16 +168,22 @@ cudaError_t launch_ktab(const double4 *com, const double4 *act, int nm, SiteSets
 //       1 static field at polarisable sites from charges
 //       2 dipole field at polarisable sites
 //       3 induction forces at active sites
+// sums: structure factors into sk (4 doubles per k, zeroed by the launcher);
+// energy: per-k energy/virial of modes 0 and 3 into scal;
+// gather: MODES 1, 2 write the field into out (zeroed by the launcher), 0 and 3 add forces
+// into f.
 cudaError_t launch_kspace_sums(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
                                SiteSets S, int kl, int km, int kn, const double *mu,
-                               double *sk, double *scal, double alpha, cudaStream_t st);
-// MODE 2 also applies the Jacobi update: e0 = total static field, eim = real-space part of
-// the dipole field (real + short-range + self), mu read, mu_out written, change/energy into
-// scal.  out receives the field for MODE 1; f the forces for MODES 0 and 3.
+                               double *sk, cudaStream_t st);
+cudaError_t launch_kspace_energy(int mode, const KVec *kv, int nk, const double *sk,
+                                 double alpha, double *scal, cudaStream_t st);
 cudaError_t launch_kspace_gather(int mode, const KVec *kv, int nk, const double2 *tab, int nm,
                                  SiteSets S, int kl, int km, int kn, const double *mu,
-                                 const double *sk, double *out, double *f, const double *e0,
-                                 const double *eim, double *mu_out, double *scal, cudaStream_t st);
+                                 const double *sk, double *out, double *f, cudaStream_t st);
+// Jacobi update: mu_out = alpha (e0 + eim + ek), change and energy into scal.
+cudaError_t launch_dip_update(int nm, SiteSets S, const double *e0, const double *eim,
+                              const double *ek, const double *mu, double *mu_out, double *scal,
+                              cudaStream_t st);
 
 // three-body
 cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
