@@ -82,7 +82,7 @@ struct ccp_context {
   int cap = 0, tri_cap = 0, pair_cap = 0;
   int *d_nbr = nullptr, *d_ncnt = nullptr;
   double4 *d_nbrv = nullptr;
-  int4 *d_tri = nullptr;
+  void *d_tri = nullptr;  // FS3 triple records
   int2 *d_pairs = nullptr;
   // reciprocal space
   KVec *d_kv = nullptr;
@@ -102,6 +102,13 @@ struct ccp_context {
   size_t h_io_cap = 0;
   // constants for the Ewald self energy
   double sumq = 0, sumq2 = 0;
+  // graph-resident Jacobi loop
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t ind_graph = nullptr;
+  cudaGraphExec_t ind_exec = nullptr;
+  double *d_istate = nullptr;  // {iterations, last change, last energy}
+  double *h_istate = nullptr;
+  std::vector<long long> ind_key;
   // phase timing (diagnostics)
   bool timing = false;
   cudaEvent_t ev[CCP_NPHASE + 1] = {};
@@ -125,6 +132,11 @@ void free_ctx(ccp_context *c) {
   if (c->h_io) cudaFreeHost(c->h_io);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
+  if (c->ind_exec) cudaGraphExecDestroy(c->ind_exec);
+  if (c->ind_graph) cudaGraphDestroy(c->ind_graph);
+  if (c->d_istate) cudaFree(c->d_istate);
+  if (c->h_istate) cudaFreeHost(c->h_istate);
+  if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   if (c->own) cudaStreamDestroy(c->own);
 }
 
@@ -154,7 +166,7 @@ int ensure_lists(ccp_context *c, int cap, int tri_cap, int pair_cap) {
   }
   if (tri_cap > c->tri_cap) {
     if (c->d_tri) cudaFree(c->d_tri);
-    CK(dalloc(&c->d_tri, (size_t)tri_cap));
+    CK(cudaMalloc(&c->d_tri, fs3_record_bytes() * (size_t)std::max(tri_cap, 1)));
     c->tri_cap = tri_cap;
   }
   if (pair_cap > c->pair_cap) {
@@ -246,6 +258,56 @@ struct EvalOut {
   int iters = 0, ntri = 0, nblend = 0, nfs2 = 0;
   bool converged = true;
 };
+
+// Builds (once per set of buffers and sizes) the CUDA graph of the Jacobi iteration: a
+// WHILE conditional node whose body is T.mu matvec -> dipole structure factors -> reciprocal
+// field -> in-place update -> convergence node.  The host launches it once per evaluation
+// and never synchronises inside the loop.
+int ensure_ind_graph(ccp_context *c) {
+  const SiteSets &S = c->S;
+  std::vector<long long> key = {
+      (long long)c->d_nbr, (long long)c->d_ncnt, (long long)c->d_T4,  (long long)c->d_TB,
+      (long long)c->d_S4,  (long long)c->d_SB,   (long long)c->d_mu,  (long long)c->d_eim,
+      (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_sk,  (long long)c->d_eik,
+      (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, c->cap, c->nm, c->nk,
+      c->kmax[0], c->kmax[1], c->kmax[2], c->maxit};
+  if (c->ind_exec && key == c->ind_key) return CCP_OK;
+  if (c->ind_exec) cudaGraphExecDestroy(c->ind_exec);
+  if (c->ind_graph) cudaGraphDestroy(c->ind_graph);
+  c->ind_exec = nullptr;
+  c->ind_graph = nullptr;
+  CK(cudaGraphCreate(&c->ind_graph, 0));
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, c->ind_graph, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, c->ind_graph, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  cudaStream_t cs = c->cap_stream;
+  CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+  cudaError_t e = launch_dip_matvec(c->d_nbr, c->d_ncnt, c->cap, c->nm, S.np, c->d_T4, c->d_TB,
+                                    c->d_S4, c->d_SB, c->d_mu, c->d_eim, cs);
+  if (e == cudaSuccess)
+    e = launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
+                           c->kmax[2], c->d_mu, c->d_sk, cs);
+  if (e == cudaSuccess)
+    e = launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
+                             c->kmax[2], c->d_mu, c->d_sk, c->d_eik, nullptr, cs);
+  if (e == cudaSuccess)
+    e = launch_dip_update(c->nm, S, c->d_e0tot, c->d_eim, c->d_eik, c->d_mu, c->d_mu, c->d_scal, cs);
+  if (e == cudaSuccess) e = launch_dip_cond(h, c->d_scal, c->d_istate, 1.0e-20, c->maxit, cs);
+  cudaGraph_t captured = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
+  if (!cuda_ok(e, "capture of the dipole loop")) return CCP_ERR_CUDA;
+  CK(e2);
+  CK(cudaGraphInstantiate(&c->ind_exec, c->ind_graph, 0));
+  c->ind_key = key;
+  return CCP_OK;
+}
 
 #define LK(call)                                        \
   do {                                                  \
@@ -355,26 +417,18 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
                              st));
       CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * nm * S.np * 3, st));
-      int it = 0;
-      double change = 10.0;
-      while (change > 1.0e-20 && it < c->maxit) {
-        CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
-        LK(launch_dip_matvec(c->d_nbr, c->d_ncnt, c->cap, nm, S.np, c->d_T4, c->d_TB, c->d_S4,
-                             c->d_SB, c->d_mu, c->d_eim, st));
-        LK(launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, st));
-        LK(launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                                c->kmax[2], c->d_mu, c->d_sk, c->d_eik, nullptr, st));
-        LK(launch_dip_update(nm, S, c->d_e0tot, c->d_eim, c->d_eik, c->d_mu, c->d_mu2, c->d_scal,
-                             st));
-        std::swap(c->d_mu, c->d_mu2);
-        CK(cudaMemcpyAsync(c->h_scal + S_IND_CHANGE, c->d_scal + S_IND_CHANGE, 2 * sizeof(double),
-                           cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        change = c->h_scal[S_IND_CHANGE];
-        o.ind_e = c->h_scal[S_IND_ENERGY];
-        it++;
+      CK(cudaMemsetAsync(c->d_istate, 0, 3 * sizeof(double), st));
+      CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
+      {
+        int r = ensure_ind_graph(c);
+        if (r) return r;
       }
+      CK(cudaGraphLaunch(c->ind_exec, st));
+      CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      const int it = (int)c->h_istate[0];
+      c->launches += 5 * it;
+      o.ind_e = c->h_istate[2];
       o.iters = it;
       o.converged = it < c->maxit;
       if (!o.converged) {
@@ -402,9 +456,8 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
                          c->d_icnt, st));
     mark(6);
     if (mask & T_FS3) {
-      LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_comb, c->d_s17, F3,
-                    c->d_coef, c->d_bgr, c->d_types, nm, ns, c->d_f, c->d_fc3, c->d_scal, c->nsm,
-                    st));
+      LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
+                    nm, ns, c->d_f, c->d_fc3, c->d_scal, c->nsm, st));
     }
     mark(7);
     CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
@@ -700,7 +753,12 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
     return CCP_ERR_CUDA;
   };
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) return fail("stream");
+  if (cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail("stream");
   c->stream = c->own;
+  if (cudaMalloc(&c->d_istate, 3 * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void **)&c->h_istate, 3 * sizeof(double)) != cudaSuccess)
+    return fail("loop state");
   const size_t n = nm, nsi = (size_t)nm * m->ns, np3 = (size_t)nm * std::max(S.np, 1) * 3;
   bool ok = dalloc(&c->d_x, n) == cudaSuccess && dalloc(&c->d_y, n) == cudaSuccess &&
             dalloc(&c->d_z, n) == cudaSuccess && dalloc(&c->d_com, n) == cudaSuccess &&

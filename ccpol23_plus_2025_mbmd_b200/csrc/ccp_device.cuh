@@ -149,6 +149,9 @@ cudaError_t launch_dip_matvec(const int *nbr, const int *ncnt, int cap, int nm, 
                               const double *SB, const double *mu, double *eim, cudaStream_t st);
 cudaError_t launch_static_total(int n, const double *a, const double *b, const double *c,
                                 const double *d, double *out, cudaStream_t st);
+// Convergence node of the graph-resident Jacobi loop; state = {iterations, change, energy}.
+cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, double *scal, double *state, double thr,
+                            int maxit, cudaStream_t st);
 cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,
                                  const double *xs, const double *ys, const double *zs,
                                  int ld, const double4 *act, const int *nbr,
@@ -185,13 +188,13 @@ cudaError_t launch_dip_update(int nm, SiteSets S, const double *e0, const double
                               const double *ek, const double *mu, double *mu_out, double *scal,
                               cudaStream_t st);
 
-// three-body
+// three-body.  FS3 triples are kept as records of fs3_record_bytes() bytes each.
+size_t fs3_record_bytes();
 cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
-                            int nm, Fs3Params P, int4 *tri, int tri_cap, int *icnt,
+                            int nm, Fs3Params P, void *rec, int tri_cap, int *icnt,
                             cudaStream_t st);
-cudaError_t launch_fs3(int precision, const int4 *tri, const int *icnt, int tri_cap,
-                       const double4 *comb, const double4 *s17, Fs3Params P,
-                       const double *coef, const double *bgr, const int *types, int nm, int ns,
+cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
+                       const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
                        double *f, double *fc3, double *scal, int nsm, cudaStream_t st);
 cudaError_t launch_fs2_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
                             int nm, Fs2Params P, int2 *pairs, int pair_cap, int *icnt,

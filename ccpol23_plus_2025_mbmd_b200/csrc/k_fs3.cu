@@ -1,0 +1,533 @@
+// k_fs3.cu -- FS3 nonadditive three-body kernels (sm_100a).
+//
+// FS3 (threebody_potential.f90:676-2062).  For a molecular triple (i,j,k) with all three COM
+// distances below 6.3 A the reference sums, over 17^3 site triples and 2^3 powers,
+//     c(types, ip,jp,kp) * e_ij e_ik e_jk * d_jk^ip d_ik^jp d_ij^kp,
+// e_ab = exp(-b r)/(1 + exp(-g (r - r0))) of the site pair, times the R_avg damping f_dmp
+// and, between 4.5 and 5.5 A, the SR/LR switch.  Every exponential belongs to a site PAIR,
+// so a block first tabulates (e, e d) and (d, d ln e/dr) for the 3 x 289 site pairs of the
+// triple; the energy and the gradient with respect to every site-pair distance,
+//     G_ab = sum_third e_ij e_ik e_jk (dln e_ab/dr P + dP/dr_ab) / r_ab,
+// then come from three passes (one per pair family) of small matrix products: with sites
+// padded from 17 to 18 (a zero-weight dummy after site 0) the six site-type blocks
+//     [0,dummy] [1,2] [3,4] [5..8] [9..12] [13..16]
+// start at even indices, and per type block of the summed site each pass accumulates
+//     M_xy(a, b) = sum_c U_x(a, c) V_y(b, c),  U_0 = e, U_1 = e d,
+// for a 2x2 tile of outputs in registers, then contracts M with that type triple's 8
+// coefficients.  Site forces are sums of G_ab times the pair vectors: the reference's
+// per-term force sum regrouped.
+#include "ccp_device.cuh"
+
+// FS3 blocks resident per SM that the register allocation targets.
+#ifndef CCP_FS3_MINBLOCKS
+#define CCP_FS3_MINBLOCKS 2
+#endif
+
+using namespace ccpd;
+
+namespace {
+
+constexpr int kPairs = 289;
+constexpr int kNt = 6;                     // FS3 site types
+constexpr int kCoef = kNt * kNt * kNt * 8;
+constexpr int kP = 18;                     // padded sites
+constexpr int kRS = 19;                    // row stride of the site-pair tables
+constexpr int kTile = 9;                   // 2x2 tiles per dimension
+constexpr int kPassThreads = 96;           // 81 tiles per pair family, warp aligned
+constexpr int kFs3Block = 320;             // 3 x 96 pass threads + one warp; 289 pair threads
+constexpr int kRecWords = 18;              // doubles per triple record
+
+__device__ __forceinline__ int pidx(int s) { return s == 0 ? 0 : s + 1; }
+__constant__ int kPType[kP] = {0, 0, 1, 1, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5};
+
+// Per-triple record written by the enumeration: COM vectors ij, ik, jk (bohr, computed as
+// the reference computes them), their lengths, f_dmp, d f_dmp / d r (with the 1/3 of
+// R_avg), the switch value and its derivative, the molecules and the R_avg branch.
+struct Fs3Rec {
+  double cv[3][3];
+  double rr[3];
+  double fdmp, dfdmp, smfun, cf;
+  int mol[3];
+  int branch;  // 0 SR, 1 LR, 2 blend
+};
+static_assert(sizeof(Fs3Rec) == kRecWords * 8, "record layout");
+
+// ------------------------------------------------------------------ FS3 triples
+// One block per molecule i: the candidates j > i from i's neighbour list that pass the
+// reference's exact bohr cut-off test are staged in shared memory, then every pair
+// (j < k) of them is tested with the reference's consistent-image j-k vector
+// (threebody_potential.f90:860-892).  Accepted triples get a full record.
+__global__ void k_fs3_enum(const double4 *__restrict__ comb, const int *__restrict__ nbr,
+                           const int *__restrict__ ncnt, int cap, int nm, Fs3Params P,
+                           Fs3Rec *rec, int tri_cap, int *icnt) {
+  extern __shared__ unsigned char smem_raw[];
+  int *lj = reinterpret_cast<int *>(smem_raw);
+  double *lx = reinterpret_cast<double *>(lj + ((cap + 1) & ~1));
+  double *ly = lx + cap, *lz = ly + cap;
+  __shared__ int nl;
+  __shared__ int wcount[32];
+  const int i = blockIdx.x;
+  if (threadIdx.x == 0) nl = 0;
+  __syncthreads();
+  const double4 ci = comb[i];
+  const int cnt = ncnt[i];
+  // the neighbour list is in increasing j; keep the order with a ballot scan per warp
+  for (int n0 = 0; n0 < cnt; n0 += blockDim.x) {
+    const int n = n0 + threadIdx.x;
+    bool keep = false;
+    int j = 0;
+    double xij = 0, yij = 0, zij = 0;
+    if (n < cnt) {
+      j = nbr[(size_t)i * cap + n];
+      if (j > i) {
+        const double4 cj = comb[j];
+        xij = minimg(xsub(ci.x, cj.x), P.boxb);
+        yij = minimg(xsub(ci.y, cj.y), P.boxb);
+        zij = minimg(xsub(ci.z, cj.z), P.boxb);
+        keep = norm2x(xij, yij, zij) < P.rc2;
+      }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (lane == 0) wcount[wid] = __popc(bal);
+    __syncthreads();
+    int off = nl;
+    for (int w = 0; w < wid; w++) off += wcount[w];
+    if (keep) {
+      const int pos = off + __popc(bal & ((1u << lane) - 1u));
+      lj[pos] = j;
+      lx[pos] = xij;
+      ly[pos] = yij;
+      lz[pos] = zij;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) nl += wcount[w];
+    __syncthreads();
+  }
+  const int L = nl;
+  const double b = P.boxb;
+  for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
+    const int a = t / L, c = t % L;
+    if (c <= a) continue;
+    const int j = lj[a], k = lj[c];
+    const double4 cj = comb[j], ck = comb[k];
+    const double dxik = xsub(ci.x, ck.x), dyik = xsub(ci.y, ck.y), dzik = xsub(ci.z, ck.z);
+    const double xik = minimg(dxik, b), yik = minimg(dyik, b), zik = minimg(dzik, b);
+    const double dik2 = norm2x(xik, yik, zik);
+    if (!(dik2 < P.rc2)) continue;
+    // xjk = dxjk + box*nint(dxij/box) - box*nint(dxik/box)  (threebody_potential.f90:883-885)
+    const double dxij = xsub(ci.x, cj.x), dyij = xsub(ci.y, cj.y), dzij = xsub(ci.z, cj.z);
+    const double xjk = xsub(xadd(xsub(cj.x, ck.x), xmul(b, round(__ddiv_rn(dxij, b)))),
+                            xmul(b, round(__ddiv_rn(dxik, b))));
+    const double yjk = xsub(xadd(xsub(cj.y, ck.y), xmul(b, round(__ddiv_rn(dyij, b)))),
+                            xmul(b, round(__ddiv_rn(dyik, b))));
+    const double zjk = xsub(xadd(xsub(cj.z, ck.z), xmul(b, round(__ddiv_rn(dzij, b)))),
+                            xmul(b, round(__ddiv_rn(dzik, b))));
+    const double djk2 = norm2x(xjk, yjk, zjk);
+    if (!(djk2 < P.rc2)) continue;
+    const double dij2 = norm2x(lx[a], ly[a], lz[a]);
+    const double rij = sqrt(dij2), rik = sqrt(dik2), rjk = sqrt(djk2);
+    const double ravg = (rij + rjk + rik) / 3.0;  // threebody_potential.f90:894-898
+    const int branch = ravg <= P.rmin ? 0 : (ravg >= P.rmax ? 1 : 2);
+    if (branch == 2) atomicAdd(&icnt[C_NBLEND_FS3], 1);
+    const int slot = atomicAdd(&icnt[C_NTRI_FS3], 1);
+    if (slot >= tri_cap) continue;
+    // global damping and switch (threebody_potential.f90:898-904, 1418-1423)
+    const double pom = exp(P.alp3 * (ravg - P.r0dmp));
+    const double ppom = 1.0 / (1.0 + pom);
+    const double fdmp = pow(ppom, P.delta33);
+    const double cfact = (ravg - P.rmin) / (P.rmax - P.rmin);
+    Fs3Rec R;
+    R.cv[0][0] = lx[a];
+    R.cv[0][1] = ly[a];
+    R.cv[0][2] = lz[a];
+    R.cv[1][0] = xik;
+    R.cv[1][1] = yik;
+    R.cv[1][2] = zik;
+    R.cv[2][0] = xjk;
+    R.cv[2][1] = yjk;
+    R.cv[2][2] = zjk;
+    R.rr[0] = rij;
+    R.rr[1] = rik;
+    R.rr[2] = rjk;
+    R.fdmp = fdmp;
+    R.dfdmp = -P.alp3 * P.delta33 * pom * ppom * fdmp * (1.0 / 3.0);
+    R.smfun = 1.0 + 2.0 * cfact * cfact * cfact - 3.0 * cfact * cfact;
+    R.cf = 2.0 / (P.rmax - P.rmin) * (cfact * cfact - cfact);
+    R.mol[0] = i;
+    R.mol[1] = j;
+    R.mol[2] = k;
+    R.branch = branch;
+    rec[slot] = R;
+  }
+}
+
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  using type = double2;
+};
+template <>
+struct Vec2<float> {
+  using type = float2;
+};
+
+template <typename T>
+struct Fs3Smem {
+  using V2 = typename Vec2<T>::type;
+  double coef[2][kCoef];     // SR, LR coefficient by type triple [ti][tj][tk][ip jp kp]
+  double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
+  double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
+  V2 uu[3][kP][kRS];         // (e, e d) of each site pair, families ij, ik, jk
+  V2 dl[3][kP][kRS];         // (d, d ln e / dr)
+  double G[3][kP][kRS];      // accumulated site-force weights
+  double red[kFs3Block / 32];
+  Fs3Rec rec;
+};
+
+template <typename T>
+__device__ __forceinline__ T t_exp(T v);
+template <>
+__device__ __forceinline__ double t_exp<double>(double v) { return exp(v); }
+template <>
+__device__ __forceinline__ float t_exp<float>(float v) { return __expf(v); }
+
+template <typename T>
+__device__ __forceinline__ T t_sqrt(T v);
+template <>
+__device__ __forceinline__ double t_sqrt<double>(double v) { return sqrt(v); }
+template <>
+__device__ __forceinline__ float t_sqrt<float>(float v) { return sqrtf(v); }
+
+template <typename T>
+__device__ __forceinline__ T t_rcp(T v);
+template <>
+__device__ __forceinline__ double t_rcp<double>(double v) { return 1.0 / v; }
+template <>
+__device__ __forceinline__ float t_rcp<float>(float v) { return __frcp_rn(v); }
+
+// Family-generic addressing of one gradient pass (offsets in V2 units of uu):
+//   fam 0: outputs (is, js), sum over ks: X = uu[ik][is][ks], Y = uu[jk][js][ks]
+//   fam 1: outputs (is, ks), sum over js: X = uu[ij][is][js], Y = uu[jk][js][ks]
+//   fam 2: outputs (js, ks), sum over is: X = uu[ij][is][js], Y = uu[ik][is][ks]
+// X carries the powers of one distance, Y of another; the output pair carries the third.
+// The coefficient c[ip*4 + jp*2 + kp] of the type triple is at tr*mr + tc*mc + tb*mb, and
+// M_u (u = 2x + y for X_x Y_y) pairs with c[pa[u]] in the kp/jp/ip = 0 sum and c[pb[u]] in
+// the = 1 sum.
+struct PassCfg {
+  int xb, xr, xs, yb, yr, ys, mr, mc, mb;
+  int pa[4], pb[4];
+};
+
+__device__ __forceinline__ PassCfg pass_cfg(int fam) {
+  constexpr int F = kP * kRS;
+  PassCfg c;
+  if (fam == 0) {
+    c = {1 * F, kRS, 1, 2 * F, kRS, 1, 288, 48, 8, {0, 4, 2, 6}, {1, 5, 3, 7}};
+  } else if (fam == 1) {
+    c = {0, kRS, 1, 2 * F, 1, kRS, 288, 8, 48, {0, 4, 1, 5}, {2, 6, 3, 7}};
+  } else {
+    c = {0, 1, kRS, 1 * F, 1, kRS, 48, 8, 288, {0, 2, 1, 3}, {4, 6, 5, 7}};
+  }
+  return c;
+}
+
+// One gradient pass for the 2x2 output tile (r0, r0+1) x (c0, c0+1): q0/q1 receive the
+// coefficient-contracted sums; P = q0 + d q1 and dP/dd = q1 for the output's distance d.
+template <typename T>
+__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__restrict__ C,
+                                         const PassCfg &g, int r0, int c0, T q0[4], T q1[4]) {
+  using V2 = typename Vec2<T>::type;
+  const V2 *U = &S.uu[0][0][0];
+  const int tr = kPType[r0], tc = kPType[c0];
+  const double *cbase = C + tr * g.mr + tc * g.mc;
+  const V2 *X0 = U + g.xb + r0 * g.xr, *X1 = X0 + g.xr;
+  const V2 *Y0 = U + g.yb + c0 * g.yr, *Y1 = Y0 + g.yr;
+#pragma unroll
+  for (int o = 0; o < 4; o++) q0[o] = q1[o] = (T)0;
+  constexpr int kStart[7] = {0, 2, 4, 6, 10, 14, 18};
+#pragma unroll
+  for (int tb = 0; tb < 6; tb++) {
+    T M[4][4];
+#pragma unroll
+    for (int o = 0; o < 4; o++)
+#pragma unroll
+      for (int u = 0; u < 4; u++) M[o][u] = (T)0;
+#pragma unroll
+    for (int c = kStart[tb]; c < kStart[tb + 1]; c++) {
+      const V2 X[2] = {X0[c * g.xs], X1[c * g.xs]};
+      const V2 Y[2] = {Y0[c * g.ys], Y1[c * g.ys]};
+#pragma unroll
+      for (int rr = 0; rr < 2; rr++)
+#pragma unroll
+        for (int cc = 0; cc < 2; cc++) {
+          const int o = rr * 2 + cc;
+          M[o][0] += X[rr].x * Y[cc].x;
+          M[o][1] += X[rr].x * Y[cc].y;
+          M[o][2] += X[rr].y * Y[cc].x;
+          M[o][3] += X[rr].y * Y[cc].y;
+        }
+    }
+    const double *cp = cbase + tb * g.mb;
+    T ca[4], cb[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      ca[u] = (T)cp[g.pa[u]];
+      cb[u] = (T)cp[g.pb[u]];
+    }
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      q0[o] += ca[0] * M[o][0] + ca[1] * M[o][1] + ca[2] * M[o][2] + ca[3] * M[o][3];
+      q1[o] += cb[0] * M[o][0] + cb[1] * M[o][1] + cb[2] * M[o][2] + cb[3] * M[o][3];
+    }
+  }
+}
+
+// One SR (v = 0) or LR (v = 1) sweep of the current triple: tabulate the site pairs, run
+// the three gradient passes, add wsite * G into S.G and return the energy sum.
+template <typename T>
+__device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
+  using V2 = typename Vec2<T>::type;
+  const int tid = threadIdx.x;
+  if (tid < kPairs) {
+    const int a = tid / kNs3, b = tid % kNs3;
+    const T bb = (T)S.bgr[v][0][tid], gg = (T)S.bgr[v][1][tid], r0 = (T)S.bgr[v][2][tid];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const int m1 = p == 2 ? 1 : 0, m2 = p == 0 ? 1 : 2;
+      const double vx = S.rec.cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
+      const double vy = S.rec.cv[p][1] + (S.site[m1][a][1] - S.site[m2][b][1]);
+      const double vz = S.rec.cv[p][2] + (S.site[m1][a][2] - S.site[m2][b][2]);
+      const T r = t_sqrt<T>((T)(vx * vx + vy * vy + vz * vz));
+      const T ex = t_exp<T>(-gg * (r - r0));
+      const T damp = t_rcp<T>((T)1 + ex);
+      const T e = t_exp<T>(-bb * r) * damp;
+      V2 u, w;
+      u.x = e;
+      u.y = e * r;
+      w.x = r;
+      w.y = -bb + gg * ex * damp;
+      S.uu[p][pidx(a)][pidx(b)] = u;
+      S.dl[p][pidx(a)][pidx(b)] = w;
+    }
+  }
+  __syncthreads();
+  double esum = 0.0;
+  const int fam = tid / kPassThreads, lt = tid % kPassThreads;
+  if (fam < 3 && lt < kTile * kTile) {
+    const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
+    const PassCfg g = pass_cfg(fam);
+    T q0[4], q1[4];
+    fs3_pass<T>(S, S.coef[v], g, r0, c0, q0, q1);
+#pragma unroll
+    for (int o = 0; o < 4; o++) {
+      const int r = r0 + (o >> 1), c = c0 + (o & 1);
+      const V2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
+      const T P = q0[o] + w.x * q1[o];
+      if (fam == 0) esum += (double)u.x * (double)P;
+      S.G[fam][r][c] += wsite * (double)(u.x * (w.y * P + q1[o]) / w.x);
+    }
+  }
+  esum = warp_sum(esum);
+  if ((tid & 31) == 0) S.red[tid >> 5] = esum;
+  __syncthreads();
+  double tot = 0.0;
+#pragma unroll
+  for (int w = 0; w < kFs3Block / 32; w++) tot += S.red[w];
+  __syncthreads();
+  return tot;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
+    k_fs3(const Fs3Rec *__restrict__ recs, const int *__restrict__ icnt, int tri_cap,
+          const double4 *__restrict__ s17, const double *__restrict__ coef,
+          const double *__restrict__ bgr, int nm, int ns, double *f, double *fc3, double *scal) {
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
+  const int tid = threadIdx.x;
+  for (int t = tid; t < 2 * kCoef; t += kFs3Block) (&S.coef[0][0])[t] = coef[t];
+  for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&S.bgr[0][0][0])[t] = bgr[t];
+  // padded dummy site: zero weight, unit distance (keeps e / d finite)
+  for (int t = tid; t < 3 * kP; t += kFs3Block) {
+    const int p = t / kP, q = t % kP;
+    V2 z, one;
+    z.x = z.y = (T)0;
+    one.x = (T)1;
+    one.y = (T)0;
+    S.uu[p][1][q] = z;
+    S.uu[p][q][1] = z;
+    S.dl[p][1][q] = one;
+    S.dl[p][q][1] = one;
+  }
+  const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
+  const double conv = kH2kcal * 418.4 / kBohr2a;
+  const size_t nfs = (size_t)nm * ns;
+  double e_tot = 0.0, v_tot = 0.0;
+  for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
+    __syncthreads();
+    if (tid < kRecWords)
+      reinterpret_cast<double *>(&S.rec)[tid] = reinterpret_cast<const double *>(recs + t)[tid];
+    for (int u = tid; u < 3 * kP * kRS; u += kFs3Block) (&S.G[0][0][0])[u] = 0.0;
+    __syncthreads();
+    if (tid < 3 * kNs3) {
+      const int m = tid / kNs3, s = tid % kNs3;
+      const double4 o = s17[(size_t)S.rec.mol[m] * kNs3 + s];
+      S.site[m][s][0] = o.x;
+      S.site[m][s][1] = o.y;
+      S.site[m][s][2] = o.z;
+    }
+    __syncthreads();
+    const double fdmp = S.rec.fdmp, dfdmp = S.rec.dfdmp;
+    const int br = S.rec.branch;
+    double energy, comc;
+    if (br != 2) {
+      const double Sv = fs3_variant<T>(S, br, fdmp);
+      energy = fdmp * Sv;
+      comc = dfdmp * Sv;
+    } else {
+      const double smfun = S.rec.smfun, smfun2 = 1.0 - smfun, cf = S.rec.cf;
+      const double Ssr = fs3_variant<T>(S, 0, fdmp * smfun);
+      const double Slr = fs3_variant<T>(S, 1, fdmp * smfun2);
+      energy = fdmp * (smfun * Ssr + smfun2 * Slr);
+      comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
+    }
+    // ---- site forces: F = -sum_partner G * (pair vector); 4 lanes per (molecule, site),
+    // each summing a quarter of the 17 partners, reduced with shuffles.
+    double vsite = 0.0;
+    {
+      const int item = tid >> 2, part = tid & 3;
+      const bool act = item < 3 * kNs3;
+      const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = pidx(s);
+      const double(*cv)[3] = S.rec.cv;
+      double fx = 0.0, fy = 0.0, fz = 0.0;
+      if (act) {
+        for (int o = part; o < kNs3; o += 4) {
+          const int po = pidx(o);
+          if (m == 0) {
+            const double g0 = S.G[0][ps][po], g1 = S.G[1][ps][po];
+            const double a0 = cv[0][0] + (S.site[0][s][0] - S.site[1][o][0]);
+            const double a1 = cv[0][1] + (S.site[0][s][1] - S.site[1][o][1]);
+            const double a2 = cv[0][2] + (S.site[0][s][2] - S.site[1][o][2]);
+            const double b0 = cv[1][0] + (S.site[0][s][0] - S.site[2][o][0]);
+            const double b1 = cv[1][1] + (S.site[0][s][1] - S.site[2][o][1]);
+            const double b2 = cv[1][2] + (S.site[0][s][2] - S.site[2][o][2]);
+            fx -= g0 * a0 + g1 * b0;
+            fy -= g0 * a1 + g1 * b1;
+            fz -= g0 * a2 + g1 * b2;
+            vsite += g0 * (a0 * a0 + a1 * a1 + a2 * a2) + g1 * (b0 * b0 + b1 * b1 + b2 * b2);
+          } else if (m == 1) {
+            const double g0 = S.G[0][po][ps], g2 = S.G[2][ps][po];
+            const double a0 = cv[0][0] + (S.site[0][o][0] - S.site[1][s][0]);
+            const double a1 = cv[0][1] + (S.site[0][o][1] - S.site[1][s][1]);
+            const double a2 = cv[0][2] + (S.site[0][o][2] - S.site[1][s][2]);
+            const double c0 = cv[2][0] + (S.site[1][s][0] - S.site[2][o][0]);
+            const double c1 = cv[2][1] + (S.site[1][s][1] - S.site[2][o][1]);
+            const double c2 = cv[2][2] + (S.site[1][s][2] - S.site[2][o][2]);
+            fx -= -g0 * a0 + g2 * c0;
+            fy -= -g0 * a1 + g2 * c1;
+            fz -= -g0 * a2 + g2 * c2;
+            vsite += g2 * (c0 * c0 + c1 * c1 + c2 * c2);
+          } else {
+            const double g1 = S.G[1][po][ps], g2 = S.G[2][po][ps];
+            const double b0 = cv[1][0] + (S.site[0][o][0] - S.site[2][s][0]);
+            const double b1 = cv[1][1] + (S.site[0][o][1] - S.site[2][s][1]);
+            const double b2 = cv[1][2] + (S.site[0][o][2] - S.site[2][s][2]);
+            const double c0 = cv[2][0] + (S.site[1][o][0] - S.site[2][s][0]);
+            const double c1 = cv[2][1] + (S.site[1][o][1] - S.site[2][s][1]);
+            const double c2 = cv[2][2] + (S.site[1][o][2] - S.site[2][s][2]);
+            fx -= -g1 * b0 - g2 * c0;
+            fy -= -g1 * b1 - g2 * c1;
+            fz -= -g1 * b2 - g2 * c2;
+          }
+        }
+      }
+#pragma unroll
+      for (int off = 1; off < 4; off <<= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, off);
+        fy += __shfl_xor_sync(0xffffffffu, fy, off);
+        fz += __shfl_xor_sync(0xffffffffu, fz, off);
+      }
+      if (act && part == 0) {
+        const size_t o = (size_t)S.rec.mol[m] * ns + s;
+        atomicAdd(&f[o], fx * conv);
+        atomicAdd(&f[nfs + o], fy * conv);
+        atomicAdd(&f[2 * nfs + o], fz * conv);
+      }
+    }
+    if (tid == kFs3Block - 1) {
+      // COM forces from the R_avg damping and switch (threebody_potential.f90:1092-1120)
+      const double(*cv)[3] = S.rec.cv;
+      const double rij = S.rec.rr[0], rik = S.rec.rr[1], rjk = S.rec.rr[2];
+      const double ux = cv[0][0] / rij, uy = cv[0][1] / rij, uz = cv[0][2] / rij;
+      const double wx = cv[1][0] / rik, wy = cv[1][1] / rik, wz = cv[1][2] / rik;
+      const double sx = cv[2][0] / rjk, sy = cv[2][1] / rjk, sz = cv[2][2] / rjk;
+      const int m0 = S.rec.mol[0], m1 = S.rec.mol[1], m2 = S.rec.mol[2];
+      atomicAdd(&fc3[m0], -comc * (ux + wx) * conv);
+      atomicAdd(&fc3[nm + m0], -comc * (uy + wy) * conv);
+      atomicAdd(&fc3[2 * nm + m0], -comc * (uz + wz) * conv);
+      atomicAdd(&fc3[m1], -comc * (-ux + sx) * conv);
+      atomicAdd(&fc3[nm + m1], -comc * (-uy + sy) * conv);
+      atomicAdd(&fc3[2 * nm + m1], -comc * (-uz + sz) * conv);
+      atomicAdd(&fc3[m2], -comc * (-wx - sx) * conv);
+      atomicAdd(&fc3[nm + m2], -comc * (-wy - sy) * conv);
+      atomicAdd(&fc3[2 * nm + m2], -comc * (-wz - sz) * conv);
+      e_tot += energy;
+      v_tot += comc * (rij + rik + rjk);
+    }
+    v_tot += vsite;
+  }
+  v_tot = warp_sum(v_tot);
+  e_tot = warp_sum(e_tot);
+  if ((tid & 31) == 0) {
+    atomicAdd(&scal[S_FS3_VIR], v_tot);
+    if (e_tot != 0.0) atomicAdd(&scal[S_FS3_E], e_tot);
+  }
+}
+
+}  // namespace
+
+size_t fs3_record_bytes() { return sizeof(Fs3Rec); }
+
+cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
+                            int nm, Fs3Params P, void *rec, int tri_cap, int *icnt,
+                            cudaStream_t st) {
+  const size_t smem = sizeof(int) * (size_t)((cap + 1) & ~1) + 3 * sizeof(double) * (size_t)cap;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(k_fs3_enum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  k_fs3_enum<<<nm, 128, smem, st>>>(comb, nbr, ncnt, cap, nm, P, static_cast<Fs3Rec *>(rec),
+                                    tri_cap, icnt);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
+                       const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
+                       double *f, double *fc3, double *scal, int nsm, cudaStream_t st) {
+  cudaError_t e;
+  const Fs3Rec *R = static_cast<const Fs3Rec *>(rec);
+  int per_sm = 0;
+  if (precision == 0) {
+    const size_t smem = sizeof(Fs3Smem<double>);
+    e = cudaFuncSetAttribute(k_fs3<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<double>, kFs3Block, smem);
+    if (per_sm < 1) per_sm = 1;
+    k_fs3<double><<<nsm * per_sm, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns,
+                                                         f, fc3, scal);
+  } else {
+    const size_t smem = sizeof(Fs3Smem<float>);
+    e = cudaFuncSetAttribute(k_fs3<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<float>, kFs3Block, smem);
+    if (per_sm < 1) per_sm = 1;
+    k_fs3<float><<<nsm * per_sm, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f,
+                                                        fc3, scal);
+  }
+  return cudaGetLastError();
+}

@@ -143,7 +143,30 @@ __global__ void k_static_total(int n, const double *__restrict__ a, const double
   if (t < n) out[t] = a[t] + b[t] + c[t] + d[t];
 }
 
+// Convergence test of the Jacobi loop (nb_induction_model.f90:1269-1372), run as the last
+// node of the loop body: records the iteration count, the squared change and the energy of
+// the iteration, clears the accumulators for the next one, and keeps the WHILE node going
+// while change > thr and fewer than maxit iterations have run.
+__global__ void k_dip_cond(cudaGraphConditionalHandle h, double *scal, double *state, double thr,
+                           int maxit) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double ch = scal[S_IND_CHANGE], en = scal[S_IND_ENERGY];
+  const int it = (int)state[0] + 1;
+  state[0] = (double)it;
+  state[1] = ch;
+  state[2] = en;
+  scal[S_IND_CHANGE] = 0.0;
+  scal[S_IND_ENERGY] = 0.0;
+  cudaGraphSetConditional(h, (ch > thr && it < maxit) ? 1u : 0u);
+}
+
 }  // namespace
+
+cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, double *scal, double *state, double thr,
+                            int maxit, cudaStream_t st) {
+  k_dip_cond<<<1, 32, 0, st>>>(h, scal, state, thr, maxit);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_dip_tensor(const double *x, const double *y, const double *z,
                               const double *xs, const double *ys, const double *zs, int ld,
