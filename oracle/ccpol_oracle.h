@@ -15,8 +15,10 @@
  * periodic invariance + central finite differences of forces and rigid virial, same
  * fixture and tolerances), ported into tests/test_oracle_fs2_kat.py, and by the same
  * finite-difference/periodicity properties applied to FS3, Ewald and induction.
- * Values for FS3, induction and Ewald are therefore "pinned by properties", not by
- * reference-produced numbers (no Fortran compiler exists to run the reference).
+ * FS2 is pinned by that test.  FS3, induction and Ewald are "parity unpinned": they are
+ * checked by properties (finite differences, periodicity, virial identity), not against
+ * reference-produced numbers, because no Fortran compiler exists here to run the
+ * reference and it ships no golden values for them.
  *
  * Units follow the reference: positions in Angstrom, energies returned in kcal/mol,
  * forces in internal units (10 J/mol/Angstrom), virial in internal units.
