@@ -123,6 +123,20 @@ def ewald_setup(ewps: float, rcut: float, box: float):
     return a.value, k1.value, k2.value, k3.value
 
 
+def kspace_ewald_fixed(model: Model, x, y, z, xs, ys, zs, lmax, mmax, nmax, alp, box, qkcpe,
+                       fxs, fys, fzs, vir, stream: int | None = None) -> None:
+    """kspace_ewald (ewald.f90:754-1173) on device arrays with the library's fixed scratch:
+    no device memory is allocated.  All arrays are torch CUDA float64 tensors on the current
+    device; qkcpe and vir are one-element tensors.  Forces and vir are added to, qkcpe is
+    overwritten.  The work is enqueued on `stream` (a cudaStream_t address, None = the legacy
+    default stream) and is not waited for."""
+    nm, ld = xs.shape
+    check(_lib.lib().ccp_kspace_ewald_fixed(
+        model.handle, nm, x.data_ptr(), y.data_ptr(), z.data_ptr(), xs.data_ptr(),
+        ys.data_ptr(), zs.data_ptr(), ld, lmax, mmax, nmax, alp, box, qkcpe.data_ptr(),
+        fxs.data_ptr(), fys.data_ptr(), fzs.data_ptr(), vir.data_ptr(), stream))
+
+
 @dataclass
 class HotPathResult:
     energies: dict

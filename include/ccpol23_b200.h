@@ -160,6 +160,35 @@ int ccp_hot_path_device(ccp_context *ctx, const double *x_device, const double *
                         double *fzfs3_device, double *idmx_device, double *idmy_device,
                         double *idmz_device);
 
+/* ------------------------------------------ reciprocal-space Ewald, fixed scratch */
+/* No counterpart in the reference.  kspace_ewald (ewald.f90:754-1173) for callers that
+   cannot let the library allocate device memory: an MD driver that hands all device memory
+   to its own pool or caching allocator up front, or that cannot afford cudaMalloc/cudaFree
+   (cudaFree synchronises the whole device) inside its per-step loop.  Every temporary lives
+   in one fixed 16 MiB device array per device (CCP_KSPACE_FIXED_SCRATCH_BYTES): with the 5
+   charged sites of the water model that covers 2048 molecules at k-max 15; a call that would
+   need more returns CCP_ERR_CAPACITY with the byte count in ccp_last_error() and launches
+   nothing.  No context is needed; `m` only supplies the site charges.
+   - All arrays are DEVICE pointers on the calling thread's current device, in the layouts of
+     ccp_kspace_ewald; forces and *vir are added to, *qkcpe is overwritten.
+   - Work is enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream) and the
+     call returns without synchronising; results are ready when the stream reaches them.
+   - The first call on each device looks the scratch array up (cudaGetSymbolAddress, which
+     also loads the module); a caller that captures streams makes one call before capturing.
+   - The scratch is shared by all calls on a device: calls whose execution overlaps (other
+     streams, other host threads) race on it and give wrong results.  Order them on one
+     stream or with events.
+   - Allocates no device memory and, on success, no host memory.  The library clears what it
+     accumulates into (forces of its own, energy sums) inside the launch sequence. */
+#define CCP_KSPACE_FIXED_SCRATCH_BYTES (16u << 20)
+int ccp_kspace_ewald_fixed(const ccp_model *m, int nm, const double *x_device,
+                           const double *y_device, const double *z_device,
+                           const double *xs_device, const double *ys_device,
+                           const double *zs_device, int ld, int lmax, int mmax, int nmax,
+                           double alp, double box, double *qkcpe_device, double *fxs_device,
+                           double *fys_device, double *fzs_device, double *vir_device,
+                           void *stream);
+
 /* ---------------------------------------------------------------- diagnostics */
 /* These have no counterpart in the reference; they serve benchmarking and profiling. */
 
