@@ -33,7 +33,7 @@ EXPORTS = [
     "ccp_ewald_self_correction", "ccp_rspace_ewald", "ccp_kspace_ewald", "ccp_nb_induction",
     "ccp_threebody_term", "ccp_hot_path", "ccp_hot_path_device", "ccp_context_last_launches",
     "ccp_context_set_timing", "ccp_context_phase_ms", "ccp_device_fma_peak",
-    "ccp_kspace_ewald_fixed",
+    "ccp_kspace_ewald_fixed", "ccp_context_set_option", "ccp_context_get_option",
 ]
 
 
@@ -90,6 +90,8 @@ def lib():
     L.ccp_threebody_term.argtypes = [vp] + [vp] * 6 + [i, d, pd, pd] + [vp] * 9 + [pd]
     L.ccp_hot_path.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_hot_path_device.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
+    L.ccp_context_set_option.argtypes = [vp, C.c_char_p, i]
+    L.ccp_context_get_option.argtypes = [vp, C.c_char_p, pi]
     L.ccp_kspace_ewald_fixed.argtypes = [vp, i] + [vp] * 6 + [i, i, i, i, d, d] + [vp] * 5 + [vp]
     _lib = L
     return L

@@ -27,6 +27,9 @@ def data_dir(variant: str) -> Path:
     return DATA / variant
 
 
+NPHASE = 9  # CCP_NPHASE
+
+
 class Model:
     """Parameters read from CONTROL, FIELD, data3b_full, data3b_full_LR_4p5."""
 
@@ -198,12 +201,24 @@ class Context:
     def set_stream(self, stream_ptr: int | None):
         check(_lib.lib().ccp_context_set_stream(self._h, stream_ptr))
 
+    def set_option(self, name: str, value: int):
+        """Execution options of the dipole solve: "graph_loop", "phase_matrix" (0/1)."""
+        check(_lib.lib().ccp_context_set_option(self._h, name.encode(), int(value)))
+
+    def get_option(self, name: str) -> int:
+        v = C.c_int()
+        check(_lib.lib().ccp_context_get_option(self._h, name.encode(), C.byref(v)))
+        return v.value
+
     def set_timing(self, on: bool = True):
         check(_lib.lib().ccp_context_set_timing(self._h, int(on)))
 
     def phase_ms(self) -> np.ndarray:
-        out = np.zeros(7)
-        check(_lib.lib().ccp_context_phase_ms(self._h, out.ctypes.data, 7))
+        """Durations (ms) of the last evaluation's phases, in the order of CCP_NPHASE's
+        comment: packing+neighbours, real space, reciprocal, induction set-up, dipole
+        iteration, induction forces, FS2, FS3 triple list, FS3 kernel."""
+        out = np.zeros(NPHASE)
+        check(_lib.lib().ccp_context_phase_ms(self._h, out.ctypes.data, NPHASE))
         return out
 
     def last_launches(self) -> int:

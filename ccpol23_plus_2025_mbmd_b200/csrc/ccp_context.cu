@@ -108,7 +108,16 @@ struct ccp_context {
   cudaGraphExec_t ind_exec = nullptr;
   double *d_istate = nullptr;  // {iterations, last change, last energy}
   double *h_istate = nullptr;
+  unsigned *d_ticket = nullptr;  // last-block ticket of the fused update kernel
+  int ind_per_iter = 0;          // kernels per Jacobi iteration of the last solve
   std::vector<long long> ind_key;
+  // phase matrix P[polarisable site][k] of the dipole iteration (when it fits kPhaseBudget)
+  double2 *d_P = nullptr;
+  size_t P_cap = 0;
+  bool use_P = false;
+  // options (ccp_context_set_option)
+  int opt_graph = 1;  // Jacobi loop as a conditional graph (1) or driven from the host (0)
+  int opt_phase = 1;  // phase matrix when it fits (1) or never (0)
   // phase timing (diagnostics)
   bool timing = false;
   cudaEvent_t ev[CCP_NPHASE + 1] = {};
@@ -135,6 +144,8 @@ void free_ctx(ccp_context *c) {
   if (c->ind_exec) cudaGraphExecDestroy(c->ind_exec);
   if (c->ind_graph) cudaGraphDestroy(c->ind_graph);
   if (c->d_istate) cudaFree(c->d_istate);
+  if (c->d_ticket) cudaFree(c->d_ticket);
+  if (c->d_P) cudaFree(c->d_P);
   if (c->h_istate) cudaFreeHost(c->h_istate);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   if (c->own) cudaStreamDestroy(c->own);
@@ -259,18 +270,74 @@ struct EvalOut {
   bool converged = true;
 };
 
-// Builds (once per set of buffers and sizes) the CUDA graph of the Jacobi iteration: a
-// WHILE conditional node whose body is T.mu matvec -> dipole structure factors -> reciprocal
-// field -> in-place update -> convergence node.  The host launches it once per evaluation
-// and never synchronises inside the loop.
-int ensure_ind_graph(ccp_context *c) {
+// Largest phase matrix kept for the dipole iteration: it is re-read twice per iteration, so
+// it pays only while it stays resident in the 126 MB L2 next to the other working arrays.
+constexpr size_t kPhaseBudget = size_t(64) << 20;
+
+constexpr double kIndThr = 1.0e-20;  // iteridm convergence threshold on sum |dmu|^2
+
+// Enqueues one Jacobi step: with the phase matrix two kernels (k_iter.cu), otherwise T.mu,
+// the tiled dipole structure factors and reciprocal field, the update and the convergence
+// node.  `handle` is used only when use_graph is set.
+cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphConditionalHandle handle,
+                             int use_graph, int *nlaunch) {
   const SiteSets &S = c->S;
+  if (c->use_P) {
+    IterArgs A{};
+    A.nbr = c->d_nbr;
+    A.ncnt = c->d_ncnt;
+    A.cap = c->cap;
+    A.nw = c->nm * S.np;
+    A.np = S.np;
+    A.T4 = c->d_T4;
+    A.TB = c->d_TB;
+    A.S4 = c->d_S4;
+    A.SB = c->d_SB;
+    A.mu = c->d_mu;
+    A.eim = c->d_eim;
+    A.e0 = c->d_e0tot;
+    A.kv = c->d_kv;
+    A.nk = c->nk;
+    A.P = c->d_P;
+    A.sk = c->d_sk;
+    A.scal = c->d_scal;
+    A.state = c->d_istate;
+    A.ticket = c->d_ticket;
+    A.thr = kIndThr;
+    A.maxit = c->maxit;
+    A.use_graph = use_graph;
+    A.handle = handle;
+    A.S = S;
+    *nlaunch = 2;
+    cudaError_t e = launch_iter_a(A, st);
+    return e == cudaSuccess ? launch_iter_b(A, st) : e;
+  }
+  *nlaunch = 5;
+  cudaError_t e = launch_tmu(c->d_nbr, c->d_ncnt, c->cap, c->nm, S.np, c->d_T4, c->d_TB, c->d_S4,
+                             c->d_SB, c->d_mu, c->d_eim, st);
+  if (e == cudaSuccess)
+    e = launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
+                           c->kmax[2], c->d_mu, c->d_sk, st);
+  if (e == cudaSuccess)
+    e = launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
+                             c->kmax[2], c->d_mu, c->d_sk, c->d_eik, nullptr, st);
+  if (e == cudaSuccess)
+    e = launch_dip_update(c->nm, S, c->d_e0tot, c->d_eim, c->d_eik, c->d_mu, c->d_mu, c->d_scal, st);
+  if (e == cudaSuccess)
+    e = launch_dip_cond(handle, use_graph, c->d_scal, c->d_istate, kIndThr, c->maxit, st);
+  return e;
+}
+
+// Builds (once per set of buffers and sizes) the CUDA graph of the Jacobi iteration: a
+// WHILE conditional node whose body is one Jacobi step ending in the convergence test.
+// The host launches it once per evaluation and never synchronises inside the loop.
+int ensure_ind_graph(ccp_context *c) {
   std::vector<long long> key = {
       (long long)c->d_nbr, (long long)c->d_ncnt, (long long)c->d_T4,  (long long)c->d_TB,
       (long long)c->d_S4,  (long long)c->d_SB,   (long long)c->d_mu,  (long long)c->d_eim,
       (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_sk,  (long long)c->d_eik,
-      (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, c->cap, c->nm, c->nk,
-      c->kmax[0], c->kmax[1], c->kmax[2], c->maxit};
+      (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
+      (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit};
   if (c->ind_exec && key == c->ind_key) return CCP_OK;
   if (c->ind_exec) cudaGraphExecDestroy(c->ind_exec);
   if (c->ind_graph) cudaGraphDestroy(c->ind_graph);
@@ -289,23 +356,55 @@ int ensure_ind_graph(ccp_context *c) {
   cudaGraph_t body = np.conditional.phGraph_out[0];
   cudaStream_t cs = c->cap_stream;
   CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-  cudaError_t e = launch_dip_matvec(c->d_nbr, c->d_ncnt, c->cap, c->nm, S.np, c->d_T4, c->d_TB,
-                                    c->d_S4, c->d_SB, c->d_mu, c->d_eim, cs);
-  if (e == cudaSuccess)
-    e = launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
-                           c->kmax[2], c->d_mu, c->d_sk, cs);
-  if (e == cudaSuccess)
-    e = launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
-                             c->kmax[2], c->d_mu, c->d_sk, c->d_eik, nullptr, cs);
-  if (e == cudaSuccess)
-    e = launch_dip_update(c->nm, S, c->d_e0tot, c->d_eim, c->d_eik, c->d_mu, c->d_mu, c->d_scal, cs);
-  if (e == cudaSuccess) e = launch_dip_cond(h, c->d_scal, c->d_istate, 1.0e-20, c->maxit, cs);
+  int nl = 0;
+  cudaError_t e = enqueue_dip_step(c, cs, h, 1, &nl);
   cudaGraph_t captured = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
   if (!cuda_ok(e, "capture of the dipole loop")) return CCP_ERR_CUDA;
   CK(e2);
   CK(cudaGraphInstantiate(&c->ind_exec, c->ind_graph, 0));
   c->ind_key = key;
+  return CCP_OK;
+}
+
+// The whole Jacobi solve from mu = 0.  The state {iterations, change, energy} is copied to
+// h_istate; in the graph form the copy completes at the evaluation's final synchronisation.
+int run_dipole_loop(ccp_context *c, cudaStream_t st) {
+  CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * c->nm * c->S.np * 3, st));
+  CK(cudaMemsetAsync(c->d_istate, 0, 3 * sizeof(double), st));
+  CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
+  CK(cudaMemsetAsync(c->d_ticket, 0, sizeof(unsigned), st));
+  if (c->use_P) CK(cudaMemsetAsync(c->d_sk, 0, sizeof(double) * 4 * (size_t)c->nk, st));
+  int per = 0;
+  if (c->opt_graph) {
+    int r = ensure_ind_graph(c);
+    if (r) return r;
+    CK(cudaGraphLaunch(c->ind_exec, st));
+    CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    per = c->use_P ? 2 : 5;
+  } else {
+    for (;;) {
+      if (!cuda_ok(enqueue_dip_step(c, st, 0, 0, &per), "dipole step")) return CCP_ERR_CUDA;
+      CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      const int it = (int)c->h_istate[0];
+      if (!(c->h_istate[1] > kIndThr && it < c->maxit)) break;
+    }
+  }
+  c->ind_per_iter = per;
+  return CCP_OK;
+}
+
+// Allocates the phase matrix when the dipole iteration can use it.
+int ensure_phase_matrix(ccp_context *c) {
+  const size_t n = (size_t)c->nm * c->S.np * c->nk;
+  c->use_P = c->opt_phase && c->nk > 0 && n * sizeof(double2) <= kPhaseBudget;
+  if (!c->use_P || n <= c->P_cap) return CCP_OK;
+  if (c->d_P) cudaFree(c->d_P);
+  c->d_P = nullptr;
+  c->P_cap = 0;
+  CK(dalloc(&c->d_P, n));
+  c->P_cap = n;
   return CCP_OK;
 }
 
@@ -359,6 +458,10 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
   F2.delta33 = c->delta33;
   if (mask & T_KSPACE || mask & T_INDUCTION) {
     int r = ensure_kspace(c, box);
+    if (r) return r;
+  }
+  if (mask & T_INDUCTION) {
+    int r = ensure_phase_matrix(c);
     if (r) return r;
   }
   // neighbour-list radius covering every consumer (each re-tests with its exact cut-off)
@@ -416,25 +519,15 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
                            c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, st));
       LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
                              st));
-      CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * nm * S.np * 3, st));
-      CK(cudaMemsetAsync(c->d_istate, 0, 3 * sizeof(double), st));
-      CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
+      if (c->use_P)
+        LK(launch_phase_matrix(c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
+                               c->d_P, st));
+      mark(4);
       {
-        int r = ensure_ind_graph(c);
+        int r = run_dipole_loop(c, st);
         if (r) return r;
       }
-      CK(cudaGraphLaunch(c->ind_exec, st));
-      CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      const int it = (int)c->h_istate[0];
-      c->launches += 5 * it;
-      o.ind_e = c->h_istate[2];
-      o.iters = it;
-      o.converged = it < c->maxit;
-      if (!o.converged) {
-        set_error("No convergence in the induced-dipole iteration (maxit reached)");
-        return CCP_ERR_NOT_CONVERGED;
-      }
+      mark(5);
       LK(launch_pair_indforce(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
                               c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_f, c->d_scal, st));
       LK(launch_kspace_sums(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
@@ -442,24 +535,27 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       LK(launch_kspace_energy(3, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, st));
       LK(launch_kspace_gather(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
                               c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, st));
+    } else {
+      mark(4);
+      mark(5);
     }
-    mark(4);
+    mark(6);
     if (mask & T_FS2) {
       LK(launch_fs2_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F2, c->d_pairs, c->pair_cap,
                          c->d_icnt, st));
       LK(launch_fs2(c->precision, c->d_pairs, c->d_icnt, c->pair_cap, c->d_comb, c->d_s17, c->d_nbr,
                     c->d_ncnt, c->cap, F2, nm, ns, c->d_f, c->d_fc2, c->d_scal, st));
     }
-    mark(5);
+    mark(7);
     if (mask & T_FS3)
       LK(launch_fs3_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F3, c->d_tri, c->tri_cap,
                          c->d_icnt, st));
-    mark(6);
+    mark(8);
     if (mask & T_FS3) {
       LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
                     nm, ns, c->d_f, c->d_fc3, c->d_scal, c->nsm, st));
     }
-    mark(7);
+    mark(9);
     CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c->h_icnt, c->d_icnt, sizeof(int) * C_COUNT, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -482,6 +578,16 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
       int r = ensure_lists(c, ncap, ntcap, npcap);
       if (r) return r;
       continue;
+    }
+    if (mask & T_INDUCTION) {
+      o.iters = (int)c->h_istate[0];
+      o.ind_e = c->h_istate[2];
+      c->launches += c->ind_per_iter * o.iters;
+      o.converged = o.iters < c->maxit;
+      if (!o.converged) {
+        set_error("No convergence in the induced-dipole iteration (maxit reached)");
+        return CCP_ERR_NOT_CONVERGED;
+      }
     }
     if (c->timing)
       for (int k = 0; k < CCP_NPHASE; k++) {
@@ -757,6 +863,8 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
     return fail("stream");
   c->stream = c->own;
   if (cudaMalloc(&c->d_istate, 3 * sizeof(double)) != cudaSuccess ||
+      cudaMalloc(&c->d_ticket, sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(c->d_ticket, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_istate, 3 * sizeof(double)) != cudaSuccess)
     return fail("loop state");
   const size_t n = nm, nsi = (size_t)nm * m->ns, np3 = (size_t)nm * std::max(S.np, 1) * 3;
@@ -851,6 +959,36 @@ int ccp_context_set_timing(ccp_context *ctx, int on) {
   if (on && !ctx->ev[0])
     for (auto &e : ctx->ev) CK(cudaEventCreate(&e));
   ctx->timing = on != 0;
+  return CCP_OK;
+}
+
+int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
+  if (!ctx || !name) return CCP_ERR_BAD_INPUT;
+  const std::string n(name);
+  if (n == "graph_loop") {
+    ctx->opt_graph = value != 0;
+  } else if (n == "phase_matrix") {
+    ctx->opt_phase = value != 0;
+  } else {
+    set_error("ccp_context_set_option: unknown option " + n);
+    return CCP_ERR_BAD_INPUT;
+  }
+  return CCP_OK;
+}
+
+int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value) {
+  if (!ctx || !name || !value) return CCP_ERR_BAD_INPUT;
+  const std::string n(name);
+  if (n == "graph_loop") {
+    *value = ctx->opt_graph;
+  } else if (n == "phase_matrix") {
+    *value = ctx->opt_phase;
+  } else if (n == "phase_matrix_active") {
+    *value = ctx->use_P ? 1 : 0;
+  } else {
+    set_error("ccp_context_get_option: unknown option " + n);
+    return CCP_ERR_BAD_INPUT;
+  }
   return CCP_OK;
 }
 

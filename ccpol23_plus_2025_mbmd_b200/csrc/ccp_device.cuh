@@ -122,6 +122,32 @@ struct Fs2Params {
   double boxb, rc2, alp3, r0dmp, delta33;
 };
 
+struct KVec {
+  double rl, rm, rn, ak;  // 2*pi*(l,m,n)/L and a(k)
+  int l, m, n, pad;
+};
+
+// Arguments of one Jacobi step of the dipole solve with the phase matrix (k_iter.cu).
+struct IterArgs {
+  const int *nbr, *ncnt;
+  int cap, nw, np;  // nw = polarisable sites = nm * np
+  const double4 *T4;
+  const double *TB;
+  const double4 *S4;
+  const double *SB;
+  double *mu, *eim;
+  const double *e0;
+  const KVec *kv;
+  int nk;
+  const double2 *P;
+  double *sk, *scal, *state;  // state = {iterations, change, energy}
+  unsigned *ticket;
+  double thr;
+  int maxit, use_graph;
+  cudaGraphConditionalHandle handle;
+  SiteSets S;
+};
+
 // ------------------------------------------------------------------ launchers
 // All launchers enqueue on `st` and return cudaGetLastError().
 cudaError_t launch_prep(const double *x, const double *y, const double *z, const double *xs,
@@ -144,14 +170,20 @@ cudaError_t launch_dip_tensor(const double *x, const double *y, const double *z,
                               const double4 *act, const int *nbr, const double4 *nbrv,
                               const int *ncnt, int cap, int nm, SiteSets S, EwaldParams P,
                               double4 *T4, double *TB, double4 *S4, double *SB, cudaStream_t st);
-cudaError_t launch_dip_matvec(const int *nbr, const int *ncnt, int cap, int nm, int np,
-                              const double4 *T4, const double *TB, const double4 *S4,
-                              const double *SB, const double *mu, double *eim, cudaStream_t st);
 cudaError_t launch_static_total(int n, const double *a, const double *b, const double *c,
                                 const double *d, double *out, cudaStream_t st);
-// Convergence node of the graph-resident Jacobi loop; state = {iterations, change, energy}.
-cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, double *scal, double *state, double thr,
-                            int maxit, cudaStream_t st);
+// Convergence node of the Jacobi loop; state = {iterations, change, energy}.  Sets the WHILE
+// node's condition only when use_graph is non-zero.
+cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, int use_graph, double *scal,
+                            double *state, double thr, int maxit, cudaStream_t st);
+// k_iter.cu
+cudaError_t launch_phase_matrix(const KVec *kv, int nk, const double2 *tab, int nm, SiteSets S,
+                                int kl, int km, int kn, double2 *P, cudaStream_t st);
+cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np, const double4 *T4,
+                       const double *TB, const double4 *S4, const double *SB, const double *mu,
+                       double *eim, cudaStream_t st);
+cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st);
+cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,
                                  const double *xs, const double *ys, const double *zs,
                                  int ld, const double4 *act, const int *nbr,
@@ -160,10 +192,6 @@ cudaError_t launch_pair_indforce(const double *x, const double *y, const double 
                                  double *scal, cudaStream_t st);
 
 // reciprocal space
-struct KVec {
-  double rl, rm, rn, ak;  // 2*pi*(l,m,n)/L and a(k)
-  int l, m, n, pad;
-};
 cudaError_t launch_ktab(const double4 *com, const double4 *act, int nm, SiteSets S,
                         double box, int kmax_l, int kmax_m, int kmax_n, double2 *tab,
                         cudaStream_t st);

@@ -38,6 +38,15 @@ constexpr int kFs3Block = 320;             // 3 x 96 pass threads + one warp; 28
 constexpr int kRecWords = 18;              // doubles per triple record
 
 __device__ __forceinline__ int pidx(int s) { return s == 0 ? 0 : s + 1; }
+// Storage order of a padded index in the site-pair tables: even indices first, then odd,
+// so the two rows (or columns) of a 2x2 output tile sit 9 rows apart and neighbouring
+// tiles hit different shared-memory banks.
+__host__ __device__ constexpr int sp(int x) { return (x & 1) * 9 + (x >> 1); }
+// Coefficients in shared memory as double2 pairs (c[2j], c[2j+1]) of each type triple, with
+// padded strides (in double2 units) so that the lanes of a warp, which differ in one type
+// index, read different banks: ti * kCi + tj * kCj + tk * kCk + j.
+constexpr int kCk = 5, kCj = 31, kCi = 187;
+constexpr int kCoef2 = 6 * kCi;
 __constant__ int kPType[kP] = {0, 0, 1, 1, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5};
 
 // Per-triple record written by the enumeration: COM vectors ij, ik, jk (bohr, computed as
@@ -177,7 +186,7 @@ struct Vec2<float> {
 template <typename T>
 struct Fs3Smem {
   using V2 = typename Vec2<T>::type;
-  double coef[2][kCoef];     // SR, LR coefficient by type triple [ti][tj][tk][ip jp kp]
+  double2 coef[2][kCoef2];   // SR, LR coefficients, padded layout (kCi, kCj, kCk)
   double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
   double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
   V2 uu[3][kP][kRS];         // (e, e d) of each site pair, families ij, ik, jk
@@ -208,43 +217,41 @@ __device__ __forceinline__ double t_rcp<double>(double v) { return 1.0 / v; }
 template <>
 __device__ __forceinline__ float t_rcp<float>(float v) { return __frcp_rn(v); }
 
-// Family-generic addressing of one gradient pass (offsets in V2 units of uu):
-//   fam 0: outputs (is, js), sum over ks: X = uu[ik][is][ks], Y = uu[jk][js][ks]
-//   fam 1: outputs (is, ks), sum over js: X = uu[ij][is][js], Y = uu[jk][js][ks]
-//   fam 2: outputs (js, ks), sum over is: X = uu[ij][is][js], Y = uu[ik][is][ks]
+// One gradient pass of family FAM for the 2x2 output tile (r0, r0+1) x (c0, c0+1):
+//   FAM 0: outputs (is, js), sum over ks: X = uu[ik][is][ks], Y = uu[jk][js][ks]
+//   FAM 1: outputs (is, ks), sum over js: X = uu[ij][is][js], Y = uu[jk][js][ks]
+//   FAM 2: outputs (js, ks), sum over is: X = uu[ij][is][js], Y = uu[ik][is][ks]
 // X carries the powers of one distance, Y of another; the output pair carries the third.
-// The coefficient c[ip*4 + jp*2 + kp] of the type triple is at tr*mr + tc*mc + tb*mb, and
-// M_u (u = 2x + y for X_x Y_y) pairs with c[pa[u]] in the kp/jp/ip = 0 sum and c[pb[u]] in
-// the = 1 sum.
-struct PassCfg {
-  int xb, xr, xs, yb, yr, ys, mr, mc, mb;
-  int pa[4], pb[4];
+// Per type block of the summed site, M_u (u = 2x + y for X_x Y_y) is contracted with the
+// type triple's coefficients: q0 with the power-0 and q1 with the power-1 coefficient of the
+// output distance, so that P = q0 + d q1 and dP/dd = q1.
+template <int FAM>
+struct PassIdx;
+template <>
+struct PassIdx<0> {  // coefficient index (ti, tj, tk) = (row, col, sum)
+  static constexpr int mr = kCi, mc = kCj, mb = kCk;
+  static constexpr unsigned pa = 0x6240, pb = 0x7351;  // 4-bit fields: u -> power index
+};
+template <>
+struct PassIdx<1> {  // (row, sum, col)
+  static constexpr int mr = kCi, mc = kCk, mb = kCj;
+  static constexpr unsigned pa = 0x5140, pb = 0x7362;  // 4-bit fields: u -> power index
+};
+template <>
+struct PassIdx<2> {  // (sum, row, col)
+  static constexpr int mr = kCj, mc = kCk, mb = kCi;
+  static constexpr unsigned pa = 0x3120, pb = 0x7564;  // 4-bit fields: u -> power index
 };
 
-__device__ __forceinline__ PassCfg pass_cfg(int fam) {
-  constexpr int F = kP * kRS;
-  PassCfg c;
-  if (fam == 0) {
-    c = {1 * F, kRS, 1, 2 * F, kRS, 1, 288, 48, 8, {0, 4, 2, 6}, {1, 5, 3, 7}};
-  } else if (fam == 1) {
-    c = {0, kRS, 1, 2 * F, 1, kRS, 288, 8, 48, {0, 4, 1, 5}, {2, 6, 3, 7}};
-  } else {
-    c = {0, 1, kRS, 1 * F, 1, kRS, 48, 8, 288, {0, 2, 1, 3}, {4, 6, 5, 7}};
-  }
-  return c;
-}
-
-// One gradient pass for the 2x2 output tile (r0, r0+1) x (c0, c0+1): q0/q1 receive the
-// coefficient-contracted sums; P = q0 + d q1 and dP/dd = q1 for the output's distance d.
-template <typename T>
-__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__restrict__ C,
-                                         const PassCfg &g, int r0, int c0, T q0[4], T q1[4]) {
+template <typename T, int FAM>
+__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double2 *__restrict__ C,
+                                         int r0, int c0, T q0[4], T q1[4]) {
   using V2 = typename Vec2<T>::type;
-  const V2 *U = &S.uu[0][0][0];
+  using I = PassIdx<FAM>;
   const int tr = kPType[r0], tc = kPType[c0];
-  const double *cbase = C + tr * g.mr + tc * g.mc;
-  const V2 *X0 = U + g.xb + r0 * g.xr, *X1 = X0 + g.xr;
-  const V2 *Y0 = U + g.yb + c0 * g.yr, *Y1 = Y0 + g.yr;
+  const double2 *cbase = C + tr * I::mr + tc * I::mc;
+  // physical rows/columns of the tile (r0, c0 even): sp(r0) = r0/2, sp(r0+1) = 9 + r0/2
+  const int ra = r0 >> 1, rb = ra + 9, ca_ = c0 >> 1, cb_ = ca_ + 9;
 #pragma unroll
   for (int o = 0; o < 4; o++) q0[o] = q1[o] = (T)0;
   constexpr int kStart[7] = {0, 2, 4, 6, 10, 14, 18};
@@ -257,8 +264,24 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__re
       for (int u = 0; u < 4; u++) M[o][u] = (T)0;
 #pragma unroll
     for (int c = kStart[tb]; c < kStart[tb + 1]; c++) {
-      const V2 X[2] = {X0[c * g.xs], X1[c * g.xs]};
-      const V2 Y[2] = {Y0[c * g.ys], Y1[c * g.ys]};
+      const int pc = sp(c);
+      V2 X[2], Y[2];
+      if (FAM == 0) {
+        X[0] = S.uu[1][ra][pc];
+        X[1] = S.uu[1][rb][pc];
+        Y[0] = S.uu[2][ca_][pc];
+        Y[1] = S.uu[2][cb_][pc];
+      } else if (FAM == 1) {
+        X[0] = S.uu[0][ra][pc];
+        X[1] = S.uu[0][rb][pc];
+        Y[0] = S.uu[2][pc][ca_];
+        Y[1] = S.uu[2][pc][cb_];
+      } else {
+        X[0] = S.uu[0][pc][ra];
+        X[1] = S.uu[0][pc][rb];
+        Y[0] = S.uu[1][pc][ca_];
+        Y[1] = S.uu[1][pc][cb_];
+      }
 #pragma unroll
       for (int rr = 0; rr < 2; rr++)
 #pragma unroll
@@ -270,12 +293,14 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__re
           M[o][3] += X[rr].y * Y[cc].y;
         }
     }
-    const double *cp = cbase + tb * g.mb;
+    const double2 *cp = cbase + tb * I::mb;
+    const double2 c01 = cp[0], c23 = cp[1], c45 = cp[2], c67 = cp[3];
+    const double cw[8] = {c01.x, c01.y, c23.x, c23.y, c45.x, c45.y, c67.x, c67.y};
     T ca[4], cb[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      ca[u] = (T)cp[g.pa[u]];
-      cb[u] = (T)cp[g.pb[u]];
+      ca[u] = (T)cw[(I::pa >> (4 * u)) & 15u];
+      cb[u] = (T)cw[(I::pb >> (4 * u)) & 15u];
     }
 #pragma unroll
     for (int o = 0; o < 4; o++) {
@@ -309,8 +334,8 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
       u.y = e * r;
       w.x = r;
       w.y = -bb + gg * ex * damp;
-      S.uu[p][pidx(a)][pidx(b)] = u;
-      S.dl[p][pidx(a)][pidx(b)] = w;
+      S.uu[p][sp(pidx(a))][sp(pidx(b))] = u;
+      S.dl[p][sp(pidx(a))][sp(pidx(b))] = w;
     }
   }
   __syncthreads();
@@ -318,12 +343,16 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
   const int fam = tid / kPassThreads, lt = tid % kPassThreads;
   if (fam < 3 && lt < kTile * kTile) {
     const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
-    const PassCfg g = pass_cfg(fam);
     T q0[4], q1[4];
-    fs3_pass<T>(S, S.coef[v], g, r0, c0, q0, q1);
+    if (fam == 0)
+      fs3_pass<T, 0>(S, S.coef[v], r0, c0, q0, q1);
+    else if (fam == 1)
+      fs3_pass<T, 1>(S, S.coef[v], r0, c0, q0, q1);
+    else
+      fs3_pass<T, 2>(S, S.coef[v], r0, c0, q0, q1);
 #pragma unroll
     for (int o = 0; o < 4; o++) {
-      const int r = r0 + (o >> 1), c = c0 + (o & 1);
+      const int r = sp(r0 + (o >> 1)), c = sp(c0 + (o & 1));
       const V2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
       const T P = q0[o] + w.x * q1[o];
       if (fam == 0) esum += (double)u.x * (double)P;
@@ -349,7 +378,15 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
   const int tid = threadIdx.x;
-  for (int t = tid; t < 2 * kCoef; t += kFs3Block) (&S.coef[0][0])[t] = coef[t];
+  for (int t = tid; t < 2 * kCoef2; t += kFs3Block) (&S.coef[0][0])[t] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int t = tid; t < 2 * kCoef / 2; t += kFs3Block) {
+    const int v = t / (kCoef / 2), r = t % (kCoef / 2);
+    const int tri = r / 4, j = r % 4;  // type triple ti*36 + tj*6 + tk, pair j of 4
+    const int ti = tri / 36, tj = (tri / 6) % 6, tk = tri % 6;
+    const double *src = coef + (size_t)v * kCoef + tri * 8 + 2 * j;
+    S.coef[v][ti * kCi + tj * kCj + tk * kCk + j] = make_double2(src[0], src[1]);
+  }
   for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&S.bgr[0][0][0])[t] = bgr[t];
   // padded dummy site: zero weight, unit distance (keeps e / d finite)
   for (int t = tid; t < 3 * kP; t += kFs3Block) {
@@ -358,10 +395,10 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
     z.x = z.y = (T)0;
     one.x = (T)1;
     one.y = (T)0;
-    S.uu[p][1][q] = z;
-    S.uu[p][q][1] = z;
-    S.dl[p][1][q] = one;
-    S.dl[p][q][1] = one;
+    S.uu[p][sp(1)][q] = z;
+    S.uu[p][q][sp(1)] = z;
+    S.dl[p][sp(1)][q] = one;
+    S.dl[p][q][sp(1)] = one;
   }
   const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
   const double conv = kH2kcal * 418.4 / kBohr2a;
@@ -401,12 +438,12 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
     {
       const int item = tid >> 2, part = tid & 3;
       const bool act = item < 3 * kNs3;
-      const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = pidx(s);
+      const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = sp(pidx(s));
       const double(*cv)[3] = S.rec.cv;
       double fx = 0.0, fy = 0.0, fz = 0.0;
       if (act) {
         for (int o = part; o < kNs3; o += 4) {
-          const int po = pidx(o);
+          const int po = sp(pidx(o));
           if (m == 0) {
             const double g0 = S.G[0][ps][po], g1 = S.G[1][ps][po];
             const double a0 = cv[0][0] + (S.site[0][s][0] - S.site[1][o][0]);

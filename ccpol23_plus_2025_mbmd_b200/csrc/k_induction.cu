@@ -7,8 +7,9 @@
 // 1468-1517) plus the Tang-Toennies correction (shortrange_efield_idm_damped, :5716-5736),
 // and, within the molecule, the erf-screened intramolecular term with the point self term
 // (self_efield_idm, :2693-2783).  The geometry is fixed during the iteration, so the
-// (d, A, B) of every site pair are computed once per evaluation and each iteration is a
-// sparse tiled matrix-vector product over the neighbour list.
+// (d, A, B) of every site pair are computed once per evaluation, stored per polarisable site
+// as T4/TB[i][p][n][q] (neighbour n of molecule i, its polarisable site q) so that the
+// per-iteration product (k_iter.cu) reads them contiguously.
 #include "ccp_device.cuh"
 
 using namespace ccpd;
@@ -28,7 +29,7 @@ __global__ void k_dip_tensor(const double *__restrict__ x, const double *__restr
   const int cnt = ncnt[i];
   for (int it = threadIdx.x; it < cnt * npp; it += blockDim.x) {
     const int n = it / npp, pq = it % npp, p = pq / np, q = pq % np;
-    const size_t o = ((size_t)i * cap + n) * npp + pq;
+    const size_t o = (((size_t)i * np + p) * cap + n) * np + q;
     const double4 c = nbrv[(size_t)i * cap + n];
     if (!(c.w < P.rcutsd)) {
       T4[o] = make_double4(0.0, 0.0, 0.0, 0.0);
@@ -85,56 +86,6 @@ __global__ void k_dip_tensor(const double *__restrict__ x, const double *__restr
   }
 }
 
-// One warp per polarisable site (i, p); lanes stride over i's neighbours.
-__global__ void __launch_bounds__(256)
-    k_dip_matvec(const int *__restrict__ nbr, const int *__restrict__ ncnt, int cap, int nm,
-                 int np, const double4 *__restrict__ T4, const double *__restrict__ TB,
-                 const double4 *__restrict__ S4, const double *__restrict__ SB,
-                 const double *__restrict__ mu, double *eim) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= nm * np) return;
-  const int i = w / np, p = w % np, npp = np * np;
-  const int cnt = ncnt[i];
-  double ex = 0.0, ey = 0.0, ez = 0.0;
-  for (int n = lane; n < cnt; n += 32) {
-    const int j = nbr[(size_t)i * cap + n];
-    const size_t o = ((size_t)i * cap + n) * npp + (size_t)p * np;
-    for (int q = 0; q < np; q++) {
-      const double4 t = T4[o + q];
-      const double b = TB[o + q];
-      const double mx = mu[((size_t)j * np + q) * 3 + 0];
-      const double my = mu[((size_t)j * np + q) * 3 + 1];
-      const double mz = mu[((size_t)j * np + q) * 3 + 2];
-      const double dm = t.w * (t.x * mx + t.y * my + t.z * mz);
-      ex += dm * t.x - b * mx;
-      ey += dm * t.y - b * my;
-      ez += dm * t.z - b * mz;
-    }
-  }
-  if (lane < np) {
-    const int q = lane;
-    const size_t o = (size_t)i * npp + (size_t)p * np + q;
-    const double4 t = S4[o];
-    const double b = SB[o];
-    const double mx = mu[((size_t)i * np + q) * 3 + 0];
-    const double my = mu[((size_t)i * np + q) * 3 + 1];
-    const double mz = mu[((size_t)i * np + q) * 3 + 2];
-    const double dm = t.w * (t.x * mx + t.y * my + t.z * mz);
-    ex += dm * t.x - b * mx;
-    ey += dm * t.y - b * my;
-    ez += dm * t.z - b * mz;
-  }
-  ex = warp_sum(ex);
-  ey = warp_sum(ey);
-  ez = warp_sum(ez);
-  if (lane == 0) {
-    eim[(size_t)w * 3 + 0] = ex;
-    eim[(size_t)w * 3 + 1] = ey;
-    eim[(size_t)w * 3 + 2] = ez;
-  }
-}
-
 // total static field E0 = r + k + self + short-range (nb_induction_model.f90:1320-1322)
 __global__ void k_static_total(int n, const double *__restrict__ a, const double *__restrict__ b,
                                const double *__restrict__ c, const double *__restrict__ d,
@@ -147,8 +98,8 @@ __global__ void k_static_total(int n, const double *__restrict__ a, const double
 // node of the loop body: records the iteration count, the squared change and the energy of
 // the iteration, clears the accumulators for the next one, and keeps the WHILE node going
 // while change > thr and fewer than maxit iterations have run.
-__global__ void k_dip_cond(cudaGraphConditionalHandle h, double *scal, double *state, double thr,
-                           int maxit) {
+__global__ void k_dip_cond(cudaGraphConditionalHandle h, int use_graph, double *scal,
+                           double *state, double thr, int maxit) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   const double ch = scal[S_IND_CHANGE], en = scal[S_IND_ENERGY];
   const int it = (int)state[0] + 1;
@@ -157,14 +108,14 @@ __global__ void k_dip_cond(cudaGraphConditionalHandle h, double *scal, double *s
   state[2] = en;
   scal[S_IND_CHANGE] = 0.0;
   scal[S_IND_ENERGY] = 0.0;
-  cudaGraphSetConditional(h, (ch > thr && it < maxit) ? 1u : 0u);
+  if (use_graph) cudaGraphSetConditional(h, (ch > thr && it < maxit) ? 1u : 0u);
 }
 
 }  // namespace
 
-cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, double *scal, double *state, double thr,
-                            int maxit, cudaStream_t st) {
-  k_dip_cond<<<1, 32, 0, st>>>(h, scal, state, thr, maxit);
+cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, int use_graph, double *scal,
+                            double *state, double thr, int maxit, cudaStream_t st) {
+  k_dip_cond<<<1, 32, 0, st>>>(h, use_graph, scal, state, thr, maxit);
   return cudaGetLastError();
 }
 
@@ -176,15 +127,6 @@ cudaError_t launch_dip_tensor(const double *x, const double *y, const double *z,
                               cudaStream_t st) {
   k_dip_tensor<<<nm, 128, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt, cap, nm, S, P, T4,
                                    TB, S4, SB);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_dip_matvec(const int *nbr, const int *ncnt, int cap, int nm, int np,
-                              const double4 *T4, const double *TB, const double4 *S4,
-                              const double *SB, const double *mu, double *eim, cudaStream_t st) {
-  const int warps = nm * np;
-  k_dip_matvec<<<(warps * 32 + 255) / 256, 256, 0, st>>>(nbr, ncnt, cap, nm, np, T4, TB, S4, SB, mu,
-                                                          eim);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,292 @@
+// k_iter.cu -- one Jacobi step of the induced-dipole solve as two kernels (sm_100a, FP64).
+//
+// iteridm (nb_induction_model.f90:1193-1407) updates every polarisable dipole from the field
+//   E = T.mu (real space + short-range + intramolecular)  +  E_k(mu) (reciprocal)  +  E0.
+// The geometry is fixed during the solve, so besides the dipole tensors (k_induction.cu) the
+// phases exp(i k.r_s) of every (polarisable site s, k-vector) pair are computed once per
+// evaluation into a matrix P[s][k] (k fastest) when it fits the L2-sized budget.  Each
+// iteration then is
+//   A  blocks [0, nA):  T.mu, one warp per polarisable site, lanes over its (neighbour, site)
+//                       tensor entries (contiguous, so the loads coalesce);
+//      blocks [nA, ..): dipole structure factors S(k) = sum_s (k.mu_s) P[s][k], one thread
+//                       per k over a chunk of sites, merged with FP64 atomics;
+//   B  one warp per polarisable site: reciprocal field sum_k k g(k, s) (lanes over k), the
+//      update mu' = alpha (E_real + E_k + E0) in place, the |mu - mu'|^2 and energy sums;
+//      the last block to finish (atomic ticket) closes the iteration: it records the
+//      iteration count, change and energy, clears the accumulators and S(k) for the next
+//      iteration and, inside the graph, sets the WHILE node's condition.
+#include "ccp_device.cuh"
+
+using namespace ccpd;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kSumSites = 32;     // polarisable sites per structure-factor block
+constexpr int kGatherSites = 4;  // polarisable sites per gather/update block
+
+// exp(i k.r) from the per-axis phase tables tab[axis][l][site], in the same product order as
+// the tiled reciprocal-space kernels (ewald.f90:960-1010).
+__device__ __forceinline__ double2 phase_at(const double2 *__restrict__ tab, size_t N, int k1,
+                                            size_t t, int l, int m, int n) {
+  const double2 el = tab[(size_t)(0 * k1 + l) * N + t];
+  const double2 em = tab[(size_t)(1 * k1 + (m < 0 ? -m : m)) * N + t];
+  const double2 en = tab[(size_t)(2 * k1 + (n < 0 ? -n : n)) * N + t];
+  double clm, slm;
+  if (m >= 0) {
+    clm = el.x * em.x - el.y * em.y;
+    slm = el.y * em.x + em.y * el.x;
+  } else {
+    clm = el.x * em.x + el.y * em.y;
+    slm = el.y * em.x - em.y * el.x;
+  }
+  double c, s;
+  if (n >= 0) {
+    c = clm * en.x - slm * en.y;
+    s = slm * en.x + clm * en.y;
+  } else {
+    c = clm * en.x + slm * en.y;
+    s = slm * en.x - clm * en.y;
+  }
+  return make_double2(c, s);
+}
+
+__global__ void k_phase_matrix(const KVec *__restrict__ kv, int nk, const double2 *__restrict__ tab,
+                               int nm, SiteSets S, int k1, double2 *P) {
+  const size_t total = (size_t)nm * S.np * nk;
+  const size_t N = (size_t)nm * S.na;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const size_t s = t / nk;
+    const int k = (int)(t - s * nk);
+    const int i = (int)(s / S.np), p = (int)(s % S.np);
+    const KVec K = kv[k];
+    P[t] = phase_at(tab, N, k1, (size_t)i * S.na + S.a_of_p[p], K.l, K.m, K.n);
+  }
+}
+
+// T.mu of polarisable site w = (i, p): entries T4/TB[i][p][n][q] for the neighbours n of i and
+// the polarisable sites q of each, plus the intramolecular entries S4/SB[i][p][q].  Called by
+// whole warps; the sum is returned to every lane.
+__device__ __forceinline__ void tmu_warp(int w, int lane, const int *__restrict__ nbr,
+                                         const int *__restrict__ ncnt, int cap, int np,
+                                         const double4 *__restrict__ T4,
+                                         const double *__restrict__ TB,
+                                         const double4 *__restrict__ S4,
+                                         const double *__restrict__ SB,
+                                         const double *__restrict__ mu, double &ex, double &ey,
+                                         double &ez) {
+  const int i = w / np;
+  const int cnt = ncnt[i];
+  const size_t base = (size_t)w * cap * np;
+  ex = ey = ez = 0.0;
+  const int n_ent = cnt * np;
+#pragma unroll 4
+  for (int e = lane; e < n_ent; e += 32) {
+    const int n = e / np, q = e - n * np;
+    const int j = nbr[(size_t)i * cap + n];
+    const double4 t = T4[base + e];
+    const double b = TB[base + e];
+    const double *m = mu + ((size_t)j * np + q) * 3;
+    const double mx = m[0], my = m[1], mz = m[2];
+    const double dm = t.w * (t.x * mx + t.y * my + t.z * mz);
+    ex += dm * t.x - b * mx;
+    ey += dm * t.y - b * my;
+    ez += dm * t.z - b * mz;
+  }
+  if (lane < np) {
+    const size_t o = (size_t)w * np + lane;
+    const double4 t = S4[o];
+    const double b = SB[o];
+    const double *m = mu + ((size_t)i * np + lane) * 3;
+    const double mx = m[0], my = m[1], mz = m[2];
+    const double dm = t.w * (t.x * mx + t.y * my + t.z * mz);
+    ex += dm * t.x - b * mx;
+    ey += dm * t.y - b * my;
+    ez += dm * t.z - b * mz;
+  }
+  ex = warp_sum(ex);
+  ey = warp_sum(ey);
+  ez = warp_sum(ez);
+}
+
+// One warp per polarisable site (the fallback path's real-space part).
+__global__ void __launch_bounds__(kThreads)
+    k_tmu(const int *__restrict__ nbr, const int *__restrict__ ncnt, int cap, int nw, int np,
+          const double4 *__restrict__ T4, const double *__restrict__ TB,
+          const double4 *__restrict__ S4, const double *__restrict__ SB,
+          const double *__restrict__ mu, double *eim) {
+  const int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= nw) return;
+  double ex, ey, ez;
+  tmu_warp(w, lane, nbr, ncnt, cap, np, T4, TB, S4, SB, mu, ex, ey, ez);
+  if (lane == 0) {
+    eim[(size_t)w * 3 + 0] = ex;
+    eim[(size_t)w * 3 + 1] = ey;
+    eim[(size_t)w * 3 + 2] = ez;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_iter_a(IterArgs A) {
+  const int nA = (A.nw + kWarps - 1) / kWarps;
+  if ((int)blockIdx.x < nA) {
+    const int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (w >= A.nw) return;
+    double ex, ey, ez;
+    tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, A.mu, ex, ey, ez);
+    if (lane == 0) {
+      A.eim[(size_t)w * 3 + 0] = ex;
+      A.eim[(size_t)w * 3 + 1] = ey;
+      A.eim[(size_t)w * 3 + 2] = ez;
+    }
+    return;
+  }
+  // structure factors: block b covers k-vectors [kt*256, kt*256+256) and sites of chunk sc
+  __shared__ double smu[kSumSites * 3];
+  const int b = blockIdx.x - nA;
+  const int nkt = (A.nk + kThreads - 1) / kThreads;
+  const int kt = b % nkt, sc = b / nkt;
+  const int s0 = sc * kSumSites, cnt = min(kSumSites, A.nw - s0);
+  for (int u = threadIdx.x; u < cnt * 3; u += kThreads) smu[u] = A.mu[(size_t)s0 * 3 + u];
+  __syncthreads();
+  const int k = kt * kThreads + threadIdx.x;
+  if (k >= A.nk) return;
+  const KVec K = A.kv[k];
+  double a0 = 0.0, a1 = 0.0;
+  const double2 *Pk = A.P + (size_t)s0 * A.nk + k;
+#pragma unroll 4
+  for (int s = 0; s < cnt; s++) {
+    const double2 ph = Pk[(size_t)s * A.nk];
+    const double dk = K.rl * smu[3 * s] + K.rm * smu[3 * s + 1] + K.rn * smu[3 * s + 2];
+    a0 += dk * ph.x;
+    a1 += dk * ph.y;
+  }
+  atomicAdd(&A.sk[(size_t)k * 4], a0);
+  atomicAdd(&A.sk[(size_t)k * 4 + 1], a1);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_iter_b(IterArgs A) {
+  // kGatherSites polarisable sites per block; the 8 warps split the k-vectors, so every
+  // k-vector's weights are loaded once per block and reused for all its sites
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w0 = blockIdx.x * kGatherSites;
+  const int ns_blk = min(kGatherSites, A.nw - w0);
+  double acc[kGatherSites][3];
+#pragma unroll
+  for (int g = 0; g < kGatherSites; g++) acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
+  const double2 *P0 = A.P + (size_t)w0 * A.nk;
+#pragma unroll 2
+  for (int k = threadIdx.x; k < A.nk; k += kThreads) {
+    const KVec K = A.kv[k];
+    // kspace_efield_idm gather (nb_induction_model.f90:2560-2600): g = -4 a_k (c S_re + s S_im)
+    const double f0 = -4.0 * K.ak * A.sk[(size_t)k * 4];
+    const double f1 = -4.0 * K.ak * A.sk[(size_t)k * 4 + 1];
+#pragma unroll
+    for (int g = 0; g < kGatherSites; g++) {
+      if (g < ns_blk) {
+        const double2 ph = P0[(size_t)g * A.nk + k];
+        const double t = ph.x * f0 + ph.y * f1;
+        acc[g][0] += K.rl * t;
+        acc[g][1] += K.rm * t;
+        acc[g][2] += K.rn * t;
+      }
+    }
+  }
+  __shared__ double part[kWarps][kGatherSites * 3];
+#pragma unroll
+  for (int g = 0; g < kGatherSites; g++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const double v = warp_sum(acc[g][c]);
+      if (lane == 0) part[wid][g * 3 + c] = v;
+    }
+  __syncthreads();
+  double ch = 0.0, en = 0.0;
+  if (threadIdx.x < ns_blk) {
+    // Jacobi update (nb_induction_model.f90:1317-1359), as k_dip_update
+    const int g = threadIdx.x, w = w0 + g;
+    double ek[3] = {0.0, 0.0, 0.0};
+    for (int u = 0; u < kWarps; u++)
+      for (int c = 0; c < 3; c++) ek[c] += part[u][g * 3 + c];
+    const double polr = A.S.apol[w % A.np];
+    double Et[3], E0[3];
+    for (int c = 0; c < 3; c++) {
+      const size_t o = (size_t)w * 3 + c;
+      E0[c] = A.e0[o];
+      Et[c] = (A.eim[o] + ek[c]) + E0[c];
+      const double m = polr * Et[c];
+      const double d = A.mu[o] - m;
+      ch += d * d;
+      A.mu[o] = m;
+    }
+    en = -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
+  }
+  ch = warp_sum(ch);  // the updating threads are all in warp 0
+  en = warp_sum(en);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    atomicAdd(&A.scal[S_IND_CHANGE], ch);
+    atomicAdd(&A.scal[S_IND_ENERGY], en);
+    __threadfence();
+    last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  // every other block has added its sums and finished reading S(k)
+  __threadfence();
+  for (int u = threadIdx.x; u < A.nk * 4; u += kThreads) A.sk[u] = 0.0;
+  if (threadIdx.x == 0) {
+    const double chg = atomicAdd(&A.scal[S_IND_CHANGE], 0.0);
+    const double ene = atomicAdd(&A.scal[S_IND_ENERGY], 0.0);
+    const int it = (int)A.state[0] + 1;
+    A.state[0] = (double)it;
+    A.state[1] = chg;
+    A.state[2] = ene;
+    A.scal[S_IND_CHANGE] = 0.0;
+    A.scal[S_IND_ENERGY] = 0.0;
+    *A.ticket = 0u;
+    if (A.use_graph) cudaGraphSetConditional(A.handle, (chg > A.thr && it < A.maxit) ? 1u : 0u);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_phase_matrix(const KVec *kv, int nk, const double2 *tab, int nm, SiteSets S,
+                                int kl, int km, int kn, double2 *P, cudaStream_t st) {
+  int k1 = kl > km ? kl : km;
+  k1 = (k1 > kn ? k1 : kn) + 1;
+  if (k1 < 2) k1 = 2;
+  const size_t total = (size_t)nm * S.np * nk;
+  if (total == 0) return cudaSuccess;
+  size_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_phase_matrix<<<(unsigned)blocks, 256, 0, st>>>(kv, nk, tab, nm, S, k1, P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np, const double4 *T4,
+                       const double *TB, const double4 *S4, const double *SB, const double *mu,
+                       double *eim, cudaStream_t st) {
+  const int nw = nm * np;
+  k_tmu<<<(nw + kWarps - 1) / kWarps, kThreads, 0, st>>>(nbr, ncnt, cap, nw, np, T4, TB, S4, SB,
+                                                         mu, eim);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st) {
+  const int nA = (A.nw + kWarps - 1) / kWarps;
+  const int nkt = (A.nk + kThreads - 1) / kThreads;
+  const int nsc = (A.nw + kSumSites - 1) / kSumSites;
+  k_iter_a<<<nA + nkt * nsc, kThreads, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
+  k_iter_b<<<(A.nw + kGatherSites - 1) / kGatherSites, kThreads, 0, st>>>(A);
+  return cudaGetLastError();
+}

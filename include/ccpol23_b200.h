@@ -198,11 +198,26 @@ int ccp_context_last_launches(const ccp_context *ctx, int *launches);
 /* When on, every evaluation records CUDA events on the launching stream between its
    phases; ccp_context_phase_ms then returns the durations (ms) of the last evaluation:
    [0] input packing + neighbour list, [1] Ewald real space + static field (real) +
-   intramolecular terms, [2] Ewald reciprocal space, [3] induction (static reciprocal
-   field, dipole iteration, forces), [4] FS2, [5] FS3 triple list, [6] FS3 kernel. */
-#define CCP_NPHASE 7
+   intramolecular terms, [2] Ewald reciprocal space, [3] induction set-up (static reciprocal
+   field, dipole tensors, phase matrix), [4] dipole iteration, [5] induction forces,
+   [6] FS2, [7] FS3 triple list, [8] FS3 kernel. */
+#define CCP_NPHASE 9
 int ccp_context_set_timing(ccp_context *ctx, int on);
 int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
+
+/* Execution options of the induced-dipole solve (results do not depend on them beyond
+   round-off):
+     "graph_loop"    1 (default): the Jacobi loop runs as one CUDA graph with a conditional
+                     WHILE node, no host round trip per iteration; 0: the host launches each
+                     iteration and reads the convergence state (profilers that cannot see
+                     kernels inside conditional graphs need this);
+     "phase_matrix"  1 (default): the per-(polarisable site, k-vector) phases are tabulated
+                     once per evaluation when the table is at most 64 MiB; 0: never (the
+                     tiled on-the-fly reciprocal kernels run every iteration).
+   ccp_context_get_option also reports "phase_matrix_active" (whether the last evaluation
+   used the table). */
+int ccp_context_set_option(ccp_context *ctx, const char *name, int value);
+int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value);
 
 /* Measured peak of the FP64 (precision CCP_FP64) or FP32 (CCP_MIXED) fused multiply-add
    pipe of `device`, in TFLOP/s (2 flops per FMA), from a register-resident FMA chain. */
