@@ -217,41 +217,44 @@ __device__ __forceinline__ double t_rcp<double>(double v) { return 1.0 / v; }
 template <>
 __device__ __forceinline__ float t_rcp<float>(float v) { return __frcp_rn(v); }
 
-// One gradient pass of family FAM for the 2x2 output tile (r0, r0+1) x (c0, c0+1):
-//   FAM 0: outputs (is, js), sum over ks: X = uu[ik][is][ks], Y = uu[jk][js][ks]
-//   FAM 1: outputs (is, ks), sum over js: X = uu[ij][is][js], Y = uu[jk][js][ks]
-//   FAM 2: outputs (js, ks), sum over is: X = uu[ij][is][js], Y = uu[ik][is][ks]
+// One gradient pass for the 2x2 output tile (r0, r0+1) x (c0, c0+1), generic over the three
+// pair families (one code path keeps the instruction footprint small):
+//   fam 0: outputs (is, js), sum over ks: X = uu[ik][is][ks], Y = uu[jk][js][ks]
+//   fam 1: outputs (is, ks), sum over js: X = uu[ij][is][js], Y = uu[jk][js][ks]
+//   fam 2: outputs (js, ks), sum over is: X = uu[ij][is][js], Y = uu[ik][is][ks]
 // X carries the powers of one distance, Y of another; the output pair carries the third.
-// Per type block of the summed site, M_u (u = 2x + y for X_x Y_y) is contracted with the
-// type triple's coefficients: q0 with the power-0 and q1 with the power-1 coefficient of the
-// output distance, so that P = q0 + d q1 and dP/dd = q1.
-template <int FAM>
-struct PassIdx;
-template <>
-struct PassIdx<0> {  // coefficient index (ti, tj, tk) = (row, col, sum)
-  static constexpr int mr = kCi, mc = kCj, mb = kCk;
-  static constexpr unsigned pa = 0x6240, pb = 0x7351;  // 4-bit fields: u -> power index
-};
-template <>
-struct PassIdx<1> {  // (row, sum, col)
-  static constexpr int mr = kCi, mc = kCk, mb = kCj;
-  static constexpr unsigned pa = 0x5140, pb = 0x7362;  // 4-bit fields: u -> power index
-};
-template <>
-struct PassIdx<2> {  // (sum, row, col)
-  static constexpr int mr = kCj, mc = kCk, mb = kCi;
-  static constexpr unsigned pa = 0x3120, pb = 0x7564;  // 4-bit fields: u -> power index
+// Offsets are in table elements of uu (physical rows/columns, see sp()).  Per type block of
+// the summed site, M_u (u = 2x + y for X_x Y_y) is contracted with the type triple's
+// coefficients: q0 with c[pa[u]] (power 0 of the output distance) and q1 with c[pb[u]], so
+// that P = q0 + d q1 and dP/dd = q1.  Coefficient offsets are in doubles of the padded table.
+struct PassCfg {
+  int xb, xr, xs, yb, yr, ys, mr, mc, mb;
+  int pa[4], pb[4];
 };
 
-template <typename T, int FAM>
-__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double2 *__restrict__ C,
-                                         int r0, int c0, T q0[4], T q1[4]) {
+__device__ __forceinline__ PassCfg pass_cfg(int fam) {
+  constexpr int F = kP * kRS;
+  PassCfg c;
+  if (fam == 0) {  // coefficient (ti, tj, tk) = (row, col, sum)
+    c = {1 * F, kRS, 1, 2 * F, kRS, 1, 2 * kCi, 2 * kCj, 2 * kCk, {0, 4, 2, 6}, {1, 5, 3, 7}};
+  } else if (fam == 1) {  // (row, sum, col)
+    c = {0, kRS, 1, 2 * F, 1, kRS, 2 * kCi, 2 * kCk, 2 * kCj, {0, 4, 1, 5}, {2, 6, 3, 7}};
+  } else {  // (sum, row, col)
+    c = {0, 1, kRS, 1 * F, 1, kRS, 2 * kCj, 2 * kCk, 2 * kCi, {0, 2, 1, 3}, {4, 6, 5, 7}};
+  }
+  return c;
+}
+
+template <typename T>
+__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__restrict__ C,
+                                         const PassCfg &g, int r0, int c0, T q0[4], T q1[4]) {
   using V2 = typename Vec2<T>::type;
-  using I = PassIdx<FAM>;
+  const V2 *U = &S.uu[0][0][0];
   const int tr = kPType[r0], tc = kPType[c0];
-  const double2 *cbase = C + tr * I::mr + tc * I::mc;
+  const double *cbase = C + tr * g.mr + tc * g.mc;
   // physical rows/columns of the tile (r0, c0 even): sp(r0) = r0/2, sp(r0+1) = 9 + r0/2
-  const int ra = r0 >> 1, rb = ra + 9, ca_ = c0 >> 1, cb_ = ca_ + 9;
+  const V2 *X0 = U + g.xb + (r0 >> 1) * g.xr, *X1 = X0 + 9 * g.xr;
+  const V2 *Y0 = U + g.yb + (c0 >> 1) * g.yr, *Y1 = Y0 + 9 * g.yr;
 #pragma unroll
   for (int o = 0; o < 4; o++) q0[o] = q1[o] = (T)0;
   constexpr int kStart[7] = {0, 2, 4, 6, 10, 14, 18};
@@ -265,23 +268,8 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double2 *__r
 #pragma unroll
     for (int c = kStart[tb]; c < kStart[tb + 1]; c++) {
       const int pc = sp(c);
-      V2 X[2], Y[2];
-      if (FAM == 0) {
-        X[0] = S.uu[1][ra][pc];
-        X[1] = S.uu[1][rb][pc];
-        Y[0] = S.uu[2][ca_][pc];
-        Y[1] = S.uu[2][cb_][pc];
-      } else if (FAM == 1) {
-        X[0] = S.uu[0][ra][pc];
-        X[1] = S.uu[0][rb][pc];
-        Y[0] = S.uu[2][pc][ca_];
-        Y[1] = S.uu[2][pc][cb_];
-      } else {
-        X[0] = S.uu[0][pc][ra];
-        X[1] = S.uu[0][pc][rb];
-        Y[0] = S.uu[1][pc][ca_];
-        Y[1] = S.uu[1][pc][cb_];
-      }
+      const V2 X[2] = {X0[pc * g.xs], X1[pc * g.xs]};
+      const V2 Y[2] = {Y0[pc * g.ys], Y1[pc * g.ys]};
 #pragma unroll
       for (int rr = 0; rr < 2; rr++)
 #pragma unroll
@@ -293,14 +281,12 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double2 *__r
           M[o][3] += X[rr].y * Y[cc].y;
         }
     }
-    const double2 *cp = cbase + tb * I::mb;
-    const double2 c01 = cp[0], c23 = cp[1], c45 = cp[2], c67 = cp[3];
-    const double cw[8] = {c01.x, c01.y, c23.x, c23.y, c45.x, c45.y, c67.x, c67.y};
+    const double *cp = cbase + tb * g.mb;
     T ca[4], cb[4];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
-      ca[u] = (T)cw[(I::pa >> (4 * u)) & 15u];
-      cb[u] = (T)cw[(I::pb >> (4 * u)) & 15u];
+      ca[u] = (T)cp[g.pa[u]];
+      cb[u] = (T)cp[g.pb[u]];
     }
 #pragma unroll
     for (int o = 0; o < 4; o++) {
@@ -319,7 +305,7 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
   if (tid < kPairs) {
     const int a = tid / kNs3, b = tid % kNs3;
     const T bb = (T)S.bgr[v][0][tid], gg = (T)S.bgr[v][1][tid], r0 = (T)S.bgr[v][2][tid];
-#pragma unroll
+#pragma unroll 1
     for (int p = 0; p < 3; p++) {
       const int m1 = p == 2 ? 1 : 0, m2 = p == 0 ? 1 : 2;
       const double vx = S.rec.cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
@@ -343,13 +329,9 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
   const int fam = tid / kPassThreads, lt = tid % kPassThreads;
   if (fam < 3 && lt < kTile * kTile) {
     const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
+    const PassCfg g = pass_cfg(fam);
     T q0[4], q1[4];
-    if (fam == 0)
-      fs3_pass<T, 0>(S, S.coef[v], r0, c0, q0, q1);
-    else if (fam == 1)
-      fs3_pass<T, 1>(S, S.coef[v], r0, c0, q0, q1);
-    else
-      fs3_pass<T, 2>(S, S.coef[v], r0, c0, q0, q1);
+    fs3_pass<T>(S, reinterpret_cast<const double *>(S.coef[v]), g, r0, c0, q0, q1);
 #pragma unroll
     for (int o = 0; o < 4; o++) {
       const int r = sp(r0 + (o >> 1)), c = sp(c0 + (o & 1));
