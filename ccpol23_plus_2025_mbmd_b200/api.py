@@ -38,10 +38,11 @@ class Model:
         h = C.c_void_p()
         check(L.ccp_model_load(str(directory).encode(), C.byref(h)))
         self._h = h
+        self._free = L.ccp_model_free  # kept: module globals may be gone at interpreter exit
 
     def __del__(self):
         if getattr(self, "_h", None):
-            _lib.lib().ccp_model_free(self._h)
+            self._free(self._h)
             self._h = None
 
     @property

@@ -69,6 +69,9 @@ struct ccp_context {
   // packed
   double4 *d_com = nullptr, *d_act = nullptr, *d_comb = nullptr, *d_s17 = nullptr;
   // accumulators
+  // site forces f[3][nm*ns]; a second block of the same size takes the three-body forces
+  // when those run concurrently on side streams (the Ewald/induction kernels add to f
+  // without atomics), and is added to f after the join
   double *d_f = nullptr, *d_fc2 = nullptr, *d_fc3 = nullptr;
   double *d_scal = nullptr;
   int *d_icnt = nullptr;
@@ -120,8 +123,15 @@ struct ccp_context {
   int opt_phase = 1;  // phase matrix when it fits (1) or never (0)
   // phase timing (diagnostics)
   bool timing = false;
-  cudaEvent_t ev[CCP_NPHASE + 1] = {};
+  cudaEvent_t ev[2 * CCP_NPHASE] = {};  // start/end of each phase, on the phase's stream
+  unsigned phase_ran = 0;
   double phase_ms[CCP_NPHASE] = {0};
+  // side streams of the three-body terms (forked from the main stream after the neighbour
+  // list, joined before the scalars are read back)
+  cudaStream_t s_fs3 = nullptr, s_fs2 = nullptr, s_main = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_j3 = nullptr, ev_j2 = nullptr, ev_jm = nullptr;
+  int opt_overlap = 1;     // three-body terms concurrent with Ewald/induction
+  int opt_fs3_tpb = 8;     // FS3 triples per block when concurrent (0 = persistent grid)
 };
 
 namespace {
@@ -148,6 +158,11 @@ void free_ctx(ccp_context *c) {
   if (c->d_P) cudaFree(c->d_P);
   if (c->h_istate) cudaFreeHost(c->h_istate);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+  if (c->s_fs3) cudaStreamDestroy(c->s_fs3);
+  if (c->s_fs2) cudaStreamDestroy(c->s_fs2);
+  if (c->s_main) cudaStreamDestroy(c->s_main);
+  for (cudaEvent_t e : {c->ev_fork, c->ev_j3, c->ev_j2, c->ev_jm})
+    if (e) cudaEventDestroy(e);
   if (c->own) cudaStreamDestroy(c->own);
 }
 
@@ -416,7 +431,7 @@ int ensure_phase_matrix(ccp_context *c) {
 
 // Runs the enabled terms on inputs already in the context's device buffers
 // (x, y, z at px.., sites at pxs.. with leading dimension ld).
-int evaluate(ccp_context *c, const double *px, const double *py, const double *pz,
+int evaluate_impl(ccp_context *c, const double *px, const double *py, const double *pz,
              const double *pxs, const double *pys, const double *pzs, int ld, double box,
              unsigned mask, EvalOut &o) {
   cudaStream_t st = c->stream;
@@ -470,92 +485,125 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
   if (mask & T_FS2) rl = std::max(rl, c->rcut3);
   rl += 0.05;
 
-  auto mark = [&](int k) {
-    if (c->timing) cudaEventRecord(c->ev[k], st);
+  // phase k runs between ev[2k] and ev[2k+1], recorded on the stream it runs on
+  auto pbeg = [&](int k, cudaStream_t s) {
+    if (c->timing) {
+      cudaEventRecord(c->ev[2 * k], s);
+      c->phase_ran |= 1u << k;
+    }
   };
+  auto pend = [&](int k, cudaStream_t s) {
+    if (c->timing) cudaEventRecord(c->ev[2 * k + 1], s);
+  };
+  const bool side = c->opt_overlap && (mask & (T_FS2 | T_FS3));
+  // Ewald + induction run on a high-priority internal stream, the three-body terms on
+  // low-priority ones, so that freed SM slots go to the latency-bound induction chain first
+  cudaStream_t s3 = side ? c->s_fs3 : st, s2 = side ? c->s_fs2 : st, sm = side ? c->s_main : st;
   for (int attempt = 0; attempt < 3; attempt++) {
     c->launches = 0;
-    mark(0);
+    c->phase_ran = 0;
+    pbeg(0, st);
     LK(launch_prep(px, py, pz, pxs, pys, pzs, nm, ld, S, c->d_com, c->d_act, c->d_comb, c->d_s17,
-                   std::min(ns, kNs3), c->d_f, 3 * nm * ns, c->d_fc2, c->d_fc3, c->d_scal,
+                   std::min(ns, kNs3), c->d_f, 6 * nm * ns, c->d_fc2, c->d_fc3, c->d_scal,
                    c->d_icnt, st));
     const bool need_nbr = mask & (T_RSPACE | T_INDUCTION | T_FS2 | T_FS3);
     if (need_nbr)
       LK(launch_neighbors(c->d_com, nm, box, rl * rl, c->cap, c->d_nbr, c->d_nbrv, c->d_ncnt,
                           c->d_icnt, st));
-    mark(1);
+    pend(0, st);
+    if (side) {
+      CK(cudaEventRecord(c->ev_fork, st));
+      CK(cudaStreamWaitEvent(s3, c->ev_fork, 0));
+      CK(cudaStreamWaitEvent(s2, c->ev_fork, 0));
+      CK(cudaStreamWaitEvent(sm, c->ev_fork, 0));
+    }
+    // three-body terms first, so that on side streams they start at once
+    double *f3 = side ? c->d_f + (size_t)3 * nm * ns : c->d_f;
+    if (mask & T_FS3) {
+      pbeg(7, s3);
+      LK(launch_fs3_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F3, c->d_tri, c->tri_cap,
+                         c->d_icnt, s3));
+      pend(7, s3);
+      pbeg(8, s3);
+      LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
+                    nm, ns, f3, c->d_fc3, c->d_scal, c->nsm, side ? c->opt_fs3_tpb : 0, s3));
+      pend(8, s3);
+    }
+    if (mask & T_FS2) {
+      pbeg(6, s2);
+      LK(launch_fs2_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F2, c->d_pairs, c->pair_cap,
+                         c->d_icnt, s2));
+      LK(launch_fs2(c->precision, c->d_pairs, c->d_icnt, c->pair_cap, c->d_comb, c->d_s17, c->d_nbr,
+                    c->d_ncnt, c->cap, F2, nm, ns, f3, c->d_fc2, c->d_scal, s2));
+      pend(6, s2);
+    }
+    pbeg(1, sm);
     if (mask & T_SELF)
       LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_f, c->d_e0slf,
-                            c->d_scal, st));
+                            c->d_scal, sm));
     if (mask & (T_RSPACE | T_INDUCTION)) {
       // the real-space kernel produces Ewald forces and the static field together; when
       // only one of the two is wanted the other output is discarded by zeroing below.
       LK(launch_pair_static(c->d_com, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt, c->cap, nm, S, P,
                             (mask & T_RSPACE) ? c->d_f : c->d_eir, c->d_e0r, c->d_e0s, c->d_scal,
-                            st));
+                            sm));
     }
-    mark(2);
+    pend(1, sm);
+    pbeg(2, sm);
     if (mask & (T_KSPACE | T_INDUCTION))
       LK(launch_ktab(c->d_com, c->d_act, nm, S, box, c->kmax[0], c->kmax[1], c->kmax[2], c->d_tab,
-                     st));
+                     sm));
     if (mask & T_KSPACE) {
       LK(launch_kspace_sums(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, st));
-      LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, st));
+                            c->d_mu, c->d_sk, sm));
+      LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sm));
       LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, st));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, sm));
     }
-    mark(3);
+    pend(2, sm);
     if (mask & T_INDUCTION) {
+      pbeg(3, sm);
       if (!(mask & T_SELF))
         LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_eir, c->d_e0slf,
-                              c->d_scal, st));
+                              c->d_scal, sm));
       LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, st));
+                            c->d_mu, c->d_sk, sm));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, st));
-      if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, st));
+                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, sm));
+      if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, sm));
       LK(launch_dip_tensor(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt,
-                           c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, st));
+                           c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, sm));
       LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
-                             st));
+                             sm));
       if (c->use_P)
         LK(launch_phase_matrix(c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                               c->d_P, st));
-      mark(4);
+                               c->d_P, sm));
+      pend(3, sm);
+      pbeg(4, sm);
       {
-        int r = run_dipole_loop(c, st);
+        int r = run_dipole_loop(c, sm);
         if (r) return r;
       }
-      mark(5);
+      pend(4, sm);
+      pbeg(5, sm);
       LK(launch_pair_indforce(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
-                              c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_f, c->d_scal, st));
+                              c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_f, c->d_scal, sm));
       LK(launch_kspace_sums(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, st));
-      LK(launch_kspace_energy(3, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, st));
+                            c->d_mu, c->d_sk, sm));
+      LK(launch_kspace_energy(3, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sm));
       LK(launch_kspace_gather(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, st));
-    } else {
-      mark(4);
-      mark(5);
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, sm));
+      pend(5, sm);
     }
-    mark(6);
-    if (mask & T_FS2) {
-      LK(launch_fs2_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F2, c->d_pairs, c->pair_cap,
-                         c->d_icnt, st));
-      LK(launch_fs2(c->precision, c->d_pairs, c->d_icnt, c->pair_cap, c->d_comb, c->d_s17, c->d_nbr,
-                    c->d_ncnt, c->cap, F2, nm, ns, c->d_f, c->d_fc2, c->d_scal, st));
+    if (side) {
+      CK(cudaEventRecord(c->ev_j3, s3));
+      CK(cudaEventRecord(c->ev_j2, s2));
+      CK(cudaEventRecord(c->ev_jm, sm));
+      CK(cudaStreamWaitEvent(st, c->ev_j3, 0));
+      CK(cudaStreamWaitEvent(st, c->ev_j2, 0));
+      CK(cudaStreamWaitEvent(st, c->ev_jm, 0));
+      LK(launch_add(3 * nm * ns, f3, c->d_f, st));
     }
-    mark(7);
-    if (mask & T_FS3)
-      LK(launch_fs3_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F3, c->d_tri, c->tri_cap,
-                         c->d_icnt, st));
-    mark(8);
-    if (mask & T_FS3) {
-      LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
-                    nm, ns, c->d_f, c->d_fc3, c->d_scal, c->nsm, st));
-    }
-    mark(9);
     CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c->h_icnt, c->d_icnt, sizeof(int) * C_COUNT, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -592,7 +640,7 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
     if (c->timing)
       for (int k = 0; k < CCP_NPHASE; k++) {
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->ev[k], c->ev[k + 1]);
+        if (c->phase_ran & (1u << k)) cudaEventElapsedTime(&ms, c->ev[2 * k], c->ev[2 * k + 1]);
         c->phase_ms[k] = ms;
       }
     const double *h = c->h_scal;
@@ -614,6 +662,18 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
   }
   set_error("internal list capacity kept overflowing");
   return CCP_ERR_CAPACITY;
+}
+
+int evaluate(ccp_context *c, const double *px, const double *py, const double *pz,
+             const double *pxs, const double *pys, const double *pzs, int ld, double box,
+             unsigned mask, EvalOut &o) {
+  const int r = evaluate_impl(c, px, py, pz, pxs, pys, pzs, ld, box, mask, o);
+  if (r) {  // no side-stream work of a failed evaluation may outlive it
+    cudaStreamSynchronize(c->s_fs3);
+    cudaStreamSynchronize(c->s_fs2);
+    cudaStreamSynchronize(c->s_main);
+  }
+  return r;
 }
 
 int check_args(ccp_context *c, const void *const *ptrs, int n, int ld) {
@@ -859,8 +919,18 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
     return CCP_ERR_CUDA;
   };
   if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess) return fail("stream");
-  if (cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess)
+  int prio_lo = 0, prio_hi = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+  if (cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->s_fs3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->s_fs2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->s_main, cudaStreamNonBlocking, prio_hi) != cudaSuccess)
     return fail("stream");
+  if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_j3, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_j2, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_jm, cudaEventDisableTiming) != cudaSuccess)
+    return fail("event");
   c->stream = c->own;
   if (cudaMalloc(&c->d_istate, 3 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->d_ticket, sizeof(unsigned)) != cudaSuccess ||
@@ -872,7 +942,7 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
             dalloc(&c->d_z, n) == cudaSuccess && dalloc(&c->d_com, n) == cudaSuccess &&
             dalloc(&c->d_comb, n) == cudaSuccess &&
             dalloc(&c->d_act, n * std::max(S.na, 1)) == cudaSuccess &&
-            dalloc(&c->d_s17, n * kNs3) == cudaSuccess && dalloc(&c->d_f, 3 * nsi) == cudaSuccess &&
+            dalloc(&c->d_s17, n * kNs3) == cudaSuccess && dalloc(&c->d_f, 6 * nsi) == cudaSuccess &&
             dalloc(&c->d_fc2, 3 * n) == cudaSuccess && dalloc(&c->d_fc3, 3 * n) == cudaSuccess &&
             dalloc(&c->d_scal, (size_t)S_COUNT) == cudaSuccess &&
             dalloc(&c->d_icnt, (size_t)C_COUNT) == cudaSuccess &&
@@ -969,6 +1039,14 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_graph = value != 0;
   } else if (n == "phase_matrix") {
     ctx->opt_phase = value != 0;
+  } else if (n == "overlap") {
+    ctx->opt_overlap = value != 0;
+  } else if (n == "fs3_triples_per_block") {
+    if (value < 0 || value > 4096) {
+      set_error("ccp_context_set_option: fs3_triples_per_block must be 0..4096");
+      return CCP_ERR_BAD_INPUT;
+    }
+    ctx->opt_fs3_tpb = value;
   } else {
     set_error("ccp_context_set_option: unknown option " + n);
     return CCP_ERR_BAD_INPUT;
@@ -985,6 +1063,10 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_phase;
   } else if (n == "phase_matrix_active") {
     *value = ctx->use_P ? 1 : 0;
+  } else if (n == "overlap") {
+    *value = ctx->opt_overlap;
+  } else if (n == "fs3_triples_per_block") {
+    *value = ctx->opt_fs3_tpb;
   } else {
     set_error("ccp_context_get_option: unknown option " + n);
     return CCP_ERR_BAD_INPUT;

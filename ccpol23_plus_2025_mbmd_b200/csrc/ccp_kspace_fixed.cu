@@ -23,7 +23,14 @@ namespace {
 constexpr size_t kFixedScratchBytes = size_t(16) << 20;  // 16 MiB per device
 constexpr int kMaxDevices = 64;
 
-__device__ __align__(256) unsigned char g_kspace_scratch[kFixedScratchBytes];
+}  // namespace
+
+// The scratch itself: one array per device that loads this library, kept until exit.  Host
+// code must not pass its name to a kernel (that is a host-side stand-in); the device address
+// comes from cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char g_kspace_scratch[kFixedScratchBytes];
+
+namespace {
 
 std::mutex g_addr_mu;
 unsigned char *g_addr[kMaxDevices] = {};

@@ -360,6 +360,7 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
   const int tid = threadIdx.x;
+  if ((int)blockIdx.x >= min(icnt[C_NTRI_FS3], tri_cap)) return;  // no triple for this block
   for (int t = tid; t < 2 * kCoef2; t += kFs3Block) (&S.coef[0][0])[t] = make_double2(0.0, 0.0);
   __syncthreads();
   for (int t = tid; t < 2 * kCoef / 2; t += kFs3Block) {
@@ -511,6 +512,17 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
 
 size_t fs3_record_bytes() { return sizeof(Fs3Rec); }
 
+namespace {
+// Persistent grid (one wave of resident blocks) when triples_per_block is 0; otherwise
+// enough short blocks for the list's capacity, about triples_per_block triples each, so
+// that blocks retire often and other streams' kernels can take their slots.
+int fs3_grid(int resident, int tri_cap, int triples_per_block) {
+  if (triples_per_block <= 0) return resident;
+  const int g = (tri_cap + triples_per_block - 1) / triples_per_block;
+  return g < 1 ? 1 : g;
+}
+}  // namespace
+
 cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
                             int nm, Fs3Params P, void *rec, int tri_cap, int *icnt,
                             cudaStream_t st) {
@@ -527,7 +539,8 @@ cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt
 
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
-                       double *f, double *fc3, double *scal, int nsm, cudaStream_t st) {
+                       double *f, double *fc3, double *scal, int nsm, int triples_per_block,
+                       cudaStream_t st) {
   cudaError_t e;
   const Fs3Rec *R = static_cast<const Fs3Rec *>(rec);
   int per_sm = 0;
@@ -537,7 +550,7 @@ cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_
     if (e != cudaSuccess) return e;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<double>, kFs3Block, smem);
     if (per_sm < 1) per_sm = 1;
-    k_fs3<double><<<nsm * per_sm, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns,
+    k_fs3<double><<<fs3_grid(nsm * per_sm, tri_cap, triples_per_block), kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns,
                                                          f, fc3, scal);
   } else {
     const size_t smem = sizeof(Fs3Smem<float>);
@@ -545,7 +558,7 @@ cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_
     if (e != cudaSuccess) return e;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<float>, kFs3Block, smem);
     if (per_sm < 1) per_sm = 1;
-    k_fs3<float><<<nsm * per_sm, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f,
+    k_fs3<float><<<fs3_grid(nsm * per_sm, tri_cap, triples_per_block), kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f,
                                                         fc3, scal);
   }
   return cudaGetLastError();

@@ -516,6 +516,21 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 }  // namespace
 
 // ------------------------------------------------------------------ launchers
+namespace {
+__global__ void k_add(int n, const double *__restrict__ a, double *b) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+    b[t] += a[t];
+}
+}  // namespace
+
+cudaError_t launch_add(int n, const double *a, double *b, cudaStream_t st) {
+  int blocks = (n + 255) / 256;
+  if (blocks > 4 * 148) blocks = 4 * 148;
+  if (blocks < 1) blocks = 1;
+  k_add<<<blocks, 256, 0, st>>>(n, a, b);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_prep(const double *x, const double *y, const double *z, const double *xs,
                         const double *ys, const double *zs, int nm, int ld, SiteSets S,
                         double4 *com, double4 *act, double4 *comb, double4 *s17, int ns3,
