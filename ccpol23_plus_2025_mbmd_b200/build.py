@@ -65,12 +65,17 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> Path:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    if changed:
+    # relink whenever the library was linked from a different set of objects (a source
+    # reverted to an earlier state reuses that state's cached object without recompiling)
+    stamp = LIBDIR / ".objects"
+    listing = "\n".join(o.name for o in objs)
+    if changed or not stamp.exists() or stamp.read_text() != listing:
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static",
                "-lrt", "-ldl", "-lpthread"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+        stamp.write_text(listing)
     return LIB
 
 
