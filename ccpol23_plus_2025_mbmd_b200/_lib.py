@@ -34,7 +34,13 @@ EXPORTS = [
     "ccp_threebody_term", "ccp_hot_path", "ccp_hot_path_device", "ccp_context_last_launches",
     "ccp_context_set_timing", "ccp_context_phase_ms", "ccp_device_fma_peak",
     "ccp_kspace_ewald_fixed", "ccp_context_set_option", "ccp_context_get_option",
+    "ccp_terms_device", "ccp_context_get_fs3_params", "ccp_context_set_fs3_params",
+    "ccp_context_fs3_param_grad",
 ]
+
+# term bits of ccp_terms_device (CCP_TERM_*)
+TERM_SELF, TERM_RSPACE, TERM_KSPACE, TERM_INDUCTION, TERM_FS2, TERM_FS3 = 1, 2, 4, 8, 16, 32
+TERM_ALL = 63
 
 
 class CcpEnergies(C.Structure):
@@ -90,6 +96,10 @@ def lib():
     L.ccp_threebody_term.argtypes = [vp] + [vp] * 6 + [i, d, pd, pd] + [vp] * 9 + [pd]
     L.ccp_hot_path.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_hot_path_device.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
+    L.ccp_terms_device.argtypes = [vp, C.c_uint] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
+    L.ccp_context_get_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
+    L.ccp_context_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
+    L.ccp_context_fs3_param_grad.argtypes = [vp, vp, vp, i, vp, vp]
     L.ccp_context_set_option.argtypes = [vp, C.c_char_p, i]
     L.ccp_context_get_option.argtypes = [vp, C.c_char_p, pi]
     L.ccp_kspace_ewald_fixed.argtypes = [vp, i] + [vp] * 6 + [i, i, i, i, d, d] + [vp] * 5 + [vp]

@@ -288,6 +288,46 @@ class Context:
                                       ld, box, C.byref(e), *[ptr(a) for a in out]))
         return HotPathResult(_energies(e), *out)
 
+    def terms_device(self, terms, x, y, z, xs, ys, zs, box, fxs=None, fys=None, fzs=None,
+                     fxfs2=None, fyfs2=None, fzfs2=None, fxfs3=None, fyfs3=None, fzfs3=None,
+                     idmx=None, idmy=None, idmz=None) -> dict:
+        """The terms selected by the bit mask `terms` (_lib.TERM_*) on torch CUDA float64
+        tensors, in the layouts of hot_path_device; energies of terms not run are 0."""
+        def dp(t):
+            return None if t is None else t.data_ptr()
+        ld = xs.shape[1]
+        e = CcpEnergies()
+        check(_lib.lib().ccp_terms_device(
+            self._h, int(terms), dp(x), dp(y), dp(z), dp(xs), dp(ys), dp(zs), ld, box, C.byref(e),
+            dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
+            dp(fzfs3), dp(idmx), dp(idmy), dp(idmz)))
+        return _energies(e)
+
+    # -- FS3 parameters --------------------------------------------------------------
+    def fs3_params(self):
+        """(cs_sr, cs_lr, bgr_sr, bgr_lr): class coefficients (nclass each) and site-pair
+        (b, g, r0) as (3, 289) arrays, index is*17 + js."""
+        n = self.model.get_int("nclass")
+        cs_sr, cs_lr = np.zeros(n), np.zeros(n)
+        b_sr, b_lr = np.zeros((3, 289)), np.zeros((3, 289))
+        check(_lib.lib().ccp_context_get_fs3_params(self._h, ptr(cs_sr), ptr(cs_lr), n,
+                                                     ptr(b_sr), ptr(b_lr)))
+        return cs_sr, cs_lr, b_sr, b_lr
+
+    def set_fs3_params(self, cs_sr, cs_lr, bgr_sr, bgr_lr):
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (cs_sr, cs_lr, bgr_sr, bgr_lr)]
+        check(_lib.lib().ccp_context_set_fs3_params(self._h, ptr(a[0]), ptr(a[1]), a[0].size,
+                                                     ptr(a[2]), ptr(a[3])))
+
+    def fs3_param_grad(self):
+        """Gradient of the last evaluation's FS3 energy (kcal/mol) with respect to
+        (cs_sr, cs_lr, bgr_sr, bgr_lr); needs set_option("fs3_param_grad", 1)."""
+        n = self.model.get_int("nclass")
+        g = [np.zeros(n), np.zeros(n), np.zeros((3, 289)), np.zeros((3, 289))]
+        check(_lib.lib().ccp_context_fs3_param_grad(self._h, *[ptr(v) for v in g[:2]], n,
+                                                     *[ptr(v) for v in g[2:]]))
+        return tuple(g)
+
     def hot_path_device(self, x, y, z, xs, ys, zs, box, fxs=None, fys=None, fzs=None,
                         fxfs2=None, fyfs2=None, fzfs2=None, fxfs3=None, fyfs3=None,
                         fzfs3=None, idmx=None, idmy=None, idmz=None) -> dict:

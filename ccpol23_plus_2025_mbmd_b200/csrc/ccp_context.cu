@@ -28,6 +28,9 @@ enum TermMask : unsigned {
   T_FS2 = 16u,
   T_FS3 = 32u,
 };
+static_assert(T_SELF == CCP_TERM_SELF && T_RSPACE == CCP_TERM_RSPACE && T_KSPACE == CCP_TERM_KSPACE &&
+                  T_INDUCTION == CCP_TERM_INDUCTION && T_FS2 == CCP_TERM_FS2 && T_FS3 == CCP_TERM_FS3,
+              "term bits of the C ABI");
 
 bool cuda_ok(cudaError_t e, const char *what) {
   if (e == cudaSuccess) return true;
@@ -97,6 +100,14 @@ struct ccp_context {
   double *d_sk = nullptr;
   // FS3 tables
   double *d_coef = nullptr, *d_bgr = nullptr;
+  // FS3 parameters of this context (host copies): class coefficients, the class of every
+  // coefficient-table entry, site-pair (b, g, r0); and the parameter-gradient buffer
+  std::vector<double> cs_sr, cs_lr, bgr_host;
+  std::vector<int> class_of_type;
+  int nclass = 0;
+  double *d_gfs3 = nullptr;
+  int opt_pgrad = 0;   // accumulate dE_FS3/d(parameters) in each evaluation
+  bool pgrad_valid = false;
   int *d_types = nullptr;
   // host staging (pinned)
   double *h_scal = nullptr;
@@ -143,6 +154,7 @@ void free_ctx(ccp_context *c) {
                 c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
                 c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
+                c->d_gfs3,
                 c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
   for (void *p : dp)
     if (p) cudaFree(p);
@@ -519,6 +531,11 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     }
     // three-body terms first, so that on side streams they start at once
     double *f3 = side ? c->d_f + (size_t)3 * nm * ns : c->d_f;
+    double *gfs3 = nullptr;
+    if ((mask & T_FS3) && c->opt_pgrad) {
+      gfs3 = c->d_gfs3;
+      CK(cudaMemsetAsync(gfs3, 0, sizeof(double) * kFs3GradLen, s3));
+    }
     if (mask & T_FS3) {
       pbeg(7, s3);
       LK(launch_fs3_enum(c->d_comb, c->d_nbr, c->d_ncnt, c->cap, nm, F3, c->d_tri, c->tri_cap,
@@ -526,7 +543,8 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       pend(7, s3);
       pbeg(8, s3);
       LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
-                    nm, ns, f3, c->d_fc3, c->d_scal, c->nsm, side ? c->opt_fs3_tpb : 0, s3));
+                    nm, ns, f3, c->d_fc3, c->d_scal, c->nsm, side ? c->opt_fs3_tpb : 0, gfs3,
+                    s3));
       pend(8, s3);
     }
     if (mask & T_FS2) {
@@ -627,6 +645,7 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       if (r) return r;
       continue;
     }
+    c->pgrad_valid = gfs3 != nullptr;
     if (mask & T_INDUCTION) {
       o.iters = (int)c->h_istate[0];
       o.ind_e = c->h_istate[2];
@@ -968,6 +987,10 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
     std::vector<double> coef(2 * m->coef_sr.size());
     std::copy(m->coef_sr.begin(), m->coef_sr.end(), coef.begin());
     std::copy(m->coef_lr.begin(), m->coef_lr.end(), coef.begin() + m->coef_sr.size());
+    c->cs_sr = m->sr.cs;
+    c->cs_lr = m->lr.cs;
+    c->class_of_type = m->class_of_type;
+    c->nclass = m->nclass;
     std::vector<double> bgr(2 * 3 * 289);
     for (int q = 0; q < 289; q++) {
       bgr[0 * 289 + q] = m->sr.b[q];
@@ -977,7 +1000,9 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
       bgr[4 * 289 + q] = m->lr.g[q];
       bgr[5 * 289 + q] = m->lr.r0[q];
     }
+    c->bgr_host = bgr;
     if (dalloc(&c->d_coef, coef.size()) != cudaSuccess || dalloc(&c->d_bgr, bgr.size()) != cudaSuccess ||
+        dalloc(&c->d_gfs3, (size_t)kFs3GradLen) != cudaSuccess ||
         dalloc(&c->d_types, (size_t)kNs3) != cudaSuccess)
       return fail("FS3 tables");
     if (cudaMemcpy(c->d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
@@ -1041,6 +1066,8 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_phase = value != 0;
   } else if (n == "overlap") {
     ctx->opt_overlap = value != 0;
+  } else if (n == "fs3_param_grad") {
+    ctx->opt_pgrad = value != 0;
   } else if (n == "fs3_triples_per_block") {
     if (value < 0 || value > 4096) {
       set_error("ccp_context_set_option: fs3_triples_per_block must be 0..4096");
@@ -1065,6 +1092,8 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->use_P ? 1 : 0;
   } else if (n == "overlap") {
     *value = ctx->opt_overlap;
+  } else if (n == "fs3_param_grad") {
+    *value = ctx->opt_pgrad;
   } else if (n == "fs3_triples_per_block") {
     *value = ctx->opt_fs3_tpb;
   } else {
@@ -1228,19 +1257,25 @@ int ccp_hot_path(ccp_context *ctx, const double *x, const double *y, const doubl
   return r;
 }
 
-int ccp_hot_path_device(ccp_context *ctx, const double *x, const double *y, const double *z,
-                        const double *xs, const double *ys, const double *zs, int ld, double box,
-                        ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
+int ccp_terms_device(ccp_context *ctx, unsigned terms, const double *x, const double *y,
+                     const double *z, const double *xs, const double *ys, const double *zs,
+                     int ld, double box, ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
                         double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3,
                         double *fzfs3, double *idmx, double *idmy, double *idmz) {
   const void *p[] = {x, y, z, xs, ys, zs, e};
   int r = check_args(ctx, p, 7, ld);
   if (r) return r;
   CK(cudaSetDevice(ctx->device));
+  if (terms & ~unsigned(CCP_TERM_ALL)) {
+    set_error("ccp_terms_device: unknown term bits");
+    return CCP_ERR_BAD_INPUT;
+  }
+  const unsigned mask = terms & hot_mask(ctx);
   EvalOut o;
-  r = evaluate(ctx, x, y, z, xs, ys, zs, ld, box, hot_mask(ctx), o);
+  r = evaluate(ctx, x, y, z, xs, ys, zs, ld, box, mask, o);
   if (r) return r;
   fill_energies(ctx, o, box, e);
+  if (!(mask & T_SELF)) e->scpe = 0.0;  // the point self energy is part of that term
   cudaStream_t st = ctx->stream;
   const int n = ctx->nm * ctx->ns;
   if (fxs || fys || fzs) {
@@ -1261,6 +1296,101 @@ int ccp_hot_path_device(ccp_context *ctx, const double *x, const double *y, cons
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(st));
+  return CCP_OK;
+}
+
+int ccp_hot_path_device(ccp_context *ctx, const double *x, const double *y, const double *z,
+                        const double *xs, const double *ys, const double *zs, int ld, double box,
+                        ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
+                        double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3,
+                        double *fzfs3, double *idmx, double *idmy, double *idmz) {
+  return ccp_terms_device(ctx, CCP_TERM_ALL, x, y, z, xs, ys, zs, ld, box, e, fxs, fys, fzs, fxfs2,
+                          fyfs2, fzfs2, fxfs3, fyfs3, fzfs3, idmx, idmy, idmz);
+}
+
+int ccp_context_get_fs3_params(const ccp_context *ctx, double *cs_sr, double *cs_lr, int ncoef,
+                               double *bgr_sr, double *bgr_lr) {
+  if (!ctx) return CCP_ERR_BAD_INPUT;
+  if (!ctx->have_fs3 || ncoef != ctx->nclass) {
+    set_error("FS3 parameters: the model has no FS3 tables or ncoef differs from its " +
+              std::to_string(ctx->nclass) + " coefficients");
+    return CCP_ERR_BAD_INPUT;
+  }
+  for (int k = 0; k < ncoef; k++) {
+    if (cs_sr) cs_sr[k] = ctx->cs_sr[k];
+    if (cs_lr) cs_lr[k] = ctx->cs_lr[k];
+  }
+  for (int k = 0; k < 3 * 289; k++) {
+    if (bgr_sr) bgr_sr[k] = ctx->bgr_host[k];
+    if (bgr_lr) bgr_lr[k] = ctx->bgr_host[3 * 289 + k];
+  }
+  return CCP_OK;
+}
+
+int ccp_context_set_fs3_params(ccp_context *ctx, const double *cs_sr, const double *cs_lr,
+                               int ncoef, const double *bgr_sr, const double *bgr_lr) {
+  if (!ctx || !cs_sr || !cs_lr || !bgr_sr || !bgr_lr) return CCP_ERR_BAD_INPUT;
+  if (!ctx->have_fs3 || ncoef != ctx->nclass) {
+    set_error("FS3 parameters: the model has no FS3 tables or ncoef differs from its " +
+              std::to_string(ctx->nclass) + " coefficients");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  for (int k = 0; k < ncoef; k++) {
+    ctx->cs_sr[k] = cs_sr[k];
+    ctx->cs_lr[k] = cs_lr[k];
+  }
+  for (int k = 0; k < 3 * 289; k++) {
+    ctx->bgr_host[k] = bgr_sr[k];
+    ctx->bgr_host[3 * 289 + k] = bgr_lr[k];
+  }
+  const size_t nt = ctx->class_of_type.size();
+  std::vector<double> coef(2 * nt);
+  for (size_t t = 0; t < nt; t++) {
+    coef[t] = ctx->cs_sr[ctx->class_of_type[t]];
+    coef[nt + t] = ctx->cs_lr[ctx->class_of_type[t]];
+  }
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->d_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_bgr, ctx->bgr_host.data(), ctx->bgr_host.size() * sizeof(double),
+                     cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
+  ctx->pgrad_valid = false;
+  return CCP_OK;
+}
+
+int ccp_context_fs3_param_grad(ccp_context *ctx, double *dcs_sr, double *dcs_lr, int ncoef,
+                               double *dbgr_sr, double *dbgr_lr) {
+  if (!ctx) return CCP_ERR_BAD_INPUT;
+  if (!ctx->have_fs3 || ncoef != ctx->nclass) {
+    set_error("FS3 parameter gradient: the model has no FS3 tables or ncoef differs from its " +
+              std::to_string(ctx->nclass) + " coefficients");
+    return CCP_ERR_BAD_INPUT;
+  }
+  if (!ctx->pgrad_valid) {
+    set_error("FS3 parameter gradient: set the fs3_param_grad option and evaluate FS3 first");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  std::vector<double> g(kFs3GradLen);
+  CK(cudaMemcpyAsync(g.data(), ctx->d_gfs3, sizeof(double) * kFs3GradLen, cudaMemcpyDeviceToHost,
+                     ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  const size_t nt = ctx->class_of_type.size();
+  std::vector<double> gs(ncoef, 0.0), gl(ncoef, 0.0);
+  for (size_t t = 0; t < nt; t++) {
+    gs[ctx->class_of_type[t]] += g[t];
+    gl[ctx->class_of_type[t]] += g[nt + t];
+  }
+  for (int k = 0; k < ncoef; k++) {
+    if (dcs_sr) dcs_sr[k] = gs[k] * kH2kcal;
+    if (dcs_lr) dcs_lr[k] = gl[k] * kH2kcal;
+  }
+  const double *gb = g.data() + 2 * nt;
+  for (int k = 0; k < 3 * 289; k++) {
+    if (dbgr_sr) dbgr_sr[k] = gb[k] * kH2kcal;
+    if (dbgr_lr) dbgr_lr[k] = gb[3 * 289 + k] * kH2kcal;
+  }
   return CCP_OK;
 }
 

@@ -150,6 +150,9 @@ struct IterArgs {
 
 // ------------------------------------------------------------------ launchers
 // All launchers enqueue on `st` and return cudaGetLastError().
+// FS3 parameter-gradient buffer (launch_fs3's gfs3): [2][216][8] coefficient-table entries,
+// then [2][3][289] (b, g, r0) of each site pair, SR then LR; energy-sum units (hartree).
+constexpr int kFs3GradLen = 2 * 216 * 8 + 2 * 3 * 289;
 // b[0..n) += a[0..n)
 cudaError_t launch_add(int n, const double *a, double *b, cudaStream_t st);
 cudaError_t launch_prep(const double *x, const double *y, const double *z, const double *xs,
@@ -225,7 +228,8 @@ cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt
                             cudaStream_t st);
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
-                       double *f, double *fc3, double *scal, int nsm, int triples_per_block, cudaStream_t st);
+                       double *f, double *fc3, double *scal, int nsm, int triples_per_block, double *gfs3,
+                       cudaStream_t st);
 cudaError_t launch_fs2_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
                             int nm, Fs2Params P, int2 *pairs, int pair_cap, int *icnt,
                             cudaStream_t st);

@@ -62,4 +62,5 @@ struct ccp_model {
   int fs3_type[ccp::kNs3];     // 0-based type of each FS3 site
   // coefficient by type: [ti*36 + tj*6 + tk][ip*4 + jp*2 + kp] for SR and LR
   std::vector<double> coef_sr, coef_lr;
+  std::vector<int> class_of_type;  // same layout: 0-based coefficient (class) index
 };

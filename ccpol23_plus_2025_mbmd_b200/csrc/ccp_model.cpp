@@ -352,6 +352,7 @@ bool type_coefficients(ccp_model &m) {
   const int nt = kNtype;
   m.coef_sr.assign(nt * nt * nt * 8, 0.0);
   m.coef_lr.assign(nt * nt * nt * 8, 0.0);
+  m.class_of_type.assign(nt * nt * nt * 8, -1);
   std::vector<int> seen(nt * nt * nt * 8, 0);
   for (int is = 0; is < kNs3; is++)
     for (int js = 0; js < kNs3; js++)
@@ -369,6 +370,7 @@ bool type_coefficients(ccp_model &m) {
             return false;
           }
           seen[t] = idx;
+          m.class_of_type[t] = idx - 1;
           m.coef_sr[t] = m.sr.cs[idx - 1];
           m.coef_lr[t] = m.lr.cs[idx - 1];
         }

@@ -196,6 +196,21 @@ struct Fs3Smem {
   Fs3Rec rec;
 };
 
+// Extra shared memory of the parameter-gradient form: this block's partial sums of
+// dS/d(coefficient table entry) and dS/d(b, g, r0), weighted like the energy, and the
+// damping factor exp(-g (r - r0)) / (1 + exp(-g (r - r0))) of each site pair.
+template <typename T>
+struct Fs3Grad {
+  double gc[2][kCoef];
+  double gb[2][3][kPairs];
+  T exd[3][kP][kRS];
+};
+
+template <typename T>
+__host__ __device__ constexpr size_t fs3_grad_offset() {
+  return (sizeof(Fs3Smem<T>) + 15) & ~size_t(15);
+}
+
 template <typename T>
 __device__ __forceinline__ T t_exp(T v);
 template <>
@@ -245,12 +260,21 @@ __device__ __forceinline__ PassCfg pass_cfg(int fam) {
   return c;
 }
 
-template <typename T>
+// With GRAD and a family-0 pass (outputs are the ij pairs), gcv also receives, for each type
+// block and power combination, wsite * sum_tile U_z(ij) M_u: the derivative of the sweep's
+// energy sum with respect to that coefficient-table entry, index 4y + 2x + z.
+template <typename T, bool GRAD>
 __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__restrict__ C,
-                                         const PassCfg &g, int r0, int c0, T q0[4], T q1[4]) {
+                                         const PassCfg &g, int r0, int c0, T q0[4], T q1[4],
+                                         double *gcv, double wsite) {
   using V2 = typename Vec2<T>::type;
   const V2 *U = &S.uu[0][0][0];
   const int tr = kPType[r0], tc = kPType[c0];
+  V2 Ut[4];
+  if (GRAD && gcv) {
+#pragma unroll
+    for (int o = 0; o < 4; o++) Ut[o] = S.uu[0][sp(r0 + (o >> 1))][sp(c0 + (o & 1))];
+  }
   const double *cbase = C + tr * g.mr + tc * g.mc;
   // physical rows/columns of the tile (r0, c0 even): sp(r0) = r0/2, sp(r0+1) = 9 + r0/2
   const V2 *X0 = U + g.xb + (r0 >> 1) * g.xr, *X1 = X0 + 9 * g.xr;
@@ -281,6 +305,21 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__re
           M[o][3] += X[rr].y * Y[cc].y;
         }
     }
+    if (GRAD && gcv) {
+      double *gt = gcv + ((tr * 6 + tc) * 6 + tb) * 8;
+#pragma unroll
+      for (int u = 0; u < 4; u++) {
+        T b0 = (T)0, b1 = (T)0;
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+          b0 += Ut[o].x * M[o][u];
+          b1 += Ut[o].y * M[o][u];
+        }
+        const int pz0 = 4 * (u & 1) + 2 * (u >> 1);
+        atomicAdd(gt + pz0, wsite * (double)b0);
+        atomicAdd(gt + pz0 + 1, wsite * (double)b1);
+      }
+    }
     const double *cp = cbase + tb * g.mb;
     T ca[4], cb[4];
 #pragma unroll
@@ -298,8 +337,8 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__re
 
 // One SR (v = 0) or LR (v = 1) sweep of the current triple: tabulate the site pairs, run
 // the three gradient passes, add wsite * G into S.G and return the energy sum.
-template <typename T>
-__device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
+template <typename T, bool GRAD>
+__device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite) {
   using V2 = typename Vec2<T>::type;
   const int tid = threadIdx.x;
   if (tid < kPairs) {
@@ -322,6 +361,7 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
       w.y = -bb + gg * ex * damp;
       S.uu[p][sp(pidx(a))][sp(pidx(b))] = u;
       S.dl[p][sp(pidx(a))][sp(pidx(b))] = w;
+      if (GRAD) GS->exd[p][sp(pidx(a))][sp(pidx(b))] = ex * damp;
     }
   }
   __syncthreads();
@@ -331,7 +371,8 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
     const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
     const PassCfg g = pass_cfg(fam);
     T q0[4], q1[4];
-    fs3_pass<T>(S, reinterpret_cast<const double *>(S.coef[v]), g, r0, c0, q0, q1);
+    fs3_pass<T, GRAD>(S, reinterpret_cast<const double *>(S.coef[v]), g, r0, c0, q0, q1,
+                      (GRAD && fam == 0) ? GS->gc[v] : nullptr, wsite);
 #pragma unroll
     for (int o = 0; o < 4; o++) {
       const int r = sp(r0 + (o >> 1)), c = sp(c0 + (o & 1));
@@ -339,6 +380,17 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
       const T P = q0[o] + w.x * q1[o];
       if (fam == 0) esum += (double)u.x * (double)P;
       S.G[fam][r][c] += wsite * (double)(u.x * (w.y * P + q1[o]) / w.x);
+      const int ra = r0 + (o >> 1), cb = c0 + (o & 1);
+      if (GRAD && ra != 1 && cb != 1) {
+        // dS/de_ab = P; de/db = -r e, de/dg = (r - r0) e x, de/dr0 = -g e x with
+        // x = exp(-g (r - r0)) / (1 + exp(-g (r - r0)))
+        const int q = (ra == 0 ? 0 : ra - 1) * kNs3 + (cb == 0 ? 0 : cb - 1);
+        const double wPe = wsite * (double)P * (double)u.x;
+        const double rr = (double)w.x, xd = (double)GS->exd[fam][r][c];
+        atomicAdd(&GS->gb[v][0][q], -wPe * rr);
+        atomicAdd(&GS->gb[v][1][q], wPe * (rr - S.bgr[v][2][q]) * xd);
+        atomicAdd(&GS->gb[v][2][q], -wPe * S.bgr[v][1][q] * xd);
+      }
     }
   }
   esum = warp_sum(esum);
@@ -351,16 +403,23 @@ __device__ double fs3_variant(Fs3Smem<T> &S, int v, double wsite) {
   return tot;
 }
 
-template <typename T>
+template <typename T, bool GRAD>
 __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
     k_fs3(const Fs3Rec *__restrict__ recs, const int *__restrict__ icnt, int tri_cap,
           const double4 *__restrict__ s17, const double *__restrict__ coef,
-          const double *__restrict__ bgr, int nm, int ns, double *f, double *fc3, double *scal) {
+          const double *__restrict__ bgr, int nm, int ns, double *f, double *fc3, double *scal,
+          double *gfs3) {
   using V2 = typename Vec2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
+  Fs3Grad<T> *GS = GRAD ? reinterpret_cast<Fs3Grad<T> *>(smem_raw + fs3_grad_offset<T>()) : nullptr;
   const int tid = threadIdx.x;
   if ((int)blockIdx.x >= min(icnt[C_NTRI_FS3], tri_cap)) return;  // no triple for this block
+  if (GRAD) {
+    for (int t = tid; t < 2 * kCoef; t += kFs3Block) (&GS->gc[0][0])[t] = 0.0;
+    for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&GS->gb[0][0][0])[t] = 0.0;
+    for (int t = tid; t < 3 * kP * kRS; t += kFs3Block) (&GS->exd[0][0][0])[t] = (T)0;
+  }
   for (int t = tid; t < 2 * kCoef2; t += kFs3Block) (&S.coef[0][0])[t] = make_double2(0.0, 0.0);
   __syncthreads();
   for (int t = tid; t < 2 * kCoef / 2; t += kFs3Block) {
@@ -405,13 +464,13 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
     const int br = S.rec.branch;
     double energy, comc;
     if (br != 2) {
-      const double Sv = fs3_variant<T>(S, br, fdmp);
+      const double Sv = fs3_variant<T, GRAD>(S, GS, br, fdmp);
       energy = fdmp * Sv;
       comc = dfdmp * Sv;
     } else {
       const double smfun = S.rec.smfun, smfun2 = 1.0 - smfun, cf = S.rec.cf;
-      const double Ssr = fs3_variant<T>(S, 0, fdmp * smfun);
-      const double Slr = fs3_variant<T>(S, 1, fdmp * smfun2);
+      const double Ssr = fs3_variant<T, GRAD>(S, GS, 0, fdmp * smfun);
+      const double Slr = fs3_variant<T, GRAD>(S, GS, 1, fdmp * smfun2);
       energy = fdmp * (smfun * Ssr + smfun2 * Slr);
       comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
     }
@@ -506,6 +565,17 @@ __global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
     atomicAdd(&scal[S_FS3_VIR], v_tot);
     if (e_tot != 0.0) atomicAdd(&scal[S_FS3_E], e_tot);
   }
+  if (GRAD) {
+    __syncthreads();
+    for (int t = tid; t < 2 * kCoef; t += kFs3Block) {
+      const double g = (&GS->gc[0][0])[t];
+      if (g != 0.0) atomicAdd(&gfs3[t], g);
+    }
+    for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) {
+      const double g = (&GS->gb[0][0][0])[t];
+      if (g != 0.0) atomicAdd(&gfs3[2 * kCoef + t], g);
+    }
+  }
 }
 
 }  // namespace
@@ -537,29 +607,42 @@ cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt
   return cudaGetLastError();
 }
 
+namespace {
+template <typename T, bool GRAD>
+cudaError_t launch_fs3_t(const Fs3Rec *R, const int *icnt, int tri_cap, const double4 *s17,
+                         const double *coef, const double *bgr, int nm, int ns, double *f,
+                         double *fc3, double *scal, int nsm, int triples_per_block, double *gfs3,
+                         cudaStream_t st) {
+  const size_t smem = GRAD ? fs3_grad_offset<T>() + sizeof(Fs3Grad<T>) : sizeof(Fs3Smem<T>);
+  cudaError_t e = cudaFuncSetAttribute(k_fs3<T, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<T, GRAD>, kFs3Block, smem);
+  if (per_sm < 1) per_sm = 1;
+  // the gradient form flushes per-block partial sums: a persistent grid keeps them few
+  const int grid = fs3_grid(nsm * per_sm, tri_cap, GRAD ? 0 : triples_per_block);
+  k_fs3<T, GRAD><<<grid, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3,
+                                                scal, gfs3);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
                        double *f, double *fc3, double *scal, int nsm, int triples_per_block,
-                       cudaStream_t st) {
-  cudaError_t e;
+                       double *gfs3, cudaStream_t st) {
   const Fs3Rec *R = static_cast<const Fs3Rec *>(rec);
-  int per_sm = 0;
   if (precision == 0) {
-    const size_t smem = sizeof(Fs3Smem<double>);
-    e = cudaFuncSetAttribute(k_fs3<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<double>, kFs3Block, smem);
-    if (per_sm < 1) per_sm = 1;
-    k_fs3<double><<<fs3_grid(nsm * per_sm, tri_cap, triples_per_block), kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns,
-                                                         f, fc3, scal);
-  } else {
-    const size_t smem = sizeof(Fs3Smem<float>);
-    e = cudaFuncSetAttribute(k_fs3<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<float>, kFs3Block, smem);
-    if (per_sm < 1) per_sm = 1;
-    k_fs3<float><<<fs3_grid(nsm * per_sm, tri_cap, triples_per_block), kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f,
-                                                        fc3, scal);
+    if (gfs3)
+      return launch_fs3_t<double, true>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal,
+                                        nsm, triples_per_block, gfs3, st);
+    return launch_fs3_t<double, false>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
+                                       triples_per_block, nullptr, st);
   }
-  return cudaGetLastError();
+  if (gfs3)
+    return launch_fs3_t<float, true>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
+                                     triples_per_block, gfs3, st);
+  return launch_fs3_t<float, false>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
+                                    triples_per_block, nullptr, st);
 }

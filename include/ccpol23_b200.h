@@ -189,6 +189,41 @@ int ccp_kspace_ewald_fixed(const ccp_model *m, int nm, const double *x_device,
                            double *fys_device, double *fzs_device, double *vir_device,
                            void *stream);
 
+/* Any subset of the hot path's terms on device arrays (layouts of ccp_hot_path_device).
+   Terms the model switches off are skipped; energies of terms not run are 0.  This is how
+   a caller evaluates, e.g., the three-body plus induction energy alone. */
+#define CCP_TERM_SELF 1u       /* ewald_self_correction */
+#define CCP_TERM_RSPACE 2u     /* rspace_ewald */
+#define CCP_TERM_KSPACE 4u     /* kspace_ewald */
+#define CCP_TERM_INDUCTION 8u  /* nb_induction */
+#define CCP_TERM_FS2 16u       /* threebody_term, FS2 part */
+#define CCP_TERM_FS3 32u       /* threebody_term, FS3 part */
+#define CCP_TERM_ALL 63u
+int ccp_terms_device(ccp_context *ctx, unsigned terms, const double *x_device,
+                     const double *y_device, const double *z_device, const double *xs_device,
+                     const double *ys_device, const double *zs_device, int ld, double box,
+                     ccp_energies *e, double *fxs_device, double *fys_device,
+                     double *fzs_device, double *fxfs2_device, double *fyfs2_device,
+                     double *fzfs2_device, double *fxfs3_device, double *fyfs3_device,
+                     double *fzfs3_device, double *idmx_device, double *idmy_device,
+                     double *idmz_device);
+
+/* ------------------------------------------- FS3 parameters and their gradient */
+/* The FS3 fit of a context, initially the model's data3b_full (SR) and data3b_full_LR_4p5
+   (LR): ncoef linear coefficients per fit (ccp_model_get_int "nclass", the cs3 array of
+   threebody_potential.f90) and the site-pair nonlinear parameters as three arrays of 289,
+   b, g and r0 of site pair (is, js) at is*17 + js (bohr units, as in the files).  Setting
+   them re-uploads the tables.  With the context option "fs3_param_grad" on, every
+   evaluation that includes FS3 also accumulates the FS3 energy's gradient with respect to
+   all of them (kcal/mol per parameter unit), read with ccp_context_fs3_param_grad.  These
+   have no counterpart in the reference, which has no derivatives with respect to its fit. */
+int ccp_context_get_fs3_params(const ccp_context *ctx, double *cs_sr, double *cs_lr, int ncoef,
+                               double *bgr_sr, double *bgr_lr);
+int ccp_context_set_fs3_params(ccp_context *ctx, const double *cs_sr, const double *cs_lr,
+                               int ncoef, const double *bgr_sr, const double *bgr_lr);
+int ccp_context_fs3_param_grad(ccp_context *ctx, double *dcs_sr, double *dcs_lr, int ncoef,
+                               double *dbgr_sr, double *dbgr_lr);
+
 /* ---------------------------------------------------------------- diagnostics */
 /* These have no counterpart in the reference; they serve benchmarking and profiling. */
 
@@ -211,6 +246,11 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
                      WHILE node, no host round trip per iteration; 0: the host launches each
                      iteration and reads the convergence state (profilers that cannot see
                      kernels inside conditional graphs need this);
+     "overlap"       1 (default): FS2 and FS3 run on low-priority side streams concurrently
+                     with the Ewald and induction kernels (on a high-priority stream);
+     "fs3_triples_per_block"  8 (default): FS3 triples per block when overlapping, so that
+                     blocks retire often (0: one persistent wave of blocks);
+     "fs3_param_grad" 0 (default): see ccp_context_fs3_param_grad;
      "phase_matrix"  1 (default): the per-(polarisable site, k-vector) phases are tabulated
                      once per evaluation when the table is at most 64 MiB; 0: never (the
                      tiled on-the-fly reciprocal kernels run every iteration).
