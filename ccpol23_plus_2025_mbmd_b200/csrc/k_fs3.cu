@@ -399,12 +399,14 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
   double tot = 0.0;
 #pragma unroll
   for (int w = 0; w < kFs3Block / 32; w++) tot += S.red[w];
-  __syncthreads();
+  // S.red is rewritten only after the next sweep's pair-phase barrier, which every thread
+  // reaches after this read, so no barrier is needed here
   return tot;
 }
 
+// The gradient form holds one block per SM (its shared memory), so it may use more registers.
 template <typename T, bool GRAD>
-__global__ void __launch_bounds__(kFs3Block, CCP_FS3_MINBLOCKS)
+__global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     k_fs3(const Fs3Rec *__restrict__ recs, const int *__restrict__ icnt, int tri_cap,
           const double4 *__restrict__ s17, const double *__restrict__ coef,
           const double *__restrict__ bgr, int nm, int ns, double *f, double *fc3, double *scal,
