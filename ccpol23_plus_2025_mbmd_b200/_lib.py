@@ -35,19 +35,21 @@ EXPORTS = [
     "ccp_context_set_timing", "ccp_context_phase_ms", "ccp_device_fma_peak",
     "ccp_kspace_ewald_fixed", "ccp_context_set_option", "ccp_context_get_option",
     "ccp_terms_device", "ccp_context_get_fs3_params", "ccp_context_set_fs3_params",
-    "ccp_context_fs3_param_grad",
+    "ccp_context_fs3_param_grad", "ccp_ccpol23plus",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
 TERM_SELF, TERM_RSPACE, TERM_KSPACE, TERM_INDUCTION, TERM_FS2, TERM_FS3 = 1, 2, 4, 8, 16, 32
-TERM_ALL = 63
+TERM_VDW = 64
+TERM_HOT = 63
+TERM_ALL = 127
 
 
 class CcpEnergies(C.Structure):
     _fields_ = [("scpe", C.c_double), ("rcpe", C.c_double), ("kcpe", C.c_double),
                 ("indpe", C.c_double), ("fs2pe", C.c_double), ("fs3pe", C.c_double),
                 ("vir", C.c_double), ("ind_iters", C.c_int), ("n_fs3_triples", C.c_int),
-                ("n_fs3_blend", C.c_int), ("n_fs2_triples", C.c_int)]
+                ("n_fs3_blend", C.c_int), ("n_fs2_triples", C.c_int), ("vdwpe", C.c_double)]
 
 
 class CcpError(RuntimeError):
@@ -96,6 +98,7 @@ def lib():
     L.ccp_threebody_term.argtypes = [vp] + [vp] * 6 + [i, d, pd, pd] + [vp] * 9 + [pd]
     L.ccp_hot_path.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_hot_path_device.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
+    L.ccp_ccpol23plus.argtypes = [vp] + [vp] * 6 + [i, d, pd] + [vp] * 3 + [pd]
     L.ccp_terms_device.argtypes = [vp, C.c_uint] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_context_get_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
     L.ccp_context_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]

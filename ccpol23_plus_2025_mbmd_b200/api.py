@@ -27,7 +27,7 @@ def data_dir(variant: str) -> Path:
     return DATA / variant
 
 
-NPHASE = 9  # CCP_NPHASE
+NPHASE = 10  # CCP_NPHASE
 
 
 class Model:
@@ -217,7 +217,7 @@ class Context:
     def phase_ms(self) -> np.ndarray:
         """Durations (ms) of the last evaluation's phases, in the order of CCP_NPHASE's
         comment: packing+neighbours, real space, reciprocal, induction set-up, dipole
-        iteration, induction forces, FS2, FS3 triple list, FS3 kernel."""
+        iteration, induction forces, FS2, FS3 triple list, FS3 kernel, 2-body term."""
         out = np.zeros(NPHASE)
         check(_lib.lib().ccp_context_phase_ms(self._h, out.ctypes.data, NPHASE))
         return out
@@ -245,6 +245,15 @@ class Context:
                                           ptr(zs), xs.shape[1], box, alp, C.byref(q), ptr(fxs),
                                           ptr(fys), ptr(fzs), C.byref(v)))
         vir[0] = v.value
+        return q.value
+
+    def ccpol23plus(self, x, y, z, xs, ys, zs, box, fxs, fys, fzs, vir):
+        """vdw_ccpol23plus.f90:174-477; overwrites fxs.. and vir[0] as the reference does."""
+        q = C.c_double()
+        ld = xs.shape[1]
+        check(_lib.lib().ccp_ccpol23plus(self._h, ptr(x), ptr(y), ptr(z), ptr(xs), ptr(ys),
+                                          ptr(zs), ld, box, C.byref(q), ptr(fxs), ptr(fys),
+                                          ptr(fzs), vir.ctypes.data_as(C.POINTER(C.c_double))))
         return q.value
 
     def kspace_ewald(self, x, y, z, xs, ys, zs, lmax, mmax, nmax, alp, box, fxs, fys, fzs, vir):

@@ -27,9 +27,11 @@ enum TermMask : unsigned {
   T_INDUCTION = 8u,
   T_FS2 = 16u,
   T_FS3 = 32u,
+  T_VDW = 64u,
 };
 static_assert(T_SELF == CCP_TERM_SELF && T_RSPACE == CCP_TERM_RSPACE && T_KSPACE == CCP_TERM_KSPACE &&
-                  T_INDUCTION == CCP_TERM_INDUCTION && T_FS2 == CCP_TERM_FS2 && T_FS3 == CCP_TERM_FS3,
+                  T_INDUCTION == CCP_TERM_INDUCTION && T_FS2 == CCP_TERM_FS2 && T_FS3 == CCP_TERM_FS3 &&
+                  T_VDW == CCP_TERM_VDW,
               "term bits of the C ABI");
 
 bool cuda_ok(cudaError_t e, const char *what) {
@@ -100,6 +102,11 @@ struct ccp_context {
   double *d_sk = nullptr;
   // FS3 tables
   double *d_coef = nullptr, *d_bgr = nullptr;
+  // ccpol23plus 2-body tables
+  bool have_vdw = false;
+  int vdw_nrows = 0, vdw_nv = 0;
+  int *d_vdw_row = nullptr, *d_vdw_site = nullptr;
+  double *d_vdw_qq = nullptr, *d_vdw_par = nullptr;
   // FS3 parameters of this context (host copies): class coefficients, the class of every
   // coefficient-table entry, site-pair (b, g, r0); and the parameter-gradient buffer
   std::vector<double> cs_sr, cs_lr, bgr_host;
@@ -154,7 +161,7 @@ void free_ctx(ccp_context *c) {
                 c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
                 c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
-                c->d_gfs3,
+                c->d_gfs3,  c->d_vdw_row, c->d_vdw_site, c->d_vdw_qq, c->d_vdw_par,
                 c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
   for (void *p : dp)
     if (p) cudaFree(p);
@@ -293,6 +300,7 @@ int ensure_host_io(ccp_context *c, size_t n) {
 struct EvalOut {
   double sumff = 0, self_vir = 0, rc_e = 0, rc_vir = 0, kc_e = 0, kc_vir = 0;
   double ind_e = 0, ind_vir = 0, fs2_e = 0, fs2_vir = 0, fs3_e = 0, fs3_vir = 0;
+  double vdw_e = 0, vdw_vir = 0;
   int iters = 0, ntri = 0, nblend = 0, nfs2 = 0;
   bool converged = true;
 };
@@ -451,6 +459,7 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
   const SiteSets &S = c->S;
   if ((mask & (T_FS2 | T_FS3)) && !c->three_body) mask &= ~(T_FS2 | T_FS3);
   if ((mask & T_FS2) && !c->s2) mask &= ~T_FS2;
+  if ((mask & T_VDW) && !c->have_vdw) mask &= ~T_VDW;
   if ((mask & T_FS3) && (!c->s3 || !c->have_fs3)) mask &= ~T_FS3;
   if ((mask & T_FS3) && ns < kNs3) {
     set_error("FS3 needs 17 sites per molecule");
@@ -507,7 +516,7 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
   auto pend = [&](int k, cudaStream_t s) {
     if (c->timing) cudaEventRecord(c->ev[2 * k + 1], s);
   };
-  const bool side = c->opt_overlap && (mask & (T_FS2 | T_FS3));
+  const bool side = c->opt_overlap && (mask & (T_FS2 | T_FS3 | T_VDW));
   // Ewald + induction run on a high-priority internal stream, the three-body terms on
   // low-priority ones, so that freed SM slots go to the latency-bound induction chain first
   cudaStream_t s3 = side ? c->s_fs3 : st, s2 = side ? c->s_fs2 : st, sm = side ? c->s_main : st;
@@ -518,7 +527,7 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     LK(launch_prep(px, py, pz, pxs, pys, pzs, nm, ld, S, c->d_com, c->d_act, c->d_comb, c->d_s17,
                    std::min(ns, kNs3), c->d_f, 6 * nm * ns, c->d_fc2, c->d_fc3, c->d_scal,
                    c->d_icnt, st));
-    const bool need_nbr = mask & (T_RSPACE | T_INDUCTION | T_FS2 | T_FS3);
+    const bool need_nbr = mask & (T_RSPACE | T_INDUCTION | T_FS2 | T_FS3 | T_VDW);
     if (need_nbr)
       LK(launch_neighbors(c->d_com, nm, box, rl * rl, c->cap, c->d_nbr, c->d_nbrv, c->d_ncnt,
                           c->d_icnt, st));
@@ -554,6 +563,13 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       LK(launch_fs2(c->precision, c->d_pairs, c->d_icnt, c->pair_cap, c->d_comb, c->d_s17, c->d_nbr,
                     c->d_ncnt, c->cap, F2, nm, ns, f3, c->d_fc2, c->d_scal, s2));
       pend(6, s2);
+    }
+    if (mask & T_VDW) {
+      pbeg(9, s2);
+      LK(launch_vdw(pxs, pys, pzs, ld, c->d_nbr, c->d_nbrv, c->d_ncnt, c->cap, nm, ns,
+                    c->rcutsd, c->d_vdw_row, c->d_vdw_qq, c->d_vdw_par, c->vdw_nrows,
+                    c->d_vdw_site, c->vdw_nv, f3, c->d_scal, s2));
+      pend(9, s2);
     }
     pbeg(1, sm);
     if (mask & T_SELF)
@@ -674,6 +690,8 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     o.fs2_vir = h[S_FS2_VIR];
     o.fs3_e = h[S_FS3_E];
     o.fs3_vir = h[S_FS3_VIR];
+    o.vdw_e = h[S_VDW_E];
+    o.vdw_vir = h[S_VDW_VIR];
     o.ntri = ic[C_NTRI_FS3];
     o.nblend = ic[C_NBLEND_FS3];
     o.nfs2 = ic[C_NTRI_FS2];
@@ -802,19 +820,28 @@ void fill_energies(ccp_context *c, const EvalOut &o, double box, ccp_energies *e
   e->indpe = kR4pie0 * o.ind_e / 418.4;
   e->fs2pe = o.fs2_e * kH2kcal;
   e->fs3pe = o.fs3_e * kH2kcal;
+  e->vdwpe = o.vdw_e / 418.4;
   e->vir = o.self_vir + o.rc_vir + 2.0 * kR4pie0 * o.kc_vir + o.ind_vir +
-           o.fs2_vir * kH2kcal * 418.4 + o.fs3_vir * kH2kcal * 418.4;
+           o.fs2_vir * kH2kcal * 418.4 + o.fs3_vir * kH2kcal * 418.4 + o.vdw_vir;
   e->ind_iters = o.iters;
   e->n_fs3_triples = o.ntri;
   e->n_fs3_blend = o.nblend;
   e->n_fs2_triples = o.nfs2;
 }
 
+unsigned allowed_mask(const ccp_context *c);
+
 unsigned hot_mask(const ccp_context *c) {
   unsigned m = T_SELF | T_RSPACE | T_KSPACE;
   if (c->induction) m |= T_INDUCTION;
   if (c->three_body) m |= T_FS2 | T_FS3;
   return m;
+}
+
+// Every term this context can evaluate: the hot path plus the 2-body term when the model is
+// ccpol23plus.
+unsigned allowed_mask(const ccp_context *c) {
+  return hot_mask(c) | (c->have_vdw ? unsigned(T_VDW) : 0u);
 }
 
 __global__ void k_scatter_out(const double *__restrict__ f, int nm, int ns, int ld, double *fx,
@@ -983,6 +1010,53 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
   if (ensure_inputs(c, m->ns) != CCP_OK) return fail("inputs");
   const int cap0 = std::min(nm - 1, 192);
   if (ensure_lists(c, std::max(cap0, 1), 96 * nm, 48 * nm) != CCP_OK) return fail("lists");
+  if (m->pot_name == "ccpol23plus" && !m->vdw.empty()) {
+    // parameter row of every site pair (name match in either order, first row wins, as the
+    // reference's row loop), charge products, and the sites that have any row
+    const int ns = m->ns;
+    std::vector<int> row(ns * ns, -1), vs;
+    std::vector<double> qq(ns * ns), par;
+    for (int a = 0; a < ns; a++)
+      for (int b = 0; b < ns; b++) {
+        qq[a * ns + b] = m->charge[a] * m->charge[b];
+        for (size_t k = 0; k < m->vdw.size(); k++) {
+          const auto &r = m->vdw[k];
+          if ((m->names[a] == r.a && m->names[b] == r.b) || (m->names[b] == r.a && m->names[a] == r.b)) {
+            row[a * ns + b] = (int)k;
+            break;
+          }
+        }
+      }
+    for (int a = 0; a < ns; a++) {
+      bool any = false;
+      for (int b = 0; b < ns; b++) any = any || row[a * ns + b] >= 0;
+      if (any) vs.push_back(a);
+    }
+    // initialization.f90:612-628: c0..c3, c6, c8, c10 to internal energy units
+    for (const auto &r : m->vdw) {
+      const double *p = r.p;
+      const double v[kVdwPar] = {p[0], p[1] * 418.4, p[2] * 418.4, p[3] * 418.4, p[4] * 418.4,
+                                 p[5] * 418.4, p[6] * 418.4, p[7] * 418.4, p[8], p[9], p[10], p[11]};
+      par.insert(par.end(), v, v + kVdwPar);
+    }
+    if ((int)m->vdw.size() > kVdwMaxRows || vs.size() > 32 || vs.empty()) {
+      set_error("ccp_context_create: ccpol23plus needs at most 64 parameter rows and 32 sites with rows");
+      free_ctx(c);
+      delete c;
+      return CCP_ERR_BAD_INPUT;
+    }
+    c->vdw_nrows = (int)m->vdw.size();
+    c->vdw_nv = (int)vs.size();
+    if (dalloc(&c->d_vdw_row, row.size()) != cudaSuccess || dalloc(&c->d_vdw_site, vs.size()) != cudaSuccess ||
+        dalloc(&c->d_vdw_qq, qq.size()) != cudaSuccess || dalloc(&c->d_vdw_par, par.size()) != cudaSuccess)
+      return fail("2-body tables");
+    if (cudaMemcpy(c->d_vdw_row, row.data(), row.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_vdw_site, vs.data(), vs.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_vdw_qq, qq.data(), qq.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->d_vdw_par, par.data(), par.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail("2-body upload");
+    c->have_vdw = true;
+  }
   if (m->have_fs3) {
     std::vector<double> coef(2 * m->coef_sr.size());
     std::copy(m->coef_sr.begin(), m->coef_sr.end(), coef.begin());
@@ -1159,6 +1233,36 @@ int ccp_rspace_ewald(ccp_context *ctx, const double *x, const double *y, const d
   return r;
 }
 
+int ccp_ccpol23plus(ccp_context *ctx, const double *x, const double *y, const double *z,
+                    const double *xs, const double *ys, const double *zs, int ld, double box,
+                    double *qvdwe, double *fxs, double *fys, double *fzs, double *vir) {
+  const void *p[] = {x, y, z, xs, ys, zs, qvdwe, fxs, fys, fzs, vir};
+  int r = check_args(ctx, p, 11, ld);
+  if (r) return r;
+  if (!ctx->have_vdw) {
+    set_error("ccp_ccpol23plus: the model's potential is not ccpol23plus");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  EvalOut o;
+  if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, T_VDW, o);
+  if (r) return r;
+  // vdw_ccpol23plus.f90:212-221: the site forces and the virial start from zero
+  for (int i = 0; i < ctx->nm; i++)
+    for (int s = 0; s < ctx->ns; s++) {
+      fxs[(size_t)i * ld + s] = 0.0;
+      fys[(size_t)i * ld + s] = 0.0;
+      fzs[(size_t)i * ld + s] = 0.0;
+    }
+  r = download_forces(ctx, ld, fxs, fys, fzs);
+  if (!r) {
+    *qvdwe = o.vdw_e / 418.4;
+    *vir = o.vdw_vir;
+  }
+  return r;
+}
+
 int ccp_kspace_ewald(ccp_context *ctx, const double *x, const double *y, const double *z,
                      const double *xs, const double *ys, const double *zs, int ld, int lmax,
                      int mmax, int nmax, double alp, double box, double *qkcpe, double *fxs,
@@ -1270,7 +1374,7 @@ int ccp_terms_device(ccp_context *ctx, unsigned terms, const double *x, const do
     set_error("ccp_terms_device: unknown term bits");
     return CCP_ERR_BAD_INPUT;
   }
-  const unsigned mask = terms & hot_mask(ctx);
+  const unsigned mask = terms & allowed_mask(ctx);
   EvalOut o;
   r = evaluate(ctx, x, y, z, xs, ys, zs, ld, box, mask, o);
   if (r) return r;
@@ -1304,7 +1408,7 @@ int ccp_hot_path_device(ccp_context *ctx, const double *x, const double *y, cons
                         ccp_energies *e, double *fxs, double *fys, double *fzs, double *fxfs2,
                         double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3,
                         double *fzfs3, double *idmx, double *idmy, double *idmz) {
-  return ccp_terms_device(ctx, CCP_TERM_ALL, x, y, z, xs, ys, zs, ld, box, e, fxs, fys, fzs, fxfs2,
+  return ccp_terms_device(ctx, CCP_TERM_HOT, x, y, z, xs, ys, zs, ld, box, e, fxs, fys, fzs, fxfs2,
                           fyfs2, fzfs2, fxfs3, fyfs3, fzfs3, idmx, idmy, idmz);
 }
 

@@ -81,6 +81,8 @@ enum ScalSlot {
   S_FS2_VIR,
   S_FS3_E,
   S_FS3_VIR,
+  S_VDW_E,
+  S_VDW_VIR,
   S_COUNT
 };
 
@@ -148,6 +150,12 @@ struct IterArgs {
   SiteSets S;
 };
 
+// ccpol23plus 2-body parameters (vdw_ccpol23plus.f90): rows of beta, c0, c1, c2, c3, c6, c8,
+// c10 (internal energy units), d1, d6, d8, d10; row[is * ns + js] = row index or -1 and
+// qq[is * ns + js] = charge product of the site pair.
+constexpr int kVdwPar = 12;
+constexpr int kVdwMaxRows = 64;
+
 // ------------------------------------------------------------------ launchers
 // All launchers enqueue on `st` and return cudaGetLastError().
 // FS3 parameter-gradient buffer (launch_fs3's gfs3): [2][216][8] coefficient-table entries,
@@ -155,6 +163,13 @@ struct IterArgs {
 constexpr int kFs3GradLen = 2 * 216 * 8 + 2 * 3 * 289;
 // b[0..n) += a[0..n)
 cudaError_t launch_add(int n, const double *a, double *b, cudaStream_t st);
+// ccpol23plus 2-body term (k_vdw.cu): site forces added to f (atomics), energy and virial
+// into scal[S_VDW_E], scal[S_VDW_VIR] (internal units).
+cudaError_t launch_vdw(const double *xs, const double *ys, const double *zs, int ld,
+                       const int *nbr, const double4 *nbrv, const int *ncnt, int cap, int nm,
+                       int ns, double rcutsd, const int *row, const double *qq,
+                       const double *par, int nrows, const int *vsite, int nv, double *f,
+                       double *scal, cudaStream_t st);
 cudaError_t launch_prep(const double *x, const double *y, const double *z, const double *xs,
                         const double *ys, const double *zs, int nm, int ld, SiteSets S,
                         double4 *com, double4 *act, double4 *comb, double4 *s17, int ns3,

@@ -55,6 +55,7 @@ typedef struct ccp_energies {
     int n_fs3_triples;    /* molecular triples inside the FS3 cut-off */
     int n_fs3_blend;      /* of which in the SR/LR switching region */
     int n_fs2_triples;    /* (spectator, pair) combinations inside the FS2 cut-off */
+    double vdwpe;     /* ccpol23plus 2-body (only when that term is evaluated) */
 } ccp_energies;
 
 /* Last error message of the calling thread (never NULL). */
@@ -120,6 +121,14 @@ int ccp_kspace_ewald(ccp_context *ctx, const double *x, const double *y, const d
                      const double *xs, const double *ys, const double *zs, int ld, int lmax,
                      int mmax, int nmax, double alp, double box, double *qkcpe, double *fxs,
                      double *fys, double *fzs, double *vir);
+
+/* ccpol23plus(xx,..,boxi,qqvdwe) -- vdw_ccpol23plus.f90:174-477, the 2-body term.  As the
+   reference, it OVERWRITES the site forces (fxs = 2-body forces of the first ns sites) and
+   SETS *vir to the 2-body virial: the MD step calls it first and the other terms add on.
+   The long-range correction, computed but not added by the reference, is not computed. */
+int ccp_ccpol23plus(ccp_context *ctx, const double *x, const double *y, const double *z,
+                    const double *xs, const double *ys, const double *zs, int ld, double box,
+                    double *qvdwe, double *fxs, double *fys, double *fzs, double *vir);
 
 /* nb_induction(xx,..,boxi,qindpe) -- nb_induction_model.f90:25-126: static field, Jacobi
    dipole iteration (iteridm, :1193-1407), induction forces.  idm* receive the induced
@@ -198,7 +207,9 @@ int ccp_kspace_ewald_fixed(const ccp_model *m, int nm, const double *x_device,
 #define CCP_TERM_INDUCTION 8u  /* nb_induction */
 #define CCP_TERM_FS2 16u       /* threebody_term, FS2 part */
 #define CCP_TERM_FS3 32u       /* threebody_term, FS3 part */
-#define CCP_TERM_ALL 63u
+#define CCP_TERM_VDW 64u       /* ccpol23plus 2-body term (vdw_ccpol23plus.f90:174-477) */
+#define CCP_TERM_HOT 63u       /* the hot path: every term but the 2-body one */
+#define CCP_TERM_ALL 127u
 int ccp_terms_device(ccp_context *ctx, unsigned terms, const double *x_device,
                      const double *y_device, const double *z_device, const double *xs_device,
                      const double *ys_device, const double *zs_device, int ld, double box,
@@ -235,8 +246,8 @@ int ccp_context_last_launches(const ccp_context *ctx, int *launches);
    [0] input packing + neighbour list, [1] Ewald real space + static field (real) +
    intramolecular terms, [2] Ewald reciprocal space, [3] induction set-up (static reciprocal
    field, dipole tensors, phase matrix), [4] dipole iteration, [5] induction forces,
-   [6] FS2, [7] FS3 triple list, [8] FS3 kernel. */
-#define CCP_NPHASE 9
+   [6] FS2, [7] FS3 triple list, [8] FS3 kernel, [9] 2-body term. */
+#define CCP_NPHASE 10
 int ccp_context_set_timing(ccp_context *ctx, int on);
 int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
 

@@ -639,6 +639,102 @@ void orc_ewald_self_correction(const orc_model *m, double alp, double box, const
 }
 
 /* ---------------------------------------------------------------- ewald.f90:177-405 */
+/* vdw_ccpol23plus.f90:174-477 */
+void orc_ccpol23plus(const orc_model *m, const double *xx, const double *yy, const double *zz,
+                     const double *xxs, const double *yys, const double *zzs, int ld,
+                     double boxi, double *qvdwe, double *fxs, double *fys, double *fzs,
+                     double *vir) {
+    const int nm = m->nm, ns = m->ns;
+    const double gamma = 20.0 / BOHR2A, sqr0 = 1.4 * BOHR2A;
+    for (int j = 0; j < nm; j++)
+        for (int js = 0; js < ns; js++) {
+            fxs[(size_t)j * ld + js] = 0.0;
+            fys[(size_t)j * ld + js] = 0.0;
+            fzs[(size_t)j * ld + js] = 0.0;
+        }
+    const int nt = nthreads();
+    acc_t *acc = acc_alloc(nt, nm, ns);
+#pragma omp parallel num_threads(nt)
+    {
+#ifdef _OPENMP
+        acc_t *A = &acc[omp_get_thread_num()];
+#else
+        acc_t *A = &acc[0];
+#endif
+#pragma omp for schedule(dynamic, 1)
+        for (int i = 0; i < nm - 1; i++) {
+            for (int j = i + 1; j < nm; j++) {
+                double xcc = minimg(xx[i] - xx[j], boxi), ycc = minimg(yy[i] - yy[j], boxi),
+                       zcc = minimg(zz[i] - zz[j], boxi);
+                double rccsq = xcc * xcc + ycc * ycc + zcc * zcc;
+                if (!(rccsq < m->rcutsd)) continue;
+                for (int is = 0; is < ns; is++) {
+                    for (int js = 0; js < ns; js++) {
+                        const int k = m->vdw_row[is * ORC_NSITE_MAX + js];
+                        if (k < 0) continue;
+                        const double *p = m->vdw[k];
+                        const double beta = p[0], c0 = p[1], c1 = p[2], c2 = p[3], c3 = p[4];
+                        const double c6 = p[5], c8 = p[6], c10 = p[7];
+                        const double d1 = p[8], d6 = p[9], d8 = p[10], d10 = p[11];
+                        double rsx = xcc + XS(xxs, is, i) - XS(xxs, js, j);
+                        double rsy = ycc + XS(yys, is, i) - XS(yys, js, j);
+                        double rsz = zcc + XS(zzs, is, i) - XS(zzs, js, j);
+                        double qis = m->charge[is], qjs = m->charge[js];
+                        double rssq = rsx * rsx + rsy * rsy + rsz * rsz;
+                        double sqr = sqrt(rssq);
+                        double eks = exp(-beta * sqr);
+                        double u_exp = eks * (c0 + c1 * sqr + c2 * pow(sqr, 2.0) + c3 * pow(sqr, 3.0));
+                        double fdamp = 1.0 / (1.0 + exp(-gamma * (sqr - sqr0)));
+                        u_exp = u_exp * fdamp;
+                        double f1 = orc_tt(1, d1, sqr);
+                        double u_ele = R4PIE0 * (f1 - 1.0) * qis * qjs / sqr;
+                        double f6 = orc_tt(6, d6, sqr), f8 = orc_tt(8, d8, sqr),
+                               f10 = orc_tt(10, d10, sqr);
+                        double r6 = rssq * rssq * rssq, r8 = rssq * r6, r10 = rssq * r8;
+                        double u_ind = -f6 * c6 / r6 - f8 * c8 / r8 - f10 * c10 / r10;
+                        A->e += u_exp + u_ele + u_ind;
+                        double du_exp = -beta * u_exp * fdamp +
+                                        eks * fdamp * (c1 + 2.0 * c2 * sqr + 3.0 * c3 * pow(sqr, 2.0)) +
+                                        gamma * exp(-gamma * (sqr - sqr0)) * pow(fdamp, 2.0) * u_exp;
+                        double df1 = orc_dtt(1, d1, sqr);
+                        double du_ele = -R4PIE0 * qis * qjs * ((f1 - 1.0) / pow(sqr, 2.0) - df1 / sqr);
+                        double df6 = orc_dtt(6, d6, sqr), df8 = orc_dtt(8, d8, sqr),
+                               df10 = orc_dtt(10, d10, sqr);
+                        double du_ind = -df6 * c6 / r6 + 6.0 * f6 * c6 / pow(sqr, 7.0) -
+                                        df8 * c8 / r8 + 8.0 * f8 * c8 / pow(sqr, 9.0) -
+                                        df10 * c10 / r10 + 10.0 * f10 * c10 / pow(sqr, 11.0);
+                        double wij = du_exp + du_ele + du_ind;
+                        double vfij = -wij / sqr;
+                        double fxsij = rsx * vfij, fysij = rsy * vfij, fzsij = rsz * vfij;
+                        size_t si = (size_t)i * ns + is, sj = (size_t)j * ns + js;
+                        A->fx[si] += fxsij;
+                        A->fy[si] += fysij;
+                        A->fz[si] += fzsij;
+                        A->fx[sj] -= fxsij;
+                        A->fy[sj] -= fysij;
+                        A->fz[sj] -= fzsij;
+                        A->v -= (rsx * fxsij + rsy * fysij + rsz * fzsij);
+                    }
+                }
+            }
+        }
+    }
+    double e = 0.0, v = 0.0;
+    for (int t = 0; t < nt; t++) {
+        for (int i = 0; i < nm; i++)
+            for (int s = 0; s < ns; s++) {
+                fxs[(size_t)i * ld + s] += acc[t].fx[(size_t)i * ns + s];
+                fys[(size_t)i * ld + s] += acc[t].fy[(size_t)i * ns + s];
+                fzs[(size_t)i * ld + s] += acc[t].fz[(size_t)i * ns + s];
+            }
+        e += acc[t].e;
+        v += acc[t].v;
+    }
+    acc_free(acc, nt);
+    *qvdwe = e / 418.4;
+    *vir = v;
+}
+
 void orc_rspace_ewald(const orc_model *m, const double *xx, const double *yy,
                       const double *zz, const double *xxs, const double *yys,
                       const double *zzs, int ld, double boxi, double alp, double *qrcpe,

@@ -36,6 +36,7 @@ extern "C" {
 #define ORC_NSITE_MAX 50
 #define ORC_NS3 17            /* FS3 sites per molecule */
 #define ORC_NTAB (17 * 17 * 17 * 8)
+#define ORC_VDW_MAX 64
 
 typedef struct orc_model {
     int nm, ns, npol;
@@ -55,7 +56,23 @@ typedef struct orc_model {
     int nlin;                             /* number of linear coefficients in the files */
     int ind_lin[ORC_NTAB];                /* 1-based coefficient index per (is,js,ks,ip,jp,kp) */
     int nclass;                           /* number of classes produced by the index fill */
+    /* ccpol23plus 2-body parameters (FIELD "vdw parameters", initialization.f90:612-628):
+       row k holds beta, c0, c1, c2, c3, c6, c8, c10, d1, d6, d8, d10 with c0..c10 already
+       in internal energy units (x 418.4); vdw_row[is*ORC_NSITE_MAX + js] is the row whose
+       site-name pair matches (is, js) in either order, or -1. */
+    int nvdw;
+    double vdw[ORC_VDW_MAX][12];
+    int vdw_row[ORC_NSITE_MAX * ORC_NSITE_MAX];
 } orc_model;
+
+/* ccpol23plus (vdw_ccpol23plus.f90:174-477): the 2-body CCpol23+ site-site energy
+   (damped exponential + short-range Coulomb correction + damped C6/C8/C10), forces and
+   virial over molecule pairs with COM distance below rcut.  As the reference, it ZEROES the
+   site forces of the first ns sites and SETS *vir before accumulating; energy in kcal/mol.
+   The long-range correction, which the reference computes but does not add, is omitted. */
+void orc_ccpol23plus(const orc_model *m, const double *x, const double *y, const double *z,
+                     const double *xs, const double *ys, const double *zs, int ld, double box,
+                     double *qvdwe, double *fxs, double *fys, double *fzs, double *vir);
 
 /* Tang-Toennies damping f_n(delta r) and its derivative (utility.f90:89-125). */
 double orc_tt(int n, double delta, double r);

@@ -50,6 +50,9 @@ class OrcModel(C.Structure):
         ("nlin", C.c_int),
         ("ind_lin", C.c_int * (17 * 17 * 17 * 8)),
         ("nclass", C.c_int),
+        ("nvdw", C.c_int),
+        ("vdw", (C.c_double * 12) * 64),
+        ("vdw_row", C.c_int * (50 * 50)),
     ]
 
 
@@ -85,6 +88,7 @@ def lib():
                                         dp, dp, dp, dp, dp, dp, pd]
         L.orc_ewald_self_correction.argtypes = [mp, d, d, dp, dp, dp, dp, dp, dp, C.c_int, pd,
                                                 dp, dp, dp, pd]
+        L.orc_ccpol23plus.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, d, pd, dp, dp, dp, pd]
         L.orc_rspace_ewald.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, d, d, pd,
                                        dp, dp, dp, pd]
         L.orc_kspace_ewald.argtypes = [mp, dp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int,
@@ -370,6 +374,21 @@ def make_model(inp: Inputs, nm: int, box: float, *, s2=None, s3=None,
     ind = np.zeros(17 * 17 * 17 * 8, dtype=np.int32)
     M.nclass = lib().orc_fill_index(ind)
     C.memmove(M.ind_lin, ind.ctypes.data, ind.nbytes)
+    # ccpol23plus rows (initialization.f90:612-628: c0..c10 to internal units, x 418.4)
+    M.nvdw = len(inp.vdw)
+    for k, (a, b, p) in enumerate(inp.vdw):
+        beta, c0, c1, c2, c3, c6, c8, c10, d1, d6, d8, d10 = p[:12]
+        for n, v in enumerate((beta, c0 * 418.4, c1 * 418.4, c2 * 418.4, c3 * 418.4, c6 * 418.4,
+                               c8 * 418.4, c10 * 418.4, d1, d6, d8, d10)):
+            M.vdw[k][n] = v
+    for i in range(50 * 50):
+        M.vdw_row[i] = -1
+    for si in range(inp.ns):
+        for sj in range(inp.ns):
+            for k, (a, b, p) in enumerate(inp.vdw):
+                if (inp.names[si] == a and inp.names[sj] == b) or (inp.names[sj] == a and inp.names[si] == b):
+                    M.vdw_row[si * 50 + sj] = k
+                    break
     return M
 
 
@@ -426,6 +445,15 @@ def ewald_self_correction(M, alp, box, x, y, z, xs, ys, zs, st: State):
     lib().orc_ewald_self_correction(C.byref(M), alp, box, _c(x), _c(y), _c(z), _c(xs), _c(ys),
                                     _c(zs), xs.shape[1], C.byref(q), st.fxs, st.fys, st.fzs,
                                     C.byref(st.vir))
+    return q.value
+
+
+def ccpol23plus(M, x, y, z, xs, ys, zs, box, st: State):
+    """2-body CCpol23+ (vdw_ccpol23plus.f90:174-477): zeroes st's site forces of the ns
+    sites and sets st.vir, as the reference does; returns the energy (kcal/mol)."""
+    q = C.c_double(0.0)
+    lib().orc_ccpol23plus(C.byref(M), _c(x), _c(y), _c(z), _c(xs), _c(ys), _c(zs),
+                          xs.shape[1], box, C.byref(q), st.fxs, st.fys, st.fzs, C.byref(st.vir))
     return q.value
 
 

@@ -65,6 +65,26 @@ def test_ewald_terms(oracle, boxes, key):
             assert abs(vir[0] - st.vir.value) <= TOL * abs(st.vir.value), (name, vir[0], st.vir.value)
 
 
+@pytest.mark.parametrize("key", ["c1", "fs2fs3_128", "ragged_37"])
+def test_ccpol23plus(oracle, boxes, key):
+    """The 2-body term (vdw_ccpol23plus.f90:174-477): energy, site forces (overwritten) and
+    virial (set) against the oracle."""
+    O = oracle
+    m, b, M = boxes[key]
+    args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
+    st = _state(O, b.nm, b.xs.shape[1])
+    for a in (st.fxs, st.fys, st.fzs):  # both zero the site forces of the ns sites first
+        a[:] = 1.0
+    eo = O.ccpol23plus(M, *args, b.box, st)
+    with _ctx(m, b) as c:
+        fx, fy, fz = (np.full_like(b.xs, 1.0) for _ in range(3))
+        vir = np.full(1, 7.0)
+        eg = c.ccpol23plus(*args, b.box, fx, fy, fz, vir)
+    assert abs(eg - eo) <= TOL * abs(eo), (eg, eo)
+    assert rel(np.stack([fx, fy, fz]), np.stack([st.fxs, st.fys, st.fzs])) <= TOL
+    assert abs(vir[0] - st.vir.value) <= TOL * abs(st.vir.value), (vir[0], st.vir.value)
+
+
 @pytest.mark.parametrize("key", ["c1", "ragged_37"])
 def test_nb_induction(oracle, boxes, key):
     O = oracle

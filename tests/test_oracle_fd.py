@@ -1,5 +1,5 @@
-"""Self-validation of the oracle for the terms the reference ships no numbers for (FS3,
-Ewald, induction): central finite differences of each term's energy against its analytic
+"""Self-validation of the oracle for the terms the reference ships no numbers for (the 2-body
+CCpol23+ term, FS3, Ewald, induction): central finite differences of each term's energy against its analytic
 COM forces, torques and rigid-scaling virial, the same identities the reference's
 validators use (initialization.f90:1093-1491, source/tests/check_fs2_periodic.py:72-84)."""
 import numpy as np
@@ -8,12 +8,14 @@ import pytest
 from ccpol23_plus_2025_mbmd_b200 import Model, data_dir
 from ccpol23_plus_2025_mbmd_b200.generator import water_box
 
-TERMS = ["self", "rspace", "kspace", "induction", "fs2", "fs3"]
+TERMS = ["vdw", "self", "rspace", "kspace", "induction", "fs2", "fs3"]
 
 
 def run_term(O, M, term, x, y, z, xs, ys, zs, box):
     st = O.State(len(x), xs.shape[1])
-    if term == "self":
+    if term == "vdw":
+        e = O.ccpol23plus(M, x, y, z, xs, ys, zs, box, st)
+    elif term == "self":
         e = O.ewald_self_correction(M, M.alpha, box, x, y, z, xs, ys, zs, st)
     elif term == "rspace":
         e = O.rspace_ewald(M, x, y, z, xs, ys, zs, box, M.alpha, st)
