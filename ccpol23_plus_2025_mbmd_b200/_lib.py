@@ -35,7 +35,8 @@ EXPORTS = [
     "ccp_context_set_timing", "ccp_context_phase_ms", "ccp_device_fma_peak",
     "ccp_kspace_ewald_fixed", "ccp_context_set_option", "ccp_context_get_option",
     "ccp_terms_device", "ccp_context_get_fs3_params", "ccp_context_set_fs3_params",
-    "ccp_context_fs3_param_grad", "ccp_ccpol23plus",
+    "ccp_context_fs3_param_grad", "ccp_ccpol23plus", "ccp_md_set_state", "ccp_md_get_state",
+    "ccp_md_nve",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
@@ -50,6 +51,11 @@ class CcpEnergies(C.Structure):
                 ("indpe", C.c_double), ("fs2pe", C.c_double), ("fs3pe", C.c_double),
                 ("vir", C.c_double), ("ind_iters", C.c_int), ("n_fs3_triples", C.c_int),
                 ("n_fs3_blend", C.c_int), ("n_fs2_triples", C.c_int), ("vdwpe", C.c_double)]
+
+
+class CcpMdStats(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("vdwpe", "cpe", "indpe", "pe3b", "pe", "tke", "rke", "te",
+                                          "sys_temp", "vir", "pres")] + [("ind_iters", C.c_int)]
 
 
 class CcpError(RuntimeError):
@@ -99,6 +105,9 @@ def lib():
     L.ccp_hot_path.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_hot_path_device.argtypes = [vp] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_ccpol23plus.argtypes = [vp] + [vp] * 6 + [i, d, pd] + [vp] * 3 + [pd]
+    L.ccp_md_set_state.argtypes = [vp, d] + [vp] * 6
+    L.ccp_md_get_state.argtypes = [vp] + [vp] * 6
+    L.ccp_md_nve.argtypes = [vp, i, d, vp]
     L.ccp_terms_device.argtypes = [vp, C.c_uint] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_context_get_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
     L.ccp_context_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]

@@ -312,6 +312,26 @@ class Context:
             dp(fzfs3), dp(idmx), dp(idmy), dp(idmz)))
         return _energies(e)
 
+    # -- NVE molecular dynamics (device-resident state) -------------------------------
+    def md_set_state(self, box, x, y, z, v, q, j):
+        """Upload a rigid-water state (COM x, y, z; velocities v (nm, 3); quaternions
+        q (nm, 4); principal-frame angular momenta j (nm, 3)) and evaluate its forces."""
+        a = [np.ascontiguousarray(t, dtype=np.float64) for t in (x, y, z, v, q, j)]
+        check(_lib.lib().ccp_md_set_state(self._h, float(box), *[ptr(t) for t in a]))
+
+    def md_get_state(self) -> dict:
+        nm = self.nm
+        out = {"x": np.zeros(nm), "y": np.zeros(nm), "z": np.zeros(nm), "v": np.zeros((nm, 3)),
+               "q": np.zeros((nm, 4)), "j": np.zeros((nm, 3))}
+        check(_lib.lib().ccp_md_get_state(self._h, *[ptr(out[k]) for k in ("x", "y", "z", "v", "q", "j")]))
+        return out
+
+    def md_nve(self, nsteps: int, dt: float) -> list:
+        """nve_1 steps on the device; per-step energies, temperature, virial, pressure."""
+        stats = (_lib.CcpMdStats * max(nsteps, 1))()
+        check(_lib.lib().ccp_md_nve(self._h, int(nsteps), float(dt), stats))
+        return [{k: getattr(s, k) for k, _ in _lib.CcpMdStats._fields_} for s in stats[:nsteps]]
+
     # -- FS3 parameters --------------------------------------------------------------
     def fs3_params(self):
         """(cs_sr, cs_lr, bgr_sr, bgr_lr): class coefficients (nclass each) and site-pair

@@ -102,6 +102,14 @@ struct ccp_context {
   double *d_sk = nullptr;
   // FS3 tables
   double *d_coef = nullptr, *d_bgr = nullptr;
+  // rigid-molecule MD state (ccp_md_*), structure of arrays on the device
+  double totm = 0, pmi[3] = {0, 0, 0};
+  double *d_pcoord = nullptr;
+  double *d_md_x = nullptr, *d_md_xs = nullptr, *d_md_v = nullptr, *d_md_q = nullptr,
+         *d_md_j = nullptr, *d_md_red = nullptr, *h_md = nullptr;
+  bool md_ready = false;
+  double md_box = 0;
+  ccp_energies md_e{};
   // ccpol23plus 2-body tables
   bool have_vdw = false;
   int vdw_nrows = 0, vdw_nv = 0;
@@ -162,6 +170,7 @@ void free_ctx(ccp_context *c) {
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
                 c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
                 c->d_gfs3,  c->d_vdw_row, c->d_vdw_site, c->d_vdw_qq, c->d_vdw_par,
+                c->d_pcoord, c->d_md_x, c->d_md_xs, c->d_md_v, c->d_md_q, c->d_md_j, c->d_md_red,
                 c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
   for (void *p : dp)
     if (p) cudaFree(p);
@@ -174,6 +183,7 @@ void free_ctx(ccp_context *c) {
   if (c->ind_graph) cudaGraphDestroy(c->ind_graph);
   if (c->d_istate) cudaFree(c->d_istate);
   if (c->d_ticket) cudaFree(c->d_ticket);
+  if (c->h_md) cudaFreeHost(c->h_md);
   if (c->d_P) cudaFree(c->d_P);
   if (c->h_istate) cudaFreeHost(c->h_istate);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
@@ -1010,6 +1020,12 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
   if (ensure_inputs(c, m->ns) != CCP_OK) return fail("inputs");
   const int cap0 = std::min(nm - 1, 192);
   if (ensure_lists(c, std::max(cap0, 1), 96 * nm, 48 * nm) != CCP_OK) return fail("lists");
+  c->totm = m->totm;
+  for (int a = 0; a < 3; a++) c->pmi[a] = m->pmi[a];
+  if (dalloc(&c->d_pcoord, m->pcoord.size()) != cudaSuccess ||
+      cudaMemcpy(c->d_pcoord, m->pcoord.data(), m->pcoord.size() * sizeof(double),
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail("principal-frame sites");
   if (m->pot_name == "ccpol23plus" && !m->vdw.empty()) {
     // parameter row of every site pair (name match in either order, first row wins, as the
     // reference's row loop), charge products, and the sites that have any row
@@ -1494,6 +1510,147 @@ int ccp_context_fs3_param_grad(ccp_context *ctx, double *dcs_sr, double *dcs_lr,
   for (int k = 0; k < 3 * 289; k++) {
     if (dbgr_sr) dbgr_sr[k] = gb[k] * kH2kcal;
     if (dbgr_lr) dbgr_lr[k] = gb[3 * 289 + k] * kH2kcal;
+  }
+  return CCP_OK;
+}
+
+// ------------------------------------------------------------- NVE molecular dynamics
+namespace {
+constexpr double kBoltz = 8.31451115e-1;  // (10 J/mol)/K
+constexpr double kPrsunt = 0.163882576;   // internal pressure unit to katm
+
+int md_alloc(ccp_context *c) {
+  if (c->d_md_x) return CCP_OK;
+  const size_t nm = c->nm;
+  CK(dalloc(&c->d_md_x, 3 * nm));
+  CK(dalloc(&c->d_md_xs, 3 * nm * (size_t)c->ns));
+  CK(dalloc(&c->d_md_v, 3 * nm));
+  CK(dalloc(&c->d_md_q, 4 * nm));
+  CK(dalloc(&c->d_md_j, 3 * nm));
+  CK(dalloc(&c->d_md_red, (size_t)3));
+  CK(cudaMallocHost((void **)&c->h_md, sizeof(double) * 13 * nm));
+  return CCP_OK;
+}
+
+// sites from the quaternions, then every term (the 2-body one too when the model has it)
+int md_forces(ccp_context *c, EvalOut &o) {
+  const size_t nm = c->nm, nsi = nm * c->ns;
+  double *x = c->d_md_x, *xs = c->d_md_xs;
+  CK(launch_md_sites(c->nm, c->ns, c->d_md_q, c->d_pcoord, xs, xs + nsi, xs + 2 * nsi,
+                     c->stream));
+  c->launches = 0;
+  int r = evaluate(c, x, x + nm, x + 2 * nm, xs, xs + nsi, xs + 2 * nsi, c->ns, c->md_box,
+                   allowed_mask(c), o);
+  if (r) return r;
+  fill_energies(c, o, c->md_box, &c->md_e);
+  return CCP_OK;
+}
+}  // namespace
+
+int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double *y,
+                     const double *z, const double *v, const double *q, const double *j) {
+  if (!ctx || !x || !y || !z || !v || !q || !j || !(box > 0.0)) return CCP_ERR_BAD_INPUT;
+  CK(cudaSetDevice(ctx->device));
+  int r = md_alloc(ctx);
+  if (r) return r;
+  const size_t nm = ctx->nm;
+  double *h = ctx->h_md;
+  for (size_t i = 0; i < nm; i++) {
+    h[i] = x[i];
+    h[nm + i] = y[i];
+    h[2 * nm + i] = z[i];
+    for (int a = 0; a < 3; a++) h[(3 + a) * nm + i] = v[3 * i + a];
+    for (int a = 0; a < 4; a++) h[(6 + a) * nm + i] = q[4 * i + a];
+    for (int a = 0; a < 3; a++) h[(10 + a) * nm + i] = j[3 * i + a];
+  }
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(ctx->d_md_x, h, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_md_v, h + 3 * nm, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_md_q, h + 6 * nm, 4 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(ctx->d_md_j, h + 10 * nm, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  ctx->md_box = box;
+  EvalOut o;
+  r = md_forces(ctx, o);
+  ctx->md_ready = r == CCP_OK;
+  return r;
+}
+
+int ccp_md_get_state(ccp_context *ctx, double *x, double *y, double *z, double *v, double *q,
+                     double *j) {
+  if (!ctx || !ctx->md_ready) {
+    set_error("ccp_md_get_state: no MD state (call ccp_md_set_state first)");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const size_t nm = ctx->nm;
+  double *h = ctx->h_md;
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(h, ctx->d_md_x, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h + 3 * nm, ctx->d_md_v, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h + 6 * nm, ctx->d_md_q, 4 * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h + 10 * nm, ctx->d_md_j, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < nm; i++) {
+    if (x) x[i] = h[i];
+    if (y) y[i] = h[nm + i];
+    if (z) z[i] = h[2 * nm + i];
+    for (int a = 0; a < 3; a++)
+      if (v) v[3 * i + a] = h[(3 + a) * nm + i];
+    for (int a = 0; a < 4; a++)
+      if (q) q[4 * i + a] = h[(6 + a) * nm + i];
+    for (int a = 0; a < 3; a++)
+      if (j) j[3 * i + a] = h[(10 + a) * nm + i];
+  }
+  return CCP_OK;
+}
+
+int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
+  if (!ctx || nsteps < 0 || !(dt > 0.0)) return CCP_ERR_BAD_INPUT;
+  if (!ctx->md_ready) {
+    set_error("ccp_md_nve: no MD state (call ccp_md_set_state first)");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const size_t nm = ctx->nm, nsi = nm * ctx->ns;
+  const int ns = ctx->ns;
+  double *x = ctx->d_md_x, *xs = ctx->d_md_xs, *v = ctx->d_md_v, *q = ctx->d_md_q,
+         *jv = ctx->d_md_j;
+  cudaStream_t st = ctx->stream;
+  const double box = ctx->md_box;
+  for (int k = 0; k < nsteps; k++) {
+    // first half kick, drift and rotation with the previous evaluation's forces
+    CK(launch_md_stage1(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
+                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, st));
+    EvalOut o;
+    int r = md_forces(ctx, o);
+    if (r) {
+      ctx->md_ready = false;
+      return r;
+    }
+    CK(launch_md_stage2(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
+                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, box,
+                        ctx->d_md_red, st));
+    CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (stats) {
+      const ccp_energies &e = ctx->md_e;
+      // md.f90:169-176 and evolve.f90:1020-1052: step energies, temperature, pressure
+      const double tke = 0.5 * ctx->totm * ctx->h_md[0], rke = 0.5 * ctx->h_md[1];
+      const double qvir = e.vir + ctx->h_md[2];
+      ccp_md_stats &S = stats[k];
+      S.vdwpe = e.vdwpe;
+      S.cpe = e.scpe + e.rcpe + e.kcpe;
+      S.indpe = e.indpe;
+      S.pe3b = e.fs2pe + e.fs3pe;
+      S.pe = S.vdwpe + S.cpe + S.indpe + S.pe3b;
+      S.tke = tke / 418.4;
+      S.rke = rke / 418.4;
+      S.te = S.tke + S.rke + S.pe;
+      S.sys_temp = 2.0 * (tke + rke) / (3.0 * kBoltz * (2.0 * ctx->nm - 1.0));
+      S.vir = qvir / 418.4;
+      S.pres = kPrsunt * (2.0 * tke - qvir) / (3.0 * box * box * box);
+      S.ind_iters = e.ind_iters;
+    }
   }
   return CCP_OK;
 }

@@ -163,6 +163,19 @@ constexpr int kVdwMaxRows = 64;
 constexpr int kFs3GradLen = 2 * 216 * 8 + 2 * 3 * 289;
 // b[0..n) += a[0..n)
 cudaError_t launch_add(int n, const double *a, double *b, cudaStream_t st);
+// NVE integrator (k_md.cu); state arrays are structures of arrays [component][nm].
+cudaError_t launch_md_stage1(int nm, int ns, const double *f, const double *fc2,
+                             const double *fc3, const double *xs, const double *ys,
+                             const double *zs, double *x, double *y, double *z, double *v,
+                             double *q, double *j, const double pmi[3], double totm, double dt,
+                             cudaStream_t st);
+cudaError_t launch_md_sites(int nm, int ns, const double *q, const double *pcoord, double *xs,
+                            double *ys, double *zs, cudaStream_t st);
+cudaError_t launch_md_stage2(int nm, int ns, const double *f, const double *fc2,
+                             const double *fc3, const double *xs, const double *ys,
+                             const double *zs, double *x, double *y, double *z, double *v,
+                             const double *q, double *j, const double pmi[3], double totm,
+                             double dt, double box, double *red, cudaStream_t st);
 // ccpol23plus 2-body term (k_vdw.cu): site forces added to f (atomics), energy and virial
 // into scal[S_VDW_E], scal[S_VDW_VIR] (internal units).
 cudaError_t launch_vdw(const double *xs, const double *ys, const double *zs, int ld,

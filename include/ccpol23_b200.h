@@ -235,6 +235,29 @@ int ccp_context_set_fs3_params(ccp_context *ctx, const double *cs_sr, const doub
 int ccp_context_fs3_param_grad(ccp_context *ctx, double *dcs_sr, double *dcs_lr, int ncoef,
                                double *dbgr_sr, double *dbgr_lr);
 
+/* --------------------------------------------------- NVE molecular dynamics (device) */
+/* The reference's rigid-molecule NVE integrator, nve_1 with the nosquish rotation
+   (evolve.f90:621-1061, 8107-8203), with the state resident on the device: centres x, y, z
+   (A), COM velocities v[3*i+a] (A/ps), unit quaternions q[4*i+a], principal-frame angular
+   momenta j[3*i+a] (amu A^2/ps).  Forces are the 2-body term (when the model is
+   ccpol23plus) plus the hot path.  ccp_md_set_state uploads a state and evaluates its forces
+   (initialization.f90:357-381); ccp_md_nve advances nsteps steps of dt ps in a fixed cubic box
+   and, when stats is not NULL, fills stats[0..nsteps-1] with each step's energies (kcal/mol),
+   temperature (K), virial (kcal/mol) and pressure (katm), as md.f90 writes them to OUTPUT.
+   Only these scalars cross PCIe per step. */
+typedef struct ccp_md_stats {
+    double vdwpe, cpe, indpe, pe3b, pe;  /* 2-body, Coulomb (self+real+reciprocal), induction,
+                                            three-body, total potential */
+    double tke, rke, te;                 /* translational, rotational, total energy */
+    double sys_temp, vir, pres;
+    int ind_iters;
+} ccp_md_stats;
+int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double *y,
+                     const double *z, const double *v, const double *q, const double *j);
+int ccp_md_get_state(ccp_context *ctx, double *x, double *y, double *z, double *v, double *q,
+                     double *j);
+int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
+
 /* ---------------------------------------------------------------- diagnostics */
 /* These have no counterpart in the reference; they serve benchmarking and profiling. */
 

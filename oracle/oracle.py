@@ -498,3 +498,176 @@ def hot_path(M, x, y, z, xs, ys, zs, box, induction=True):
     e["fs2pe"], e["fs3pe"] = threebody_term(M, x, y, z, xs, ys, zs, box, st)
     e["vir"] = st.vir.value
     return e, st
+
+
+# ------------------------------------------------------------------- NVE integration
+BOLTZ = 8.31451115e-1     # (10 J/mol)/K (utility.f90)
+PRSUNT = 0.163882576      # internal pressure unit to katm
+
+
+def force_field(M, inp_flags, pcoord, x, y, z, q, box, ld):
+    """sites + every force routine of one MD step, in nve_1's order (evolve.f90:800-877):
+    ccpol23plus (zeroes the forces and sets vir), Ewald self/real/reciprocal, nb_induction,
+    threebody_term.  Returns (xs, ys, zs, State, energies)."""
+    induction, three_body = inp_flags
+    nm = len(x)
+    xs, ys, zs = sites(pcoord, q, ld)
+    st = State(nm, ld)
+    e = {}
+    e["vdwpe"] = ccpol23plus(M, x, y, z, xs, ys, zs, box, st)
+    e["scpe"] = ewald_self_correction(M, M.alpha, box, x, y, z, xs, ys, zs, st)
+    e["rcpe"] = rspace_ewald(M, x, y, z, xs, ys, zs, box, M.alpha, st)
+    e["kcpe"] = kspace_ewald(M, x, y, z, xs, ys, zs, M.kmax1, M.kmax2, M.kmax3, M.alpha, box, st)
+    e["indpe"] = 0.0
+    if induction:
+        e["indpe"], status, _ = nb_induction(M, x, y, z, xs, ys, zs, box, st)
+        assert status == 0
+    e["fs2pe"] = e["fs3pe"] = 0.0
+    if three_body:
+        e["fs2pe"], e["fs3pe"] = threebody_term(M, x, y, z, xs, ys, zs, box, st)
+    return xs, ys, zs, st, e
+
+
+def _com_force_torque(st, xs, ys, zs, ns, three_body):
+    """evolve.f90:664-704: per-molecule force and torque from the site forces (plus the
+    three-body COM forces), and the site-site to molecule-molecule virial correction."""
+    fxs, fys, fzs = st.fxs[:, :ns], st.fys[:, :ns], st.fzs[:, :ns]
+    sx, sy, sz = xs[:, :ns], ys[:, :ns], zs[:, :ns]
+    nm = fxs.shape[0]
+    F = np.zeros((nm, 3))
+    T = np.zeros((nm, 3))
+    lvir = 0.0
+    for i in range(nm):
+        qf = [0.0, 0.0, 0.0]
+        qt = [0.0, 0.0, 0.0]
+        for s in range(ns):
+            qf[0] += fxs[i, s]
+            qf[1] += fys[i, s]
+            qf[2] += fzs[i, s]
+            qt[0] += sy[i, s] * fzs[i, s] - sz[i, s] * fys[i, s]
+            qt[1] += sz[i, s] * fxs[i, s] - sx[i, s] * fzs[i, s]
+            qt[2] += sx[i, s] * fys[i, s] - sy[i, s] * fxs[i, s]
+            lvir += fxs[i, s] * sx[i, s] + fys[i, s] * sy[i, s] + fzs[i, s] * sz[i, s]
+        F[i] = qf
+        T[i] = qt
+        if three_body:
+            F[i, 0] += st.fxfs2[i] + st.fxfs3[i]
+            F[i, 1] += st.fyfs2[i] + st.fyfs3[i]
+            F[i, 2] += st.fzfs2[i] + st.fzfs3[i]
+    return F, T, lvir
+
+
+def _quat_torque_and_momenta(q, T, J):
+    """Principal-frame torque, quaternion torque and quaternion momenta (evolve.f90:712-741)."""
+    q0, q1, q2, q3 = q
+    r = quat_to_rot(q0, q1, q2, q3)
+    tqx = T[0] * r[0] + T[1] * r[3] + T[2] * r[6]
+    tqy = T[0] * r[1] + T[1] * r[4] + T[2] * r[7]
+    tqz = T[0] * r[2] + T[1] * r[5] + T[2] * r[8]
+    qt = [2.0 * (-q1 * tqx - q2 * tqy - q3 * tqz), 2.0 * (q0 * tqx - q3 * tqy + q2 * tqz),
+          2.0 * (q3 * tqx + q0 * tqy - q1 * tqz), 2.0 * (-q2 * tqx + q1 * tqy + q0 * tqz)]
+    ox, oy, oz = J
+    p = [2.0 * (-q1 * ox - q2 * oy - q3 * oz), 2.0 * (q0 * ox - q3 * oy + q2 * oz),
+         2.0 * (q3 * ox + q0 * oy - q1 * oz), 2.0 * (-q2 * ox + q1 * oy + q0 * oz)]
+    return qt, p
+
+
+def _momenta_to_j(q, p):
+    q0, q1, q2, q3 = q
+    return [0.5 * (-q1 * p[0] + q0 * p[1] + q3 * p[2] - q2 * p[3]),
+            0.5 * (-q2 * p[0] - q3 * p[1] + q0 * p[2] + q1 * p[3]),
+            0.5 * (-q3 * p[0] + q2 * p[1] - q1 * p[2] + q0 * p[3])]
+
+
+def nosquish(tstep, q, p, pmi):
+    """evolve.f90:8107-8203: free rotation of a rigid body by symplectic splitting, 10
+    sub-steps of z/2, y/2, x, y/2, z/2 rotations."""
+    qq0, qq1, qq2, qq3 = q
+    pp0, pp1, pp2, pp3 = p
+    mrot = 10
+    ov4, ov8 = 0.25, 0.125
+    trstep = tstep / float(mrot)
+    for _ in range(mrot):
+        zetaz = ov8 / pmi[2] * trstep * (-pp0 * qq3 + pp1 * qq2 - pp2 * qq1 + pp3 * qq0)
+        cs, sn = np.cos(zetaz), np.sin(zetaz)
+        qn1 = [cs * qq0 - sn * qq3, cs * qq1 + sn * qq2, cs * qq2 - sn * qq1, cs * qq3 + sn * qq0]
+        pq2 = [cs * pp0 - sn * pp3, cs * pp1 + sn * pp2, cs * pp2 - sn * pp1, cs * pp3 + sn * pp0]
+        zetay = ov8 / pmi[1] * trstep * (-pq2[0] * qn1[2] - pq2[1] * qn1[3] + pq2[2] * qn1[0] + pq2[3] * qn1[1])
+        cs, sn = np.cos(zetay), np.sin(zetay)
+        qn2 = [cs * qn1[0] - sn * qn1[2], cs * qn1[1] - sn * qn1[3], cs * qn1[2] + sn * qn1[0], cs * qn1[3] + sn * qn1[1]]
+        pq3 = [cs * pq2[0] - sn * pq2[2], cs * pq2[1] - sn * pq2[3], cs * pq2[2] + sn * pq2[0], cs * pq2[3] + sn * pq2[1]]
+        zetax = ov4 / pmi[0] * trstep * (-pq3[0] * qn2[1] + pq3[1] * qn2[0] + pq3[2] * qn2[3] - pq3[3] * qn2[2])
+        cs, sn = np.cos(zetax), np.sin(zetax)
+        qn3 = [cs * qn2[0] - sn * qn2[1], cs * qn2[1] + sn * qn2[0], cs * qn2[2] + sn * qn2[3], cs * qn2[3] - sn * qn2[2]]
+        pq4 = [cs * pq3[0] - sn * pq3[1], cs * pq3[1] + sn * pq3[0], cs * pq3[2] + sn * pq3[3], cs * pq3[3] - sn * pq3[2]]
+        zetay = ov8 / pmi[1] * trstep * (-pq4[0] * qn3[2] - pq4[1] * qn3[3] + pq4[2] * qn3[0] + pq4[3] * qn3[1])
+        cs, sn = np.cos(zetay), np.sin(zetay)
+        qn2 = [cs * qn3[0] - sn * qn3[2], cs * qn3[1] - sn * qn3[3], cs * qn3[2] + sn * qn3[0], cs * qn3[3] + sn * qn3[1]]
+        pq3 = [cs * pq4[0] - sn * pq4[2], cs * pq4[1] - sn * pq4[3], cs * pq4[2] + sn * pq4[0], cs * pq4[3] + sn * pq4[1]]
+        zetaz = ov8 / pmi[2] * trstep * (-pq3[0] * qn2[3] + pq3[1] * qn2[2] - pq3[2] * qn2[1] + pq3[3] * qn2[0])
+        cs, sn = np.cos(zetaz), np.sin(zetaz)
+        qq0, qq1, qq2, qq3 = (cs * qn2[0] - sn * qn2[3], cs * qn2[1] + sn * qn2[2],
+                              cs * qn2[2] - sn * qn2[1], cs * qn2[3] + sn * qn2[0])
+        pp0, pp1, pp2, pp3 = (cs * pq3[0] - sn * pq3[3], cs * pq3[1] + sn * pq3[2],
+                              cs * pq3[2] - sn * pq3[1], cs * pq3[3] + sn * pq3[0])
+    return [qq0, qq1, qq2, qq3], [pp0, pp1, pp2, pp3]
+
+
+class MDState:
+    """Rigid-water MD state of the reference's NVE integrator: COM positions x, y, z (A),
+    COM velocities v (nm, 3) (A/ps), unit quaternions q (nm, 4), principal-frame angular
+    momenta j (nm, 3) (amu A^2/ps)."""
+
+    def __init__(self, x, y, z, v, q, j):
+        self.x, self.y, self.z = (np.array(a, dtype=np.float64) for a in (x, y, z))
+        self.v = np.array(v, dtype=np.float64)
+        self.q = np.array(q, dtype=np.float64)
+        self.j = np.array(j, dtype=np.float64)
+
+
+def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld):
+    """nve_1 (evolve.f90:621-1061) for nsteps steps with the oracle's forces, starting from
+    a force evaluation at the initial state (initialization.f90:357-381).  Returns the per-step
+    energies (kcal/mol: vdw, coul, ind, 3b, pe, ke, te; temperature; virial, pressure)."""
+    nm = len(s.x)
+    ns = pcoord.shape[0]
+    three_body = flags[1]
+    xs, ys, zs, st, e = force_field(M, flags, pcoord, s.x, s.y, s.z, s.q, box, ld)
+    out = []
+    for _ in range(nsteps):
+        F, T, _ = _com_force_torque(st, xs, ys, zs, ns, three_body)
+        P = np.zeros((nm, 4))
+        for i in range(nm):
+            qt, p = _quat_torque_and_momenta(s.q[i], T[i], s.j[i])
+            P[i] = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
+            s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
+        s.x = s.x + dt * s.v[:, 0]
+        s.y = s.y + dt * s.v[:, 1]
+        s.z = s.z + dt * s.v[:, 2]
+        for i in range(nm):
+            qn, pn = nosquish(dt, list(s.q[i]), list(P[i]), pmi)
+            s.q[i] = qn
+            s.j[i] = _momenta_to_j(qn, pn)
+        xs, ys, zs, st, e = force_field(M, flags, pcoord, s.x, s.y, s.z, s.q, box, ld)
+        F, T, lvir = _com_force_torque(st, xs, ys, zs, ns, three_body)
+        for i in range(nm):
+            qt, p = _quat_torque_and_momenta(s.q[i], T[i], s.j[i])
+            p = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
+            s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
+            s.j[i] = _momenta_to_j(s.q[i], p)
+        s.x = s.x - box * np.round(s.x / box)
+        s.y = s.y - box * np.round(s.y / box)
+        s.z = s.z - box * np.round(s.z / box)
+        tke = 0.5 * totm * float(np.sum(s.v[:, 0] ** 2 + s.v[:, 1] ** 2 + s.v[:, 2] ** 2))
+        rke = 0.5 * float(np.sum(s.j[:, 0] ** 2 / pmi[0] + s.j[:, 1] ** 2 / pmi[1] + s.j[:, 2] ** 2 / pmi[2]))
+        cpe = e["scpe"] + e["rcpe"] + e["kcpe"]
+        pe3 = e["fs2pe"] + e["fs3pe"]
+        pe = e["vdwpe"] + cpe + e["indpe"] + pe3
+        ke = tke / 418.4 + rke / 418.4
+        qvir = st.vir.value + lvir
+        out.append({"vdwpe": e["vdwpe"], "cpe": cpe, "indpe": e["indpe"], "pe3b": pe3, "pe": pe,
+                    "tke": tke / 418.4, "rke": rke / 418.4, "te": ke + pe,
+                    "sys_temp": 2.0 * (tke + rke) / (3.0 * BOLTZ * (2.0 * nm - 1.0)),
+                    "vir": qvir / 418.4,
+                    "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * box ** 3)})
+    return out

@@ -1,0 +1,61 @@
+"""The device NVE integrator (nve_1 + nosquish, evolve.f90:621-1061, 8107-8203) against the
+oracle's step-by-step restatement of the same integrator with the oracle's forces: state and
+per-step energies after a few steps of a 37-water FS2+FS3 box."""
+import numpy as np
+import pytest
+
+from ccpol23_plus_2025_mbmd_b200 import Context, Model, data_dir
+from ccpol23_plus_2025_mbmd_b200.generator import water_box
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.0005   # ps, as the benchmark configurations
+NSTEPS = 3
+
+
+@pytest.fixture(scope="module")
+def md_case(product, oracle):
+    O = oracle
+    m = Model(data_dir("fs2fs3"))
+    b = water_box(m, 37, 10.37, 9)
+    inp = O.read_inputs(data_dir("fs2fs3"))
+    pcoord, pmi, totm = O.principal_frame(inp)
+    M = O.make_model(inp, b.nm, b.box)
+    s = O.MDState(b.x, b.y, b.z, b.v, b.q, b.jb)
+    ref = O.nve_run(M, (True, True), pcoord, pmi, totm, s, b.box, DT, NSTEPS, b.xs.shape[1])
+    return m, b, s, ref
+
+
+def test_nve_matches_oracle_integrator(md_case):
+    m, b, s_ref, ref = md_case
+    with Context(m, b.nm, b.box) as c:
+        c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
+        stats = c.md_nve(NSTEPS, DT)
+        st = c.md_get_state()
+    for k, (g, o) in enumerate(zip(stats, ref)):
+        for key in ("vdwpe", "cpe", "indpe", "pe3b", "pe", "tke", "rke", "te", "vir"):
+            assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1.0), (k, key, g[key], o[key])
+        assert g["sys_temp"] == pytest.approx(o["sys_temp"], rel=1e-9)
+        assert g["pres"] == pytest.approx(o["pres"], rel=1e-8, abs=1e-9)
+    assert rel(np.stack([st["x"], st["y"], st["z"]]), np.stack([s_ref.x, s_ref.y, s_ref.z])) <= 1e-12
+    assert rel(st["v"], s_ref.v) <= 1e-9
+    assert rel(st["q"], s_ref.q) <= 1e-12
+    assert rel(st["j"], s_ref.j) <= 1e-9
+
+
+def test_nve_continues_across_calls(md_case):
+    """Two calls of one step each equal one call of two steps (the forces of the last
+    evaluation stay on the device between calls)."""
+    m, b, _, _ = md_case
+    out = []
+    for split in ((2,), (1, 1)):
+        with Context(m, b.nm, b.box) as c:
+            c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
+            stats = []
+            for n in split:
+                stats += c.md_nve(n, DT)
+            out.append((stats[-1]["te"], c.md_get_state()))
+    assert out[0][0] == pytest.approx(out[1][0], rel=1e-12)
+    assert rel(out[0][1]["v"], out[1][1]["v"]) <= 1e-12
