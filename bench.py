@@ -266,6 +266,57 @@ def run_single(which, host_loop=False):
                               "n_fs2_triples": e["n_fs2_triples"]}), flush=True)
 
 
+def equilibrate(ctx, box, nsteps, temp=298.0, every=20):
+    """Velocity-rescaled MD from the synthetic start (its jittered lattice is far from
+    equilibrium): every `every` steps the COM velocities and angular momenta are scaled to
+    the target temperature.  Returns the state."""
+    ctx.md_set_state(box.box, box.x, box.y, box.z, box.v, box.q, box.jb)
+    for _ in range(max(nsteps // every, 0)):
+        st = ctx.md_nve(every, DT_PS)
+        f = np.sqrt(temp / st[-1]["sys_temp"])
+        s = ctx.md_get_state()
+        ctx.md_set_state(box.box, s["x"], s["y"], s["z"], s["v"] * f, s["q"], s["j"] * f)
+    return ctx.md_get_state()
+
+
+def run_nve(nsteps, nequil):
+    """Rigid-water NVE MD on the device (2-body + hot path + nve_1), FP64 and mixed forms from
+    the same equilibrated state: time per MD step and the energy drift (linear fit of the
+    total energy, kcal/mol per ns).  Prints one JSON line; not the headline metric."""
+    import torch
+    from ccpol23_plus_2025_mbmd_b200 import Context
+    model, box, cfg = build_inputs(0)
+    with Context(model, box.nm, box.box, device=0) as ctx:
+        s0 = equilibrate(ctx, box, nequil)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with Context(model, box.nm, box.box, device=0, precision=prec) as ctx:
+            ctx.md_set_state(box.box, s0["x"], s0["y"], s0["z"], s0["v"], s0["q"], s0["j"])
+            ctx.md_nve(5, DT_PS)  # warm-up: list sizes, graphs
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = ctx.md_nve(nsteps, DT_PS)
+            wall = time.perf_counter() - t0
+        te = np.array([s["te"] for s in st])
+        t_ns = np.arange(1, nsteps + 1) * DT_PS * 1e-3
+        slope = float(np.polyfit(t_ns, te, 1)[0]) if nsteps > 1 else 0.0
+        out[prec] = {"ms_per_md_step": wall / nsteps * 1e3,
+                     "ns_day": ns_per_day(nsteps / wall),
+                     "drift_kcal_mol_per_ns": slope,
+                     "drift_per_molecule_kcal_mol_per_ns": slope / box.nm,
+                     "te_first": float(te[0]), "te_last": float(te[-1]),
+                     "te_rms_fluct": float(np.std(te)),
+                     "temp_mean_K": float(np.mean([s["sys_temp"] for s in st]))}
+    line = {"metric": "NVE MD, 512 H2O FS2+FS3 (2-body + hot path + nve_1 integrator)",
+            "steps": nsteps, "dt_ps": DT_PS, "wall_clock_timed": True,
+            "equilibration": f"{nequil} steps, velocities rescaled to 298 K every 20 steps, FP64",
+            "config": {"nm": box.nm, "box_A": box.box, "variant": cfg["variant"], "seed": cfg["seed"]},
+            "fp64": out["fp64"], "mixed": out["mixed"],
+            "drift_ratio_mixed_over_fp64": (abs(out["mixed"]["drift_kcal_mol_per_ns"]) /
+                                             max(abs(out["fp64"]["drift_kcal_mol_per_ns"]), 1e-30))}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -276,6 +327,10 @@ def main():
     ap.add_argument("--single", choices=["fp64", "mixed", "both"],
                     help="three device-resident evaluations per form, phase times of the last "
                          "(profiling; no timing loop)")
+    ap.add_argument("--nve", type=int, default=0, metavar="STEPS",
+                    help="run STEPS NVE MD steps per form and print the drift line instead")
+    ap.add_argument("--nve-equil", type=int, default=4000, metavar="STEPS",
+                    help="velocity-rescaled equilibration steps before the NVE run")
     ap.add_argument("--host-loop", action="store_true",
                     help="with --single: drive the dipole iteration from the host, so that "
                          "profilers see its kernels")
@@ -285,6 +340,9 @@ def main():
         return
     if args.single:
         run_single(args.single, args.host_loop)
+        return
+    if args.nve:
+        run_nve(args.nve, args.nve_equil)
         return
     import torch
     rank, world, local = dist_env()
