@@ -140,13 +140,14 @@ struct ccp_context {
   unsigned *d_ticket = nullptr;  // last-block ticket of the fused update kernel
   int ind_per_iter = 0;          // kernels per Jacobi iteration of the last solve
   std::vector<long long> ind_key;
-  // phase matrix P[polarisable site][k] of the dipole iteration (when it fits kPhaseBudget)
+  // phase factors of the polarisable sites for the dipole iteration (k_iter.cu), when they
+  // fit kPhaseBudget: XY[site][l][m] then Z[site][n]
   double2 *d_P = nullptr;
   size_t P_cap = 0;
   bool use_P = false;
   // options (ccp_context_set_option)
   int opt_graph = 1;  // Jacobi loop as a conditional graph (1) or driven from the host (0)
-  int opt_phase = 1;  // phase matrix when it fits (1) or never (0)
+  int opt_phase = 1;  // phase-factor tables when they fit (1) or never (0)
   // phase timing (diagnostics)
   bool timing = false;
   cudaEvent_t ev[2 * CCP_NPHASE] = {};  // start/end of each phase, on the phase's stream
@@ -315,13 +316,13 @@ struct EvalOut {
   bool converged = true;
 };
 
-// Largest phase matrix kept for the dipole iteration: it is re-read twice per iteration, so
-// it pays only while it stays resident in the 126 MB L2 next to the other working arrays.
-constexpr size_t kPhaseBudget = size_t(64) << 20;
+// Largest phase-factor tables kept for the dipole iteration (nlm + nz complex numbers per
+// polarisable site: 5 MB at 512 waters, 46 MB at 2048).
+constexpr size_t kPhaseBudget = size_t(1) << 30;
 
 constexpr double kIndThr = 1.0e-20;  // iteridm convergence threshold on sum |dmu|^2
 
-// Enqueues one Jacobi step: with the phase matrix two kernels (k_iter.cu), otherwise T.mu,
+// Enqueues one Jacobi step: with the phase factors two kernels (k_iter.cu), otherwise T.mu,
 // the tiled dipole structure factors and reciprocal field, the update and the convergence
 // node.  `handle` is used only when use_graph is set.
 cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphConditionalHandle handle,
@@ -343,7 +344,12 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
     A.e0 = c->d_e0tot;
     A.kv = c->d_kv;
     A.nk = c->nk;
-    A.P = c->d_P;
+    A.mmax = c->kmax[1];
+    A.nmax = c->kmax[2];
+    A.nlm = (c->kmax[0] + 1) * (2 * c->kmax[1] + 1);
+    A.nz = 2 * c->kmax[2] + 1;
+    A.XY = c->d_P;
+    A.Z = c->d_P + (size_t)A.nw * A.nlm;
     A.sk = c->d_sk;
     A.scal = c->d_scal;
     A.state = c->d_istate;
@@ -440,9 +446,10 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
   return CCP_OK;
 }
 
-// Allocates the phase matrix when the dipole iteration can use it.
+// Allocates the phase-factor tables when the dipole iteration can use them.
 int ensure_phase_matrix(ccp_context *c) {
-  const size_t n = (size_t)c->nm * c->S.np * c->nk;
+  const size_t n = (size_t)c->nm * c->S.np *
+                   ((size_t)(c->kmax[0] + 1) * (2 * c->kmax[1] + 1) + 2 * c->kmax[2] + 1);
   c->use_P = c->opt_phase && c->nk > 0 && n * sizeof(double2) <= kPhaseBudget;
   if (!c->use_P || n <= c->P_cap) return CCP_OK;
   if (c->d_P) cudaFree(c->d_P);
@@ -620,8 +627,9 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
                              sm));
       if (c->use_P)
-        LK(launch_phase_matrix(c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                               c->d_P, sm));
+        LK(launch_phase_factors(c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2], c->d_P,
+                                c->d_P + (size_t)nm * S.np * (c->kmax[0] + 1) * (2 * c->kmax[1] + 1),
+                                sm));
       pend(3, sm);
       pbeg(4, sm);
       {

@@ -141,7 +141,9 @@ struct IterArgs {
   const double *e0;
   const KVec *kv;
   int nk;
-  const double2 *P;
+  const double2 *XY;  // [nw][nlm] exp(i(l x + m y)), lm = l (2 mmax + 1) + m + mmax
+  const double2 *Z;   // [nw][nz] exp(i n z) (conjugated for n < 0), nz = 2 nmax + 1
+  int nlm, nz, mmax, nmax;
   double *sk, *scal, *state;  // state = {iterations, change, energy}
   unsigned *ticket;
   double thr;
@@ -210,8 +212,8 @@ cudaError_t launch_static_total(int n, const double *a, const double *b, const d
 cudaError_t launch_dip_cond(cudaGraphConditionalHandle h, int use_graph, double *scal,
                             double *state, double thr, int maxit, cudaStream_t st);
 // k_iter.cu
-cudaError_t launch_phase_matrix(const KVec *kv, int nk, const double2 *tab, int nm, SiteSets S,
-                                int kl, int km, int kn, double2 *P, cudaStream_t st);
+cudaError_t launch_phase_factors(const double2 *tab, int nm, SiteSets S, int kl, int km, int kn,
+                                 double2 *XY, double2 *Z, cudaStream_t st);
 cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np, const double4 *T4,
                        const double *TB, const double4 *S4, const double *SB, const double *mu,
                        double *eim, cudaStream_t st);

@@ -3,12 +3,14 @@
 // iteridm (nb_induction_model.f90:1193-1407) updates every polarisable dipole from the field
 //   E = T.mu (real space + short-range + intramolecular)  +  E_k(mu) (reciprocal)  +  E0.
 // The geometry is fixed during the solve, so besides the dipole tensors (k_induction.cu) the
-// phases exp(i k.r_s) of every (polarisable site s, k-vector) pair are computed once per
-// evaluation into a matrix P[s][k] (k fastest) when it fits the L2-sized budget.  Each
-// iteration then is
+// phases exp(i k.r_s) of the polarisable sites are prepared once per evaluation, factored as
+// exp(i(l x + m y)) for every (l, m) and exp(i n z) for every n of each site (the product
+// order of the reference's recurrence, ewald.f90:960-1010): a (site, k-vector) phase is then
+// one complex product of two table entries, and the tables (nlm + nz per site) stay in L2
+// where the full (site, k) matrix would not.  Each iteration then is
 //   A  blocks [0, nA):  T.mu, one warp per polarisable site, lanes over its (neighbour, site)
 //                       tensor entries (contiguous, so the loads coalesce);
-//      blocks [nA, ..): dipole structure factors S(k) = sum_s (k.mu_s) P[s][k], one thread
+//      blocks [nA, ..): dipole structure factors S(k) = sum_s (k.mu_s) e^{ik.r_s}, one thread
 //                       per k over a chunk of sites, merged with FP64 atomics;
 //   B  one warp per polarisable site: reciprocal field sum_k k g(k, s) (lanes over k), the
 //      update mu' = alpha (E_real + E_k + E0) in place, the |mu - mu'|^2 and energy sums;
@@ -26,44 +28,47 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kSumSites = 32;     // polarisable sites per structure-factor block
 constexpr int kGatherSites = 4;  // polarisable sites per gather/update block
 
-// exp(i k.r) from the per-axis phase tables tab[axis][l][site], in the same product order as
-// the tiled reciprocal-space kernels (ewald.f90:960-1010).
-__device__ __forceinline__ double2 phase_at(const double2 *__restrict__ tab, size_t N, int k1,
-                                            size_t t, int l, int m, int n) {
-  const double2 el = tab[(size_t)(0 * k1 + l) * N + t];
-  const double2 em = tab[(size_t)(1 * k1 + (m < 0 ? -m : m)) * N + t];
-  const double2 en = tab[(size_t)(2 * k1 + (n < 0 ? -n : n)) * N + t];
-  double clm, slm;
-  if (m >= 0) {
-    clm = el.x * em.x - el.y * em.y;
-    slm = el.y * em.x + em.y * el.x;
-  } else {
-    clm = el.x * em.x + el.y * em.y;
-    slm = el.y * em.x - em.y * el.x;
-  }
-  double c, s;
-  if (n >= 0) {
-    c = clm * en.x - slm * en.y;
-    s = slm * en.x + clm * en.y;
-  } else {
-    c = clm * en.x + slm * en.y;
-    s = slm * en.x - clm * en.y;
-  }
-  return make_double2(c, s);
-}
-
-__global__ void k_phase_matrix(const KVec *__restrict__ kv, int nk, const double2 *__restrict__ tab,
-                               int nm, SiteSets S, int k1, double2 *P) {
-  const size_t total = (size_t)nm * S.np * nk;
+// Phase factors of polarisable site w from the per-axis tables tab[axis][l][site] (ewald.f90:
+// 960-1010): XY[w][l][m] = exp(i l x) exp(+-i |m| y) in the reference's product order, and
+// Z[w][n] = exp(i |n| z), conjugated for n < 0, so that the phase of k = (l, m, n) is
+// XY[l][m] * Z[n] exactly as the reference's final product.
+__global__ void k_phase_factors(const double2 *__restrict__ tab, int nm, SiteSets S, int k1,
+                                int lmax, int mmax, int nmax, double2 *XY, double2 *Z) {
+  const int nw = nm * S.np;
+  const int M = 2 * mmax + 1, nlm = (lmax + 1) * M, nz = 2 * nmax + 1;
   const size_t N = (size_t)nm * S.na;
+  const size_t total = (size_t)nw * (nlm + nz);
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
        t += (size_t)gridDim.x * blockDim.x) {
-    const size_t s = t / nk;
-    const int k = (int)(t - s * nk);
-    const int i = (int)(s / S.np), p = (int)(s % S.np);
-    const KVec K = kv[k];
-    P[t] = phase_at(tab, N, k1, (size_t)i * S.na + S.a_of_p[p], K.l, K.m, K.n);
+    const int w = (int)(t / (nlm + nz)), u = (int)(t - (size_t)w * (nlm + nz));
+    const int i = w / S.np, p = w % S.np;
+    const size_t st = (size_t)i * S.na + S.a_of_p[p];
+    if (u < nlm) {
+      const int l = u / M, m = u % M - mmax;
+      const double2 el = tab[(size_t)(0 * k1 + l) * N + st];
+      const double2 em = tab[(size_t)(1 * k1 + (m < 0 ? -m : m)) * N + st];
+      double clm, slm;
+      if (m >= 0) {
+        clm = el.x * em.x - el.y * em.y;
+        slm = el.y * em.x + em.y * el.x;
+      } else {
+        clm = el.x * em.x + el.y * em.y;
+        slm = el.y * em.x - em.y * el.x;
+      }
+      XY[(size_t)w * nlm + u] = make_double2(clm, slm);
+    } else {
+      const int n = u - nlm - nmax;
+      const double2 en = tab[(size_t)(2 * k1 + (n < 0 ? -n : n)) * N + st];
+      Z[(size_t)w * nz + (u - nlm)] = make_double2(en.x, n < 0 ? -en.y : en.y);
+    }
   }
+}
+
+// phase of k = (l, m, n) at site w from its factor rows
+__device__ __forceinline__ double2 kphase(const double2 *__restrict__ xyw,
+                                          const double2 *__restrict__ zw, int lm, int ni) {
+  const double2 a = xyw[lm], b = zw[ni];
+  return make_double2(a.x * b.x - a.y * b.y, a.y * b.x + a.x * b.y);
 }
 
 // T.mu of polarisable site w = (i, p): entries T4/TB[i][p][n][q] for the neighbours n of i and
@@ -156,11 +161,11 @@ __global__ void __launch_bounds__(kThreads)
   const int k = kt * kThreads + threadIdx.x;
   if (k >= A.nk) return;
   const KVec K = A.kv[k];
+  const int lm = K.l * (2 * A.mmax + 1) + K.m + A.mmax, ni = K.n + A.nmax;
   double a0 = 0.0, a1 = 0.0;
-  const double2 *Pk = A.P + (size_t)s0 * A.nk + k;
 #pragma unroll 4
   for (int s = 0; s < cnt; s++) {
-    const double2 ph = Pk[(size_t)s * A.nk];
+    const double2 ph = kphase(A.XY + (size_t)(s0 + s) * A.nlm, A.Z + (size_t)(s0 + s) * A.nz, lm, ni);
     const double dk = K.rl * smu[3 * s] + K.rm * smu[3 * s + 1] + K.rn * smu[3 * s + 2];
     a0 += dk * ph.x;
     a1 += dk * ph.y;
@@ -179,17 +184,18 @@ __global__ void __launch_bounds__(kThreads)
   double acc[kGatherSites][3];
 #pragma unroll
   for (int g = 0; g < kGatherSites; g++) acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
-  const double2 *P0 = A.P + (size_t)w0 * A.nk;
 #pragma unroll 2
   for (int k = threadIdx.x; k < A.nk; k += kThreads) {
     const KVec K = A.kv[k];
+    const int lm = K.l * (2 * A.mmax + 1) + K.m + A.mmax, ni = K.n + A.nmax;
     // kspace_efield_idm gather (nb_induction_model.f90:2560-2600): g = -4 a_k (c S_re + s S_im)
     const double f0 = -4.0 * K.ak * A.sk[(size_t)k * 4];
     const double f1 = -4.0 * K.ak * A.sk[(size_t)k * 4 + 1];
 #pragma unroll
     for (int g = 0; g < kGatherSites; g++) {
       if (g < ns_blk) {
-        const double2 ph = P0[(size_t)g * A.nk + k];
+        const double2 ph = kphase(A.XY + (size_t)(w0 + g) * A.nlm, A.Z + (size_t)(w0 + g) * A.nz,
+                                  lm, ni);
         const double t = ph.x * f0 + ph.y * f1;
         acc[g][0] += K.rl * t;
         acc[g][1] += K.rm * t;
@@ -256,16 +262,16 @@ __global__ void __launch_bounds__(kThreads)
 
 }  // namespace
 
-cudaError_t launch_phase_matrix(const KVec *kv, int nk, const double2 *tab, int nm, SiteSets S,
-                                int kl, int km, int kn, double2 *P, cudaStream_t st) {
+cudaError_t launch_phase_factors(const double2 *tab, int nm, SiteSets S, int kl, int km, int kn,
+                                 double2 *XY, double2 *Z, cudaStream_t st) {
   int k1 = kl > km ? kl : km;
   k1 = (k1 > kn ? k1 : kn) + 1;
   if (k1 < 2) k1 = 2;
-  const size_t total = (size_t)nm * S.np * nk;
+  const size_t total = (size_t)nm * S.np * ((size_t)(kl + 1) * (2 * km + 1) + 2 * kn + 1);
   if (total == 0) return cudaSuccess;
   size_t blocks = (total + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
-  k_phase_matrix<<<(unsigned)blocks, 256, 0, st>>>(kv, nk, tab, nm, S, k1, P);
+  k_phase_factors<<<(unsigned)blocks, 256, 0, st>>>(tab, nm, S, k1, kl, km, kn, XY, Z);
   return cudaGetLastError();
 }
 

@@ -268,7 +268,7 @@ int ccp_context_last_launches(const ccp_context *ctx, int *launches);
    phases; ccp_context_phase_ms then returns the durations (ms) of the last evaluation:
    [0] input packing + neighbour list, [1] Ewald real space + static field (real) +
    intramolecular terms, [2] Ewald reciprocal space, [3] induction set-up (static reciprocal
-   field, dipole tensors, phase matrix), [4] dipole iteration, [5] induction forces,
+   field, dipole tensors, phase factors), [4] dipole iteration, [5] induction forces,
    [6] FS2, [7] FS3 triple list, [8] FS3 kernel, [9] 2-body term. */
 #define CCP_NPHASE 10
 int ccp_context_set_timing(ccp_context *ctx, int on);
@@ -285,8 +285,9 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
      "fs3_triples_per_block"  8 (default): FS3 triples per block when overlapping, so that
                      blocks retire often (0: one persistent wave of blocks);
      "fs3_param_grad" 0 (default): see ccp_context_fs3_param_grad;
-     "phase_matrix"  1 (default): the per-(polarisable site, k-vector) phases are tabulated
-                     once per evaluation when the table is at most 64 MiB; 0: never (the
+     "phase_matrix"  1 (default): the polarisable sites' phases are tabulated once per
+                     evaluation as exp(i(l x + m y)) and exp(i n z) factors (when they take at
+                     most 1 GiB), so a (site, k) phase is one complex product; 0: never (the
                      tiled on-the-fly reciprocal kernels run every iteration).
    ccp_context_get_option also reports "phase_matrix_active" (whether the last evaluation
    used the table). */

@@ -131,7 +131,9 @@ def test_linear_coefficient_gradient_reproduces_energy(setup):
     g_sr, g_lr, _, _ = ctx.fs3_param_grad()
     cs_sr, cs_lr, _, _ = ctx.fs3_params()
     lin = float(np.dot(cs_sr, g_sr) + np.dot(cs_lr, g_lr))
-    assert abs(lin - e["fs3pe"]) <= 1e-10 * abs(e["fs3pe"]), (lin, e["fs3pe"])
+    # both sides are sums with heavy cancellation (sum |c g| / |sum c g| ~ 1e5), accumulated
+    # in different orders with FP64 atomics: agreement is bounded by ~1e-16 x 1e5 x terms
+    assert abs(lin - e["fs3pe"]) <= 1e-9 * abs(e["fs3pe"]), (lin, e["fs3pe"])
     ctx.set_option("fs3_param_grad", 0)
 
 
