@@ -36,7 +36,7 @@ EXPORTS = [
     "ccp_kspace_ewald_fixed", "ccp_context_set_option", "ccp_context_get_option",
     "ccp_terms_device", "ccp_context_get_fs3_params", "ccp_context_set_fs3_params",
     "ccp_context_fs3_param_grad", "ccp_ccpol23plus", "ccp_md_set_state", "ccp_md_get_state",
-    "ccp_md_nve",
+    "ccp_md_nve", "ccp_md_get_dipoles",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
@@ -108,6 +108,7 @@ def lib():
     L.ccp_md_set_state.argtypes = [vp, d] + [vp] * 6
     L.ccp_md_get_state.argtypes = [vp] + [vp] * 6
     L.ccp_md_nve.argtypes = [vp, i, d, vp]
+    L.ccp_md_get_dipoles.argtypes = [vp, i, vp, vp, vp]
     L.ccp_terms_device.argtypes = [vp, C.c_uint] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_context_get_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
     L.ccp_context_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]

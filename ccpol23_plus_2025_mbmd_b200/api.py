@@ -326,6 +326,13 @@ class Context:
         check(_lib.lib().ccp_md_get_state(self._h, *[ptr(out[k]) for k in ("x", "y", "z", "v", "q", "j")]))
         return out
 
+    def md_dipoles(self):
+        """Induced dipoles (nm, ns) x 3 of the current MD state."""
+        ns = self.model.ns
+        out = [np.zeros((self.nm, ns)) for _ in range(3)]
+        check(_lib.lib().ccp_md_get_dipoles(self._h, ns, *[ptr(a) for a in out]))
+        return out
+
     def md_nve(self, nsteps: int, dt: float) -> list:
         """nve_1 steps on the device; per-step energies, temperature, virial, pressure."""
         stats = (_lib.CcpMdStats * max(nsteps, 1))()

@@ -1612,6 +1612,15 @@ int ccp_md_get_state(ccp_context *ctx, double *x, double *y, double *z, double *
   return CCP_OK;
 }
 
+int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, double *idmz) {
+  if (!ctx || !ctx->md_ready || ld < ctx->ns) {
+    set_error("ccp_md_get_dipoles: no MD state or ld below the sites per molecule");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  return download_dipoles(ctx, ld, idmx, idmy, idmz);
+}
+
 int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
   if (!ctx || nsteps < 0 || !(dt > 0.0)) return CCP_ERR_BAD_INPUT;
   if (!ctx->md_ready) {

@@ -450,6 +450,7 @@ int ccp_model_get_int(const ccp_model *m, const char *name, int *value) {
   else if (n == "nclass") *value = m->nclass;
   else if (n == "nlin") *value = (int)m->sr.cs.size();
   else if (n == "have_fs3") *value = m->have_fs3;
+  else if (n == "ensemble_nve") *value = m->ensemble == "nve";
   else {
     set_error("unknown int parameter " + n);
     return CCP_ERR_BAD_INPUT;

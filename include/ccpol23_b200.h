@@ -257,6 +257,9 @@ int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double
 int ccp_md_get_state(ccp_context *ctx, double *x, double *y, double *z, double *v, double *q,
                      double *j);
 int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
+/* Induced dipoles of the current MD state (its last evaluation), idm*[i*ld + is], for
+   HISTORY output; non-polarisable sites get 0. */
+int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, double *idmz);
 
 /* ---------------------------------------------------------------- diagnostics */
 /* These have no counterpart in the reference; they serve benchmarking and profiling. */

@@ -59,3 +59,46 @@ def test_nve_continues_across_calls(md_case):
             out.append((stats[-1]["te"], c.md_get_state()))
     assert out[0][0] == pytest.approx(out[1][0], rel=1e-12)
     assert rel(out[0][1]["v"], out[1][1]["v"]) <= 1e-12
+
+
+def _run_dir(path, nm, nsteps, hist, restart):
+    import shutil
+    path.mkdir()
+    src = data_dir("fs2fs3")
+    for f in ("FIELD", "CONTROL", "data3b_full", "data3b_full_LR_4p5"):
+        shutil.copy(src / f, path / f)
+    ctl = (path / "CONTROL").read_text().splitlines()
+    ctl[1] = "   nve  1.0  2.0     # ensemble"
+    ctl[5] = f"   {nsteps}    # nsteps"
+    ctl[9] = f"   {hist}     # history frequency"
+    ctl[15] = f"   {'T' if restart else 'F'}     # restart"
+    (path / "CONTROL").write_text("\n".join(ctl) + "\n")
+    fld = (path / "FIELD").read_text().splitlines()
+    fld[1] = f"  {nm}    nom    -number of molecules"
+    (path / "FIELD").write_text("\n".join(fld) + "\n")
+    return path
+
+
+def test_md_driver_files_and_restart(product, tmp_path):
+    """The md.f90-style driver: OUTPUT rows, HISTORY frames, REVCON; and 2 + 2 steps through
+    a REVCON restart equal 4 steps in one run."""
+    import shutil
+    from ccpol23_plus_2025_mbmd_b200.md import read_revcon, run
+    a = _run_dir(tmp_path / "a", 37, 4, 2, False)
+    stats = run(a)
+    out = (a / "OUTPUT").read_text().splitlines()
+    assert len(out) == 3 + 4
+    assert abs(float(out[-1].split()[9]) - stats[-1]["te"]) <= 1e-7 * abs(stats[-1]["te"])
+    hist = (a / "HISTORY").read_text().splitlines()
+    assert sum(1 for ln in hist if ln.startswith("timestep")) == 2
+    ra = read_revcon(a / "REVCON", 37)
+    assert ra["step"] == 4
+    b = _run_dir(tmp_path / "b", 37, 2, 2, False)
+    run(b)
+    c = _run_dir(tmp_path / "c", 37, 2, 2, True)
+    shutil.copy(b / "REVCON", c / "REVCON")
+    run(c)
+    rc = read_revcon(c / "REVCON", 37)
+    assert rc["step"] == 4 and abs(rc["t"] - ra["t"]) < 1e-15
+    for k in ("x", "y", "z", "v", "q", "j"):
+        assert rel(rc[k], ra[k]) <= 1e-10, k
