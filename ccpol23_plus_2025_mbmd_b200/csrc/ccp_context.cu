@@ -589,15 +589,18 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       pend(9, s2);
     }
     pbeg(1, sm);
-    if (mask & T_SELF)
+    if (mask & (T_RSPACE | T_INDUCTION)) {
+      // one kernel gives the real-space Ewald forces, the static field and (for the self
+      // term or the induction) the intramolecular terms; an output that the mask does not
+      // ask for goes to the scratch field buffer
+      const bool with_self = mask & (T_SELF | T_INDUCTION);
+      LK(launch_pair_static(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
+                            c->d_ncnt, c->cap, nm, S, P, (mask & T_RSPACE) ? c->d_f : c->d_eir,
+                            c->d_e0r, c->d_e0s, with_self ? 1 : 0,
+                            (mask & T_SELF) ? c->d_f : c->d_eir, c->d_e0slf, c->d_scal, sm));
+    } else if (mask & T_SELF) {
       LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_f, c->d_e0slf,
                             c->d_scal, sm));
-    if (mask & (T_RSPACE | T_INDUCTION)) {
-      // the real-space kernel produces Ewald forces and the static field together; when
-      // only one of the two is wanted the other output is discarded by zeroing below.
-      LK(launch_pair_static(c->d_com, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt, c->cap, nm, S, P,
-                            (mask & T_RSPACE) ? c->d_f : c->d_eir, c->d_e0r, c->d_e0s, c->d_scal,
-                            sm));
     }
     pend(1, sm);
     pbeg(2, sm);
@@ -614,9 +617,6 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     pend(2, sm);
     if (mask & T_INDUCTION) {
       pbeg(3, sm);
-      if (!(mask & T_SELF))
-        LK(launch_self_static(px, py, pz, pxs, pys, pzs, nm, ld, S, P, c->d_eir, c->d_e0slf,
-                              c->d_scal, sm));
       LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
                             c->d_mu, c->d_sk, sm));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],

@@ -192,10 +192,12 @@ cudaError_t launch_prep(const double *x, const double *y, const double *z, const
                         int *icnt, cudaStream_t st);
 cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
                              int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st);
-cudaError_t launch_pair_static(const double4 *com, const double4 *act, const int *nbr,
-                               const double4 *nbrv, const int *ncnt, int cap, int nm,
-                               SiteSets S, EwaldParams P, double *f, double *e0r,
-                               double *e0s, double *scal, cudaStream_t st);
+cudaError_t launch_pair_static(const double *x, const double *y, const double *z,
+                               const double *xs, const double *ys, const double *zs, int ld,
+                               const double4 *act, const int *nbr, const double4 *nbrv,
+                               const int *ncnt, int cap, int nm, SiteSets S, EwaldParams P,
+                               double *f, double *e0r, double *e0s, int with_self, double *fself,
+                               double *e0slf, double *scal, cudaStream_t st);
 cudaError_t launch_self_static(const double *x, const double *y, const double *z,
                                const double *xs, const double *ys, const double *zs, int nm,
                                int ld, SiteSets S, EwaldParams P, double *f, double *e0slf,

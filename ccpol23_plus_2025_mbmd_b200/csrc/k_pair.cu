@@ -12,8 +12,6 @@ using namespace ccpd;
 
 namespace {
 
-constexpr int kWarpsPerBlock = 4;
-
 __device__ __forceinline__ double4 ld4(const double4 *p) { return *p; }
 
 // ------------------------------------------------------------------------ prep
@@ -100,135 +98,200 @@ __global__ void k_neighbors(const double4 *__restrict__ com, int nm, double box,
 
 // ------------------------------------------- Ewald real space + static field (real+TT)
 // rspace_ewald (ewald.f90:177-405), rspace_efield_stat (nb_induction_model.f90:128-293),
-// shortrange_efield_stat_damped (nb_induction_model.f90:5454-5629).
-template <int NQ, int NP>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-    k_pair_static(const double4 *__restrict__ act, const int *__restrict__ nbr,
+// shortrange_efield_stat_damped (nb_induction_model.f90:5454-5629) and, with `with_self`,
+// the intramolecular terms of ewald_self_correction (ewald.f90:101-147) and self_efield_stat
+// (nb_induction_model.f90:977-1115).
+//
+// One block per molecule i, one warp per row: rows [0, nq) are i's charged sites (Ewald
+// forces on them), rows [nq, nq + np) its polarisable sites (static field at them).  The 32
+// lanes of a row stride over i's neighbours, so no warp mixes the two kinds of row, and the
+// rows x 32 threads of every molecule keep enough warps resident to hide the latency of the
+// erfc/exp chains.  The intramolecular pairs of a row go to its lanes (one partner each).
+template <int R>
+__global__ void __launch_bounds__(R * 32)
+    k_pair_static(const double *__restrict__ x, const double *__restrict__ y,
+                  const double *__restrict__ z, const double *__restrict__ xs,
+                  const double *__restrict__ ys, const double *__restrict__ zs, int ld,
+                  const double4 *__restrict__ act, const int *__restrict__ nbr,
                   const double4 *__restrict__ nbrv, const int *__restrict__ ncnt, int cap,
                   int nm, SiteSets S, EwaldParams P, double *f, double *e0r, double *e0s,
-                  double *scal) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= nm) return;
-  const int na = S.na, ns = S.ns;
-  double4 si_q[NQ], si_p[NP];
-#pragma unroll
-  for (int a = 0; a < NQ; a++)
-    si_q[a] = a < S.nq ? ld4(&act[(size_t)i * na + S.a_of_q[a]]) : make_double4(0, 0, 0, 0);
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-    si_p[p] = p < S.np ? ld4(&act[(size_t)i * na + S.a_of_p[p]]) : make_double4(0, 0, 0, 0);
-  double F[NQ][3], E0[NP][3], Es[NP][3];
-#pragma unroll
-  for (int a = 0; a < NQ; a++) F[a][0] = F[a][1] = F[a][2] = 0.0;
-#pragma unroll
-  for (int p = 0; p < NP; p++) E0[p][0] = E0[p][1] = E0[p][2] = Es[p][0] = Es[p][1] = Es[p][2] = 0.0;
-  double e = 0.0, v = 0.0;
+                  int with_self, double *fself, double *e0slf, double *scal) {
+  __shared__ double red[R][4];
+  const int i = blockIdx.x;
+  const int row = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int nq = S.nq, np = S.np, na = S.na, ns = S.ns;
+  const bool qrow = row < nq, live = row < nq + np;
   const double alp = P.alpha;
-  const int cnt = ncnt[i];
-  for (int n = lane; n < cnt; n += 32) {
-    const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
-    if (!(c.w < P.rcutsd)) continue;
-    const int j = nbr[(size_t)i * cap + n];
-    const bool half = j > i;
-    double4 sj_q[NQ];
-#pragma unroll
-    for (int b = 0; b < NQ; b++)
-      sj_q[b] = b < S.nq ? ld4(&act[(size_t)j * na + S.a_of_q[b]]) : make_double4(0, 0, 0, 0);
-#pragma unroll
-    for (int a = 0; a < NQ; a++) {
-      if (a >= S.nq) break;
-#pragma unroll
-      for (int b = 0; b < NQ; b++) {
-        if (b >= S.nq) break;
-        const double rx = (c.x + si_q[a].x) - sj_q[b].x;
-        const double ry = (c.y + si_q[a].y) - sj_q[b].y;
-        const double rz = (c.z + si_q[a].z) - sj_q[b].z;
-        const double rssq = rx * rx + ry * ry + rz * rz;
-        const double drr = sqrt(rssq);
-        const double ec = erfc(alp * drr);
-        const double qq = kR4pie0 * si_q[a].w * sj_q[b].w;
-        const double ad = alp * drr;
-        const double fc = qq * (ec / drr + P.twosqpi * alp * exp(-(ad * ad)));
-        const double cf = fc / rssq;
-        const double fx = rx * cf, fy = ry * cf, fz = rz * cf;
-        F[a][0] += fx;
-        F[a][1] += fy;
-        F[a][2] += fz;
-        if (half) {
-          e += qq * ec / drr;
-          v -= rx * fx + ry * fy + rz * fz;
+  // row sums: a = force (charge row) or real-space field (polarisable row), b = short-range
+  // field, s = intramolecular force or field
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, e = 0.0, v = 0.0, sff = 0.0, svir = 0.0;
+  if (live) {
+    const int ai = qrow ? S.a_of_q[row] : S.a_of_p[row - nq];
+    const double4 si = ld4(&act[(size_t)i * na + ai]);
+    const int cnt = ncnt[i];
+    for (int n = lane; n < cnt; n += 32) {
+      const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
+      if (!(c.w < P.rcutsd)) continue;
+      const int j = nbr[(size_t)i * cap + n];
+      const bool half = j > i;
+      for (int b = 0; b < nq; b++) {
+        const double4 sj = ld4(&act[(size_t)j * na + S.a_of_q[b]]);
+        if (qrow) {
+          const double rx = (c.x + si.x) - sj.x;
+          const double ry = (c.y + si.y) - sj.y;
+          const double rz = (c.z + si.z) - sj.z;
+          const double rssq = rx * rx + ry * ry + rz * rz;
+          const double drr = sqrt(rssq);
+          const double ec = erfc(alp * drr);
+          const double qq = kR4pie0 * si.w * sj.w;
+          const double ad = alp * drr;
+          const double fc = qq * (ec / drr + P.twosqpi * alp * exp(-(ad * ad)));
+          const double cf = fc / rssq;
+          const double fx = rx * cf, fy = ry * cf, fz = rz * cf;
+          a0 += fx;
+          a1 += fy;
+          a2 += fz;
+          if (half) {
+            e += qq * ec / drr;
+            v -= rx * fx + ry * fy + rz * fz;
+          }
+        } else {
+          const double qj = sj.w;
+          const double dx = c.x + (si.x - sj.x);
+          const double dy = c.y + (si.y - sj.y);
+          const double dz = c.z + (si.z - sj.z);
+          const double d2 = dx * dx + dy * dy + dz * dz;
+          const double dist = sqrt(d2);
+          const double ad = alp * dist;
+          const double expar2 = exp(-(ad * ad));
+          const double d1i = erfc(alp * dist) / dist;
+          const double d2i = 1.0 / d2;
+          const double d3i = d2i * (d1i + P.twosqpi * alp * expar2);
+          a0 += qj * dx * d3i;
+          a1 += qj * dy * d3i;
+          a2 += qj * dz * d3i;
+          if (P.damped) {
+            const double r1 = 1.0 / dist;
+            const double r3 = r1 * r1 * r1;
+            const double g = (tt<2>(P.delta2, dist) - 1.0) * qj * r3;
+            b0 += g * dx;
+            b1 += g * dy;
+            b2 += g * dz;
+          }
         }
       }
     }
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      if (p >= S.np) break;
-#pragma unroll
-      for (int b = 0; b < NQ; b++) {
-        if (b >= S.nq) break;
-        const double qj = sj_q[b].w;
-        const double dx = c.x + (si_p[p].x - sj_q[b].x);
-        const double dy = c.y + (si_p[p].y - sj_q[b].y);
-        const double dz = c.z + (si_p[p].z - sj_q[b].z);
+    // intramolecular terms, as the reference forms them: (x + xs_a) - (x + xs_b), so that
+    // coincident sites give exactly zero
+    if (with_self) {
+      const double xi = x[i], yi = y[i], zi = z[i];
+      if (qrow) {
+        const int b = lane;
+        if (b < nq && b != row) {
+          const int sa = S.qsite[row], sb = S.qsite[b];
+          const double chg = S.q[S.a_of_q[row]] * S.q[S.a_of_q[b]];
+          const size_t oa = (size_t)i * ld + sa, ob = (size_t)i * ld + sb;
+          const double dx = (xi + xs[oa]) - (xi + xs[ob]);
+          const double dy = (yi + ys[oa]) - (yi + ys[ob]);
+          const double dz = (zi + zs[oa]) - (zi + zs[ob]);
+          const double drr = sqrt(dx * dx + dy * dy + dz * dz);
+          const double ef = erf(alp * drr);
+          const double ad = alp * drr;
+          const double fs = -kR4pie0 * chg *
+                            (ef / (drr * drr * drr) - P.twosqpi * alp * exp(-(ad * ad)) / (drr * drr));
+          s0 = dx * fs;
+          s1 = dy * fs;
+          s2 = dz * fs;
+          if (row < b) {  // each unordered pair once, as the reference's a < b loop
+            sff = ef * chg / drr;
+            svir = -(dx * s0 + dy * s1 + dz * s2);
+          }
+        }
+      } else if (lane < S.nself_q) {
+        const int bq = S.self_q[lane];
+        const int sp = S.psite[row - nq], sb = S.qsite[bq];
+        const double qj = S.q[S.a_of_q[bq]];
+        const size_t op = (size_t)i * ld + sp, ob = (size_t)i * ld + sb;
+        const double dx = (xi + xs[op]) - (xi + xs[ob]);
+        const double dy = (yi + ys[op]) - (yi + ys[ob]);
+        const double dz = (zi + zs[op]) - (zi + zs[ob]);
         const double d2 = dx * dx + dy * dy + dz * dz;
-        const double dist = sqrt(d2);
-        const double ad = alp * dist;
-        const double expar2 = exp(-(ad * ad));
-        const double d1i = erfc(alp * dist) / dist;
-        const double d2i = 1.0 / d2;
-        const double d3i = d2i * (d1i + P.twosqpi * alp * expar2);
-        E0[p][0] += qj * dx * d3i;
-        E0[p][1] += qj * dy * d3i;
-        E0[p][2] += qj * dz * d3i;
-        if (P.damped) {
-          const double r1 = 1.0 / dist;
-          const double r3 = r1 * r1 * r1;
-          const double g = (tt<2>(P.delta2, dist) - 1.0) * qj * r3;
-          Es[p][0] += g * dx;
-          Es[p][1] += g * dy;
-          Es[p][2] += g * dz;
+        if (d2 != 0.0) {
+          const double drr = sqrt(d2);
+          const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i;
+          const double ad = alp * drr;
+          const double g = erf(alp * drr) * d3i - P.twosqpi * alp * exp(-(ad * ad)) * d2i;
+          s0 = -qj * dx * g;
+          s1 = -qj * dy * g;
+          s2 = -qj * dz * g;
         }
       }
     }
   }
-#pragma unroll
-  for (int a = 0; a < NQ; a++)
-#pragma unroll
-    for (int k = 0; k < 3; k++) F[a][k] = warp_sum(F[a][k]);
-#pragma unroll
-  for (int p = 0; p < NP; p++)
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      E0[p][k] = warp_sum(E0[p][k]);
-      Es[p][k] = warp_sum(Es[p][k]);
-    }
+  a0 = warp_sum(a0);
+  a1 = warp_sum(a1);
+  a2 = warp_sum(a2);
+  b0 = warp_sum(b0);
+  b1 = warp_sum(b1);
+  b2 = warp_sum(b2);
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
   e = warp_sum(e);
   v = warp_sum(v);
+  sff = warp_sum(sff);
+  svir = warp_sum(svir);
   if (lane == 0) {
-    const size_t nfs = (size_t)nm * ns;
-#pragma unroll
-    for (int a = 0; a < NQ; a++) {
-      if (a >= S.nq) break;
-      const size_t o = (size_t)i * ns + S.qsite[a];
-      f[o] += F[a][0];
-      f[nfs + o] += F[a][1];
-      f[2 * nfs + o] += F[a][2];
-    }
-#pragma unroll
-    for (int p = 0; p < NP; p++) {
-      if (p >= S.np) break;
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        e0r[((size_t)i * S.np + p) * 3 + k] = E0[p][k];
-        e0s[((size_t)i * S.np + p) * 3 + k] = Es[p][k];
+    if (live) {
+      const size_t nfs = (size_t)nm * ns;
+      if (qrow) {
+        const size_t o = (size_t)i * ns + S.qsite[row];
+        f[o] += a0;
+        f[nfs + o] += a1;
+        f[2 * nfs + o] += a2;
+        if (with_self) {
+          fself[o] += s0;
+          fself[nfs + o] += s1;
+          fself[2 * nfs + o] += s2;
+        }
+      } else {
+        const size_t o = ((size_t)i * np + (row - nq)) * 3;
+        e0r[o] = a0;
+        e0r[o + 1] = a1;
+        e0r[o + 2] = a2;
+        e0s[o] = b0;
+        e0s[o + 1] = b1;
+        e0s[o + 2] = b2;
+        if (with_self) {
+          e0slf[o] = s0;
+          e0slf[o + 1] = s1;
+          e0slf[o + 2] = s2;
+        }
       }
     }
-    atomicAdd(&scal[S_RC_E], e);
-    atomicAdd(&scal[S_RC_VIR], v);
+    red[row][0] = e;
+    red[row][1] = v;
+    red[row][2] = sff;
+    red[row][3] = svir;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double te = 0.0, tv = 0.0, tf = 0.0, ts = 0.0;
+    for (int r = 0; r < R; r++) {
+      te += red[r][0];
+      tv += red[r][1];
+      tf += red[r][2];
+      ts += red[r][3];
+    }
+    atomicAdd(&scal[S_RC_E], te);
+    atomicAdd(&scal[S_RC_VIR], tv);
+    if (with_self) {
+      atomicAdd(&scal[S_SELF_SUMFF], tf);
+      atomicAdd(&scal[S_SELF_VIR], ts);
+    }
   }
 }
-
 // --------------------------------------------- intramolecular static terms (per molecule)
 // ewald_self_correction intramolecular part (ewald.f90:101-147) and self_efield_stat
 // (nb_induction_model.f90:977-1115).  Both use (x + xs_a) - (x + xs_b), as the reference
@@ -374,8 +437,10 @@ __device__ __forceinline__ void ind_pair(double dx, double dy, double dz, double
   out.fz = fz;
 }
 
-template <int NA>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+// One block per molecule i, one warp per active site a of i (a row); the lanes of a row
+// stride over i's neighbours and take one intramolecular partner each.
+template <int R>
+__global__ void __launch_bounds__(R * 32)
     k_pair_indforce(const double *__restrict__ x, const double *__restrict__ y,
                     const double *__restrict__ z, const double *__restrict__ xs,
                     const double *__restrict__ ys, const double *__restrict__ zs, int ld,
@@ -383,133 +448,127 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32)
                     const double4 *__restrict__ nbrv, const int *__restrict__ ncnt, int cap,
                     int nm, SiteSets S, EwaldParams P, const double *__restrict__ mu,
                     double *f, double *scal) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (i >= nm) return;
+  __shared__ double red[R];
+  const int i = blockIdx.x;
+  const int a = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int na = S.na, np = S.np;
-  double4 sa[NA];
-  double ma[NA][3];
-#pragma unroll
-  for (int a = 0; a < NA; a++) {
-    sa[a] = a < na ? ld4(&act[(size_t)i * na + a]) : make_double4(0, 0, 0, 0);
-    const int p = a < na ? S.p_of_a[a] : -1;
-    for (int k = 0; k < 3; k++) ma[a][k] = p >= 0 ? mu[((size_t)i * np + p) * 3 + k] : 0.0;
-  }
-  double F[NA][3];
-#pragma unroll
-  for (int a = 0; a < NA; a++) F[a][0] = F[a][1] = F[a][2] = 0.0;
-  double vir = 0.0;
-  const int cnt = ncnt[i];
-  for (int n = lane; n < cnt; n += 32) {
-    const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
-    if (!(c.w < P.rcutsd)) continue;
-    const int j = nbr[(size_t)i * cap + n];
-    const bool half = j > i;
-    for (int b = 0; b < na; b++) {
-      const double4 sb = ld4(&act[(size_t)j * na + b]);
-      const int pbi = S.p_of_a[b];
-      const bool pb = pbi >= 0;
-      double mbx = 0.0, mby = 0.0, mbz = 0.0;
-      if (pb) {
-        mbx = mu[((size_t)j * np + pbi) * 3 + 0];
-        mby = mu[((size_t)j * np + pbi) * 3 + 1];
-        mbz = mu[((size_t)j * np + pbi) * 3 + 2];
-      }
-#pragma unroll
-      for (int a = 0; a < NA; a++) {
-        if (a >= na) break;
-        const bool pa = S.p_of_a[a] >= 0;
-        if (!pa && !(pb && sa[a].w != 0.0)) continue;
-        const double dx = c.x + (sa[a].x - sb.x);
-        const double dy = c.y + (sa[a].y - sb.y);
-        const double dz = c.z + (sa[a].z - sb.z);
+  const bool live = a < na;
+  double fx = 0.0, fy = 0.0, fz = 0.0, vir = 0.0;
+  double qa = 0.0, max = 0.0, may = 0.0, maz = 0.0;
+  if (live) {
+    const double4 sa = ld4(&act[(size_t)i * na + a]);
+    qa = sa.w;
+    const int pai = S.p_of_a[a];
+    const bool pa = pai >= 0;
+    if (pa) {
+      max = mu[((size_t)i * np + pai) * 3 + 0];
+      may = mu[((size_t)i * np + pai) * 3 + 1];
+      maz = mu[((size_t)i * np + pai) * 3 + 2];
+    }
+    const int cnt = ncnt[i];
+    for (int n = lane; n < cnt; n += 32) {
+      const double4 c = ld4(&nbrv[(size_t)i * cap + n]);
+      if (!(c.w < P.rcutsd)) continue;
+      const int j = nbr[(size_t)i * cap + n];
+      const bool half = j > i;
+      for (int b = 0; b < na; b++) {
+        const int pbi = S.p_of_a[b];
+        const bool pb = pbi >= 0;
+        if (!pa && !(pb && qa != 0.0)) continue;
+        const double4 sb = ld4(&act[(size_t)j * na + b]);
+        double mbx = 0.0, mby = 0.0, mbz = 0.0;
+        if (pb) {
+          mbx = mu[((size_t)j * np + pbi) * 3 + 0];
+          mby = mu[((size_t)j * np + pbi) * 3 + 1];
+          mbz = mu[((size_t)j * np + pbi) * 3 + 2];
+        }
+        const double dx = c.x + (sa.x - sb.x);
+        const double dy = c.y + (sa.y - sb.y);
+        const double dz = c.z + (sa.z - sb.z);
         IndPair r;
-        ind_pair(dx, dy, dz, sa[a].w, ma[a][0], ma[a][1], ma[a][2], pa, sb.w, mbx, mby, mbz,
-                 pb, P, r);
-        F[a][0] += r.fx;
-        F[a][1] += r.fy;
-        F[a][2] += r.fz;
+        ind_pair(dx, dy, dz, qa, max, may, maz, pa, sb.w, mbx, mby, mbz, pb, P, r);
+        fx += r.fx;
+        fy += r.fy;
+        fz += r.fz;
         if (half) vir -= dx * r.fx + dy * r.fy + dz * r.fz;
       }
     }
-  }
-  // intramolecular (self_forces): lanes split the site pairs (a < b); both sides.
-  const double alp = P.alpha, alp3 = alp * alp * alp, alp5 = alp3 * alp * alp;
-  const double xi = x[i], yi = y[i], zi = z[i];
-  for (int pr = lane; pr < na * na; pr += 32) {
-    const int a = pr / na, b = pr % na;
-    if (b <= a) continue;
-    const int s_a = S.asite[a], s_b = S.asite[b];
-    const size_t oa = (size_t)i * ld + s_a, ob = (size_t)i * ld + s_b;
-    const double dx = (xi + xs[oa]) - (xi + xs[ob]);
-    const double dy = (yi + ys[oa]) - (yi + ys[ob]);
-    const double dz = (zi + zs[oa]) - (zi + zs[ob]);
-    const double d2 = dx * dx + dy * dy + dz * dz;
-    if (d2 == 0.0) continue;
-    const double drr = sqrt(d2);
-    const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d4i = d2i * d2i;
-    const double d5i = d3i * d2i, d6i = d3i * d3i, d7i = d6i * d1i;
-    const double ad = alp * drr;
-    const double expar2 = exp(-(ad * ad));
-    const double ef = erf(alp * drr);
-    const double ts = P.twosqpi;
-    // erf-screened kernels of the intramolecular correction (negated interactions)
-    const double d3ii = ef * d3i - ts * alp * expar2 * d2i;
-    const double d5ii = ef * d5i - ts * alp * expar2 * d4i - (2.0 / 3.0) * ts * alp3 * expar2 * d2i;
-    const double d7ii = ef * d7i - ts * alp * expar2 * d6i - (2.0 / 3.0) * ts * alp3 * expar2 * d4i -
-                        (4.0 / 15.0) * ts * alp5 * expar2 * d2i;
-    // side a (from b) with d, side b (from a) with -d
-    for (int side = 0; side < 2; side++) {
-      const int u = side == 0 ? a : b, w = side == 0 ? b : a;
-      const double sgn = side == 0 ? 1.0 : -1.0;
-      const double ex = sgn * dx, ey = sgn * dy, ez = sgn * dz;
-      const double qu = sa[u].w, qw = sa[w].w;
-      const double mux = ma[u][0], muy = ma[u][1], muz = ma[u][2];
-      const double mwx = ma[w][0], mwy = ma[w][1], mwz = ma[w][2];
-      const double doti = mux * ex + muy * ey + muz * ez;
-      const double dotj = mwx * ex + mwy * ey + mwz * ez;
-      const double mm = mux * mwx + muy * mwy + muz * mwz;
-      // field E = -(3 d5 dotj e - mw d3); gradient = -(qw(...) + dipole part)
-      const double s = 3.0 * d5ii * dotj;
-      double fx = -qu * (s * ex - mwx * d3ii), fy = -qu * (s * ey - mwy * d3ii),
-             fz = -qu * (s * ez - mwz * d3ii);
-      const double c1 = -3.0 * qw * d5ii * doti - 15.0 * d7ii * doti * dotj + 3.0 * d5ii * mm;
-      fx -= c1 * ex + qw * mux * d3ii + 3.0 * d5ii * (mux * dotj + mwx * doti);
-      fy -= c1 * ey + qw * muy * d3ii + 3.0 * d5ii * (muy * dotj + mwy * doti);
-      fz -= c1 * ez + qw * muz * d3ii + 3.0 * d5ii * (muz * dotj + mwz * doti);
-      // accumulate to a register slot: unrolled select keeps F in registers
-#pragma unroll
-      for (int t = 0; t < NA; t++)
-        if (t == u) {
-          F[t][0] += fx;
-          F[t][1] += fy;
-          F[t][2] += fz;
+    // intramolecular (self_forces): lane w takes site a's side of the pair (a, w), with
+    // d = (x + xs_a) - (x + xs_w); the pair's virial is counted once, on the a < w side
+    const int w = lane;
+    if (w < na && w != a) {
+      const double alp = P.alpha, alp3 = alp * alp * alp, alp5 = alp3 * alp * alp;
+      const double xi = x[i], yi = y[i], zi = z[i];
+      const size_t oa = (size_t)i * ld + S.asite[a], ow = (size_t)i * ld + S.asite[w];
+      const double ex = (xi + xs[oa]) - (xi + xs[ow]);
+      const double ey = (yi + ys[oa]) - (yi + ys[ow]);
+      const double ez = (zi + zs[oa]) - (zi + zs[ow]);
+      const double d2 = ex * ex + ey * ey + ez * ez;
+      if (d2 != 0.0) {
+        const double drr = sqrt(d2);
+        const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d4i = d2i * d2i;
+        const double d5i = d3i * d2i, d6i = d3i * d3i, d7i = d6i * d1i;
+        const double ad = alp * drr;
+        const double expar2 = exp(-(ad * ad));
+        const double ef = erf(alp * drr);
+        const double ts = P.twosqpi;
+        // erf-screened kernels of the intramolecular correction (negated interactions)
+        const double d3ii = ef * d3i - ts * alp * expar2 * d2i;
+        const double d5ii = ef * d5i - ts * alp * expar2 * d4i - (2.0 / 3.0) * ts * alp3 * expar2 * d2i;
+        const double d7ii = ef * d7i - ts * alp * expar2 * d6i - (2.0 / 3.0) * ts * alp3 * expar2 * d4i -
+                            (4.0 / 15.0) * ts * alp5 * expar2 * d2i;
+        const double4 sw = ld4(&act[(size_t)i * na + w]);
+        const double qw = sw.w;
+        const int pwi = S.p_of_a[w];
+        double mwx = 0.0, mwy = 0.0, mwz = 0.0;
+        if (pwi >= 0) {
+          mwx = mu[((size_t)i * np + pwi) * 3 + 0];
+          mwy = mu[((size_t)i * np + pwi) * 3 + 1];
+          mwz = mu[((size_t)i * np + pwi) * 3 + 2];
         }
-      if (side == 0) vir -= ex * fx + ey * fy + ez * fz;
+        const double doti = max * ex + may * ey + maz * ez;
+        const double dotj = mwx * ex + mwy * ey + mwz * ez;
+        const double mm = max * mwx + may * mwy + maz * mwz;
+        // field E = -(3 d5 dotj e - mw d3); gradient = -(qw(...) + dipole part)
+        const double s = 3.0 * d5ii * dotj;
+        double gx = -qa * (s * ex - mwx * d3ii), gy = -qa * (s * ey - mwy * d3ii),
+               gz = -qa * (s * ez - mwz * d3ii);
+        const double c1 = -3.0 * qw * d5ii * doti - 15.0 * d7ii * doti * dotj + 3.0 * d5ii * mm;
+        gx -= c1 * ex + qw * max * d3ii + 3.0 * d5ii * (max * dotj + mwx * doti);
+        gy -= c1 * ey + qw * may * d3ii + 3.0 * d5ii * (may * dotj + mwy * doti);
+        gz -= c1 * ez + qw * maz * d3ii + 3.0 * d5ii * (maz * dotj + mwz * doti);
+        fx += gx;
+        fy += gy;
+        fz += gz;
+        if (a < w) vir -= ex * gx + ey * gy + ez * gz;
+      }
     }
   }
-#pragma unroll
-  for (int a = 0; a < NA; a++)
-#pragma unroll
-    for (int k = 0; k < 3; k++) F[a][k] = warp_sum(F[a][k]);
+  fx = warp_sum(fx);
+  fy = warp_sum(fy);
+  fz = warp_sum(fz);
   vir = warp_sum(vir);
   if (lane == 0) {
-    // point self terms: field += selffac mu, gradient diagonal -= selffac q
-    const double selffac = 4.0 * alp3 / (3.0 * sqrt(kPi));
-    const size_t nfs = (size_t)nm * S.ns;
-#pragma unroll
-    for (int a = 0; a < NA; a++) {
-      if (a >= na) break;
-      const double q = sa[a].w;
-      const double px = q * selffac * ma[a][0] - selffac * q * ma[a][0];
-      const double py = q * selffac * ma[a][1] - selffac * q * ma[a][1];
-      const double pz = q * selffac * ma[a][2] - selffac * q * ma[a][2];
+    if (live) {
+      // point self terms: field += selffac mu, gradient diagonal -= selffac q
+      const double alp = P.alpha, alp3 = alp * alp * alp;
+      const double selffac = 4.0 * alp3 / (3.0 * sqrt(kPi));
+      const double px = qa * selffac * max - selffac * qa * max;
+      const double py = qa * selffac * may - selffac * qa * may;
+      const double pz = qa * selffac * maz - selffac * qa * maz;
+      const size_t nfs = (size_t)nm * S.ns;
       const size_t o = (size_t)i * S.ns + S.asite[a];
-      f[o] += kR4pie0 * (F[a][0] + px);
-      f[nfs + o] += kR4pie0 * (F[a][1] + py);
-      f[2 * nfs + o] += kR4pie0 * (F[a][2] + pz);
+      f[o] += kR4pie0 * (fx + px);
+      f[nfs + o] += kR4pie0 * (fy + py);
+      f[2 * nfs + o] += kR4pie0 * (fz + pz);
     }
-    atomicAdd(&scal[S_IND_VIR_R], kR4pie0 * vir);
+    red[a] = vir;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int r = 0; r < R; r++) t += red[r];
+    atomicAdd(&scal[S_IND_VIR_R], kR4pie0 * t);
   }
 }
 
@@ -551,19 +610,20 @@ cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlis
   return cudaGetLastError();
 }
 
-cudaError_t launch_pair_static(const double4 *com, const double4 *act, const int *nbr,
-                               const double4 *nbrv, const int *ncnt, int cap, int nm,
-                               SiteSets S, EwaldParams P, double *f, double *e0r,
-                               double *e0s, double *scal, cudaStream_t st) {
-  (void)com;
-  const int threads = kWarpsPerBlock * 32;
-  const int blocks = (nm + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  if (S.nq <= 5 && S.np <= 3)
-    k_pair_static<5, 3><<<blocks, threads, 0, st>>>(act, nbr, nbrv, ncnt, cap, nm, S, P, f, e0r,
-                                                    e0s, scal);
+cudaError_t launch_pair_static(const double *x, const double *y, const double *z,
+                               const double *xs, const double *ys, const double *zs, int ld,
+                               const double4 *act, const int *nbr, const double4 *nbrv,
+                               const int *ncnt, int cap, int nm, SiteSets S, EwaldParams P,
+                               double *f, double *e0r, double *e0s, int with_self, double *fself,
+                               double *e0slf, double *scal, cudaStream_t st) {
+  if (nm < 1) return cudaSuccess;
+  if (S.nq + S.np <= 8)
+    k_pair_static<8><<<nm, 8 * 32, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt, cap,
+                                            nm, S, P, f, e0r, e0s, with_self, fself, e0slf, scal);
   else
-    k_pair_static<kMaxQ, kMaxP><<<blocks, threads, 0, st>>>(act, nbr, nbrv, ncnt, cap, nm, S, P,
-                                                            f, e0r, e0s, scal);
+    k_pair_static<kMaxQ + kMaxP><<<nm, (kMaxQ + kMaxP) * 32, 0, st>>>(
+        x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt, cap, nm, S, P, f, e0r, e0s, with_self,
+        fself, e0slf, scal);
   return cudaGetLastError();
 }
 
@@ -583,13 +643,12 @@ cudaError_t launch_pair_indforce(const double *x, const double *y, const double 
                                  const double4 *nbrv, const int *ncnt, int cap, int nm,
                                  SiteSets S, EwaldParams P, const double *mu, double *f,
                                  double *scal, cudaStream_t st) {
-  const int threads = kWarpsPerBlock * 32;
-  const int blocks = (nm + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (nm < 1) return cudaSuccess;
   if (S.na <= 8)
-    k_pair_indforce<8><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt,
-                                                   cap, nm, S, P, mu, f, scal);
+    k_pair_indforce<8><<<nm, 8 * 32, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv, ncnt, cap,
+                                              nm, S, P, mu, f, scal);
   else
-    k_pair_indforce<kMaxA><<<blocks, threads, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv,
-                                                       ncnt, cap, nm, S, P, mu, f, scal);
+    k_pair_indforce<kMaxA><<<nm, kMaxA * 32, 0, st>>>(x, y, z, xs, ys, zs, ld, act, nbr, nbrv,
+                                                      ncnt, cap, nm, S, P, mu, f, scal);
   return cudaGetLastError();
 }
