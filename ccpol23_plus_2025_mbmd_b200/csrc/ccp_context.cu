@@ -135,7 +135,7 @@ struct ccp_context {
   cudaStream_t cap_stream = nullptr;
   cudaGraph_t ind_graph = nullptr;
   cudaGraphExec_t ind_exec = nullptr;
-  double *d_istate = nullptr;  // {iterations, last change, last energy}
+  double *d_istate = nullptr;  // {iterations, last change, last energy, finished}
   double *h_istate = nullptr;
   unsigned *d_ticket = nullptr;  // last-block ticket of the fused update kernel
   int ind_per_iter = 0;          // kernels per Jacobi iteration of the last solve
@@ -159,6 +159,7 @@ struct ccp_context {
   cudaEvent_t ev_fork = nullptr, ev_j3 = nullptr, ev_j2 = nullptr, ev_jm = nullptr;
   int opt_overlap = 1;     // three-body terms concurrent with Ewald/induction
   int opt_fs3_tpb = 8;     // FS3 triples per block when concurrent (0 = persistent grid)
+  int opt_fs3_bps = 0;     // when concurrent, at most this many FS3 blocks per SM (0 = no cap)
 };
 
 namespace {
@@ -379,8 +380,11 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
   return e;
 }
 
+constexpr int kDipUnroll = 2;  // Jacobi steps per pass of the graph's WHILE body
+
 // Builds (once per set of buffers and sizes) the CUDA graph of the Jacobi iteration: a
-// WHILE conditional node whose body is one Jacobi step ending in the convergence test.
+// WHILE conditional node whose body is one or more Jacobi steps, each ending in the
+// convergence test.
 // The host launches it once per evaluation and never synchronises inside the loop.
 int ensure_ind_graph(ccp_context *c) {
   std::vector<long long> key = {
@@ -408,7 +412,12 @@ int ensure_ind_graph(ccp_context *c) {
   cudaStream_t cs = c->cap_stream;
   CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   int nl = 0;
-  cudaError_t e = enqueue_dip_step(c, cs, h, 1, &nl);
+  // with the phase tables the body holds kDipUnroll Jacobi steps: a step's update kernel
+  // returns at once when an earlier step of the same pass has finished the solve, so the
+  // count of steps taken is unchanged while the per-pass cost of the WHILE node is shared
+  const int unroll = c->use_P ? kDipUnroll : 1;
+  cudaError_t e = cudaSuccess;
+  for (int u = 0; u < unroll && e == cudaSuccess; u++) e = enqueue_dip_step(c, cs, h, 1, &nl);
   cudaGraph_t captured = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
   if (!cuda_ok(e, "capture of the dipole loop")) return CCP_ERR_CUDA;
@@ -422,7 +431,7 @@ int ensure_ind_graph(ccp_context *c) {
 // h_istate; in the graph form the copy completes at the evaluation's final synchronisation.
 int run_dipole_loop(ccp_context *c, cudaStream_t st) {
   CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * c->nm * c->S.np * 3, st));
-  CK(cudaMemsetAsync(c->d_istate, 0, 3 * sizeof(double), st));
+  CK(cudaMemsetAsync(c->d_istate, 0, 4 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_ticket, 0, sizeof(unsigned), st));
   if (c->use_P) CK(cudaMemsetAsync(c->d_sk, 0, sizeof(double) * 4 * (size_t)c->nk, st));
@@ -569,7 +578,8 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       pend(7, s3);
       pbeg(8, s3);
       LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
-                    nm, ns, f3, c->d_fc3, c->d_scal, c->nsm, side ? c->opt_fs3_tpb : 0, gfs3,
+                    nm, ns, f3, c->d_fc3, c->d_scal, c->nsm, side ? c->opt_fs3_tpb : 0,
+                    side ? c->opt_fs3_bps : 0, gfs3,
                     s3));
       pend(8, s3);
     }
@@ -996,7 +1006,7 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
       cudaEventCreateWithFlags(&c->ev_jm, cudaEventDisableTiming) != cudaSuccess)
     return fail("event");
   c->stream = c->own;
-  if (cudaMalloc(&c->d_istate, 3 * sizeof(double)) != cudaSuccess ||
+  if (cudaMalloc(&c->d_istate, 4 * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->d_ticket, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(c->d_ticket, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_istate, 3 * sizeof(double)) != cudaSuccess)
@@ -1172,6 +1182,12 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
       return CCP_ERR_BAD_INPUT;
     }
     ctx->opt_fs3_tpb = value;
+  } else if (n == "fs3_blocks_per_sm") {
+    if (value < 0 || value > 32) {
+      set_error("ccp_context_set_option: fs3_blocks_per_sm must be 0..32");
+      return CCP_ERR_BAD_INPUT;
+    }
+    ctx->opt_fs3_bps = value;
   } else {
     set_error("ccp_context_set_option: unknown option " + n);
     return CCP_ERR_BAD_INPUT;
@@ -1194,6 +1210,8 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_pgrad;
   } else if (n == "fs3_triples_per_block") {
     *value = ctx->opt_fs3_tpb;
+  } else if (n == "fs3_blocks_per_sm") {
+    *value = ctx->opt_fs3_bps;
   } else {
     set_error("ccp_context_get_option: unknown option " + n);
     return CCP_ERR_BAD_INPUT;

@@ -144,7 +144,7 @@ struct IterArgs {
   const double2 *XY;  // [nw][nlm] exp(i(l x + m y)), lm = l (2 mmax + 1) + m + mmax
   const double2 *Z;   // [nw][nz] exp(i n z) (conjugated for n < 0), nz = 2 nmax + 1
   int nlm, nz, mmax, nmax;
-  double *sk, *scal, *state;  // state = {iterations, change, energy}
+  double *sk, *scal, *state;  // state = {iterations, change, energy, finished}
   unsigned *ticket;
   double thr;
   int maxit, use_graph;
@@ -260,8 +260,8 @@ cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt
                             cudaStream_t st);
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
-                       double *f, double *fc3, double *scal, int nsm, int triples_per_block, double *gfs3,
-                       cudaStream_t st);
+                       double *f, double *fc3, double *scal, int nsm, int triples_per_block,
+                       int blocks_per_sm, double *gfs3, cudaStream_t st);
 cudaError_t launch_fs2_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
                             int nm, Fs2Params P, int2 *pairs, int pair_cap, int *icnt,
                             cudaStream_t st);

@@ -613,8 +613,8 @@ namespace {
 template <typename T, bool GRAD>
 cudaError_t launch_fs3_t(const Fs3Rec *R, const int *icnt, int tri_cap, const double4 *s17,
                          const double *coef, const double *bgr, int nm, int ns, double *f,
-                         double *fc3, double *scal, int nsm, int triples_per_block, double *gfs3,
-                         cudaStream_t st) {
+                         double *fc3, double *scal, int nsm, int triples_per_block,
+                         int blocks_per_sm, double *gfs3, cudaStream_t st) {
   const size_t smem = GRAD ? fs3_grad_offset<T>() + sizeof(Fs3Grad<T>) : sizeof(Fs3Smem<T>);
   cudaError_t e = cudaFuncSetAttribute(k_fs3<T, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -623,7 +623,10 @@ cudaError_t launch_fs3_t(const Fs3Rec *R, const int *icnt, int tri_cap, const do
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fs3<T, GRAD>, kFs3Block, smem);
   if (per_sm < 1) per_sm = 1;
   // the gradient form flushes per-block partial sums: a persistent grid keeps them few
-  const int grid = fs3_grid(nsm * per_sm, tri_cap, GRAD ? 0 : triples_per_block);
+  int grid = fs3_grid(nsm * per_sm, tri_cap, GRAD ? 0 : triples_per_block);
+  // a cap makes the grid persistent on fewer slots, leaving the rest to concurrent kernels
+  if (blocks_per_sm > 0 && blocks_per_sm < per_sm && grid > nsm * blocks_per_sm)
+    grid = nsm * blocks_per_sm;
   k_fs3<T, GRAD><<<grid, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3,
                                                 scal, gfs3);
   return cudaGetLastError();
@@ -633,18 +636,18 @@ cudaError_t launch_fs3_t(const Fs3Rec *R, const int *icnt, int tri_cap, const do
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
                        double *f, double *fc3, double *scal, int nsm, int triples_per_block,
-                       double *gfs3, cudaStream_t st) {
+                       int blocks_per_sm, double *gfs3, cudaStream_t st) {
   const Fs3Rec *R = static_cast<const Fs3Rec *>(rec);
   if (precision == 0) {
     if (gfs3)
       return launch_fs3_t<double, true>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal,
-                                        nsm, triples_per_block, gfs3, st);
+                                        nsm, triples_per_block, blocks_per_sm, gfs3, st);
     return launch_fs3_t<double, false>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
-                                       triples_per_block, nullptr, st);
+                                       triples_per_block, blocks_per_sm, nullptr, st);
   }
   if (gfs3)
     return launch_fs3_t<float, true>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
-                                     triples_per_block, gfs3, st);
+                                     triples_per_block, blocks_per_sm, gfs3, st);
   return launch_fs3_t<float, false>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
-                                    triples_per_block, nullptr, st);
+                                    triples_per_block, blocks_per_sm, nullptr, st);
 }

@@ -16,7 +16,9 @@
 //      update mu' = alpha (E_real + E_k + E0) in place, the |mu - mu'|^2 and energy sums;
 //      the last block to finish (atomic ticket) closes the iteration: it records the
 //      iteration count, change and energy, clears the accumulators and S(k) for the next
-//      iteration and, inside the graph, sets the WHILE node's condition.
+//      iteration, marks the solve finished when it has converged (state[3]: a later B in
+//      the same pass of a graph body that unrolls several steps then returns at once) and,
+//      inside the graph, sets the WHILE node's condition.
 #include "ccp_device.cuh"
 
 using namespace ccpd;
@@ -136,6 +138,8 @@ __global__ void __launch_bounds__(kThreads)
 
 __global__ void __launch_bounds__(kThreads)
     k_iter_a(IterArgs A) {
+  // no test of the finished flag here: a step after the finish only rewrites the T.mu
+  // scratch and S(k), which the next use clears, and it saves a dependent load per step
   const int nA = (A.nw + kWarps - 1) / kWarps;
   if ((int)blockIdx.x < nA) {
     const int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
@@ -178,6 +182,7 @@ __global__ void __launch_bounds__(kThreads)
     k_iter_b(IterArgs A) {
   // kGatherSites polarisable sites per block; the 8 warps split the k-vectors, so every
   // k-vector's weights are loaded once per block and reused for all its sites
+  if (A.state[3] != 0.0) return;  // the solve finished in an earlier step of this pass
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int w0 = blockIdx.x * kGatherSites;
   const int ns_blk = min(kGatherSites, A.nw - w0);
@@ -256,7 +261,9 @@ __global__ void __launch_bounds__(kThreads)
     A.scal[S_IND_CHANGE] = 0.0;
     A.scal[S_IND_ENERGY] = 0.0;
     *A.ticket = 0u;
-    if (A.use_graph) cudaGraphSetConditional(A.handle, (chg > A.thr && it < A.maxit) ? 1u : 0u);
+    const bool more = chg > A.thr && it < A.maxit;
+    if (!more) A.state[3] = 1.0;
+    if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
   }
 }
 
