@@ -287,6 +287,9 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
                      with the Ewald and induction kernels (on a high-priority stream);
      "fs3_triples_per_block"  8 (default): FS3 triples per block when overlapping, so that
                      blocks retire often (0: one persistent wave of blocks);
+     "fs3_blocks_per_sm"  0 (default, no cap): when overlapping, at most this many FS3
+                     blocks per SM (a persistent grid on that many slots), leaving the rest
+                     of each SM to the Ewald and induction kernels;
      "fs3_param_grad" 0 (default): see ccp_context_fs3_param_grad;
      "phase_matrix"  1 (default): the polarisable sites' phases are tabulated once per
                      evaluation as exp(i(l x + m y)) and exp(i n z) factors (when they take at
