@@ -5,8 +5,9 @@ A step is one evaluation of the hot path of the 512-water FS2+FS3 box (L = 24.84
 seeded synthetic configuration): Ewald self/intramolecular, real and reciprocal sums,
 the induced-dipole solve with induction forces, FS2 and FS3 (SR/LR/blend).  The 2-body
 term and the integrator are outside this path.  ns/day = steps/s x 0.0005 ps x 86400 / 1000
-(dt = 0.5 fs).  The headline value is the mixed-precision form when its relative force
-error against the FP64 form is <= 1e-5, else the FP64 form; both are reported.
+(dt = 0.5 fs).  The headline value is the faster of the FP64 form and the mixed-precision
+form, the latter only when its relative force errors against the FP64 form (site forces,
+per-molecule forces, torques) are all <= 1e-5; both forms are reported.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
@@ -392,6 +393,7 @@ def main():
                      "e2e_ns_day": world * ns_per_day(1.0 / e2e), "e2e_ms": e2e * 1e3,
                      "triples_per_s": world * e["n_fs3_triples"] / (ms * 1e-3),
                      "fs3_ms": float(np.mean(r["phases"][:, 8])),
+                     "fs3_isolated_ms": r["fs3_isolated_ms"],
                      "phase_ms": [float(v) for v in r["phases"].mean(0)],
                      "ind_iters": e["ind_iters"], "n_fs3_triples": e["n_fs3_triples"],
                      "n_fs3_blend": e["n_fs3_blend"], "n_fs2_triples": e["n_fs2_triples"],
@@ -416,7 +418,8 @@ def main():
     tqerr = rl(Qmx, Q64)
     c3err = rl(fmx["com3"], f64["com3"])
     eerr = abs(fmx["energies"]["fs3pe"] - f64["energies"]["fs3pe"]) / abs(f64["energies"]["fs3pe"])
-    head = "mixed" if max(ferr, molerr, tqerr) <= 1e-5 else "fp64"
+    mixed_ok = max(ferr, molerr, tqerr) <= 1e-5
+    head = "mixed" if mixed_ok and out["mixed"]["ns_day"] > out["fp64"]["ns_day"] else "fp64"
     H = out[head]
     # roofline of the dominant kernel (FS3) of the headline form
     e = results[head]["energies"]
@@ -441,7 +444,7 @@ def main():
         "fp64": out["fp64"], "mixed": out["mixed"],
         "mixed_vs_fp64": {"rel_site_force_err": ferr, "rel_molecule_force_err": molerr,
                           "rel_molecule_torque_err": tqerr, "rel_fs3_com_force_err": c3err,
-                          "rel_fs3_energy_err": eerr},
+                          "rel_fs3_energy_err": eerr, "within_1e-5": mixed_ok},
         "e2e": {"value": H["e2e_ns_day"], "unit": "ns/day",
                 "h2d_bytes_per_step": results[head]["h2d"], "d2h_bytes_per_step": results[head]["d2h"]},
         "roofline": {"bound": "fp32_pipe" if head == "mixed" else "fp64_pipe",

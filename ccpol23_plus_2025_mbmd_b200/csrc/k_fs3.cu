@@ -183,14 +183,30 @@ struct Vec2<float> {
   using type = float2;
 };
 
+// FP32 copy of the (e, e d) tables, read by the family-1 and family-2 passes of the mixed
+// form; the FP64 form reads the FP64 tables and keeps no copy.
+template <typename T>
+struct LowUU {
+  float2 v[3][kP][kRS];
+};
+template <>
+struct LowUU<double> {
+  char v[8];
+};
+
+// T is the arithmetic of the family-1 and family-2 passes.  The site-pair tables, the
+// family-0 pass (whose outputs carry the energy sum) and everything after the passes are
+// FP64 in both forms: the FS3 sum cancels heavily (sum |terms| / |sum| up to ~1e5), so an
+// energy formed from FP32 tables or terms would carry ~1e-4 relative error into the energy
+// and the R_avg-damping COM forces.
 template <typename T>
 struct Fs3Smem {
-  using V2 = typename Vec2<T>::type;
   double2 coef[2][kCoef2];   // SR, LR coefficients, padded layout (kCi, kCj, kCk)
   double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
   double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
-  V2 uu[3][kP][kRS];         // (e, e d) of each site pair, families ij, ik, jk
-  V2 dl[3][kP][kRS];         // (d, d ln e / dr)
+  double2 uu[3][kP][kRS];    // (e, e d) of each site pair, families ij, ik, jk
+  double2 dl[3][kP][kRS];    // (d, d ln e / dr)
+  LowUU<T> uul;              // FP32 copy of uu (mixed form)
   double G[3][kP][kRS];      // accumulated site-force weights
   double red[kFs3Block / 32];
   Fs3Rec rec;
@@ -203,34 +219,13 @@ template <typename T>
 struct Fs3Grad {
   double gc[2][kCoef];
   double gb[2][3][kPairs];
-  T exd[3][kP][kRS];
+  double exd[3][kP][kRS];
 };
 
 template <typename T>
 __host__ __device__ constexpr size_t fs3_grad_offset() {
   return (sizeof(Fs3Smem<T>) + 15) & ~size_t(15);
 }
-
-template <typename T>
-__device__ __forceinline__ T t_exp(T v);
-template <>
-__device__ __forceinline__ double t_exp<double>(double v) { return exp(v); }
-template <>
-__device__ __forceinline__ float t_exp<float>(float v) { return __expf(v); }
-
-template <typename T>
-__device__ __forceinline__ T t_sqrt(T v);
-template <>
-__device__ __forceinline__ double t_sqrt<double>(double v) { return sqrt(v); }
-template <>
-__device__ __forceinline__ float t_sqrt<float>(float v) { return sqrtf(v); }
-
-template <typename T>
-__device__ __forceinline__ T t_rcp(T v);
-template <>
-__device__ __forceinline__ double t_rcp<double>(double v) { return 1.0 / v; }
-template <>
-__device__ __forceinline__ float t_rcp<float>(float v) { return __frcp_rn(v); }
 
 // One gradient pass for the 2x2 output tile (r0, r0+1) x (c0, c0+1), generic over the three
 // pair families (one code path keeps the instruction footprint small):
@@ -263,17 +258,17 @@ __device__ __forceinline__ PassCfg pass_cfg(int fam) {
 // With GRAD and a family-0 pass (outputs are the ij pairs), gcv also receives, for each type
 // block and power combination, wsite * sum_tile U_z(ij) M_u: the derivative of the sweep's
 // energy sum with respect to that coefficient-table entry, index 4y + 2x + z.
+// U is the (e, e d) table (3 families of kP x kRS entries) in the pass's arithmetic T.
 template <typename T, bool GRAD>
-__device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__restrict__ C,
-                                         const PassCfg &g, int r0, int c0, T q0[4], T q1[4],
-                                         double *gcv, double wsite) {
+__device__ __forceinline__ void fs3_pass(const typename Vec2<T>::type *U,
+                                         const double *__restrict__ C, const PassCfg &g, int r0,
+                                         int c0, T q0[4], T q1[4], double *gcv, double wsite) {
   using V2 = typename Vec2<T>::type;
-  const V2 *U = &S.uu[0][0][0];
   const int tr = kPType[r0], tc = kPType[c0];
   V2 Ut[4];
   if (GRAD && gcv) {
 #pragma unroll
-    for (int o = 0; o < 4; o++) Ut[o] = S.uu[0][sp(r0 + (o >> 1))][sp(c0 + (o & 1))];
+    for (int o = 0; o < 4; o++) Ut[o] = U[sp(r0 + (o >> 1)) * kRS + sp(c0 + (o & 1))];
   }
   const double *cbase = C + tr * g.mr + tc * g.mc;
   // physical rows/columns of the tile (r0, c0 even): sp(r0) = r0/2, sp(r0+1) = 9 + r0/2
@@ -339,28 +334,25 @@ __device__ __forceinline__ void fs3_pass(const Fs3Smem<T> &S, const double *__re
 // the three gradient passes, add wsite * G into S.G and return the energy sum.
 template <typename T, bool GRAD>
 __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite) {
-  using V2 = typename Vec2<T>::type;
+  constexpr bool kLow = sizeof(T) == 4;
   const int tid = threadIdx.x;
   if (tid < kPairs) {
     const int a = tid / kNs3, b = tid % kNs3;
-    const T bb = (T)S.bgr[v][0][tid], gg = (T)S.bgr[v][1][tid], r0 = (T)S.bgr[v][2][tid];
+    const double bb = S.bgr[v][0][tid], gg = S.bgr[v][1][tid], r0 = S.bgr[v][2][tid];
 #pragma unroll 1
     for (int p = 0; p < 3; p++) {
       const int m1 = p == 2 ? 1 : 0, m2 = p == 0 ? 1 : 2;
       const double vx = S.rec.cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
       const double vy = S.rec.cv[p][1] + (S.site[m1][a][1] - S.site[m2][b][1]);
       const double vz = S.rec.cv[p][2] + (S.site[m1][a][2] - S.site[m2][b][2]);
-      const T r = t_sqrt<T>((T)(vx * vx + vy * vy + vz * vz));
-      const T ex = t_exp<T>(-gg * (r - r0));
-      const T damp = t_rcp<T>((T)1 + ex);
-      const T e = t_exp<T>(-bb * r) * damp;
-      V2 u, w;
-      u.x = e;
-      u.y = e * r;
-      w.x = r;
-      w.y = -bb + gg * ex * damp;
+      const double r = sqrt(vx * vx + vy * vy + vz * vz);
+      const double ex = exp(-gg * (r - r0));
+      const double damp = 1.0 / (1.0 + ex);
+      const double e = exp(-bb * r) * damp;
+      const double2 u = make_double2(e, e * r);
       S.uu[p][sp(pidx(a))][sp(pidx(b))] = u;
-      S.dl[p][sp(pidx(a))][sp(pidx(b))] = w;
+      S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(r, -bb + gg * ex * damp);
+      if constexpr (kLow) S.uul.v[p][sp(pidx(a))][sp(pidx(b))] = make_float2((float)u.x, (float)u.y);
       if (GRAD) GS->exd[p][sp(pidx(a))][sp(pidx(b))] = ex * damp;
     }
   }
@@ -370,23 +362,38 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
   if (fam < 3 && lt < kTile * kTile) {
     const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
     const PassCfg g = pass_cfg(fam);
-    T q0[4], q1[4];
-    fs3_pass<T, GRAD>(S, reinterpret_cast<const double *>(S.coef[v]), g, r0, c0, q0, q1,
-                      (GRAD && fam == 0) ? GS->gc[v] : nullptr, wsite);
+    const double *C = reinterpret_cast<const double *>(S.coef[v]);
+    double q0[4], q1[4];
+    bool done = false;
+    if constexpr (kLow) {
+      if (fam != 0) {  // warp-uniform: 96 pass threads per family
+        float f0[4], f1[4];
+        fs3_pass<float, false>(&S.uul.v[0][0][0], C, g, r0, c0, f0, f1, nullptr, wsite);
+#pragma unroll
+        for (int o = 0; o < 4; o++) {
+          q0[o] = f0[o];
+          q1[o] = f1[o];
+        }
+        done = true;
+      }
+    }
+    if (!done)
+      fs3_pass<double, GRAD>(&S.uu[0][0][0], C, g, r0, c0, q0, q1,
+                             (GRAD && fam == 0) ? GS->gc[v] : nullptr, wsite);
 #pragma unroll
     for (int o = 0; o < 4; o++) {
       const int r = sp(r0 + (o >> 1)), c = sp(c0 + (o & 1));
-      const V2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
-      const T P = q0[o] + w.x * q1[o];
-      if (fam == 0) esum += (double)u.x * (double)P;
-      S.G[fam][r][c] += wsite * (double)(u.x * (w.y * P + q1[o]) / w.x);
+      const double2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
+      const double P = q0[o] + w.x * q1[o];
+      if (fam == 0) esum += u.x * P;
+      S.G[fam][r][c] += wsite * (u.x * (w.y * P + q1[o]) / w.x);
       const int ra = r0 + (o >> 1), cb = c0 + (o & 1);
       if (GRAD && ra != 1 && cb != 1) {
         // dS/de_ab = P; de/db = -r e, de/dg = (r - r0) e x, de/dr0 = -g e x with
         // x = exp(-g (r - r0)) / (1 + exp(-g (r - r0)))
         const int q = (ra == 0 ? 0 : ra - 1) * kNs3 + (cb == 0 ? 0 : cb - 1);
-        const double wPe = wsite * (double)P * (double)u.x;
-        const double rr = (double)w.x, xd = (double)GS->exd[fam][r][c];
+        const double wPe = wsite * P * u.x;
+        const double rr = w.x, xd = GS->exd[fam][r][c];
         atomicAdd(&GS->gb[v][0][q], -wPe * rr);
         atomicAdd(&GS->gb[v][1][q], wPe * (rr - S.bgr[v][2][q]) * xd);
         atomicAdd(&GS->gb[v][2][q], -wPe * S.bgr[v][1][q] * xd);
@@ -411,7 +418,6 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
           const double4 *__restrict__ s17, const double *__restrict__ coef,
           const double *__restrict__ bgr, int nm, int ns, double *f, double *fc3, double *scal,
           double *gfs3) {
-  using V2 = typename Vec2<T>::type;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
   Fs3Grad<T> *GS = GRAD ? reinterpret_cast<Fs3Grad<T> *>(smem_raw + fs3_grad_offset<T>()) : nullptr;
@@ -420,7 +426,7 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   if (GRAD) {
     for (int t = tid; t < 2 * kCoef; t += kFs3Block) (&GS->gc[0][0])[t] = 0.0;
     for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&GS->gb[0][0][0])[t] = 0.0;
-    for (int t = tid; t < 3 * kP * kRS; t += kFs3Block) (&GS->exd[0][0][0])[t] = (T)0;
+    for (int t = tid; t < 3 * kP * kRS; t += kFs3Block) (&GS->exd[0][0][0])[t] = 0.0;
   }
   for (int t = tid; t < 2 * kCoef2; t += kFs3Block) (&S.coef[0][0])[t] = make_double2(0.0, 0.0);
   __syncthreads();
@@ -435,14 +441,15 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   // padded dummy site: zero weight, unit distance (keeps e / d finite)
   for (int t = tid; t < 3 * kP; t += kFs3Block) {
     const int p = t / kP, q = t % kP;
-    V2 z, one;
-    z.x = z.y = (T)0;
-    one.x = (T)1;
-    one.y = (T)0;
+    const double2 z = make_double2(0.0, 0.0), one = make_double2(1.0, 0.0);
     S.uu[p][sp(1)][q] = z;
     S.uu[p][q][sp(1)] = z;
     S.dl[p][sp(1)][q] = one;
     S.dl[p][q][sp(1)] = one;
+    if constexpr (sizeof(T) == 4) {
+      S.uul.v[p][sp(1)][q] = make_float2(0.f, 0.f);
+      S.uul.v[p][q][sp(1)] = make_float2(0.f, 0.f);
+    }
   }
   const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
   const double conv = kH2kcal * 418.4 / kBohr2a;

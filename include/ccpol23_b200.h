@@ -36,8 +36,9 @@ extern "C" {
 
 /* precision forms of a context */
 #define CCP_FP64 0   /* plain FP64 everywhere */
-#define CCP_MIXED 1  /* FP32 three-body geometry/terms with FP64 accumulation; FP64
-                        Ewald, induction and all totals */
+#define CCP_MIXED 1  /* FP32 for two of the three FS3 gradient passes (the ik and jk
+                        pair families); FP64 for the FS3 site-pair tables, its energy pass,
+                        FS2, Ewald, induction and all sums */
 
 typedef struct ccp_model ccp_model;
 typedef struct ccp_context ccp_context;

@@ -200,11 +200,12 @@ def test_fs2_known_answer_on_gpu(product):
 
 
 def test_mixed_precision_hot_path(product, boxes):
-    """Mixed form (FP32 three-body terms, FP64 accumulation, FP64 Ewald/induction) against
-    the FP64 form on the same box: site forces and torques within 1e-5.  The FS3 sum itself is
-    ill-conditioned (sum |terms| / |sum| is 1e4-6e5 per molecular triple with coefficients up
-    to 9e5 of both signs), so its FP32 energy error is ~1e-4 relative; the per-molecule force,
-    which carries the FS3 COM term proportional to that energy, is bounded at 5e-5."""
+    """Mixed form (FP32 ik/jk gradient passes of FS3; FP64 FS3 tables and energy pass, FS2,
+    Ewald and induction) against the FP64 form on the same box: site forces and torques
+    within 1e-5, per-molecule forces within 2e-5.  The FS3 sum is ill-conditioned (sum |terms| / |sum| is
+    1e4-6e5 per molecular triple, coefficients up to 9e5 of both signs), which is why its
+    energy pass, and with it the R_avg-damping COM force, stays FP64: the FS3 energy then
+    agrees with the FP64 form to round-off."""
     m, b, M = boxes["fs2fs3_128"]
     out = {}
     for prec in ("fp64", "mixed"):
@@ -224,13 +225,16 @@ def test_mixed_precision_hot_path(product, boxes):
     Fmx = np.stack([out["mixed"].fxs, out["mixed"].fys, out["mixed"].fzs])
     assert rel(Fmx, F64) <= MIXED_FTOL, rel(Fmx, F64)
     assert rel(qmx, q64) <= MIXED_FTOL, rel(qmx, q64)
-    # the per-molecule force includes the FS3 COM force, d f_dmp/dR_avg times the FS3
-    # energy sum, whose FP32 error is set by the sum's conditioning (see module docstring)
-    assert rel(tmx, t64) <= 5 * MIXED_FTOL, rel(tmx, t64)
+    # the per-molecule sums cancel more than the site forces they add up; at 512 waters
+    # this error is 7e-6, in this 128-water box 1.2e-5
+    assert rel(tmx, t64) <= 2 * MIXED_FTOL, rel(tmx, t64)
+    C64 = np.stack([out["fp64"].fxfs3, out["fp64"].fyfs3, out["fp64"].fzfs3])
+    Cmx = np.stack([out["mixed"].fxfs3, out["mixed"].fyfs3, out["mixed"].fzfs3])
+    assert rel(Cmx, C64) <= 1e-10, rel(Cmx, C64)
     e64, emx = out["fp64"].energies, out["mixed"].energies
-    for k in ("scpe", "rcpe", "kcpe", "indpe"):
+    for k in ("scpe", "rcpe", "kcpe", "indpe", "fs2pe"):
         assert emx[k] == pytest.approx(e64[k], rel=1e-12)
-    assert abs(emx["fs3pe"] - e64["fs3pe"]) <= 1e-3 * abs(e64["fs3pe"])
+    assert emx["fs3pe"] == pytest.approx(e64["fs3pe"], rel=1e-10)
 
 
 def test_maxit_reports_not_converged(product, boxes):
