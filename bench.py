@@ -280,6 +280,56 @@ def equilibrate(ctx, box, nsteps, temp=298.0, every=20):
     return ctx.md_get_state()
 
 
+def run_batch(nframes, steps, warmup):
+    """Batches of independent 256-water FS3 frames (L = 19.71 A, seed 4004 + f), the
+    three-body plus induction terms that the autograd binding evaluates: device-resident
+    inputs, frames one by one on one context against one ccp_batch_terms_device call per
+    batch (slots 1 / 8 / nframes).  Wall time per batch on the host, device synchronised on
+    both sides; prints one JSON line, not the headline metric."""
+    import torch
+    from ccpol23_plus_2025_mbmd_b200 import Batch, Context, Model, data_dir, _lib
+    from ccpol23_plus_2025_mbmd_b200.generator import CONFIGS, water_box
+    cfg = CONFIGS["c4_256"]
+    model = Model(data_dir(cfg["variant"]))
+    boxes = [water_box(model, cfg["nm"], cfg["box"], cfg["seed"] + f) for f in range(nframes)]
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    x, y, z, xs, ys, zs = (T(np.stack([getattr(b, k) for b in boxes]))
+                           for k in ("x", "y", "z", "xs", "ys", "zs"))
+    f = [torch.zeros_like(xs) for _ in range(3)]
+    terms = _lib.TERM_INDUCTION | _lib.TERM_FS2 | _lib.TERM_FS3
+    nm, L = cfg["nm"], cfg["box"]
+
+    def timed(run):
+        for _ in range(warmup):
+            run()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            run()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / steps
+
+    out = {}
+    with Context(model, nm, L) as c:
+        def one_by_one():
+            for k in range(nframes):
+                c.terms_device(terms, x[k], y[k], z[k], xs[k], ys[k], zs[k], L, f[0][k], f[1][k],
+                               f[2][k])
+        out["frame_by_frame"] = timed(one_by_one)
+    for slots in sorted({1, 8, nframes}):
+        with Batch(model, nm, L, slots=slots) as b:
+            out[f"batch_slots{slots}"] = timed(
+                lambda: b.terms_device(terms, L, x, y, z, xs, ys, zs, *f))
+    line = {"metric": f"batch of {nframes} x {nm}-water FS3 frames, three-body + induction",
+            "unit": "ms per batch", "steps": steps, "warmup": warmup,
+            "config": {"nm": nm, "box_A": L, "variant": cfg["variant"], "seed": cfg["seed"],
+                       "frames": nframes},
+            **{k: v * 1e3 for k, v in out.items()},
+            "frames_per_s": {k: nframes / v for k, v in out.items()}}
+    print(json.dumps(line), flush=True)
+
+
 def run_nve(nsteps, nequil):
     """Rigid-water NVE MD on the device (2-body + hot path + nve_1), FP64 and mixed forms from
     the same equilibrated state: time per MD step and the energy drift (linear fit of the
@@ -332,6 +382,9 @@ def main():
                     help="run STEPS NVE MD steps per form and print the drift line instead")
     ap.add_argument("--nve-equil", type=int, default=4000, metavar="STEPS",
                     help="velocity-rescaled equilibration steps before the NVE run")
+    ap.add_argument("--batch", type=int, default=0, metavar="FRAMES",
+                    help="time FRAMES 256-water FS3 frames (three-body + induction terms) one "
+                         "by one and as one batch call, and print that line instead")
     ap.add_argument("--host-loop", action="store_true",
                     help="with --single: drive the dipole iteration from the host, so that "
                          "profilers see its kernels")
@@ -344,6 +397,9 @@ def main():
         return
     if args.nve:
         run_nve(args.nve, args.nve_equil)
+        return
+    if args.batch:
+        run_batch(args.batch, args.steps, args.warmup)
         return
     import torch
     rank, world, local = dist_env()

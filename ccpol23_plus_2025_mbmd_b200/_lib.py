@@ -36,7 +36,9 @@ EXPORTS = [
     "ccp_kspace_ewald_fixed", "ccp_context_set_option", "ccp_context_get_option",
     "ccp_terms_device", "ccp_context_get_fs3_params", "ccp_context_set_fs3_params",
     "ccp_context_fs3_param_grad", "ccp_ccpol23plus", "ccp_md_set_state", "ccp_md_get_state",
-    "ccp_md_nve", "ccp_md_get_dipoles",
+    "ccp_md_nve", "ccp_md_get_dipoles", "ccp_batch_create", "ccp_batch_destroy",
+    "ccp_batch_slots", "ccp_batch_context", "ccp_batch_set_option", "ccp_batch_set_fs3_params",
+    "ccp_batch_terms_device",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
@@ -116,6 +118,14 @@ def lib():
     L.ccp_context_set_option.argtypes = [vp, C.c_char_p, i]
     L.ccp_context_get_option.argtypes = [vp, C.c_char_p, pi]
     L.ccp_kspace_ewald_fixed.argtypes = [vp, i] + [vp] * 6 + [i, i, i, i, d, d] + [vp] * 5 + [vp]
+    L.ccp_batch_create.argtypes = [vp, i, d, i, i, i, C.POINTER(vp)]
+    L.ccp_batch_destroy.argtypes = [vp]
+    L.ccp_batch_slots.argtypes = [vp, pi]
+    L.ccp_batch_context.argtypes = [vp, i, C.POINTER(vp)]
+    L.ccp_batch_set_option.argtypes = [vp, C.c_char_p, i]
+    L.ccp_batch_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
+    L.ccp_batch_terms_device.argtypes = ([vp, C.c_uint, i, vp] + [vp] * 6 + [i, vp] + [vp] * 12
+                                         + [vp, i])
     _lib = L
     return L
 

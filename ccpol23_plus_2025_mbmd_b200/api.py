@@ -377,3 +377,79 @@ class Context:
             dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
             dp(fzfs3), dp(idmx), dp(idmy), dp(idmz)))
         return _energies(e)
+
+
+class Batch:
+    """Independent frames of ``nm`` molecules evaluated concurrently: ``slots`` contexts
+    (own device buffers and CUDA streams each), frame f on slot f % slots, one host worker
+    thread per slot inside the library (``ccp_batch_terms_device``)."""
+
+    def __init__(self, model: Model, nm: int, box0: float, slots: int = 8, device: int = 0,
+                 precision: str = "fp64"):
+        prec = {"fp64": _lib.CCP_FP64, "mixed": _lib.CCP_MIXED}[precision]
+        h = C.c_void_p()
+        check(_lib.lib().ccp_batch_create(model.handle, nm, box0, slots, device, prec,
+                                          C.byref(h)))
+        self._h = h
+        self.model = model
+        self.nm = nm
+        self.slots = slots
+        self.precision = precision
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.lib().ccp_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may already be gone
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_option(self, name: str, value: int):
+        check(_lib.lib().ccp_batch_set_option(self._h, name.encode(), int(value)))
+
+    def set_fs3_params(self, cs_sr, cs_lr, bgr_sr, bgr_lr):
+        a = [np.ascontiguousarray(v, dtype=np.float64) for v in (cs_sr, cs_lr, bgr_sr, bgr_lr)]
+        check(_lib.lib().ccp_batch_set_fs3_params(self._h, ptr(a[0]), ptr(a[1]), a[0].size,
+                                                   ptr(a[2]), ptr(a[3])))
+
+    def fs3_params(self):
+        """The FS3 fit of slot 0 (every slot holds the same fit)."""
+        h = C.c_void_p()
+        check(_lib.lib().ccp_batch_context(self._h, 0, C.byref(h)))
+        n = self.model.get_int("nclass")
+        cs_sr, cs_lr = np.zeros(n), np.zeros(n)
+        b_sr, b_lr = np.zeros((3, 289)), np.zeros((3, 289))
+        check(_lib.lib().ccp_context_get_fs3_params(h, ptr(cs_sr), ptr(cs_lr), n, ptr(b_sr),
+                                                     ptr(b_lr)))
+        return cs_sr, cs_lr, b_sr, b_lr
+
+    def terms_device(self, terms, box, x, y, z, xs, ys, zs, fxs=None, fys=None, fzs=None,
+                     fxfs2=None, fyfs2=None, fzfs2=None, fxfs3=None, fyfs3=None, fzfs3=None,
+                     idmx=None, idmy=None, idmz=None, pgrad=None) -> list:
+        """The terms selected by ``terms`` for every frame.  x, y, z: (nframes, nm) and xs,
+        ys, zs: (nframes, nm, ld) torch CUDA float64 tensors, outputs likewise; ``box`` is a
+        sequence of nframes box lengths; ``pgrad`` an optional (nframes, 2 nclass + 1734)
+        float64 numpy array for the per-frame FS3 parameter gradients.  Returns the
+        per-frame energy dicts."""
+        def dp(t):
+            return None if t is None else t.data_ptr()
+        nf = x.shape[0]
+        ld = xs.shape[2]
+        boxes = np.ascontiguousarray(np.broadcast_to(np.asarray(box, dtype=np.float64), (nf,)))
+        e = (CcpEnergies * max(nf, 1))()
+        plen = 0 if pgrad is None else pgrad.shape[1]
+        check(_lib.lib().ccp_batch_terms_device(
+            self._h, int(terms), nf, ptr(boxes), dp(x), dp(y), dp(z), dp(xs), dp(ys), dp(zs), ld,
+            e, dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
+            dp(fzfs3), dp(idmx), dp(idmy), dp(idmz), ptr(pgrad), plen))
+        return [_energies(e[f]) for f in range(nf)]
+

@@ -17,7 +17,12 @@ The adjoint is hand-written in the library, not traced:
 
 One forward call is one evaluation (energy, forces and, when any FS3 parameter requires a
 gradient, the parameter gradient); backward only scales them by the incoming gradient.
-Frames of a batch are separate calls on the same context.
+
+Batches: with a ``Batch`` in place of the context, ``com`` (B, nm, 3) and ``sites``
+(B, nm, ns, 3) hold B independent frames and the result is the (B,) vector of their
+energies.  The frames are evaluated concurrently (``ccp_batch_terms_device``); the
+parameter gradient of frame f is kept per frame, so backward weights it by the incoming
+gradient of that frame's energy.
 """
 from __future__ import annotations
 
@@ -69,12 +74,59 @@ class _ThreeBodyInduction(torch.autograd.Function):
         return (None, None, grad * g_com, grad * g_sites, *gp)
 
 
+class _ThreeBodyInductionBatch(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, batch, box, com, sites, cs_sr, cs_lr, bgr_sr, bgr_lr):
+        dev = com.device
+        params = [cs_sr, cs_lr, bgr_sr, bgr_lr]
+        cur = batch.fs3_params()
+        new = [p.detach().cpu().numpy().astype(np.float64).reshape(c.shape) for p, c in zip(params, cur)]
+        if any(not np.array_equal(a, b) for a, b in zip(new, cur)):
+            batch.set_fs3_params(*new)
+        want_p = any(p.requires_grad for p in params)
+        batch.set_option("fs3_param_grad", 1 if want_p else 0)
+        nf, nm, ns = sites.shape[0], sites.shape[1], sites.shape[2]
+        x, y, z = (com[:, :, a].contiguous() for a in range(3))
+        xs, ys, zs = (sites[:, :, :, a].contiguous() for a in range(3))
+        f = [torch.zeros((nf, nm, ns), dtype=torch.float64, device=dev) for _ in range(3)]
+        c2 = [torch.zeros((nf, nm), dtype=torch.float64, device=dev) for _ in range(3)]
+        c3 = [torch.zeros((nf, nm), dtype=torch.float64, device=dev) for _ in range(3)]
+        ncoef = cur[0].size
+        pg = np.zeros((nf, 2 * ncoef + 2 * 3 * 289)) if want_p else None
+        terms = _lib.TERM_INDUCTION | _lib.TERM_FS2 | _lib.TERM_FS3
+        es = batch.terms_device(terms, box, x, y, z, xs, ys, zs, *f, *c2, *c3, pgrad=pg)
+        energy = [e["fs2pe"] + e["fs3pe"] + e["indpe"] for e in es]
+        F = torch.stack(f, dim=-1)                                     # (nf, nm, ns, 3)
+        Fc = torch.stack([c2[a] + c3[a] for a in range(3)], dim=-1)    # (nf, nm, 3)
+        fctx.save_for_backward(-(F.sum(dim=2) + Fc) / KCAL, -F / KCAL)
+        if want_p:
+            parts = np.split(pg, [ncoef, 2 * ncoef, 2 * ncoef + 867], axis=1)
+            fctx.gp = [torch.as_tensor(g, device=p.device, dtype=p.dtype).reshape((nf,) + tuple(p.shape))
+                       for g, p in zip(parts, params)]
+        else:
+            fctx.gp = [None] * 4
+        return torch.tensor(energy, dtype=torch.float64, device=dev)
+
+    @staticmethod
+    def backward(fctx, grad):
+        g_com, g_sites = fctx.saved_tensors
+        gp = [None if g is None else torch.tensordot(grad.to(g.device), g, dims=1) for g in fctx.gp]
+        return (None, None, grad[:, None, None] * g_com, grad[:, None, None, None] * g_sites, *gp)
+
+
 def three_body_induction_energy(context, box, com, sites, cs_sr, cs_lr, bgr_sr, bgr_lr):
-    """FS2 + FS3 + induction energy (kcal/mol) with analytic gradients (see module doc)."""
+    """FS2 + FS3 + induction energy (kcal/mol) with analytic gradients (see module doc).
+    With a ``Batch`` as ``context``: batched frames, (B,) energies; ``box`` is one length or
+    one per frame."""
+    from .api import Batch
+    if isinstance(context, Batch):
+        return _ThreeBodyInductionBatch.apply(context, box, com, sites, cs_sr, cs_lr, bgr_sr,
+                                              bgr_lr)
     return _ThreeBodyInduction.apply(context, box, com, sites, cs_sr, cs_lr, bgr_sr, bgr_lr)
 
 
 def fs3_param_tensors(context, device, requires_grad=True):
-    """The context's current FS3 fit as float64 tensors, ready to be optimised."""
+    """The current FS3 fit of a context (or batch) as float64 tensors, ready to be
+    optimised."""
     return [torch.tensor(a, dtype=torch.float64, device=device, requires_grad=requires_grad)
             for a in context.fs3_params()]

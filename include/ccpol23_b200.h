@@ -236,6 +236,39 @@ int ccp_context_set_fs3_params(ccp_context *ctx, const double *cs_sr, const doub
 int ccp_context_fs3_param_grad(ccp_context *ctx, double *dcs_sr, double *dcs_lr, int ncoef,
                                double *dbgr_sr, double *dbgr_lr);
 
+/* ------------------------------------------------------ batches of independent frames */
+/* No counterpart in the reference, which evaluates one configuration per call.  A batch
+   owns `slots` contexts of nm molecules (own device buffers and CUDA streams each).
+   ccp_batch_terms_device evaluates nframes independent frames: frame f runs on slot
+   f % slots, with one host worker thread per slot, so up to `slots` frames are in flight on
+   the GPU at once.  Results equal those of ccp_terms_device called frame by frame.  Device
+   arrays hold the frames one after another: x[f*nm + i], xs[(f*nm + i)*ld + s] (and the
+   same for every output), box[f] and e[f] on the host.  With pgrad non-null (the option
+   "fs3_param_grad" on, set with ccp_batch_set_option) frame f's FS3 parameter gradient goes
+   to pgrad[f*pgrad_len ...]: dcs_sr, dcs_lr (ncoef each), dbgr_sr, dbgr_lr (867 each),
+   pgrad_len = 2 ncoef + 1734.  The first failing frame's status is returned, with its index
+   in ccp_last_error(); a slot stops at its first failure.  Calls on one batch must not
+   overlap. */
+typedef struct ccp_batch ccp_batch;
+int ccp_batch_create(const ccp_model *m, int nm, double box0, int slots, int device,
+                     int precision, ccp_batch **out);
+int ccp_batch_destroy(ccp_batch *b);
+int ccp_batch_slots(const ccp_batch *b, int *slots);
+/* the context of one slot (options, FS3 parameters, diagnostics of its last frame) */
+int ccp_batch_context(ccp_batch *b, int slot, ccp_context **ctx);
+int ccp_batch_set_option(ccp_batch *b, const char *name, int value);
+int ccp_batch_set_fs3_params(ccp_batch *b, const double *cs_sr, const double *cs_lr, int ncoef,
+                             const double *bgr_sr, const double *bgr_lr);
+int ccp_batch_terms_device(ccp_batch *b, unsigned terms, int nframes, const double *box,
+                           const double *x_device, const double *y_device,
+                           const double *z_device, const double *xs_device,
+                           const double *ys_device, const double *zs_device, int ld,
+                           ccp_energies *e, double *fxs_device, double *fys_device,
+                           double *fzs_device, double *fxfs2_device, double *fyfs2_device,
+                           double *fzfs2_device, double *fxfs3_device, double *fyfs3_device,
+                           double *fzfs3_device, double *idmx_device, double *idmy_device,
+                           double *idmz_device, double *pgrad, int pgrad_len);
+
 /* --------------------------------------------------- NVE molecular dynamics (device) */
 /* The reference's rigid-molecule NVE integrator, nve_1 with the nosquish rotation
    (evolve.f90:621-1061, 8107-8203), with the state resident on the device: centres x, y, z
