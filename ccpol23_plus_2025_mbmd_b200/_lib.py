@@ -38,7 +38,7 @@ EXPORTS = [
     "ccp_context_fs3_param_grad", "ccp_ccpol23plus", "ccp_md_set_state", "ccp_md_get_state",
     "ccp_md_nve", "ccp_md_get_dipoles", "ccp_batch_create", "ccp_batch_destroy",
     "ccp_batch_slots", "ccp_batch_context", "ccp_batch_set_option", "ccp_batch_set_fs3_params",
-    "ccp_batch_terms_device",
+    "ccp_batch_terms_device", "ccp_md_set_equilibration", "ccp_md_get_stats",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
@@ -111,6 +111,8 @@ def lib():
     L.ccp_md_get_state.argtypes = [vp] + [vp] * 6
     L.ccp_md_nve.argtypes = [vp, i, d, vp]
     L.ccp_md_get_dipoles.argtypes = [vp, i, vp, vp, vp]
+    L.ccp_md_set_equilibration.argtypes = [vp, d, i]
+    L.ccp_md_get_stats.argtypes = [vp, vp]
     L.ccp_terms_device.argtypes = [vp, C.c_uint] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_context_get_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
     L.ccp_context_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]

@@ -333,6 +333,16 @@ class Context:
         check(_lib.lib().ccp_md_get_dipoles(self._h, ns, *[ptr(a) for a in out]))
         return out
 
+    def md_set_equilibration(self, temp0: float, nsteps: int):
+        """The next nsteps md_nve steps rescale velocities and angular momenta to temp0."""
+        check(_lib.lib().ccp_md_set_equilibration(self._h, float(temp0), int(nsteps)))
+
+    def md_stats(self) -> dict:
+        """Statistics of the current MD state (no step)."""
+        s = _lib.CcpMdStats()
+        check(_lib.lib().ccp_md_get_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in _lib.CcpMdStats._fields_}
+
     def md_nve(self, nsteps: int, dt: float) -> list:
         """nve_1 steps on the device; per-step energies, temperature, virial, pressure."""
         stats = (_lib.CcpMdStats * max(nsteps, 1))()

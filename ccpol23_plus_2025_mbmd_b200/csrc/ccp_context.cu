@@ -109,6 +109,8 @@ struct ccp_context {
          *d_md_j = nullptr, *d_md_red = nullptr, *h_md = nullptr;
   bool md_ready = false;
   double md_box = 0;
+  int md_eq_left = 0;      // MD steps still to be followed by the equilibration rescale
+  double md_eq_temp = 0;   // its target temperature (K)
   ccp_energies md_e{};
   // ccpol23plus 2-body tables
   bool have_vdw = false;
@@ -1639,6 +1641,34 @@ int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, dou
   return download_dipoles(ctx, ld, idmx, idmy, idmz);
 }
 
+}  // extern "C"
+
+namespace {
+// md.f90:169-176 and evolve.f90:1020-1052 (initialization.f90:76-89, 386-399 for the initial
+// state): energies of the last evaluation, kinetic energies, temperature, virial and pressure
+// from the sums in h_md = {sum v^2, sum J^2 / I, sum f . xs}
+void md_fill_stats(const ccp_context *ctx, ccp_md_stats &S) {
+  const ccp_energies &e = ctx->md_e;
+  const double box = ctx->md_box;
+  const double tke = 0.5 * ctx->totm * ctx->h_md[0], rke = 0.5 * ctx->h_md[1];
+  const double qvir = e.vir + ctx->h_md[2];
+  S.vdwpe = e.vdwpe;
+  S.cpe = e.scpe + e.rcpe + e.kcpe;
+  S.indpe = e.indpe;
+  S.pe3b = e.fs2pe + e.fs3pe;
+  S.pe = S.vdwpe + S.cpe + S.indpe + S.pe3b;
+  S.tke = tke / 418.4;
+  S.rke = rke / 418.4;
+  S.te = S.tke + S.rke + S.pe;
+  S.sys_temp = 2.0 * (tke + rke) / (3.0 * kBoltz * (2.0 * ctx->nm - 1.0));
+  S.vir = qvir / 418.4;
+  S.pres = kPrsunt * (2.0 * tke - qvir) / (3.0 * box * box * box);
+  S.ind_iters = e.ind_iters;
+}
+}  // namespace
+
+extern "C" {
+
 int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
   if (!ctx || nsteps < 0 || !(dt > 0.0)) return CCP_ERR_BAD_INPUT;
   if (!ctx->md_ready) {
@@ -1667,26 +1697,46 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
                         ctx->d_md_red, st));
     CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (stats) {
-      const ccp_energies &e = ctx->md_e;
-      // md.f90:169-176 and evolve.f90:1020-1052: step energies, temperature, pressure
+    if (stats) md_fill_stats(ctx, stats[k]);
+    if (ctx->md_eq_left > 0) {
+      // md.f90:187-193: after the step, velocities and angular momenta to temp0
+      // (equilibrationGRU, utility.f90:353-368; trans_temp / rot_temp :196-227)
       const double tke = 0.5 * ctx->totm * ctx->h_md[0], rke = 0.5 * ctx->h_md[1];
-      const double qvir = e.vir + ctx->h_md[2];
-      ccp_md_stats &S = stats[k];
-      S.vdwpe = e.vdwpe;
-      S.cpe = e.scpe + e.rcpe + e.kcpe;
-      S.indpe = e.indpe;
-      S.pe3b = e.fs2pe + e.fs3pe;
-      S.pe = S.vdwpe + S.cpe + S.indpe + S.pe3b;
-      S.tke = tke / 418.4;
-      S.rke = rke / 418.4;
-      S.te = S.tke + S.rke + S.pe;
-      S.sys_temp = 2.0 * (tke + rke) / (3.0 * kBoltz * (2.0 * ctx->nm - 1.0));
-      S.vir = qvir / 418.4;
-      S.pres = kPrsunt * (2.0 * tke - qvir) / (3.0 * box * box * box);
-      S.ind_iters = e.ind_iters;
+      const double ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * kBoltz);
+      const double rtemp = 2.0 * rke / ((3.0 * nm) * kBoltz);
+      CK(launch_md_scale(ctx->nm, v, sqrt(ctx->md_eq_temp / ttemp), jv,
+                         sqrt(ctx->md_eq_temp / rtemp), st));
+      ctx->md_eq_left--;
     }
   }
+  return CCP_OK;
+}
+
+int ccp_md_set_equilibration(ccp_context *ctx, double temp0, int nsteps) {
+  if (!ctx || nsteps < 0 || (nsteps > 0 && !(temp0 > 0.0))) {
+    set_error("ccp_md_set_equilibration: need temp0 > 0 and nsteps >= 0");
+    return CCP_ERR_BAD_INPUT;
+  }
+  ctx->md_eq_temp = temp0;
+  ctx->md_eq_left = nsteps;
+  return CCP_OK;
+}
+
+int ccp_md_get_stats(ccp_context *ctx, ccp_md_stats *stats) {
+  if (!ctx || !stats) return CCP_ERR_BAD_INPUT;
+  if (!ctx->md_ready) {
+    set_error("ccp_md_get_stats: no MD state (call ccp_md_set_state first)");
+    return CCP_ERR_BAD_INPUT;
+  }
+  CK(cudaSetDevice(ctx->device));
+  const size_t nm = ctx->nm, nsi = nm * ctx->ns;
+  cudaStream_t st = ctx->stream;
+  const double *xs = ctx->d_md_xs;
+  CK(launch_md_sums(ctx->nm, ctx->ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
+                    ctx->d_md_v, ctx->d_md_j, ctx->pmi, ctx->d_md_red, st));
+  CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  md_fill_stats(ctx, *stats);
   return CCP_OK;
 }
 

@@ -178,6 +178,12 @@ cudaError_t launch_md_stage2(int nm, int ns, const double *f, const double *fc2,
                              const double *zs, double *x, double *y, double *z, double *v,
                              const double *q, double *j, const double pmi[3], double totm,
                              double dt, double box, double *red, cudaStream_t st);
+// Statistics sums of the current state into red = {sum v^2, sum J^2 / I, sum f . xs}.
+cudaError_t launch_md_sums(int nm, int ns, const double *f, const double *fc2, const double *fc3,
+                           const double *xs, const double *ys, const double *zs, const double *v,
+                           const double *j, const double pmi[3], double *red, cudaStream_t st);
+// v *= fv, j *= fj (3 nm each).
+cudaError_t launch_md_scale(int nm, double *v, double fv, double *j, double fj, cudaStream_t st);
 // ccpol23plus 2-body term (k_vdw.cu): site forces added to f (atomics), energy and virial
 // into scal[S_VDW_E], scal[S_VDW_VIR] (internal units).
 cudaError_t launch_vdw(const double *xs, const double *ys, const double *zs, int ld,

@@ -213,7 +213,61 @@ __global__ void k_md_stage2(int nm, int ns, const double *__restrict__ f,
   }
 }
 
+// Kinetic sums and the COM virial of the current state without moving it (the statistics
+// of initialization.f90:76-89, 386-399): v^2, J^2 / I and sum f . xs.
+__global__ void k_md_sums(int nm, int ns, const double *__restrict__ f,
+                          const double *__restrict__ fc2, const double *__restrict__ fc3,
+                          const double *__restrict__ xs, const double *__restrict__ ys,
+                          const double *__restrict__ zs, const double *__restrict__ v,
+                          const double *__restrict__ jv, double pmi0, double pmi1, double pmi2,
+                          double *red) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v2 = 0.0, j2 = 0.0, lv = 0.0;
+  if (i < nm) {
+    double F[3], T[3], lvir;
+    force_torque(i, nm, ns, f, fc2, fc3, xs, ys, zs, F, T, lvir);
+    const double vx = v[i], vy = v[nm + i], vz = v[2 * nm + i];
+    const double J0 = jv[i], J1 = jv[nm + i], J2 = jv[2 * nm + i];
+    v2 = vx * vx + vy * vy + vz * vz;
+    j2 = J0 * J0 / pmi0 + J1 * J1 / pmi1 + J2 * J2 / pmi2;
+    lv = lvir;
+  }
+  v2 = warp_sum(v2);
+  j2 = warp_sum(j2);
+  lv = warp_sum(lv);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&red[0], v2);
+    atomicAdd(&red[1], j2);
+    atomicAdd(&red[2], lv);
+  }
+}
+
+// Velocity rescaling of the equilibration phase (rescale_velocities, utility.f90:257-275):
+// COM velocities by fv, angular momenta by fj.
+__global__ void k_md_scale(int n, double *v, double fv, double *jv, double fj) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+    v[t] *= fv;
+    jv[t] *= fj;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_md_sums(int nm, int ns, const double *f, const double *fc2, const double *fc3,
+                           const double *xs, const double *ys, const double *zs, const double *v,
+                           const double *j, const double pmi[3], double *red, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(red, 0, 3 * sizeof(double), st);
+  if (e != cudaSuccess) return e;
+  k_md_sums<<<(nm + 127) / 128, 128, 0, st>>>(nm, ns, f, fc2, fc3, xs, ys, zs, v, j, pmi[0], pmi[1],
+                                              pmi[2], red);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_md_scale(int nm, double *v, double fv, double *j, double fj, cudaStream_t st) {
+  const int n = 3 * nm;
+  k_md_scale<<<(n + 255) / 256, 256, 0, st>>>(n, v, fv, j, fj);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_md_stage1(int nm, int ns, const double *f, const double *fc2,
                              const double *fc3, const double *xs, const double *ys,

@@ -4,15 +4,17 @@
 
 RUN_DIR holds the reference's inputs: CONTROL, FIELD, data3b_full, data3b_full_LR_4p5 and,
 when CONTROL's restart flag is T, REVCON.  The run writes, in the reference's formats:
-- OUTPUT: one row per step (md.f90:213-215);
+- OUTPUT: the initial state's row when the run starts at t = 0, then one row per step
+  (md.f90:148-152, 213-215);
 - HISTORY: sites 1-5 of every molecule with their induced dipoles, every hist_freq steps
   (md.f90:227-238);
 - REVCON: the final state (md.f90:266-276).
 
 The state stays on the device between steps; only the per-step scalars and the HISTORY frames
-come back.  Without a REVCON the start is the seeded lattice of generator.water_box at the
-FIELD's molecule count and 0.997 g/cm^3, with Maxwell-Boltzmann velocities at CONTROL's
-temperature.  The reference also writes induced-dipole sums (fort.501) and averages; this
+come back.  Steps up to CONTROL's nequil rescale the velocities and angular momenta to its
+temperature after the step, as the reference does for nve.  Without a REVCON the start is
+the seeded lattice of generator.water_box at the FIELD's molecule count and 0.997 g/cm^3,
+with Maxwell-Boltzmann velocities at CONTROL's temperature.  The reference also writes induced-dipole sums (fort.501) and averages; this
 driver does not.
 """
 from __future__ import annotations
@@ -65,12 +67,17 @@ def _e16(v):  # Fortran 1p,e16.8
     return f"{v:16.8E}"
 
 
-def output_row(step, t, s, nm, box, totm):
-    """One OUTPUT row (md.f90:169-176, 213-215): '(1x,i8,1p,15e16.8)'."""
+def output_row(step, t, s, nm, box, totm, initial=False):
+    """One OUTPUT row (md.f90:169-176, 213-215): '(1x,i8,1p,15e16.8)'.  The row of the
+    initial state (md.f90:119-152) forms HV as -pe/nm + 0.0019872036 T, the rows of the
+    steps as (-pe + 0.0019872036 T)/nm; both as the reference writes them."""
     volm = box ** 3
     rho = (totm * nm) / (volm * 1e-24 * 6.022e23)
     enth = (s["pe"] + (s["pres"] * volm) * 2.42e-26) / nm
-    hv = (-s["pe"] + 0.0019872036 * s["sys_temp"]) / nm
+    if initial:
+        hv = -s["pe"] / nm + 0.0019872036 * s["sys_temp"]
+    else:
+        hv = (-s["pe"] + 0.0019872036 * s["sys_temp"]) / nm
     vals = (t, s["sys_temp"], s["tke"] + s["rke"], s["vdwpe"], s["cpe"], s["indpe"], s["pe3b"],
             s["pe"], s["te"], s["vir"], s["pres"], volm, rho, enth, hv)
     return " " + f"{step:8d}" + "".join(_e16(v) for v in vals)
@@ -137,10 +144,14 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
     stats = []
     with Context(m, nm, box, device=device, precision=precision) as c:
         c.md_set_state(box, state["x"], state["y"], state["z"], state["v"], state["q"], state["j"])
+        # md.f90:187-193: steps up to nequil are followed by the velocity rescaling
+        c.md_set_equilibration(m.get_double("temp0"), min(max(nequil - step0, 0), nsteps))
         with open(out_dir / "OUTPUT", "w") as fo, open(out_dir / "HISTORY", "w") as fh:
             fo.write("-" * 250 + "\n")
             fo.write("".join(f"{c_:>16s}" for c_ in OUTPUT_COLUMNS) + "\n")
             fo.write("-" * 250 + "\n")
+            if t0 == 0.0:  # md.f90:148-152: the initial state's row
+                fo.write(output_row(step0, t0, c.md_stats(), nm, box, totm, initial=True) + "\n")
             fh.write(" Created by Ommair\n" + f"{0:10d}{1:10d}{nm * 3:10d}\n")
             done = 0
             while done < nsteps:

@@ -294,6 +294,15 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
 /* Induced dipoles of the current MD state (its last evaluation), idm*[i*ld + is], for
    HISTORY output; non-polarisable sites get 0. */
 int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, double *idmz);
+/* The next nsteps steps of ccp_md_nve are equilibration steps (md.f90:187-193, `step <=
+   nequil` with the nve ensemble): after each, COM velocities and angular momenta are scaled
+   to temp0 by sqrt(temp0 / T_trans) and sqrt(temp0 / T_rot) (equilibrationGRU,
+   utility.f90:353-368).  The step's statistics are those before the scaling, as the
+   reference's OUTPUT row. */
+int ccp_md_set_equilibration(ccp_context *ctx, double temp0, int nsteps);
+/* Statistics of the current MD state without a step (the step-0 row that md.f90:148-152
+   writes for a run starting at t = 0; initialization.f90:76-89, 386-399). */
+int ccp_md_get_stats(ccp_context *ctx, ccp_md_stats *stats);
 
 /* ---------------------------------------------------------------- diagnostics */
 /* These have no counterpart in the reference; they serve benchmarking and profiling. */

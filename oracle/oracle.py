@@ -625,10 +625,35 @@ class MDState:
         self.j = np.array(j, dtype=np.float64)
 
 
-def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld):
+def state_stats(M, flags, pcoord, pmi, totm, s: MDState, box, ld):
+    """Statistics of the state itself, no step (initialization.f90:76-89, 357-399): the
+    energies of a force evaluation there, kinetic energies of v and j, temperature, virial
+    (vir + sum f . xs) and pressure, in the units of nve_run's rows."""
+    nm = len(s.x)
+    ns = pcoord.shape[0]
+    xs, ys, zs, st, e = force_field(M, flags, pcoord, s.x, s.y, s.z, s.q, box, ld)
+    _, _, lvir = _com_force_torque(st, xs, ys, zs, ns, flags[1])
+    tke = 0.5 * totm * float(np.sum(s.v[:, 0] ** 2 + s.v[:, 1] ** 2 + s.v[:, 2] ** 2))
+    rke = 0.5 * float(np.sum(s.j[:, 0] ** 2 / pmi[0] + s.j[:, 1] ** 2 / pmi[1] + s.j[:, 2] ** 2 / pmi[2]))
+    cpe = e["scpe"] + e["rcpe"] + e["kcpe"]
+    pe3 = e["fs2pe"] + e["fs3pe"]
+    pe = e["vdwpe"] + cpe + e["indpe"] + pe3
+    qvir = st.vir.value + lvir
+    return {"vdwpe": e["vdwpe"], "cpe": cpe, "indpe": e["indpe"], "pe3b": pe3, "pe": pe,
+            "tke": tke / 418.4, "rke": rke / 418.4, "te": (tke + rke) / 418.4 + pe,
+            "sys_temp": 2.0 * (tke + rke) / (3.0 * BOLTZ * (2.0 * nm - 1.0)),
+            "vir": qvir / 418.4, "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * box ** 3)}
+
+
+def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, temp0=None,
+            nequil=0):
     """nve_1 (evolve.f90:621-1061) for nsteps steps with the oracle's forces, starting from
     a force evaluation at the initial state (initialization.f90:357-381).  Returns the per-step
-    energies (kcal/mol: vdw, coul, ind, 3b, pe, ke, te; temperature; virial, pressure)."""
+    energies (kcal/mol: vdw, coul, ind, 3b, pe, ke, te; temperature; virial, pressure).
+    During the first nequil steps the velocities and angular momenta are rescaled after the
+    step to temp0 (md.f90:187-193, equilibrationGRU utility.f90:353-368 with
+    rescale_velocities :257-275 and the temperatures of trans_temp / rot_temp :196-227);
+    the step's statistics are those before the rescale."""
     nm = len(s.x)
     ns = pcoord.shape[0]
     three_body = flags[1]
@@ -670,4 +695,9 @@ def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld):
                     "sys_temp": 2.0 * (tke + rke) / (3.0 * BOLTZ * (2.0 * nm - 1.0)),
                     "vir": qvir / 418.4,
                     "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * box ** 3)})
+        if len(out) <= nequil:
+            ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * BOLTZ)
+            rtemp = 2.0 * rke / ((3.0 * nm) * BOLTZ)
+            s.v = s.v * np.sqrt(temp0 / ttemp)
+            s.j = s.j * np.sqrt(temp0 / rtemp)
     return out

@@ -61,7 +61,51 @@ def test_nve_continues_across_calls(md_case):
     assert rel(out[0][1]["v"], out[1][1]["v"]) <= 1e-12
 
 
-def _run_dir(path, nm, nsteps, hist, restart):
+def test_nve_equilibration_matches_oracle(product, oracle):
+    """Equilibration steps (md.f90:187-193): after each of the first nequil steps the COM
+    velocities and angular momenta are rescaled to temp0; the rows report the state before
+    the rescale."""
+    O = oracle
+    m = Model(data_dir("fs2fs3"))
+    b = water_box(m, 37, 10.37, 9, temperature=450.0)
+    inp = O.read_inputs(data_dir("fs2fs3"))
+    pcoord, pmi, totm = O.principal_frame(inp)
+    M = O.make_model(inp, b.nm, b.box)
+    s = O.MDState(b.x, b.y, b.z, b.v, b.q, b.jb)
+    ref = O.nve_run(M, (True, True), pcoord, pmi, totm, s, b.box, DT, 3, b.xs.shape[1],
+                    temp0=298.15, nequil=2)
+    with Context(m, b.nm, b.box) as c:
+        c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
+        c.md_set_equilibration(298.15, 2)
+        stats = c.md_nve(3, DT)
+        st = c.md_get_state()
+    for k, (g, o) in enumerate(zip(stats, ref)):
+        for key in ("tke", "rke", "te", "pe"):
+            assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1.0), (k, key, g[key], o[key])
+    assert rel(st["v"], s.v) <= 1e-9
+    assert rel(st["j"], s.j) <= 1e-9
+    # the rescale took the 450 K start towards 298 K
+    assert stats[1]["sys_temp"] < stats[0]["sys_temp"]
+
+
+def test_md_stats_of_initial_state(product, oracle):
+    O = oracle
+    m = Model(data_dir("fs2fs3"))
+    b = water_box(m, 37, 10.37, 9)
+    inp = O.read_inputs(data_dir("fs2fs3"))
+    pcoord, pmi, totm = O.principal_frame(inp)
+    M = O.make_model(inp, b.nm, b.box)
+    s = O.MDState(b.x, b.y, b.z, b.v, b.q, b.jb)
+    ref = O.state_stats(M, (True, True), pcoord, pmi, totm, s, b.box, b.xs.shape[1])
+    with Context(m, b.nm, b.box) as c:
+        c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
+        g = c.md_stats()
+    for key in ("vdwpe", "cpe", "indpe", "pe3b", "pe", "tke", "rke", "te", "vir", "sys_temp"):
+        assert abs(g[key] - ref[key]) <= 1e-9 * max(abs(ref[key]), 1.0), (key, g[key], ref[key])
+    assert g["pres"] == pytest.approx(ref["pres"], rel=1e-8, abs=1e-9)
+
+
+def _run_dir(path, nm, nsteps, hist, restart, nequil=0):
     import shutil
     path.mkdir()
     src = data_dir("fs2fs3")
@@ -70,6 +114,7 @@ def _run_dir(path, nm, nsteps, hist, restart):
     ctl = (path / "CONTROL").read_text().splitlines()
     ctl[1] = "   nve  1.0  2.0     # ensemble"
     ctl[5] = f"   {nsteps}    # nsteps"
+    ctl[7] = f"   {nequil}    # nequil"
     ctl[9] = f"   {hist}     # history frequency"
     ctl[15] = f"   {'T' if restart else 'F'}     # restart"
     (path / "CONTROL").write_text("\n".join(ctl) + "\n")
@@ -81,21 +126,24 @@ def _run_dir(path, nm, nsteps, hist, restart):
 
 def test_md_driver_files_and_restart(product, tmp_path):
     """The md.f90-style driver: OUTPUT rows, HISTORY frames, REVCON; and 2 + 2 steps through
-    a REVCON restart equal 4 steps in one run."""
+    a REVCON restart equal 4 steps in one run, with the equilibration rescale (nequil = 3)
+    running across the restart."""
     import shutil
     from ccpol23_plus_2025_mbmd_b200.md import read_revcon, run
-    a = _run_dir(tmp_path / "a", 37, 4, 2, False)
+    a = _run_dir(tmp_path / "a", 37, 4, 2, False, nequil=3)
     stats = run(a)
     out = (a / "OUTPUT").read_text().splitlines()
-    assert len(out) == 3 + 4
+    assert len(out) == 3 + 1 + 4  # header, the initial state's row (t = 0), 4 steps
+    assert int(out[3].split()[0]) == 0 and int(out[-1].split()[0]) == 4
     assert abs(float(out[-1].split()[9]) - stats[-1]["te"]) <= 1e-7 * abs(stats[-1]["te"])
     hist = (a / "HISTORY").read_text().splitlines()
-    assert sum(1 for ln in hist if ln.startswith("timestep")) == 2
+    # frames every 2 steps, only after the equilibration (md.f90:220): step 4
+    assert [int(ln.split()[1]) for ln in hist if ln.startswith("timestep")] == [4]
     ra = read_revcon(a / "REVCON", 37)
     assert ra["step"] == 4
-    b = _run_dir(tmp_path / "b", 37, 2, 2, False)
+    b = _run_dir(tmp_path / "b", 37, 2, 2, False, nequil=3)
     run(b)
-    c = _run_dir(tmp_path / "c", 37, 2, 2, True)
+    c = _run_dir(tmp_path / "c", 37, 2, 2, True, nequil=3)
     shutil.copy(b / "REVCON", c / "REVCON")
     run(c)
     rc = read_revcon(c / "REVCON", 37)
