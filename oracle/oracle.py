@@ -645,6 +645,9 @@ def state_stats(M, flags, pcoord, pmi, totm, s: MDState, box, ld):
             "vir": qvir / 418.4, "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * box ** 3)}
 
 
+BETTA = 0.007372  # isothermal compressibility of the Berendsen barostat (evolve.f90:7514)
+
+
 def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, temp0=None,
             nequil=0):
     """nve_1 (evolve.f90:621-1061) for nsteps steps with the oracle's forces, starting from
@@ -654,21 +657,60 @@ def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, temp0=
     step to temp0 (md.f90:187-193, equilibrationGRU utility.f90:353-368 with
     rescale_velocities :257-275 and the temperatures of trans_temp / rot_temp :196-227);
     the step's statistics are those before the rescale."""
+    return md_run(M, flags, pcoord, pmi, totm, s, box, dt, nsteps, ld, "nve", temp0=temp0,
+                  nequil=nequil)
+
+
+def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensemble, temp0=None,
+           nequil=0, taut=None, pres0=None, taup=None, rcut=None):
+    """The reference's rigid-molecule integrators with the oracle's forces:
+    - "nve": nve_1 (evolve.f90:621-1061), with the equilibration rescale of nve_run;
+    - "nvt_b": nvt_b (evolve.f90:1063-1644): nve_1's steps without the periodic wrap, then
+      velocities and angular momenta times chit = sqrt(1 + dt/taut (temp0/T - 1)) of the
+      system temperature T; the statistics are those after the scaling;
+    - "npt_b": npt_b_1 (evolve.f90:7485-8104): before the step the Berendsen barostat
+      chip = 1 + betta dt (P - pres0)/taup from the current kinetic energy and virial scales
+      the volume by chip, the box by chip^(1/3) and the centres inside the drift
+      (x = s x + dt v), with k-max reset for the new box (ewald_setup, rcut); after it the
+      system's COM velocity (utility.f90:293-351) is removed, the nvt_b thermostat applied,
+      and the centres are wrapped into the new box.
+    pres0 is in internal units (katm / PRSUNT, initialization.f90:160).  Rows carry the box
+    and volume of the step.  Mutates s; returns the per-step rows."""
     nm = len(s.x)
     ns = pcoord.shape[0]
     three_body = flags[1]
+    volm = box ** 3.0
     xs, ys, zs, st, e = force_field(M, flags, pcoord, s.x, s.y, s.z, s.q, box, ld)
     out = []
+
+    def kinetic():
+        tke = 0.5 * totm * float(np.sum(s.v[:, 0] ** 2 + s.v[:, 1] ** 2 + s.v[:, 2] ** 2))
+        rke = 0.5 * float(np.sum(s.j[:, 0] ** 2 / pmi[0] + s.j[:, 1] ** 2 / pmi[1] +
+                                 s.j[:, 2] ** 2 / pmi[2]))
+        return tke, rke
+
+    def systemp(tke, rke):
+        return 2.0 * (tke + rke) / (3.0 * BOLTZ * (2.0 * nm - 1.0))
+
     for _ in range(nsteps):
-        F, T, _ = _com_force_torque(st, xs, ys, zs, ns, three_body)
+        F, T, lvir0 = _com_force_torque(st, xs, ys, zs, ns, three_body)
+        scale = 1.0
+        if ensemble == "npt_b":
+            tke0, _ = kinetic()
+            qpres = (2.0 * tke0 - (st.vir.value + lvir0)) / (3.0 * volm)
+            chip = 1.0 + BETTA * dt * (qpres - pres0) / taup
+            scale = chip ** (1.0 / 3.0)
+            volm = volm * chip
+            box = scale * box
+            _, M.kmax1, M.kmax2, M.kmax3 = ewald_setup(rcut, box)
         P = np.zeros((nm, 4))
         for i in range(nm):
             qt, p = _quat_torque_and_momenta(s.q[i], T[i], s.j[i])
             P[i] = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
             s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
-        s.x = s.x + dt * s.v[:, 0]
-        s.y = s.y + dt * s.v[:, 1]
-        s.z = s.z + dt * s.v[:, 2]
+        s.x = scale * s.x + dt * s.v[:, 0]
+        s.y = scale * s.y + dt * s.v[:, 1]
+        s.z = scale * s.z + dt * s.v[:, 2]
         for i in range(nm):
             qn, pn = nosquish(dt, list(s.q[i]), list(P[i]), pmi)
             s.q[i] = qn
@@ -680,22 +722,32 @@ def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, temp0=
             p = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
             s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
             s.j[i] = _momenta_to_j(s.q[i], p)
-        s.x = s.x - box * np.round(s.x / box)
-        s.y = s.y - box * np.round(s.y / box)
-        s.z = s.z - box * np.round(s.z / box)
-        tke = 0.5 * totm * float(np.sum(s.v[:, 0] ** 2 + s.v[:, 1] ** 2 + s.v[:, 2] ** 2))
-        rke = 0.5 * float(np.sum(s.j[:, 0] ** 2 / pmi[0] + s.j[:, 1] ** 2 / pmi[1] + s.j[:, 2] ** 2 / pmi[2]))
+        tke, rke = kinetic()
+        if ensemble == "npt_b":  # utility.f90:293-351: remove the system's COM velocity
+            vcom = np.zeros(3)
+            for i in range(nm):
+                vcom = vcom + totm * s.v[i] / (nm * totm)
+            s.v = s.v - vcom
+            tke, rke = kinetic()
+        if ensemble in ("nvt_b", "npt_b"):
+            chit = np.sqrt(1.0 + dt / taut * (temp0 / systemp(tke, rke) - 1.0))
+            s.v = chit * s.v
+            s.j = chit * s.j
+            tke, rke = kinetic()
+        if ensemble in ("nve", "npt_b"):
+            s.x = s.x - box * np.round(s.x / box)
+            s.y = s.y - box * np.round(s.y / box)
+            s.z = s.z - box * np.round(s.z / box)
         cpe = e["scpe"] + e["rcpe"] + e["kcpe"]
         pe3 = e["fs2pe"] + e["fs3pe"]
         pe = e["vdwpe"] + cpe + e["indpe"] + pe3
-        ke = tke / 418.4 + rke / 418.4
         qvir = st.vir.value + lvir
         out.append({"vdwpe": e["vdwpe"], "cpe": cpe, "indpe": e["indpe"], "pe3b": pe3, "pe": pe,
-                    "tke": tke / 418.4, "rke": rke / 418.4, "te": ke + pe,
-                    "sys_temp": 2.0 * (tke + rke) / (3.0 * BOLTZ * (2.0 * nm - 1.0)),
-                    "vir": qvir / 418.4,
-                    "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * box ** 3)})
-        if len(out) <= nequil:
+                    "tke": tke / 418.4, "rke": rke / 418.4, "te": (tke + rke) / 418.4 + pe,
+                    "sys_temp": systemp(tke, rke), "vir": qvir / 418.4,
+                    "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * volm), "box": box,
+                    "volm": volm})
+        if ensemble == "nve" and len(out) <= nequil:
             ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * BOLTZ)
             rtemp = 2.0 * rke / ((3.0 * nm) * BOLTZ)
             s.v = s.v * np.sqrt(temp0 / ttemp)
