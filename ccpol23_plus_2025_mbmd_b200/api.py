@@ -343,6 +343,19 @@ class Context:
         check(_lib.lib().ccp_md_get_stats(self._h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in _lib.CcpMdStats._fields_}
 
+    def md_set_ensemble(self, ensemble: str, temp0: float = 0.0, taut: float = 0.0,
+                        pres0_katm: float = 0.0, taup: float = 0.0):
+        """Ensemble of md_run: "nve" (nve_1), "nvt_b" (nvt_b) or "npt_b" (npt_b_1), with
+        CONTROL's temp0 (K), taut (ps), pres0 (katm) and taup (ps)."""
+        check(_lib.lib().ccp_md_set_ensemble(self._h, _lib.MD_ENSEMBLES[ensemble], float(temp0),
+                                             float(taut), float(pres0_katm), float(taup)))
+
+    def md_run(self, nsteps: int, dt: float) -> list:
+        """nsteps steps of the ensemble set by md_set_ensemble; per-step statistics."""
+        stats = (_lib.CcpMdStats * max(nsteps, 1))()
+        check(_lib.lib().ccp_md_run(self._h, int(nsteps), float(dt), stats))
+        return [{k: getattr(s, k) for k, _ in _lib.CcpMdStats._fields_} for s in stats[:nsteps]]
+
     def md_nve(self, nsteps: int, dt: float) -> list:
         """nve_1 steps on the device; per-step energies, temperature, virial, pressure."""
         stats = (_lib.CcpMdStats * max(nsteps, 1))()

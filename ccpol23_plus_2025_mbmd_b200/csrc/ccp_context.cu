@@ -109,6 +109,9 @@ struct ccp_context {
          *d_md_j = nullptr, *d_md_red = nullptr, *h_md = nullptr;
   bool md_ready = false;
   double md_box = 0;
+  double md_volm = 0;      // MD box volume (the barostat scales it, evolve.f90:7604-7606)
+  int md_ens = 0;          // ensemble of ccp_md_run (CCP_MD_*)
+  double md_temp0 = 0, md_taut = 0, md_pres0 = 0, md_taup = 0;  // pres0 in internal units
   int md_eq_left = 0;      // MD steps still to be followed by the equilibration rescale
   double md_eq_temp = 0;   // its target temperature (K)
   ccp_energies md_e{};
@@ -1555,7 +1558,7 @@ int md_alloc(ccp_context *c) {
   CK(dalloc(&c->d_md_v, 3 * nm));
   CK(dalloc(&c->d_md_q, 4 * nm));
   CK(dalloc(&c->d_md_j, 3 * nm));
-  CK(dalloc(&c->d_md_red, (size_t)3));
+  CK(dalloc(&c->d_md_red, (size_t)6));
   CK(cudaMallocHost((void **)&c->h_md, sizeof(double) * 13 * nm));
   return CCP_OK;
 }
@@ -1597,6 +1600,7 @@ int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double
   CK(cudaMemcpyAsync(ctx->d_md_q, h + 6 * nm, 4 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(ctx->d_md_j, h + 10 * nm, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
   ctx->md_box = box;
+  ctx->md_volm = pow(box, 3.0);
   EvalOut o;
   r = md_forces(ctx, o);
   ctx->md_ready = r == CCP_OK;
@@ -1644,13 +1648,13 @@ int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, dou
 }  // extern "C"
 
 namespace {
+constexpr double kBetta = 0.007372;  // Berendsen barostat compressibility (evolve.f90:7514)
+
 // md.f90:169-176 and evolve.f90:1020-1052 (initialization.f90:76-89, 386-399 for the initial
-// state): energies of the last evaluation, kinetic energies, temperature, virial and pressure
-// from the sums in h_md = {sum v^2, sum J^2 / I, sum f . xs}
-void md_fill_stats(const ccp_context *ctx, ccp_md_stats &S) {
+// state): energies of the last evaluation, the given kinetic energies (internal units), the
+// temperature, virial (vir + the sum f . xs in h_md[2]) and pressure over md_volm.
+void md_fill_stats(const ccp_context *ctx, double tke, double rke, ccp_md_stats &S) {
   const ccp_energies &e = ctx->md_e;
-  const double box = ctx->md_box;
-  const double tke = 0.5 * ctx->totm * ctx->h_md[0], rke = 0.5 * ctx->h_md[1];
   const double qvir = e.vir + ctx->h_md[2];
   S.vdwpe = e.vdwpe;
   S.cpe = e.scpe + e.rcpe + e.kcpe;
@@ -1662,8 +1666,112 @@ void md_fill_stats(const ccp_context *ctx, ccp_md_stats &S) {
   S.te = S.tke + S.rke + S.pe;
   S.sys_temp = 2.0 * (tke + rke) / (3.0 * kBoltz * (2.0 * ctx->nm - 1.0));
   S.vir = qvir / 418.4;
-  S.pres = kPrsunt * (2.0 * tke - qvir) / (3.0 * box * box * box);
+  S.pres = kPrsunt * (2.0 * tke - qvir) / (3.0 * ctx->md_volm);
   S.ind_iters = e.ind_iters;
+  S.box = ctx->md_box;
+  S.volm = ctx->md_volm;
+}
+
+void md_fill_stats(const ccp_context *ctx, ccp_md_stats &S) {
+  md_fill_stats(ctx, 0.5 * ctx->totm * ctx->h_md[0], 0.5 * ctx->h_md[1], S);
+}
+
+// npt_b_1 before the step (evolve.f90:7568-7607): the pressure of the current state sets
+// the Berendsen barostat chip; volume times chip, box times chip^(1/3), k-max for the new
+// box (ewald_setup).  Returns the centres' scale chip^(1/3) in *scale.
+int md_barostat(ccp_context *ctx, double dt, double *scale) {
+  const size_t nm = ctx->nm, nsi = nm * ctx->ns;
+  double *xs = ctx->d_md_xs;
+  cudaStream_t st = ctx->stream;
+  CK(launch_md_sums(ctx->nm, ctx->ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi,
+                    xs + 2 * nsi, ctx->d_md_v, ctx->d_md_j, ctx->pmi, ctx->d_md_red, st));
+  CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const double tke0 = 0.5 * ctx->totm * ctx->h_md[0];
+  const double qpres = (2.0 * tke0 - (ctx->md_e.vir + ctx->h_md[2])) / (3.0 * ctx->md_volm);
+  const double chip = 1.0 + kBetta * dt * (qpres - ctx->md_pres0) / ctx->md_taup;
+  *scale = pow(chip, 1.0 / 3.0);
+  ctx->md_volm = ctx->md_volm * chip;
+  ctx->md_box = *scale * ctx->md_box;
+  double a;
+  int k1, k2, k3;
+  const int r = ccp_ewald_setup(kEwp, ctx->rcut, ctx->md_box, &a, &k1, &k2, &k3);
+  if (r) return r;
+  ctx->kmax[0] = k1;
+  ctx->kmax[1] = k2;
+  ctx->kmax[2] = k3;
+  return CCP_OK;
+}
+
+// nsteps steps of the ensemble `kind` (CCP_MD_*): nve_1 (evolve.f90:621-1061), nvt_b
+// (:1063-1644) or npt_b_1 (:7485-8104).  They share the kicks, drift and nosquish rotation
+// (stage 1 and 2 kernels); nvt_b does not wrap the centres, npt_b_1 wraps them after its
+// thermostat into the new box.
+int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *stats) {
+  CK(cudaSetDevice(ctx->device));
+  const size_t nm = ctx->nm, nsi = nm * ctx->ns;
+  const int ns = ctx->ns;
+  double *x = ctx->d_md_x, *xs = ctx->d_md_xs, *v = ctx->d_md_v, *q = ctx->d_md_q,
+         *jv = ctx->d_md_j;
+  cudaStream_t st = ctx->stream;
+  const double zero[3] = {0.0, 0.0, 0.0};
+  const double dof_sys = 3.0 * kBoltz * (2.0 * ctx->nm - 1.0);
+  for (int k = 0; k < nsteps; k++) {
+    double scale = 1.0;
+    if (kind == CCP_MD_NPT_B) {
+      const int r = md_barostat(ctx, dt, &scale);
+      if (r) return r;
+    }
+    // first half kick, drift and rotation with the previous evaluation's forces
+    CK(launch_md_stage1(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
+                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, scale, st));
+    EvalOut o;
+    int r = md_forces(ctx, o);
+    if (r) {
+      ctx->md_ready = false;
+      return r;
+    }
+    CK(launch_md_stage2(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
+                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, ctx->md_box,
+                        kind == CCP_MD_NVE ? 1 : 0, ctx->d_md_red, st));
+    CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const double *h = ctx->h_md;
+    double tke = 0.5 * ctx->totm * h[0];
+    const double rke = 0.5 * h[1];
+    if (kind == CCP_MD_NVE) {
+      if (stats) md_fill_stats(ctx, tke, rke, stats[k]);
+      if (ctx->md_eq_left > 0) {
+        // md.f90:187-193: after the step, velocities and angular momenta to temp0
+        // (equilibrationGRU, utility.f90:353-368; trans_temp / rot_temp :196-227)
+        const double ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * kBoltz);
+        const double rtemp = 2.0 * rke / ((3.0 * nm) * kBoltz);
+        CK(launch_md_scale(ctx->nm, v, zero, sqrt(ctx->md_eq_temp / ttemp), jv,
+                           sqrt(ctx->md_eq_temp / rtemp), st));
+        ctx->md_eq_left--;
+      }
+      continue;
+    }
+    double c[3] = {0.0, 0.0, 0.0};
+    if (kind == CCP_MD_NPT_B) {
+      // utility.f90:293-351: the system's COM velocity (every molecule of mass totm), removed
+      // before the thermostat; sum (v - c)^2 = sum v^2 - 2 c . sum v + nm c^2
+      double c2 = 0.0, cs = 0.0;
+      for (int a = 0; a < 3; a++) {
+        c[a] = h[3 + a] / (double)nm;
+        c2 += c[a] * c[a];
+        cs += c[a] * h[3 + a];
+      }
+      tke = 0.5 * ctx->totm * (h[0] - 2.0 * cs + (double)nm * c2);
+    }
+    // evolve.f90:1598-1606 / 8047-8055: Berendsen thermostat on the system temperature
+    const double tsys = 2.0 * (tke + rke) / dof_sys;
+    const double chit = sqrt(1.0 + dt / ctx->md_taut * (ctx->md_temp0 / tsys - 1.0));
+    CK(launch_md_scale(ctx->nm, v, c, chit, jv, chit, st));
+    if (kind == CCP_MD_NPT_B) CK(launch_md_wrap(ctx->nm, x, x + nm, x + 2 * nm, ctx->md_box, st));
+    if (stats) md_fill_stats(ctx, chit * chit * tke, chit * chit * rke, stats[k]);
+  }
+  return CCP_OK;
 }
 }  // namespace
 
@@ -1675,41 +1783,32 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
     set_error("ccp_md_nve: no MD state (call ccp_md_set_state first)");
     return CCP_ERR_BAD_INPUT;
   }
-  CK(cudaSetDevice(ctx->device));
-  const size_t nm = ctx->nm, nsi = nm * ctx->ns;
-  const int ns = ctx->ns;
-  double *x = ctx->d_md_x, *xs = ctx->d_md_xs, *v = ctx->d_md_v, *q = ctx->d_md_q,
-         *jv = ctx->d_md_j;
-  cudaStream_t st = ctx->stream;
-  const double box = ctx->md_box;
-  for (int k = 0; k < nsteps; k++) {
-    // first half kick, drift and rotation with the previous evaluation's forces
-    CK(launch_md_stage1(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
-                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, st));
-    EvalOut o;
-    int r = md_forces(ctx, o);
-    if (r) {
-      ctx->md_ready = false;
-      return r;
-    }
-    CK(launch_md_stage2(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
-                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, box,
-                        ctx->d_md_red, st));
-    CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    if (stats) md_fill_stats(ctx, stats[k]);
-    if (ctx->md_eq_left > 0) {
-      // md.f90:187-193: after the step, velocities and angular momenta to temp0
-      // (equilibrationGRU, utility.f90:353-368; trans_temp / rot_temp :196-227)
-      const double tke = 0.5 * ctx->totm * ctx->h_md[0], rke = 0.5 * ctx->h_md[1];
-      const double ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * kBoltz);
-      const double rtemp = 2.0 * rke / ((3.0 * nm) * kBoltz);
-      CK(launch_md_scale(ctx->nm, v, sqrt(ctx->md_eq_temp / ttemp), jv,
-                         sqrt(ctx->md_eq_temp / rtemp), st));
-      ctx->md_eq_left--;
-    }
+  return md_steps(ctx, CCP_MD_NVE, nsteps, dt, stats);
+}
+
+int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
+                        double pres0_katm, double taup) {
+  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NPT_B ||
+      (ensemble != CCP_MD_NVE && !(temp0 > 0.0 && taut > 0.0)) ||
+      (ensemble == CCP_MD_NPT_B && !(taup > 0.0))) {
+    set_error("ccp_md_set_ensemble: unknown ensemble or non-positive temp0 / taut / taup");
+    return CCP_ERR_BAD_INPUT;
   }
+  ctx->md_ens = ensemble;
+  ctx->md_temp0 = temp0;
+  ctx->md_taut = taut;
+  ctx->md_pres0 = pres0_katm / kPrsunt;  // initialization.f90:160
+  ctx->md_taup = taup;
   return CCP_OK;
+}
+
+int ccp_md_run(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
+  if (!ctx || nsteps < 0 || !(dt > 0.0)) return CCP_ERR_BAD_INPUT;
+  if (!ctx->md_ready) {
+    set_error("ccp_md_run: no MD state (call ccp_md_set_state first)");
+    return CCP_ERR_BAD_INPUT;
+  }
+  return md_steps(ctx, ctx->md_ens, nsteps, dt, stats);
 }
 
 int ccp_md_set_equilibration(ccp_context *ctx, double temp0, int nsteps) {

@@ -130,7 +130,7 @@ __global__ void k_md_stage1(int nm, int ns, const double *__restrict__ f,
                             const double *__restrict__ xs, const double *__restrict__ ys,
                             const double *__restrict__ zs, double *x, double *y, double *z,
                             double *v, double *qv, double *jv, double pmi0, double pmi1,
-                            double pmi2, double totm, double dt) {
+                            double pmi2, double totm, double dt, double scale) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nm) return;
   double F[3], T[3], lvir;
@@ -145,9 +145,15 @@ __global__ void k_md_stage1(int nm, int ns, const double *__restrict__ f,
   v[i] = vx;
   v[nm + i] = vy;
   v[2 * nm + i] = vz;
-  x[i] = x[i] + dt * vx;
-  y[i] = y[i] + dt * vy;
-  z[i] = z[i] + dt * vz;
+  if (scale == 1.0) {
+    x[i] = x[i] + dt * vx;
+    y[i] = y[i] + dt * vy;
+    z[i] = z[i] + dt * vz;
+  } else {  // npt_b_1 (evolve.f90:7612-7616): the barostat scales the centres in the drift
+    x[i] = scale * x[i] + dt * vx;
+    y[i] = scale * y[i] + dt * vy;
+    z[i] = scale * z[i] + dt * vz;
+  }
   const double pmi[3] = {pmi0, pmi1, pmi2};
   nosquish(dt, q, p, pmi);
   double Jn[3];
@@ -176,9 +182,9 @@ __global__ void k_md_stage2(int nm, int ns, const double *__restrict__ f,
                             const double *__restrict__ zs, double *x, double *y, double *z,
                             double *v, const double *__restrict__ qv, double *jv, double pmi0,
                             double pmi1, double pmi2, double totm, double dt, double box,
-                            double *red) {
+                            int wrap, double *red) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double v2 = 0.0, j2 = 0.0, lv = 0.0;
+  double v2 = 0.0, j2 = 0.0, lv = 0.0, sv[3] = {0.0, 0.0, 0.0};
   if (i < nm) {
     double F[3], T[3], lvir;
     force_torque(i, nm, ns, f, fc2, fc3, xs, ys, zs, F, T, lvir);
@@ -195,21 +201,37 @@ __global__ void k_md_stage2(int nm, int ns, const double *__restrict__ f,
     double Jn[3];
     momenta_to_j(q, p, Jn);
     for (int k = 0; k < 3; k++) jv[k * nm + i] = Jn[k];
-    // evolve.f90:1009-1015: periodic wrap of the centres of mass
-    x[i] = minimg(x[i], box);
-    y[i] = minimg(y[i], box);
-    z[i] = minimg(z[i], box);
+    if (wrap) {  // evolve.f90:1009-1015: periodic wrap of the centres of mass
+      x[i] = minimg(x[i], box);
+      y[i] = minimg(y[i], box);
+      z[i] = minimg(z[i], box);
+    }
     v2 = vx * vx + vy * vy + vz * vz;
+    sv[0] = vx;
+    sv[1] = vy;
+    sv[2] = vz;
     j2 = Jn[0] * Jn[0] / pmi0 + Jn[1] * Jn[1] / pmi1 + Jn[2] * Jn[2] / pmi2;
     lv = lvir;
   }
   v2 = warp_sum(v2);
   j2 = warp_sum(j2);
   lv = warp_sum(lv);
+  for (int k = 0; k < 3; k++) sv[k] = warp_sum(sv[k]);
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(&red[0], v2);
     atomicAdd(&red[1], j2);
     atomicAdd(&red[2], lv);
+    for (int k = 0; k < 3; k++) atomicAdd(&red[3 + k], sv[k]);
+  }
+}
+
+// Periodic wrap of the centres into the box (npt_b_1 does it after its thermostat,
+// evolve.f90:8094-8098).
+__global__ void k_md_wrap(int nm, double *x, double *y, double *z, double box) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nm; i += gridDim.x * blockDim.x) {
+    x[i] = minimg(x[i], box);
+    y[i] = minimg(y[i], box);
+    z[i] = minimg(z[i], box);
   }
 }
 
@@ -242,11 +264,14 @@ __global__ void k_md_sums(int nm, int ns, const double *__restrict__ f,
   }
 }
 
-// Velocity rescaling of the equilibration phase (rescale_velocities, utility.f90:257-275):
-// COM velocities by fv, angular momenta by fj.
-__global__ void k_md_scale(int n, double *v, double fv, double *jv, double fj) {
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    v[t] *= fv;
+// Velocity rescaling (rescale_velocities, utility.f90:257-275, and the Berendsen thermostat
+// of nvt_b / npt_b_1): COM velocities v = fv (v - c), angular momenta by fj; c is the
+// system's COM velocity that npt_b_1 removes first (evolve.f90:8029-8055), else 0.
+__global__ void k_md_scale(int nm, double *v, double cx, double cy, double cz, double fv,
+                           double *jv, double fj) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * nm; t += gridDim.x * blockDim.x) {
+    const double c = t < nm ? cx : (t < 2 * nm ? cy : cz);
+    v[t] = fv * (v[t] - c);
     jv[t] *= fj;
   }
 }
@@ -263,9 +288,15 @@ cudaError_t launch_md_sums(int nm, int ns, const double *f, const double *fc2, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_md_scale(int nm, double *v, double fv, double *j, double fj, cudaStream_t st) {
+cudaError_t launch_md_scale(int nm, double *v, const double c[3], double fv, double *j, double fj,
+                            cudaStream_t st) {
   const int n = 3 * nm;
-  k_md_scale<<<(n + 255) / 256, 256, 0, st>>>(n, v, fv, j, fj);
+  k_md_scale<<<(n + 255) / 256, 256, 0, st>>>(nm, v, c[0], c[1], c[2], fv, j, fj);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_md_wrap(int nm, double *x, double *y, double *z, double box, cudaStream_t st) {
+  k_md_wrap<<<(nm + 255) / 256, 256, 0, st>>>(nm, x, y, z, box);
   return cudaGetLastError();
 }
 
@@ -273,9 +304,9 @@ cudaError_t launch_md_stage1(int nm, int ns, const double *f, const double *fc2,
                              const double *fc3, const double *xs, const double *ys,
                              const double *zs, double *x, double *y, double *z, double *v,
                              double *q, double *j, const double pmi[3], double totm, double dt,
-                             cudaStream_t st) {
+                             double scale, cudaStream_t st) {
   k_md_stage1<<<(nm + 127) / 128, 128, 0, st>>>(nm, ns, f, fc2, fc3, xs, ys, zs, x, y, z, v, q, j,
-                                                pmi[0], pmi[1], pmi[2], totm, dt);
+                                                pmi[0], pmi[1], pmi[2], totm, dt, scale);
   return cudaGetLastError();
 }
 
@@ -290,10 +321,10 @@ cudaError_t launch_md_stage2(int nm, int ns, const double *f, const double *fc2,
                              const double *fc3, const double *xs, const double *ys,
                              const double *zs, double *x, double *y, double *z, double *v,
                              const double *q, double *j, const double pmi[3], double totm,
-                             double dt, double box, double *red, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(red, 0, 3 * sizeof(double), st);
+                             double dt, double box, int wrap, double *red, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(red, 0, 6 * sizeof(double), st);
   if (e != cudaSuccess) return e;
   k_md_stage2<<<(nm + 127) / 128, 128, 0, st>>>(nm, ns, f, fc2, fc3, xs, ys, zs, x, y, z, v, q, j,
-                                                pmi[0], pmi[1], pmi[2], totm, dt, box, red);
+                                                pmi[0], pmi[1], pmi[2], totm, dt, box, wrap, red);
   return cudaGetLastError();
 }

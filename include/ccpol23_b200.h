@@ -285,12 +285,29 @@ typedef struct ccp_md_stats {
     double tke, rke, te;                 /* translational, rotational, total energy */
     double sys_temp, vir, pres;
     int ind_iters;
+    double box, volm;                    /* box length (A) and volume (A^3) of the step */
 } ccp_md_stats;
 int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double *y,
                      const double *z, const double *v, const double *q, const double *j);
 int ccp_md_get_state(ccp_context *ctx, double *x, double *y, double *z, double *v, double *q,
                      double *j);
 int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
+/* Ensembles of ccp_md_run, with CONTROL's temp0 (K), taut (ps), pres0 (katm) and taup (ps):
+     CCP_MD_NVE    nve_1, as ccp_md_nve (default);
+     CCP_MD_NVT_B  nvt_b (evolve.f90:1063-1644): after each step, COM velocities and angular
+                   momenta times sqrt(1 + dt/taut (temp0/T - 1)), T the system temperature;
+                   the centres are not wrapped; the statistics follow the scaling;
+     CCP_MD_NPT_B  npt_b_1 (evolve.f90:7485-8104): before each step the Berendsen barostat
+                   chip = 1 + 0.007372 dt (P - pres0)/taup scales the volume by chip, the box
+                   and the centres (in the drift) by chip^(1/3), with k-max reset for the new
+                   box; after it the system's COM velocity is removed, the nvt_b thermostat
+                   applied and the centres wrapped into the new box. */
+#define CCP_MD_NVE 0
+#define CCP_MD_NVT_B 1
+#define CCP_MD_NPT_B 2
+int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
+                        double pres0_katm, double taup);
+int ccp_md_run(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
 /* Induced dipoles of the current MD state (its last evaluation), idm*[i*ld + is], for
    HISTORY output; non-polarisable sites get 0. */
 int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, double *idmz);

@@ -150,3 +150,34 @@ def test_md_driver_files_and_restart(product, tmp_path):
     assert rc["step"] == 4 and abs(rc["t"] - ra["t"]) < 1e-15
     for k in ("x", "y", "z", "v", "q", "j"):
         assert rel(rc[k], ra[k]) <= 1e-10, k
+
+
+@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b"])
+def test_berendsen_ensembles_match_oracle(product, oracle, ensemble):
+    """nvt_b and npt_b_1 (evolve.f90:1063-1644, 7485-8104) on the device against the oracle's
+    restatement: per-step statistics, box and final state after 3 steps."""
+    O = oracle
+    m = Model(data_dir("fs2fs3"))
+    b = water_box(m, 37, 10.37, 9)
+    inp = O.read_inputs(data_dir("fs2fs3"))
+    pcoord, pmi, totm = O.principal_frame(inp)
+    M = O.make_model(inp, b.nm, b.box)
+    s = O.MDState(b.x, b.y, b.z, b.v, b.q, b.jb)
+    temp0, taut, pres0, taup = 298.15, 0.05, 0.001, 0.1
+    ref = O.md_run(M, (True, True), pcoord, pmi, totm, s, b.box, DT, 3, b.xs.shape[1], ensemble,
+                   temp0=temp0, taut=taut, pres0=pres0 / O.PRSUNT, taup=taup,
+                   rcut=m.get_double("rcut"))
+    with Context(m, b.nm, b.box) as c:
+        c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
+        c.md_set_ensemble(ensemble, temp0, taut, pres0, taup)
+        stats = c.md_run(3, DT)
+        st = c.md_get_state()
+    for k, (g, o) in enumerate(zip(stats, ref)):
+        for key in ("pe", "tke", "rke", "te", "sys_temp", "vir", "box", "volm"):
+            assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1.0), (k, key, g[key], o[key])
+        assert g["pres"] == pytest.approx(o["pres"], rel=1e-8, abs=1e-9)
+    if ensemble == "npt_b":
+        assert stats[-1]["box"] != b.box
+    assert rel(np.stack([st["x"], st["y"], st["z"]]), np.stack([s.x, s.y, s.z])) <= 1e-12
+    assert rel(st["v"], s.v) <= 1e-9
+    assert rel(st["j"], s.j) <= 1e-9
