@@ -451,6 +451,10 @@ int ccp_model_get_int(const ccp_model *m, const char *name, int *value) {
   else if (n == "nlin") *value = (int)m->sr.cs.size();
   else if (n == "have_fs3") *value = m->have_fs3;
   else if (n == "ensemble_nve") *value = m->ensemble == "nve";
+  else if (n == "ensemble_kind")  // CCP_MD_* of the ensembles the device integrator runs, else -1
+    *value = m->ensemble == "nve" ? CCP_MD_NVE
+                                  : (m->ensemble == "nvt_b" ? CCP_MD_NVT_B
+                                                            : (m->ensemble == "npt_b" ? CCP_MD_NPT_B : -1));
   else {
     set_error("unknown int parameter " + n);
     return CCP_ERR_BAD_INPUT;

@@ -1,4 +1,5 @@
-"""NVE molecular dynamics driver with the reference's files (md.f90 for the nve ensemble).
+"""Molecular dynamics driver with the reference's files (md.f90 for the nve, nvt_b and npt_b
+ensembles; nve_1, nvt_b and npt_b_1 of evolve.f90 as motion() selects them).
 
     python -m ccpol23_plus_2025_mbmd_b200.md RUN_DIR [--steps N] [--precision fp64|mixed]
 
@@ -11,8 +12,11 @@ when CONTROL's restart flag is T, REVCON.  The run writes, in the reference's fo
 - REVCON: the final state (md.f90:266-276).
 
 The state stays on the device between steps; only the per-step scalars and the HISTORY frames
-come back.  Steps up to CONTROL's nequil rescale the velocities and angular momenta to its
-temperature after the step, as the reference does for nve.  Without a REVCON the start is
+come back.  With nve, steps up to CONTROL's nequil rescale the velocities and angular
+momenta to its temperature after the step, as the reference does.  With npt_b the box
+changes every step; OUTPUT rows carry each step's volume and density, HISTORY frames the
+box of their step and REVCON the final box.  The REVCON thermostat fields (chit, chip) are
+written as 0.  Without a REVCON the start is
 the seeded lattice of generator.water_box at the FIELD's molecule count and 0.997 g/cm^3,
 with Maxwell-Boltzmann velocities at CONTROL's temperature.  The reference also writes induced-dipole sums (fort.501) and averages; this
 driver does not.
@@ -68,10 +72,11 @@ def _e16(v):  # Fortran 1p,e16.8
 
 
 def output_row(step, t, s, nm, box, totm, initial=False):
+    # the step's volume when the statistics carry it (npt_b changes the box), else box^3
     """One OUTPUT row (md.f90:169-176, 213-215): '(1x,i8,1p,15e16.8)'.  The row of the
     initial state (md.f90:119-152) forms HV as -pe/nm + 0.0019872036 T, the rows of the
     steps as (-pe + 0.0019872036 T)/nm; both as the reference writes them."""
-    volm = box ** 3
+    volm = s.get("volm") or box ** 3
     rho = (totm * nm) / (volm * 1e-24 * 6.022e23)
     enth = (s["pe"] + (s["pres"] * volm) * 2.42e-26) / nm
     if initial:
@@ -116,12 +121,15 @@ def _field_names(directory):
 
 
 def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
-    """An NVE run from RUN_DIR's inputs; returns the per-step statistics."""
+    """A run of CONTROL's ensemble (nve, nvt_b or npt_b) from RUN_DIR's inputs; returns the
+    per-step statistics."""
     directory = Path(directory)
     out_dir = Path(out_dir or directory)
     m = Model(directory)
-    if not m.get_int("ensemble_nve"):
-        raise ValueError("CONTROL's ensemble is not nve: this driver integrates NVE only")
+    kind = m.get_int("ensemble_kind")
+    if kind < 0:
+        raise ValueError("CONTROL's ensemble is not one of nve, nvt_b, npt_b")
+    ensemble = ("nve", "nvt_b", "npt_b")[kind]
     nm, ns = m.get_int("nm"), m.ns
     nsteps = m.get_int("nsteps") if nsteps is None else nsteps
     dt = m.get_double("dt")
@@ -144,8 +152,10 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
     stats = []
     with Context(m, nm, box, device=device, precision=precision) as c:
         c.md_set_state(box, state["x"], state["y"], state["z"], state["v"], state["q"], state["j"])
-        # md.f90:187-193: steps up to nequil are followed by the velocity rescaling
-        c.md_set_equilibration(m.get_double("temp0"), min(max(nequil - step0, 0), nsteps))
+        c.md_set_ensemble(ensemble, m.get_double("temp0"), m.get_double("taut"),
+                          m.get_double("pres0"), m.get_double("taup"))
+        if ensemble == "nve":  # md.f90:187-193: steps up to nequil are followed by a rescale
+            c.md_set_equilibration(m.get_double("temp0"), min(max(nequil - step0, 0), nsteps))
         with open(out_dir / "OUTPUT", "w") as fo, open(out_dir / "HISTORY", "w") as fh:
             fo.write("-" * 250 + "\n")
             fo.write("".join(f"{c_:>16s}" for c_ in OUTPUT_COLUMNS) + "\n")
@@ -156,12 +166,13 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
             done = 0
             while done < nsteps:
                 n = min(hist - (step0 + done) % hist or hist, nsteps - done)
-                chunk = c.md_nve(n, dt)
+                chunk = c.md_run(n, dt)
                 for k, s in enumerate(chunk):
                     step = step0 + done + k + 1
                     fo.write(output_row(step, t0 + (done + k + 1) * dt, s, nm, box, totm) + "\n")
                 stats += chunk
                 done += n
+                box = chunk[-1]["box"]
                 if (step0 + done) % hist == 0 and step0 + done > nequil:
                     st = c.md_get_state()
                     q = st["q"]

@@ -105,14 +105,14 @@ def test_md_stats_of_initial_state(product, oracle):
     assert g["pres"] == pytest.approx(ref["pres"], rel=1e-8, abs=1e-9)
 
 
-def _run_dir(path, nm, nsteps, hist, restart, nequil=0):
+def _run_dir(path, nm, nsteps, hist, restart, nequil=0, ensemble="nve  1.0  2.0"):
     import shutil
     path.mkdir()
     src = data_dir("fs2fs3")
     for f in ("FIELD", "CONTROL", "data3b_full", "data3b_full_LR_4p5"):
         shutil.copy(src / f, path / f)
     ctl = (path / "CONTROL").read_text().splitlines()
-    ctl[1] = "   nve  1.0  2.0     # ensemble"
+    ctl[1] = f"   {ensemble}     # ensemble"
     ctl[5] = f"   {nsteps}    # nsteps"
     ctl[7] = f"   {nequil}    # nequil"
     ctl[9] = f"   {hist}     # history frequency"
@@ -181,3 +181,17 @@ def test_berendsen_ensembles_match_oracle(product, oracle, ensemble):
     assert rel(np.stack([st["x"], st["y"], st["z"]]), np.stack([s.x, s.y, s.z])) <= 1e-12
     assert rel(st["v"], s.v) <= 1e-9
     assert rel(st["j"], s.j) <= 1e-9
+
+
+def test_md_driver_npt_b(product, tmp_path):
+    """The driver with the shipped CONTROL's ensemble (npt_b, taut 1 ps, taup 2 ps): the box
+    changes every step, OUTPUT's volume column follows it and REVCON holds the final box."""
+    from ccpol23_plus_2025_mbmd_b200.md import read_revcon, run
+    a = _run_dir(tmp_path / "a", 37, 3, 3, False, ensemble="npt_b  1.0  2.0")
+    stats = run(a)
+    boxes = [s["box"] for s in stats]
+    assert len(set(boxes)) == 3
+    out = (a / "OUTPUT").read_text().splitlines()
+    for row, s in zip(out[4:], stats):
+        assert abs(float(row.split()[12]) - s["volm"]) <= 1e-7 * s["volm"]
+    assert read_revcon(a / "REVCON", 37)["box"] == pytest.approx(boxes[-1], rel=1e-15)
