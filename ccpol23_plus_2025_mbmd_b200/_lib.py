@@ -39,7 +39,7 @@ EXPORTS = [
     "ccp_md_nve", "ccp_md_get_dipoles", "ccp_batch_create", "ccp_batch_destroy",
     "ccp_batch_slots", "ccp_batch_context", "ccp_batch_set_option", "ccp_batch_set_fs3_params",
     "ccp_batch_terms_device", "ccp_md_set_equilibration", "ccp_md_get_stats",
-    "ccp_md_set_ensemble", "ccp_md_run",
+    "ccp_md_set_ensemble", "ccp_md_run", "ccp_md_set_thermostat",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
@@ -47,7 +47,7 @@ TERM_SELF, TERM_RSPACE, TERM_KSPACE, TERM_INDUCTION, TERM_FS2, TERM_FS3 = 1, 2, 
 TERM_VDW = 64
 
 # ensembles of ccp_md_run (CCP_MD_*)
-MD_ENSEMBLES = {"nve": 0, "nvt_b": 1, "npt_b": 2}
+MD_ENSEMBLES = {"nve": 0, "nvt_b": 1, "npt_b": 2, "nvt_h": 3}
 TERM_HOT = 63
 TERM_ALL = 127
 
@@ -62,7 +62,7 @@ class CcpEnergies(C.Structure):
 class CcpMdStats(C.Structure):
     _fields_ = [(k, C.c_double) for k in ("vdwpe", "cpe", "indpe", "pe3b", "pe", "tke", "rke", "te",
                                           "sys_temp", "vir", "pres")] + [("ind_iters", C.c_int)] + \
-        [("box", C.c_double), ("volm", C.c_double)]
+        [(k, C.c_double) for k in ("box", "volm", "chit", "chip", "consv")]
 
 
 class CcpError(RuntimeError):
@@ -120,6 +120,7 @@ def lib():
     L.ccp_md_get_stats.argtypes = [vp, vp]
     L.ccp_md_set_ensemble.argtypes = [vp, i, d, d, d, d]
     L.ccp_md_run.argtypes = [vp, i, d, vp]
+    L.ccp_md_set_thermostat.argtypes = [vp, d, d]
     L.ccp_terms_device.argtypes = [vp, C.c_uint] + [vp] * 6 + [i, d, C.POINTER(CcpEnergies)] + [vp] * 12
     L.ccp_context_get_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]
     L.ccp_context_set_fs3_params.argtypes = [vp, vp, vp, i, vp, vp]

@@ -345,10 +345,14 @@ class Context:
 
     def md_set_ensemble(self, ensemble: str, temp0: float = 0.0, taut: float = 0.0,
                         pres0_katm: float = 0.0, taup: float = 0.0):
-        """Ensemble of md_run: "nve" (nve_1), "nvt_b" (nvt_b) or "npt_b" (npt_b_1), with
-        CONTROL's temp0 (K), taut (ps), pres0 (katm) and taup (ps)."""
+        """Ensemble of md_run: "nve" (nve_1), "nvt_b" (nvt_b), "npt_b" (npt_b_1) or "nvt_h"
+        (nvt_hov_3), with CONTROL's temp0 (K), taut (ps), pres0 (katm) and taup (ps)."""
         check(_lib.lib().ccp_md_set_ensemble(self._h, _lib.MD_ENSEMBLES[ensemble], float(temp0),
                                              float(taut), float(pres0_katm), float(taup)))
+
+    def md_set_thermostat(self, chit: float, chip: float = 0.0):
+        """Thermostat and barostat variables (REVCON's chit, chip)."""
+        check(_lib.lib().ccp_md_set_thermostat(self._h, float(chit), float(chip)))
 
     def md_run(self, nsteps: int, dt: float) -> list:
         """nsteps steps of the ensemble set by md_set_ensemble; per-step statistics."""

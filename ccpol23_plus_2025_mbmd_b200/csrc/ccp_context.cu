@@ -112,6 +112,7 @@ struct ccp_context {
   double md_volm = 0;      // MD box volume (the barostat scales it, evolve.f90:7604-7606)
   int md_ens = 0;          // ensemble of ccp_md_run (CCP_MD_*)
   double md_temp0 = 0, md_taut = 0, md_pres0 = 0, md_taup = 0;  // pres0 in internal units
+  double md_chit = 0, md_chip = 0, md_cint = 0;  // thermostat / barostat variables (REVCON)
   int md_eq_left = 0;      // MD steps still to be followed by the equilibration rescale
   double md_eq_temp = 0;   // its target temperature (K)
   ccp_energies md_e{};
@@ -1670,6 +1671,14 @@ void md_fill_stats(const ccp_context *ctx, double tke, double rke, ccp_md_stats 
   S.ind_iters = e.ind_iters;
   S.box = ctx->md_box;
   S.volm = ctx->md_volm;
+  S.chit = ctx->md_chit;
+  S.chip = ctx->md_chip;
+  // nvt_hov_3's conserved part of the thermostat (evolve.f90:3797): 0.5 qmass chit^2 + ceng cint
+  const double sigma0 = (6.0 * ctx->nm - 3.0) * kBoltz * ctx->md_temp0 / 2.0;
+  S.consv = ctx->md_ens == CCP_MD_NVT_H
+                ? 0.5 * (2.0 * sigma0 * ctx->md_taut * ctx->md_taut) * ctx->md_chit * ctx->md_chit +
+                      2.0 * sigma0 * ctx->md_cint
+                : 0.0;
 }
 
 void md_fill_stats(const ccp_context *ctx, ccp_md_stats &S) {
@@ -1690,6 +1699,7 @@ int md_barostat(ccp_context *ctx, double dt, double *scale) {
   const double tke0 = 0.5 * ctx->totm * ctx->h_md[0];
   const double qpres = (2.0 * tke0 - (ctx->md_e.vir + ctx->h_md[2])) / (3.0 * ctx->md_volm);
   const double chip = 1.0 + kBetta * dt * (qpres - ctx->md_pres0) / ctx->md_taup;
+  ctx->md_chip = chip;
   *scale = pow(chip, 1.0 / 3.0);
   ctx->md_volm = ctx->md_volm * chip;
   ctx->md_box = *scale * ctx->md_box;
@@ -1733,7 +1743,7 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
     }
     CK(launch_md_stage2(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
                         x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, ctx->md_box,
-                        kind == CCP_MD_NVE ? 1 : 0, ctx->d_md_red, st));
+                        (kind == CCP_MD_NVE || kind == CCP_MD_NVT_H) ? 1 : 0, ctx->d_md_red, st));
     CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const double *h = ctx->h_md;
@@ -1752,6 +1762,26 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
       }
       continue;
     }
+    if (kind == CCP_MD_NVT_H) {
+      // nvt_hov_3 (evolve.f90:3590-3600): the Nose-Hoover thermostat of nptqscl_t_dl4
+      // (:8305-8369) with its time step dt/4, pmass = chip = 0
+      const double sigma0 = (6.0 * nm - 3.0) * kBoltz * ctx->md_temp0 / 2.0;
+      const double qmass = 2.0 * sigma0 * ctx->md_taut * ctx->md_taut, ceng = 2.0 * sigma0;
+      const double tq = 0.25 * dt, hq = 0.5 * tq, qq = 0.25 * tq;
+      double chit = ctx->md_chit, cint = ctx->md_cint;
+      cint = cint + qq * chit;
+      chit = chit + hq * (2.0 * (tke + rke) - ceng) / qmass;
+      cint = cint + hq * chit;
+      const double sc = exp(-tq * chit);
+      CK(launch_md_scale(ctx->nm, v, zero, sc, jv, sc, st));
+      const double tk2 = tke * pow(sc, 2.0), rk2 = rke * pow(sc, 2.0);
+      chit = chit + hq * (2.0 * (tk2 + rk2) - ceng) / qmass;
+      cint = cint + qq * chit;
+      ctx->md_chit = chit;
+      ctx->md_cint = cint;
+      if (stats) md_fill_stats(ctx, tk2, rk2, stats[k]);
+      continue;
+    }
     double c[3] = {0.0, 0.0, 0.0};
     if (kind == CCP_MD_NPT_B) {
       // utility.f90:293-351: the system's COM velocity (every molecule of mass totm), removed
@@ -1767,6 +1797,7 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
     // evolve.f90:1598-1606 / 8047-8055: Berendsen thermostat on the system temperature
     const double tsys = 2.0 * (tke + rke) / dof_sys;
     const double chit = sqrt(1.0 + dt / ctx->md_taut * (ctx->md_temp0 / tsys - 1.0));
+    ctx->md_chit = chit;
     CK(launch_md_scale(ctx->nm, v, c, chit, jv, chit, st));
     if (kind == CCP_MD_NPT_B) CK(launch_md_wrap(ctx->nm, x, x + nm, x + 2 * nm, ctx->md_box, st));
     if (stats) md_fill_stats(ctx, chit * chit * tke, chit * chit * rke, stats[k]);
@@ -1788,7 +1819,7 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
 
 int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
                         double pres0_katm, double taup) {
-  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NPT_B ||
+  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NVT_H ||
       (ensemble != CCP_MD_NVE && !(temp0 > 0.0 && taut > 0.0)) ||
       (ensemble == CCP_MD_NPT_B && !(taup > 0.0))) {
     set_error("ccp_md_set_ensemble: unknown ensemble or non-positive temp0 / taut / taup");
@@ -1799,6 +1830,14 @@ int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double tau
   ctx->md_taut = taut;
   ctx->md_pres0 = pres0_katm / kPrsunt;  // initialization.f90:160
   ctx->md_taup = taup;
+  return CCP_OK;
+}
+
+int ccp_md_set_thermostat(ccp_context *ctx, double chit, double chip) {
+  if (!ctx) return CCP_ERR_BAD_INPUT;
+  ctx->md_chit = chit;
+  ctx->md_chip = chip;
+  ctx->md_cint = 0.0;  // initialization.f90:172
   return CCP_OK;
 }
 

@@ -15,8 +15,9 @@ The state stays on the device between steps; only the per-step scalars and the H
 come back.  With nve, steps up to CONTROL's nequil rescale the velocities and angular
 momenta to its temperature after the step, as the reference does.  With npt_b the box
 changes every step; OUTPUT rows carry each step's volume and density, HISTORY frames the
-box of their step and REVCON the final box.  The REVCON thermostat fields (chit, chip) are
-written as 0.  Without a REVCON the start is
+box of their step and REVCON the final box.  REVCON carries the thermostat and barostat
+variables (chit, chip) of the last step, and a restart takes them back (nvt_h continues its
+thermostat from chit).  Without a REVCON the start is
 the seeded lattice of generator.water_box at the FIELD's molecule count and 0.997 g/cm^3,
 with Maxwell-Boltzmann velocities at CONTROL's temperature.  The reference also writes induced-dipole sums (fort.501) and averages; this
 driver does not.
@@ -128,18 +129,18 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
     m = Model(directory)
     kind = m.get_int("ensemble_kind")
     if kind < 0:
-        raise ValueError("CONTROL's ensemble is not one of nve, nvt_b, npt_b")
-    ensemble = ("nve", "nvt_b", "npt_b")[kind]
+        raise ValueError("CONTROL's ensemble is not one of nve, nvt_b, npt_b, nvt_h")
+    ensemble = ("nve", "nvt_b", "npt_b", "nvt_h")[kind]
     nm, ns = m.get_int("nm"), m.ns
     nsteps = m.get_int("nsteps") if nsteps is None else nsteps
     dt = m.get_double("dt")
     hist = max(m.get_int("hist_freq"), 1)
     nequil = m.get_int("nequil")
     totm = m.get_double("totm")
-    step0, t0 = 0, 0.0
+    step0, t0, chit, chip = 0, 0.0, 0.0, 0.0
     if m.get_int("restart"):
         rc = read_revcon(directory / "REVCON", nm)
-        box, step0, t0 = rc["box"], rc["step"], rc["t"]
+        box, step0, t0, chit, chip = rc["box"], rc["step"], rc["t"], rc["chit"], rc["chip"]
         state = rc
         for a in ("x", "y", "z"):  # initialization.f90:72-77: images into the box
             state[a] = state[a] - box * np.round(state[a] / box)
@@ -154,6 +155,7 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
         c.md_set_state(box, state["x"], state["y"], state["z"], state["v"], state["q"], state["j"])
         c.md_set_ensemble(ensemble, m.get_double("temp0"), m.get_double("taut"),
                           m.get_double("pres0"), m.get_double("taup"))
+        c.md_set_thermostat(chit, chip)
         if ensemble == "nve":  # md.f90:187-193: steps up to nequil are followed by a rescale
             c.md_set_equilibration(m.get_double("temp0"), min(max(nequil - step0, 0), nsteps))
         with open(out_dir / "OUTPUT", "w") as fo, open(out_dir / "HISTORY", "w") as fh:
@@ -182,7 +184,9 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
                     fh.write(history_frame(step0 + done, dt, box, names, masses, charges, st,
                                            xs, ys, zs, c.md_dipoles()))
         st = c.md_get_state()
-    write_revcon(out_dir / "REVCON", step0 + nsteps, t0 + nsteps * dt, box, st)
+    if stats:
+        chit, chip = stats[-1]["chit"], stats[-1]["chip"]
+    write_revcon(out_dir / "REVCON", step0 + nsteps, t0 + nsteps * dt, box, st, chit, chip)
     return stats
 
 

@@ -286,6 +286,9 @@ typedef struct ccp_md_stats {
     double sys_temp, vir, pres;
     int ind_iters;
     double box, volm;                    /* box length (A) and volume (A^3) of the step */
+    double chit, chip;                   /* thermostat and barostat variables after the step
+                                            (REVCON's chit, chip) */
+    double consv;                        /* nvt_h: 0.5 qmass chit^2 + ceng cint; else 0 */
 } ccp_md_stats;
 int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double *y,
                      const double *z, const double *v, const double *q, const double *j);
@@ -301,13 +304,20 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
                    chip = 1 + 0.007372 dt (P - pres0)/taup scales the volume by chip, the box
                    and the centres (in the drift) by chip^(1/3), with k-max reset for the new
                    box; after it the system's COM velocity is removed, the nvt_b thermostat
-                   applied and the centres wrapped into the new box. */
+                   applied and the centres wrapped into the new box;
+     CCP_MD_NVT_H  nvt_hov_3 (evolve.f90:3316-3834): nve_1's step, then the Nose-Hoover
+                   thermostat of nptqscl_t_dl4 (:8305-8369) with its step dt/4 on the
+                   thermostat variable chit (ccp_md_set_thermostat; 0 for a fresh run). */
 #define CCP_MD_NVE 0
 #define CCP_MD_NVT_B 1
 #define CCP_MD_NPT_B 2
+#define CCP_MD_NVT_H 3
 int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
                         double pres0_katm, double taup);
 int ccp_md_run(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
+/* Thermostat and barostat variables, as REVCON carries them (initialization.f90:62); the
+   thermostat's integral (cint) restarts at 0 (initialization.f90:172). */
+int ccp_md_set_thermostat(ccp_context *ctx, double chit, double chip);
 /* Induced dipoles of the current MD state (its last evaluation), idm*[i*ld + is], for
    HISTORY output; non-polarisable sites get 0. */
 int ccp_md_get_dipoles(ccp_context *ctx, int ld, double *idmx, double *idmy, double *idmz);

@@ -662,7 +662,7 @@ def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, temp0=
 
 
 def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensemble, temp0=None,
-           nequil=0, taut=None, pres0=None, taup=None, rcut=None):
+           nequil=0, taut=None, pres0=None, taup=None, rcut=None, chit0=0.0):
     """The reference's rigid-molecule integrators with the oracle's forces:
     - "nve": nve_1 (evolve.f90:621-1061), with the equilibration rescale of nve_run;
     - "nvt_b": nvt_b (evolve.f90:1063-1644): nve_1's steps without the periodic wrap, then
@@ -674,14 +674,22 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
       (x = s x + dt v), with k-max reset for the new box (ewald_setup, rcut); after it the
       system's COM velocity (utility.f90:293-351) is removed, the nvt_b thermostat applied,
       and the centres are wrapped into the new box.
+    - "nvt_h": nvt_hov_3 (evolve.f90:3316-3834): nve_1's step, then the Nose-Hoover
+      thermostat of nptqscl_t_dl4 (evolve.f90:8305-8369) with its step dt/4, from the
+      thermostat variable chit (chit0 at the start, 0 for a fresh run, initialization.f90:169);
+      the statistics follow the scaling.
     pres0 is in internal units (katm / PRSUNT, initialization.f90:160).  Rows carry the box
-    and volume of the step.  Mutates s; returns the per-step rows."""
+    and volume of the step and, for nvt_h, chit and the conserved quantity.  Mutates s;
+    returns the per-step rows."""
     nm = len(s.x)
     ns = pcoord.shape[0]
     three_body = flags[1]
     volm = box ** 3.0
     xs, ys, zs, st, e = force_field(M, flags, pcoord, s.x, s.y, s.z, s.q, box, ld)
     out = []
+    chit, cint = chit0, 0.0
+    sigma0 = (6.0 * nm - 3.0) * BOLTZ * (temp0 or 0.0) / 2.0  # sigma_Text, utility.f90:240-255
+    qmass, ceng = 2.0 * sigma0 * (taut or 0.0) ** 2, 2.0 * sigma0
 
     def kinetic():
         tke = 0.5 * totm * float(np.sum(s.v[:, 0] ** 2 + s.v[:, 1] ** 2 + s.v[:, 2] ** 2))
@@ -734,7 +742,20 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
             s.v = chit * s.v
             s.j = chit * s.j
             tke, rke = kinetic()
-        if ensemble in ("nve", "npt_b"):
+        if ensemble == "nvt_h":  # nptqscl_t_dl4 with ttt = dt/4, pmass = chip = 0
+            tq = 0.25 * dt
+            hq, qq = 0.5 * tq, 0.25 * tq
+            cint = cint + qq * chit
+            chit = chit + hq * (2.0 * (tke + rke) - ceng) / qmass
+            cint = cint + hq * chit
+            sc = np.exp(-tq * chit)
+            s.v = sc * s.v
+            s.j = sc * s.j
+            tke, rke = tke * sc ** 2.0, rke * sc ** 2.0
+            chit = chit + hq * (2.0 * (tke + rke) - ceng) / qmass
+            cint = cint + qq * chit
+            tke, rke = kinetic()
+        if ensemble in ("nve", "npt_b", "nvt_h"):
             s.x = s.x - box * np.round(s.x / box)
             s.y = s.y - box * np.round(s.y / box)
             s.z = s.z - box * np.round(s.z / box)
@@ -746,7 +767,8 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
                     "tke": tke / 418.4, "rke": rke / 418.4, "te": (tke + rke) / 418.4 + pe,
                     "sys_temp": systemp(tke, rke), "vir": qvir / 418.4,
                     "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * volm), "box": box,
-                    "volm": volm})
+                    "volm": volm, "chit": chit,
+                    "consv": 0.5 * qmass * chit ** 2.0 + ceng * cint})
         if ensemble == "nve" and len(out) <= nequil:
             ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * BOLTZ)
             rtemp = 2.0 * rke / ((3.0 * nm) * BOLTZ)

@@ -152,10 +152,11 @@ def test_md_driver_files_and_restart(product, tmp_path):
         assert rel(rc[k], ra[k]) <= 1e-10, k
 
 
-@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b"])
-def test_berendsen_ensembles_match_oracle(product, oracle, ensemble):
-    """nvt_b and npt_b_1 (evolve.f90:1063-1644, 7485-8104) on the device against the oracle's
-    restatement: per-step statistics, box and final state after 3 steps."""
+@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b", "nvt_h"])
+def test_thermostat_ensembles_match_oracle(product, oracle, ensemble):
+    """nvt_b, npt_b_1 and nvt_hov_3 (evolve.f90:1063-1644, 7485-8104, 3316-3834) on the
+    device against the oracle's restatement: per-step statistics, box, thermostat variable
+    and final state after 3 steps (nvt_h from a non-zero chit, as after a restart)."""
     O = oracle
     m = Model(data_dir("fs2fs3"))
     b = water_box(m, 37, 10.37, 9)
@@ -166,16 +167,20 @@ def test_berendsen_ensembles_match_oracle(product, oracle, ensemble):
     temp0, taut, pres0, taup = 298.15, 0.05, 0.001, 0.1
     ref = O.md_run(M, (True, True), pcoord, pmi, totm, s, b.box, DT, 3, b.xs.shape[1], ensemble,
                    temp0=temp0, taut=taut, pres0=pres0 / O.PRSUNT, taup=taup,
-                   rcut=m.get_double("rcut"))
+                   rcut=m.get_double("rcut"), chit0=0.3)
     with Context(m, b.nm, b.box) as c:
         c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
         c.md_set_ensemble(ensemble, temp0, taut, pres0, taup)
+        c.md_set_thermostat(0.3, 0.0)
         stats = c.md_run(3, DT)
         st = c.md_get_state()
     for k, (g, o) in enumerate(zip(stats, ref)):
         for key in ("pe", "tke", "rke", "te", "sys_temp", "vir", "box", "volm"):
             assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1.0), (k, key, g[key], o[key])
         assert g["pres"] == pytest.approx(o["pres"], rel=1e-8, abs=1e-9)
+        if ensemble == "nvt_h":
+            assert g["chit"] == pytest.approx(o["chit"], rel=1e-9, abs=1e-12)
+            assert g["consv"] == pytest.approx(o["consv"], rel=1e-9, abs=1e-9)
     if ensemble == "npt_b":
         assert stats[-1]["box"] != b.box
     assert rel(np.stack([st["x"], st["y"], st["z"]]), np.stack([s.x, s.y, s.z])) <= 1e-12
@@ -195,3 +200,24 @@ def test_md_driver_npt_b(product, tmp_path):
     for row, s in zip(out[4:], stats):
         assert abs(float(row.split()[12]) - s["volm"]) <= 1e-7 * s["volm"]
     assert read_revcon(a / "REVCON", 37)["box"] == pytest.approx(boxes[-1], rel=1e-15)
+
+
+def test_md_driver_nvt_h_restart(product, tmp_path):
+    """nvt_h through the driver: 2 + 2 steps through a REVCON restart (which carries the
+    thermostat variable chit) equal 4 steps in one run."""
+    import shutil
+    from ccpol23_plus_2025_mbmd_b200.md import read_revcon, run
+    ens = "nvt_h  0.05  2.0"
+    a = _run_dir(tmp_path / "a", 37, 4, 4, False, ensemble=ens)
+    run(a)
+    ra = read_revcon(a / "REVCON", 37)
+    assert ra["chit"] != 0.0
+    b = _run_dir(tmp_path / "b", 37, 2, 2, False, ensemble=ens)
+    run(b)
+    c = _run_dir(tmp_path / "c", 37, 2, 2, True, ensemble=ens)
+    shutil.copy(b / "REVCON", c / "REVCON")
+    run(c)
+    rc = read_revcon(c / "REVCON", 37)
+    assert rc["chit"] == pytest.approx(ra["chit"], rel=1e-12)
+    for k in ("x", "y", "z", "v", "q", "j"):
+        assert rel(rc[k], ra[k]) <= 1e-10, k
