@@ -1559,7 +1559,7 @@ int md_alloc(ccp_context *c) {
   CK(dalloc(&c->d_md_v, 3 * nm));
   CK(dalloc(&c->d_md_q, 4 * nm));
   CK(dalloc(&c->d_md_j, 3 * nm));
-  CK(dalloc(&c->d_md_red, (size_t)6));
+  CK(dalloc(&c->d_md_red, (size_t)9));
   CK(cudaMallocHost((void **)&c->h_md, sizeof(double) * 13 * nm));
   return CCP_OK;
 }
@@ -1693,7 +1693,8 @@ int md_barostat(ccp_context *ctx, double dt, double *scale) {
   double *xs = ctx->d_md_xs;
   cudaStream_t st = ctx->stream;
   CK(launch_md_sums(ctx->nm, ctx->ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi,
-                    xs + 2 * nsi, ctx->d_md_v, ctx->d_md_j, ctx->pmi, ctx->d_md_red, st));
+                    xs + 2 * nsi, ctx->d_md_v, ctx->d_md_j, ctx->d_md_x, ctx->pmi,
+                    ctx->d_md_red, st));
   CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   const double tke0 = 0.5 * ctx->totm * ctx->h_md[0];
@@ -1711,6 +1712,72 @@ int md_barostat(ccp_context *ctx, double dt, double *scale) {
   ctx->kmax[1] = k2;
   ctx->kmax[2] = k3;
   return CCP_OK;
+}
+
+// Nose-Hoover thermostat and barostat variables of nvt_hov_3 / npt_hov_2 (evolve.f90:
+// 3391-3398, 5642-5650; sigma_Text utility.f90:240-255): masses and the thermostat's energy.
+struct NhConsts {
+  double qmass, ceng, pmass;
+};
+NhConsts nh_consts(const ccp_context *ctx, int kind) {
+  const double dof = 6.0 * ctx->nm - 3.0, dofr = 3.0 * ctx->nm;
+  const double sigma0 = dof * kBoltz * ctx->md_temp0 / 2.0;
+  NhConsts c{2.0 * sigma0 * ctx->md_taut * ctx->md_taut, 2.0 * sigma0, 0.0};
+  if (kind == CCP_MD_NPT_H) {
+    const double tmpt = (2.0 * sigma0) / (kBoltz * dof);
+    c.ceng = 2.0 * sigma0 + kBoltz * tmpt;
+    c.pmass = ((dof - dofr) + 3.0) * kBoltz * tmpt * ctx->md_taup * ctx->md_taup;
+  }
+  return c;
+}
+
+// The kinetic energies and velocity scale factors a thermostat / barostat sequence acts on:
+// the scalings are products, applied to the device state once the sequence is done.
+struct NhState {
+  double tke, rke, fv, fj;
+};
+
+// nptqscl_t_dl4 (evolve.f90:8305-8369) with time step ttt
+void nh_thermo(ccp_context *ctx, const NhConsts &c, double ttt, NhState &s) {
+  const double h = 0.5 * ttt, q = 0.25 * ttt, f1 = c.pmass * pow(ctx->md_chip, 2.0);
+  double chit = ctx->md_chit, cint = ctx->md_cint;
+  cint = cint + q * chit;
+  chit = chit + h * (2.0 * (s.tke + s.rke) + f1 - c.ceng) / c.qmass;
+  cint = cint + h * chit;
+  const double sc = exp(-ttt * chit);
+  s.fv *= sc;
+  s.fj *= sc;
+  s.tke = s.tke * pow(sc, 2.0);
+  s.rke = s.rke * pow(sc, 2.0);
+  chit = chit + h * (2.0 * (s.tke + s.rke) + f1 - c.ceng) / c.qmass;
+  cint = cint + q * chit;
+  ctx->md_chit = chit;
+  ctx->md_cint = cint;
+}
+
+// nptqscl_p_dl4 (evolve.f90:8435-8495) with time step ttt, box boxi and virial qvir
+void nh_baro(ccp_context *ctx, const NhConsts &c, double ttt, double boxi, double qvir,
+             NhState &s) {
+  const double h = 0.5 * ttt, q = 0.25 * ttt, vi = pow(boxi, 3.0), chit = ctx->md_chit;
+  double chip = ctx->md_chip;
+  chip = chip * exp(-q * chit);
+  chip = chip + h * ((2.0 * s.tke - qvir) - 3.0 * ctx->md_pres0 * vi) / c.pmass;
+  chip = chip * exp(-q * chit);
+  const double sc = exp(-ttt * chip);
+  s.fv *= sc;
+  s.tke = s.tke * pow(sc, 2.0);
+  chip = chip * exp(-q * chit);
+  chip = chip + h * ((2.0 * s.tke - qvir) - 3.0 * ctx->md_pres0 * vi) / c.pmass;
+  chip = chip * exp(-q * chit);
+  ctx->md_chip = chip;
+}
+
+// npt_hov_2's thermostat / barostat / thermostat sequence (evolve.f90:5661-5665, 6061-6065)
+void nh_sequence(ccp_context *ctx, const NhConsts &c, double dt, double boxi, double qvir,
+                 NhState &s) {
+  nh_thermo(ctx, c, 0.25 * dt, s);
+  nh_baro(ctx, c, 0.5 * dt, boxi, qvir, s);
+  nh_thermo(ctx, c, 0.25 * dt, s);
 }
 
 // nsteps steps of the ensemble `kind` (CCP_MD_*): nve_1 (evolve.f90:621-1061), nvt_b
@@ -1732,9 +1799,34 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
       const int r = md_barostat(ctx, dt, &scale);
       if (r) return r;
     }
+    const double *centre = nullptr;
+    double cen[3] = {0.0, 0.0, 0.0}, boxi = 0.0, volmi = 0.0;
+    NhConsts nhc{0.0, 0.0, 0.0};
+    if (kind == CCP_MD_NPT_H) {
+      // npt_hov_2 before the step (evolve.f90:5661-5712): thermostat / barostat / thermostat
+      // on the current state, new volume exp(3 dt chip) V, centres scaled by exp(dt chip)
+      // about the system's centre (the mean of the centres: the site offsets of a molecule
+      // sum to zero about it) in the drift
+      nhc = nh_consts(ctx, kind);
+      CK(launch_md_sums(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
+                        v, jv, x, ctx->pmi, ctx->d_md_red, st));
+      CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 9 * sizeof(double), cudaMemcpyDeviceToHost,
+                         st));
+      CK(cudaStreamSynchronize(st));
+      const double *h0 = ctx->h_md;
+      NhState ns0{0.5 * ctx->totm * h0[0], 0.5 * h0[1], 1.0, 1.0};
+      nh_sequence(ctx, nhc, dt, ctx->md_box, ctx->md_e.vir + h0[2], ns0);
+      for (int a = 0; a < 3; a++) cen[a] = h0[6 + a] / (double)nm;
+      CK(launch_md_scale(ctx->nm, v, zero, ns0.fv, jv, ns0.fj, st));
+      volmi = pow(ctx->md_box, 3.0) * exp(3.0 * dt * ctx->md_chip);
+      boxi = pow(volmi, 1.0 / 3.0);
+      scale = exp(dt * ctx->md_chip);
+      centre = cen;
+    }
     // first half kick, drift and rotation with the previous evaluation's forces
     CK(launch_md_stage1(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
-                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, scale, st));
+                        x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, scale, centre,
+                        st));
     EvalOut o;
     int r = md_forces(ctx, o);
     if (r) {
@@ -1759,6 +1851,37 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
         CK(launch_md_scale(ctx->nm, v, zero, sqrt(ctx->md_eq_temp / ttemp), jv,
                            sqrt(ctx->md_eq_temp / rtemp), st));
         ctx->md_eq_left--;
+      }
+      continue;
+    }
+    if (kind == CCP_MD_NPT_H) {
+      // npt_hov_2 after the step (evolve.f90:6061-6103): the sequence again with the new box
+      // and virial, then the new box, COM-velocity removal and the wrap into the new box
+      NhState ns1{tke, rke, 1.0, 1.0};
+      nh_sequence(ctx, nhc, dt, boxi, ctx->md_e.vir + h[2], ns1);
+      ctx->md_box = boxi;
+      ctx->md_volm = volmi;
+      double a_;
+      int k1, k2, k3;
+      r = ccp_ewald_setup(kEwp, ctx->rcut, ctx->md_box, &a_, &k1, &k2, &k3);
+      if (r) return r;
+      ctx->kmax[0] = k1;
+      ctx->kmax[1] = k2;
+      ctx->kmax[2] = k3;
+      double c[3], c2 = 0.0, cs = 0.0;
+      for (int a = 0; a < 3; a++) {
+        c[a] = h[3 + a] / (double)nm;
+        c2 += c[a] * c[a];
+        cs += c[a] * h[3 + a];
+      }
+      const double tk = ns1.fv * ns1.fv * 0.5 * ctx->totm * (h[0] - 2.0 * cs + (double)nm * c2);
+      CK(launch_md_scale(ctx->nm, v, c, ns1.fv, jv, ns1.fj, st));
+      CK(launch_md_wrap(ctx->nm, x, x + nm, x + 2 * nm, ctx->md_box, st));
+      if (stats) {
+        md_fill_stats(ctx, tk, ns1.rke, stats[k]);
+        stats[k].consv = 0.5 * nhc.qmass * pow(ctx->md_chit, 2.0) +
+                         0.5 * nhc.pmass * pow(ctx->md_chip, 2.0) + nhc.ceng * ctx->md_cint +
+                         ctx->md_pres0 * volmi;
       }
       continue;
     }
@@ -1819,9 +1942,9 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
 
 int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
                         double pres0_katm, double taup) {
-  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NVT_H ||
+  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NPT_H ||
       (ensemble != CCP_MD_NVE && !(temp0 > 0.0 && taut > 0.0)) ||
-      (ensemble == CCP_MD_NPT_B && !(taup > 0.0))) {
+      ((ensemble == CCP_MD_NPT_B || ensemble == CCP_MD_NPT_H) && !(taup > 0.0))) {
     set_error("ccp_md_set_ensemble: unknown ensemble or non-positive temp0 / taut / taup");
     return CCP_ERR_BAD_INPUT;
   }
@@ -1871,7 +1994,7 @@ int ccp_md_get_stats(ccp_context *ctx, ccp_md_stats *stats) {
   cudaStream_t st = ctx->stream;
   const double *xs = ctx->d_md_xs;
   CK(launch_md_sums(ctx->nm, ctx->ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
-                    ctx->d_md_v, ctx->d_md_j, ctx->pmi, ctx->d_md_red, st));
+                    ctx->d_md_v, ctx->d_md_j, ctx->d_md_x, ctx->pmi, ctx->d_md_red, st));
   CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   md_fill_stats(ctx, *stats);

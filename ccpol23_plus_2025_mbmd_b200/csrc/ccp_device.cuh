@@ -170,7 +170,7 @@ cudaError_t launch_md_stage1(int nm, int ns, const double *f, const double *fc2,
                              const double *fc3, const double *xs, const double *ys,
                              const double *zs, double *x, double *y, double *z, double *v,
                              double *q, double *j, const double pmi[3], double totm, double dt,
-                             double scale, cudaStream_t st);
+                             double scale, const double centre[3], cudaStream_t st);
 cudaError_t launch_md_sites(int nm, int ns, const double *q, const double *pcoord, double *xs,
                             double *ys, double *zs, cudaStream_t st);
 cudaError_t launch_md_stage2(int nm, int ns, const double *f, const double *fc2,
@@ -179,10 +179,12 @@ cudaError_t launch_md_stage2(int nm, int ns, const double *f, const double *fc2,
                              const double *q, double *j, const double pmi[3], double totm,
                              double dt, double box, int wrap, double *red, cudaStream_t st);
 // launch_md_stage2's red (6 doubles): {sum v^2, sum J^2 / I, sum f . xs, sum v (3)}.
-// Statistics sums of the current state into red = {sum v^2, sum J^2 / I, sum f . xs}.
+// Sums of the current state into red (9 doubles) = {sum v^2, sum J^2 / I, sum f . xs,
+// sum v (3), sum of the centres x (3)}.
 cudaError_t launch_md_sums(int nm, int ns, const double *f, const double *fc2, const double *fc3,
                            const double *xs, const double *ys, const double *zs, const double *v,
-                           const double *j, const double pmi[3], double *red, cudaStream_t st);
+                           const double *j, const double *x, const double pmi[3], double *red,
+                           cudaStream_t st);
 // v = fv (v - c) per axis, j *= fj (3 nm each); x, y, z into [-box/2, box/2).
 cudaError_t launch_md_scale(int nm, double *v, const double c[3], double fv, double *j, double fj,
                             cudaStream_t st);

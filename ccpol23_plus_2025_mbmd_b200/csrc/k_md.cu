@@ -130,7 +130,8 @@ __global__ void k_md_stage1(int nm, int ns, const double *__restrict__ f,
                             const double *__restrict__ xs, const double *__restrict__ ys,
                             const double *__restrict__ zs, double *x, double *y, double *z,
                             double *v, double *qv, double *jv, double pmi0, double pmi1,
-                            double pmi2, double totm, double dt, double scale) {
+                            double pmi2, double totm, double dt, double scale, double cx,
+                            double cy, double cz, int centred) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= nm) return;
   double F[3], T[3], lvir;
@@ -145,7 +146,11 @@ __global__ void k_md_stage1(int nm, int ns, const double *__restrict__ f,
   v[i] = vx;
   v[nm + i] = vy;
   v[2 * nm + i] = vz;
-  if (scale == 1.0) {
+  if (centred) {  // npt_hov_2 (evolve.f90:5708-5712): scaled about the system's centre
+    x[i] = scale * (x[i] - cx) + dt * vx + cx;
+    y[i] = scale * (y[i] - cy) + dt * vy + cy;
+    z[i] = scale * (z[i] - cz) + dt * vz + cz;
+  } else if (scale == 1.0) {
     x[i] = x[i] + dt * vx;
     y[i] = y[i] + dt * vy;
     z[i] = z[i] + dt * vz;
@@ -241,10 +246,10 @@ __global__ void k_md_sums(int nm, int ns, const double *__restrict__ f,
                           const double *__restrict__ fc2, const double *__restrict__ fc3,
                           const double *__restrict__ xs, const double *__restrict__ ys,
                           const double *__restrict__ zs, const double *__restrict__ v,
-                          const double *__restrict__ jv, double pmi0, double pmi1, double pmi2,
-                          double *red) {
+                          const double *__restrict__ jv, const double *__restrict__ x,
+                          double pmi0, double pmi1, double pmi2, double *red) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double v2 = 0.0, j2 = 0.0, lv = 0.0;
+  double v2 = 0.0, j2 = 0.0, lv = 0.0, sv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   if (i < nm) {
     double F[3], T[3], lvir;
     force_torque(i, nm, ns, f, fc2, fc3, xs, ys, zs, F, T, lvir);
@@ -253,14 +258,22 @@ __global__ void k_md_sums(int nm, int ns, const double *__restrict__ f,
     v2 = vx * vx + vy * vy + vz * vz;
     j2 = J0 * J0 / pmi0 + J1 * J1 / pmi1 + J2 * J2 / pmi2;
     lv = lvir;
+    sv[0] = vx;
+    sv[1] = vy;
+    sv[2] = vz;
+    sv[3] = x[i];
+    sv[4] = x[nm + i];
+    sv[5] = x[2 * nm + i];
   }
   v2 = warp_sum(v2);
   j2 = warp_sum(j2);
   lv = warp_sum(lv);
+  for (int k = 0; k < 6; k++) sv[k] = warp_sum(sv[k]);
   if ((threadIdx.x & 31) == 0) {
     atomicAdd(&red[0], v2);
     atomicAdd(&red[1], j2);
     atomicAdd(&red[2], lv);
+    for (int k = 0; k < 6; k++) atomicAdd(&red[3 + k], sv[k]);
   }
 }
 
@@ -280,11 +293,12 @@ __global__ void k_md_scale(int nm, double *v, double cx, double cy, double cz, d
 
 cudaError_t launch_md_sums(int nm, int ns, const double *f, const double *fc2, const double *fc3,
                            const double *xs, const double *ys, const double *zs, const double *v,
-                           const double *j, const double pmi[3], double *red, cudaStream_t st) {
-  cudaError_t e = cudaMemsetAsync(red, 0, 3 * sizeof(double), st);
+                           const double *j, const double *x, const double pmi[3], double *red,
+                           cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(red, 0, 9 * sizeof(double), st);
   if (e != cudaSuccess) return e;
-  k_md_sums<<<(nm + 127) / 128, 128, 0, st>>>(nm, ns, f, fc2, fc3, xs, ys, zs, v, j, pmi[0], pmi[1],
-                                              pmi[2], red);
+  k_md_sums<<<(nm + 127) / 128, 128, 0, st>>>(nm, ns, f, fc2, fc3, xs, ys, zs, v, j, x, pmi[0],
+                                              pmi[1], pmi[2], red);
   return cudaGetLastError();
 }
 
@@ -304,9 +318,10 @@ cudaError_t launch_md_stage1(int nm, int ns, const double *f, const double *fc2,
                              const double *fc3, const double *xs, const double *ys,
                              const double *zs, double *x, double *y, double *z, double *v,
                              double *q, double *j, const double pmi[3], double totm, double dt,
-                             double scale, cudaStream_t st) {
+                             double scale, const double centre[3], cudaStream_t st) {
   k_md_stage1<<<(nm + 127) / 128, 128, 0, st>>>(nm, ns, f, fc2, fc3, xs, ys, zs, x, y, z, v, q, j,
-                                                pmi[0], pmi[1], pmi[2], totm, dt, scale);
+                                                pmi[0], pmi[1], pmi[2], totm, dt, scale,
+      centre ? centre[0] : 0.0, centre ? centre[1] : 0.0, centre ? centre[2] : 0.0, centre ? 1 : 0);
   return cudaGetLastError();
 }
 

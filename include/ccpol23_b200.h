@@ -288,7 +288,8 @@ typedef struct ccp_md_stats {
     double box, volm;                    /* box length (A) and volume (A^3) of the step */
     double chit, chip;                   /* thermostat and barostat variables after the step
                                             (REVCON's chit, chip) */
-    double consv;                        /* nvt_h: 0.5 qmass chit^2 + ceng cint; else 0 */
+    double consv;                        /* nvt_h: 0.5 qmass chit^2 + ceng cint; npt_h adds
+                                            0.5 pmass chip^2 + pres0 V; else 0 */
 } ccp_md_stats;
 int ccp_md_set_state(ccp_context *ctx, double box, const double *x, const double *y,
                      const double *z, const double *v, const double *q, const double *j);
@@ -307,11 +308,18 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
                    applied and the centres wrapped into the new box;
      CCP_MD_NVT_H  nvt_hov_3 (evolve.f90:3316-3834): nve_1's step, then the Nose-Hoover
                    thermostat of nptqscl_t_dl4 (:8305-8369) with its step dt/4 on the
-                   thermostat variable chit (ccp_md_set_thermostat; 0 for a fresh run). */
+                   thermostat variable chit (ccp_md_set_thermostat; 0 for a fresh run);
+     CCP_MD_NPT_H  npt_hov_2 (evolve.f90:5567-6155): before and after each step the
+                   Nose-Hoover thermostat (dt/4), barostat nptqscl_p_dl4 (dt/2, :8435-8495),
+                   thermostat sequence; volume times exp(3 dt chip), centres scaled by
+                   exp(dt chip) about the system's centre in the drift; the step's forces use
+                   the old box, the new box applies after the step, then the COM velocity is
+                   removed and the centres wrapped. */
 #define CCP_MD_NVE 0
 #define CCP_MD_NVT_B 1
 #define CCP_MD_NPT_B 2
 #define CCP_MD_NVT_H 3
+#define CCP_MD_NPT_H 4
 int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
                         double pres0_katm, double taup);
 int ccp_md_run(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);

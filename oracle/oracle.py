@@ -662,7 +662,7 @@ def nve_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, temp0=
 
 
 def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensemble, temp0=None,
-           nequil=0, taut=None, pres0=None, taup=None, rcut=None, chit0=0.0):
+           nequil=0, taut=None, pres0=None, taup=None, rcut=None, chit0=0.0, chip0=0.0):
     """The reference's rigid-molecule integrators with the oracle's forces:
     - "nve": nve_1 (evolve.f90:621-1061), with the equilibration rescale of nve_run;
     - "nvt_b": nvt_b (evolve.f90:1063-1644): nve_1's steps without the periodic wrap, then
@@ -677,7 +677,14 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
     - "nvt_h": nvt_hov_3 (evolve.f90:3316-3834): nve_1's step, then the Nose-Hoover
       thermostat of nptqscl_t_dl4 (evolve.f90:8305-8369) with its step dt/4, from the
       thermostat variable chit (chit0 at the start, 0 for a fresh run, initialization.f90:169);
-      the statistics follow the scaling.
+      the statistics follow the scaling;
+    - "npt_h": npt_hov_2 (evolve.f90:5567-6155): before and after the step the thermostat /
+      barostat / thermostat sequence of nptqscl_t_dl4 (dt/4) and nptqscl_p_dl4 (dt/2,
+      :8435-8495); the volume grows by exp(3 dt chip) and the centres are scaled by
+      exp(dt chip) about the system's centre (taken as the mean of the centres: the site
+      offsets sum to zero about each centre) in the drift; the forces of the step still use
+      the old box and its k-max; the new box takes effect after the step, before the COM
+      velocity is removed and the centres wrapped.
     pres0 is in internal units (katm / PRSUNT, initialization.f90:160).  Rows carry the box
     and volume of the step and, for nvt_h, chit and the conserved quantity.  Mutates s;
     returns the per-step rows."""
@@ -687,9 +694,15 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
     volm = box ** 3.0
     xs, ys, zs, st, e = force_field(M, flags, pcoord, s.x, s.y, s.z, s.q, box, ld)
     out = []
-    chit, cint = chit0, 0.0
-    sigma0 = (6.0 * nm - 3.0) * BOLTZ * (temp0 or 0.0) / 2.0  # sigma_Text, utility.f90:240-255
+    chit, chip, cint = chit0, chip0, 0.0
+    dof, dofr = 6.0 * nm - 3.0, 3.0 * nm
+    sigma0 = dof * BOLTZ * (temp0 or 0.0) / 2.0  # sigma_Text, utility.f90:240-255
     qmass, ceng = 2.0 * sigma0 * (taut or 0.0) ** 2, 2.0 * sigma0
+    pmass = 0.0
+    if ensemble == "npt_h":  # evolve.f90:5644-5650
+        tmpt = (2.0 * sigma0) / (BOLTZ * dof)
+        ceng = 2.0 * sigma0 + BOLTZ * tmpt
+        pmass = ((dof - dofr) + 3.0) * BOLTZ * tmpt * taup ** 2
 
     def kinetic():
         tke = 0.5 * totm * float(np.sum(s.v[:, 0] ** 2 + s.v[:, 1] ** 2 + s.v[:, 2] ** 2))
@@ -700,9 +713,49 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
     def systemp(tke, rke):
         return 2.0 * (tke + rke) / (3.0 * BOLTZ * (2.0 * nm - 1.0))
 
+    def thermo(ttt):  # nptqscl_t_dl4 (evolve.f90:8305-8369)
+        nonlocal chit, cint
+        h, q = 0.5 * ttt, 0.25 * ttt
+        f1 = pmass * chip ** 2.0
+        cint = cint + q * chit
+        tke, rke = kinetic()
+        chit = chit + h * (2.0 * (tke + rke) + f1 - ceng) / qmass
+        cint = cint + h * chit
+        sc = np.exp(-ttt * chit)
+        s.v = sc * s.v
+        s.j = sc * s.j
+        tke, rke = tke * sc ** 2.0, rke * sc ** 2.0
+        chit = chit + h * (2.0 * (tke + rke) + f1 - ceng) / qmass
+        cint = cint + q * chit
+
+    def baro(ttt, boxi, qvir):  # nptqscl_p_dl4 (evolve.f90:8435-8495)
+        nonlocal chip
+        h, q = 0.5 * ttt, 0.25 * ttt
+        vi = boxi ** 3.0
+        chip = chip * np.exp(-q * chit)
+        tke, _ = kinetic()
+        chip = chip + h * ((2.0 * tke - qvir) - 3.0 * pres0 * vi) / pmass
+        chip = chip * np.exp(-q * chit)
+        sc = np.exp(-ttt * chip)
+        s.v = sc * s.v
+        tke = tke * sc ** 2.0
+        chip = chip * np.exp(-q * chit)
+        chip = chip + h * ((2.0 * tke - qvir) - 3.0 * pres0 * vi) / pmass
+        chip = chip * np.exp(-q * chit)
+
     for _ in range(nsteps):
         F, T, lvir0 = _com_force_torque(st, xs, ys, zs, ns, three_body)
         scale = 1.0
+        centre = np.zeros(3)
+        if ensemble == "npt_h":
+            qvir0 = st.vir.value + lvir0
+            thermo(0.25 * dt)
+            baro(0.5 * dt, box, qvir0)
+            thermo(0.25 * dt)
+            volmi = box ** 3.0 * np.exp(3.0 * dt * chip)
+            boxi = volmi ** (1.0 / 3.0)
+            scale = np.exp(dt * chip)
+            centre = np.array([s.x.mean(), s.y.mean(), s.z.mean()])
         if ensemble == "npt_b":
             tke0, _ = kinetic()
             qpres = (2.0 * tke0 - (st.vir.value + lvir0)) / (3.0 * volm)
@@ -716,9 +769,14 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
             qt, p = _quat_torque_and_momenta(s.q[i], T[i], s.j[i])
             P[i] = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
             s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
-        s.x = scale * s.x + dt * s.v[:, 0]
-        s.y = scale * s.y + dt * s.v[:, 1]
-        s.z = scale * s.z + dt * s.v[:, 2]
+        if ensemble == "npt_h":  # evolve.f90:5708-5712
+            s.x = scale * (s.x - centre[0]) + dt * s.v[:, 0] + centre[0]
+            s.y = scale * (s.y - centre[1]) + dt * s.v[:, 1] + centre[1]
+            s.z = scale * (s.z - centre[2]) + dt * s.v[:, 2] + centre[2]
+        else:
+            s.x = scale * s.x + dt * s.v[:, 0]
+            s.y = scale * s.y + dt * s.v[:, 1]
+            s.z = scale * s.z + dt * s.v[:, 2]
         for i in range(nm):
             qn, pn = nosquish(dt, list(s.q[i]), list(P[i]), pmi)
             s.q[i] = qn
@@ -730,8 +788,13 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
             p = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
             s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
             s.j[i] = _momenta_to_j(s.q[i], p)
+        if ensemble == "npt_h":  # evolve.f90:6061-6080
+            thermo(0.25 * dt)
+            baro(0.5 * dt, boxi, st.vir.value + lvir)
+            thermo(0.25 * dt)
+            box, volm = boxi, volmi
         tke, rke = kinetic()
-        if ensemble == "npt_b":  # utility.f90:293-351: remove the system's COM velocity
+        if ensemble in ("npt_b", "npt_h"):  # utility.f90:293-351: remove the system's COM velocity
             vcom = np.zeros(3)
             for i in range(nm):
                 vcom = vcom + totm * s.v[i] / (nm * totm)
@@ -755,7 +818,7 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
             chit = chit + hq * (2.0 * (tke + rke) - ceng) / qmass
             cint = cint + qq * chit
             tke, rke = kinetic()
-        if ensemble in ("nve", "npt_b", "nvt_h"):
+        if ensemble in ("nve", "npt_b", "nvt_h", "npt_h"):
             s.x = s.x - box * np.round(s.x / box)
             s.y = s.y - box * np.round(s.y / box)
             s.z = s.z - box * np.round(s.z / box)
@@ -767,8 +830,9 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
                     "tke": tke / 418.4, "rke": rke / 418.4, "te": (tke + rke) / 418.4 + pe,
                     "sys_temp": systemp(tke, rke), "vir": qvir / 418.4,
                     "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * volm), "box": box,
-                    "volm": volm, "chit": chit,
-                    "consv": 0.5 * qmass * chit ** 2.0 + ceng * cint})
+                    "volm": volm, "chit": chit, "chip": chip,
+                    "consv": 0.5 * qmass * chit ** 2.0 + ceng * cint + (
+                        0.5 * pmass * chip ** 2.0 + pres0 * volm if ensemble == "npt_h" else 0.0)})
         if ensemble == "nve" and len(out) <= nequil:
             ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * BOLTZ)
             rtemp = 2.0 * rke / ((3.0 * nm) * BOLTZ)

@@ -152,11 +152,12 @@ def test_md_driver_files_and_restart(product, tmp_path):
         assert rel(rc[k], ra[k]) <= 1e-10, k
 
 
-@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b", "nvt_h"])
+@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b", "nvt_h", "npt_h"])
 def test_thermostat_ensembles_match_oracle(product, oracle, ensemble):
-    """nvt_b, npt_b_1 and nvt_hov_3 (evolve.f90:1063-1644, 7485-8104, 3316-3834) on the
-    device against the oracle's restatement: per-step statistics, box, thermostat variable
-    and final state after 3 steps (nvt_h from a non-zero chit, as after a restart)."""
+    """nvt_b, npt_b_1, nvt_hov_3 and npt_hov_2 (evolve.f90:1063-1644, 7485-8104, 3316-3834,
+    5567-6155) on the device against the oracle's restatement: per-step statistics, box,
+    thermostat and barostat variables and final state after 3 steps (the Nose-Hoover
+    ensembles from non-zero chit and chip, as after a restart)."""
     O = oracle
     m = Model(data_dir("fs2fs3"))
     b = water_box(m, 37, 10.37, 9)
@@ -167,21 +168,23 @@ def test_thermostat_ensembles_match_oracle(product, oracle, ensemble):
     temp0, taut, pres0, taup = 298.15, 0.05, 0.001, 0.1
     ref = O.md_run(M, (True, True), pcoord, pmi, totm, s, b.box, DT, 3, b.xs.shape[1], ensemble,
                    temp0=temp0, taut=taut, pres0=pres0 / O.PRSUNT, taup=taup,
-                   rcut=m.get_double("rcut"), chit0=0.3)
+                   rcut=m.get_double("rcut"), chit0=0.3, chip0=0.02)
     with Context(m, b.nm, b.box) as c:
         c.md_set_state(b.box, b.x, b.y, b.z, b.v, b.q, b.jb)
         c.md_set_ensemble(ensemble, temp0, taut, pres0, taup)
-        c.md_set_thermostat(0.3, 0.0)
+        c.md_set_thermostat(0.3, 0.02)
         stats = c.md_run(3, DT)
         st = c.md_get_state()
     for k, (g, o) in enumerate(zip(stats, ref)):
         for key in ("pe", "tke", "rke", "te", "sys_temp", "vir", "box", "volm"):
             assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1.0), (k, key, g[key], o[key])
         assert g["pres"] == pytest.approx(o["pres"], rel=1e-8, abs=1e-9)
-        if ensemble == "nvt_h":
+        if ensemble in ("nvt_h", "npt_h"):
             assert g["chit"] == pytest.approx(o["chit"], rel=1e-9, abs=1e-12)
             assert g["consv"] == pytest.approx(o["consv"], rel=1e-9, abs=1e-9)
-    if ensemble == "npt_b":
+        if ensemble == "npt_h":
+            assert g["chip"] == pytest.approx(o["chip"], rel=1e-9, abs=1e-12)
+    if ensemble in ("npt_b", "npt_h"):
         assert stats[-1]["box"] != b.box
     assert rel(np.stack([st["x"], st["y"], st["z"]]), np.stack([s.x, s.y, s.z])) <= 1e-12
     assert rel(st["v"], s.v) <= 1e-9
