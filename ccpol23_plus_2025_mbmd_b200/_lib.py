@@ -47,7 +47,8 @@ TERM_SELF, TERM_RSPACE, TERM_KSPACE, TERM_INDUCTION, TERM_FS2, TERM_FS3 = 1, 2, 
 TERM_VDW = 64
 
 # ensembles of ccp_md_run (CCP_MD_*)
-MD_ENSEMBLES = {"nve": 0, "nvt_b": 1, "npt_b": 2, "nvt_h": 3, "npt_h": 4}
+MD_ENSEMBLES = {"nve": 0, "nvt_b": 1, "npt_b": 2, "nvt_h": 3, "npt_h": 4,
+                "npt_mtk": 5}
 TERM_HOT = 63
 TERM_ALL = 127
 

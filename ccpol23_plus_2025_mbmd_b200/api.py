@@ -346,7 +346,7 @@ class Context:
     def md_set_ensemble(self, ensemble: str, temp0: float = 0.0, taut: float = 0.0,
                         pres0_katm: float = 0.0, taup: float = 0.0):
         """Ensemble of md_run: "nve" (nve_1), "nvt_b" (nvt_b), "npt_b" (npt_b_1), "nvt_h"
-        (nvt_hov_3) or "npt_h" (npt_hov_2), with CONTROL's temp0 (K), taut (ps), pres0 (katm) and taup (ps)."""
+        (nvt_hov_3), "npt_h" (npt_hov_2) or "npt_mtk" (npt_mtk), with CONTROL's temp0 (K), taut (ps), pres0 (katm) and taup (ps)."""
         check(_lib.lib().ccp_md_set_ensemble(self._h, _lib.MD_ENSEMBLES[ensemble], float(temp0),
                                              float(taut), float(pres0_katm), float(taup)))
 

@@ -1717,13 +1717,14 @@ int md_barostat(ccp_context *ctx, double dt, double *scale) {
 // Nose-Hoover thermostat and barostat variables of nvt_hov_3 / npt_hov_2 (evolve.f90:
 // 3391-3398, 5642-5650; sigma_Text utility.f90:240-255): masses and the thermostat's energy.
 struct NhConsts {
-  double qmass, ceng, pmass;
+  double qmass, ceng, pmass, fmtk;  // fmtk: npt_mtk's 3/(dof - dofr) (evolve.f90:8510), else 0
 };
 NhConsts nh_consts(const ccp_context *ctx, int kind) {
   const double dof = 6.0 * ctx->nm - 3.0, dofr = 3.0 * ctx->nm;
   const double sigma0 = dof * kBoltz * ctx->md_temp0 / 2.0;
-  NhConsts c{2.0 * sigma0 * ctx->md_taut * ctx->md_taut, 2.0 * sigma0, 0.0};
-  if (kind == CCP_MD_NPT_H) {
+  NhConsts c{2.0 * sigma0 * ctx->md_taut * ctx->md_taut, 2.0 * sigma0, 0.0, 0.0};
+  if (kind == CCP_MD_NPT_MTK) c.fmtk = 3.0 / (dof - dofr);
+  if (kind == CCP_MD_NPT_H || kind == CCP_MD_NPT_MTK) {
     const double tmpt = (2.0 * sigma0) / (kBoltz * dof);
     c.ceng = 2.0 * sigma0 + kBoltz * tmpt;
     c.pmass = ((dof - dofr) + 3.0) * kBoltz * tmpt * ctx->md_taup * ctx->md_taup;
@@ -1755,19 +1756,20 @@ void nh_thermo(ccp_context *ctx, const NhConsts &c, double ttt, NhState &s) {
   ctx->md_cint = cint;
 }
 
-// nptqscl_p_dl4 (evolve.f90:8435-8495) with time step ttt, box boxi and virial qvir
+// nptqscl_p_dl4 (evolve.f90:8435-8495), or nptqscl_p_dl4_mtk (:8497-8558) when c.fmtk is
+// set, with time step ttt, box boxi and virial qvir
 void nh_baro(ccp_context *ctx, const NhConsts &c, double ttt, double boxi, double qvir,
              NhState &s) {
   const double h = 0.5 * ttt, q = 0.25 * ttt, vi = pow(boxi, 3.0), chit = ctx->md_chit;
   double chip = ctx->md_chip;
   chip = chip * exp(-q * chit);
-  chip = chip + h * ((2.0 * s.tke - qvir) - 3.0 * ctx->md_pres0 * vi) / c.pmass;
+  chip = chip + h * ((2.0 * (1.0 + c.fmtk) * s.tke - qvir) - 3.0 * ctx->md_pres0 * vi) / c.pmass;
   chip = chip * exp(-q * chit);
-  const double sc = exp(-ttt * chip);
+  const double sc = exp(-ttt * (1.0 + c.fmtk) * chip);
   s.fv *= sc;
   s.tke = s.tke * pow(sc, 2.0);
   chip = chip * exp(-q * chit);
-  chip = chip + h * ((2.0 * s.tke - qvir) - 3.0 * ctx->md_pres0 * vi) / c.pmass;
+  chip = chip + h * ((2.0 * (1.0 + c.fmtk) * s.tke - qvir) - 3.0 * ctx->md_pres0 * vi) / c.pmass;
   chip = chip * exp(-q * chit);
   ctx->md_chip = chip;
 }
@@ -1802,8 +1804,9 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
     const double *centre = nullptr;
     double cen[3] = {0.0, 0.0, 0.0}, boxi = 0.0, volmi = 0.0;
     NhConsts nhc{0.0, 0.0, 0.0};
-    if (kind == CCP_MD_NPT_H) {
-      // npt_hov_2 before the step (evolve.f90:5661-5712): thermostat / barostat / thermostat
+    const bool nh_baro = kind == CCP_MD_NPT_H || kind == CCP_MD_NPT_MTK;
+    if (nh_baro) {
+      // npt_hov_2 / npt_mtk before the step (evolve.f90:5661-5712): thermostat / barostat / thermostat
       // on the current state, new volume exp(3 dt chip) V, centres scaled by exp(dt chip)
       // about the system's centre (the mean of the centres: the site offsets of a molecule
       // sum to zero about it) in the drift
@@ -1821,7 +1824,7 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
       volmi = pow(ctx->md_box, 3.0) * exp(3.0 * dt * ctx->md_chip);
       boxi = pow(volmi, 1.0 / 3.0);
       scale = exp(dt * ctx->md_chip);
-      centre = cen;
+      if (kind == CCP_MD_NPT_H) centre = cen;  // npt_mtk scales about the origin
     }
     // first half kick, drift and rotation with the previous evaluation's forces
     CK(launch_md_stage1(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
@@ -1854,8 +1857,8 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
       }
       continue;
     }
-    if (kind == CCP_MD_NPT_H) {
-      // npt_hov_2 after the step (evolve.f90:6061-6103): the sequence again with the new box
+    if (nh_baro) {
+      // npt_hov_2 / npt_mtk after the step (evolve.f90:6061-6103): the sequence again with the new box
       // and virial, then the new box, COM-velocity removal and the wrap into the new box
       NhState ns1{tke, rke, 1.0, 1.0};
       nh_sequence(ctx, nhc, dt, boxi, ctx->md_e.vir + h[2], ns1);
@@ -1942,9 +1945,9 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats) {
 
 int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
                         double pres0_katm, double taup) {
-  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NPT_H ||
+  if (!ctx || ensemble < CCP_MD_NVE || ensemble > CCP_MD_NPT_MTK ||
       (ensemble != CCP_MD_NVE && !(temp0 > 0.0 && taut > 0.0)) ||
-      ((ensemble == CCP_MD_NPT_B || ensemble == CCP_MD_NPT_H) && !(taup > 0.0))) {
+      (ensemble >= CCP_MD_NPT_B && ensemble != CCP_MD_NVT_H && !(taup > 0.0))) {
     set_error("ccp_md_set_ensemble: unknown ensemble or non-positive temp0 / taut / taup");
     return CCP_ERR_BAD_INPUT;
   }

@@ -456,7 +456,8 @@ int ccp_model_get_int(const ccp_model *m, const char *name, int *value) {
                                   : (m->ensemble == "nvt_b" ? CCP_MD_NVT_B
                                                             : (m->ensemble == "npt_b" ? CCP_MD_NPT_B
                                                                : (m->ensemble == "nvt_h" ? CCP_MD_NVT_H
-                                                                  : (m->ensemble == "npt_h" ? CCP_MD_NPT_H : -1))));
+                                                                  : (m->ensemble == "npt_h" ? CCP_MD_NPT_H
+                                                                     : (m->ensemble == "npt_mtk" ? CCP_MD_NPT_MTK : -1)))));
   else {
     set_error("unknown int parameter " + n);
     return CCP_ERR_BAD_INPUT;

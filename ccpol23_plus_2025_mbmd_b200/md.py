@@ -129,8 +129,9 @@ def run(directory, nsteps=None, precision="fp64", device=0, out_dir=None):
     m = Model(directory)
     kind = m.get_int("ensemble_kind")
     if kind < 0:
-        raise ValueError("CONTROL's ensemble is not one of nve, nvt_b, npt_b, nvt_h, npt_h")
-    ensemble = ("nve", "nvt_b", "npt_b", "nvt_h", "npt_h")[kind]
+        raise ValueError("CONTROL's ensemble is not one of nve, nvt_b, npt_b, nvt_h, npt_h, "
+                         "npt_mtk")
+    ensemble = ("nve", "nvt_b", "npt_b", "nvt_h", "npt_h", "npt_mtk")[kind]
     nm, ns = m.get_int("nm"), m.ns
     nsteps = m.get_int("nsteps") if nsteps is None else nsteps
     dt = m.get_double("dt")

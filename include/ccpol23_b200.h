@@ -314,12 +314,15 @@ int ccp_md_nve(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);
                    thermostat sequence; volume times exp(3 dt chip), centres scaled by
                    exp(dt chip) about the system's centre in the drift; the step's forces use
                    the old box, the new box applies after the step, then the COM velocity is
-                   removed and the centres wrapped. */
+                   removed and the centres wrapped;
+     CCP_MD_NPT_MTK npt_mtk (evolve.f90:6158-6745): npt_h with the MTK barostat
+                   nptqscl_p_dl4_mtk (:8497-8558) and the centres scaled about the origin. */
 #define CCP_MD_NVE 0
 #define CCP_MD_NVT_B 1
 #define CCP_MD_NPT_B 2
 #define CCP_MD_NVT_H 3
 #define CCP_MD_NPT_H 4
+#define CCP_MD_NPT_MTK 5
 int ccp_md_set_ensemble(ccp_context *ctx, int ensemble, double temp0, double taut,
                         double pres0_katm, double taup);
 int ccp_md_run(ccp_context *ctx, int nsteps, double dt, ccp_md_stats *stats);

@@ -684,7 +684,10 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
       exp(dt chip) about the system's centre (taken as the mean of the centres: the site
       offsets sum to zero about each centre) in the drift; the forces of the step still use
       the old box and its k-max; the new box takes effect after the step, before the COM
-      velocity is removed and the centres wrapped.
+      velocity is removed and the centres wrapped;
+    - "npt_mtk": npt_mtk (evolve.f90:6158-6745): npt_h with the MTK barostat
+      nptqscl_p_dl4_mtk (:8497-8558, kinetic term and velocity scaling times 1 + 3/(dof-dofr))
+      and the centres scaled about the origin.
     pres0 is in internal units (katm / PRSUNT, initialization.f90:160).  Rows carry the box
     and volume of the step and, for nvt_h, chit and the conserved quantity.  Mutates s;
     returns the per-step rows."""
@@ -699,7 +702,9 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
     sigma0 = dof * BOLTZ * (temp0 or 0.0) / 2.0  # sigma_Text, utility.f90:240-255
     qmass, ceng = 2.0 * sigma0 * (taut or 0.0) ** 2, 2.0 * sigma0
     pmass = 0.0
-    if ensemble == "npt_h":  # evolve.f90:5644-5650
+    nh_baro = ensemble in ("npt_h", "npt_mtk")
+    fmtk = 3.0 / (dof - dofr) if ensemble == "npt_mtk" else 0.0  # evolve.f90:8510
+    if nh_baro:  # evolve.f90:5644-5650
         tmpt = (2.0 * sigma0) / (BOLTZ * dof)
         ceng = 2.0 * sigma0 + BOLTZ * tmpt
         pmass = ((dof - dofr) + 3.0) * BOLTZ * tmpt * taup ** 2
@@ -734,20 +739,20 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
         vi = boxi ** 3.0
         chip = chip * np.exp(-q * chit)
         tke, _ = kinetic()
-        chip = chip + h * ((2.0 * tke - qvir) - 3.0 * pres0 * vi) / pmass
+        chip = chip + h * ((2.0 * (1.0 + fmtk) * tke - qvir) - 3.0 * pres0 * vi) / pmass
         chip = chip * np.exp(-q * chit)
-        sc = np.exp(-ttt * chip)
+        sc = np.exp(-ttt * (1.0 + fmtk) * chip)
         s.v = sc * s.v
         tke = tke * sc ** 2.0
         chip = chip * np.exp(-q * chit)
-        chip = chip + h * ((2.0 * tke - qvir) - 3.0 * pres0 * vi) / pmass
+        chip = chip + h * ((2.0 * (1.0 + fmtk) * tke - qvir) - 3.0 * pres0 * vi) / pmass
         chip = chip * np.exp(-q * chit)
 
     for _ in range(nsteps):
         F, T, lvir0 = _com_force_torque(st, xs, ys, zs, ns, three_body)
         scale = 1.0
         centre = np.zeros(3)
-        if ensemble == "npt_h":
+        if nh_baro:
             qvir0 = st.vir.value + lvir0
             thermo(0.25 * dt)
             baro(0.5 * dt, box, qvir0)
@@ -788,13 +793,13 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
             p = [p[k] + qt[k] * 0.5 * dt for k in range(4)]
             s.v[i] = s.v[i] + 0.5 * F[i] * dt / totm
             s.j[i] = _momenta_to_j(s.q[i], p)
-        if ensemble == "npt_h":  # evolve.f90:6061-6080
+        if nh_baro:  # evolve.f90:6061-6080
             thermo(0.25 * dt)
             baro(0.5 * dt, boxi, st.vir.value + lvir)
             thermo(0.25 * dt)
             box, volm = boxi, volmi
         tke, rke = kinetic()
-        if ensemble in ("npt_b", "npt_h"):  # utility.f90:293-351: remove the system's COM velocity
+        if ensemble in ("npt_b", "npt_h", "npt_mtk"):  # utility.f90:293-351: remove the COM velocity
             vcom = np.zeros(3)
             for i in range(nm):
                 vcom = vcom + totm * s.v[i] / (nm * totm)
@@ -818,7 +823,7 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
             chit = chit + hq * (2.0 * (tke + rke) - ceng) / qmass
             cint = cint + qq * chit
             tke, rke = kinetic()
-        if ensemble in ("nve", "npt_b", "nvt_h", "npt_h"):
+        if ensemble in ("nve", "npt_b", "nvt_h", "npt_h", "npt_mtk"):
             s.x = s.x - box * np.round(s.x / box)
             s.y = s.y - box * np.round(s.y / box)
             s.z = s.z - box * np.round(s.z / box)
@@ -832,7 +837,7 @@ def md_run(M, flags, pcoord, pmi, totm, s: MDState, box, dt, nsteps, ld, ensembl
                     "pres": PRSUNT * (2.0 * tke - qvir) / (3.0 * volm), "box": box,
                     "volm": volm, "chit": chit, "chip": chip,
                     "consv": 0.5 * qmass * chit ** 2.0 + ceng * cint + (
-                        0.5 * pmass * chip ** 2.0 + pres0 * volm if ensemble == "npt_h" else 0.0)})
+                        0.5 * pmass * chip ** 2.0 + pres0 * volm if nh_baro else 0.0)})
         if ensemble == "nve" and len(out) <= nequil:
             ttemp = 2.0 * tke / ((3.0 * nm - 3.0) * BOLTZ)
             rtemp = 2.0 * rke / ((3.0 * nm) * BOLTZ)

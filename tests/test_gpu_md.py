@@ -152,7 +152,7 @@ def test_md_driver_files_and_restart(product, tmp_path):
         assert rel(rc[k], ra[k]) <= 1e-10, k
 
 
-@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b", "nvt_h", "npt_h"])
+@pytest.mark.parametrize("ensemble", ["nvt_b", "npt_b", "nvt_h", "npt_h", "npt_mtk"])
 def test_thermostat_ensembles_match_oracle(product, oracle, ensemble):
     """nvt_b, npt_b_1, nvt_hov_3 and npt_hov_2 (evolve.f90:1063-1644, 7485-8104, 3316-3834,
     5567-6155) on the device against the oracle's restatement: per-step statistics, box,
@@ -179,12 +179,12 @@ def test_thermostat_ensembles_match_oracle(product, oracle, ensemble):
         for key in ("pe", "tke", "rke", "te", "sys_temp", "vir", "box", "volm"):
             assert abs(g[key] - o[key]) <= 1e-9 * max(abs(o[key]), 1.0), (k, key, g[key], o[key])
         assert g["pres"] == pytest.approx(o["pres"], rel=1e-8, abs=1e-9)
-        if ensemble in ("nvt_h", "npt_h"):
+        if ensemble in ("nvt_h", "npt_h", "npt_mtk"):
             assert g["chit"] == pytest.approx(o["chit"], rel=1e-9, abs=1e-12)
             assert g["consv"] == pytest.approx(o["consv"], rel=1e-9, abs=1e-9)
-        if ensemble == "npt_h":
+        if ensemble in ("npt_h", "npt_mtk"):
             assert g["chip"] == pytest.approx(o["chip"], rel=1e-9, abs=1e-12)
-    if ensemble in ("npt_b", "npt_h"):
+    if ensemble in ("npt_b", "npt_h", "npt_mtk"):
         assert stats[-1]["box"] != b.box
     assert rel(np.stack([st["x"], st["y"], st["z"]]), np.stack([s.x, s.y, s.z])) <= 1e-12
     assert rel(st["v"], s.v) <= 1e-9
