@@ -633,8 +633,11 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     pend(2, sm);
     if (mask & T_INDUCTION) {
       pbeg(3, sm);
-      LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, sm));
+      // the static field's structure factors (charges, mode 1) are the Ewald sums' (mode 0):
+      // when those ran, d_sk still holds them
+      if (!(mask & T_KSPACE))
+        LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                              c->kmax[2], c->d_mu, c->d_sk, sm));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
                               c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, sm));
       if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, sm));
