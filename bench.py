@@ -516,7 +516,11 @@ def main():
                              "same kernel with the three-body terms not overlapped",
                      "isolated": {"duration_ms": iso_s * 1e3, "achieved": iso,
                                   "frac": iso / peak},
-                     "traffic": None},
+                     # DRAM bytes (read + write) of one FP64 launch from the ncu capture in
+                     # profiles/k_fs3_double_512_fs2fs3.md: the triple records only, the
+                     # tables and sites stay in L2 / shared memory
+                     "traffic": 5.2e6 if head == "fp64" else None,
+                     "traffic_unit": "bytes per launch"},
         "gpu_launches": int(results[head]["launches"]),
         "clocks": clocks,
         "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
