@@ -409,7 +409,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from ccpol23_plus_2025_mbmd_b200 import Context
-    from ccpol23_plus_2025_mbmd_b200.api import fma_peak_tflops
+    from ccpol23_plus_2025_mbmd_b200.api import fma_peak_tflops, mufu_peak_tops
 
     model, box, cfg = build_inputs(rank)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
@@ -432,6 +432,7 @@ def main():
     clocks = clk.summary()
     peak64 = fma_peak_tflops(local, "fp64")
     peak32 = fma_peak_tflops(local, "mixed")
+    peak_mufu = mufu_peak_tops(local)
 
     def agg(v):
         if world == 1:
@@ -523,7 +524,7 @@ def main():
                      "traffic_unit": "bytes per launch"},
         "gpu_launches": int(results[head]["launches"]),
         "clocks": clocks,
-        "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32},
+        "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32, "mufu_exp_tops": peak_mufu},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         dt, cores, eo, st = cpu_baseline(box, cfg)

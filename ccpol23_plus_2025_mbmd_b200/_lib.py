@@ -39,7 +39,7 @@ EXPORTS = [
     "ccp_md_nve", "ccp_md_get_dipoles", "ccp_batch_create", "ccp_batch_destroy",
     "ccp_batch_slots", "ccp_batch_context", "ccp_batch_set_option", "ccp_batch_set_fs3_params",
     "ccp_batch_terms_device", "ccp_md_set_equilibration", "ccp_md_get_stats",
-    "ccp_md_set_ensemble", "ccp_md_run", "ccp_md_set_thermostat",
+    "ccp_md_set_ensemble", "ccp_md_run", "ccp_md_set_thermostat", "ccp_device_mufu_peak",
 ]
 
 # term bits of ccp_terms_device (CCP_TERM_*)
@@ -105,6 +105,7 @@ def lib():
     L.ccp_context_set_timing.argtypes = [vp, i]
     L.ccp_context_phase_ms.argtypes = [vp, vp, i]
     L.ccp_device_fma_peak.argtypes = [i, i, pd]
+    L.ccp_device_mufu_peak.argtypes = [i, pd]
     L.ccp_ewald_self_correction.argtypes = [vp, d, d] + [vp] * 6 + [i, pd] + [vp] * 3 + [pd]
     L.ccp_rspace_ewald.argtypes = [vp] + [vp] * 6 + [i, d, d, pd] + [vp] * 3 + [pd]
     L.ccp_kspace_ewald.argtypes = [vp] + [vp] * 6 + [i, i, i, i, d, d, pd] + [vp] * 3 + [pd]

@@ -118,6 +118,13 @@ def fma_peak_tflops(device: int = 0, precision: str = "fp64") -> float:
     return v.value
 
 
+def mufu_peak_tops(device: int = 0) -> float:
+    """Measured special-function (MUFU exp) peak of the device (Tops/s)."""
+    v = C.c_double()
+    check(_lib.lib().ccp_device_mufu_peak(device, C.byref(v)))
+    return v.value
+
+
 def ewald_setup(ewps: float, rcut: float, box: float):
     """ewald.f90:17-43 -> (alpha, kmax1, kmax2, kmax3)."""
     a = C.c_double()

@@ -384,6 +384,9 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
 /* Measured peak of the FP64 (precision CCP_FP64) or FP32 (CCP_MIXED) fused multiply-add
    pipe of `device`, in TFLOP/s (2 flops per FMA), from a register-resident FMA chain. */
 int ccp_device_fma_peak(int device, int precision, double *tflops);
+/* Measured peak of the special-function pipe (MUFU): single-precision hardware
+   exponentials per second (Tops/s), from 8 independent exp chains per thread. */
+int ccp_device_mufu_peak(int device, double *tops);
 
 #ifdef __cplusplus
 }
