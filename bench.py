@@ -330,6 +330,53 @@ def run_batch(nframes, steps, warmup):
     print(json.dumps(line), flush=True)
 
 
+def run_fort401(steps):
+    """The configuration of the only timing the reference ships (its fort.401: 97.59 s for one
+    MD step, npt_b ensemble, 256 waters FS2+FS3, 1 MPI rank): a seeded 256-water FS2+FS3 box
+    at the C4 density (L = 19.71 A), the device npt_b_1 step (2-body + hot path + integrator)
+    timed over `steps` steps after 3 warm-up steps, and the oracle's full force evaluation of
+    the same box (2-body + hot path; the integrator is negligible beside it) on 1 host thread
+    and on all of them.  Prints one JSON line; not the headline metric."""
+    import torch
+    from ccpol23_plus_2025_mbmd_b200 import Context, Model, data_dir
+    from ccpol23_plus_2025_mbmd_b200.generator import water_box
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    model = Model(data_dir("fs2fs3"))
+    nm, L, seed = 256, 19.71, 4004
+    box = water_box(model, nm, L, seed)
+    with Context(model, nm, L, device=0) as ctx:
+        ctx.md_set_state(L, box.x, box.y, box.z, box.v, box.q, box.jb)
+        ctx.md_set_ensemble("npt_b", model.get_double("temp0"), model.get_double("taut"),
+                            model.get_double("pres0"), model.get_double("taup"))
+        ctx.md_run(3, DT_PS)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.md_run(steps, DT_PS)
+        gpu_s = (time.perf_counter() - t0) / steps
+    O.build()
+    inp = O.read_inputs(data_dir("fs2fs3"))
+    pcoord, _, _ = O.principal_frame(inp)
+    cpu = {}
+    for threads in (1, os.cpu_count() or 1):
+        O.set_threads(threads)
+        M = O.make_model(inp, nm, L)
+        t0 = time.perf_counter()
+        O.force_field(M, (True, True), pcoord, box.x, box.y, box.z, box.q, L, box.xs.shape[1])
+        cpu[threads] = time.perf_counter() - t0
+    line = {"metric": "s per MD step, 256 H2O FS2+FS3, npt_b (the reference's fort.401 case)",
+            "reference_published_s_per_step": 97.59,
+            "reference_published_note": "fort.401 of the reference: 1 MPI rank on its authors' "
+                                        "cluster CPU (hardware unknown)",
+            "gpu_s_per_step": gpu_s, "gpu_steps": steps,
+            "oracle_force_evaluation_s": {f"{k}_threads": v for k, v in cpu.items()},
+            "gpu_speedup_vs_published": 97.59 / gpu_s,
+            "gpu_speedup_vs_oracle_1_thread": cpu[1] / gpu_s,
+            "config": {"nm": nm, "box_A": L, "variant": "fs2fs3", "seed": seed,
+                       "ensemble": "npt_b", "wall_clock_timed": True}}
+    print(json.dumps(line), flush=True)
+
+
 def run_nve(nsteps, nequil):
     """Rigid-water NVE MD on the device (2-body + hot path + nve_1), FP64 and mixed forms from
     the same equilibrated state: time per MD step and the energy drift (linear fit of the
@@ -385,6 +432,9 @@ def main():
     ap.add_argument("--batch", type=int, default=0, metavar="FRAMES",
                     help="time FRAMES 256-water FS3 frames (three-body + induction terms) one "
                          "by one and as one batch call, and print that line instead")
+    ap.add_argument("--fort401", action="store_true",
+                    help="time the reference's own published case (256 waters, npt_b, one MD "
+                         "step) on the device and on 1 and all host threads, and print that line")
     ap.add_argument("--host-loop", action="store_true",
                     help="with --single: drive the dipole iteration from the host, so that "
                          "profilers see its kernels")
@@ -400,6 +450,9 @@ def main():
         return
     if args.batch:
         run_batch(args.batch, args.steps, args.warmup)
+        return
+    if args.fort401:
+        run_fort401(args.steps)
         return
     import torch
     rank, world, local = dist_env()
