@@ -45,6 +45,18 @@ def ns_per_day(steps_per_s: float) -> float:
     return steps_per_s * DT_PS * 86400.0 / 1000.0
 
 
+def max_over_ranks(v: float, world: int, device: str = "cuda") -> float:
+    """The maximum of v over the ranks (every rank takes part and gets it): per-step times of
+    replicas are reported at the slowest rank's pace."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -488,11 +500,7 @@ def main():
     peak_mufu = mufu_peak_tops(local)
 
     def agg(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks(v, world)
 
     out = {}
     for prec, r in results.items():
