@@ -45,20 +45,19 @@ __device__ __forceinline__ double tt(double delta, double r) {
   double dr = delta * r, term = 1.0, sum = 1.0;
 #pragma unroll
   for (int i = 1; i <= N; i++) {
-    term = term * dr / (double)i;
+    term = term * dr * (1.0 / (double)i);
     sum += term;
   }
   return 1.0 - exp(-dr) * sum;
 }
 template <int N>
 __device__ __forceinline__ double dtt(double delta, double r) {
-  double f = 1.0, dr = delta * r, p = 1.0;
+  constexpr double kInvFact = N == 2 ? 1.0 / 2.0 : (N == 3 ? 1.0 / 6.0 : 1.0 / 24.0);
+  static_assert(N >= 2 && N <= 4, "Tang-Toennies order");
+  double dr = delta * r, p = 1.0;
 #pragma unroll
-  for (int i = 1; i <= N; i++) {
-    f *= (double)i;
-    p *= dr;
-  }
-  return delta * exp(-dr) * p / f;
+  for (int i = 1; i <= N; i++) p *= dr;
+  return delta * exp(-dr) * p * kInvFact;
 }
 
 }  // namespace ccpd

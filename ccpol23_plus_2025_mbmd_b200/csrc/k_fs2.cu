@@ -102,17 +102,19 @@ __global__ void __launch_bounds__(128)
     const double dki2 = norm2x(xki, yki, zki), dkj2 = norm2x(xkj, ykj, zkj);
     if (!(dki2 < P.rc2 && dkj2 < P.rc2)) continue;
     const double sdki = sqrt(dki2), sdkj = sqrt(dkj2);
+    // flr = (1 / (1 + pom))^delta33, formed as exp(-delta33 log1p(pom))
     double pom = exp(P.alp3 * (sdki - P.r0dmp));
     const double pomki = 1.0 / (1.0 + pom);
-    const double flrki = pow(pomki, P.delta33);
+    const double flrki = exp(-P.delta33 * log1p(pom));
     const double dflrki = -P.alp3 * P.delta33 * pom * pomki * flrki;
     const double dflrkiv = -P.alp3 * P.delta33 * pom * pomki * sdki;
     pom = exp(P.alp3 * (sdkj - P.r0dmp));
     const double pomkj = 1.0 / (1.0 + pom);
-    const double flrkj = pow(pomkj, P.delta33);
+    const double flrkj = exp(-P.delta33 * log1p(pom));
     const double dflrkj = -P.alp3 * P.delta33 * pom * pomkj * flrkj;
     const double dflrkjv = -P.alp3 * P.delta33 * pom * pomkj * sdkj;
     const double fl = flrki * flrkj;
+    const double cki = dflrki * flrkj / sdki, ckj = dflrkj * flrki / sdkj;
     nspec++;
     double ck_x = 0, ck_y = 0, ck_z = 0;  // COM force on k
     for (int ks = 0; ks < 5; ks++) {
@@ -121,18 +123,18 @@ __global__ void __launch_bounds__(128)
       const double dxkqi = xki + sk.x - g3 * xij * dij1i;
       const double dykqi = yki + sk.y - g3 * yij * dij1i;
       const double dzkqi = zki + sk.z - g3 * zij * dij1i;
-      const double dkqi1i = 1.0 / sqrt(dxkqi * dxkqi + dykqi * dykqi + dzkqi * dzkqi);
+      const double dkqi1i = rsqrt(dxkqi * dxkqi + dykqi * dykqi + dzkqi * dzkqi);
       const double dkqi3i = dkqi1i * dkqi1i * dkqi1i;
       const double dxkqj = xkj + sk.x + g3 * xij * dij1i;
       const double dykqj = ykj + sk.y + g3 * yij * dij1i;
       const double dzkqj = zkj + sk.z + g3 * zij * dij1i;
-      const double dkqj1i = 1.0 / sqrt(dxkqj * dxkqj + dykqj * dykqj + dzkqj * dzkqj);
+      const double dkqj1i = rsqrt(dxkqj * dxkqj + dykqj * dykqj + dzkqj * dzkqj);
       const double dkqj3i = dkqj1i * dkqj1i * dkqj1i;
       const double dxkci = xki + sk.x, dykci = yki + sk.y, dzkci = zki + sk.z;
-      const double dkci1i = 1.0 / sqrt(dxkci * dxkci + dykci * dykci + dzkci * dzkci);
+      const double dkci1i = rsqrt(dxkci * dxkci + dykci * dykci + dzkci * dzkci);
       const double dkci3i = dkci1i * dkci1i * dkci1i;
       const double dxkcj = xkj + sk.x, dykcj = ykj + sk.y, dzkcj = zkj + sk.z;
-      const double dkcj1i = 1.0 / sqrt(dxkcj * dxkcj + dykcj * dykcj + dzkcj * dzkcj);
+      const double dkcj1i = rsqrt(dxkcj * dxkcj + dykcj * dykcj + dzkcj * dzkcj);
       const double dkcj3i = dkcj1i * dkcj1i * dkcj1i;
       const double term0 = dkci1i + dkcj1i - dkqi1i - dkqj1i;
       const double qE = qks * E;
@@ -152,8 +154,8 @@ __global__ void __launch_bounds__(128)
       atomicAdd(&f[nfs + so], -fky * fl * conv);
       atomicAdd(&f[2 * nfs + so], -fkz * fl * conv);
       // COM forces from the long-range damping and the exchange-charge positions
-      const double tki = qE * term0 * dflrki * flrkj / sdki;
-      const double tkj = qE * term0 * dflrkj * flrki / sdkj;
+      const double tki = qE * term0 * cki;
+      const double tkj = qE * term0 * ckj;
       ck_x += -tki * xki - tkj * xkj;
       ck_y += -tki * yki - tkj * ykj;
       ck_z += -tki * zki - tkj * zkj;

@@ -47,7 +47,6 @@ __host__ __device__ constexpr int sp(int x) { return (x & 1) * 9 + (x >> 1); }
 // index, read different banks: ti * kCi + tj * kCj + tk * kCk + j.
 constexpr int kCk = 5, kCj = 31, kCi = 187;
 constexpr int kCoef2 = 6 * kCi;
-__constant__ int kPType[kP] = {0, 0, 1, 1, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4, 5, 5, 5, 5};
 
 // Per-triple record written by the enumeration: COM vectors ij, ik, jk (bohr, computed as
 // the reference computes them), their lengths, f_dmp, d f_dmp / d r (with the 1/3 of
@@ -205,7 +204,11 @@ struct Fs3Smem {
   double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
   double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
   double2 uu[3][kP][kRS];    // (e, e d) of each site pair, families ij, ik, jk
-  double2 dl[3][kP][kRS];    // (d, d ln e / dr)
+  // force weights of each site pair: with P = q0 + d q1 the passes' output and l = d ln e / dr,
+  // the weight G = e (l P + q1) / d is (e l / d) q0 + (e l + e / d) q1, so the table holds
+  // (e l / d, e l + e / d) and the passes' epilogue needs no division; the parameter-gradient
+  // form keeps (d, l)
+  double2 dl[3][kP][kRS];
   LowUU<T> uul;              // FP32 copy of uu (mixed form)
   double G[3][kP][kRS];      // accumulated site-force weights
   double red[kFs3Block / 32];
@@ -264,7 +267,8 @@ __device__ __forceinline__ void fs3_pass(const typename Vec2<T>::type *U,
                                          const double *__restrict__ C, const PassCfg &g, int r0,
                                          int c0, T q0[4], T q1[4], double *gcv, double wsite) {
   using V2 = typename Vec2<T>::type;
-  const int tr = kPType[r0], tc = kPType[c0];
+  // site types of the padded indices: [0,2) [2,4) [4,6) [6,10) [10,14) [14,18)
+  const int tr = r0 < 6 ? r0 >> 1 : (r0 + 6) >> 2, tc = c0 < 6 ? c0 >> 1 : (c0 + 6) >> 2;
   V2 Ut[4];
   if (GRAD && gcv) {
 #pragma unroll
@@ -347,13 +351,24 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
       const double vz = S.rec.cv[p][2] + (S.site[m1][a][2] - S.site[m2][b][2]);
       const double r = sqrt(vx * vx + vy * vy + vz * vz);
       const double ex = exp(-gg * (r - r0));
-      const double damp = 1.0 / (1.0 + ex);
-      const double e = exp(-bb * r) * damp;
-      const double2 u = make_double2(e, e * r);
+      double2 u;
+      if constexpr (GRAD) {
+        const double damp = 1.0 / (1.0 + ex);
+        const double e = exp(-bb * r) * damp;
+        u = make_double2(e, e * r);
+        S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(r, -bb + gg * ex * damp);
+        GS->exd[p][sp(pidx(a))][sp(pidx(b))] = ex * damp;
+      } else {
+        // one division gives both the damping 1/(1+x) and 1/r
+        const double t = 1.0 / ((1.0 + ex) * r);
+        const double eor = exp(-bb * r) * t;  // e / r
+        const double e = eor * r;
+        const double dln = -bb + gg * ex * (t * r);
+        u = make_double2(e, e * r);
+        S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(eor * dln, e * dln + eor);
+      }
       S.uu[p][sp(pidx(a))][sp(pidx(b))] = u;
-      S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(r, -bb + gg * ex * damp);
       if constexpr (kLow) S.uul.v[p][sp(pidx(a))][sp(pidx(b))] = make_float2((float)u.x, (float)u.y);
-      if (GRAD) GS->exd[p][sp(pidx(a))][sp(pidx(b))] = ex * damp;
     }
   }
   __syncthreads();
@@ -384,6 +399,11 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
     for (int o = 0; o < 4; o++) {
       const int r = sp(r0 + (o >> 1)), c = sp(c0 + (o & 1));
       const double2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
+      if constexpr (!GRAD) {
+        if (fam == 0) esum += u.x * q0[o] + u.y * q1[o];
+        S.G[fam][r][c] += wsite * (w.x * q0[o] + w.y * q1[o]);
+        continue;
+      }
       const double P = q0[o] + w.x * q1[o];
       if (fam == 0) esum += u.x * P;
       S.G[fam][r][c] += wsite * (u.x * (w.y * P + q1[o]) / w.x);
@@ -441,7 +461,7 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   // padded dummy site: zero weight, unit distance (keeps e / d finite)
   for (int t = tid; t < 3 * kP; t += kFs3Block) {
     const int p = t / kP, q = t % kP;
-    const double2 z = make_double2(0.0, 0.0), one = make_double2(1.0, 0.0);
+    const double2 z = make_double2(0.0, 0.0), one = make_double2(GRAD ? 1.0 : 0.0, 0.0);
     S.uu[p][sp(1)][q] = z;
     S.uu[p][q][sp(1)] = z;
     S.dl[p][sp(1)][q] = one;
@@ -550,9 +570,10 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
       // COM forces from the R_avg damping and switch (threebody_potential.f90:1092-1120)
       const double(*cv)[3] = S.rec.cv;
       const double rij = S.rec.rr[0], rik = S.rec.rr[1], rjk = S.rec.rr[2];
-      const double ux = cv[0][0] / rij, uy = cv[0][1] / rij, uz = cv[0][2] / rij;
-      const double wx = cv[1][0] / rik, wy = cv[1][1] / rik, wz = cv[1][2] / rik;
-      const double sx = cv[2][0] / rjk, sy = cv[2][1] / rjk, sz = cv[2][2] / rjk;
+      const double iij = 1.0 / rij, iik = 1.0 / rik, ijk = 1.0 / rjk;
+      const double ux = cv[0][0] * iij, uy = cv[0][1] * iij, uz = cv[0][2] * iij;
+      const double wx = cv[1][0] * iik, wy = cv[1][1] * iik, wz = cv[1][2] * iik;
+      const double sx = cv[2][0] * ijk, sy = cv[2][1] * ijk, sz = cv[2][2] * ijk;
       const int m0 = S.rec.mol[0], m1 = S.rec.mol[1], m2 = S.rec.mol[2];
       atomicAdd(&fc3[m0], -comc * (ux + wx) * conv);
       atomicAdd(&fc3[nm + m0], -comc * (uy + wy) * conv);

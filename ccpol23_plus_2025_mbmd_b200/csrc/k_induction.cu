@@ -41,14 +41,14 @@ __global__ void k_dip_tensor(const double *__restrict__ x, const double *__restr
     const double4 sq = act[(size_t)j * S.na + S.a_of_p[q]];
     const double dx = c.x + sp.x - sq.x, dy = c.y + sp.y - sq.y, dz = c.z + sp.z - sq.z;
     const double d2 = dx * dx + dy * dy + dz * dz;
-    const double drr = sqrt(d2);
-    const double d1i = 1.0 / drr, d2i = d1i * d1i, d3i = d2i * d1i, d5i = d3i * d2i;
+    const double d1i = rsqrt(d2), drr = d2 * d1i, d2i = d1i * d1i, d3i = d2i * d1i;
+    const double d5i = d3i * d2i;
     const double ad = alp * drr;
     const double expar2 = exp(-(ad * ad));
     const double ec = erfc(alp * drr);
     const double d3ii = ec * d3i + P.twosqpi * alp * expar2 * d2i;
     const double d5ii = ec * d5i + P.twosqpi * alp * expar2 * d2i * d2i +
-                        2.0 * P.twosqpi * alp3 * expar2 * d2i / 3.0;
+                        (2.0 / 3.0) * P.twosqpi * alp3 * expar2 * d2i;
     double A = 3.0 * d5ii, B = d3ii;
     if (P.damped) {
       const double g = tt<3>(P.delta3, drr) - 1.0;
@@ -80,7 +80,7 @@ __global__ void k_dip_tensor(const double *__restrict__ x, const double *__restr
     const double ef = erf(alp * drr);
     const double d3ii = ef * d3i - P.twosqpi * alp * expar2 * d2i;
     const double d5ii = ef * d5i - P.twosqpi * alp * expar2 * d2i * d2i -
-                        2.0 * P.twosqpi * alp3 * expar2 * d2i / 3.0;
+                        (2.0 / 3.0) * P.twosqpi * alp3 * expar2 * d2i;
     S4[o] = make_double4(dx, dy, dz, -3.0 * d5ii);
     SB[o] = -d3ii;
   }

@@ -142,18 +142,18 @@ __global__ void __launch_bounds__(R * 32)
           const double ry = (c.y + si.y) - sj.y;
           const double rz = (c.z + si.z) - sj.z;
           const double rssq = rx * rx + ry * ry + rz * rz;
-          const double drr = sqrt(rssq);
+          const double ri = rsqrt(rssq), drr = rssq * ri;
           const double ec = erfc(alp * drr);
           const double qq = kR4pie0 * si.w * sj.w;
           const double ad = alp * drr;
-          const double fc = qq * (ec / drr + P.twosqpi * alp * exp(-(ad * ad)));
-          const double cf = fc / rssq;
+          const double fc = qq * (ec * ri + P.twosqpi * alp * exp(-(ad * ad)));
+          const double cf = fc * (ri * ri);
           const double fx = rx * cf, fy = ry * cf, fz = rz * cf;
           a0 += fx;
           a1 += fy;
           a2 += fz;
           if (half) {
-            e += qq * ec / drr;
+            e += qq * ec * ri;
             v -= rx * fx + ry * fy + rz * fz;
           }
         } else {
@@ -162,18 +162,17 @@ __global__ void __launch_bounds__(R * 32)
           const double dy = c.y + (si.y - sj.y);
           const double dz = c.z + (si.z - sj.z);
           const double d2 = dx * dx + dy * dy + dz * dz;
-          const double dist = sqrt(d2);
+          const double ri = rsqrt(d2), dist = d2 * ri;
           const double ad = alp * dist;
           const double expar2 = exp(-(ad * ad));
-          const double d1i = erfc(alp * dist) / dist;
-          const double d2i = 1.0 / d2;
+          const double d1i = erfc(alp * dist) * ri;
+          const double d2i = ri * ri;
           const double d3i = d2i * (d1i + P.twosqpi * alp * expar2);
           a0 += qj * dx * d3i;
           a1 += qj * dy * d3i;
           a2 += qj * dz * d3i;
           if (P.damped) {
-            const double r1 = 1.0 / dist;
-            const double r3 = r1 * r1 * r1;
+            const double r3 = ri * ri * ri;
             const double g = (tt<2>(P.delta2, dist) - 1.0) * qj * r3;
             b0 += g * dx;
             b1 += g * dy;
@@ -381,17 +380,16 @@ __device__ __forceinline__ void ind_pair(double dx, double dy, double dz, double
                                          const EwaldParams &P, IndPair &out) {
   const double alp = P.alpha, alp3 = alp * alp * alp, alp5 = alp3 * alp * alp;
   const double d2 = dx * dx + dy * dy + dz * dz;
-  const double dist = sqrt(d2);
-  const double d1i = 1.0 / dist, d2i = d1i * d1i, d3i = d2i * d1i, d4i = d2i * d2i;
-  const double d5i = d3i * d2i, d6i = d3i * d3i, d7i = d5i * d2i;
+  const double d1i = rsqrt(d2), dist = d2 * d1i, d2i = d1i * d1i, d3i = d2i * d1i;
+  const double d4i = d2i * d2i, d5i = d3i * d2i, d6i = d3i * d3i, d7i = d5i * d2i;
   const double ad = alp * dist;
   const double expar2 = exp(-(ad * ad));
   const double ec = erfc(alp * dist);
   const double ts = P.twosqpi;
   const double d3ii = ec * d3i + ts * alp * expar2 * d2i;
-  const double d5ii = ec * d5i + ts * alp * expar2 * d4i + 2.0 * ts * alp3 * expar2 * d2i / 3.0;
-  const double d7ii = ec * d7i + ts * alp * expar2 * d6i + 2.0 * ts * alp3 * expar2 * d4i / 3.0 +
-                      4.0 * ts * alp5 * expar2 * d2i / 15.0;
+  const double d5ii = ec * d5i + ts * alp * expar2 * d4i + (2.0 / 3.0) * ts * alp3 * expar2 * d2i;
+  const double d7ii = ec * d7i + ts * alp * expar2 * d6i + (2.0 / 3.0) * ts * alp3 * expar2 * d4i +
+                      (4.0 / 15.0) * ts * alp5 * expar2 * d2i;
   const double doti = max * dx + may * dy + maz * dz;
   const double dotj = mbx * dx + mby * dy + mbz * dz;
   const double mm = max * mbx + may * mby + maz * mbz;
