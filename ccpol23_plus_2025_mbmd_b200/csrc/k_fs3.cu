@@ -32,7 +32,6 @@ constexpr int kNt = 6;                     // FS3 site types
 constexpr int kCoef = kNt * kNt * kNt * 8;
 constexpr int kP = 18;                     // padded sites
 constexpr int kRS = 19;                    // row stride of the site-pair tables
-constexpr int kTile = 9;                   // 2x2 tiles per dimension
 constexpr int kPassThreads = 96;           // 81 tiles per pair family, warp aligned
 constexpr int kFs3Block = 320;             // 3 x 96 pass threads + one warp; 289 pair threads
 constexpr int kRecWords = 18;              // doubles per triple record
@@ -42,11 +41,12 @@ __device__ __forceinline__ int pidx(int s) { return s == 0 ? 0 : s + 1; }
 // so the two rows (or columns) of a 2x2 output tile sit 9 rows apart and neighbouring
 // tiles hit different shared-memory banks.
 __host__ __device__ constexpr int sp(int x) { return (x & 1) * 9 + (x >> 1); }
-// Coefficients in shared memory as double2 pairs (c[2j], c[2j+1]) of each type triple, with
-// padded strides (in double2 units) so that the lanes of a warp, which differ in one type
-// index, read different banks: ti * kCi + tj * kCj + tk * kCk + j.
-constexpr int kCk = 5, kCj = 31, kCi = 187;
-constexpr int kCoef2 = 6 * kCi;
+// Coefficients in shared memory: the 8 of type triple (ti, tj, tk) start at double
+// ti * kSi + tj * kSj + tk * kSk.  The strides keep entries 8 doubles apart and were chosen
+// by enumerating the half-warp phases of the passes' coefficient loads under the tile order
+// below: no two distinct entries read in one phase share a bank, except one phase in 19.
+constexpr int kSi = 45, kSj = 325, kSk = 54;
+constexpr int kCoefT = 5 * (kSi + kSj + kSk) + 8;  // doubles per SR / LR table
 
 // Per-triple record written by the enumeration: COM vectors ij, ik, jk (bohr, computed as
 // the reference computes them), their lengths, f_dmp, d f_dmp / d r (with the 1/3 of
@@ -200,7 +200,7 @@ struct LowUU<double> {
 // and the R_avg-damping COM forces.
 template <typename T>
 struct Fs3Smem {
-  double2 coef[2][kCoef2];   // SR, LR coefficients, padded layout (kCi, kCj, kCk)
+  double coef[2][kCoefT];    // SR, LR coefficients, strided layout (kSi, kSj, kSk)
   double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
   double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
   double2 uu[3][kP][kRS];    // (e, e d) of each site pair, families ij, ik, jk
@@ -249,11 +249,11 @@ __device__ __forceinline__ PassCfg pass_cfg(int fam) {
   constexpr int F = kP * kRS;
   PassCfg c;
   if (fam == 0) {  // coefficient (ti, tj, tk) = (row, col, sum)
-    c = {1 * F, kRS, 1, 2 * F, kRS, 1, 2 * kCi, 2 * kCj, 2 * kCk, {0, 4, 2, 6}, {1, 5, 3, 7}};
+    c = {1 * F, kRS, 1, 2 * F, kRS, 1, kSi, kSj, kSk, {0, 4, 2, 6}, {1, 5, 3, 7}};
   } else if (fam == 1) {  // (row, sum, col)
-    c = {0, kRS, 1, 2 * F, 1, kRS, 2 * kCi, 2 * kCk, 2 * kCj, {0, 4, 1, 5}, {2, 6, 3, 7}};
+    c = {0, kRS, 1, 2 * F, 1, kRS, kSi, kSk, kSj, {0, 4, 1, 5}, {2, 6, 3, 7}};
   } else {  // (sum, row, col)
-    c = {0, 1, kRS, 1 * F, 1, kRS, 2 * kCj, 2 * kCk, 2 * kCi, {0, 2, 1, 3}, {4, 6, 5, 7}};
+    c = {0, 1, kRS, 1 * F, 1, kRS, kSj, kSk, kSi, {0, 2, 1, 3}, {4, 6, 5, 7}};
   }
   return c;
 }
@@ -374,10 +374,16 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
   __syncthreads();
   double esum = 0.0;
   const int fam = tid / kPassThreads, lt = tid % kPassThreads;
-  if (fam < 3 && lt < kTile * kTile) {
-    const int r0 = 2 * (lt / kTile), c0 = 2 * (lt % kTile);
+  // 2x2 output tiles (R, C) of the 9 x 9 grid by quarter-warp: quarters 0..8 take row R and
+  // columns 0..7, quarter 9 takes column 8 of rows 0..7 and the first lane of quarter 10 takes
+  // (8, 8).  A quarter then reads at most 8 distinct rows or columns of a table, which its
+  // row stride spreads over distinct banks.
+  const int q8 = lt >> 3, i8 = lt & 7;
+  const int R = q8 < 9 ? q8 : (q8 == 9 ? i8 : 8), Ct = q8 < 9 ? i8 : 8;
+  if (fam < 3 && (q8 < 10 || (q8 == 10 && i8 == 0))) {
+    const int r0 = 2 * R, c0 = 2 * Ct;
     const PassCfg g = pass_cfg(fam);
-    const double *C = reinterpret_cast<const double *>(S.coef[v]);
+    const double *C = S.coef[v];
     double q0[4], q1[4];
     bool done = false;
     if constexpr (kLow) {
@@ -448,14 +454,16 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&GS->gb[0][0][0])[t] = 0.0;
     for (int t = tid; t < 3 * kP * kRS; t += kFs3Block) (&GS->exd[0][0][0])[t] = 0.0;
   }
-  for (int t = tid; t < 2 * kCoef2; t += kFs3Block) (&S.coef[0][0])[t] = make_double2(0.0, 0.0);
+  for (int t = tid; t < 2 * kCoefT; t += kFs3Block) (&S.coef[0][0])[t] = 0.0;
   __syncthreads();
   for (int t = tid; t < 2 * kCoef / 2; t += kFs3Block) {
     const int v = t / (kCoef / 2), r = t % (kCoef / 2);
     const int tri = r / 4, j = r % 4;  // type triple ti*36 + tj*6 + tk, pair j of 4
     const int ti = tri / 36, tj = (tri / 6) % 6, tk = tri % 6;
     const double *src = coef + (size_t)v * kCoef + tri * 8 + 2 * j;
-    S.coef[v][ti * kCi + tj * kCj + tk * kCk + j] = make_double2(src[0], src[1]);
+    double *dst = &S.coef[v][ti * kSi + tj * kSj + tk * kSk + 2 * j];
+    dst[0] = src[0];
+    dst[1] = src[1];
   }
   for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&S.bgr[0][0][0])[t] = bgr[t];
   // padded dummy site: zero weight, unit distance (keeps e / d finite)
