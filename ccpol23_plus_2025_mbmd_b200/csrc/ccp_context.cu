@@ -94,6 +94,7 @@ struct ccp_context {
   int2 *d_pairs = nullptr;
   // reciprocal space
   KVec *d_kv = nullptr;
+  KGather *d_kg = nullptr;
   int nk = 0, nk_cap = 0;
   double kv_box = -1, kv_alpha = -1;
   int kv_kmax[3] = {-1, -1, -1};
@@ -176,7 +177,7 @@ void free_ctx(ccp_context *c) {
                 c->d_act, c->d_comb, c->d_s17,  c->d_f,     c->d_fc2,  c->d_fc3,   c->d_scal,
                 c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
-                c->d_pairs, c->d_kv, c->d_tab,  c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
+                c->d_pairs, c->d_kv, c->d_kg, c->d_tab, c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
                 c->d_gfs3,  c->d_vdw_row, c->d_vdw_site, c->d_vdw_qq, c->d_vdw_par,
                 c->d_pcoord, c->d_md_x, c->d_md_xs, c->d_md_v, c->d_md_q, c->d_md_j, c->d_md_red,
                 c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
@@ -286,12 +287,23 @@ int ensure_kspace(ccp_context *c, double box) {
   c->nk = (int)kv.size();
   if (c->nk > c->nk_cap) {
     if (c->d_kv) cudaFree(c->d_kv);
+    if (c->d_kg) cudaFree(c->d_kg);
     if (c->d_sk) cudaFree(c->d_sk);
     CK(dalloc(&c->d_kv, (size_t)c->nk));
+    CK(dalloc(&c->d_kg, (size_t)c->nk));
     CK(dalloc(&c->d_sk, (size_t)c->nk * 4));
     c->nk_cap = c->nk;
   }
   if (c->nk) CK(cudaMemcpyAsync(c->d_kv, kv.data(), sizeof(KVec) * c->nk, cudaMemcpyHostToDevice, c->stream));
+  std::vector<KGather> kg(c->nk);
+  for (int k = 0; k < c->nk; k++) {
+    const KVec &K = kv[k];
+    kg[k] = {K.rl, K.rm, K.rn,
+             ((K.l * (2 * c->kmax[1] + 1) + K.m + c->kmax[1]) << 8) | (K.n + c->kmax[2]), 0};
+  }
+  if (c->nk)
+    CK(cudaMemcpyAsync(c->d_kg, kg.data(), sizeof(KGather) * c->nk, cudaMemcpyHostToDevice,
+                       c->stream));
   int k1 = std::max(c->kmax[0], std::max(c->kmax[1], c->kmax[2])) + 1;
   k1 = std::max(k1, 2);
   const size_t tab = (size_t)3 * k1 * c->nm * c->S.na;
@@ -333,7 +345,7 @@ constexpr double kIndThr = 1.0e-20;  // iteridm convergence threshold on sum |dm
 // the tiled dipole structure factors and reciprocal field, the update and the convergence
 // node.  `handle` is used only when use_graph is set.
 cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphConditionalHandle handle,
-                             int use_graph, int *nlaunch) {
+                             int use_graph, int par, int *nlaunch) {
   const SiteSets &S = c->S;
   if (c->use_P) {
     IterArgs A{};
@@ -350,6 +362,7 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
     A.eim = c->d_eim;
     A.e0 = c->d_e0tot;
     A.kv = c->d_kv;
+    A.kg = c->d_kg;
     A.nk = c->nk;
     A.mmax = c->kmax[1];
     A.nmax = c->kmax[2];
@@ -358,6 +371,7 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
     A.XY = c->d_P;
     A.Z = c->d_P + (size_t)A.nw * A.nlm;
     A.sk = c->d_sk;
+    A.par = par;
     A.scal = c->d_scal;
     A.state = c->d_istate;
     A.ticket = c->d_ticket;
@@ -387,6 +401,7 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
 }
 
 constexpr int kDipUnroll = 2;  // Jacobi steps per pass of the graph's WHILE body
+static_assert(kDipUnroll % 2 == 0, "the steps of a pass alternate the S(k) buffer parity");
 
 // Builds (once per set of buffers and sizes) the CUDA graph of the Jacobi iteration: a
 // WHILE conditional node whose body is one or more Jacobi steps, each ending in the
@@ -397,6 +412,7 @@ int ensure_ind_graph(ccp_context *c) {
       (long long)c->d_nbr, (long long)c->d_ncnt, (long long)c->d_T4,  (long long)c->d_TB,
       (long long)c->d_S4,  (long long)c->d_SB,   (long long)c->d_mu,  (long long)c->d_eim,
       (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_sk,  (long long)c->d_eik,
+      (long long)c->d_kg,
       (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
       (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit};
   if (c->ind_exec && key == c->ind_key) return CCP_OK;
@@ -423,7 +439,7 @@ int ensure_ind_graph(ccp_context *c) {
   // count of steps taken is unchanged while the per-pass cost of the WHILE node is shared
   const int unroll = c->use_P ? kDipUnroll : 1;
   cudaError_t e = cudaSuccess;
-  for (int u = 0; u < unroll && e == cudaSuccess; u++) e = enqueue_dip_step(c, cs, h, 1, &nl);
+  for (int u = 0; u < unroll && e == cudaSuccess; u++) e = enqueue_dip_step(c, cs, h, 1, u & 1, &nl);
   cudaGraph_t captured = nullptr;
   cudaError_t e2 = cudaStreamEndCapture(cs, &captured);
   if (!cuda_ok(e, "capture of the dipole loop")) return CCP_ERR_CUDA;
@@ -449,8 +465,9 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
     CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     per = c->use_P ? 2 : 5;
   } else {
-    for (;;) {
-      if (!cuda_ok(enqueue_dip_step(c, st, 0, 0, &per), "dipole step")) return CCP_ERR_CUDA;
+    for (int step = 0;; step++) {
+      if (!cuda_ok(enqueue_dip_step(c, st, 0, 0, step & 1, &per), "dipole step"))
+        return CCP_ERR_CUDA;
       CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       const int it = (int)c->h_istate[0];
@@ -465,7 +482,9 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
 int ensure_phase_matrix(ccp_context *c) {
   const size_t n = (size_t)c->nm * c->S.np *
                    ((size_t)(c->kmax[0] + 1) * (2 * c->kmax[1] + 1) + 2 * c->kmax[2] + 1);
-  c->use_P = c->opt_phase && c->nk > 0 && n * sizeof(double2) <= kPhaseBudget;
+  // the gather records pack the phase-table row of n in 8 bits
+  c->use_P = c->opt_phase && c->nk > 0 && n * sizeof(double2) <= kPhaseBudget &&
+             2 * c->kmax[2] + 1 <= 255;
   if (!c->use_P || n <= c->P_cap) return CCP_OK;
   if (c->d_P) cudaFree(c->d_P);
   c->d_P = nullptr;

@@ -128,6 +128,13 @@ struct KVec {
   int l, m, n, pad;
 };
 
+// The reciprocal gather's view of a k-vector: its components and its rows in the phase
+// tables, lmni = (l (2 mmax + 1) + m + mmax) << 8 | (n + nmax); 32 bytes, one L2 sector.
+struct KGather {
+  double rl, rm, rn;
+  int lmni, pad;
+};
+
 // Arguments of one Jacobi step of the dipole solve with the phase matrix (k_iter.cu).
 struct IterArgs {
   const int *nbr, *ncnt;
@@ -139,11 +146,15 @@ struct IterArgs {
   double *mu, *eim;
   const double *e0;
   const KVec *kv;
+  const KGather *kg;
   int nk;
   const double2 *XY;  // [nw][nlm] exp(i(l x + m y)), lm = l (2 mmax + 1) + m + mmax
   const double2 *Z;   // [nw][nz] exp(i n z) (conjugated for n < 0), nz = 2 nmax + 1
   int nlm, nz, mmax, nmax;
+  // sk[k] holds two S(k) buffers, (re, im) of steps of parity 0 and 1: a step accumulates
+  // into its own and clears the other, which the previous step's gather has finished with
   double *sk, *scal, *state;  // state = {iterations, change, energy, finished}
+  int par;                    // parity of this step
   unsigned *ticket;
   double thr;
   int maxit, use_graph;

@@ -9,16 +9,19 @@
 // one complex product of two table entries, and the tables (nlm + nz per site) stay in L2
 // where the full (site, k) matrix would not.  Each iteration then is
 //   A  blocks [0, nA):  T.mu, one warp per polarisable site, lanes over its (neighbour, site)
-//                       tensor entries (contiguous, so the loads coalesce);
-//      blocks [nA, ..): dipole structure factors S(k) = sum_s (k.mu_s) e^{ik.r_s}, one thread
-//                       per k over a chunk of sites, merged with FP64 atomics;
+//                       tensor entries (contiguous, so the loads coalesce); these blocks also
+//                       clear the S(k) buffer of the other step parity;
+//      blocks [nA, ..): dipole structure factors -4 a(k) S(k), S(k) = sum_s (k.mu_s)
+//                       e^{ik.r_s}, one thread per k over a chunk of sites, merged with FP64
+//                       atomics into this step's buffer;
 //   B  one warp per polarisable site: reciprocal field sum_k k g(k, s) (lanes over k), the
 //      update mu' = alpha (E_real + E_k + E0) in place, the |mu - mu'|^2 and energy sums;
 //      the last block to finish (atomic ticket) closes the iteration: it records the
-//      iteration count, change and energy, clears the accumulators and S(k) for the next
-//      iteration, marks the solve finished when it has converged (state[3]: a later B in
-//      the same pass of a graph body that unrolls several steps then returns at once) and,
-//      inside the graph, sets the WHILE node's condition.
+//      iteration count, change and energy, clears the accumulators for the next iteration,
+//      marks the solve finished when it has converged (state[3]: a later B in the same pass
+//      of a graph body that unrolls several steps then returns at once) and, inside the
+//      graph, sets the WHILE node's condition.  S(k) alternates between two buffers by step
+//      parity, so no block has to clear it after the gather.
 #include "ccp_device.cuh"
 
 using namespace ccpd;
@@ -142,6 +145,10 @@ __global__ void __launch_bounds__(kThreads)
   // scratch and S(k), which the next use clears, and it saves a dependent load per step
   const int nA = (A.nw + kWarps - 1) / kWarps;
   if ((int)blockIdx.x < nA) {
+    // the other parity's buffer: its last reader, the previous step's gather, has finished
+    double2 *other = reinterpret_cast<double2 *>(A.sk) + (A.par ^ 1);
+    for (int k = blockIdx.x * kThreads + threadIdx.x; k < A.nk; k += nA * kThreads)
+      other[2 * (size_t)k] = make_double2(0.0, 0.0);
     const int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (w >= A.nw) return;
@@ -174,8 +181,10 @@ __global__ void __launch_bounds__(kThreads)
     a0 += dk * ph.x;
     a1 += dk * ph.y;
   }
-  atomicAdd(&A.sk[(size_t)k * 4], a0);
-  atomicAdd(&A.sk[(size_t)k * 4 + 1], a1);
+  // kspace_efield_idm's weight (nb_induction_model.f90:2560-2600), applied before the merge
+  const double g = -4.0 * K.ak;
+  atomicAdd(&A.sk[(size_t)k * 4 + 2 * A.par], g * a0);
+  atomicAdd(&A.sk[(size_t)k * 4 + 2 * A.par + 1], g * a1);
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -189,13 +198,14 @@ __global__ void __launch_bounds__(kThreads)
   double acc[kGatherSites][3];
 #pragma unroll
   for (int g = 0; g < kGatherSites; g++) acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
+  const double2 *skp = reinterpret_cast<const double2 *>(A.sk) + A.par;
 #pragma unroll 2
   for (int k = threadIdx.x; k < A.nk; k += kThreads) {
-    const KVec K = A.kv[k];
-    const int lm = K.l * (2 * A.mmax + 1) + K.m + A.mmax, ni = K.n + A.nmax;
+    const KGather K = A.kg[k];
+    const int lm = K.lmni >> 8, ni = K.lmni & 255;
     // kspace_efield_idm gather (nb_induction_model.f90:2560-2600): g = -4 a_k (c S_re + s S_im)
-    const double f0 = -4.0 * K.ak * A.sk[(size_t)k * 4];
-    const double f1 = -4.0 * K.ak * A.sk[(size_t)k * 4 + 1];
+    const double2 f = skp[2 * (size_t)k];
+    const double f0 = f.x, f1 = f.y;
 #pragma unroll
     for (int g = 0; g < kGatherSites; g++) {
       if (g < ns_blk) {
@@ -248,9 +258,8 @@ __global__ void __launch_bounds__(kThreads)
   }
   __syncthreads();
   if (!last) return;
-  // every other block has added its sums and finished reading S(k)
+  // every other block has added its sums
   __threadfence();
-  for (int u = threadIdx.x; u < A.nk * 4; u += kThreads) A.sk[u] = 0.0;
   if (threadIdx.x == 0) {
     const double chg = atomicAdd(&A.scal[S_IND_CHANGE], 0.0);
     const double ene = atomicAdd(&A.scal[S_IND_ENERGY], 0.0);
