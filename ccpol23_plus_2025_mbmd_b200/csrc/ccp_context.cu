@@ -136,6 +136,11 @@ struct ccp_context {
   int *h_icnt = nullptr;
   double *h_io = nullptr;
   size_t h_io_cap = 0;
+  // pinned copies of the results of a host-buffer evaluation (site forces, FS2 and FS3 COM
+  // forces, dipoles), queued before the evaluation's one synchronisation when dl_req is set
+  double *h_out = nullptr;
+  size_t h_out_cap = 0;
+  bool dl_req = false;
   // constants for the Ewald self energy
   double sumq = 0, sumq2 = 0;
   // graph-resident Jacobi loop
@@ -173,7 +178,8 @@ namespace {
 
 void free_ctx(ccp_context *c) {
   cudaSetDevice(c->device);
-  void *dp[] = {c->d_x,   c->d_y,   c->d_z,     c->d_xs,    c->d_ys,   c->d_zs,    c->d_com,
+  // d_y, d_z live in d_x's allocation and d_ys, d_zs in d_xs's
+  void *dp[] = {c->d_x,   c->d_xs,  c->d_com,
                 c->d_act, c->d_comb, c->d_s17,  c->d_f,     c->d_fc2,  c->d_fc3,   c->d_scal,
                 c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
@@ -186,6 +192,7 @@ void free_ctx(ccp_context *c) {
   if (c->h_scal) cudaFreeHost(c->h_scal);
   if (c->h_icnt) cudaFreeHost(c->h_icnt);
   if (c->h_io) cudaFreeHost(c->h_io);
+  if (c->h_out) cudaFreeHost(c->h_out);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->ind_exec) cudaGraphExecDestroy(c->ind_exec);
@@ -206,11 +213,12 @@ void free_ctx(ccp_context *c) {
 
 int ensure_inputs(ccp_context *c, int ld) {
   if (ld <= c->ld_cap) return CCP_OK;
-  double **bufs[] = {&c->d_xs, &c->d_ys, &c->d_zs};
-  for (double **b : bufs) {
-    if (*b) cudaFree(*b);
-    CK(dalloc(b, (size_t)c->nm * ld));
-  }
+  // one allocation for the three site-offset arrays, so that an upload is one copy
+  if (c->d_xs) cudaFree(c->d_xs);
+  c->d_xs = c->d_ys = c->d_zs = nullptr;
+  CK(dalloc(&c->d_xs, 3 * (size_t)c->nm * ld));
+  c->d_ys = c->d_xs + (size_t)c->nm * ld;
+  c->d_zs = c->d_ys + (size_t)c->nm * ld;
   c->ld_cap = ld;
   return CCP_OK;
 }
@@ -694,6 +702,17 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       CK(cudaStreamWaitEvent(st, c->ev_jm, 0));
       LK(launch_add(3 * nm * ns, f3, c->d_f, st));
     }
+    if (c->dl_req) {
+      const size_t n = (size_t)nm * c->ns, np3 = (size_t)nm * c->S.np * 3;
+      double *h = c->h_out;
+      CK(cudaMemcpyAsync(h, c->d_f, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(h + 3 * n, c->d_fc2, 3 * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(h + 3 * n + 3 * nm, c->d_fc3, 3 * nm * sizeof(double),
+                         cudaMemcpyDeviceToHost, st));
+      if (np3)
+        CK(cudaMemcpyAsync(h + 3 * n + 6 * nm, c->d_mu, np3 * sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
+    }
     CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(c->h_icnt, c->d_icnt, sizeof(int) * C_COUNT, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -802,13 +821,50 @@ int upload(ccp_context *c, const double *x, const double *y, const double *z, co
   std::memcpy(h + 3 * nm + ns, ys, ns * sizeof(double));
   std::memcpy(h + 3 * nm + 2 * ns, zs, ns * sizeof(double));
   cudaStream_t st = c->stream;
-  CK(cudaMemcpyAsync(c->d_x, h, nm * sizeof(double), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->d_y, h + nm, nm * sizeof(double), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->d_z, h + 2 * nm, nm * sizeof(double), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->d_xs, h + 3 * nm, ns * sizeof(double), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->d_ys, h + 3 * nm + ns, ns * sizeof(double), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(c->d_zs, h + 3 * nm + 2 * ns, ns * sizeof(double), cudaMemcpyHostToDevice, st));
+  // d_x, d_y, d_z and d_xs, d_ys, d_zs are two contiguous blocks
+  CK(cudaMemcpyAsync(c->d_x, h, 3 * nm * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(c->d_xs, h + 3 * nm, 3 * ns * sizeof(double), cudaMemcpyHostToDevice, st));
   return CCP_OK;
+}
+
+// Pinned result buffer of ccp_hot_path: site forces, FS2 and FS3 COM forces and dipoles.
+int ensure_host_out(ccp_context *c) {
+  const size_t n = 3 * (size_t)c->nm * c->ns + 6 * (size_t)c->nm + (size_t)c->nm * c->S.np * 3;
+  if (n <= c->h_out_cap) return CCP_OK;
+  if (c->h_out) cudaFreeHost(c->h_out);
+  c->h_out = nullptr;
+  CK(cudaMallocHost((void **)&c->h_out, n * sizeof(double)));
+  c->h_out_cap = n;
+  return CCP_OK;
+}
+
+// Unpack the results that evaluate() copied into h_out into the caller's arrays: site forces
+// added into the ld layout, COM forces copied, dipoles written at the polarisable sites.
+void unpack_host_out(const ccp_context *c, int ld, double *fxs, double *fys, double *fzs,
+                     double *fxfs2, double *fyfs2, double *fzfs2, double *fxfs3, double *fyfs3,
+                     double *fzfs3, double *mx, double *my, double *mz) {
+  const size_t nm = c->nm, n = nm * c->ns;
+  const double *h = c->h_out;
+  double *f[3] = {fxs, fys, fzs};
+  for (int a = 0; a < 3; a++) {
+    if (!f[a]) continue;
+    const double *src = h + a * n;
+    for (size_t i = 0; i < nm; i++)
+      for (int s = 0; s < c->ns; s++) f[a][i * ld + s] += src[i * c->ns + s];
+  }
+  double *com[6] = {fxfs2, fyfs2, fzfs2, fxfs3, fyfs3, fzfs3};
+  for (int a = 0; a < 6; a++)
+    if (com[a]) std::memcpy(com[a], h + 3 * n + a * nm, nm * sizeof(double));
+  double *m[3] = {mx, my, mz};
+  const double *mu = h + 3 * n + 6 * nm;
+  for (int a = 0; a < 3; a++) {
+    if (!m[a]) continue;
+    for (size_t i = 0; i < nm; i++) {
+      for (int s = 0; s < c->ns; s++) m[a][i * ld + s] = 0.0;
+      for (int p = 0; p < c->S.np; p++)
+        m[a][i * ld + c->S.psite[p]] = mu[(i * c->S.np + p) * 3 + a];
+    }
+  }
 }
 
 // Download the compact site forces and add them into the caller's (ld-layout) arrays.
@@ -1040,8 +1096,7 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
       cudaMallocHost((void **)&c->h_istate, 3 * sizeof(double)) != cudaSuccess)
     return fail("loop state");
   const size_t n = nm, nsi = (size_t)nm * m->ns, np3 = (size_t)nm * std::max(S.np, 1) * 3;
-  bool ok = dalloc(&c->d_x, n) == cudaSuccess && dalloc(&c->d_y, n) == cudaSuccess &&
-            dalloc(&c->d_z, n) == cudaSuccess && dalloc(&c->d_com, n) == cudaSuccess &&
+  bool ok = dalloc(&c->d_x, 3 * n) == cudaSuccess && dalloc(&c->d_com, n) == cudaSuccess &&
             dalloc(&c->d_comb, n) == cudaSuccess &&
             dalloc(&c->d_act, n * std::max(S.na, 1)) == cudaSuccess &&
             dalloc(&c->d_s17, n * kNs3) == cudaSuccess && dalloc(&c->d_f, 6 * nsi) == cudaSuccess &&
@@ -1058,6 +1113,8 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
             dalloc(&c->d_S4, n * std::max(S.np, 1) * std::max(S.np, 1)) == cudaSuccess &&
             dalloc(&c->d_SB, n * std::max(S.np, 1) * std::max(S.np, 1)) == cudaSuccess;
   if (!ok) return fail("device allocation");
+  c->d_y = c->d_x + n;  // x, y, z share one allocation, so that an upload is one copy
+  c->d_z = c->d_y + n;
   if (cudaMemset(c->d_e0s, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
   if (cudaMemset(c->d_mu, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
   if (cudaMallocHost((void **)&c->h_scal, sizeof(double) * S_COUNT) != cudaSuccess ||
@@ -1420,15 +1477,17 @@ int ccp_hot_path(ccp_context *ctx, const double *x, const double *y, const doubl
   if (r) return r;
   CK(cudaSetDevice(ctx->device));
   r = upload(ctx, x, y, z, xs, ys, zs, ld);
+  if (!r) r = ensure_host_out(ctx);
   EvalOut o;
+  // the results' copies are queued before the evaluation's one synchronisation
+  ctx->dl_req = true;
   if (!r) r = evaluate(ctx, ctx->d_x, ctx->d_y, ctx->d_z, ctx->d_xs, ctx->d_ys, ctx->d_zs, ld, box, hot_mask(ctx), o);
+  ctx->dl_req = false;
   if (r) return r;
   fill_energies(ctx, o, box, e);
-  r = download_forces(ctx, ld, fxs, fys, fzs);
-  if (!r) r = download_com(ctx, ctx->d_fc2, fxfs2, fyfs2, fzfs2);
-  if (!r) r = download_com(ctx, ctx->d_fc3, fxfs3, fyfs3, fzfs3);
-  if (!r) r = download_dipoles(ctx, ld, idmx, idmy, idmz);
-  return r;
+  unpack_host_out(ctx, ld, fxs, fys, fzs, fxfs2, fyfs2, fzfs2, fxfs3, fyfs3, fzfs3, idmx, idmy,
+                  idmz);
+  return CCP_OK;
 }
 
 int ccp_terms_device(ccp_context *ctx, unsigned terms, const double *x, const double *y,
