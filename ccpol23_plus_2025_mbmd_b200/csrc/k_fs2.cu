@@ -4,7 +4,8 @@
 // eta exp(-beta r) over the 3x3 O/H site pairs, interacting with the five 3-body charges of
 // a spectator k, with long-range dampings of the two spectator distances.  The nine
 // exchange terms of a pair do not depend on the spectator, so one warp per pair (i < j)
-// computes them once and its lanes then walk the spectators k.
+// computes them once; its lanes then test i's neighbours against both cut-offs, queue the
+// spectators that pass, and evaluate them 32 at a time.
 #include "ccp_device.cuh"
 
 using namespace ccpd;
@@ -90,17 +91,15 @@ __global__ void __launch_bounds__(128)
   double e_loc = 0.0, v_loc = 0.0, A_loc = 0.0;
   double Ci[3] = {0, 0, 0}, Cj[3] = {0, 0, 0};
   int nspec = 0;
-  const int cnt = ncnt[i];
-  for (int n = lane; n < cnt; n += 32) {
-    const int k = nbr[(size_t)i * cap + n];
-    if (k == j) continue;
+  // One spectator k that passed both cut-offs: its five 3-body charges against the pair's
+  // exchange quadrupole.
+  auto spectator = [&](int k) {
     const double4 ck = comb[k];
     const double xki = minimg(xsub(ck.x, ci.x), P.boxb);
     const double yki = minimg(xsub(ck.y, ci.y), P.boxb);
     const double zki = minimg(xsub(ck.z, ci.z), P.boxb);
     const double xkj = xadd(xki, xij), ykj = xadd(yki, yij), zkj = xadd(zki, zij);
     const double dki2 = norm2x(xki, yki, zki), dkj2 = norm2x(xkj, ykj, zkj);
-    if (!(dki2 < P.rc2 && dkj2 < P.rc2)) continue;
     const double sdki = sqrt(dki2), sdkj = sqrt(dkj2);
     // flr = (1 / (1 + pom))^delta33, formed as exp(-delta33 log1p(pom))
     double pom = exp(P.alp3 * (sdki - P.r0dmp));
@@ -188,7 +187,43 @@ __global__ void __launch_bounds__(128)
     atomicAdd(&fc2[k], ck_x * conv);
     atomicAdd(&fc2[nm + k], ck_y * conv);
     atomicAdd(&fc2[2 * nm + k], ck_z * conv);
+  };
+  // The spectators are i's neighbours k != j within the cut-off of both i and j; only a
+  // fraction pass, so the warp first queues them (ballot + prefix into shared memory) and
+  // evaluates them 32 at a time with every lane busy.
+  __shared__ int kq_all[4][64];
+  int *kq = kq_all[threadIdx.x >> 5];
+  const unsigned below = (1u << lane) - 1u;
+  int nq = 0;
+  const int cnt = ncnt[i];
+  for (int n0 = 0; n0 < cnt; n0 += 32) {
+    const int n = n0 + lane;
+    bool pass = false;
+    int k = 0;
+    if (n < cnt) {
+      k = nbr[(size_t)i * cap + n];
+      if (k != j) {
+        const double4 ck = comb[k];
+        const double xki = minimg(xsub(ck.x, ci.x), P.boxb);
+        const double yki = minimg(xsub(ck.y, ci.y), P.boxb);
+        const double zki = minimg(xsub(ck.z, ci.z), P.boxb);
+        const double xkj = xadd(xki, xij), ykj = xadd(yki, yij), zkj = xadd(zki, zij);
+        pass = norm2x(xki, yki, zki) < P.rc2 && norm2x(xkj, ykj, zkj) < P.rc2;
+      }
+    }
+    const unsigned bal = __ballot_sync(0xffffffffu, pass);
+    if (pass) kq[nq + __popc(bal & below)] = k;
+    nq += __popc(bal);
+    __syncwarp();
+    if (nq >= 32) {
+      spectator(kq[lane]);
+      __syncwarp();
+      if (lane < nq - 32) kq[lane] = kq[32 + lane];
+      nq -= 32;
+      __syncwarp();
+    }
   }
+  if (lane < nq) spectator(kq[lane]);
   e_loc = warp_sum(e_loc);
   v_loc = warp_sum(v_loc);
   A_loc = warp_sum(A_loc);
