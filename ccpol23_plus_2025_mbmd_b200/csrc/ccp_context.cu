@@ -169,6 +169,10 @@ struct ccp_context {
   // list, joined before the scalars are read back)
   cudaStream_t s_fs3 = nullptr, s_fs2 = nullptr, s_main = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_j3 = nullptr, ev_j2 = nullptr, ev_jm = nullptr;
+  // the reciprocal-space branch of the Ewald/induction chain (k tables, structure factors,
+  // gathers) on its own high-priority stream beside the real-space kernels
+  cudaStream_t s_kspace = nullptr;
+  cudaEvent_t ev_k1 = nullptr, ev_k2 = nullptr, ev_lp = nullptr;
   int opt_overlap = 1;     // three-body terms concurrent with Ewald/induction
   int opt_fs3_tpb = 8;     // FS3 triples per block when concurrent (0 = persistent grid)
   int opt_fs3_bps = 0;     // when concurrent, at most this many FS3 blocks per SM (0 = no cap)
@@ -206,7 +210,8 @@ void free_ctx(ccp_context *c) {
   if (c->s_fs3) cudaStreamDestroy(c->s_fs3);
   if (c->s_fs2) cudaStreamDestroy(c->s_fs2);
   if (c->s_main) cudaStreamDestroy(c->s_main);
-  for (cudaEvent_t e : {c->ev_fork, c->ev_j3, c->ev_j2, c->ev_jm})
+  if (c->s_kspace) cudaStreamDestroy(c->s_kspace);
+  for (cudaEvent_t e : {c->ev_fork, c->ev_j3, c->ev_j2, c->ev_jm, c->ev_k1, c->ev_k2, c->ev_lp})
     if (e) cudaEventDestroy(e);
   if (c->own) cudaStreamDestroy(c->own);
 }
@@ -591,11 +596,17 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       LK(launch_neighbors(c->d_com, nm, box, rl * rl, c->cap, c->d_nbr, c->d_nbrv, c->d_ncnt,
                           c->d_icnt, st));
     pend(0, st);
+    // with the terms overlapping, the reciprocal-space branch runs on its own stream; its
+    // forces go to the three-body block f3, which receives atomic additions only, while the
+    // real-space kernels add to d_f without atomics
+    const bool kfork = side && (mask & (T_KSPACE | T_INDUCTION));
+    cudaStream_t sk = kfork ? c->s_kspace : sm;
     if (side) {
       CK(cudaEventRecord(c->ev_fork, st));
       CK(cudaStreamWaitEvent(s3, c->ev_fork, 0));
       CK(cudaStreamWaitEvent(s2, c->ev_fork, 0));
       CK(cudaStreamWaitEvent(sm, c->ev_fork, 0));
+      if (kfork) CK(cudaStreamWaitEvent(sk, c->ev_fork, 0));
     }
     // three-body terms first, so that on side streams they start at once
     double *f3 = side ? c->d_f + (size_t)3 * nm * ns : c->d_f;
@@ -646,36 +657,39 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                             c->d_scal, sm));
     }
     pend(1, sm);
-    pbeg(2, sm);
+    double *fk = kfork ? f3 : c->d_f;
+    pbeg(2, sk);
     if (mask & (T_KSPACE | T_INDUCTION))
       LK(launch_ktab(c->d_com, c->d_act, nm, S, box, c->kmax[0], c->kmax[1], c->kmax[2], c->d_tab,
-                     sm));
+                     sk));
     if (mask & T_KSPACE) {
       LK(launch_kspace_sums(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, sm));
-      LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sm));
+                            c->d_mu, c->d_sk, sk));
+      LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sk));
       LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, sm));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, fk, sk));
     }
-    pend(2, sm);
+    pend(2, sk);
     if (mask & T_INDUCTION) {
       pbeg(3, sm);
       // the static field's structure factors (charges, mode 1) are the Ewald sums' (mode 0):
       // when those ran, d_sk still holds them
       if (!(mask & T_KSPACE))
         LK(launch_kspace_sums(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, sm));
+                              c->kmax[2], c->d_mu, c->d_sk, sk));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, c->d_f, sm));
-      if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, sm));
-      LK(launch_dip_tensor(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt,
-                           c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, sm));
-      LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
-                             sm));
+                              c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, fk, sk));
       if (c->use_P)
         LK(launch_phase_factors(c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2], c->d_P,
                                 c->d_P + (size_t)nm * S.np * (c->kmax[0] + 1) * (2 * c->kmax[1] + 1),
-                                sm));
+                                sk));
+      if (kfork) CK(cudaEventRecord(c->ev_k1, sk));
+      if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, sm));
+      LK(launch_dip_tensor(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt,
+                           c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, sm));
+      if (kfork) CK(cudaStreamWaitEvent(sm, c->ev_k1, 0));
+      LK(launch_static_total(nm * S.np * 3, c->d_e0r, c->d_e0k, c->d_e0slf, c->d_e0s, c->d_e0tot,
+                             sm));
       pend(3, sm);
       pbeg(4, sm);
       {
@@ -684,14 +698,25 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
       }
       pend(4, sm);
       pbeg(5, sm);
+      if (kfork) {
+        CK(cudaEventRecord(c->ev_lp, sm));
+        CK(cudaStreamWaitEvent(sk, c->ev_lp, 0));
+      }
       LK(launch_pair_indforce(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv,
                               c->d_ncnt, c->cap, nm, S, P, c->d_mu, c->d_f, c->d_scal, sm));
       LK(launch_kspace_sums(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
-                            c->d_mu, c->d_sk, sm));
-      LK(launch_kspace_energy(3, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sm));
+                            c->d_mu, c->d_sk, sk));
+      LK(launch_kspace_energy(3, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sk));
       LK(launch_kspace_gather(3, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
-                              c->kmax[2], c->d_mu, c->d_sk, nullptr, c->d_f, sm));
+                              c->kmax[2], c->d_mu, c->d_sk, nullptr, fk, sk));
+      if (kfork) {
+        CK(cudaEventRecord(c->ev_k2, sk));
+        CK(cudaStreamWaitEvent(sm, c->ev_k2, 0));
+      }
       pend(5, sm);
+    } else if (kfork) {
+      CK(cudaEventRecord(c->ev_k2, sk));
+      CK(cudaStreamWaitEvent(sm, c->ev_k2, 0));
     }
     if (side) {
       CK(cudaEventRecord(c->ev_j3, s3));
@@ -784,6 +809,7 @@ int evaluate(ccp_context *c, const double *px, const double *py, const double *p
     cudaStreamSynchronize(c->s_fs3);
     cudaStreamSynchronize(c->s_fs2);
     cudaStreamSynchronize(c->s_main);
+    cudaStreamSynchronize(c->s_kspace);
   }
   return r;
 }
@@ -1082,12 +1108,16 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
   if (cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->s_fs3, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
       cudaStreamCreateWithPriority(&c->s_fs2, cudaStreamNonBlocking, prio_lo) != cudaSuccess ||
-      cudaStreamCreateWithPriority(&c->s_main, cudaStreamNonBlocking, prio_hi) != cudaSuccess)
+      cudaStreamCreateWithPriority(&c->s_main, cudaStreamNonBlocking, prio_hi) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->s_kspace, cudaStreamNonBlocking, prio_hi) != cudaSuccess)
     return fail("stream");
   if (cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_j3, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->ev_j2, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&c->ev_jm, cudaEventDisableTiming) != cudaSuccess)
+      cudaEventCreateWithFlags(&c->ev_jm, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_k1, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_k2, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->ev_lp, cudaEventDisableTiming) != cudaSuccess)
     return fail("event");
   c->stream = c->own;
   if (cudaMalloc(&c->d_istate, 4 * sizeof(double)) != cudaSuccess ||
