@@ -335,9 +335,10 @@ __device__ __forceinline__ void fs3_pass(const typename Vec2<T>::type *U,
 }
 
 // One SR (v = 0) or LR (v = 1) sweep of the current triple: tabulate the site pairs, run
-// the three gradient passes, add wsite * G into S.G and return the energy sum.
+// the three gradient passes, store (first sweep of the triple) or add wsite * G into S.G and
+// return the energy sum.
 template <typename T, bool GRAD>
-__device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite) {
+__device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite, bool first) {
   constexpr bool kLow = sizeof(T) == 4;
   const int tid = threadIdx.x;
   if (tid < kPairs) {
@@ -407,12 +408,14 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
       const double2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
       if constexpr (!GRAD) {
         if (fam == 0) esum += u.x * q0[o] + u.y * q1[o];
-        S.G[fam][r][c] += wsite * (w.x * q0[o] + w.y * q1[o]);
+        const double gw = wsite * (w.x * q0[o] + w.y * q1[o]);
+        S.G[fam][r][c] = first ? gw : S.G[fam][r][c] + gw;
         continue;
       }
       const double P = q0[o] + w.x * q1[o];
       if (fam == 0) esum += u.x * P;
-      S.G[fam][r][c] += wsite * (u.x * (w.y * P + q1[o]) / w.x);
+      const double gw = wsite * (u.x * (w.y * P + q1[o]) / w.x);
+      S.G[fam][r][c] = first ? gw : S.G[fam][r][c] + gw;
       const int ra = r0 + (o >> 1), cb = c0 + (o & 1);
       if (GRAD && ra != 1 && cb != 1) {
         // dS/de_ab = P; de/db = -r e, de/dg = (r - r0) e x, de/dr0 = -g e x with
@@ -485,13 +488,14 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   double e_tot = 0.0, v_tot = 0.0;
   for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
     __syncthreads();
+    // warp 0 stages the record; warps 2-3 stage the site offsets, reading the molecule
+    // indices from the record in global memory (the passes store every entry of S.G, so it
+    // needs no clearing)
     if (tid < kRecWords)
       reinterpret_cast<double *>(&S.rec)[tid] = reinterpret_cast<const double *>(recs + t)[tid];
-    for (int u = tid; u < 3 * kP * kRS; u += kFs3Block) (&S.G[0][0][0])[u] = 0.0;
-    __syncthreads();
-    if (tid < 3 * kNs3) {
-      const int m = tid / kNs3, s = tid % kNs3;
-      const double4 o = s17[(size_t)S.rec.mol[m] * kNs3 + s];
+    if (tid >= 64 && tid < 64 + 3 * kNs3) {
+      const int m = (tid - 64) / kNs3, s = (tid - 64) % kNs3;
+      const double4 o = s17[(size_t)recs[t].mol[m] * kNs3 + s];
       S.site[m][s][0] = o.x;
       S.site[m][s][1] = o.y;
       S.site[m][s][2] = o.z;
@@ -501,13 +505,13 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     const int br = S.rec.branch;
     double energy, comc;
     if (br != 2) {
-      const double Sv = fs3_variant<T, GRAD>(S, GS, br, fdmp);
+      const double Sv = fs3_variant<T, GRAD>(S, GS, br, fdmp, true);
       energy = fdmp * Sv;
       comc = dfdmp * Sv;
     } else {
       const double smfun = S.rec.smfun, smfun2 = 1.0 - smfun, cf = S.rec.cf;
-      const double Ssr = fs3_variant<T, GRAD>(S, GS, 0, fdmp * smfun);
-      const double Slr = fs3_variant<T, GRAD>(S, GS, 1, fdmp * smfun2);
+      const double Ssr = fs3_variant<T, GRAD>(S, GS, 0, fdmp * smfun, true);
+      const double Slr = fs3_variant<T, GRAD>(S, GS, 1, fdmp * smfun2, false);
       energy = fdmp * (smfun * Ssr + smfun2 * Slr);
       comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
     }
