@@ -1,0 +1,70 @@
+"""The evaluation's stream layouts give the same results: with the terms overlapping, FS3,
+FS2 and the reciprocal-space branch run on their own streams and add their forces into a
+separate block; with `overlap` off everything runs in order on one stream.  Also a term mask
+that forks the reciprocal branch without the induction (k-space Ewald + FS3) equals the sum
+of its terms run one at a time."""
+import numpy as np
+import pytest
+
+from ccpol23_plus_2025_mbmd_b200 import Context, Model, _lib, data_dir
+from ccpol23_plus_2025_mbmd_b200.generator import water_box
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+ENERGIES = ("scpe", "rcpe", "kcpe", "indpe", "fs2pe", "fs3pe", "vir")
+
+
+@pytest.fixture(scope="module")
+def box(product):
+    m = Model(data_dir("fs2fs3"))
+    return m, water_box(m, 128, 15.64, 77, ld=28)
+
+
+def _dev(a):
+    import torch
+    return torch.as_tensor(np.ascontiguousarray(a), device=torch.device("cuda:0"))
+
+
+def _zeros(shape):
+    import torch
+    return torch.zeros(shape, dtype=torch.float64, device=torch.device("cuda:0"))
+
+
+def _run(m, b, terms, overlap):
+    nm, ld = b.xs.shape
+    args = [_dev(a) for a in (b.x, b.y, b.z, b.xs, b.ys, b.zs)]
+    f = [_zeros((nm, ld)) for _ in range(3)]
+    c2 = [_zeros(nm) for _ in range(3)]
+    c3 = [_zeros(nm) for _ in range(3)]
+    mu = [_zeros((nm, ld)) for _ in range(3)]
+    with Context(m, nm, b.box) as c:
+        c.set_option("overlap", overlap)
+        e = c.terms_device(terms, *args, b.box, *f, *c2, *c3, *mu)
+    fn = lambda ts: np.stack([t.cpu().numpy() for t in ts])
+    return e, fn(f), fn(c2), fn(c3), fn(mu)
+
+
+def test_overlap_matches_in_order(box):
+    m, b = box
+    e1, f1, c21, c31, mu1 = _run(m, b, _lib.TERM_HOT, 1)
+    e0, f0, c20, c30, mu0 = _run(m, b, _lib.TERM_HOT, 0)
+    for k in ENERGIES:
+        assert e1[k] == pytest.approx(e0[k], rel=1e-12), k
+    assert e1["ind_iters"] == e0["ind_iters"]
+    assert rel(f1, f0) <= 1e-12
+    assert rel(c21, c20) <= 1e-12
+    assert rel(c31, c30) <= 1e-12
+    assert rel(mu1, mu0) <= 1e-12
+
+
+def test_kspace_with_fs3_equals_separate_terms(box):
+    m, b = box
+    eb, fb, _, c3b, _ = _run(m, b, _lib.TERM_KSPACE | _lib.TERM_FS3, 1)
+    ek, fk, _, _, _ = _run(m, b, _lib.TERM_KSPACE, 1)
+    e3, f3, _, c33, _ = _run(m, b, _lib.TERM_FS3, 1)
+    assert eb["kcpe"] == pytest.approx(ek["kcpe"], rel=1e-12)
+    assert eb["fs3pe"] == pytest.approx(e3["fs3pe"], rel=1e-12)
+    assert rel(fb, fk + f3) <= 1e-12
+    assert rel(c3b, c33) <= 1e-12
