@@ -36,7 +36,8 @@ __constant__ double kCharge3b[5] = {0.258504607653328389, 0.564050362569283648,
                                     0.564050362569283648, -0.693302666395947953,
                                     -0.693302666395947953};
 
-__global__ void __launch_bounds__(128)
+// 4 blocks (16 warps) per SM: 128 registers a thread, against 154 unbounded
+__global__ void __launch_bounds__(128, 4)
     k_fs2(const int2 *__restrict__ pairs, const int *__restrict__ icnt, int pair_cap,
           const double4 *__restrict__ comb, const double4 *__restrict__ s17,
           const int *__restrict__ nbr, const int *__restrict__ ncnt, int cap, Fs2Params P,
