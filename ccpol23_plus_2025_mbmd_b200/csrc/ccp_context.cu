@@ -101,6 +101,8 @@ struct ccp_context {
   double2 *d_tab = nullptr;
   size_t tab_cap = 0;
   double *d_sk = nullptr;
+  double *d_skj = nullptr;  // the dipole loop's own S(k) buffers, so that the Ewald sums in
+                            // d_sk can still be gathered while the loop runs
   // FS3 tables
   double *d_coef = nullptr, *d_bgr = nullptr;
   // rigid-molecule MD state (ccp_md_*), structure of arrays on the device
@@ -187,7 +189,8 @@ void free_ctx(ccp_context *c) {
                 c->d_act, c->d_comb, c->d_s17,  c->d_f,     c->d_fc2,  c->d_fc3,   c->d_scal,
                 c->d_icnt, c->d_mu, c->d_e0r,   c->d_e0k,   c->d_e0slf, c->d_e0s,  c->d_eir,
                 c->d_eik, c->d_eislf, c->d_eis, c->d_nbr,   c->d_ncnt, c->d_nbrv,  c->d_tri,
-                c->d_pairs, c->d_kv, c->d_kg, c->d_tab, c->d_sk,    c->d_coef, c->d_bgr,   c->d_types,
+                c->d_pairs, c->d_kv, c->d_kg, c->d_tab, c->d_sk, c->d_skj, c->d_coef, c->d_bgr,
+                c->d_types,
                 c->d_gfs3,  c->d_vdw_row, c->d_vdw_site, c->d_vdw_qq, c->d_vdw_par,
                 c->d_pcoord, c->d_md_x, c->d_md_xs, c->d_md_v, c->d_md_q, c->d_md_j, c->d_md_red,
                 c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
@@ -302,9 +305,11 @@ int ensure_kspace(ccp_context *c, double box) {
     if (c->d_kv) cudaFree(c->d_kv);
     if (c->d_kg) cudaFree(c->d_kg);
     if (c->d_sk) cudaFree(c->d_sk);
+    if (c->d_skj) cudaFree(c->d_skj);
     CK(dalloc(&c->d_kv, (size_t)c->nk));
     CK(dalloc(&c->d_kg, (size_t)c->nk));
     CK(dalloc(&c->d_sk, (size_t)c->nk * 4));
+    CK(dalloc(&c->d_skj, (size_t)c->nk * 4));
     c->nk_cap = c->nk;
   }
   if (c->nk) CK(cudaMemcpyAsync(c->d_kv, kv.data(), sizeof(KVec) * c->nk, cudaMemcpyHostToDevice, c->stream));
@@ -383,7 +388,7 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
     A.nz = 2 * c->kmax[2] + 1;
     A.XY = c->d_P;
     A.Z = c->d_P + (size_t)A.nw * A.nlm;
-    A.sk = c->d_sk;
+    A.sk = c->d_skj;
     A.par = par;
     A.scal = c->d_scal;
     A.state = c->d_istate;
@@ -402,10 +407,10 @@ cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphCondition
                              c->d_SB, c->d_mu, c->d_eim, st);
   if (e == cudaSuccess)
     e = launch_kspace_sums(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
-                           c->kmax[2], c->d_mu, c->d_sk, st);
+                           c->kmax[2], c->d_mu, c->d_skj, st);
   if (e == cudaSuccess)
     e = launch_kspace_gather(2, c->d_kv, c->nk, c->d_tab, c->nm, S, c->kmax[0], c->kmax[1],
-                             c->kmax[2], c->d_mu, c->d_sk, c->d_eik, nullptr, st);
+                             c->kmax[2], c->d_mu, c->d_skj, c->d_eik, nullptr, st);
   if (e == cudaSuccess)
     e = launch_dip_update(c->nm, S, c->d_e0tot, c->d_eim, c->d_eik, c->d_mu, c->d_mu, c->d_scal, st);
   if (e == cudaSuccess)
@@ -424,7 +429,7 @@ int ensure_ind_graph(ccp_context *c) {
   std::vector<long long> key = {
       (long long)c->d_nbr, (long long)c->d_ncnt, (long long)c->d_T4,  (long long)c->d_TB,
       (long long)c->d_S4,  (long long)c->d_SB,   (long long)c->d_mu,  (long long)c->d_eim,
-      (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_sk,  (long long)c->d_eik,
+      (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_skj, (long long)c->d_eik,
       (long long)c->d_kg,
       (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
       (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit};
@@ -469,7 +474,7 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
   CK(cudaMemsetAsync(c->d_istate, 0, 4 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_ticket, 0, sizeof(unsigned), st));
-  if (c->use_P) CK(cudaMemsetAsync(c->d_sk, 0, sizeof(double) * 4 * (size_t)c->nk, st));
+  if (c->use_P) CK(cudaMemsetAsync(c->d_skj, 0, sizeof(double) * 4 * (size_t)c->nk, st));
   int per = 0;
   if (c->opt_graph) {
     int r = ensure_ind_graph(c);
@@ -662,9 +667,14 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     if (mask & (T_KSPACE | T_INDUCTION))
       LK(launch_ktab(c->d_com, c->d_act, nm, S, box, c->kmax[0], c->kmax[1], c->kmax[2], c->d_tab,
                      sk));
-    if (mask & T_KSPACE) {
+    if (mask & T_KSPACE)
       LK(launch_kspace_sums(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2],
                             c->d_mu, c->d_sk, sk));
+    // the Ewald energy and forces from those sums: here when the chain is serial, or after
+    // the dipole loop's inputs on the reciprocal branch's stream, beside the loop (which uses
+    // its own S(k) buffers)
+    const bool ewald_late = kfork && (mask & T_INDUCTION);
+    if ((mask & T_KSPACE) && !ewald_late) {
       LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sk));
       LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
                               c->kmax[2], c->d_mu, c->d_sk, nullptr, fk, sk));
@@ -684,6 +694,11 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                                 c->d_P + (size_t)nm * S.np * (c->kmax[0] + 1) * (2 * c->kmax[1] + 1),
                                 sk));
       if (kfork) CK(cudaEventRecord(c->ev_k1, sk));
+      if ((mask & T_KSPACE) && ewald_late) {
+        LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sk));
+        LK(launch_kspace_gather(0, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
+                                c->kmax[2], c->d_mu, c->d_sk, nullptr, fk, sk));
+      }
       if (!c->damped) CK(cudaMemsetAsync(c->d_e0s, 0, sizeof(double) * nm * S.np * 3, sm));
       LK(launch_dip_tensor(px, py, pz, pxs, pys, pzs, ld, c->d_act, c->d_nbr, c->d_nbrv, c->d_ncnt,
                            c->cap, nm, S, P, c->d_T4, c->d_TB, c->d_S4, c->d_SB, sm));
