@@ -405,13 +405,20 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
 #pragma unroll
     for (int o = 0; o < 4; o++) {
       const int r = sp(r0 + (o >> 1)), c = sp(c0 + (o & 1));
-      const double2 u = S.uu[fam][r][c], w = S.dl[fam][r][c];
+      const double2 w = S.dl[fam][r][c];
       if constexpr (!GRAD) {
-        if (fam == 0) esum += u.x * q0[o] + u.y * q1[o];
+        if (fam == 0) {  // warp-uniform: only the ij family's outputs carry the energy
+          const double2 u = S.uu[0][r][c];
+          esum += u.x * q0[o] + u.y * q1[o];
+        }
         const double gw = wsite * (w.x * q0[o] + w.y * q1[o]);
-        S.G[fam][r][c] = first ? gw : S.G[fam][r][c] + gw;
+        if (first)
+          S.G[fam][r][c] = gw;
+        else
+          S.G[fam][r][c] += gw;
         continue;
       }
+      const double2 u = S.uu[fam][r][c];
       const double P = q0[o] + w.x * q1[o];
       if (fam == 0) esum += u.x * P;
       const double gw = wsite * (u.x * (w.y * P + q1[o]) / w.x);
