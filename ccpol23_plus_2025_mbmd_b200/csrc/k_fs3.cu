@@ -336,16 +336,18 @@ __device__ __forceinline__ void fs3_pass(const typename Vec2<T>::type *U,
 
 // One SR (v = 0) or LR (v = 1) sweep of the current triple: tabulate the site pairs, run
 // the three gradient passes, store (first sweep of the triple) or add wsite * G into S.G and
-// return the energy sum.
+// return the energy sum.  With keep_ij the ij family's tables already hold this molecule
+// pair and variant (the previous sweep of the block had them) and are not tabulated again.
 template <typename T, bool GRAD>
-__device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite, bool first) {
+__device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite, bool first,
+                              bool keep_ij) {
   constexpr bool kLow = sizeof(T) == 4;
   const int tid = threadIdx.x;
   if (tid < kPairs) {
     const int a = tid / kNs3, b = tid % kNs3;
     const double bb = S.bgr[v][0][tid], gg = S.bgr[v][1][tid], r0 = S.bgr[v][2][tid];
 #pragma unroll 1
-    for (int p = 0; p < 3; p++) {
+    for (int p = keep_ij ? 1 : 0; p < 3; p++) {
       const int m1 = p == 2 ? 1 : 0, m2 = p == 0 ? 1 : 2;
       const double vx = S.rec.cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
       const double vy = S.rec.cv[p][1] + (S.site[m1][a][1] - S.site[m2][b][1]);
@@ -458,7 +460,13 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
   Fs3Grad<T> *GS = GRAD ? reinterpret_cast<Fs3Grad<T> *>(smem_raw + fs3_grad_offset<T>()) : nullptr;
   const int tid = threadIdx.x;
-  if ((int)blockIdx.x >= min(icnt[C_NTRI_FS3], tri_cap)) return;  // no triple for this block
+  // each block takes a contiguous run of the triple list: the enumeration writes the triples
+  // of one molecule pair (i, j) next to each other, so consecutive triples often share the
+  // ij site-pair tables
+  const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
+  const int chunk = (ntri + (int)gridDim.x - 1) / (int)gridDim.x;
+  const int t_begin = (int)blockIdx.x * chunk, t_end = min(t_begin + chunk, ntri);
+  if (t_begin >= t_end) return;  // no triple for this block
   if (GRAD) {
     for (int t = tid; t < 2 * kCoef; t += kFs3Block) (&GS->gc[0][0])[t] = 0.0;
     for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) (&GS->gb[0][0][0])[t] = 0.0;
@@ -489,11 +497,11 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
       S.uul.v[p][q][sp(1)] = make_float2(0.f, 0.f);
     }
   }
-  const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
   const double conv = kH2kcal * 418.4 / kBohr2a;
   const size_t nfs = (size_t)nm * ns;
   double e_tot = 0.0, v_tot = 0.0;
-  for (int t = blockIdx.x; t < ntri; t += gridDim.x) {
+  int have_i = -1, have_j = -1, have_v = -1;  // molecule pair and variant of the ij tables
+  for (int t = t_begin; t < t_end; t++) {
     __syncthreads();
     // warp 0 stages the record; warps 2-3 stage the site offsets, reading the molecule
     // indices from the record in global memory (the passes store every entry of S.G, so it
@@ -511,14 +519,32 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     const double fdmp = S.rec.fdmp, dfdmp = S.rec.dfdmp;
     const int br = S.rec.branch;
     double energy, comc;
+    const bool same_ij = S.rec.mol[0] == have_i && S.rec.mol[1] == have_j;
+    have_i = S.rec.mol[0];
+    have_j = S.rec.mol[1];
+    // one sweep (SR or LR branch) or two (blend); of two, the one whose ij tables are already
+    // in place goes first.  One call site keeps the kernel's instruction footprint small.
+    const double smfun = S.rec.smfun, smfun2 = 1.0 - smfun;
+    const int nsweep = br == 2 ? 2 : 1;
+    const bool lr_first = br == 2 && same_ij && have_v == 1;
+    double Ssr = 0.0, Slr = 0.0;
+#pragma unroll 1
+    for (int w = 0; w < nsweep; w++) {
+      const int v = br != 2 ? br : ((w == 0) == lr_first ? 1 : 0);
+      const double ws = br != 2 ? fdmp : fdmp * (v == 0 ? smfun : smfun2);
+      const double Sv = fs3_variant<T, GRAD>(S, GS, v, ws, w == 0, w == 0 && same_ij && have_v == v);
+      if (v == 0)
+        Ssr = Sv;
+      else
+        Slr = Sv;
+      have_v = v;
+    }
     if (br != 2) {
-      const double Sv = fs3_variant<T, GRAD>(S, GS, br, fdmp, true);
+      const double Sv = br == 0 ? Ssr : Slr;
       energy = fdmp * Sv;
       comc = dfdmp * Sv;
     } else {
-      const double smfun = S.rec.smfun, smfun2 = 1.0 - smfun, cf = S.rec.cf;
-      const double Ssr = fs3_variant<T, GRAD>(S, GS, 0, fdmp * smfun, true);
-      const double Slr = fs3_variant<T, GRAD>(S, GS, 1, fdmp * smfun2, false);
+      const double cf = S.rec.cf;
       energy = fdmp * (smfun * Ssr + smfun2 * Slr);
       comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
     }
