@@ -557,45 +557,35 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
       const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = sp(pidx(s));
       const double(*cv)[3] = S.rec.cv;
       double fx = 0.0, fy = 0.0, fz = 0.0;
+      // the item's two pair families ("links"): family, whether this molecule is the second
+      // of the family's pair (then the weight is G[partner][this] and the pair vector points
+      // from the partner's site), the partner molecule; the virial counts each molecular
+      // pair once (ij and ik from molecule i, jk from molecule j)
+      const int fa = m == 2 ? 1 : 0, fb = m == 0 ? 1 : 2;
+      const bool ta = m != 0, tb = m == 2;
+      const int pa = m == 0 ? 1 : 0, pb = m == 2 ? 1 : 2;
+      const double sga = ta ? -1.0 : 1.0, sgb = tb ? -1.0 : 1.0;
+      const double wva = m == 0 ? 1.0 : 0.0, wvb = m != 2 ? 1.0 : 0.0;
       if (act) {
+        const double x0 = S.site[m][s][0], x1 = S.site[m][s][1], x2 = S.site[m][s][2];
+        const double *ga_row = &S.G[fa][0][0], *gb_row = &S.G[fb][0][0];
+#pragma unroll 1
         for (int o = part; o < kNs3; o += 4) {
           const int po = sp(pidx(o));
-          if (m == 0) {
-            const double g0 = S.G[0][ps][po], g1 = S.G[1][ps][po];
-            const double a0 = cv[0][0] + (S.site[0][s][0] - S.site[1][o][0]);
-            const double a1 = cv[0][1] + (S.site[0][s][1] - S.site[1][o][1]);
-            const double a2 = cv[0][2] + (S.site[0][s][2] - S.site[1][o][2]);
-            const double b0 = cv[1][0] + (S.site[0][s][0] - S.site[2][o][0]);
-            const double b1 = cv[1][1] + (S.site[0][s][1] - S.site[2][o][1]);
-            const double b2 = cv[1][2] + (S.site[0][s][2] - S.site[2][o][2]);
-            fx -= g0 * a0 + g1 * b0;
-            fy -= g0 * a1 + g1 * b1;
-            fz -= g0 * a2 + g1 * b2;
-            vsite += g0 * (a0 * a0 + a1 * a1 + a2 * a2) + g1 * (b0 * b0 + b1 * b1 + b2 * b2);
-          } else if (m == 1) {
-            const double g0 = S.G[0][po][ps], g2 = S.G[2][ps][po];
-            const double a0 = cv[0][0] + (S.site[0][o][0] - S.site[1][s][0]);
-            const double a1 = cv[0][1] + (S.site[0][o][1] - S.site[1][s][1]);
-            const double a2 = cv[0][2] + (S.site[0][o][2] - S.site[1][s][2]);
-            const double c0 = cv[2][0] + (S.site[1][s][0] - S.site[2][o][0]);
-            const double c1 = cv[2][1] + (S.site[1][s][1] - S.site[2][o][1]);
-            const double c2 = cv[2][2] + (S.site[1][s][2] - S.site[2][o][2]);
-            fx -= -g0 * a0 + g2 * c0;
-            fy -= -g0 * a1 + g2 * c1;
-            fz -= -g0 * a2 + g2 * c2;
-            vsite += g2 * (c0 * c0 + c1 * c1 + c2 * c2);
-          } else {
-            const double g1 = S.G[1][po][ps], g2 = S.G[2][po][ps];
-            const double b0 = cv[1][0] + (S.site[0][o][0] - S.site[2][s][0]);
-            const double b1 = cv[1][1] + (S.site[0][o][1] - S.site[2][s][1]);
-            const double b2 = cv[1][2] + (S.site[0][o][2] - S.site[2][s][2]);
-            const double c0 = cv[2][0] + (S.site[1][o][0] - S.site[2][s][0]);
-            const double c1 = cv[2][1] + (S.site[1][o][1] - S.site[2][s][1]);
-            const double c2 = cv[2][2] + (S.site[1][o][2] - S.site[2][s][2]);
-            fx -= -g1 * b0 - g2 * c0;
-            fy -= -g1 * b1 - g2 * c1;
-            fz -= -g1 * b2 - g2 * c2;
-          }
+          const double ga = ga_row[ta ? po * kRS + ps : ps * kRS + po];
+          const double gb = gb_row[tb ? po * kRS + ps : ps * kRS + po];
+          // (this - partner) site offsets, negated for a transposed link: exact
+          const double a0 = cv[fa][0] + sga * (x0 - S.site[pa][o][0]);
+          const double a1 = cv[fa][1] + sga * (x1 - S.site[pa][o][1]);
+          const double a2 = cv[fa][2] + sga * (x2 - S.site[pa][o][2]);
+          const double b0 = cv[fb][0] + sgb * (x0 - S.site[pb][o][0]);
+          const double b1 = cv[fb][1] + sgb * (x1 - S.site[pb][o][1]);
+          const double b2 = cv[fb][2] + sgb * (x2 - S.site[pb][o][2]);
+          const double sa = sga * ga, sb = sgb * gb;
+          fx -= sa * a0 + sb * b0;
+          fy -= sa * a1 + sb * b1;
+          fz -= sa * a2 + sb * b2;
+          vsite += wva * ga * (a0 * a0 + a1 * a1 + a2 * a2) + wvb * gb * (b0 * b0 + b1 * b1 + b2 * b2);
         }
       }
 #pragma unroll
