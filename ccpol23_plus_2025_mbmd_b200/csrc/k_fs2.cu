@@ -195,36 +195,39 @@ __global__ void __launch_bounds__(128, 4)
   __shared__ int kq_all[4][64];
   int *kq = kq_all[threadIdx.x >> 5];
   const unsigned below = (1u << lane) - 1u;
-  int nq = 0;
+  int nq = 0, n0 = 0;
   const int cnt = ncnt[i];
-  for (int n0 = 0; n0 < cnt; n0 += 32) {
-    const int n = n0 + lane;
-    bool pass = false;
-    int k = 0;
-    if (n < cnt) {
-      k = nbr[(size_t)i * cap + n];
-      if (k != j) {
-        const double4 ck = comb[k];
-        const double xki = minimg(xsub(ck.x, ci.x), P.boxb);
-        const double yki = minimg(xsub(ck.y, ci.y), P.boxb);
-        const double zki = minimg(xsub(ck.z, ci.z), P.boxb);
-        const double xkj = xadd(xki, xij), ykj = xadd(yki, yij), zkj = xadd(zki, zij);
-        pass = norm2x(xki, yki, zki) < P.rc2 && norm2x(xkj, ykj, zkj) < P.rc2;
+  for (;;) {
+    // fill the queue to 32 (or to the end of the list), then evaluate up to 32 spectators;
+    // one call site keeps the kernel small
+    while (nq < 32 && n0 < cnt) {
+      const int n = n0 + lane;
+      bool pass = false;
+      int k = 0;
+      if (n < cnt) {
+        k = nbr[(size_t)i * cap + n];
+        if (k != j) {
+          const double4 ck = comb[k];
+          const double xki = minimg(xsub(ck.x, ci.x), P.boxb);
+          const double yki = minimg(xsub(ck.y, ci.y), P.boxb);
+          const double zki = minimg(xsub(ck.z, ci.z), P.boxb);
+          const double xkj = xadd(xki, xij), ykj = xadd(yki, yij), zkj = xadd(zki, zij);
+          pass = norm2x(xki, yki, zki) < P.rc2 && norm2x(xkj, ykj, zkj) < P.rc2;
+        }
       }
+      const unsigned bal = __ballot_sync(0xffffffffu, pass);
+      if (pass) kq[nq + __popc(bal & below)] = k;
+      nq += __popc(bal);
+      n0 += 32;
+      __syncwarp();
     }
-    const unsigned bal = __ballot_sync(0xffffffffu, pass);
-    if (pass) kq[nq + __popc(bal & below)] = k;
-    nq += __popc(bal);
+    if (nq == 0) break;
+    if (lane < nq) spectator(kq[lane]);
     __syncwarp();
-    if (nq >= 32) {
-      spectator(kq[lane]);
-      __syncwarp();
-      if (lane < nq - 32) kq[lane] = kq[32 + lane];
-      nq -= 32;
-      __syncwarp();
-    }
+    if (lane < nq - 32) kq[lane] = kq[32 + lane];
+    nq = nq > 32 ? nq - 32 : 0;
+    __syncwarp();
   }
-  if (lane < nq) spectator(kq[lane]);
   e_loc = warp_sum(e_loc);
   v_loc = warp_sum(v_loc);
   A_loc = warp_sum(A_loc);
