@@ -5,8 +5,8 @@
 //     c(types, ip,jp,kp) * e_ij e_ik e_jk * d_jk^ip d_ik^jp d_ij^kp,
 // e_ab = exp(-b r)/(1 + exp(-g (r - r0))) of the site pair, times the R_avg damping f_dmp
 // and, between 4.5 and 5.5 A, the SR/LR switch.  Every exponential belongs to a site PAIR,
-// so a block first tabulates (e, e d) and (d, d ln e/dr) for the 3 x 289 site pairs of the
-// triple; the energy and the gradient with respect to every site-pair distance,
+// so a block first tabulates e, e d and the force-weight factors for the 3 x 289 site pairs
+// of the triple; the energy and the gradient with respect to every site-pair distance,
 //     G_ab = sum_third e_ij e_ik e_jk (dln e_ab/dr P + dP/dr_ab) / r_ab,
 // then come from three passes (one per pair family) of small matrix products: with sites
 // padded from 17 to 18 (a zero-weight dummy after site 0) the six site-type blocks
@@ -16,6 +16,9 @@
 // for a 2x2 tile of outputs in registers, then contracts M with that type triple's 8
 // coefficients.  Site forces are sums of G_ab times the pair vectors: the reference's
 // per-term force sum regrouped.
+//
+// A block takes a contiguous run of the triple list, one triple at a time (SR, LR or both
+// sweeps), so that consecutive triples of one molecule pair (i, j) reuse its ij tables.
 #include "ccp_device.cuh"
 
 // FS3 blocks resident per SM that the register allocation targets.
