@@ -2,7 +2,8 @@
 FS2 and the reciprocal-space branch run on their own streams and add their forces into a
 separate block; with `overlap` off everything runs in order on one stream.  Also a term mask
 that forks the reciprocal branch without the induction (k-space Ewald + FS3) equals the sum
-of its terms run one at a time."""
+of its terms run one at a time, and FS3 blocks of one triple each (no reuse of a molecule
+pair's tables between triples) give the results of the default runs of several triples."""
 import numpy as np
 import pytest
 
@@ -32,7 +33,7 @@ def _zeros(shape):
     return torch.zeros(shape, dtype=torch.float64, device=torch.device("cuda:0"))
 
 
-def _run(m, b, terms, overlap):
+def _run(m, b, terms, overlap, **opts):
     nm, ld = b.xs.shape
     args = [_dev(a) for a in (b.x, b.y, b.z, b.xs, b.ys, b.zs)]
     f = [_zeros((nm, ld)) for _ in range(3)]
@@ -41,6 +42,8 @@ def _run(m, b, terms, overlap):
     mu = [_zeros((nm, ld)) for _ in range(3)]
     with Context(m, nm, b.box) as c:
         c.set_option("overlap", overlap)
+        for k, v in opts.items():
+            c.set_option(k, v)
         e = c.terms_device(terms, *args, b.box, *f, *c2, *c3, *mu)
     fn = lambda ts: np.stack([t.cpu().numpy() for t in ts])
     return e, fn(f), fn(c2), fn(c3), fn(mu)
@@ -68,3 +71,23 @@ def test_kspace_with_fs3_equals_separate_terms(box):
     assert eb["fs3pe"] == pytest.approx(e3["fs3pe"], rel=1e-12)
     assert rel(fb, fk + f3) <= 1e-12
     assert rel(c3b, c33) <= 1e-12
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fs3_table_reuse_matches_single_triple_blocks(box, precision):
+    m, b = box
+    nm, ld = b.xs.shape
+    out = []
+    for tpb in (8, 1):
+        args = [_dev(a) for a in (b.x, b.y, b.z, b.xs, b.ys, b.zs)]
+        f = [_zeros((nm, ld)) for _ in range(3)]
+        c3 = [_zeros(nm) for _ in range(3)]
+        with Context(m, nm, b.box, precision=precision) as c:
+            c.set_option("fs3_triples_per_block", tpb)
+            e = c.terms_device(_lib.TERM_FS3, *args, b.box, *f, None, None, None, *c3)
+        out.append((e, np.stack([t.cpu().numpy() for t in f]), np.stack([t.cpu().numpy() for t in c3])))
+    (e8, f8, c8), (e1, f1, c1) = out
+    assert e8["fs3pe"] == pytest.approx(e1["fs3pe"], rel=1e-12)
+    assert e8["vir"] == pytest.approx(e1["vir"], rel=1e-12)
+    assert rel(f8, f1) <= 1e-12
+    assert rel(c8, c1) <= 1e-12
