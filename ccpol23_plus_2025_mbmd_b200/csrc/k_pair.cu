@@ -23,20 +23,23 @@ __global__ void k_prep(const double *__restrict__ x, const double *__restrict__ 
                        double *scal, int *icnt) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   int stride = gridDim.x * blockDim.x;
+  // one thread per molecule, per (molecule, active site) and per (molecule, FS site): the
+  // conversions to bohr are divisions, as the reference forms them
   for (int i = t; i < nm; i += stride) {
     com[i] = make_double4(x[i], y[i], z[i], 0.0);
     comb[i] = make_double4(x[i] / kBohr2a, y[i] / kBohr2a, z[i] / kBohr2a, 0.0);
-    for (int a = 0; a < S.na; a++) {
-      size_t o = (size_t)i * ld + S.asite[a];
-      act[(size_t)i * S.na + a] = make_double4(xs[o], ys[o], zs[o], S.q[a]);
-    }
-    for (int s = 0; s < ns3; s++) {
-      size_t o = (size_t)i * ld + s;
-      s17[(size_t)i * kNs3 + s] =
-          make_double4(xs[o] / kBohr2a, ys[o] / kBohr2a, zs[o] / kBohr2a, 0.0);
-    }
     fc2[i] = fc2[nm + i] = fc2[2 * nm + i] = 0.0;
     fc3[i] = fc3[nm + i] = fc3[2 * nm + i] = 0.0;
+  }
+  for (int u = t; u < nm * S.na; u += stride) {
+    const int i = u / S.na, a = u - i * S.na;
+    const size_t o = (size_t)i * ld + S.asite[a];
+    act[u] = make_double4(xs[o], ys[o], zs[o], S.q[a]);
+  }
+  for (int u = t; u < nm * ns3; u += stride) {
+    const int i = u / ns3, s = u - i * ns3;
+    const size_t o = (size_t)i * ld + s;
+    s17[(size_t)i * kNs3 + s] = make_double4(xs[o] / kBohr2a, ys[o] / kBohr2a, zs[o] / kBohr2a, 0.0);
   }
   for (int k = t; k < nf; k += stride) f[k] = 0.0;
   if (t < S_COUNT) scal[t] = 0.0;
