@@ -362,42 +362,49 @@ constexpr double kIndThr = 1.0e-20;  // iteridm convergence threshold on sum |dm
 // Enqueues one Jacobi step: with the phase factors two kernels (k_iter.cu), otherwise T.mu,
 // the tiled dipole structure factors and reciprocal field, the update and the convergence
 // node.  `handle` is used only when use_graph is set.
+IterArgs make_iter_args(ccp_context *c, cudaGraphConditionalHandle handle, int use_graph,
+                        int par) {
+  const SiteSets &S = c->S;
+  IterArgs A{};
+  A.nbr = c->d_nbr;
+  A.ncnt = c->d_ncnt;
+  A.cap = c->cap;
+  A.nw = c->nm * S.np;
+  A.np = S.np;
+  A.T4 = c->d_T4;
+  A.TB = c->d_TB;
+  A.S4 = c->d_S4;
+  A.SB = c->d_SB;
+  A.mu = c->d_mu;
+  A.eim = c->d_eim;
+  A.e0 = c->d_e0tot;
+  A.kv = c->d_kv;
+  A.kg = c->d_kg;
+  A.nk = c->nk;
+  A.mmax = c->kmax[1];
+  A.nmax = c->kmax[2];
+  A.nlm = (c->kmax[0] + 1) * (2 * c->kmax[1] + 1);
+  A.nz = 2 * c->kmax[2] + 1;
+  A.XY = c->d_P;
+  A.Z = c->d_P ? c->d_P + (size_t)A.nw * A.nlm : nullptr;
+  A.sk = c->d_skj;
+  A.par = par;
+  A.scal = c->d_scal;
+  A.state = c->d_istate;
+  A.ticket = c->d_ticket;
+  A.thr = kIndThr;
+  A.maxit = c->maxit;
+  A.use_graph = use_graph;
+  A.handle = handle;
+  A.S = S;
+  return A;
+}
+
 cudaError_t enqueue_dip_step(ccp_context *c, cudaStream_t st, cudaGraphConditionalHandle handle,
                              int use_graph, int par, int *nlaunch) {
   const SiteSets &S = c->S;
   if (c->use_P) {
-    IterArgs A{};
-    A.nbr = c->d_nbr;
-    A.ncnt = c->d_ncnt;
-    A.cap = c->cap;
-    A.nw = c->nm * S.np;
-    A.np = S.np;
-    A.T4 = c->d_T4;
-    A.TB = c->d_TB;
-    A.S4 = c->d_S4;
-    A.SB = c->d_SB;
-    A.mu = c->d_mu;
-    A.eim = c->d_eim;
-    A.e0 = c->d_e0tot;
-    A.kv = c->d_kv;
-    A.kg = c->d_kg;
-    A.nk = c->nk;
-    A.mmax = c->kmax[1];
-    A.nmax = c->kmax[2];
-    A.nlm = (c->kmax[0] + 1) * (2 * c->kmax[1] + 1);
-    A.nz = 2 * c->kmax[2] + 1;
-    A.XY = c->d_P;
-    A.Z = c->d_P + (size_t)A.nw * A.nlm;
-    A.sk = c->d_skj;
-    A.par = par;
-    A.scal = c->d_scal;
-    A.state = c->d_istate;
-    A.ticket = c->d_ticket;
-    A.thr = kIndThr;
-    A.maxit = c->maxit;
-    A.use_graph = use_graph;
-    A.handle = handle;
-    A.S = S;
+    const IterArgs A = make_iter_args(c, handle, use_graph, par);
     *nlaunch = 2;
     cudaError_t e = launch_iter_a(A, st);
     return e == cudaSuccess ? launch_iter_b(A, st) : e;
@@ -441,15 +448,27 @@ int ensure_ind_graph(ccp_context *c) {
   CK(cudaGraphCreate(&c->ind_graph, 0));
   cudaGraphConditionalHandle h;
   CK(cudaGraphConditionalHandleCreate(&h, c->ind_graph, 1, cudaGraphCondAssignDefault));
+  cudaStream_t cs = c->cap_stream;
+  // the first Jacobi step (from mu = 0) is one kernel node ahead of the WHILE node, whose
+  // condition it sets
+  CK(cudaStreamBeginCaptureToGraph(cs, c->ind_graph, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeRelaxed));
+  const cudaError_t ef = launch_dip_first(make_iter_args(c, h, 1, 0), cs);
+  cudaGraph_t captured_first = nullptr;
+  const cudaError_t ef2 = cudaStreamEndCapture(cs, &captured_first);
+  if (!cuda_ok(ef, "capture of the first dipole step")) return CCP_ERR_CUDA;
+  CK(ef2);
+  cudaGraphNode_t first = nullptr;
+  size_t nfirst = 1;
+  CK(cudaGraphGetNodes(c->ind_graph, &first, &nfirst));
   cudaGraphNodeParams np = {};
   np.type = cudaGraphNodeTypeConditional;
   np.conditional.handle = h;
   np.conditional.type = cudaGraphCondTypeWhile;
   np.conditional.size = 1;
   cudaGraphNode_t node;
-  CK(cudaGraphAddNode(&node, c->ind_graph, nullptr, 0, &np));
+  CK(cudaGraphAddNode(&node, c->ind_graph, &first, 1, &np));
   cudaGraph_t body = np.conditional.phGraph_out[0];
-  cudaStream_t cs = c->cap_stream;
   CK(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
   int nl = 0;
   // with the phase tables the body holds kDipUnroll Jacobi steps: a step's update kernel
@@ -470,7 +489,7 @@ int ensure_ind_graph(ccp_context *c) {
 // The whole Jacobi solve from mu = 0.  The state {iterations, change, energy} is copied to
 // h_istate; in the graph form the copy completes at the evaluation's final synchronisation.
 int run_dipole_loop(ccp_context *c, cudaStream_t st) {
-  CK(cudaMemsetAsync(c->d_mu, 0, sizeof(double) * c->nm * c->S.np * 3, st));
+  // the first step writes every dipole, so d_mu needs no clearing
   CK(cudaMemsetAsync(c->d_istate, 0, 4 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_ticket, 0, sizeof(unsigned), st));
@@ -483,14 +502,17 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
     CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     per = c->use_P ? 2 : 5;
   } else {
+    if (!cuda_ok(launch_dip_first(make_iter_args(c, 0, 0, 0), st), "first dipole step"))
+      return CCP_ERR_CUDA;
     for (int step = 0;; step++) {
-      if (!cuda_ok(enqueue_dip_step(c, st, 0, 0, step & 1, &per), "dipole step"))
-        return CCP_ERR_CUDA;
       CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
       const int it = (int)c->h_istate[0];
       if (!(c->h_istate[1] > kIndThr && it < c->maxit)) break;
+      if (!cuda_ok(enqueue_dip_step(c, st, 0, 0, step & 1, &per), "dipole step"))
+        return CCP_ERR_CUDA;
     }
+    if (!per) per = c->use_P ? 2 : 5;
   }
   c->ind_per_iter = per;
   return CCP_OK;
@@ -780,7 +802,7 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     if (mask & T_INDUCTION) {
       o.iters = (int)c->h_istate[0];
       o.ind_e = c->h_istate[2];
-      c->launches += c->ind_per_iter * o.iters;
+      c->launches += 1 + c->ind_per_iter * (o.iters - 1);  // the first step is one kernel
       o.converged = o.iters < c->maxit;
       if (!o.converged) {
         set_error("No convergence in the induced-dipole iteration (maxit reached)");

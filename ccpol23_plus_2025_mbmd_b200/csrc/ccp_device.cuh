@@ -240,6 +240,7 @@ cudaError_t launch_phase_factors(const double2 *tab, int nm, SiteSets S, int kl,
 cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np, const double4 *T4,
                        const double *TB, const double4 *S4, const double *SB, const double *mu,
                        double *eim, cudaStream_t st);
+cudaError_t launch_dip_first(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,

@@ -276,7 +276,56 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The first Jacobi step from mu = 0 (nb_induction_model.f90:1317-1359), where T.mu and the
+// reciprocal field are zero: mu = alpha E0, with the change and energy sums the full step
+// forms, in one block.  It records iteration 1 in the state and, inside the graph, sets the
+// WHILE node's condition, so the loop starts at the second step.
+constexpr int kFirstThreads = 1024;
+__global__ void __launch_bounds__(kFirstThreads) k_dip_first(IterArgs A) {
+  double ch = 0.0, en = 0.0;
+  for (int w = threadIdx.x; w < A.nw; w += kFirstThreads) {
+    const double polr = A.S.apol[w % A.np];
+    double Et[3], E0[3];
+    for (int c = 0; c < 3; c++) {
+      const size_t o = (size_t)w * 3 + c;
+      E0[c] = A.e0[o];
+      Et[c] = (0.0 + 0.0) + E0[c];
+      const double m = polr * Et[c];
+      const double d = 0.0 - m;
+      ch += d * d;
+      A.mu[o] = m;
+    }
+    en += -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
+  }
+  __shared__ double red[2][kFirstThreads / 32];
+  ch = warp_sum(ch);
+  en = warp_sum(en);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = ch;
+    red[1][threadIdx.x >> 5] = en;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double chg = 0.0, ene = 0.0;
+    for (int u = 0; u < kFirstThreads / 32; u++) {
+      chg += red[0][u];
+      ene += red[1][u];
+    }
+    A.state[0] = 1.0;
+    A.state[1] = chg;
+    A.state[2] = ene;
+    const bool more = chg > A.thr && 1 < A.maxit;
+    A.state[3] = more ? 0.0 : 1.0;
+    if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_dip_first(const IterArgs &A, cudaStream_t st) {
+  k_dip_first<<<1, kFirstThreads, 0, st>>>(A);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_phase_factors(const double2 *tab, int nm, SiteSets S, int kl, int km, int kn,
                                  double2 *XY, double2 *Z, cudaStream_t st) {
