@@ -218,19 +218,43 @@ def cpu_baseline(box, cfg, max_seconds=60.0):
     return dt, cores, e, st
 
 
+def _generator_module():
+    """The box generator, loaded from its file without importing the package (whose
+    __init__ loads the library): the reference arm must run the oracle alone."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "_ccp_box_generator", ROOT / "ccpol23_plus_2025_mbmd_b200" / "generator.py")
+    if spec.name in sys.modules:
+        return sys.modules[spec.name]
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[spec.name] = mod  # its dataclass resolves annotations through sys.modules
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def reference_inputs(config=CONFIG, rank=0):
+    """The benchmark box built by the oracle alone (its input readers, principal frame and
+    site placement; the same seeded generator): bit-identical to build_inputs', with nothing
+    of the package imported or loaded.  Returns (oracle module, oracle model, box, config)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    gen = _generator_module()
+    cfg = gen.CONFIGS[config]
+    inp = O.read_inputs(ROOT / "ccpol23_plus_2025_mbmd_b200" / "data" / cfg["variant"])
+    box = gen.water_box(O.SiteFrame(inp), cfg["nm"], cfg["box"], cfg["seed"] + rank)
+    O.build()
+    M = O.make_model(inp, box.nm, box.box)
+    return O, M, box, cfg
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    model, box, cfg = build_inputs(0)
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle as O
-    from ccpol23_plus_2025_mbmd_b200 import data_dir
-    O.build()
+    O, M, box, cfg = reference_inputs()
     cores = os.cpu_count() or 1
     O.set_threads(cores)
-    M = O.make_model(O.read_inputs(data_dir(cfg["variant"])), box.nm, box.box)
-    # no warm-up steps: a CPU step has nothing to warm and each one takes tens of seconds
+    # no warm-up steps: a CPU step has nothing to warm and each one takes seconds
     times = []
     budget = 240.0
     t_start = time.perf_counter()
@@ -251,7 +275,9 @@ def run_reference(args):
                    "box_A": box.box, "variant": cfg["variant"], "seed": cfg["seed"]},
         "cpu_baseline": {"value": val, "unit": "ns/day", "cores": cores, "kind": "port",
                          "sample": f"{len(times)} of {args.steps} requested full hot-path "
-                                   f"evaluations of the 512-water box (time-capped at {budget:.0f} s)"},
+                                   f"evaluations of the 512-water box (time-capped at "
+                                   f"{budget:.0f} s); oracle built with {O.BUILD_FLAGS}, "
+                                   f"{cores} OpenMP threads"},
         "e2e": {"value": val, "unit": "ns/day", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -599,7 +625,8 @@ def main():
         line["cpu_baseline"] = {"value": ns_per_day(1.0 / dt), "unit": "ns/day", "cores": cores,
                                 "kind": "port",
                                 "sample": "1 full hot-path evaluation of the same 512-water box "
-                                          f"({dt:.1f} s on {cores} threads)"}
+                                          f"({dt:.1f} s on {cores} threads; oracle built with "
+                                          "gcc -O3 -fopenmp -ffp-contract=off)"}
         Fo = np.stack([st.fxs, st.fys, st.fzs])
         line["parity_vs_oracle"] = {
             "fp64_rel_force_err": float(np.linalg.norm(f64["forces"] - Fo) / np.linalg.norm(Fo)),

@@ -151,5 +151,7 @@ def ptr(a) -> int | None:
     """Address of a C-contiguous float64 numpy array (None passes NULL)."""
     if a is None:
         return None
-    assert isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous):
+        raise ValueError("expected a C-contiguous float64 numpy array, got "
+                         f"{type(a).__name__} {getattr(a, 'dtype', '')}")
     return a.ctypes.data

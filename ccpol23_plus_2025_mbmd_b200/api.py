@@ -30,6 +30,43 @@ def data_dir(variant: str) -> Path:
 NPHASE = 10  # CCP_NPHASE
 
 
+def _device_array(t, shape, name, device=None):
+    """Checks that ``t`` is a contiguous float64 CUDA tensor of ``shape`` on ``device`` (an
+    ordinal; None = the current device) and returns its device address.  The library reads and writes these buffers
+    through raw pointers, so a wrong dtype, stride, size or device would make its kernels
+    read or write outside them; every such case is refused here instead."""
+    import torch
+    if not isinstance(t, torch.Tensor):
+        raise ValueError(f"{name}: expected a torch tensor, got {type(t).__name__}")
+    if not t.is_cuda:
+        raise ValueError(f"{name}: expected a CUDA tensor, got one on {t.device}")
+    if t.dtype != torch.float64:
+        raise ValueError(f"{name}: expected float64, got {t.dtype}")
+    if device is None:
+        device = torch.cuda.current_device()
+    if t.device.index != device:
+        raise ValueError(f"{name}: on cuda:{t.device.index}, expected cuda:{device}")
+    if tuple(t.shape) != tuple(shape):
+        raise ValueError(f"{name}: shape {tuple(t.shape)}, expected {tuple(shape)}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name}: must be contiguous")
+    return t.data_ptr()
+
+
+def _optional_device_array(t, shape, name, device):
+    return None if t is None else _device_array(t, shape, name, device)
+
+
+def _site_layout(xs, ns, name="xs"):
+    """(nm, ld) of a site array, with ld >= the model's sites per molecule."""
+    if len(xs.shape) != 2:
+        raise ValueError(f"{name}: expected (nm, ld), got shape {tuple(xs.shape)}")
+    nm, ld = int(xs.shape[0]), int(xs.shape[1])
+    if ld < ns:
+        raise ValueError(f"{name}: ld = {ld} is below the model's {ns} sites per molecule")
+    return nm, ld
+
+
 class Model:
     """Parameters read from CONTROL, FIELD, data3b_full, data3b_full_LR_4p5."""
 
@@ -137,15 +174,21 @@ def ewald_setup(ewps: float, rcut: float, box: float):
 def kspace_ewald_fixed(model: Model, x, y, z, xs, ys, zs, lmax, mmax, nmax, alp, box, qkcpe,
                        fxs, fys, fzs, vir, stream: int | None = None) -> None:
     """kspace_ewald (ewald.f90:754-1173) on device arrays with the library's fixed scratch:
-    no device memory is allocated.  All arrays are torch CUDA float64 tensors on the current
-    device; qkcpe and vir are one-element tensors.  Forces and vir are added to, qkcpe is
-    overwritten.  The work is enqueued on `stream` (a cudaStream_t address, None = the legacy
-    default stream) and is not waited for."""
-    nm, ld = xs.shape
+    no device memory is allocated.  All arrays are contiguous torch CUDA float64 tensors on
+    the current device: x, y, z (nm,), xs, ys, zs and the forces (nm, ld); qkcpe and vir
+    have one element each.  Forces and vir are added to, qkcpe is overwritten.  The work is
+    enqueued on `stream` (a cudaStream_t address, None = the legacy default stream) and is
+    not waited for.  Arguments that do not match raise ValueError before the library is
+    called."""
+    dev = None  # the current device
+    nm, ld = _site_layout(xs, model.ns)
+    a = [_device_array(t, (nm,), n, dev) for t, n in ((x, "x"), (y, "y"), (z, "z"))]
+    a += [_device_array(t, (nm, ld), n, dev) for t, n in ((xs, "xs"), (ys, "ys"), (zs, "zs"))]
+    q = _device_array(qkcpe, (1,), "qkcpe", dev)
+    f = [_device_array(t, (nm, ld), n, dev) for t, n in ((fxs, "fxs"), (fys, "fys"), (fzs, "fzs"))]
+    v = _device_array(vir, (1,), "vir", dev)
     check(_lib.lib().ccp_kspace_ewald_fixed(
-        model.handle, nm, x.data_ptr(), y.data_ptr(), z.data_ptr(), xs.data_ptr(),
-        ys.data_ptr(), zs.data_ptr(), ld, lmax, mmax, nmax, alp, box, qkcpe.data_ptr(),
-        fxs.data_ptr(), fys.data_ptr(), fzs.data_ptr(), vir.data_ptr(), stream))
+        model.handle, nm, *a, ld, lmax, mmax, nmax, alp, box, q, *f, v, stream))
 
 
 @dataclass
@@ -180,7 +223,9 @@ class Context:
         self._h = h
         self.model = model
         self.nm = nm
+        self.device = device
         self.precision = precision
+        self.stream = None  # cudaStream_t address set by set_stream (None: the context's own)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -207,7 +252,25 @@ class Context:
         check(_lib.lib().ccp_context_set_maxit(self._h, maxit))
 
     def set_stream(self, stream_ptr: int | None):
+        """Enqueue the context's work on a caller's CUDA stream (a cudaStream_t address, e.g.
+        ``torch.cuda.current_stream().cuda_stream``); None returns to the context's own."""
         check(_lib.lib().ccp_context_set_stream(self._h, stream_ptr))
+        self.stream = stream_ptr
+
+    def _device_args(self, x, y, z, xs, ys, zs, outs):
+        """Validated device addresses of the inputs and of the optional outputs (site arrays
+        (nm, ld), COM-force arrays (nm,), dipoles (nm, ld), in that order of ``outs``)."""
+        nm, ld = _site_layout(xs, self.model.ns)
+        if nm != self.nm:
+            raise ValueError(f"xs: {nm} molecules, the context holds {self.nm}")
+        d = self.device
+        a = [_device_array(t, (nm,), n, d) for t, n in ((x, "x"), (y, "y"), (z, "z"))]
+        a += [_device_array(t, (nm, ld), n, d) for t, n in ((xs, "xs"), (ys, "ys"), (zs, "zs"))]
+        shapes = [(nm, ld)] * 3 + [(nm,)] * 6 + [(nm, ld)] * 3
+        names = ["fxs", "fys", "fzs", "fxfs2", "fyfs2", "fzfs2", "fxfs3", "fyfs3", "fzfs3",
+                 "idmx", "idmy", "idmz"]
+        o = [_optional_device_array(t, sh, n, d) for t, sh, n in zip(outs, shapes, names)]
+        return a, ld, o
 
     def set_option(self, name: str, value: int):
         """Execution options of the dipole solve: "graph_loop", "phase_matrix" (0/1)."""
@@ -307,16 +370,13 @@ class Context:
     def terms_device(self, terms, x, y, z, xs, ys, zs, box, fxs=None, fys=None, fzs=None,
                      fxfs2=None, fyfs2=None, fzfs2=None, fxfs3=None, fyfs3=None, fzfs3=None,
                      idmx=None, idmy=None, idmz=None) -> dict:
-        """The terms selected by the bit mask `terms` (_lib.TERM_*) on torch CUDA float64
-        tensors, in the layouts of hot_path_device; energies of terms not run are 0."""
-        def dp(t):
-            return None if t is None else t.data_ptr()
-        ld = xs.shape[1]
+        """The terms selected by the bit mask `terms` (_lib.TERM_*) on contiguous torch CUDA
+        float64 tensors on the context's device, in the layouts of hot_path_device; energies
+        of terms not run are 0.  Mismatched arrays raise ValueError."""
+        a, ld, o = self._device_args(x, y, z, xs, ys, zs, (fxs, fys, fzs, fxfs2, fyfs2, fzfs2,
+                                                           fxfs3, fyfs3, fzfs3, idmx, idmy, idmz))
         e = CcpEnergies()
-        check(_lib.lib().ccp_terms_device(
-            self._h, int(terms), dp(x), dp(y), dp(z), dp(xs), dp(ys), dp(zs), ld, box, C.byref(e),
-            dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
-            dp(fzfs3), dp(idmx), dp(idmy), dp(idmz)))
+        check(_lib.lib().ccp_terms_device(self._h, int(terms), *a, ld, box, C.byref(e), *o))
         return _energies(e)
 
     # -- NVE molecular dynamics (device-resident state) -------------------------------
@@ -401,15 +461,12 @@ class Context:
     def hot_path_device(self, x, y, z, xs, ys, zs, box, fxs=None, fys=None, fzs=None,
                         fxfs2=None, fyfs2=None, fzfs2=None, fxfs3=None, fyfs3=None,
                         fzfs3=None, idmx=None, idmy=None, idmz=None) -> dict:
-        """All arrays are torch CUDA float64 tensors (or None); nothing crosses PCIe."""
-        def dp(t):
-            return None if t is None else t.data_ptr()
-        ld = xs.shape[1]
+        """All arrays are contiguous torch CUDA float64 tensors on the context's device (or
+        None); nothing crosses PCIe.  Mismatched arrays raise ValueError."""
+        a, ld, o = self._device_args(x, y, z, xs, ys, zs, (fxs, fys, fzs, fxfs2, fyfs2, fzfs2,
+                                                           fxfs3, fyfs3, fzfs3, idmx, idmy, idmz))
         e = CcpEnergies()
-        check(_lib.lib().ccp_hot_path_device(
-            self._h, dp(x), dp(y), dp(z), dp(xs), dp(ys), dp(zs), ld, box, C.byref(e),
-            dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
-            dp(fzfs3), dp(idmx), dp(idmy), dp(idmz)))
+        check(_lib.lib().ccp_hot_path_device(self._h, *a, ld, box, C.byref(e), *o))
         return _energies(e)
 
 
@@ -428,6 +485,7 @@ class Batch:
         self.model = model
         self.nm = nm
         self.slots = slots
+        self.device = device
         self.precision = precision
 
     def close(self):
@@ -474,16 +532,31 @@ class Batch:
         sequence of nframes box lengths; ``pgrad`` an optional (nframes, 2 nclass + 1734)
         float64 numpy array for the per-frame FS3 parameter gradients.  Returns the
         per-frame energy dicts."""
-        def dp(t):
-            return None if t is None else t.data_ptr()
-        nf = x.shape[0]
-        ld = xs.shape[2]
+        nf = int(x.shape[0]) if len(x.shape) == 2 else -1
+        if nf < 1 or len(xs.shape) != 3:
+            raise ValueError(f"x: expected (nframes, nm), xs: (nframes, nm, ld); got "
+                             f"{tuple(x.shape)} and {tuple(xs.shape)}")
+        nm, ld = _site_layout(xs[0], self.model.ns)
+        if nm != self.nm:
+            raise ValueError(f"xs: {nm} molecules per frame, the batch holds {self.nm}")
+        d = self.device
+        a = [_device_array(t, (nf, nm), n, d) for t, n in ((x, "x"), (y, "y"), (z, "z"))]
+        a += [_device_array(t, (nf, nm, ld), n, d) for t, n in ((xs, "xs"), (ys, "ys"),
+                                                                 (zs, "zs"))]
+        shapes = [(nf, nm, ld)] * 3 + [(nf, nm)] * 6 + [(nf, nm, ld)] * 3
+        names = ["fxs", "fys", "fzs", "fxfs2", "fyfs2", "fzfs2", "fxfs3", "fyfs3", "fzfs3",
+                 "idmx", "idmy", "idmz"]
+        outs = (fxs, fys, fzs, fxfs2, fyfs2, fzfs2, fxfs3, fyfs3, fzfs3, idmx, idmy, idmz)
+        o = [_optional_device_array(t, sh, n, d) for t, sh, n in zip(outs, shapes, names)]
         boxes = np.ascontiguousarray(np.broadcast_to(np.asarray(box, dtype=np.float64), (nf,)))
         e = (CcpEnergies * max(nf, 1))()
-        plen = 0 if pgrad is None else pgrad.shape[1]
+        plen = 0
+        if pgrad is not None:
+            if pgrad.dtype != np.float64 or pgrad.ndim != 2 or pgrad.shape[0] != nf or \
+                    not pgrad.flags.c_contiguous:
+                raise ValueError("pgrad: expected a C-contiguous float64 (nframes, n) array")
+            plen = pgrad.shape[1]
         check(_lib.lib().ccp_batch_terms_device(
-            self._h, int(terms), nf, ptr(boxes), dp(x), dp(y), dp(z), dp(xs), dp(ys), dp(zs), ld,
-            e, dp(fxs), dp(fys), dp(fzs), dp(fxfs2), dp(fyfs2), dp(fzfs2), dp(fxfs3), dp(fyfs3),
-            dp(fzfs3), dp(idmx), dp(idmy), dp(idmz), ptr(pgrad), plen))
+            self._h, int(terms), nf, ptr(boxes), *a, ld, e, *o, ptr(pgrad), plen))
         return [_energies(e[f]) for f in range(nf)]
 

@@ -32,6 +32,7 @@ import torch
 from . import _lib
 
 KCAL = 418.4  # internal force unit (10 J/mol/A) per kcal/mol/A
+CUDA_STREAM_LEGACY = 1  # cudaStreamLegacy: the legacy default stream, named explicitly
 
 
 class _ThreeBodyInduction(torch.autograd.Function):
@@ -52,7 +53,17 @@ class _ThreeBodyInduction(torch.autograd.Function):
         c2 = [torch.zeros(nm, dtype=torch.float64, device=dev) for _ in range(3)]
         c3 = [torch.zeros(nm, dtype=torch.float64, device=dev) for _ in range(3)]
         terms = _lib.TERM_INDUCTION | _lib.TERM_FS2 | _lib.TERM_FS3
-        e = context.terms_device(terms, x, y, z, xs, ys, zs, box, *f, *c2, *c3)
+        # The input copies and the zero-filled outputs above are queued on torch's current
+        # stream; the evaluation runs on the context's stream.  Queue it on torch's stream for
+        # this call so that it starts after them (the call returns once it has finished).
+        # torch's default stream has the handle 0, which the library reads as "the context's
+        # own stream"; cudaStreamLegacy (1) names that default stream explicitly.
+        prev = context.stream
+        context.set_stream(torch.cuda.current_stream(dev).cuda_stream or CUDA_STREAM_LEGACY)
+        try:
+            e = context.terms_device(terms, x, y, z, xs, ys, zs, box, *f, *c2, *c3)
+        finally:
+            context.set_stream(prev)
         energy = e["fs2pe"] + e["fs3pe"] + e["indpe"]
         F = torch.stack(f, dim=-1)                                     # (nm, ns, 3)
         Fc = torch.stack([c2[a] + c3[a] for a in range(3)], dim=-1)    # (nm, 3)
@@ -94,6 +105,10 @@ class _ThreeBodyInductionBatch(torch.autograd.Function):
         ncoef = cur[0].size
         pg = np.zeros((nf, 2 * ncoef + 2 * 3 * 289)) if want_p else None
         terms = _lib.TERM_INDUCTION | _lib.TERM_FS2 | _lib.TERM_FS3
+        # Every slot of the batch runs on its own streams, which do not wait for torch's
+        # stream: finish the input copies and the zero fills queued above first (the call
+        # returns once every frame has finished).
+        torch.cuda.current_stream(dev).synchronize()
         es = batch.terms_device(terms, box, x, y, z, xs, ys, zs, *f, *c2, *c3, pgrad=pg)
         energy = [e["fs2pe"] + e["fs3pe"] + e["indpe"] for e in es]
         F = torch.stack(f, dim=-1)                                     # (nf, nm, ns, 3)

@@ -189,8 +189,15 @@ extern "C" int ccp_kspace_ewald_fixed(const ccp_model *m, int nm, const double *
                                       " k-vectors; the fixed scratch holds " +
                                       std::to_string(kFixedScratchBytes) + " bytes");
 
+  // The launch checks below read the thread's last CUDA error.  An error that earlier work of
+  // the caller left pending would be reported as this call's own, so such a call is refused
+  // before anything is launched, and the pending error is left in place for its owner.
+  cudaError_t e = cudaPeekAtLastError();
+  if (e != cudaSuccess)
+    return fail(CCP_ERR_CUDA, std::string("a CUDA error from earlier work is pending (nothing "
+                                          "launched): ") + cudaGetErrorString(e));
   int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(CCP_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fail(CCP_ERR_BAD_INPUT, "device ordinal above 63");
   unsigned char *base;

@@ -9,6 +9,11 @@ oxygen-oxygen distance below 2.5 A under the minimum image (offending molecules 
 redrawn).  COM velocities are Maxwell-Boltzmann at the target temperature with the drift
 removed; body-frame angular momenta are Gaussian with variance k_B T I_a.  COMs are wrapped
 into [-L/2, L/2) as the reference does when it reads a REVCON (initialization.f90:71-75).
+
+The module imports nothing from the package at load time: ``water_box`` needs from its
+``model`` only ``pcoord``, ``pmi``, ``get_double("totm")`` and ``sites(q, ld)``, which the
+library's Model and the oracle's SiteFrame both provide, so the CPU reference timing builds
+the same box without loading the library.
 """
 from __future__ import annotations
 
@@ -80,7 +85,6 @@ def water_box(model, nm: int, box: float, seed: int, *, ld: int | None = None,
     com = np.empty((nm, 3))
     q = np.empty((nm, 4))
     oxy = np.empty((nm, 3))
-    from .api import Model  # noqa: F401  (model is an api.Model)
 
     def rot(qq):
         q0, q1, q2, q3 = qq

@@ -100,7 +100,10 @@ int ccp_context_destroy(ccp_context *ctx);
 int ccp_context_set_ewald(ccp_context *ctx, double alpha, int k1, int k2, int k3);
 /* Cap on dipole iterations (reference: maxit = 500, nb_induction_model.f90:1221). */
 int ccp_context_set_maxit(ccp_context *ctx, int maxit);
-/* Run subsequent device work on this cudaStream_t (NULL = the context's own stream). */
+/* Run subsequent device work on this cudaStream_t (NULL = the context's own stream; the
+   legacy default stream is named by cudaStreamLegacy).  An evaluation then starts after the
+   work already queued on that stream, which is how a caller orders it after its own input
+   copies. */
 int ccp_context_set_stream(ccp_context *ctx, void *stream);
 
 /* ------------------------------------------- reference entry points (host buffers) */
@@ -184,12 +187,24 @@ int ccp_hot_path_device(ccp_context *ctx, const double *x_device, const double *
    - Work is enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream) and the
      call returns without synchronising; results are ready when the stream reaches them.
    - The first call on each device looks the scratch array up (cudaGetSymbolAddress, which
-     also loads the module); a caller that captures streams makes one call before capturing.
+     also loads the module) and keeps its address for the life of the process; a caller
+     that captures streams makes one call before capturing.  The kept address belongs to the
+     device's primary context (the one the CUDA runtime API uses): calls from a different
+     driver context, or after cudaDeviceReset, are not supported.
    - The scratch is shared by all calls on a device: calls whose execution overlaps (other
      streams, other host threads) race on it and give wrong results.  Order them on one
      stream or with events.
    - Allocates no device memory and, on success, no host memory.  The library clears what it
-     accumulates into (forces of its own, energy sums) inside the launch sequence. */
+     accumulates into (forces of its own, energy sums) inside the launch sequence.
+   Refusals, all returned before anything is launched:
+   - CCP_ERR_BAD_INPUT: a NULL pointer; nm < 1; ld below the model's sites per molecule;
+     lmax, mmax or nmax below 1; box or alp not positive; a model with no charged sites or
+     with more charged sites per molecule than the library's compact site set holds (8);
+     a device ordinal above 63;
+   - CCP_ERR_CAPACITY: lmax, mmax or nmax above 64, or scratch needs above 16 MiB (the byte
+     count is in ccp_last_error());
+   - CCP_ERR_CUDA: a CUDA error of earlier work still pending on the calling thread (it is
+     left pending), or cudaGetDevice / cudaGetSymbolAddress failing. */
 #define CCP_KSPACE_FIXED_SCRATCH_BYTES (16u << 20)
 int ccp_kspace_ewald_fixed(const ccp_model *m, int nm, const double *x_device,
                            const double *y_device, const double *z_device,

@@ -58,6 +58,9 @@ class OrcModel(C.Structure):
 
 _lib = None
 
+# The compiler flags of the Makefile's build, reported beside every CPU timing of the oracle.
+BUILD_FLAGS = "gcc -O3 -fopenmp -ffp-contract=off"
+
 
 def build():
     """Compile the oracle with its Makefile (gcc)."""
@@ -307,12 +310,32 @@ def principal_frame(inp: Inputs):
     return pc, pmi, totm
 
 
+class SiteFrame:
+    """The molecular frame of the inputs (principal axes, moments, mass) with the site
+    placement of molecular_sites.f90:14-47: what the box generator needs from a model, here
+    computed by the oracle alone."""
+
+    def __init__(self, inp: Inputs):
+        self.pcoord, self.pmi, self.totm = principal_frame(inp)
+        self.ns = inp.ns
+
+    def get_double(self, name):
+        if name != "totm":
+            raise KeyError(name)
+        return self.totm
+
+    def sites(self, q, ld=None):
+        return sites(self.pcoord, q, ld)
+
+
 def quat_to_rot(q0, q1, q2, q3):
-    """molecular_sites.f90:93-111 (row-major 3x3 flattened as rott(1..9))."""
+    """molecular_sites.f90:93-111 (row-major 3x3 flattened as rott(1..9)).  Fortran's
+    integer power q0**2 is the product q0*q0 (numpy's float power can differ by an ulp)."""
+    a0, a1, a2, a3 = q0 * q0, q1 * q1, q2 * q2, q3 * q3
     return np.array([
-        q0 ** 2 + q1 ** 2 - q2 ** 2 - q3 ** 2, 2.0 * (q1 * q2 - q0 * q3), 2.0 * (q1 * q3 + q0 * q2),
-        2.0 * (q1 * q2 + q0 * q3), q0 ** 2 - q1 ** 2 + q2 ** 2 - q3 ** 2, 2.0 * (q2 * q3 - q0 * q1),
-        2.0 * (q1 * q3 - q0 * q2), 2.0 * (q2 * q3 + q0 * q1), q0 ** 2 - q1 ** 2 - q2 ** 2 + q3 ** 2])
+        a0 + a1 - a2 - a3, 2.0 * (q1 * q2 - q0 * q3), 2.0 * (q1 * q3 + q0 * q2),
+        2.0 * (q1 * q2 + q0 * q3), a0 - a1 + a2 - a3, 2.0 * (q2 * q3 - q0 * q1),
+        2.0 * (q1 * q3 - q0 * q2), 2.0 * (q2 * q3 + q0 * q1), a0 - a1 - a2 + a3])
 
 
 def sites(pcoord: np.ndarray, q: np.ndarray, ld: int | None = None):

@@ -1,0 +1,202 @@
+"""Oracle parity at the benchmark configurations themselves.
+
+- 512 waters FS2+FS3 (L = 24.84 A, seed 2002; the box of the headline measurement): the FP64
+  form against the oracle's full hot path at 1e-10 -- all six energies, the virial, site
+  forces, both COM force sets, induced dipoles -- and the same Jacobi iteration count; the
+  mixed form against the same oracle within its force bar.
+- One 256-water FS3 frame (L = 19.71 A, seed 4004; a frame of the 32-frame batch): the
+  autograd position gradient against the oracle's forces at 1e-10, central finite differences
+  of positions (h = 1e-5 A) and of FS3 parameters (relative step 1e-6).
+- 2048 waters FS2+FS3 (L = 39.40 A, seed 5005): the mixed form against the FP64 form, site
+  forces, per-molecule forces and torques within 1e-5 (the oracle takes minutes there).
+"""
+import numpy as np
+import pytest
+
+from ccpol23_plus_2025_mbmd_b200 import Context, Model, data_dir
+from ccpol23_plus_2025_mbmd_b200.generator import CONFIGS, water_box
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10          # FP64 form vs oracle
+MIXED_FTOL = 1e-5    # mixed form: site forces, per-molecule forces, torques
+KCAL = 418.4
+ENERGIES = ("scpe", "rcpe", "kcpe", "indpe", "fs2pe", "fs3pe")
+
+
+def _box(name):
+    cfg = CONFIGS[name]
+    m = Model(data_dir(cfg["variant"]))
+    return m, water_box(m, cfg["nm"], cfg["box"], cfg["seed"]), cfg
+
+
+def _mol_force_torque(b, F, c2, c3):
+    """Per-molecule forces (site forces summed plus the three-body COM forces) and torques
+    about the centre of mass."""
+    tot = F.sum(2) + c2 + c3
+    tq = np.stack([(b.ys * F[2] - b.zs * F[1]).sum(1), (b.zs * F[0] - b.xs * F[2]).sum(1),
+                   (b.xs * F[1] - b.ys * F[0]).sum(1)])
+    return tot, tq
+
+
+@pytest.fixture(scope="module")
+def c2_512(product, oracle):
+    m, b, cfg = _box("c2_512")
+    M = oracle.make_model(oracle.read_inputs(data_dir(cfg["variant"])), b.nm, b.box)
+    eo, st = oracle.hot_path(M, b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    assert eo["ind_status"] == 0
+    return m, b, eo, st
+
+
+def test_512_fp64_hot_path_matches_oracle(c2_512):
+    m, b, eo, st = c2_512
+    with Context(m, b.nm, b.box, precision="fp64") as c:
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    e = r.energies
+    for k in ENERGIES:
+        assert abs(e[k] - eo[k]) <= TOL * abs(eo[k]), (k, e[k], eo[k])
+    assert abs(e["vir"] - eo["vir"]) <= TOL * abs(eo["vir"]), (e["vir"], eo["vir"])
+    assert e["ind_iters"] == eo["ind_iters"] == 28
+    assert rel(np.stack([r.fxs, r.fys, r.fzs]), np.stack([st.fxs, st.fys, st.fzs])) <= TOL
+    assert rel(np.stack([r.fxfs2, r.fyfs2, r.fzfs2]),
+               np.stack([st.fxfs2, st.fyfs2, st.fzfs2])) <= TOL
+    assert rel(np.stack([r.fxfs3, r.fyfs3, r.fzfs3]),
+               np.stack([st.fxfs3, st.fyfs3, st.fzfs3])) <= TOL
+    assert rel(np.stack([r.idmx, r.idmy, r.idmz]), np.stack([st.idmx, st.idmy, st.idmz])) <= TOL
+
+
+def test_512_mixed_hot_path_against_oracle(c2_512):
+    m, b, eo, st = c2_512
+    with Context(m, b.nm, b.box, precision="mixed") as c:
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    F = np.stack([r.fxs, r.fys, r.fzs])
+    Fo = np.stack([st.fxs, st.fys, st.fzs])
+    T, Q = _mol_force_torque(b, F, np.stack([r.fxfs2, r.fyfs2, r.fzfs2]),
+                             np.stack([r.fxfs3, r.fyfs3, r.fzfs3]))
+    To, Qo = _mol_force_torque(b, Fo, np.stack([st.fxfs2, st.fyfs2, st.fzfs2]),
+                               np.stack([st.fxfs3, st.fyfs3, st.fzfs3]))
+    assert rel(F, Fo) <= MIXED_FTOL, rel(F, Fo)
+    assert rel(T, To) <= MIXED_FTOL, rel(T, To)
+    assert rel(Q, Qo) <= MIXED_FTOL, rel(Q, Qo)
+    e = r.energies
+    for k in ENERGIES:
+        assert abs(e[k] - eo[k]) <= 1e-6 * abs(eo[k]), (k, e[k], eo[k])
+
+
+@pytest.fixture(scope="module")
+def c4_frame(product):
+    import torch
+    from ccpol23_plus_2025_mbmd_b200.autograd import fs3_param_tensors
+    m, b, cfg = _box("c4_256")
+    dev = torch.device("cuda:0")
+    com = torch.tensor(np.stack([b.x, b.y, b.z], axis=1), dtype=torch.float64, device=dev)
+    sites = torch.tensor(np.stack([b.xs, b.ys, b.zs], axis=2), dtype=torch.float64, device=dev)
+    ctx = Context(m, b.nm, b.box)
+    params = fs3_param_tensors(ctx, dev)
+    yield m, b, cfg, ctx, com, sites, params
+    ctx.close()
+
+
+def _energy(ctx, b, com, sites, params):
+    from ccpol23_plus_2025_mbmd_b200.autograd import three_body_induction_energy
+    return three_body_induction_energy(ctx, b.box, com, sites, *params)
+
+
+def test_256_frame_gradient_matches_oracle_forces(c4_frame, oracle):
+    m, b, cfg, ctx, com, sites, params = c4_frame
+    c = com.clone().requires_grad_(True)
+    s = sites.clone().requires_grad_(True)
+    E = _energy(ctx, b, c, s, [p.detach() for p in params])
+    E.backward()
+    O = oracle
+    M = O.make_model(O.read_inputs(data_dir(cfg["variant"])), b.nm, b.box)
+    st = O.State(b.nm, b.xs.shape[1])
+    args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
+    e2, e3 = O.threebody_term(M, *args, b.box, st)
+    ei, status, _ = O.nb_induction(M, *args, b.box, st)
+    assert status == 0
+    assert abs(E.item() - (e2 + e3 + ei)) <= TOL * abs(e2 + e3 + ei)
+    F = np.stack([st.fxs, st.fys, st.fzs], axis=2)
+    Fc = np.stack([st.fxfs2 + st.fxfs3, st.fyfs2 + st.fyfs3, st.fzfs2 + st.fzfs3], axis=1)
+    assert rel(s.grad.cpu().numpy(), -F / KCAL) <= TOL
+    assert rel(c.grad.cpu().numpy(), -(F.sum(axis=1) + Fc) / KCAL) <= TOL
+
+
+def test_256_frame_gradient_finite_differences(c4_frame):
+    """Central differences with h = 1e-5 A of molecular centres and of site groups (sites
+    that coincide move together), against the analytic gradient."""
+    m, b, cfg, ctx, com, sites, params = c4_frame
+    fixed = [p.detach() for p in params]
+    c = com.clone().requires_grad_(True)
+    s = sites.clone().requires_grad_(True)
+    _energy(ctx, b, c, s, fixed).backward()
+    gc, gs = c.grad.cpu().numpy(), s.grad.cpu().numpy()
+    h = 1e-5
+    rng = np.random.default_rng(11)
+    off = np.stack([b.xs[0], b.ys[0], b.zs[0]], axis=1)
+    same = np.all(np.abs(off[:, None, :] - off[None, :, :]) == 0.0, axis=2)
+    scale = max(np.abs(gc).max(), np.abs(gs).max())
+    for _ in range(6):
+        i, a = rng.integers(b.nm), rng.integers(3)
+        cp, cm = com.clone(), com.clone()
+        cp[i, a] += h
+        cm[i, a] -= h
+        fd = (_energy(ctx, b, cp, sites, fixed).item() -
+              _energy(ctx, b, cm, sites, fixed).item()) / (2 * h)
+        assert abs(fd - gc[i, a]) <= 1e-6 * scale, ("com", i, a, fd, gc[i, a])
+        k = rng.integers(sites.shape[1])
+        group = [q for q in range(sites.shape[1]) if same[k, q]]
+        sp_, sm_ = sites.clone(), sites.clone()
+        for q in group:
+            sp_[i, q, a] += h
+            sm_[i, q, a] -= h
+        fd = (_energy(ctx, b, com, sp_, fixed).item() -
+              _energy(ctx, b, com, sm_, fixed).item()) / (2 * h)
+        an = sum(gs[i, q, a] for q in group)
+        assert abs(fd - an) <= 1e-6 * scale, ("site", i, group, a, fd, an)
+
+
+def test_256_frame_parameter_gradient_finite_differences(c4_frame):
+    """The largest gradients of each FS3 parameter set against central differences with a
+    relative step of 1e-6."""
+    m, b, cfg, ctx, com, sites, params = c4_frame
+    p = [q.detach().clone().requires_grad_(True) for q in params]
+    _energy(ctx, b, com, sites, p).backward()
+    grads = [q.grad.cpu().numpy().reshape(-1) for q in p]
+    base = [q.detach().cpu().numpy().reshape(-1) for q in p]
+    checked = 0
+    for w in range(4):
+        for k in np.argsort(-np.abs(grads[w]))[:3]:
+            if grads[w][k] == 0.0:
+                continue
+            step = 1e-6 * max(abs(base[w][k]), 1e-3)
+            vals = []
+            for sgn in (1.0, -1.0):
+                q = [t.detach().clone() for t in p]
+                q[w].view(-1)[k] += sgn * step
+                vals.append(_energy(ctx, b, com, sites, q).item())
+            fd = (vals[0] - vals[1]) / (2 * step)
+            assert abs(fd - grads[w][k]) <= 1e-5 * abs(grads[w][k]), (w, k, fd, grads[w][k])
+            checked += 1
+    assert checked >= 9
+    _energy(ctx, b, com, sites, [q.detach() for q in params])  # restore the fit
+
+
+def test_2048_mixed_form_within_force_bar(product):
+    m, b, cfg = _box("c5_2048")
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with Context(m, b.nm, b.box, precision=prec) as c:
+            out[prec] = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+
+    def parts(r):
+        F = np.stack([r.fxs, r.fys, r.fzs])
+        T, Q = _mol_force_torque(b, F, np.stack([r.fxfs2, r.fyfs2, r.fzfs2]),
+                                 np.stack([r.fxfs3, r.fyfs3, r.fzfs3]))
+        return F, T, Q
+
+    for name, a, ref in zip(("site force", "molecule force", "torque"), parts(out["mixed"]),
+                            parts(out["fp64"])):
+        assert rel(a, ref) <= MIXED_FTOL, (name, rel(a, ref))

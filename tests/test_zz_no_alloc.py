@@ -45,15 +45,17 @@ def test_fixed_scratch_matches_context(product, variant, nm, L, seed, ld):
 
 
 def test_fixed_scratch_rejects_oversize(product):
-    """A box whose tables exceed the fixed scratch is refused before anything is launched
-    (the stride-0 views only carry the shape; no element is read)."""
+    """A box whose tables exceed the fixed scratch is refused by the C entry point before
+    anything is launched: the buffers passed are real but far smaller than the molecule
+    count claims, which is safe only because nothing reads them."""
     import torch
+    from ccpol23_plus_2025_mbmd_b200 import _lib
     m = Model(data_dir("fs3"))
-    cell = torch.zeros(1, dtype=torch.float64, device="cuda:0")
-    nm = 100000
-    mol = cell.expand(nm)
-    site = cell.expand(nm, 28)
-    with pytest.raises(CcpError) as e:
-        kspace_ewald_fixed(m, mol, mol, mol, site, site, site, 14, 14, 14, 0.358, 150.0,
-                           cell, site, site, site, cell)
-    assert e.value.code == 6 and "bytes of scratch" in str(e.value)
+    buf = torch.zeros(28, dtype=torch.float64, device="cuda:0")
+    p = buf.data_ptr()
+    rc = _lib.lib().ccp_kspace_ewald_fixed(m.handle, 100000, p, p, p, p, p, p, 28, 14, 14, 14,
+                                           0.358, 150.0, p, p, p, p, p, None)
+    assert rc == 6
+    assert "bytes of scratch" in _lib.lib().ccp_last_error().decode()
+    torch.cuda.synchronize()
+    assert float(buf.abs().sum()) == 0.0  # untouched
