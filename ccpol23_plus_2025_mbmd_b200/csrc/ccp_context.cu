@@ -84,6 +84,7 @@ struct ccp_context {
   double *d_mu = nullptr, *d_e0r = nullptr, *d_e0k = nullptr, *d_e0slf = nullptr, *d_e0s = nullptr;
   double *d_eir = nullptr, *d_eik = nullptr, *d_eislf = nullptr, *d_eis = nullptr;
   double *d_mu2 = nullptr, *d_e0tot = nullptr, *d_eim = nullptr;
+  double *d_pcg = nullptr;  // PCG vectors u, w, s, p of the dipole solve (4 x npol x 3)
   double4 *d_T4 = nullptr, *d_S4 = nullptr;
   double *d_TB = nullptr, *d_SB = nullptr;
   // lists
@@ -149,7 +150,7 @@ struct ccp_context {
   cudaStream_t cap_stream = nullptr;
   cudaGraph_t ind_graph = nullptr;
   cudaGraphExec_t ind_exec = nullptr;
-  double *d_istate = nullptr;  // {iterations, last change, last energy, finished}
+  double *d_istate = nullptr;  // kIterStateLen slots (IterStateSlot)
   double *h_istate = nullptr;
   unsigned *d_ticket = nullptr;  // last-block ticket of the fused update kernel
   int ind_per_iter = 0;          // kernels per Jacobi iteration of the last solve
@@ -162,6 +163,12 @@ struct ccp_context {
   // options (ccp_context_set_option)
   int opt_graph = 1;  // Jacobi loop as a conditional graph (1) or driven from the host (0)
   int opt_phase = 1;  // phase-factor tables when they fit (1) or never (0)
+  // dipole solver: Jacobi at the reference's criterion (0), PCG at the reference's criterion
+  // (1), PCG at an RMS criterion of dip_tol_debye (2); PCG needs the phase tables and falls
+  // back to Jacobi (at the reference's criterion) without them
+  int opt_solver = 0;
+  double dip_tol_debye = 1e-8;
+  bool pcg_active = false;  // the solver of the last solve was PCG
   // phase timing (diagnostics)
   bool timing = false;
   cudaEvent_t ev[2 * CCP_NPHASE] = {};  // start/end of each phase, on the phase's stream
@@ -193,7 +200,8 @@ void free_ctx(ccp_context *c) {
                 c->d_types,
                 c->d_gfs3,  c->d_vdw_row, c->d_vdw_site, c->d_vdw_qq, c->d_vdw_par,
                 c->d_pcoord, c->d_md_x, c->d_md_xs, c->d_md_v, c->d_md_q, c->d_md_j, c->d_md_red,
-                c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB};
+                c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB,
+                c->d_pcg};
   for (void *p : dp)
     if (p) cudaFree(p);
   if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -358,6 +366,16 @@ struct EvalOut {
 constexpr size_t kPhaseBudget = size_t(1) << 30;
 
 constexpr double kIndThr = 1.0e-20;  // iteridm convergence threshold on sum |dmu|^2
+constexpr double kDebyePerEA = 4.80320471;  // Debye per e*Angstrom (dipoles are in e*A)
+
+// Whether the next solve is PCG, and its convergence threshold on sum |dmu|^2 (PCG: sum |u|^2
+// at the iterate, the Jacobi update there).
+bool pcg_solver(const ccp_context *c) { return c->opt_solver != 0 && c->use_P; }
+double ind_threshold(const ccp_context *c) {
+  if (!pcg_solver(c) || c->opt_solver == 1) return kIndThr;
+  const double t = c->dip_tol_debye / kDebyePerEA;
+  return (double)c->nm * c->S.np * t * t;
+}
 
 // Enqueues one Jacobi step: with the phase factors two kernels (k_iter.cu), otherwise T.mu,
 // the tiled dipole structure factors and reciprocal field, the update and the convergence
@@ -392,7 +410,14 @@ IterArgs make_iter_args(ccp_context *c, cudaGraphConditionalHandle handle, int u
   A.scal = c->d_scal;
   A.state = c->d_istate;
   A.ticket = c->d_ticket;
-  A.thr = kIndThr;
+  A.thr = ind_threshold(c);
+  if (pcg_solver(c)) {
+    const size_t np3 = (size_t)A.nw * 3;
+    A.cu = c->d_pcg;
+    A.cw = c->d_pcg + np3;
+    A.cs = c->d_pcg + 2 * np3;
+    A.cp = c->d_pcg + 3 * np3;
+  }
   A.maxit = c->maxit;
   A.use_graph = use_graph;
   A.handle = handle;
@@ -439,7 +464,12 @@ int ensure_ind_graph(ccp_context *c) {
       (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_skj, (long long)c->d_eik,
       (long long)c->d_kg,
       (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
-      (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit};
+      (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit,
+      (long long)pcg_solver(c), (long long)c->opt_solver, (long long)c->d_pcg};
+  double thr = ind_threshold(c);
+  long long thr_bits;
+  std::memcpy(&thr_bits, &thr, sizeof thr_bits);
+  key.push_back(thr_bits);
   if (c->ind_exec && key == c->ind_key) return CCP_OK;
   if (c->ind_exec) cudaGraphExecDestroy(c->ind_exec);
   if (c->ind_graph) cudaGraphDestroy(c->ind_graph);
@@ -453,7 +483,8 @@ int ensure_ind_graph(ccp_context *c) {
   // condition it sets
   CK(cudaStreamBeginCaptureToGraph(cs, c->ind_graph, nullptr, nullptr, 0,
                                    cudaStreamCaptureModeRelaxed));
-  const cudaError_t ef = launch_dip_first(make_iter_args(c, h, 1, 0), cs);
+  const IterArgs A0 = make_iter_args(c, h, 1, 0);
+  const cudaError_t ef = A0.cu ? launch_pcg_first(A0, cs) : launch_dip_first(A0, cs);
   cudaGraph_t captured_first = nullptr;
   const cudaError_t ef2 = cudaStreamEndCapture(cs, &captured_first);
   if (!cuda_ok(ef, "capture of the first dipole step")) return CCP_ERR_CUDA;
@@ -490,7 +521,11 @@ int ensure_ind_graph(ccp_context *c) {
 // h_istate; in the graph form the copy completes at the evaluation's final synchronisation.
 int run_dipole_loop(ccp_context *c, cudaStream_t st) {
   // the first step writes every dipole, so d_mu needs no clearing
-  CK(cudaMemsetAsync(c->d_istate, 0, 4 * sizeof(double), st));
+  const bool pcg = pcg_solver(c);
+  c->pcg_active = pcg;
+  if (pcg && !c->d_pcg) CK(dalloc(&c->d_pcg, 4 * (size_t)c->nm * c->S.np * 3));
+  const double thr = ind_threshold(c);
+  CK(cudaMemsetAsync(c->d_istate, 0, kIterStateLen * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_scal + S_IND_CHANGE, 0, 2 * sizeof(double), st));
   CK(cudaMemsetAsync(c->d_ticket, 0, sizeof(unsigned), st));
   if (c->use_P) CK(cudaMemsetAsync(c->d_skj, 0, sizeof(double) * 4 * (size_t)c->nk, st));
@@ -502,13 +537,18 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
     CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     per = c->use_P ? 2 : 5;
   } else {
-    if (!cuda_ok(launch_dip_first(make_iter_args(c, 0, 0, 0), st), "first dipole step"))
+    const IterArgs A0 = make_iter_args(c, 0, 0, 0);
+    if (!cuda_ok(pcg ? launch_pcg_first(A0, st) : launch_dip_first(A0, st), "first dipole step"))
       return CCP_ERR_CUDA;
     for (int step = 0;; step++) {
-      CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
-      CK(cudaStreamSynchronize(st));
-      const int it = (int)c->h_istate[0];
-      if (!(c->h_istate[1] > kIndThr && it < c->maxit)) break;
+      // the PCG start takes no step, so its first step always runs
+      if (!pcg || step > 0) {
+        CK(cudaMemcpyAsync(c->h_istate, c->d_istate, 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                           st));
+        CK(cudaStreamSynchronize(st));
+        const int it = (int)c->h_istate[0];
+        if (!(c->h_istate[1] > thr && it < c->maxit)) break;
+      }
       if (!cuda_ok(enqueue_dip_step(c, st, 0, 0, step & 1, &per), "dipole step"))
         return CCP_ERR_CUDA;
     }
@@ -802,7 +842,8 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
     if (mask & T_INDUCTION) {
       o.iters = (int)c->h_istate[0];
       o.ind_e = c->h_istate[2];
-      c->launches += 1 + c->ind_per_iter * (o.iters - 1);  // the first step is one kernel
+      // the Jacobi first step is one kernel; the PCG start takes no step
+      c->launches += 1 + c->ind_per_iter * (c->pcg_active ? o.iters : o.iters - 1);
       o.converged = o.iters < c->maxit;
       if (!o.converged) {
         set_error("No convergence in the induced-dipole iteration (maxit reached)");
@@ -1070,6 +1111,9 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
   auto *c = new ccp_context();
   c->device = device;
   c->precision = precision;
+  // the mixed form solves for the dipoles by PCG to 1e-8 D RMS, the FP64 form by the
+  // reference's Jacobi iteration and criterion
+  c->opt_solver = precision == CCP_MIXED ? 2 : 0;
   c->nm = nm;
   c->ns = m->ns;
   c->npol = m->npol;
@@ -1157,7 +1201,7 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
       cudaEventCreateWithFlags(&c->ev_lp, cudaEventDisableTiming) != cudaSuccess)
     return fail("event");
   c->stream = c->own;
-  if (cudaMalloc(&c->d_istate, 4 * sizeof(double)) != cudaSuccess ||
+  if (cudaMalloc(&c->d_istate, kIterStateLen * sizeof(double)) != cudaSuccess ||
       cudaMalloc(&c->d_ticket, sizeof(unsigned)) != cudaSuccess ||
       cudaMemset(c->d_ticket, 0, sizeof(unsigned)) != cudaSuccess ||
       cudaMallocHost((void **)&c->h_istate, 3 * sizeof(double)) != cudaSuccess)
@@ -1324,6 +1368,13 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_graph = value != 0;
   } else if (n == "phase_matrix") {
     ctx->opt_phase = value != 0;
+  } else if (n == "dipole_solver") {
+    if (value < 0 || value > 2) {
+      set_error("ccp_context_set_option: dipole_solver must be 0 (Jacobi), 1 (PCG, the "
+                "reference's criterion) or 2 (PCG, 1e-8 D RMS)");
+      return CCP_ERR_BAD_INPUT;
+    }
+    ctx->opt_solver = value;
   } else if (n == "overlap") {
     ctx->opt_overlap = value != 0;
   } else if (n == "fs3_param_grad") {
@@ -1356,6 +1407,10 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_phase;
   } else if (n == "phase_matrix_active") {
     *value = ctx->use_P ? 1 : 0;
+  } else if (n == "dipole_solver") {
+    *value = ctx->opt_solver;
+  } else if (n == "dipole_solver_pcg_active") {
+    *value = ctx->pcg_active ? 1 : 0;
   } else if (n == "overlap") {
     *value = ctx->opt_overlap;
   } else if (n == "fs3_param_grad") {

@@ -135,7 +135,8 @@ struct KGather {
   int lmni, pad;
 };
 
-// Arguments of one Jacobi step of the dipole solve with the phase matrix (k_iter.cu).
+// Arguments of one step of the dipole solve with the phase matrix (k_iter.cu): a Jacobi step,
+// or with cu.. set a preconditioned-conjugate-gradient step.
 struct IterArgs {
   const int *nbr, *ncnt;
   int cap, nw, np;  // nw = polarisable sites = nm * np
@@ -153,13 +154,29 @@ struct IterArgs {
   int nlm, nz, mmax, nmax;
   // sk[k] holds two S(k) buffers, (re, im) of steps of parity 0 and 1: a step accumulates
   // into its own and clears the other, which the previous step's gather has finished with
-  double *sk, *scal, *state;  // state = {iterations, change, energy, finished}
+  double *sk, *scal, *state;  // state: see IterStateSlot
   int par;                    // parity of this step
   unsigned *ticket;
   double thr;
   int maxit, use_graph;
   cudaGraphConditionalHandle handle;
   SiteSets S;
+  // preconditioned conjugate gradients (k_iter.cu): the vectors u (preconditioned residual),
+  // w = A u, s = A p and p of every polarisable site component; mu holds the iterate x
+  double *cu, *cw, *cs, *cp;
+};
+
+// Slots of the dipole solve's state array (doubles).
+enum IterStateSlot {
+  kIterIters = 0,    // steps taken
+  kIterChange,       // sum |dmu|^2 of the last step (Jacobi) or sum |u|^2 at the iterate (PCG)
+  kIterEnergy,       // induction energy sum of the last step
+  kIterFinished,     // 1 once the solve has converged (or hit maxit)
+  kIterAlpha,        // PCG: step length of the next update
+  kIterBeta,         // PCG: direction weight of the next update
+  kIterGamma,        // PCG: (r, u) of the current iterate
+  kIterAcc,          // PCG: 4 accumulators (gamma, delta, change, energy) of a step
+  kIterStateLen = kIterAcc + 4
 };
 
 // ccpol23plus 2-body parameters (vdw_ccpol23plus.f90): rows of beta, c0, c1, c2, c3, c6, c8,
@@ -241,6 +258,8 @@ cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np,
                        const double *TB, const double4 *S4, const double *SB, const double *mu,
                        double *eim, cudaStream_t st);
 cudaError_t launch_dip_first(const IterArgs &A, cudaStream_t st);
+// Start of the PCG form of the solve (A.cu.. set): x = 0, u = alpha E0, state cleared.
+cudaError_t launch_pcg_first(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st);
 cudaError_t launch_pair_indforce(const double *x, const double *y, const double *z,

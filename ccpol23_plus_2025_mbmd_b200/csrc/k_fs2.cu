@@ -35,8 +35,44 @@ __global__ void k_fs2_enum(const double4 *__restrict__ comb, const int *__restri
 __constant__ double kCharge3b[5] = {0.258504607653328389, 0.564050362569283648,
                                     0.564050362569283648, -0.693302666395947953,
                                     -0.693302666395947953};
+__constant__ float kCharge3bf[5] = {0.258504607653328389f, 0.564050362569283648f,
+                                    0.564050362569283648f, -0.693302666395947953f,
+                                    -0.693302666395947953f};
 
-// 4 blocks (16 warps) per SM: 128 registers a thread, against 154 unbounded
+// Mixed form: one spectator site ks of charge q seen from the pair, in FP32.  The FS2 terms
+// are differences between the spectator's interaction with the pair's centres and with the
+// exchange charges displaced by d = -+ g3 r_ij/|r_ij| (threebody_potential.f90:392-583), and
+// formed literally they cancel to ~1e-3 of their parts.  Here every difference is formed from
+// the displacement itself, with c the spectator site seen from a centre, e = c + d from the
+// exchange charge, ic = 1/|c|, ie = 1/|e| and dl = |e|^2 - |c|^2 = d.(2c + d):
+//   1/|c| - 1/|e| = dl ic^2 ie^2 / (ic + ie)                                (= D)
+//   e/|e|^3 - c/|c|^3 = d ie^3 - D (ie^2 + ie ic + ic^2) c                  (= G)
+// so the FP32 terms keep ~1e-7 relative accuracy.
+struct Fs2Side {
+  float D, ie3;   // 1/|c| - 1/|e| and 1/|e|^3
+  float3 G, e;    // e/|e|^3 - c/|c|^3 and e
+};
+__device__ __forceinline__ Fs2Side fs2_side(float cx, float cy, float cz, float dx, float dy,
+                                            float dz) {
+  Fs2Side r;
+  const float ex = cx + dx, ey = cy + dy, ez = cz + dz;
+  const float ic = rsqrtf(cx * cx + cy * cy + cz * cz);
+  const float ie = rsqrtf(ex * ex + ey * ey + ez * ez);
+  const float dl = dx * (2.0f * cx + dx) + dy * (2.0f * cy + dy) + dz * (2.0f * cz + dz);
+  const float ic2 = ic * ic, ie2 = ie * ie;
+  r.D = dl * ic2 * ie2 / (ic + ie);
+  r.ie3 = ie2 * ie;
+  const float w = r.D * (ie2 + ie * ic + ic2);
+  r.G = make_float3(dx * r.ie3 - w * cx, dy * r.ie3 - w * cy, dz * r.ie3 - w * cz);
+  r.e = make_float3(ex, ey, ez);
+  return r;
+}
+
+// 4 blocks (16 warps) per SM: 128 registers a thread, against 154 unbounded.  LOW: the mixed
+// form, whose spectator terms run in FP32 (fs2_side) with per-spectator sums promoted into
+// the FP64 accumulators; the pair's exchange sums, the cut-off tests and every accumulation
+// across spectators stay FP64.
+template <bool LOW>
 __global__ void __launch_bounds__(128, 4)
     k_fs2(const int2 *__restrict__ pairs, const int *__restrict__ icnt, int pair_cap,
           const double4 *__restrict__ comb, const double4 *__restrict__ s17,
@@ -189,6 +225,90 @@ __global__ void __launch_bounds__(128, 4)
     atomicAdd(&fc2[nm + k], ck_y * conv);
     atomicAdd(&fc2[2 * nm + k], ck_z * conv);
   };
+  // The same spectator in FP32 (mixed form); identical terms, regrouped as in fs2_side.
+  auto spectator32 = [&](int k) {
+    const double4 ck = comb[k];
+    const double xki = minimg(xsub(ck.x, ci.x), P.boxb);
+    const double yki = minimg(xsub(ck.y, ci.y), P.boxb);
+    const double zki = minimg(xsub(ck.z, ci.z), P.boxb);
+    const float kix = (float)xki, kiy = (float)yki, kiz = (float)zki;
+    const float kjx = (float)xadd(xki, xij), kjy = (float)xadd(yki, yij),
+                kjz = (float)xadd(zki, zij);
+    const float alp3 = (float)P.alp3, r0 = (float)P.r0dmp, d33 = (float)P.delta33;
+    const float sdki = sqrtf(kix * kix + kiy * kiy + kiz * kiz);
+    const float sdkj = sqrtf(kjx * kjx + kjy * kjy + kjz * kjz);
+    float pom = expf(alp3 * (sdki - r0));
+    const float pomki = 1.0f / (1.0f + pom);
+    const float flrki = expf(-d33 * log1pf(pom));
+    const float dflrki = -alp3 * d33 * pom * pomki * flrki;
+    const float dflrkiv = -alp3 * d33 * pom * pomki * sdki;
+    pom = expf(alp3 * (sdkj - r0));
+    const float pomkj = 1.0f / (1.0f + pom);
+    const float flrkj = expf(-d33 * log1pf(pom));
+    const float dflrkj = -alp3 * d33 * pom * pomkj * flrkj;
+    const float dflrkjv = -alp3 * d33 * pom * pomkj * sdkj;
+    const float fl = flrki * flrkj;
+    const float cki = dflrki * flrkj / sdki, ckj = dflrkj * flrki / sdkj;
+    nspec++;
+    const float rx = (float)xij, ry = (float)yij, rz = (float)zij;
+    const float g = (float)g3, r1 = (float)dij1i, r3 = (float)dij3i;
+    const float hx = g * rx * r1, hy = g * ry * r1, hz = g * rz * r1;  // g3 r_ij / |r_ij|
+    const float Ef = (float)E, Evf = (float)Ev;
+    float e_s = 0.f, v_s = 0.f, a_s = 0.f, ckx = 0.f, cky = 0.f, ckz = 0.f;
+    float cix = 0.f, ciy = 0.f, ciz = 0.f, cjx = 0.f, cjy = 0.f, cjz = 0.f;
+    for (int ks = 0; ks < 5; ks++) {
+      const float qks = kCharge3bf[ks];
+      const double4 sk = s17[(size_t)k * kNs3 + ks];
+      const float skx = (float)sk.x, sky = (float)sk.y, skz = (float)sk.z;
+      // from i's centre with the exchange charge at -g3 r^; from j's at +g3 r^
+      const Fs2Side A = fs2_side(kix + skx, kiy + sky, kiz + skz, -hx, -hy, -hz);
+      const Fs2Side B = fs2_side(kjx + skx, kjy + sky, kjz + skz, hx, hy, hz);
+      const float term0 = A.D + B.D;
+      const float qE = qks * Ef;
+      e_s += qE * term0 * fl;
+      const float dqi = rx * A.e.x + ry * A.e.y + rz * A.e.z;
+      const float dqj = rx * B.e.x + ry * B.e.y + rz * B.e.z;
+      const float h = dqi * A.ie3 - dqj * B.ie3;
+      const float Hx = A.e.x * A.ie3 - B.e.x * B.ie3, Hy = A.e.y * A.ie3 - B.e.y * B.ie3,
+                  Hz = A.e.z * A.ie3 - B.e.z * B.ie3;
+      v_s += (qks * Evf + (dflrkiv + dflrkjv) * qE) * term0 * fl + qE * g * r1 * h * fl;
+      a_s += qks * term0 * fl;
+      // spectator site force
+      const float fkx = qE * (A.G.x + B.G.x), fky = qE * (A.G.y + B.G.y),
+                  fkz = qE * (A.G.z + B.G.z);
+      const size_t so = (size_t)k * ns + ks;
+      atomicAdd(&f[so], (double)(-fkx * fl) * conv);
+      atomicAdd(&f[nfs + so], (double)(-fky * fl) * conv);
+      atomicAdd(&f[2 * nfs + so], (double)(-fkz * fl) * conv);
+      const float tki = qE * term0 * cki, tkj = qE * term0 * ckj;
+      ckx += -tki * kix - tkj * kjx;
+      cky += -tki * kiy - tkj * kjy;
+      ckz += -tki * kiz - tkj * kjz;
+      const float gh = g * r1, gh3 = g * r3 * h;
+      const float fxi = qE * (-A.G.x - gh * Hx + gh3 * rx), fyi = qE * (-A.G.y - gh * Hy + gh3 * ry),
+                  fzi = qE * (-A.G.z - gh * Hz + gh3 * rz);
+      const float fxj = qE * (-B.G.x + gh * Hx - gh3 * rx), fyj = qE * (-B.G.y + gh * Hy - gh3 * ry),
+                  fzj = qE * (-B.G.z + gh * Hz - gh3 * rz);
+      cix += -fxi * fl + tki * kix;
+      ciy += -fyi * fl + tki * kiy;
+      ciz += -fzi * fl + tki * kiz;
+      cjx += -fxj * fl + tkj * kjx;
+      cjy += -fyj * fl + tkj * kjy;
+      cjz += -fzj * fl + tkj * kjz;
+    }
+    e_loc += (double)e_s;
+    v_loc += (double)v_s;
+    A_loc += (double)a_s;
+    Ci[0] += (double)cix;
+    Ci[1] += (double)ciy;
+    Ci[2] += (double)ciz;
+    Cj[0] += (double)cjx;
+    Cj[1] += (double)cjy;
+    Cj[2] += (double)cjz;
+    atomicAdd(&fc2[k], (double)ckx * conv);
+    atomicAdd(&fc2[nm + k], (double)cky * conv);
+    atomicAdd(&fc2[2 * nm + k], (double)ckz * conv);
+  };
   // The spectators are i's neighbours k != j within the cut-off of both i and j; only a
   // fraction pass, so the warp first queues them (ballot + prefix into shared memory) and
   // evaluates them 32 at a time with every lane busy.
@@ -222,7 +342,12 @@ __global__ void __launch_bounds__(128, 4)
       __syncwarp();
     }
     if (nq == 0) break;
-    if (lane < nq) spectator(kq[lane]);
+    if (lane < nq) {
+      if constexpr (LOW)
+        spectator32(kq[lane]);
+      else
+        spectator(kq[lane]);
+    }
     __syncwarp();
     if (lane < nq - 32) kq[lane] = kq[32 + lane];
     nq = nq > 32 ? nq - 32 : 0;
@@ -272,13 +397,17 @@ cudaError_t launch_fs2(int precision, const int2 *pairs, const int *icnt, int pa
                        const double4 *comb, const double4 *s17, const int *nbr,
                        const int *ncnt, int cap, Fs2Params P, int nm, int ns, double *f,
                        double *fc2, double *scal, cudaStream_t st) {
-  (void)precision;
   // one warp per pair; the pair count is on the device, so launch for the capacity and
   // let surplus warps exit at once.
   const int warps = pair_cap;
   const int threads = 128;
   const int blocks = (warps * 32 + threads - 1) / threads;
-  k_fs2<<<blocks, threads, 0, st>>>(pairs, icnt, pair_cap, comb, s17, nbr, ncnt, cap, P, nm, ns,
-                                    f, fc2, scal, const_cast<int *>(icnt) + C_NTRI_FS2);
+  int *nc = const_cast<int *>(icnt) + C_NTRI_FS2;
+  if (precision == 1)  // CCP_MIXED
+    k_fs2<true><<<blocks, threads, 0, st>>>(pairs, icnt, pair_cap, comb, s17, nbr, ncnt, cap, P,
+                                            nm, ns, f, fc2, scal, nc);
+  else
+    k_fs2<false><<<blocks, threads, 0, st>>>(pairs, icnt, pair_cap, comb, s17, nbr, ncnt, cap, P,
+                                             nm, ns, f, fc2, scal, nc);
   return cudaGetLastError();
 }

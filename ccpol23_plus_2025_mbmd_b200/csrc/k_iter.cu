@@ -76,17 +76,79 @@ __device__ __forceinline__ double2 kphase(const double2 *__restrict__ xyw,
   return make_double2(a.x * b.x - a.y * b.y, a.y * b.x + a.x * b.y);
 }
 
+// The vector a T.mu product reads: the dipoles themselves (Jacobi).
+struct MuIn {
+  const double *__restrict__ mu;
+  __device__ __forceinline__ double3 operator()(size_t site, int) const {
+    const double *m = mu + site * 3;
+    return make_double3(m[0], m[1], m[2]);
+  }
+};
+
+// Preconditioned conjugate gradients (the mixed form's dipole solve) for the same linear
+// system as the Jacobi step: A mu = E0 with A mu = mu / alpha - F(mu), F(mu) the field of the
+// dipoles (T.mu real space + reciprocal + intramolecular corrections, which is symmetric), and
+// the preconditioner M^-1 = diag(alpha), so that the preconditioned residual u = alpha (E0 -
+// A x) = alpha (E0 + F(x)) - x is exactly the Jacobi update at the iterate x.  The recurrences
+// are Chronopoulos and Gear's one-reduction form (Chronopoulos & Gear, J. Comput. Appl. Math.
+// 25 (1989) 153-168): with w = A u and s = A p,
+//   p = u + beta p,  s = w + beta s,  x += alpha p,  u -= alpha M^-1 s,  w = A u,
+//   gamma = (u, M u), delta = (w, u), beta' = gamma' / gamma,
+//   alpha' = gamma' / (delta' - beta' gamma' / alpha),
+// so one step is one product A u and one merged reduction, as a Jacobi step is.  The new u
+// of a site is needed by every reader of the product before the update kernel can store it,
+// so readers form it where they read it (pcg_s, pcg_u) from the stored u, w and s and the two
+// scalars of the step; the update kernel forms the same values with the same operations
+// (explicit roundings, no contraction), so all of them see the same u.
+__device__ __forceinline__ double pcg_s(double w, double s, double beta) {
+  return __fma_rn(beta, s, w);
+}
+__device__ __forceinline__ double pcg_u(double u, double s_new, double apol, double alpha) {
+  return __fma_rn(-alpha, __dmul_rn(apol, s_new), u);
+}
+struct PcgIn {
+  const double *__restrict__ u;
+  const double *__restrict__ w;
+  const double *__restrict__ s;
+  double alpha, beta, a0, a1, a2, a3;  // step scalars; polarisabilities of sites 0..3
+  __device__ __forceinline__ double apol(int q) const {
+    return q == 0 ? a0 : (q == 1 ? a1 : (q == 2 ? a2 : a3));
+  }
+  __device__ __forceinline__ double comp(size_t o, double ap) const {
+    return pcg_u(u[o], pcg_s(w[o], s[o], beta), ap, alpha);
+  }
+  __device__ __forceinline__ double3 operator()(size_t site, int q) const {
+    const double ap = apol(q);
+    const size_t o = site * 3;
+    return make_double3(comp(o, ap), comp(o + 1, ap), comp(o + 2, ap));
+  }
+};
+
+__device__ __forceinline__ PcgIn pcg_in(const IterArgs &A) {
+  PcgIn in;
+  in.u = A.cu;
+  in.w = A.cw;
+  in.s = A.cs;
+  in.alpha = A.state[kIterAlpha];
+  in.beta = A.state[kIterBeta];
+  in.a0 = A.S.apol[0];
+  in.a1 = A.np > 1 ? A.S.apol[1] : 0.0;
+  in.a2 = A.np > 2 ? A.S.apol[2] : 0.0;
+  in.a3 = A.np > 3 ? A.S.apol[3] : 0.0;
+  return in;
+}
+
 // T.mu of polarisable site w = (i, p): entries T4/TB[i][p][n][q] for the neighbours n of i and
 // the polarisable sites q of each, plus the intramolecular entries S4/SB[i][p][q].  Called by
-// whole warps; the sum is returned to every lane.
+// whole warps; the sum is returned to every lane.  `in` gives the vector multiplied.
+template <typename In>
 __device__ __forceinline__ void tmu_warp(int w, int lane, const int *__restrict__ nbr,
                                          const int *__restrict__ ncnt, int cap, int np,
                                          const double4 *__restrict__ T4,
                                          const double *__restrict__ TB,
                                          const double4 *__restrict__ S4,
-                                         const double *__restrict__ SB,
-                                         const double *__restrict__ mu, double &ex, double &ey,
-                                         double &ez) {
+                                         const double *__restrict__ SB, const In &in,
+                                         double &ex, double &ey, double &ez) {
   const int i = w / np;
   const int cnt = ncnt[i];
   const size_t base = (size_t)w * cap * np;
@@ -98,8 +160,8 @@ __device__ __forceinline__ void tmu_warp(int w, int lane, const int *__restrict_
     const int j = nbr[(size_t)i * cap + n];
     const double4 t = T4[base + e];
     const double b = TB[base + e];
-    const double *m = mu + ((size_t)j * np + q) * 3;
-    const double mx = m[0], my = m[1], mz = m[2];
+    const double3 m = in((size_t)j * np + q, q);
+    const double mx = m.x, my = m.y, mz = m.z;
     const double dm = t.w * (t.x * mx + t.y * my + t.z * mz);
     ex += dm * t.x - b * mx;
     ey += dm * t.y - b * my;
@@ -109,8 +171,8 @@ __device__ __forceinline__ void tmu_warp(int w, int lane, const int *__restrict_
     const size_t o = (size_t)w * np + lane;
     const double4 t = S4[o];
     const double b = SB[o];
-    const double *m = mu + ((size_t)i * np + lane) * 3;
-    const double mx = m[0], my = m[1], mz = m[2];
+    const double3 m = in((size_t)i * np + lane, lane);
+    const double mx = m.x, my = m.y, mz = m.z;
     const double dm = t.w * (t.x * mx + t.y * my + t.z * mz);
     ex += dm * t.x - b * mx;
     ey += dm * t.y - b * my;
@@ -131,7 +193,7 @@ __global__ void __launch_bounds__(kThreads)
   const int lane = threadIdx.x & 31;
   if (w >= nw) return;
   double ex, ey, ez;
-  tmu_warp(w, lane, nbr, ncnt, cap, np, T4, TB, S4, SB, mu, ex, ey, ez);
+  tmu_warp(w, lane, nbr, ncnt, cap, np, T4, TB, S4, SB, MuIn{mu}, ex, ey, ez);
   if (lane == 0) {
     eim[(size_t)w * 3 + 0] = ex;
     eim[(size_t)w * 3 + 1] = ey;
@@ -139,11 +201,14 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+template <bool PCG>
 __global__ void __launch_bounds__(kThreads)
     k_iter_a(IterArgs A) {
   // no test of the finished flag here: a step after the finish only rewrites the T.mu
   // scratch and S(k), which the next use clears, and it saves a dependent load per step
   const int nA = (A.nw + kWarps - 1) / kWarps;
+  PcgIn pin;
+  if constexpr (PCG) pin = pcg_in(A);
   if ((int)blockIdx.x < nA) {
     // the other parity's buffer: its last reader, the previous step's gather, has finished
     double2 *other = reinterpret_cast<double2 *>(A.sk) + (A.par ^ 1);
@@ -153,7 +218,11 @@ __global__ void __launch_bounds__(kThreads)
     const int lane = threadIdx.x & 31;
     if (w >= A.nw) return;
     double ex, ey, ez;
-    tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, A.mu, ex, ey, ez);
+    if constexpr (PCG)
+      tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, pin, ex, ey, ez);
+    else
+      tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, MuIn{A.mu}, ex, ey,
+               ez);
     if (lane == 0) {
       A.eim[(size_t)w * 3 + 0] = ex;
       A.eim[(size_t)w * 3 + 1] = ey;
@@ -167,7 +236,14 @@ __global__ void __launch_bounds__(kThreads)
   const int nkt = (A.nk + kThreads - 1) / kThreads;
   const int kt = b % nkt, sc = b / nkt;
   const int s0 = sc * kSumSites, cnt = min(kSumSites, A.nw - s0);
-  for (int u = threadIdx.x; u < cnt * 3; u += kThreads) smu[u] = A.mu[(size_t)s0 * 3 + u];
+  for (int u = threadIdx.x; u < cnt * 3; u += kThreads) {
+    if constexpr (PCG) {
+      const int site = s0 + u / 3;
+      smu[u] = pin.comp((size_t)s0 * 3 + u, pin.apol(site % A.np));
+    } else {
+      smu[u] = A.mu[(size_t)s0 * 3 + u];
+    }
+  }
   __syncthreads();
   const int k = kt * kThreads + threadIdx.x;
   if (k >= A.nk) return;
@@ -187,11 +263,90 @@ __global__ void __launch_bounds__(kThreads)
   atomicAdd(&A.sk[(size_t)k * 4 + 2 * A.par + 1], g * a1);
 }
 
+// The PCG step's update for the kGatherSites sites of a block, after the reciprocal field of
+// u is in `part`: the vectors of the step (s, p, x, u, w = A u) in place, the partial sums
+// of (u, M u), (w, u), |u|^2 and the energy -1/2 x.E0 (the reference's energy expression at
+// the iterate), and in the last block to finish the step's scalars and the convergence test
+// on sum |u|^2, the Jacobi update's norm at the iterate.
+__device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk,
+                                           const double (*part)[kGatherSites * 3]) {
+  double gam = 0.0, del = 0.0, ch = 0.0, en = 0.0;
+  if ((int)threadIdx.x < ns_blk) {
+    const int g = threadIdx.x, w = w0 + g;
+    double ek[3] = {0.0, 0.0, 0.0};
+    for (int u = 0; u < kWarps; u++)
+      for (int c = 0; c < 3; c++) ek[c] += part[u][g * 3 + c];
+    const double ap = A.S.apol[w % A.np];
+    const double ca = A.state[kIterAlpha], cb = A.state[kIterBeta];
+    for (int c = 0; c < 3; c++) {
+      const size_t o = (size_t)w * 3 + c;
+      const double u0 = A.cu[o];
+      const double s = pcg_s(A.cw[o], A.cs[o], cb);
+      const double p = __fma_rn(cb, A.cp[o], u0);
+      const double x = __fma_rn(ca, p, A.mu[o]);
+      const double u = pcg_u(u0, s, ap, ca);
+      const double wv = u / ap - (A.eim[o] + ek[c]);
+      A.cs[o] = s;
+      A.cp[o] = p;
+      A.mu[o] = x;
+      A.cu[o] = u;
+      A.cw[o] = wv;
+      gam += u * u / ap;
+      del += wv * u;
+      ch += u * u;
+      en += -0.5 * x * A.e0[o];
+    }
+  }
+  gam = warp_sum(gam);  // the updating threads are all in warp 0
+  del = warp_sum(del);
+  ch = warp_sum(ch);
+  en = warp_sum(en);
+  __shared__ bool last;
+  double *acc = A.state + kIterAcc;
+  if (threadIdx.x == 0) {
+    atomicAdd(acc + 0, gam);
+    atomicAdd(acc + 1, del);
+    atomicAdd(acc + 2, ch);
+    atomicAdd(acc + 3, en);
+    __threadfence();
+    last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x == 0) {
+    const double g1 = atomicAdd(acc + 0, 0.0), d1 = atomicAdd(acc + 1, 0.0);
+    const double chg = atomicAdd(acc + 2, 0.0), ene = atomicAdd(acc + 3, 0.0);
+    for (int k = 0; k < 4; k++) acc[k] = 0.0;
+    *A.ticket = 0u;
+    int it = (int)A.state[kIterIters] + 1;
+    A.state[kIterChange] = chg;
+    A.state[kIterEnergy] = ene;
+    bool more = chg > A.thr && it < A.maxit;
+    if (more) {
+      const double beta = it == 1 ? 0.0 : g1 / A.state[kIterGamma];
+      const double alpha = it == 1 ? g1 / d1 : g1 / (d1 - beta * g1 / A.state[kIterAlpha]);
+      if (alpha > 0.0 && alpha < 1e300) {
+        A.state[kIterAlpha] = alpha;
+        A.state[kIterBeta] = beta;
+        A.state[kIterGamma] = g1;
+      } else {  // breakdown (not positive definite): reported as no convergence
+        it = A.maxit;
+        more = false;
+      }
+    }
+    A.state[kIterIters] = (double)it;
+    if (!more) A.state[kIterFinished] = 1.0;
+    if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
+  }
+}
+
+template <bool PCG>
 __global__ void __launch_bounds__(kThreads)
     k_iter_b(IterArgs A) {
   // kGatherSites polarisable sites per block; the 8 warps split the k-vectors, so every
   // k-vector's weights are loaded once per block and reused for all its sites
-  if (A.state[3] != 0.0) return;  // the solve finished in an earlier step of this pass
+  if (A.state[kIterFinished] != 0.0) return;  // finished in an earlier step of this pass
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int w0 = blockIdx.x * kGatherSites;
   const int ns_blk = min(kGatherSites, A.nw - w0);
@@ -227,6 +382,10 @@ __global__ void __launch_bounds__(kThreads)
       if (lane == 0) part[wid][g * 3 + c] = v;
     }
   __syncthreads();
+  if constexpr (PCG) {
+    pcg_update(A, w0, ns_blk, part);
+    return;
+  }
   double ch = 0.0, en = 0.0;
   if (threadIdx.x < ns_blk) {
     // Jacobi update (nb_induction_model.f90:1317-1359), as k_dip_update
@@ -263,15 +422,15 @@ __global__ void __launch_bounds__(kThreads)
   if (threadIdx.x == 0) {
     const double chg = atomicAdd(&A.scal[S_IND_CHANGE], 0.0);
     const double ene = atomicAdd(&A.scal[S_IND_ENERGY], 0.0);
-    const int it = (int)A.state[0] + 1;
-    A.state[0] = (double)it;
-    A.state[1] = chg;
-    A.state[2] = ene;
+    const int it = (int)A.state[kIterIters] + 1;
+    A.state[kIterIters] = (double)it;
+    A.state[kIterChange] = chg;
+    A.state[kIterEnergy] = ene;
     A.scal[S_IND_CHANGE] = 0.0;
     A.scal[S_IND_ENERGY] = 0.0;
     *A.ticket = 0u;
     const bool more = chg > A.thr && it < A.maxit;
-    if (!more) A.state[3] = 1.0;
+    if (!more) A.state[kIterFinished] = 1.0;
     if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
   }
 }
@@ -311,12 +470,30 @@ __global__ void __launch_bounds__(kFirstThreads) k_dip_first(IterArgs A) {
       chg += red[0][u];
       ene += red[1][u];
     }
-    A.state[0] = 1.0;
-    A.state[1] = chg;
-    A.state[2] = ene;
+    A.state[kIterIters] = 1.0;
+    A.state[kIterChange] = chg;
+    A.state[kIterEnergy] = ene;
     const bool more = chg > A.thr && 1 < A.maxit;
-    A.state[3] = more ? 0.0 : 1.0;
+    A.state[kIterFinished] = more ? 0.0 : 1.0;
     if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
+  }
+}
+
+// The start of the PCG solve: x = 0, u = alpha E0 (the Jacobi first step's dipoles), w, s
+// and p zero and the step scalars zero, so that the first step forms w = A u and its scalars
+// from them (k_iter_a/k_iter_b with PCG); inside the graph it lets the WHILE node run.
+__global__ void __launch_bounds__(kFirstThreads) k_pcg_first(IterArgs A) {
+  for (int o = threadIdx.x; o < A.nw * 3; o += kFirstThreads) {
+    A.mu[o] = 0.0;
+    A.cu[o] = A.S.apol[(o / 3) % A.np] * A.e0[o];
+    A.cw[o] = 0.0;
+    A.cs[o] = 0.0;
+    A.cp[o] = 0.0;
+  }
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < kIterStateLen; k++) A.state[k] = 0.0;
+    if (A.maxit < 1) A.state[kIterFinished] = 1.0;
+    if (A.use_graph) cudaGraphSetConditional(A.handle, A.maxit >= 1 ? 1u : 0u);
   }
 }
 
@@ -324,6 +501,11 @@ __global__ void __launch_bounds__(kFirstThreads) k_dip_first(IterArgs A) {
 
 cudaError_t launch_dip_first(const IterArgs &A, cudaStream_t st) {
   k_dip_first<<<1, kFirstThreads, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pcg_first(const IterArgs &A, cudaStream_t st) {
+  k_pcg_first<<<1, kFirstThreads, 0, st>>>(A);
   return cudaGetLastError();
 }
 
@@ -353,11 +535,18 @@ cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st) {
   const int nA = (A.nw + kWarps - 1) / kWarps;
   const int nkt = (A.nk + kThreads - 1) / kThreads;
   const int nsc = (A.nw + kSumSites - 1) / kSumSites;
-  k_iter_a<<<nA + nkt * nsc, kThreads, 0, st>>>(A);
+  if (A.cu)
+    k_iter_a<true><<<nA + nkt * nsc, kThreads, 0, st>>>(A);
+  else
+    k_iter_a<false><<<nA + nkt * nsc, kThreads, 0, st>>>(A);
   return cudaGetLastError();
 }
 
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
-  k_iter_b<<<(A.nw + kGatherSites - 1) / kGatherSites, kThreads, 0, st>>>(A);
+  const int nb = (A.nw + kGatherSites - 1) / kGatherSites;
+  if (A.cu)
+    k_iter_b<true><<<nb, kThreads, 0, st>>>(A);
+  else
+    k_iter_b<false><<<nb, kThreads, 0, st>>>(A);
   return cudaGetLastError();
 }

@@ -1,0 +1,138 @@
+"""The mixed-precision form's own parts against the FP64 form and the oracle.
+
+- The dipole solve by preconditioned conjugate gradients (PCG; the mixed form's default, to
+  1e-8 D RMS): at the reference's own criterion it reproduces the oracle's Jacobi solution;
+  its graph and host-driven loops agree; it reports non-convergence at maxit like Jacobi.
+- FS2 with FP32 spectator terms: energy, site forces and COM forces against the FP64 form.
+"""
+import numpy as np
+import pytest
+
+from ccpol23_plus_2025_mbmd_b200 import CcpError, Context, Model, data_dir
+from ccpol23_plus_2025_mbmd_b200.generator import CONFIGS, water_box
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+PCG_TOL = 1e-9  # PCG at the reference's criterion vs the oracle's Jacobi solution
+
+
+@pytest.fixture(scope="module")
+def boxes(product, oracle):
+    out = {}
+    for key, variant, nm, L, seed, ld in [("c1", "fs3", 128, 15.64, 1001, 28),
+                                          ("ragged_37", "fs2fs3", 37, 10.37, 9, 31)]:
+        m = Model(data_dir(variant))
+        b = water_box(m, nm, L, seed, ld=ld)
+        M = oracle.make_model(oracle.read_inputs(data_dir(variant)), nm, L)
+        out[key] = (m, b, M)
+    return out
+
+
+def _induction(c, b):
+    fx, fy, fz, mx, my, mz = (np.zeros_like(b.xs) for _ in range(6))
+    vir = np.zeros(1)
+    e, it = c.nb_induction(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box, mx, my, mz, fx, fy, fz, vir)
+    return e, it, np.stack([mx, my, mz]), np.stack([fx, fy, fz]), vir[0]
+
+
+@pytest.mark.parametrize("key", ["c1", "ragged_37"])
+def test_pcg_at_reference_criterion_matches_oracle(oracle, boxes, key):
+    O = oracle
+    m, b, M = boxes[key]
+    st = O.State(b.nm, b.xs.shape[1])
+    eo, status, it_o = O.nb_induction(M, b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box, st)
+    assert status == 0
+    with Context(m, b.nm, b.box, precision="fp64") as c:
+        c.set_option("dipole_solver", 1)
+        e, it, mu, F, vir = _induction(c, b)
+        assert c.get_option("dipole_solver_pcg_active") == 1
+    assert it < it_o, (it, it_o)
+    assert abs(e - eo) <= PCG_TOL * abs(eo), (e, eo)
+    assert rel(mu, np.stack([st.idmx, st.idmy, st.idmz])) <= PCG_TOL
+    assert rel(F, np.stack([st.fxs, st.fys, st.fzs])) <= PCG_TOL
+    assert abs(vir - st.vir.value) <= PCG_TOL * abs(st.vir.value)
+
+
+def test_solver_defaults(boxes):
+    m, b, M = boxes["ragged_37"]
+    with Context(m, b.nm, b.box, precision="fp64") as c:
+        assert c.get_option("dipole_solver") == 0
+        _induction(c, b)
+        assert c.get_option("dipole_solver_pcg_active") == 0
+    with Context(m, b.nm, b.box, precision="mixed") as c:
+        assert c.get_option("dipole_solver") == 2
+        _induction(c, b)
+        assert c.get_option("dipole_solver_pcg_active") == 1
+        with pytest.raises(CcpError):
+            c.set_option("dipole_solver", 3)
+
+
+def test_pcg_graph_and_host_loops_agree(boxes):
+    m, b, M = boxes["c1"]
+    out = []
+    for graph in (1, 0):
+        with Context(m, b.nm, b.box, precision="mixed") as c:
+            c.set_option("graph_loop", graph)
+            out.append(_induction(c, b))
+    assert out[0][1] == out[1][1]
+    assert rel(out[0][2], out[1][2]) <= 1e-13
+    assert abs(out[0][0] - out[1][0]) <= 1e-13 * abs(out[1][0])
+
+
+def test_pcg_maxit_reports_not_converged(boxes):
+    m, b, M = boxes["ragged_37"]
+    with Context(m, b.nm, b.box, precision="mixed") as c:
+        c.set_maxit(2)
+        with pytest.raises(CcpError) as e:
+            _induction(c, b)
+        assert e.value.code == 2
+        c.set_maxit(500)
+        e, it, *_ = _induction(c, b)  # the context stays usable
+        assert 2 < it < 500
+
+
+def test_mixed_solver_error_against_fp64(product):
+    """At the benchmark box the mixed form's dipoles (PCG to 1e-8 D RMS) stay within 1e-7 of
+    the FP64 form's (Jacobi at the reference's criterion), in fewer steps."""
+    cfg = CONFIGS["c2_512"]
+    m = Model(data_dir(cfg["variant"]))
+    b = water_box(m, cfg["nm"], cfg["box"], cfg["seed"])
+    r = {}
+    for prec in ("fp64", "mixed"):
+        with Context(m, b.nm, b.box, precision=prec) as c:
+            r[prec] = _induction(c, b)
+    assert r["mixed"][1] < r["fp64"][1]
+    assert rel(r["mixed"][2], r["fp64"][2]) <= 1e-7
+    assert rel(r["mixed"][3], r["fp64"][3]) <= 1e-7
+    assert abs(r["mixed"][0] - r["fp64"][0]) <= 1e-8 * abs(r["fp64"][0])
+
+
+@pytest.mark.parametrize("name", ["c2_512", "ragged_37"])
+def test_mixed_fs2_against_fp64(product, boxes, name):
+    """FS2 with FP32 spectator terms: its energy within 1e-6 and its COM forces within 1e-5 of
+    the FP64 kernel's; the three-body site forces and virial (FS2 and FS3 together, the
+    threebody_term outputs) within 1e-5."""
+    if name == "ragged_37":
+        m, b, _ = boxes[name]
+    else:
+        cfg = CONFIGS[name]
+        m = Model(data_dir(cfg["variant"]))
+        b = water_box(m, cfg["nm"], cfg["box"], cfg["seed"])
+    out = {}
+    for prec in ("fp64", "mixed"):
+        with Context(m, b.nm, b.box, precision=prec) as c:
+            fx, fy, fz = (np.zeros_like(b.xs) for _ in range(3))
+            c2 = [np.zeros(b.nm) for _ in range(3)]
+            c3 = [np.zeros(b.nm) for _ in range(3)]
+            vir = np.zeros(1)
+            e2, e3 = c.threebody_term(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box, fx, fy, fz, *c2,
+                                      *c3, vir)
+            out[prec] = (e2, np.stack([fx, fy, fz]), np.stack(c2), vir[0])
+    e64, F64, C64, v64 = out["fp64"]
+    emx, Fmx, Cmx, vmx = out["mixed"]
+    assert abs(emx - e64) <= 1e-6 * abs(e64), (emx, e64)
+    assert rel(Cmx, C64) <= 1e-5, rel(Cmx, C64)
+    assert rel(Fmx, F64) <= 1e-5, rel(Fmx, F64)
+    assert abs(vmx - v64) <= 1e-5 * abs(v64), (vmx, v64)
