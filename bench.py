@@ -33,6 +33,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "ns/day @512 H2O FS2+FS3: mixed vs FP64 GPU at rel force err <=1e-5; triples/s"
+# the large-box configuration (bench.py --config c5_2048), reported with the same keys
+METRIC_C5 = "ns/day @2048 H2O FS2+FS3: mixed vs FP64 GPU at rel force err <=1e-5; triples/s"
 DT_PS = 0.0005
 CONFIG = "c2_512"
 # Algorithmic work of one FS3 site-triple evaluation (energy + gradient, one SR or LR
@@ -111,10 +113,10 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def build_inputs(rank: int):
+def build_inputs(rank: int, config: str = CONFIG):
     from ccpol23_plus_2025_mbmd_b200 import Model, data_dir
     from ccpol23_plus_2025_mbmd_b200.generator import CONFIGS, water_box
-    cfg = CONFIGS[CONFIG]
+    cfg = CONFIGS[config]
     model = Model(data_dir(cfg["variant"]))
     box = water_box(model, cfg["nm"], cfg["box"], cfg["seed"] + rank)
     return model, box, cfg
@@ -201,6 +203,23 @@ def time_e2e(ctx, box, steps, warmup, flush, torch):
     h2d = 8 * (3 * nm + 3 * nm * ld)
     d2h = 8 * (3 * nm * ns + 6 * nm + 3 * nm * npol) + 8 * 16 + 4 * 5
     return times, h2d, d2h
+
+
+def time_md_steps(model, box, state, prec, steps, device, torch):
+    """Whole rigid-water NVE MD steps (2-body term + hot path + nve_1 integrator, state on
+    the device, per-step scalars back to the host) from `state`, wall-clock timed around
+    ccp_md_nve so that every host round trip of a step is inside."""
+    from ccpol23_plus_2025_mbmd_b200 import Context
+    with Context(model, box.nm, box.box, device=device, precision=prec) as ctx:
+        ctx.md_set_state(box.box, state["x"], state["y"], state["z"], state["v"], state["q"],
+                         state["j"])
+        ctx.md_nve(5, DT_PS)  # warm-up: list sizes, graphs
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = ctx.md_nve(steps, DT_PS)
+        wall = time.perf_counter() - t0
+    return {"ms_per_md_step": wall / steps * 1e3, "ns_day": ns_per_day(steps / wall),
+            "steps": steps, "ind_iters_mean": float(np.mean([s["ind_iters"] for s in st]))}
 
 
 def cpu_baseline(box, cfg, max_seconds=60.0):
@@ -460,6 +479,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", default=CONFIG, choices=[CONFIG, "c5_2048"],
+                    help="c5_2048: the same measurement on the 2048-water box (L = 39.40 A)")
+    ap.add_argument("--md-steps", type=int, default=100,
+                    help="whole NVE MD steps timed per form for the md_step keys (0: skip)")
+    ap.add_argument("--md-equil", type=int, default=200,
+                    help="velocity-rescaled FP64 steps before the md_step timing")
     ap.add_argument("--single", choices=["fp64", "mixed", "both"],
                     help="three device-resident evaluations per form, phase times of the last "
                          "(profiling; no timing loop)")
@@ -502,7 +527,7 @@ def main():
     from ccpol23_plus_2025_mbmd_b200 import Context
     from ccpol23_plus_2025_mbmd_b200.api import fma_peak_tflops, mufu_peak_tops
 
-    model, box, cfg = build_inputs(rank)
+    model, box, cfg = build_inputs(rank, args.config)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     results = {}
     with ClockSampler(local) as clk:
@@ -520,6 +545,13 @@ def main():
                 r["h2d"], r["d2h"] = h2d, d2h
                 r["fs3_isolated_ms"] = time_fs3_isolated(ctx, box, torch)
                 results[prec] = r
+        # whole MD steps of both forms from one short velocity-rescaled equilibration
+        md = {}
+        if args.md_steps > 0:
+            with Context(model, box.nm, box.box, device=local, precision="fp64") as ctx:
+                s0 = equilibrate(ctx, box, args.md_equil)
+            for prec in ("fp64", "mixed"):
+                md[prec] = time_md_steps(model, box, s0, prec, args.md_steps, local, torch)
     clocks = clk.summary()
     peak64 = fma_peak_tflops(local, "fp64")
     peak32 = fma_peak_tflops(local, "mixed")
@@ -579,18 +611,31 @@ def main():
     iso_s = results[head]["fs3_isolated_ms"] * 1e-3
     iso = FS3_FLOP_PER_SITE_TRIPLE * site_triples / iso_s / 1e12
     line = {
-        "metric": METRIC, "value": out[head]["ns_day"], "unit": "ns/day", "n_gpus": world,
+        "metric": METRIC if args.config == CONFIG else METRIC_C5,
+        "value": out[head]["ns_day"], "unit": "ns/day", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": H["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64" if head == "mixed" else "f64",
         "data": "synthetic (seeded jittered-lattice water box, 298 K)",
-        "config": {"workload": "512 H2O FS2+FS3 hot-path force evaluation (Ewald self/real/"
+        "config": {"workload": f"{box.nm} H2O FS2+FS3 hot-path force evaluation (Ewald self/real/"
                                "recip + induced-dipole solve + induction forces + FS2 + FS3)",
                    "nm": box.nm, "box_A": box.box, "variant": cfg["variant"], "seed": cfg["seed"],
                    "form": head, "l2": "flushed between timed steps (256 MB write)",
                    "parallelism": f"replicas x{world}"},
         "triples_per_s": H["triples_per_s"],
         "fp64": out["fp64"], "mixed": out["mixed"],
+        "mixed_speedup_over_fp64": {
+            "device": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+            "e2e": out["fp64"]["e2e_ms"] / out["mixed"]["e2e_ms"],
+            "fs3_isolated": out["fp64"]["fs3_isolated_ms"] / out["mixed"]["fs3_isolated_ms"]},
+        "md_step": ({**md, "workload": f"NVE MD step, {box.nm} H2O FS2+FS3: 2-body + hot path + "
+                                       "nve_1 integrator, per-step scalars to the host",
+                     "equilibration": f"{args.md_equil} FP64 steps, velocities rescaled to "
+                                      "298 K every 20 steps",
+                     "timing": "wall clock around ccp_md_nve (host round trips inside)",
+                     "mixed_speedup_over_fp64": md["fp64"]["ms_per_md_step"] /
+                                                md["mixed"]["ms_per_md_step"]}
+                    if md else None),
         "mixed_vs_fp64": {"rel_site_force_err": ferr, "rel_molecule_force_err": molerr,
                           "rel_molecule_torque_err": tqerr, "rel_fs3_com_force_err": c3err,
                           "rel_fs3_energy_err": eerr, "within_1e-5": mixed_ok},
@@ -620,11 +665,11 @@ def main():
         "clocks": clocks,
         "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32, "mufu_exp_tops": peak_mufu},
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.config == CONFIG:
         dt, cores, eo, st = cpu_baseline(box, cfg)
         line["cpu_baseline"] = {"value": ns_per_day(1.0 / dt), "unit": "ns/day", "cores": cores,
                                 "kind": "port",
-                                "sample": "1 full hot-path evaluation of the same 512-water box "
+                                "sample": f"1 full hot-path evaluation of the same {box.nm}-water box "
                                           f"({dt:.1f} s on {cores} threads; oracle built with "
                                           "gcc -O3 -fopenmp -ffp-contract=off)"}
         Fo = np.stack([st.fxs, st.fys, st.fzs])

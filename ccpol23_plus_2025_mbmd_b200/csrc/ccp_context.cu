@@ -90,6 +90,10 @@ struct ccp_context {
   // lists
   int cap = 0, tri_cap = 0, pair_cap = 0;
   int *d_nbr = nullptr, *d_ncnt = nullptr;
+  int *d_cells = nullptr;  // cell-list scratch (launch_neighbors_cells)
+  size_t cells_cap = 0;
+  int opt_cells = 1;       // cell-list neighbour search where the box allows it
+  bool cells_active = false;
   double4 *d_nbrv = nullptr;
   void *d_tri = nullptr;  // FS3 triple records
   int2 *d_pairs = nullptr;
@@ -201,7 +205,7 @@ void free_ctx(ccp_context *c) {
                 c->d_gfs3,  c->d_vdw_row, c->d_vdw_site, c->d_vdw_qq, c->d_vdw_par,
                 c->d_pcoord, c->d_md_x, c->d_md_xs, c->d_md_v, c->d_md_q, c->d_md_j, c->d_md_red,
                 c->d_mu2, c->d_e0tot, c->d_eim, c->d_T4, c->d_S4, c->d_TB, c->d_SB,
-                c->d_pcg};
+                c->d_pcg, c->d_cells};
   for (void *p : dp)
     if (p) cudaFree(p);
   if (c->h_scal) cudaFreeHost(c->h_scal);
@@ -659,9 +663,30 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                    std::min(ns, kNs3), c->d_f, 6 * nm * ns, c->d_fc2, c->d_fc3, c->d_scal,
                    c->d_icnt, st));
     const bool need_nbr = mask & (T_RSPACE | T_INDUCTION | T_FS2 | T_FS3 | T_VDW);
-    if (need_nbr)
-      LK(launch_neighbors(c->d_com, nm, box, rl * rl, c->cap, c->d_nbr, c->d_nbrv, c->d_ncnt,
-                          c->d_icnt, st));
+    if (need_nbr) {
+      // the cell-list search when the box holds 5+ cells of side >= rl/2 per axis and its
+      // kept candidates fit a block's shared memory; the all-pairs scan otherwise (same lists)
+      const int nc = c->opt_cells && (size_t)c->cap * (sizeof(double4) + sizeof(int)) <= 48 * 1024
+                         ? cell_grid(box, rl)
+                         : 0;
+      c->cells_active = nc > 0;
+      if (nc) {
+        const size_t need = cell_scratch_ints(nc, nm);
+        if (need > c->cells_cap) {
+          if (c->d_cells) cudaFree(c->d_cells);
+          c->d_cells = nullptr;
+          c->cells_cap = 0;
+          CK(dalloc(&c->d_cells, need));
+          c->cells_cap = need;
+        }
+        c->launches += 3;  // four kernels; LK counts one
+        LK(launch_neighbors_cells(c->d_com, nm, box, rl * rl, nc, c->cap, c->d_cells, c->d_nbr,
+                                  c->d_nbrv, c->d_ncnt, c->d_icnt, st));
+      } else {
+        LK(launch_neighbors(c->d_com, nm, box, rl * rl, c->cap, c->d_nbr, c->d_nbrv, c->d_ncnt,
+                            c->d_icnt, st));
+      }
+    }
     pend(0, st);
     // with the terms overlapping, the reciprocal-space branch runs on its own stream; its
     // forces go to the three-body block f3, which receives atomic additions only, while the
@@ -1368,6 +1393,8 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_graph = value != 0;
   } else if (n == "phase_matrix") {
     ctx->opt_phase = value != 0;
+  } else if (n == "cell_list") {
+    ctx->opt_cells = value != 0;
   } else if (n == "dipole_solver") {
     if (value < 0 || value > 2) {
       set_error("ccp_context_set_option: dipole_solver must be 0 (Jacobi), 1 (PCG, the "
@@ -1409,6 +1436,10 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->use_P ? 1 : 0;
   } else if (n == "dipole_solver") {
     *value = ctx->opt_solver;
+  } else if (n == "cell_list") {
+    *value = ctx->opt_cells;
+  } else if (n == "cell_list_active") {
+    *value = ctx->cells_active ? 1 : 0;
   } else if (n == "dipole_solver_pcg_active") {
     *value = ctx->pcg_active ? 1 : 0;
   } else if (n == "overlap") {
@@ -1857,9 +1888,11 @@ constexpr double kBetta = 0.007372;  // Berendsen barostat compressibility (evol
 // md.f90:169-176 and evolve.f90:1020-1052 (initialization.f90:76-89, 386-399 for the initial
 // state): energies of the last evaluation, the given kinetic energies (internal units), the
 // temperature, virial (vir + the sum f . xs in h_md[2]) and pressure over md_volm.
-void md_fill_stats(const ccp_context *ctx, double tke, double rke, ccp_md_stats &S) {
-  const ccp_energies &e = ctx->md_e;
-  const double qvir = e.vir + ctx->h_md[2];
+// `e` and `red` (the step's reductions, red[2] = sum f . xs) default to the context's last.
+void md_fill_stats(const ccp_context *ctx, double tke, double rke, ccp_md_stats &S,
+                   const ccp_energies *ep = nullptr, const double *red = nullptr) {
+  const ccp_energies &e = ep ? *ep : ctx->md_e;
+  const double qvir = e.vir + (red ? red : ctx->h_md)[2];
   S.vdwpe = e.vdwpe;
   S.cpe = e.scpe + e.rcpe + e.kcpe;
   S.indpe = e.indpe;
@@ -1998,6 +2031,12 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
   cudaStream_t st = ctx->stream;
   const double zero[3] = {0.0, 0.0, 0.0};
   const double dof_sys = 3.0 * kBoltz * (2.0 * ctx->nm - 1.0);
+  // NVE steps without an equilibration rescale take no host decision from their kinetic
+  // energies: a step's reductions are copied without a synchronisation, and its statistics
+  // are filled after the next step's evaluation, whose own synchronisation covers the copy
+  int pend = -1;
+  ccp_energies pend_e{};
+  const double *pend_red = nullptr;
   for (int k = 0; k < nsteps; k++) {
     double scale = 1.0;
     if (kind == CCP_MD_NPT_B) {
@@ -2042,6 +2081,21 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
     CK(launch_md_stage2(ctx->nm, ns, ctx->d_f, ctx->d_fc2, ctx->d_fc3, xs, xs + nsi, xs + 2 * nsi,
                         x, x + nm, x + 2 * nm, v, q, jv, ctx->pmi, ctx->totm, dt, ctx->md_box,
                         (kind == CCP_MD_NVE || kind == CCP_MD_NVT_H) ? 1 : 0, ctx->d_md_red, st));
+    if (pend >= 0) {  // the previous step's copy completed in this step's evaluation
+      if (stats) {
+        const double *r0 = pend_red;
+        md_fill_stats(ctx, 0.5 * ctx->totm * r0[0], 0.5 * r0[1], stats[pend], &pend_e, r0);
+      }
+      pend = -1;
+    }
+    if (kind == CCP_MD_NVE && ctx->md_eq_left == 0) {
+      double *slot = ctx->h_md + 16 + 8 * (k & 1);  // h_md holds >= 39 doubles (nm >= 3)
+      CK(cudaMemcpyAsync(slot, ctx->d_md_red, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
+      pend = k;
+      pend_e = ctx->md_e;
+      pend_red = slot;
+      continue;
+    }
     CK(cudaMemcpyAsync(ctx->h_md, ctx->d_md_red, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const double *h = ctx->h_md;
@@ -2130,6 +2184,12 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
     CK(launch_md_scale(ctx->nm, v, c, chit, jv, chit, st));
     if (kind == CCP_MD_NPT_B) CK(launch_md_wrap(ctx->nm, x, x + nm, x + 2 * nm, ctx->md_box, st));
     if (stats) md_fill_stats(ctx, chit * chit * tke, chit * chit * rke, stats[k]);
+  }
+  if (pend >= 0) {
+    CK(cudaStreamSynchronize(st));
+    if (stats)
+      md_fill_stats(ctx, 0.5 * ctx->totm * pend_red[0], 0.5 * pend_red[1], stats[pend], &pend_e,
+                    pend_red);
   }
   return CCP_OK;
 }

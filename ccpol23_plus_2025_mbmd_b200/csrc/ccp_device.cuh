@@ -230,6 +230,15 @@ cudaError_t launch_prep(const double *x, const double *y, const double *z, const
                         int *icnt, cudaStream_t st);
 cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
                              int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st);
+// Cell-list form of launch_neighbors (same lists): cells per axis for a box and list radius
+// (0 when the box holds fewer than six cells of side >= rlist/2 per axis, or more than
+// kMaxCellsPerAxis), the int scratch it needs, and the launcher.
+constexpr int kMaxCellsPerAxis = 64;
+int cell_grid(double box, double rlist);
+size_t cell_scratch_ints(int nc, int nm);
+cudaError_t launch_neighbors_cells(const double4 *com, int nm, double box, double rlist2,
+                                   int nc, int cap, int *scratch, int *nbr, double4 *nbrv,
+                                   int *ncnt, int *icnt, cudaStream_t st);
 cudaError_t launch_pair_static(const double *x, const double *y, const double *z,
                                const double *xs, const double *ys, const double *zs, int ld,
                                const double4 *act, const int *nbr, const double4 *nbrv,

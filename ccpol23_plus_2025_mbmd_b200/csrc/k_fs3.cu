@@ -118,9 +118,15 @@ __global__ void k_fs3_enum(const double4 *__restrict__ comb, const int *__restri
   }
   const int L = nl;
   const double b = P.boxb;
-  for (int t = threadIdx.x; t < L * L; t += blockDim.x) {
-    const int a = t / L, c = t % L;
-    if (c <= a) continue;
+  // the pairs a < c of the staged candidates, by their index in row-major upper-triangle
+  // order: row a starts at a L - a (a + 1) / 2
+  const int npairs = L * (L - 1) / 2;
+  for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
+    const double h = 2.0 * L - 1.0;
+    int a = (int)floor(0.5 * (h - sqrt(h * h - 8.0 * t)));
+    while (a > 0 && a * L - a * (a + 1) / 2 > t) a--;
+    while ((a + 1) * L - (a + 1) * (a + 2) / 2 <= t) a++;
+    const int c = t - (a * L - a * (a + 1) / 2) + a + 1;
     const int j = lj[a], k = lj[c];
     const double4 cj = comb[j], ck = comb[k];
     const double dxik = xsub(ci.x, ck.x), dyik = xsub(ci.y, ck.y), dzik = xsub(ci.z, ck.z);

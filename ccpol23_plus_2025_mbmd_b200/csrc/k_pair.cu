@@ -99,6 +99,132 @@ __global__ void k_neighbors(const double4 *__restrict__ com, int nm, double box,
   }
 }
 
+// ------------------------------------------------------------ cell-list neighbours
+// For boxes of at least five cells of side >= rlist/2 per axis: molecules are binned by their
+// wrapped centre, and molecule i's candidates are the members of the 5 x 5 x 5 cells around
+// its own (two cells of side >= rlist/2 on either side cover every centre within rlist under
+// the minimum image, and five distinct cells per axis visit none twice).  Each candidate gets
+// the same exact minimum-image test as in k_neighbors, and the kept ones are written in
+// increasing j, so the list equals k_neighbors' entry for entry.
+constexpr int kStencil = 125;
+
+__device__ __forceinline__ int cell_axis(double x, double box, double side, int nc) {
+  const double p = x - box * floor(x / box);
+  int c = (int)(p / side);
+  return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+}
+
+__global__ void k_cell_assign(const double4 *__restrict__ com, int nm, double box, int nc,
+                              int *cell_of, int *count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nm) return;
+  const double side = box / nc;
+  const double4 c = com[i];
+  const int cell = (cell_axis(c.z, box, side, nc) * nc + cell_axis(c.y, box, side, nc)) * nc +
+                   cell_axis(c.x, box, side, nc);
+  cell_of[i] = cell;
+  atomicAdd(&count[cell], 1);
+}
+
+// One block: exclusive scan of the cell counts into start[0..ncells] and cursor[0..ncells).
+__global__ void __launch_bounds__(1024) k_cell_scan(int ncells, const int *__restrict__ count,
+                                                    int *start, int *cursor) {
+  __shared__ int part[1024];
+  const int per = (ncells + 1023) / 1024;
+  const int c0 = min(ncells, (int)threadIdx.x * per), c1 = min(ncells, c0 + per);
+  int sum = 0;
+  for (int c = c0; c < c1; c++) sum += count[c];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const int v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int o = part[threadIdx.x] - sum;
+  for (int c = c0; c < c1; c++) {
+    start[c] = o;
+    cursor[c] = o;
+    o += count[c];
+  }
+  if (threadIdx.x == 1023) start[ncells] = part[1023];
+}
+
+__global__ void k_cell_fill(int nm, const int *__restrict__ cell_of, int *cursor, int *members) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nm) members[atomicAdd(&cursor[cell_of[i]], 1)] = i;
+}
+
+// One block per molecule i; dynamic shared memory holds up to `cap` kept candidates.
+__global__ void k_neighbors_cells(const double4 *__restrict__ com, int nm, double box,
+                                  double rlist2, int cap, int nc, const int *__restrict__ cell_of,
+                                  const int *__restrict__ start, const int *__restrict__ members,
+                                  int *nbr, double4 *nbrv, int *ncnt, int *icnt) {
+  extern __shared__ unsigned char smem_raw[];
+  double4 *kv = reinterpret_cast<double4 *>(smem_raw);
+  int *kj = reinterpret_cast<int *>(kv + cap);
+  __shared__ int cs[kStencil], pre[kStencil + 1];
+  __shared__ int nkept;
+  const int i = blockIdx.x;
+  const int t = threadIdx.x;
+  const int c = cell_of[i];
+  if (t < kStencil) {
+    const int cx = c % nc, cy = (c / nc) % nc, cz = c / (nc * nc);
+    const int dx = t % 5 - 2, dy = (t / 5) % 5 - 2, dz = t / 25 - 2;
+    const int cell = (((cz + dz + nc) % nc) * nc + (cy + dy + nc) % nc) * nc + (cx + dx + nc) % nc;
+    cs[t] = start[cell];
+    pre[t + 1] = start[cell + 1] - start[cell];
+  }
+  if (t == 0) {
+    nkept = 0;
+    pre[0] = 0;
+  }
+  __syncthreads();
+  if (t == 0)
+    for (int k = 0; k < kStencil; k++) pre[k + 1] += pre[k];
+  __syncthreads();
+  const int total = pre[kStencil];
+  const double4 ci = com[i];
+  for (int e = t; e < total; e += blockDim.x) {
+    int lo = 0, hi = kStencil;  // pre[lo] <= e < pre[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (pre[mid] <= e)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    const int j = members[cs[lo] + (e - pre[lo])];
+    if (j == i) continue;
+    const double4 cj = com[j];
+    const double xcc = minimg(xsub(ci.x, cj.x), box);
+    const double ycc = minimg(xsub(ci.y, cj.y), box);
+    const double zcc = minimg(xsub(ci.z, cj.z), box);
+    const double r2 = norm2x(xcc, ycc, zcc);
+    if (!(r2 < rlist2)) continue;
+    const int pos = atomicAdd(&nkept, 1);
+    if (pos < cap) {
+      kj[pos] = j;
+      kv[pos] = make_double4(xcc, ycc, zcc, r2);
+    }
+  }
+  __syncthreads();
+  const int n = nkept, m = n < cap ? n : cap;
+  // rank of each kept j among the kept (the j are distinct): increasing j
+  for (int e = t; e < m; e += blockDim.x) {
+    const int j = kj[e];
+    int r = 0;
+    for (int q = 0; q < m; q++) r += kj[q] < j;
+    nbr[(size_t)i * cap + r] = j;
+    nbrv[(size_t)i * cap + r] = kv[e];
+  }
+  if (t == 0) {
+    ncnt[i] = m;
+    if (n > cap) atomicMax(&icnt[C_OVERFLOW], n);
+  }
+}
+
 // ------------------------------------------- Ewald real space + static field (real+TT)
 // rspace_ewald (ewald.f90:177-405), rspace_efield_stat (nb_induction_model.f90:128-293),
 // shortrange_efield_stat_damped (nb_induction_model.f90:5454-5629) and, with `with_self`,
@@ -608,6 +734,36 @@ cudaError_t launch_prep(const double *x, const double *y, const double *z, const
 cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
                              int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st) {
   k_neighbors<<<nm, 128, 0, st>>>(com, nm, box, rlist2, cap, nbr, nbrv, ncnt, icnt);
+  return cudaGetLastError();
+}
+
+int cell_grid(double box, double rlist) {
+  // five cells per axis are the minimum for distinct stencil cells, and at five the stencil
+  // spans the whole box, so the cells pay from six on
+  const int nc = (int)floor(2.0 * box / rlist);
+  return nc >= 6 && nc <= kMaxCellsPerAxis ? nc : 0;
+}
+
+size_t cell_scratch_ints(int nc, int nm) {
+  const size_t ncells = (size_t)nc * nc * nc;
+  return 3 * ncells + 1 + 2 * (size_t)nm;
+}
+
+cudaError_t launch_neighbors_cells(const double4 *com, int nm, double box, double rlist2,
+                                   int nc, int cap, int *scratch, int *nbr, double4 *nbrv,
+                                   int *ncnt, int *icnt, cudaStream_t st) {
+  const int ncells = nc * nc * nc;
+  int *count = scratch, *cursor = count + ncells, *start = cursor + ncells;
+  int *cell_of = start + ncells + 1, *members = cell_of + nm;
+  cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int) * ncells, st);
+  if (e != cudaSuccess) return e;
+  const int nb = (nm + 255) / 256;
+  k_cell_assign<<<nb, 256, 0, st>>>(com, nm, box, nc, cell_of, count);
+  k_cell_scan<<<1, 1024, 0, st>>>(ncells, count, start, cursor);
+  k_cell_fill<<<nb, 256, 0, st>>>(nm, cell_of, cursor, members);
+  const size_t smem = (size_t)cap * (sizeof(double4) + sizeof(int));
+  k_neighbors_cells<<<nm, 128, smem, st>>>(com, nm, box, rlist2, cap, nc, cell_of, start, members,
+                                           nbr, nbrv, ncnt, icnt);
   return cudaGetLastError();
 }
 

@@ -65,3 +65,25 @@ def test_relabelling_invariance(box):
     F1, C1 = _forces(r1)
     assert rel(F1, F0[:, perm]) <= 1e-9
     assert rel(C1, C0[:, perm]) <= 1e-9
+
+
+def test_cell_list_matches_all_pairs(product):
+    """At 2048 waters the neighbour lists come from the cell-list search; with it switched off
+    the all-pairs scan must give the same lists, hence the same triples, pairs, iteration
+    count and results (atomic summation order aside)."""
+    cfg = CONFIGS["c5_2048"]
+    m = Model(data_dir(cfg["variant"]))
+    b = water_box(m, cfg["nm"], cfg["box"], cfg["seed"])
+    out = {}
+    for cells in (1, 0):
+        with Context(m, b.nm, b.box) as c:
+            c.set_option("cell_list", cells)
+            out[cells] = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+            assert c.get_option("cell_list_active") == cells
+    e1, e0 = out[1].energies, out[0].energies
+    for k in ("ind_iters", "n_fs3_triples", "n_fs3_blend", "n_fs2_triples"):
+        assert e1[k] == e0[k], k
+    for k in ENERGIES:
+        assert e1[k] == pytest.approx(e0[k], rel=1e-12), k
+    for a, c in zip(_forces(out[1]), _forces(out[0])):
+        assert rel(a, c) <= 1e-12
