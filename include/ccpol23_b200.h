@@ -37,8 +37,10 @@ extern "C" {
 /* precision forms of a context */
 #define CCP_FP64 0   /* plain FP64 everywhere */
 #define CCP_MIXED 1  /* FP32 for two of the three FS3 gradient passes (the ik and jk
-                        pair families); FP64 for the FS3 site-pair tables, its energy pass,
-                        FS2, Ewald, induction and all sums */
+                        pair families) and for FS2's spectator terms; the induced dipoles
+                        by preconditioned conjugate gradients in FP64 to 1e-8 D RMS (option
+                        "dipole_solver"); FP64 for the FS3 site-pair tables and energy pass,
+                        Ewald, the induction fields and forces, and all sums */
 
 typedef struct ccp_model ccp_model;
 typedef struct ccp_context ccp_context;
@@ -52,7 +54,7 @@ typedef struct ccp_energies {
     double fs2pe;     /* FS2 three-body */
     double fs3pe;     /* FS3 three-body */
     double vir;       /* virial added by these terms (internal units) */
-    int ind_iters;    /* Jacobi iterations taken */
+    int ind_iters;    /* dipole-solve steps taken (Jacobi iterations, or PCG steps) */
     int n_fs3_triples;    /* molecular triples inside the FS3 cut-off */
     int n_fs3_blend;      /* of which in the SR/LR switching region */
     int n_fs2_triples;    /* (spectator, pair) combinations inside the FS2 cut-off */
@@ -390,9 +392,19 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
      "phase_matrix"  1 (default): the polarisable sites' phases are tabulated once per
                      evaluation as exp(i(l x + m y)) and exp(i n z) factors (when they take at
                      most 1 GiB), so a (site, k) phase is one complex product; 0: never (the
-                     tiled on-the-fly reciprocal kernels run every iteration).
+                     tiled on-the-fly reciprocal kernels run every iteration);
+     "dipole_solver" 0 (CCP_FP64 default): the reference's Jacobi iteration and criterion
+                     (sum |dmu|^2 < 1e-20 e^2 A^2); 1: preconditioned conjugate gradients
+                     (preconditioner diag(alpha), so the convergence quantity is the Jacobi
+                     update at the iterate) to the same criterion; 2 (CCP_MIXED default): PCG
+                     to an RMS update of 1e-8 D per polarisable site.  PCG needs the phase
+                     table; without it the solve is Jacobi.  ind_iters then counts PCG steps;
+     "cell_list"     1 (default): the neighbour lists come from a cell list when the box holds
+                     six or more cells of half the list radius per axis (the same lists as the
+                     all-pairs scan); 0: always the all-pairs scan.
    ccp_context_get_option also reports "phase_matrix_active" (whether the last evaluation
-   used the table). */
+   used the table), "dipole_solver_pcg_active" (whether its dipole solve was PCG) and
+   "cell_list_active" (whether its neighbour lists came from the cell list). */
 int ccp_context_set_option(ccp_context *ctx, const char *name, int value);
 int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value);
 
