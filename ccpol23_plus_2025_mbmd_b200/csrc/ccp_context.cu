@@ -172,6 +172,8 @@ struct ccp_context {
   // back to Jacobi (at the reference's criterion) without them
   int opt_solver = 0;
   double dip_tol_debye = 1e-8;
+  int opt_pdl = 1;  // the dipole-step kernels with programmatic dependent launch
+  int opt_fs3_low = 1;  // mixed form: FS3's ik/jk gradient passes in FP32 (0: all FP64)
   bool pcg_active = false;  // the solver of the last solve was PCG
   // phase timing (diagnostics)
   bool timing = false;
@@ -415,6 +417,7 @@ IterArgs make_iter_args(ccp_context *c, cudaGraphConditionalHandle handle, int u
   A.state = c->d_istate;
   A.ticket = c->d_ticket;
   A.thr = ind_threshold(c);
+  A.pdl = c->opt_pdl;
   if (pcg_solver(c)) {
     const size_t np3 = (size_t)A.nw * 3;
     A.cu = c->d_pcg;
@@ -469,7 +472,8 @@ int ensure_ind_graph(ccp_context *c) {
       (long long)c->d_kg,
       (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
       (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit,
-      (long long)pcg_solver(c), (long long)c->opt_solver, (long long)c->d_pcg};
+      (long long)pcg_solver(c), (long long)c->opt_solver, (long long)c->d_pcg,
+      (long long)c->opt_pdl};
   double thr = ind_threshold(c);
   long long thr_bits;
   std::memcpy(&thr_bits, &thr, sizeof thr_bits);
@@ -713,7 +717,8 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                          c->d_icnt, s3));
       pend(7, s3);
       pbeg(8, s3);
-      LK(launch_fs3(c->precision, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
+      const int fs3_prec = c->precision == CCP_MIXED && c->opt_fs3_low ? CCP_MIXED : CCP_FP64;
+      LK(launch_fs3(fs3_prec, c->d_tri, c->d_icnt, c->tri_cap, c->d_s17, c->d_coef, c->d_bgr,
                     nm, ns, f3, c->d_fc3, c->d_scal, c->nsm, side ? c->opt_fs3_tpb : 0,
                     side ? c->opt_fs3_bps : 0, gfs3,
                     s3));
@@ -1395,6 +1400,10 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_phase = value != 0;
   } else if (n == "cell_list") {
     ctx->opt_cells = value != 0;
+  } else if (n == "pdl") {
+    ctx->opt_pdl = value != 0;
+  } else if (n == "fs3_fp32_passes") {
+    ctx->opt_fs3_low = value != 0;
   } else if (n == "dipole_solver") {
     if (value < 0 || value > 2) {
       set_error("ccp_context_set_option: dipole_solver must be 0 (Jacobi), 1 (PCG, the "
@@ -1438,6 +1447,10 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_solver;
   } else if (n == "cell_list") {
     *value = ctx->opt_cells;
+  } else if (n == "pdl") {
+    *value = ctx->opt_pdl;
+  } else if (n == "fs3_fp32_passes") {
+    *value = ctx->opt_fs3_low;
   } else if (n == "cell_list_active") {
     *value = ctx->cells_active ? 1 : 0;
   } else if (n == "dipole_solver_pcg_active") {

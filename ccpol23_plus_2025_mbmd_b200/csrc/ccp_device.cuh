@@ -28,6 +28,21 @@ __device__ __forceinline__ double norm2x(double x, double y, double z) {
   return xadd(xadd(xmul(x, x), xmul(y, y)), xmul(z, z));
 }
 
+// Compensated FP64 accumulator (Neumaier's variant of Kahan summation: the rounding error of
+// every addition is carried in c, whichever operand is larger).  Used for the per-thread and
+// per-block energy and virial sums of the three-body kernels, whose terms come in with both
+// signs and magnitudes far above their sum.
+struct CompSum {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double x) {
+    const double t = __dadd_rn(s, x);
+    c = __dadd_rn(c, fabs(s) >= fabs(x) ? __dadd_rn(__dsub_rn(s, t), x)
+                                        : __dadd_rn(__dsub_rn(x, t), s));
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return __dadd_rn(s, c); }
+};
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -164,6 +179,9 @@ struct IterArgs {
   // preconditioned conjugate gradients (k_iter.cu): the vectors u (preconditioned residual),
   // w = A u, s = A p and p of every polarisable site component; mu holds the iterate x
   double *cu, *cw, *cs, *cp;
+  // launch the two kernels of a step with programmatic dependent launch: each lets the next
+  // kernel's blocks launch early and waits for its predecessor's results itself
+  int pdl;
 };
 
 // Slots of the dipole solve's state array (doubles).

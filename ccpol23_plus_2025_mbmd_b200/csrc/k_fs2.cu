@@ -125,7 +125,8 @@ __global__ void __launch_bounds__(128, 4)
   const double E = warp_sum(eq), Ev = warp_sum(evq);
   const double conv = kH2kcal * 418.4 / kBohr2a;
   const size_t nfs = (size_t)nm * ns;
-  double e_loc = 0.0, v_loc = 0.0, A_loc = 0.0;
+  CompSum e_loc, v_loc;  // this lane's energy and virial over its spectators
+  double A_loc = 0.0;
   double Ci[3] = {0, 0, 0}, Cj[3] = {0, 0, 0};
   int nspec = 0;
   // One spectator k that passed both cut-offs: its five 3-body charges against the pair's
@@ -174,10 +175,10 @@ __global__ void __launch_bounds__(128, 4)
       const double dkcj3i = dkcj1i * dkcj1i * dkcj1i;
       const double term0 = dkci1i + dkcj1i - dkqi1i - dkqj1i;
       const double qE = qks * E;
-      e_loc += qE * term0 * fl;
+      e_loc.add(qE * term0 * fl);
       const double termxy1 = (dxkqi * xij + dykqi * yij + dzkqi * zij) * g3 * dij1i * dkqi3i;
       const double termxy2 = (dxkqj * xij + dykqj * yij + dzkqj * zij) * g3 * dij1i * dkqj3i;
-      v_loc += (qks * Ev + (dflrkiv + dflrkjv) * qE) * term0 * fl + qE * (termxy1 - termxy2) * fl;
+      v_loc.add((qks * Ev + (dflrkiv + dflrkjv) * qE) * term0 * fl + qE * (termxy1 - termxy2) * fl);
       A_loc += qks * term0 * fl;
       const double dotkqi = xij * dxkqi + yij * dykqi + zij * dzkqi;
       const double dotkqj = xij * dxkqj + yij * dykqj + zij * dzkqj;
@@ -296,8 +297,8 @@ __global__ void __launch_bounds__(128, 4)
       cjy += -fyj * fl + tkj * kjy;
       cjz += -fzj * fl + tkj * kjz;
     }
-    e_loc += (double)e_s;
-    v_loc += (double)v_s;
+    e_loc.add((double)e_s);
+    v_loc.add((double)v_s);
     A_loc += (double)a_s;
     Ci[0] += (double)cix;
     Ci[1] += (double)ciy;
@@ -353,8 +354,7 @@ __global__ void __launch_bounds__(128, 4)
     nq = nq > 32 ? nq - 32 : 0;
     __syncwarp();
   }
-  e_loc = warp_sum(e_loc);
-  v_loc = warp_sum(v_loc);
+  const double e_w = warp_sum(e_loc.value()), v_w = warp_sum(v_loc.value());
   A_loc = warp_sum(A_loc);
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -377,8 +377,8 @@ __global__ void __launch_bounds__(128, 4)
       atomicAdd(&fc2[c * nm + i], Ci[c] * conv);
       atomicAdd(&fc2[c * nm + j], Cj[c] * conv);
     }
-    atomicAdd(&scal[S_FS2_E], e_loc);
-    atomicAdd(&scal[S_FS2_VIR], v_loc);
+    atomicAdd(&scal[S_FS2_E], e_w);
+    atomicAdd(&scal[S_FS2_VIR], v_w);
   }
   for (int o = 16; o > 0; o >>= 1) nspec += __shfl_xor_sync(0xffffffffu, nspec, o);
   if (lane == 0 && nspec) atomicAdd(ncomb, nspec);

@@ -211,7 +211,7 @@ template <typename T>
 struct Fs3Smem {
   double coef[2][kCoefT];    // SR, LR coefficients, strided layout (kSi, kSj, kSk)
   double bgr[2][3][kPairs];  // SR, LR b, g, r0 of each site pair
-  double site[3][kNs3][3];   // site offsets (bohr) of i, j, k
+  double site[3][3][kNs3][3];  // site offsets (bohr) of i, j, k, per staging slot
   double2 uu[3][kP][kRS];    // (e, e d) of each site pair, families ij, ik, jk
   // force weights of each site pair: with P = q0 + d q1 the passes' output and l = d ln e / dr,
   // the weight G = e (l P + q1) / d is (e l / d) q0 + (e l + e / d) q1, so the table holds
@@ -219,9 +219,9 @@ struct Fs3Smem {
   // form keeps (d, l)
   double2 dl[3][kP][kRS];
   LowUU<T> uul;              // FP32 copy of uu (mixed form)
-  double G[3][kP][kRS];      // accumulated site-force weights
+  double G[2][3][kP][kRS];   // accumulated site-force weights, two triples in flight
   double red[kFs3Block / 32];
-  Fs3Rec rec;
+  Fs3Rec rec[3];             // staging slots: previous, current and next triple
 };
 
 // Extra shared memory of the parameter-gradient form: this block's partial sums of
@@ -343,47 +343,58 @@ __device__ __forceinline__ void fs3_pass(const typename Vec2<T>::type *U,
   }
 }
 
-// One SR (v = 0) or LR (v = 1) sweep of the current triple: tabulate the site pairs, run
-// the three gradient passes, store (first sweep of the triple) or add wsite * G into S.G and
-// return the energy sum.  With keep_ij the ij family's tables already hold this molecule
-// pair and variant (the previous sweep of the block had them) and are not tabulated again.
+// The pair phase of one SR (v = 0) or LR (v = 1) sweep of the triple in staging slot `sl`:
+// tabulate (e, e d) and the force-weight factors of its site pairs.  With keep_ij the ij
+// family's tables already hold this molecule pair and variant (the previous sweep of the
+// block had them) and are not tabulated again.  No barrier: the caller adds it.
 template <typename T, bool GRAD>
-__device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite, bool first,
-                              bool keep_ij) {
+__device__ __forceinline__ void fs3_pairs(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, int sl,
+                                          bool keep_ij) {
   constexpr bool kLow = sizeof(T) == 4;
   const int tid = threadIdx.x;
-  if (tid < kPairs) {
-    const int a = tid / kNs3, b = tid % kNs3;
-    const double bb = S.bgr[v][0][tid], gg = S.bgr[v][1][tid], r0 = S.bgr[v][2][tid];
+  if (tid >= kPairs) return;
+  const Fs3Rec &R = S.rec[sl];
+  const double(*site)[kNs3][3] = S.site[sl];
+  const int a = tid / kNs3, b = tid % kNs3;
+  const double bb = S.bgr[v][0][tid], gg = S.bgr[v][1][tid], r0 = S.bgr[v][2][tid];
 #pragma unroll 1
-    for (int p = keep_ij ? 1 : 0; p < 3; p++) {
-      const int m1 = p == 2 ? 1 : 0, m2 = p == 0 ? 1 : 2;
-      const double vx = S.rec.cv[p][0] + (S.site[m1][a][0] - S.site[m2][b][0]);
-      const double vy = S.rec.cv[p][1] + (S.site[m1][a][1] - S.site[m2][b][1]);
-      const double vz = S.rec.cv[p][2] + (S.site[m1][a][2] - S.site[m2][b][2]);
-      const double r = sqrt(vx * vx + vy * vy + vz * vz);
-      const double ex = exp(-gg * (r - r0));
-      double2 u;
-      if constexpr (GRAD) {
-        const double damp = 1.0 / (1.0 + ex);
-        const double e = exp(-bb * r) * damp;
-        u = make_double2(e, e * r);
-        S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(r, -bb + gg * ex * damp);
-        GS->exd[p][sp(pidx(a))][sp(pidx(b))] = ex * damp;
-      } else {
-        // one division gives both the damping 1/(1+x) and 1/r
-        const double t = 1.0 / ((1.0 + ex) * r);
-        const double eor = exp(-bb * r) * t;  // e / r
-        const double e = eor * r;
-        const double dln = -bb + gg * ex * (t * r);
-        u = make_double2(e, e * r);
-        S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(eor * dln, e * dln + eor);
-      }
-      S.uu[p][sp(pidx(a))][sp(pidx(b))] = u;
-      if constexpr (kLow) S.uul.v[p][sp(pidx(a))][sp(pidx(b))] = make_float2((float)u.x, (float)u.y);
+  for (int p = keep_ij ? 1 : 0; p < 3; p++) {
+    const int m1 = p == 2 ? 1 : 0, m2 = p == 0 ? 1 : 2;
+    const double vx = R.cv[p][0] + (site[m1][a][0] - site[m2][b][0]);
+    const double vy = R.cv[p][1] + (site[m1][a][1] - site[m2][b][1]);
+    const double vz = R.cv[p][2] + (site[m1][a][2] - site[m2][b][2]);
+    const double r = sqrt(vx * vx + vy * vy + vz * vz);
+    const double ex = exp(-gg * (r - r0));
+    double2 u;
+    if constexpr (GRAD) {
+      const double damp = 1.0 / (1.0 + ex);
+      const double e = exp(-bb * r) * damp;
+      u = make_double2(e, e * r);
+      S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(r, -bb + gg * ex * damp);
+      GS->exd[p][sp(pidx(a))][sp(pidx(b))] = ex * damp;
+    } else {
+      // one division gives both the damping 1/(1+x) and 1/r
+      const double t = 1.0 / ((1.0 + ex) * r);
+      const double eor = exp(-bb * r) * t;  // e / r
+      const double e = eor * r;
+      const double dln = -bb + gg * ex * (t * r);
+      u = make_double2(e, e * r);
+      S.dl[p][sp(pidx(a))][sp(pidx(b))] = make_double2(eor * dln, e * dln + eor);
     }
+    S.uu[p][sp(pidx(a))][sp(pidx(b))] = u;
+    if constexpr (kLow) S.uul.v[p][sp(pidx(a))][sp(pidx(b))] = make_float2((float)u.x, (float)u.y);
   }
-  __syncthreads();
+}
+
+// The three gradient passes of the sweep whose tables the pair phase wrote: store (first
+// sweep of the triple) or add wsite * G into the force-weight buffer G, and return the
+// sweep's energy sum to every thread.  Ends with a barrier.
+template <typename T, bool GRAD>
+__device__ __forceinline__ double fs3_passes(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v,
+                                             double wsite, bool first,
+                                             double (*G)[kP][kRS]) {
+  constexpr bool kLow = sizeof(T) == 4;
+  const int tid = threadIdx.x;
   double esum = 0.0;
   const int fam = tid / kPassThreads, lt = tid % kPassThreads;
   // 2x2 output tiles (R, C) of the 9 x 9 grid by quarter-warp: quarters 0..8 take row R and
@@ -424,16 +435,16 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
         }
         const double gw = wsite * (w.x * q0[o] + w.y * q1[o]);
         if (first)
-          S.G[fam][r][c] = gw;
+          G[fam][r][c] = gw;
         else
-          S.G[fam][r][c] += gw;
+          G[fam][r][c] += gw;
         continue;
       }
       const double2 u = S.uu[fam][r][c];
       const double P = q0[o] + w.x * q1[o];
       if (fam == 0) esum += u.x * P;
       const double gw = wsite * (u.x * (w.y * P + q1[o]) / w.x);
-      S.G[fam][r][c] = first ? gw : S.G[fam][r][c] + gw;
+      G[fam][r][c] = first ? gw : G[fam][r][c] + gw;
       const int ra = r0 + (o >> 1), cb = c0 + (o & 1);
       if (GRAD && ra != 1 && cb != 1) {
         // dS/de_ab = P; de/db = -r e, de/dg = (r - r0) e x, de/dr0 = -g e x with
@@ -458,7 +469,121 @@ __device__ double fs3_variant(Fs3Smem<T> &S, Fs3Grad<T> *GS, int v, double wsite
   return tot;
 }
 
+// Stages the record and site offsets of triple t into slot sl: threads [kPairs, kFs3Block),
+// which the pair phase leaves idle, copy the record and the 3 x 17 site offsets.
+template <typename T>
+__device__ __forceinline__ void fs3_stage(Fs3Smem<T> &S, const Fs3Rec *__restrict__ recs,
+                                          const double4 *__restrict__ s17, int t, int sl) {
+  const int u = (int)threadIdx.x - kPairs;
+  if (u < 0) return;
+  constexpr int kStagers = kFs3Block - kPairs;
+  if (u < kRecWords)
+    reinterpret_cast<double *>(&S.rec[sl])[u] = reinterpret_cast<const double *>(recs + t)[u];
+  for (int k = u; k < 3 * kNs3; k += kStagers) {
+    const int m = k / kNs3, s = k % kNs3;
+    const double4 o = s17[(size_t)recs[t].mol[m] * kNs3 + s];
+    S.site[sl][m][s][0] = o.x;
+    S.site[sl][m][s][1] = o.y;
+    S.site[sl][m][s][2] = o.z;
+  }
+}
+
+// Site forces of the triple in slot sl from its force weights G (F = -sum_partner G * pair
+// vector; 4 lanes per (molecule, site), each summing a quarter of the 17 partners, reduced
+// with shuffles), the R_avg damping/switch COM forces (threebody_potential.f90:1092-1120,
+// weight comc, by the block's last thread) and the triple's virial; returns this thread's
+// share of the virial.
+template <typename T>
+__device__ __forceinline__ double fs3_forces(const Fs3Smem<T> &S, int sl,
+                                             const double (*G)[kP][kRS], double comc, int nm,
+                                             int ns, double *f, double *fc3) {
+  const int tid = threadIdx.x;
+  const double conv = kH2kcal * 418.4 / kBohr2a;
+  const size_t nfs = (size_t)nm * ns;
+  const Fs3Rec &R = S.rec[sl];
+  const double(*site)[kNs3][3] = S.site[sl];
+  double vsite = 0.0;
+  {
+    const int item = tid >> 2, part = tid & 3;
+    const bool act = item < 3 * kNs3;
+    const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = sp(pidx(s));
+    const double(*cv)[3] = R.cv;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    // the item's two pair families ("links"): family, whether this molecule is the second
+    // of the family's pair (then the weight is G[partner][this] and the pair vector points
+    // from the partner's site), the partner molecule; the virial counts each molecular
+    // pair once (ij and ik from molecule i, jk from molecule j)
+    const int fa = m == 2 ? 1 : 0, fb = m == 0 ? 1 : 2;
+    const bool ta = m != 0, tb = m == 2;
+    const int pa = m == 0 ? 1 : 0, pb = m == 2 ? 1 : 2;
+    const double sga = ta ? -1.0 : 1.0, sgb = tb ? -1.0 : 1.0;
+    const double wva = m == 0 ? 1.0 : 0.0, wvb = m != 2 ? 1.0 : 0.0;
+    if (act) {
+      const double x0 = site[m][s][0], x1 = site[m][s][1], x2 = site[m][s][2];
+      const double *ga_row = &G[fa][0][0], *gb_row = &G[fb][0][0];
+#pragma unroll 1
+      for (int o = part; o < kNs3; o += 4) {
+        const int po = sp(pidx(o));
+        const double ga = ga_row[ta ? po * kRS + ps : ps * kRS + po];
+        const double gb = gb_row[tb ? po * kRS + ps : ps * kRS + po];
+        // (this - partner) site offsets, negated for a transposed link: exact
+        const double a0 = cv[fa][0] + sga * (x0 - site[pa][o][0]);
+        const double a1 = cv[fa][1] + sga * (x1 - site[pa][o][1]);
+        const double a2 = cv[fa][2] + sga * (x2 - site[pa][o][2]);
+        const double b0 = cv[fb][0] + sgb * (x0 - site[pb][o][0]);
+        const double b1 = cv[fb][1] + sgb * (x1 - site[pb][o][1]);
+        const double b2 = cv[fb][2] + sgb * (x2 - site[pb][o][2]);
+        const double sa = sga * ga, sb = sgb * gb;
+        fx -= sa * a0 + sb * b0;
+        fy -= sa * a1 + sb * b1;
+        fz -= sa * a2 + sb * b2;
+        vsite += wva * ga * (a0 * a0 + a1 * a1 + a2 * a2) + wvb * gb * (b0 * b0 + b1 * b1 + b2 * b2);
+      }
+    }
+#pragma unroll
+    for (int off = 1; off < 4; off <<= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, off);
+      fy += __shfl_xor_sync(0xffffffffu, fy, off);
+      fz += __shfl_xor_sync(0xffffffffu, fz, off);
+    }
+    if (act && part == 0) {
+      const size_t o = (size_t)R.mol[m] * ns + s;
+      atomicAdd(&f[o], fx * conv);
+      atomicAdd(&f[nfs + o], fy * conv);
+      atomicAdd(&f[2 * nfs + o], fz * conv);
+    }
+  }
+  if (tid == kFs3Block - 1) {
+    const double(*cv)[3] = R.cv;
+    const double rij = R.rr[0], rik = R.rr[1], rjk = R.rr[2];
+    const double iij = 1.0 / rij, iik = 1.0 / rik, ijk = 1.0 / rjk;
+    const double ux = cv[0][0] * iij, uy = cv[0][1] * iij, uz = cv[0][2] * iij;
+    const double wx = cv[1][0] * iik, wy = cv[1][1] * iik, wz = cv[1][2] * iik;
+    const double sx = cv[2][0] * ijk, sy = cv[2][1] * ijk, sz = cv[2][2] * ijk;
+    const int m0 = R.mol[0], m1 = R.mol[1], m2 = R.mol[2];
+    atomicAdd(&fc3[m0], -comc * (ux + wx) * conv);
+    atomicAdd(&fc3[nm + m0], -comc * (uy + wy) * conv);
+    atomicAdd(&fc3[2 * nm + m0], -comc * (uz + wz) * conv);
+    atomicAdd(&fc3[m1], -comc * (-ux + sx) * conv);
+    atomicAdd(&fc3[nm + m1], -comc * (-uy + sy) * conv);
+    atomicAdd(&fc3[2 * nm + m1], -comc * (-uz + sz) * conv);
+    atomicAdd(&fc3[m2], -comc * (-wx - sx) * conv);
+    atomicAdd(&fc3[nm + m2], -comc * (-wy - sy) * conv);
+    atomicAdd(&fc3[2 * nm + m2], -comc * (-wz - sz) * conv);
+    vsite += comc * (rij + rik + rjk);
+  }
+  return vsite;
+}
+
 // The gradient form holds one block per SM (its shared memory), so it may use more registers.
+//
+// Per sweep the block runs two barrier-separated phases: A, the pair phase of the sweep
+// (threads < 289) -- on a triple's first sweep together with the site and COM forces of the
+// block's previous triple (threads < 204 and the last thread) and the staging of its next
+// triple (threads >= 289) -- and B, the three passes.  The force weights G alternate between
+// two buffers by triple, and records and site offsets rotate through three staging slots, so
+// that the previous triple's forces, this triple's tables and the next triple's staging
+// never touch the same memory.
 template <typename T, bool GRAD>
 __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     k_fs3(const Fs3Rec *__restrict__ recs, const int *__restrict__ icnt, int tri_cap,
@@ -506,34 +631,22 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
       S.uul.v[p][q][sp(1)] = make_float2(0.f, 0.f);
     }
   }
-  const double conv = kH2kcal * 418.4 / kBohr2a;
-  const size_t nfs = (size_t)nm * ns;
-  double e_tot = 0.0, v_tot = 0.0;
+  fs3_stage(S, recs, s17, t_begin, 0);
+  __syncthreads();
+  CompSum e_tot, v_tot;  // this thread's energy and virial over the block's triples
   int have_i = -1, have_j = -1, have_v = -1;  // molecule pair and variant of the ij tables
+  double comc_prev = 0.0;                     // COM-force weight of the previous triple
   for (int t = t_begin; t < t_end; t++) {
-    __syncthreads();
-    // warp 0 stages the record; warps 2-3 stage the site offsets, reading the molecule
-    // indices from the record in global memory (the passes store every entry of S.G, so it
-    // needs no clearing)
-    if (tid < kRecWords)
-      reinterpret_cast<double *>(&S.rec)[tid] = reinterpret_cast<const double *>(recs + t)[tid];
-    if (tid >= 64 && tid < 64 + 3 * kNs3) {
-      const int m = (tid - 64) / kNs3, s = (tid - 64) % kNs3;
-      const double4 o = s17[(size_t)recs[t].mol[m] * kNs3 + s];
-      S.site[m][s][0] = o.x;
-      S.site[m][s][1] = o.y;
-      S.site[m][s][2] = o.z;
-    }
-    __syncthreads();
-    const double fdmp = S.rec.fdmp, dfdmp = S.rec.dfdmp;
-    const int br = S.rec.branch;
-    double energy, comc;
-    const bool same_ij = S.rec.mol[0] == have_i && S.rec.mol[1] == have_j;
-    have_i = S.rec.mol[0];
-    have_j = S.rec.mol[1];
+    const int k = t - t_begin, sl = k % 3, sl_prev = (k + 2) % 3, sl_next = (k + 1) % 3;
+    const Fs3Rec &R = S.rec[sl];
+    const double fdmp = R.fdmp, dfdmp = R.dfdmp;
+    const int br = R.branch;
+    const bool same_ij = R.mol[0] == have_i && R.mol[1] == have_j;
+    have_i = R.mol[0];
+    have_j = R.mol[1];
     // one sweep (SR or LR branch) or two (blend); of two, the one whose ij tables are already
     // in place goes first.  One call site keeps the kernel's instruction footprint small.
-    const double smfun = S.rec.smfun, smfun2 = 1.0 - smfun;
+    const double smfun = R.smfun, smfun2 = 1.0 - smfun;
     const int nsweep = br == 2 ? 2 : 1;
     const bool lr_first = br == 2 && same_ij && have_v == 1;
     double Ssr = 0.0, Slr = 0.0;
@@ -541,7 +654,13 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     for (int w = 0; w < nsweep; w++) {
       const int v = br != 2 ? br : ((w == 0) == lr_first ? 1 : 0);
       const double ws = br != 2 ? fdmp : fdmp * (v == 0 ? smfun : smfun2);
-      const double Sv = fs3_variant<T, GRAD>(S, GS, v, ws, w == 0, w == 0 && same_ij && have_v == v);
+      if (w == 0) {
+        if (k > 0) v_tot.add(fs3_forces(S, sl_prev, S.G[(k - 1) & 1], comc_prev, nm, ns, f, fc3));
+        if (t + 1 < t_end) fs3_stage(S, recs, s17, t + 1, sl_next);
+      }
+      fs3_pairs<T, GRAD>(S, GS, v, sl, w == 0 && same_ij && have_v == v);
+      __syncthreads();
+      const double Sv = fs3_passes<T, GRAD>(S, GS, v, ws, w == 0, S.G[k & 1]);
       if (v == 0)
         Ssr = Sv;
       else
@@ -550,94 +669,21 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     }
     if (br != 2) {
       const double Sv = br == 0 ? Ssr : Slr;
-      energy = fdmp * Sv;
-      comc = dfdmp * Sv;
+      if (tid == kFs3Block - 1) e_tot.add(fdmp * Sv);
+      comc_prev = dfdmp * Sv;
     } else {
-      const double cf = S.rec.cf;
-      energy = fdmp * (smfun * Ssr + smfun2 * Slr);
-      comc = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
+      const double cf = R.cf;
+      if (tid == kFs3Block - 1) e_tot.add(fdmp * (smfun * Ssr + smfun2 * Slr));
+      comc_prev = Ssr * (dfdmp * smfun + fdmp * cf) + Slr * (dfdmp * smfun2 - fdmp * cf);
     }
-    // ---- site forces: F = -sum_partner G * (pair vector); 4 lanes per (molecule, site),
-    // each summing a quarter of the 17 partners, reduced with shuffles.
-    double vsite = 0.0;
-    {
-      const int item = tid >> 2, part = tid & 3;
-      const bool act = item < 3 * kNs3;
-      const int m = act ? item / kNs3 : 0, s = act ? item % kNs3 : 0, ps = sp(pidx(s));
-      const double(*cv)[3] = S.rec.cv;
-      double fx = 0.0, fy = 0.0, fz = 0.0;
-      // the item's two pair families ("links"): family, whether this molecule is the second
-      // of the family's pair (then the weight is G[partner][this] and the pair vector points
-      // from the partner's site), the partner molecule; the virial counts each molecular
-      // pair once (ij and ik from molecule i, jk from molecule j)
-      const int fa = m == 2 ? 1 : 0, fb = m == 0 ? 1 : 2;
-      const bool ta = m != 0, tb = m == 2;
-      const int pa = m == 0 ? 1 : 0, pb = m == 2 ? 1 : 2;
-      const double sga = ta ? -1.0 : 1.0, sgb = tb ? -1.0 : 1.0;
-      const double wva = m == 0 ? 1.0 : 0.0, wvb = m != 2 ? 1.0 : 0.0;
-      if (act) {
-        const double x0 = S.site[m][s][0], x1 = S.site[m][s][1], x2 = S.site[m][s][2];
-        const double *ga_row = &S.G[fa][0][0], *gb_row = &S.G[fb][0][0];
-#pragma unroll 1
-        for (int o = part; o < kNs3; o += 4) {
-          const int po = sp(pidx(o));
-          const double ga = ga_row[ta ? po * kRS + ps : ps * kRS + po];
-          const double gb = gb_row[tb ? po * kRS + ps : ps * kRS + po];
-          // (this - partner) site offsets, negated for a transposed link: exact
-          const double a0 = cv[fa][0] + sga * (x0 - S.site[pa][o][0]);
-          const double a1 = cv[fa][1] + sga * (x1 - S.site[pa][o][1]);
-          const double a2 = cv[fa][2] + sga * (x2 - S.site[pa][o][2]);
-          const double b0 = cv[fb][0] + sgb * (x0 - S.site[pb][o][0]);
-          const double b1 = cv[fb][1] + sgb * (x1 - S.site[pb][o][1]);
-          const double b2 = cv[fb][2] + sgb * (x2 - S.site[pb][o][2]);
-          const double sa = sga * ga, sb = sgb * gb;
-          fx -= sa * a0 + sb * b0;
-          fy -= sa * a1 + sb * b1;
-          fz -= sa * a2 + sb * b2;
-          vsite += wva * ga * (a0 * a0 + a1 * a1 + a2 * a2) + wvb * gb * (b0 * b0 + b1 * b1 + b2 * b2);
-        }
-      }
-#pragma unroll
-      for (int off = 1; off < 4; off <<= 1) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, off);
-        fy += __shfl_xor_sync(0xffffffffu, fy, off);
-        fz += __shfl_xor_sync(0xffffffffu, fz, off);
-      }
-      if (act && part == 0) {
-        const size_t o = (size_t)S.rec.mol[m] * ns + s;
-        atomicAdd(&f[o], fx * conv);
-        atomicAdd(&f[nfs + o], fy * conv);
-        atomicAdd(&f[2 * nfs + o], fz * conv);
-      }
-    }
-    if (tid == kFs3Block - 1) {
-      // COM forces from the R_avg damping and switch (threebody_potential.f90:1092-1120)
-      const double(*cv)[3] = S.rec.cv;
-      const double rij = S.rec.rr[0], rik = S.rec.rr[1], rjk = S.rec.rr[2];
-      const double iij = 1.0 / rij, iik = 1.0 / rik, ijk = 1.0 / rjk;
-      const double ux = cv[0][0] * iij, uy = cv[0][1] * iij, uz = cv[0][2] * iij;
-      const double wx = cv[1][0] * iik, wy = cv[1][1] * iik, wz = cv[1][2] * iik;
-      const double sx = cv[2][0] * ijk, sy = cv[2][1] * ijk, sz = cv[2][2] * ijk;
-      const int m0 = S.rec.mol[0], m1 = S.rec.mol[1], m2 = S.rec.mol[2];
-      atomicAdd(&fc3[m0], -comc * (ux + wx) * conv);
-      atomicAdd(&fc3[nm + m0], -comc * (uy + wy) * conv);
-      atomicAdd(&fc3[2 * nm + m0], -comc * (uz + wz) * conv);
-      atomicAdd(&fc3[m1], -comc * (-ux + sx) * conv);
-      atomicAdd(&fc3[nm + m1], -comc * (-uy + sy) * conv);
-      atomicAdd(&fc3[2 * nm + m1], -comc * (-uz + sz) * conv);
-      atomicAdd(&fc3[m2], -comc * (-wx - sx) * conv);
-      atomicAdd(&fc3[nm + m2], -comc * (-wy - sy) * conv);
-      atomicAdd(&fc3[2 * nm + m2], -comc * (-wz - sz) * conv);
-      e_tot += energy;
-      v_tot += comc * (rij + rik + rjk);
-    }
-    v_tot += vsite;
   }
-  v_tot = warp_sum(v_tot);
-  e_tot = warp_sum(e_tot);
+  // the forces of the block's last triple (its G and slot are final after the last barrier)
+  v_tot.add(fs3_forces(S, (t_end - 1 - t_begin) % 3, S.G[(t_end - 1 - t_begin) & 1], comc_prev,
+                       nm, ns, f, fc3));
+  const double vt = warp_sum(v_tot.value()), et = warp_sum(e_tot.value());
   if ((tid & 31) == 0) {
-    atomicAdd(&scal[S_FS3_VIR], v_tot);
-    if (e_tot != 0.0) atomicAdd(&scal[S_FS3_E], e_tot);
+    atomicAdd(&scal[S_FS3_VIR], vt);
+    if (et != 0.0) atomicAdd(&scal[S_FS3_E], et);
   }
   if (GRAD) {
     __syncthreads();

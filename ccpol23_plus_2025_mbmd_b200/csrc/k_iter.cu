@@ -29,6 +29,15 @@ using namespace ccpd;
 namespace {
 
 constexpr int kThreads = 256;
+
+// Programmatic dependent launch (sm_90+): `launch_dependents` lets the next kernel in the
+// stream (launched with programmatic stream serialization) start its blocks once every block
+// of this one has executed it; `wait` blocks until the preceding kernel has completed and its
+// writes are visible.  Both are no-ops in a kernel launched without the attribute.
+__device__ __forceinline__ void pdl_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 constexpr int kWarps = kThreads / 32;
 constexpr int kSumSites = 32;     // polarisable sites per structure-factor block
 constexpr int kGatherSites = 4;  // polarisable sites per gather/update block
@@ -206,6 +215,8 @@ __global__ void __launch_bounds__(kThreads)
     k_iter_a(IterArgs A) {
   // no test of the finished flag here: a step after the finish only rewrites the T.mu
   // scratch and S(k), which the next use clears, and it saves a dependent load per step
+  pdl_launch_dependents();
+  pdl_wait();  // the previous step's dipoles (and its gather's last use of the S(k) buffer)
   const int nA = (A.nw + kWarps - 1) / kWarps;
   PcgIn pin;
   if constexpr (PCG) pin = pcg_in(A);
@@ -346,6 +357,8 @@ __global__ void __launch_bounds__(kThreads)
     k_iter_b(IterArgs A) {
   // kGatherSites polarisable sites per block; the 8 warps split the k-vectors, so every
   // k-vector's weights are loaded once per block and reused for all its sites
+  pdl_launch_dependents();
+  pdl_wait();  // T.mu, S(k) and the step scalars of this step's first kernel
   if (A.state[kIterFinished] != 0.0) return;  // finished in an earlier step of this pass
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int w0 = blockIdx.x * kGatherSites;
@@ -531,22 +544,31 @@ cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np,
   return cudaGetLastError();
 }
 
+// Launches a step kernel, with programmatic stream serialization when A.pdl is set.
+template <typename Kernel>
+cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = A.pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, A);
+}
+
 cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st) {
   const int nA = (A.nw + kWarps - 1) / kWarps;
   const int nkt = (A.nk + kThreads - 1) / kThreads;
   const int nsc = (A.nw + kSumSites - 1) / kSumSites;
-  if (A.cu)
-    k_iter_a<true><<<nA + nkt * nsc, kThreads, 0, st>>>(A);
-  else
-    k_iter_a<false><<<nA + nkt * nsc, kThreads, 0, st>>>(A);
-  return cudaGetLastError();
+  return A.cu ? launch_step(k_iter_a<true>, nA + nkt * nsc, A, st)
+              : launch_step(k_iter_a<false>, nA + nkt * nsc, A, st);
 }
 
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
   const int nb = (A.nw + kGatherSites - 1) / kGatherSites;
-  if (A.cu)
-    k_iter_b<true><<<nb, kThreads, 0, st>>>(A);
-  else
-    k_iter_b<false><<<nb, kThreads, 0, st>>>(A);
-  return cudaGetLastError();
+  return A.cu ? launch_step(k_iter_b<true>, nb, A, st) : launch_step(k_iter_b<false>, nb, A, st);
 }

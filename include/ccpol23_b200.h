@@ -399,6 +399,11 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
                      update at the iterate) to the same criterion; 2 (CCP_MIXED default): PCG
                      to an RMS update of 1e-8 D per polarisable site.  PCG needs the phase
                      table; without it the solve is Jacobi.  ind_iters then counts PCG steps;
+     "fs3_fp32_passes" 1 (default): in the CCP_MIXED form FS3's ik and jk gradient passes run
+                     in FP32; 0: they run in FP64 as in CCP_FP64 (the rest of the mixed form
+                     unchanged);
+     "pdl"           1 (default): the two kernels of a dipole step are launched with
+                     programmatic dependent launch (each starts while its predecessor drains);
      "cell_list"     1 (default): the neighbour lists come from a cell list when the box holds
                      six or more cells of half the list radius per axis (the same lists as the
                      all-pairs scan); 0: always the all-pairs scan.

@@ -11,8 +11,12 @@ drift with FS3 on, and little with it off.
 Two halves, so that the slow oracle half can run on any CPU:
   python tests/drift_study.py oracle OUT.json   # equilibrate and run the oracle (CPU only)
   python tests/drift_study.py gpu OUT.json      # device runs from the same state, comparison
-The box is 37 waters FS2+FS3 at L = 10.37 A (seed 9), dt = 0.5 fs; the start is the state
-after a velocity-rescaled equilibration of the oracle with FS3 off.
+The box is 80 waters of the FS3 variant (flags T T F) at L = 13.39 A (1 g/cm^3, seed 9),
+dt = 0.5 fs, with the real-space and 2-body cut-off lowered from 9 to 6.5 A so that every
+cut-off (FS3's 6.3 A included) stays below half the box: with a cut-off beyond L/2 the
+minimum image itself switches pairs between images discontinuously, in the reference as
+here, and that would swamp the effect studied.  The start is the state after a
+velocity-rescaled equilibration of the oracle with FS3 off.
 """
 from __future__ import annotations
 
@@ -28,7 +32,8 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "oracle"))
 
 DT = 0.0005          # ps
-NM, L, SEED = 37, 10.37, 9
+NM, L, SEED = 80, 13.39, 9
+VARIANT, RCUT = "fs3", 6.5
 N_EQUIL = 400        # rescaled FS3-off steps before the comparison runs
 N_RUN = 300          # steps of each comparison run
 N_LONG = 20000       # steps of the device-only runs that fix the slopes
@@ -45,9 +50,10 @@ def run_oracle(out):
     from ccpol23_plus_2025_mbmd_b200.generator import water_box
     O.build()
     O.set_threads(0)
-    m = Model(data_dir("fs2fs3"))
+    m = Model(data_dir(VARIANT))
     b = water_box(m, NM, L, SEED)
-    inp = O.read_inputs(data_dir("fs2fs3"))
+    inp = O.read_inputs(data_dir(VARIANT))
+    inp.control["rcut"] = RCUT
     pcoord, pmi, totm = O.principal_frame(inp)
     ld = b.xs.shape[1]
     s = O.MDState(b.x, b.y, b.z, b.v, b.q, b.jb)
@@ -73,8 +79,9 @@ def run_gpu(out):
     s0 = {k: np.array(v) for k, v in res["start"].items()}
     res["gpu"] = {}
     for s3 in (1, 0):
-        m = Model(data_dir("fs2fs3"))
+        m = Model(data_dir(VARIANT))
         m.set("S3_term", s3)
+        m.set("rcut", RCUT)
         with Context(m, NM, L) as c:
             c.md_set_state(L, s0["x"], s0["y"], s0["z"], s0["v"], s0["q"], s0["j"])
             te = [r["te"] for r in c.md_nve(N_RUN, DT)]
@@ -90,7 +97,7 @@ def run_gpu(out):
             "long_steps": N_LONG}
     summary = {k: v for k, v in res["gpu"].items()}
     summary["config"] = {"nm": NM, "box_A": L, "seed": SEED, "dt_ps": DT, "equil": N_EQUIL,
-                         "run": N_RUN}
+                         "run": N_RUN, "variant": VARIANT, "rcut_A": RCUT}
     print(json.dumps(summary), flush=True)
     Path(out).write_text(json.dumps(res))
 

@@ -148,7 +148,9 @@ def test_mixed_form_position_gradient(setup):
             cc = com.clone().requires_grad_(True)
             _energy(c2, b, cc, s, fixed).backward()
             out[prec] = (cc.grad.cpu().numpy(), s.grad.cpu().numpy())
-    # site gradients carry the induction part in FP64; the FS3 COM part inherits the
-    # conditioning of the FS3 sum in FP32 (see the mixed-precision parity test)
-    assert rel(out["mixed"][1], out["fp64"][1]) <= 1e-4
-    assert rel(out["mixed"][0], out["fp64"][0]) <= 1e-3
+    # measured on this box: site gradients 2.5e-6, molecular-centre gradients 6.6e-5 apart.
+    # The centre gradient of a molecule is the sum of its site forces plus the three-body
+    # COM forces, a sum that cancels to a small fraction of its parts, so the FP32 terms of
+    # the mixed form (FS3's ik/jk gradient passes, FS2's spectator terms) weigh more in it
+    assert rel(out["mixed"][1], out["fp64"][1]) <= 1e-5
+    assert rel(out["mixed"][0], out["fp64"][0]) <= 2e-4
