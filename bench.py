@@ -353,7 +353,7 @@ def run_batch(nframes, steps, warmup):
     """Batches of independent 256-water FS3 frames (L = 19.71 A, seed 4004 + f), the
     three-body plus induction terms that the autograd binding evaluates: device-resident
     inputs, frames one by one on one context against one ccp_batch_terms_device call per
-    batch (slots 1 / 8 / nframes).  Wall time per batch on the host, device synchronised on
+    batch (slots 1 / 8 / nframes), with FS3 fused over the frames (one launch set) and not.  Wall time per batch on the host, device synchronised on
     both sides; prints one JSON line, not the headline metric."""
     import torch
     from ccpol23_plus_2025_mbmd_b200 import Batch, Context, Model, data_dir, _lib
@@ -387,9 +387,11 @@ def run_batch(nframes, steps, warmup):
                                f[2][k])
         out["frame_by_frame"] = timed(one_by_one)
     for slots in sorted({1, 8, nframes}):
-        with Batch(model, nm, L, slots=slots) as b:
-            out[f"batch_slots{slots}"] = timed(
-                lambda: b.terms_device(terms, L, x, y, z, xs, ys, zs, *f))
+        for fuse in (1, 0):
+            with Batch(model, nm, L, slots=slots) as b:
+                b.set_option("fuse_fs3", fuse)
+                out[f"batch_slots{slots}" + ("" if fuse else "_unfused")] = timed(
+                    lambda: b.terms_device(terms, L, x, y, z, xs, ys, zs, *f))
     line = {"metric": f"batch of {nframes} x {nm}-water FS3 frames, three-body + induction",
             "unit": "ms per batch", "steps": steps, "warmup": warmup,
             "config": {"nm": nm, "box_A": L, "variant": cfg["variant"], "seed": cfg["seed"],

@@ -7,6 +7,13 @@
 // most of the GPU idle (its dipole iteration is latency-bound).  Results are identical to
 // separate single-frame calls.  The reference evaluates one configuration per call; this
 // has no counterpart there.
+//
+// FS3, the costliest term of a frame, is fused across the frames when they share one box
+// length (option "fuse_fs3", on by default): the batch packs every frame's molecules one
+// frame after another and runs one neighbour search, one triple enumeration and one FS3
+// launch for all of them on its own stream (batch_fs3_launch), while the slots evaluate the
+// other terms; the FS3 forces, energies and parameter gradients are then added per frame
+// (batch_fs3_finish).  The results equal the single-frame calls'.
 #include <string>
 #include <thread>
 #include <vector>
@@ -16,6 +23,8 @@
 struct ccp_batch {
   std::vector<ccp_context *> ctx;
   int nm = 0;
+  bool fuse_fs3 = true;
+  ccp::BatchFs3 fs3;
 };
 
 namespace {
@@ -55,6 +64,7 @@ int ccp_batch_create(const ccp_model *m, int nm, double box0, int slots, int dev
 
 int ccp_batch_destroy(ccp_batch *b) {
   if (!b) return CCP_ERR_BAD_INPUT;
+  ccp::batch_fs3_free(b->fs3);
   for (ccp_context *c : b->ctx) ccp_context_destroy(c);
   delete b;
   return CCP_OK;
@@ -73,7 +83,11 @@ int ccp_batch_context(ccp_batch *b, int slot, ccp_context **ctx) {
 }
 
 int ccp_batch_set_option(ccp_batch *b, const char *name, int value) {
-  if (!b) return CCP_ERR_BAD_INPUT;
+  if (!b || !name) return CCP_ERR_BAD_INPUT;
+  if (std::string(name) == "fuse_fs3") {
+    b->fuse_fs3 = value != 0;
+    return CCP_OK;
+  }
   for (ccp_context *c : b->ctx) {
     const int r = ccp_context_set_option(c, name, value);
     if (r) return r;
@@ -110,18 +124,34 @@ int ccp_batch_terms_device(ccp_batch *b, unsigned terms, int nframes, const doub
     if (ncoef < 1 || pgrad_len != 2 * ncoef + 2 * 3 * 289)
       return fail(CCP_ERR_BAD_INPUT, "ccp_batch_terms_device: pgrad_len is not 2 ncoef + 1734");
   }
+  // FS3 of all frames in one launch set when they share one box length
+  bool fused = b->fuse_fs3 && (terms & CCP_TERM_FS3) && nframes > 1 && x && y && z && xs && ys &&
+               zs;
+  for (int f = 1; fused && f < nframes; f++) fused = box[f] == box[0];
+  int model_s3 = 0;
+  if (fused) {
+    ccp_context_get_option(b->ctx[0], "fs3_available", &model_s3);
+    fused = model_s3 != 0;
+  }
+  unsigned rest = terms;
+  if (fused) {
+    const int r = ccp::batch_fs3_launch(b->ctx[0], b->fs3, nframes, box[0], x, y, z, xs, ys, zs,
+                                        ld, pgrad != nullptr);
+    if (r) return fail(r, std::string("ccp_batch_terms_device: fused FS3: ") + ccp_last_error());
+    rest &= ~unsigned(CCP_TERM_FS3);
+  }
   std::vector<int> status(nframes, CCP_OK);
   std::vector<std::string> msg(nframes);
   auto work = [&](int slot) {
     ccp_context *c = b->ctx[slot];
     for (int f = slot; f < nframes; f += slots) {
       const size_t o = (size_t)f * nm, os = (size_t)f * nsite;
-      int r = ccp_terms_device(c, terms, off(x, o), off(y, o), off(z, o), off(xs, os), off(ys, os),
+      int r = ccp_terms_device(c, rest, off(x, o), off(y, o), off(z, o), off(xs, os), off(ys, os),
                                off(zs, os), ld, box[f], e + f, off(fxs, os), off(fys, os),
                                off(fzs, os), off(fxfs2, o), off(fyfs2, o), off(fzfs2, o),
                                off(fxfs3, o), off(fyfs3, o), off(fzfs3, o), off(idmx, os),
                                off(idmy, os), off(idmz, os));
-      if (!r && pgrad) {
+      if (!r && pgrad && !fused) {
         double *g = pgrad + (size_t)f * pgrad_len;
         r = ccp_context_fs3_param_grad(c, g, g + ncoef, ncoef, g + 2 * ncoef,
                                        g + 2 * ncoef + 3 * 289);
@@ -141,8 +171,18 @@ int ccp_batch_terms_device(ccp_batch *b, unsigned terms, int nframes, const doub
     for (int s = 0; s < nt; s++) th.emplace_back(work, s);
     for (std::thread &t : th) t.join();
   }
-  for (int f = 0; f < nframes; f++)
-    if (status[f]) return fail(status[f], "frame " + std::to_string(f) + ": " + msg[f]);
+  int first_bad = -1;
+  for (int f = 0; f < nframes && first_bad < 0; f++)
+    if (status[f]) first_bad = f;
+  if (fused) {
+    // always completes the fused launch, so that no work of this call outlives it
+    const int r = ccp::batch_fs3_finish(b->ctx[0], b->fs3, nframes, ld, e, fxs, fys, fzs, fxfs3,
+                                        fyfs3, fzfs3, pgrad, pgrad_len);
+    if (r && first_bad < 0)
+      return fail(r, std::string("ccp_batch_terms_device: fused FS3: ") + ccp_last_error());
+  }
+  if (first_bad >= 0)
+    return fail(status[first_bad], "frame " + std::to_string(first_bad) + ": " + msg[first_bad]);
   return CCP_OK;
 }
 

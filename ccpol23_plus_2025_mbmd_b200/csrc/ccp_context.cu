@@ -588,6 +588,20 @@ int ensure_phase_matrix(ccp_context *c) {
     if (!cuda_ok((call), #call)) return CCP_ERR_CUDA;   \
   } while (0)
 
+// FS3's cut-off, damping and switch constants (threebody_potential.f90:860-904, 1418-1423) in
+// bohr for a box of `box` Angstrom.
+Fs3Params fs3_params(const ccp_context *c, double box) {
+  Fs3Params F3;
+  F3.boxb = box / kBohr2a;
+  F3.rc2 = std::pow(6.3, 2.0) * std::pow(kBohr2a, -2.0);
+  F3.alp3 = c->alpha3 * kBohr2a;
+  F3.r0dmp = 6.20446 / kBohr2a;
+  F3.delta33 = c->delta33;
+  F3.rmin = 4.5 / kBohr2a;
+  F3.rmax = 5.5 / kBohr2a;
+  return F3;
+}
+
 // Runs the enabled terms on inputs already in the context's device buffers
 // (x, y, z at px.., sites at pxs.. with leading dimension ld).
 int evaluate_impl(ccp_context *c, const double *px, const double *py, const double *pz,
@@ -617,14 +631,7 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
   P.delta3 = 1.55 / kBohr2a;
   P.damped = c->damped ? 1 : 0;
   const double boxb = box / kBohr2a;
-  Fs3Params F3;
-  F3.boxb = boxb;
-  F3.rc2 = std::pow(6.3, 2.0) * std::pow(kBohr2a, -2.0);
-  F3.alp3 = c->alpha3 * kBohr2a;
-  F3.r0dmp = 6.20446 / kBohr2a;
-  F3.delta33 = c->delta33;
-  F3.rmin = 4.5 / kBohr2a;
-  F3.rmax = 5.5 / kBohr2a;
+  const Fs3Params F3 = fs3_params(c, box);
   Fs2Params F2;
   F2.boxb = boxb;
   F2.rc2 = c->rcutsd3 * std::pow(kBohr2a, -2.0);
@@ -1447,6 +1454,8 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_solver;
   } else if (n == "cell_list") {
     *value = ctx->opt_cells;
+  } else if (n == "fs3_available") {
+    *value = ctx->three_body && ctx->s3 && ctx->have_fs3 && ctx->ns >= kNs3 ? 1 : 0;
   } else if (n == "pdl") {
     *value = ctx->opt_pdl;
   } else if (n == "fs3_fp32_passes") {
@@ -2281,3 +2290,209 @@ int ccp_md_get_stats(ccp_context *ctx, ccp_md_stats *stats) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------ batches: fused FS3
+namespace {
+
+// Packs the centres (Angstrom and bohr) and FS3 site offsets (bohr) of every molecule of a
+// batch, frames one after another as the caller's arrays hold them, with the same
+// conversions as k_prep; clears the force, counter and energy buffers.
+__global__ void k_batch_fs3_prep(const double *__restrict__ x, const double *__restrict__ y,
+                                 const double *__restrict__ z, const double *__restrict__ xs,
+                                 const double *__restrict__ ys, const double *__restrict__ zs,
+                                 int nt, int ld, int ns, double4 *com, double4 *comb, double4 *s17,
+                                 double *f, double *fc3, int *icnt, double *scal, int nscal,
+                                 int *counts, int ncounts) {
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  for (int i = t0; i < nt; i += stride) {
+    com[i] = make_double4(x[i], y[i], z[i], 0.0);
+    comb[i] = make_double4(x[i] / kBohr2a, y[i] / kBohr2a, z[i] / kBohr2a, 0.0);
+    fc3[i] = fc3[nt + i] = fc3[2 * nt + i] = 0.0;
+  }
+  for (int u = t0; u < nt * kNs3; u += stride) {
+    const int i = u / kNs3, s = u - i * kNs3;
+    const size_t o = (size_t)i * ld + s;
+    s17[u] = make_double4(xs[o] / kBohr2a, ys[o] / kBohr2a, zs[o] / kBohr2a, 0.0);
+  }
+  for (size_t u = t0; u < 3 * (size_t)nt * ns; u += stride) f[u] = 0.0;
+  for (int u = t0; u < nscal; u += stride) scal[u] = 0.0;
+  for (int u = t0; u < ncounts; u += stride) counts[u] = 0;
+  if (t0 < C_COUNT) icnt[t0] = 0;
+}
+
+int batch_fs3_alloc(ccp_context *c, BatchFs3 &B, int nframes, int cap, int tri_cap) {
+  const int nt = nframes * c->nm;
+  if (B.device == c->device && nt <= B.nm_total && nframes <= B.nframes && cap <= B.cap &&
+      tri_cap <= B.tri_cap)
+    return CCP_OK;
+  const int nt_a = std::max(nt, B.nm_total), nf_a = std::max(nframes, B.nframes);
+  const int cap_a = std::max(cap, B.cap), tri_a = std::max(tri_cap, B.tri_cap);
+  void *stream = B.stream;
+  B.stream = nullptr;
+  batch_fs3_free(B);
+  B.stream = stream;
+  B.device = c->device;
+  B.nm_total = nt_a;
+  B.nframes = nf_a;
+  B.cap = cap_a;
+  B.tri_cap = tri_a;
+  const size_t n = nt_a, ns = c->ns;
+  double4 *com, *comb, *s17, *nbrv;
+  CK(dalloc(&com, n));
+  B.com = com;
+  CK(dalloc(&comb, n));
+  B.comb = comb;
+  CK(dalloc(&s17, n * kNs3));
+  B.s17 = s17;
+  CK(dalloc(&nbrv, n * cap_a));
+  B.nbrv = nbrv;
+  CK(dalloc(&B.nbr, n * cap_a));
+  CK(dalloc(&B.ncnt, n));
+  CK(dalloc(&B.icnt, (size_t)C_COUNT));
+  CK(dalloc(&B.counts, 2 * (size_t)nf_a));
+  CK(cudaMalloc(&B.tri, fs3_record_bytes() * (size_t)tri_a));
+  CK(dalloc(&B.f, 3 * n * ns));
+  CK(dalloc(&B.fc3, 3 * n));
+  CK(dalloc(&B.scal, (size_t)nf_a * S_COUNT));
+  CK(dalloc(&B.gfs3, (size_t)nf_a * kFs3GradLen));
+  CK(cudaMallocHost((void **)&B.h_icnt, sizeof(int) * C_COUNT));
+  CK(cudaMallocHost((void **)&B.h_counts, sizeof(int) * 2 * nf_a));
+  CK(cudaMallocHost((void **)&B.h_scal, sizeof(double) * ((size_t)nf_a * S_COUNT +
+                                                          (size_t)nf_a * kFs3GradLen)));
+  return CCP_OK;
+}
+
+}  // namespace
+
+namespace ccp {
+
+void batch_fs3_free(BatchFs3 &B) {
+  if (B.device >= 0) cudaSetDevice(B.device);
+  void *dp[] = {B.com, B.comb, B.s17, B.nbrv, B.nbr, B.ncnt, B.icnt, B.counts, B.tri,
+                B.f, B.fc3, B.scal, B.gfs3};
+  for (void *p : dp)
+    if (p) cudaFree(p);
+  if (B.h_icnt) cudaFreeHost(B.h_icnt);
+  if (B.h_counts) cudaFreeHost(B.h_counts);
+  if (B.h_scal) cudaFreeHost(B.h_scal);
+  if (B.stream) cudaStreamDestroy(static_cast<cudaStream_t>(B.stream));
+  B = BatchFs3();
+}
+
+// Enqueues the FS3 term of `nframes` frames of c->nm molecules (the caller's frame-strided
+// device arrays, one box length for all) as one neighbour search, one triple enumeration and
+// one FS3 launch on the batch's own stream.  The list capacities are checked once (one
+// synchronisation after the enumeration) and grown if a frame needed more.  `grad`: also
+// the per-frame FS3 parameter gradients.  batch_fs3_finish completes the call.
+int batch_fs3_launch(ccp_context *c, BatchFs3 &B, int nframes, double box, const double *x,
+                     const double *y, const double *z, const double *xs, const double *ys,
+                     const double *zs, int ld, bool grad) {
+  CK(cudaSetDevice(c->device));
+  if (!c->three_body || !c->s3 || !c->have_fs3 || c->ns < kNs3) {
+    set_error("fused FS3: the model has no FS3 term");
+    return CCP_ERR_BAD_INPUT;
+  }
+  if (!B.stream) {
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    cudaStream_t st;
+    CK(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio_lo));
+    B.stream = st;
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(B.stream);
+  const int nm = c->nm, nt = nframes * nm;
+  int cap = std::max(B.cap, std::min(nm - 1, c->cap));
+  int tri_cap = std::max(B.tri_cap, c->tri_cap * nframes);
+  const double rl = 6.3 + 0.05;  // FS3's cut-off and the list margin of an evaluation
+  const Fs3Params F3 = fs3_params(c, box);
+  for (int attempt = 0;; attempt++) {
+    int r = batch_fs3_alloc(c, B, nframes, cap, tri_cap);
+    if (r) return r;
+    cap = B.cap;
+    tri_cap = B.tri_cap;
+    k_batch_fs3_prep<<<148 * 4, 256, 0, st>>>(
+        x, y, z, xs, ys, zs, nt, ld, c->ns, static_cast<double4 *>(B.com),
+        static_cast<double4 *>(B.comb), static_cast<double4 *>(B.s17), B.f, B.fc3, B.icnt,
+        B.scal, nframes * S_COUNT, B.counts, 2 * nframes);
+    CK(cudaGetLastError());
+    if (grad) CK(cudaMemsetAsync(B.gfs3, 0, sizeof(double) * nframes * kFs3GradLen, st));
+    CK(launch_neighbors(static_cast<double4 *>(B.com), nt, box, rl * rl, cap, B.nbr,
+                        static_cast<double4 *>(B.nbrv), B.ncnt, B.icnt, st, nm));
+    CK(launch_fs3_enum(static_cast<double4 *>(B.comb), B.nbr, B.ncnt, cap, nt, F3, B.tri, tri_cap,
+                       B.icnt, st));
+    CK(cudaMemcpyAsync(B.h_icnt, B.icnt, sizeof(int) * C_COUNT, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int *ic = B.h_icnt;
+    bool grow = false;
+    if (ic[C_OVERFLOW] > 0) {
+      cap = std::min(nm, ic[C_OVERFLOW] + 32);
+      grow = true;
+    }
+    if (ic[C_NTRI_FS3] > tri_cap) {
+      tri_cap = ic[C_NTRI_FS3] + ic[C_NTRI_FS3] / 4 + 64;
+      grow = true;
+    }
+    if (!grow) break;
+    if (attempt == 2) {
+      set_error("fused FS3: the lists overflowed after growing");
+      return CCP_ERR_CAPACITY;
+    }
+  }
+  const int prec = c->precision == CCP_MIXED && c->opt_fs3_low ? CCP_MIXED : CCP_FP64;
+  CK(launch_fs3(prec, B.tri, B.icnt, tri_cap, static_cast<double4 *>(B.s17), c->d_coef, c->d_bgr,
+                nt, c->ns, B.f, B.fc3, B.scal, c->nsm, c->opt_fs3_tpb, 0, grad ? B.gfs3 : nullptr,
+                st, nm, S_COUNT));
+  CK(launch_fs3_frame_counts(B.tri, B.icnt, tri_cap, nm, B.counts, st));
+  return CCP_OK;
+}
+
+// Completes batch_fs3_launch: adds the FS3 site forces into the caller's (frame-strided)
+// fxs.., writes the FS3 COM forces, adds each frame's FS3 energy, virial and triple counts
+// to e[f] and, with pgrad, writes each frame's parameter gradient (layout of
+// ccp_batch_terms_device).
+int batch_fs3_finish(ccp_context *c, BatchFs3 &B, int nframes, int ld, ccp_energies *e,
+                     double *fxs, double *fys, double *fzs, double *fxfs3, double *fyfs3,
+                     double *fzfs3, double *pgrad, int pgrad_len) {
+  CK(cudaSetDevice(c->device));
+  cudaStream_t st = static_cast<cudaStream_t>(B.stream);
+  const int nt = nframes * c->nm;
+  if (fxs || fys || fzs) {
+    k_scatter_out<<<(nt * c->ns + 255) / 256, 256, 0, st>>>(B.f, nt, c->ns, ld, fxs, fys, fzs);
+    CK(cudaGetLastError());
+  }
+  double *c3[3] = {fxfs3, fyfs3, fzfs3};
+  for (int a = 0; a < 3; a++)
+    if (c3[a])
+      CK(cudaMemcpyAsync(c3[a], B.fc3 + (size_t)a * nt, sizeof(double) * nt,
+                         cudaMemcpyDeviceToDevice, st));
+  double *hs = B.h_scal, *hg = B.h_scal + (size_t)nframes * S_COUNT;
+  CK(cudaMemcpyAsync(hs, B.scal, sizeof(double) * nframes * S_COUNT, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(B.h_counts, B.counts, sizeof(int) * 2 * nframes, cudaMemcpyDeviceToHost, st));
+  if (pgrad)
+    CK(cudaMemcpyAsync(hg, B.gfs3, sizeof(double) * nframes * kFs3GradLen,
+                       cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const size_t ntype = c->class_of_type.size();
+  const int ncoef = c->nclass;
+  for (int f = 0; f < nframes; f++) {
+    const double *sc = hs + (size_t)f * S_COUNT;
+    e[f].fs3pe = sc[S_FS3_E] * kH2kcal;
+    e[f].vir += sc[S_FS3_VIR] * kH2kcal * 418.4;
+    e[f].n_fs3_triples = B.h_counts[2 * f];
+    e[f].n_fs3_blend = B.h_counts[2 * f + 1];
+    if (!pgrad) continue;
+    // fold the coefficient-table entries onto the classes (ccp_context_fs3_param_grad)
+    const double *g = hg + (size_t)f * kFs3GradLen;
+    double *out = pgrad + (size_t)f * pgrad_len;
+    for (int k = 0; k < 2 * ncoef; k++) out[k] = 0.0;
+    for (size_t t = 0; t < ntype; t++) {
+      out[c->class_of_type[t]] += g[t];
+      out[ncoef + c->class_of_type[t]] += g[ntype + t];
+    }
+    for (int k = 0; k < 2 * ncoef; k++) out[k] *= kH2kcal;
+    for (int k = 0; k < 2 * 3 * 289; k++) out[2 * ncoef + k] = g[2 * ntype + k] * kH2kcal;
+  }
+  return CCP_OK;
+}
+
+}  // namespace ccp

@@ -247,7 +247,8 @@ cudaError_t launch_prep(const double *x, const double *y, const double *z, const
                         double *f, int nf, double *fc2, double *fc3, double *scal,
                         int *icnt, cudaStream_t st);
 cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
-                             int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st);
+                             int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st,
+                             int frame_nm = 0);
 // Cell-list form of launch_neighbors (same lists): cells per axis for a box and list radius
 // (0 when the box holds fewer than six cells of side >= rlist/2 per axis, or more than
 // kMaxCellsPerAxis), the int scratch it needs, and the launcher.
@@ -326,10 +327,18 @@ size_t fs3_record_bytes();
 cudaError_t launch_fs3_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
                             int nm, Fs3Params P, void *rec, int tri_cap, int *icnt,
                             cudaStream_t st);
+// With frame_nm > 0 the molecules come in frames of frame_nm (one list of triples for the
+// independent boxes of a batch): frame f's energy and virial go to scal + f * scal_stride and
+// its parameter gradient to gfs3 + f * kFs3GradLen.
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
                        double *f, double *fc3, double *scal, int nsm, int triples_per_block,
-                       int blocks_per_sm, double *gfs3, cudaStream_t st);
+                       int blocks_per_sm, double *gfs3, cudaStream_t st, int frame_nm = 0,
+                       int scal_stride = 0);
+// Triples and blend-region triples per frame into counts[2 f], counts[2 f + 1] (cleared by
+// the caller).
+cudaError_t launch_fs3_frame_counts(const void *rec, const int *icnt, int tri_cap, int frame_nm,
+                                    int *counts, cudaStream_t st);
 cudaError_t launch_fs2_enum(const double4 *comb, const int *nbr, const int *ncnt, int cap,
                             int nm, Fs2Params P, int2 *pairs, int pair_cap, int *icnt,
                             cudaStream_t st);

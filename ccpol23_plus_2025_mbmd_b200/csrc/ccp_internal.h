@@ -25,6 +25,28 @@ constexpr double kEwp = 1.0e-6;
 
 void set_error(const std::string &msg);
 
+// Device state of a batch's fused FS3 evaluation: the molecules of all frames packed one
+// frame after another, one neighbour search, one triple list and one FS3 launch for the
+// whole batch (ccp_context.cu: batch_fs3_*; used by ccp_batch.cpp).
+struct BatchFs3 {
+  int nm_total = 0, nframes = 0, cap = 0, tri_cap = 0;
+  void *com = nullptr, *comb = nullptr, *s17 = nullptr, *nbrv = nullptr;  // double4 arrays
+  int *nbr = nullptr, *ncnt = nullptr, *icnt = nullptr, *counts = nullptr;
+  void *tri = nullptr;
+  double *f = nullptr, *fc3 = nullptr, *scal = nullptr, *gfs3 = nullptr;
+  int *h_icnt = nullptr, *h_counts = nullptr;
+  double *h_scal = nullptr;
+  void *stream = nullptr;  // cudaStream_t
+  int device = -1;
+};
+void batch_fs3_free(BatchFs3 &B);
+int batch_fs3_launch(ccp_context *c, BatchFs3 &B, int nframes, double box, const double *x,
+                     const double *y, const double *z, const double *xs, const double *ys,
+                     const double *zs, int ld, bool grad);
+int batch_fs3_finish(ccp_context *c, BatchFs3 &B, int nframes, int ld, ccp_energies *e,
+                     double *fxs, double *fys, double *fzs, double *fxfs3, double *fyfs3,
+                     double *fzfs3, double *pgrad, int pgrad_len);
+
 struct Fs3Table {
   double b[289], g[289], r0[289];  // [is*17 + js]
   std::vector<double> cs;          // linear coefficients in file order

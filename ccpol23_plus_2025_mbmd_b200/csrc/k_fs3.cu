@@ -584,12 +584,17 @@ __device__ __forceinline__ double fs3_forces(const Fs3Smem<T> &S, int sl,
 // two buffers by triple, and records and site offsets rotate through three staging slots, so
 // that the previous triple's forces, this triple's tables and the next triple's staging
 // never touch the same memory.
+//
+// The molecules may come in frames of frame_nm (the independent boxes of a batch, one list
+// of triples): a frame's energy, virial and parameter-gradient sums go to scal + frame *
+// scal_stride and gfs3 + frame * kFs3GradLen, flushed whenever a block's run of triples
+// crosses into the next frame.  frame_nm = nm for a single box.
 template <typename T, bool GRAD>
 __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
     k_fs3(const Fs3Rec *__restrict__ recs, const int *__restrict__ icnt, int tri_cap,
           const double4 *__restrict__ s17, const double *__restrict__ coef,
           const double *__restrict__ bgr, int nm, int ns, double *f, double *fc3, double *scal,
-          double *gfs3) {
+          double *gfs3, int frame_nm, int scal_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Fs3Smem<T> &S = *reinterpret_cast<Fs3Smem<T> *>(smem_raw);
   Fs3Grad<T> *GS = GRAD ? reinterpret_cast<Fs3Grad<T> *>(smem_raw + fs3_grad_offset<T>()) : nullptr;
@@ -636,6 +641,32 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   CompSum e_tot, v_tot;  // this thread's energy and virial over the block's triples
   int have_i = -1, have_j = -1, have_v = -1;  // molecule pair and variant of the ij tables
   double comc_prev = 0.0;                     // COM-force weight of the previous triple
+  int frame = S.rec[0].mol[0] / frame_nm;     // frame of the sums being accumulated
+  // adds this block's sums of `frame` to its slots and clears them (every thread calls it;
+  // the parameter-gradient table is complete: the last passes ended with a barrier, and the
+  // next ones start after the next one)
+  auto flush = [&]() {
+    const double vt = warp_sum(v_tot.value()), et = warp_sum(e_tot.value());
+    if ((tid & 31) == 0) {
+      atomicAdd(&scal[(size_t)frame * scal_stride + S_FS3_VIR], vt);
+      if (et != 0.0) atomicAdd(&scal[(size_t)frame * scal_stride + S_FS3_E], et);
+    }
+    v_tot = CompSum();
+    e_tot = CompSum();
+    if (GRAD) {
+      double *gf = gfs3 + (size_t)frame * kFs3GradLen;
+      for (int u = tid; u < 2 * kCoef; u += kFs3Block) {
+        double &g = (&GS->gc[0][0])[u];
+        if (g != 0.0) atomicAdd(&gf[u], g);
+        g = 0.0;
+      }
+      for (int u = tid; u < 2 * 3 * kPairs; u += kFs3Block) {
+        double &g = (&GS->gb[0][0][0])[u];
+        if (g != 0.0) atomicAdd(&gf[2 * kCoef + u], g);
+        g = 0.0;
+      }
+    }
+  };
   for (int t = t_begin; t < t_end; t++) {
     const int k = t - t_begin, sl = k % 3, sl_prev = (k + 2) % 3, sl_next = (k + 1) % 3;
     const Fs3Rec &R = S.rec[sl];
@@ -656,6 +687,10 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
       const double ws = br != 2 ? fdmp : fdmp * (v == 0 ? smfun : smfun2);
       if (w == 0) {
         if (k > 0) v_tot.add(fs3_forces(S, sl_prev, S.G[(k - 1) & 1], comc_prev, nm, ns, f, fc3));
+        if (R.mol[0] / frame_nm != frame) {  // the previous triple closed its frame's sums
+          flush();
+          frame = R.mol[0] / frame_nm;
+        }
         if (t + 1 < t_end) fs3_stage(S, recs, s17, t + 1, sl_next);
       }
       fs3_pairs<T, GRAD>(S, GS, v, sl, w == 0 && same_ij && have_v == v);
@@ -680,21 +715,18 @@ __global__ void __launch_bounds__(kFs3Block, GRAD ? 1 : CCP_FS3_MINBLOCKS)
   // the forces of the block's last triple (its G and slot are final after the last barrier)
   v_tot.add(fs3_forces(S, (t_end - 1 - t_begin) % 3, S.G[(t_end - 1 - t_begin) & 1], comc_prev,
                        nm, ns, f, fc3));
-  const double vt = warp_sum(v_tot.value()), et = warp_sum(e_tot.value());
-  if ((tid & 31) == 0) {
-    atomicAdd(&scal[S_FS3_VIR], vt);
-    if (et != 0.0) atomicAdd(&scal[S_FS3_E], et);
-  }
-  if (GRAD) {
-    __syncthreads();
-    for (int t = tid; t < 2 * kCoef; t += kFs3Block) {
-      const double g = (&GS->gc[0][0])[t];
-      if (g != 0.0) atomicAdd(&gfs3[t], g);
-    }
-    for (int t = tid; t < 2 * 3 * kPairs; t += kFs3Block) {
-      const double g = (&GS->gb[0][0][0])[t];
-      if (g != 0.0) atomicAdd(&gfs3[2 * kCoef + t], g);
-    }
+  if (GRAD) __syncthreads();  // every pass's atomics into the gradient table are done
+  flush();
+}
+
+// Triples and blend-region triples of each frame (counts[2 f], counts[2 f + 1]).
+__global__ void k_fs3_frame_counts(const Fs3Rec *__restrict__ recs, const int *__restrict__ icnt,
+                                   int tri_cap, int frame_nm, int *counts) {
+  const int ntri = min(icnt[C_NTRI_FS3], tri_cap);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntri; t += gridDim.x * blockDim.x) {
+    const int fr = recs[t].mol[0] / frame_nm;
+    atomicAdd(&counts[2 * fr], 1);
+    if (recs[t].branch == 2) atomicAdd(&counts[2 * fr + 1], 1);
   }
 }
 
@@ -732,7 +764,8 @@ template <typename T, bool GRAD>
 cudaError_t launch_fs3_t(const Fs3Rec *R, const int *icnt, int tri_cap, const double4 *s17,
                          const double *coef, const double *bgr, int nm, int ns, double *f,
                          double *fc3, double *scal, int nsm, int triples_per_block,
-                         int blocks_per_sm, double *gfs3, cudaStream_t st) {
+                         int blocks_per_sm, double *gfs3, int frame_nm, int scal_stride,
+                         cudaStream_t st) {
   const size_t smem = GRAD ? fs3_grad_offset<T>() + sizeof(Fs3Grad<T>) : sizeof(Fs3Smem<T>);
   cudaError_t e = cudaFuncSetAttribute(k_fs3<T, GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
@@ -746,26 +779,39 @@ cudaError_t launch_fs3_t(const Fs3Rec *R, const int *icnt, int tri_cap, const do
   if (blocks_per_sm > 0 && blocks_per_sm < per_sm && grid > nsm * blocks_per_sm)
     grid = nsm * blocks_per_sm;
   k_fs3<T, GRAD><<<grid, kFs3Block, smem, st>>>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3,
-                                                scal, gfs3);
+                                                scal, gfs3, frame_nm, scal_stride);
   return cudaGetLastError();
 }
 }  // namespace
 
+cudaError_t launch_fs3_frame_counts(const void *rec, const int *icnt, int tri_cap, int frame_nm,
+                                    int *counts, cudaStream_t st) {
+  k_fs3_frame_counts<<<148 * 4, 256, 0, st>>>(static_cast<const Fs3Rec *>(rec), icnt, tri_cap,
+                                              frame_nm, counts);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fs3(int precision, const void *rec, const int *icnt, int tri_cap,
                        const double4 *s17, const double *coef, const double *bgr, int nm, int ns,
                        double *f, double *fc3, double *scal, int nsm, int triples_per_block,
-                       int blocks_per_sm, double *gfs3, cudaStream_t st) {
+                       int blocks_per_sm, double *gfs3, cudaStream_t st, int frame_nm,
+                       int scal_stride) {
   const Fs3Rec *R = static_cast<const Fs3Rec *>(rec);
+  if (frame_nm <= 0) frame_nm = nm;
   if (precision == 0) {
     if (gfs3)
       return launch_fs3_t<double, true>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal,
-                                        nsm, triples_per_block, blocks_per_sm, gfs3, st);
+                                        nsm, triples_per_block, blocks_per_sm, gfs3, frame_nm,
+                                        scal_stride, st);
     return launch_fs3_t<double, false>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
-                                       triples_per_block, blocks_per_sm, nullptr, st);
+                                       triples_per_block, blocks_per_sm, nullptr, frame_nm,
+                                       scal_stride, st);
   }
   if (gfs3)
     return launch_fs3_t<float, true>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
-                                     triples_per_block, blocks_per_sm, gfs3, st);
+                                     triples_per_block, blocks_per_sm, gfs3, frame_nm,
+                                     scal_stride, st);
   return launch_fs3_t<float, false>(R, icnt, tri_cap, s17, coef, bgr, nm, ns, f, fc3, scal, nsm,
-                                    triples_per_block, blocks_per_sm, nullptr, st);
+                                    triples_per_block, blocks_per_sm, nullptr, frame_nm,
+                                    scal_stride, st);
 }

@@ -49,8 +49,9 @@ __global__ void k_prep(const double *__restrict__ x, const double *__restrict__ 
 // ------------------------------------------------------------------- neighbours
 // One block per molecule i: candidates j != i with the reference's minimum-image COM
 // vector (computed exactly as the reference does) and |r|^2 < rlist2, written in
-// increasing j.
-__global__ void k_neighbors(const double4 *__restrict__ com, int nm, double box,
+// increasing j.  The molecules come in frames of frame_nm (independent boxes of one batch;
+// frame_nm = nm for a single box): the candidates of i are the molecules of its own frame.
+__global__ void k_neighbors(const double4 *__restrict__ com, int nm, int frame_nm, double box,
                             double rlist2, int cap, int *nbr, double4 *nbrv, int *ncnt,
                             int *icnt) {
   __shared__ int warp_tot[32];
@@ -60,11 +61,12 @@ __global__ void k_neighbors(const double4 *__restrict__ com, int nm, double box,
   __syncthreads();
   const double4 ci = com[i];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int j0 = 0; j0 < nm; j0 += blockDim.x) {
+  const int jb = (i / frame_nm) * frame_nm, je = min(jb + frame_nm, nm);
+  for (int j0 = jb; j0 < je; j0 += blockDim.x) {
     int j = j0 + threadIdx.x;
     bool keep = false;
     double4 v;
-    if (j < nm && j != i) {
+    if (j < je && j != i) {
       double4 cj = com[j];
       double xcc = minimg(xsub(ci.x, cj.x), box);
       double ycc = minimg(xsub(ci.y, cj.y), box);
@@ -732,8 +734,10 @@ cudaError_t launch_prep(const double *x, const double *y, const double *z, const
 }
 
 cudaError_t launch_neighbors(const double4 *com, int nm, double box, double rlist2, int cap,
-                             int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st) {
-  k_neighbors<<<nm, 128, 0, st>>>(com, nm, box, rlist2, cap, nbr, nbrv, ncnt, icnt);
+                             int *nbr, double4 *nbrv, int *ncnt, int *icnt, cudaStream_t st,
+                             int frame_nm) {
+  k_neighbors<<<nm, 128, 0, st>>>(com, nm, frame_nm > 0 ? frame_nm : nm, box, rlist2, cap, nbr,
+                                  nbrv, ncnt, icnt);
   return cudaGetLastError();
 }
 
