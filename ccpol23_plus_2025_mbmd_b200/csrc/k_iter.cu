@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(kThreads)
     k_iter_a(IterArgs A) {
   // no test of the finished flag here: a step after the finish only rewrites the T.mu
   // scratch and S(k), which the next use clears, and it saves a dependent load per step
-  pdl_launch_dependents();
   pdl_wait();  // the previous step's dipoles (and its gather's last use of the S(k) buffer)
   const int nA = (A.nw + kWarps - 1) / kWarps;
   PcgIn pin;
@@ -234,6 +233,9 @@ __global__ void __launch_bounds__(kThreads)
     else
       tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, MuIn{A.mu}, ex, ey,
                ez);
+    // the next kernel may launch once every block is this far: late enough that its blocks
+    // do not hold SM slots (which concurrent kernels could use) for long while they wait
+    pdl_launch_dependents();
     if (lane == 0) {
       A.eim[(size_t)w * 3 + 0] = ex;
       A.eim[(size_t)w * 3 + 1] = ey;
@@ -268,6 +270,7 @@ __global__ void __launch_bounds__(kThreads)
     a0 += dk * ph.x;
     a1 += dk * ph.y;
   }
+  pdl_launch_dependents();
   // kspace_efield_idm's weight (nb_induction_model.f90:2560-2600), applied before the merge
   const double g = -4.0 * K.ak;
   atomicAdd(&A.sk[(size_t)k * 4 + 2 * A.par], g * a0);
@@ -357,7 +360,6 @@ __global__ void __launch_bounds__(kThreads)
     k_iter_b(IterArgs A) {
   // kGatherSites polarisable sites per block; the 8 warps split the k-vectors, so every
   // k-vector's weights are loaded once per block and reused for all its sites
-  pdl_launch_dependents();
   pdl_wait();  // T.mu, S(k) and the step scalars of this step's first kernel
   if (A.state[kIterFinished] != 0.0) return;  // finished in an earlier step of this pass
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -386,6 +388,7 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
+  pdl_launch_dependents();  // the gather, the bulk of the kernel, is done
   __shared__ double part[kWarps][kGatherSites * 3];
 #pragma unroll
   for (int g = 0; g < kGatherSites; g++)

@@ -110,18 +110,15 @@ def test_mixed_solver_error_against_fp64(product):
 
 
 @pytest.mark.parametrize("name", ["c2_512", "ragged_37"])
-def test_mixed_fs2_against_fp64(product, boxes, name):
-    """FS2 with FP32 spectator terms: its energy within 1e-4 (the FS2 sum over a spectator's
-    five neutral-summing charges and over spectators of both signs cancels to ~1e-2-1e-3 of
-    its terms; 2.7e-5 measured at 512 waters) and its COM forces within 1e-5 of the FP64
-    kernel's; the three-body site forces and virial (FS2 and FS3 together, the
-    threebody_term outputs) within 1e-5."""
-    if name == "ragged_37":
-        m, b, _ = boxes[name]
-    else:
-        cfg = CONFIGS[name]
-        m = Model(data_dir(cfg["variant"]))
-        b = water_box(m, cfg["nm"], cfg["box"], cfg["seed"])
+def test_mixed_fs2_against_fp64(product, name):
+    """FS2 alone (FS3 switched off in the model) with FP32 spectator terms against the FP64
+    kernel: energy within 1e-4 (the FS2 sum over a spectator's five charges, which add up to
+    zero, and over spectators of both signs cancels to ~1e-2-1e-3 of its terms; 2.7e-5
+    measured at 512 waters), site forces, COM forces and virial within 1e-5."""
+    cfg = CONFIGS[name] if name in CONFIGS else dict(nm=37, box=10.37, variant="fs2fs3", seed=9)
+    m = Model(data_dir(cfg["variant"]))
+    m.set("S3_term", 0)
+    b = water_box(m, cfg["nm"], cfg["box"], cfg["seed"], ld=31 if name == "ragged_37" else None)
     out = {}
     for prec in ("fp64", "mixed"):
         with Context(m, b.nm, b.box, precision=prec) as c:
@@ -131,6 +128,7 @@ def test_mixed_fs2_against_fp64(product, boxes, name):
             vir = np.zeros(1)
             e2, e3 = c.threebody_term(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box, fx, fy, fz, *c2,
                                       *c3, vir)
+            assert e3 == 0.0
             out[prec] = (e2, np.stack([fx, fy, fz]), np.stack(c2), vir[0])
     e64, F64, C64, v64 = out["fp64"]
     emx, Fmx, Cmx, vmx = out["mixed"]
