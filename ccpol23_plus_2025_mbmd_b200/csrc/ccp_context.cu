@@ -174,6 +174,7 @@ struct ccp_context {
   double dip_tol_debye = 1e-8;
   int opt_pdl = 1;  // the dipole-step kernels with programmatic dependent launch
   int opt_fs3_low = 1;  // mixed form: FS3's ik/jk gradient passes in FP32 (0: all FP64)
+  int opt_fs3_prio = 0;  // FS3's stream at the high priority of the Ewald/induction chain
   bool pcg_active = false;  // the solver of the last solve was PCG
   // phase timing (diagnostics)
   bool timing = false;
@@ -1411,6 +1412,19 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_pdl = value != 0;
   } else if (n == "fs3_fp32_passes") {
     ctx->opt_fs3_low = value != 0;
+  } else if (n == "fs3_high_priority") {
+    // FS3's side stream at the chain's high priority (1) or the low one (0)
+    if ((value != 0) != (ctx->opt_fs3_prio != 0)) {
+      CK(cudaSetDevice(ctx->device));
+      CK(cudaStreamSynchronize(ctx->s_fs3));
+      int prio_lo = 0, prio_hi = 0;
+      cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+      cudaStream_t s = nullptr;
+      CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, value ? prio_hi : prio_lo));
+      cudaStreamDestroy(ctx->s_fs3);
+      ctx->s_fs3 = s;
+      ctx->opt_fs3_prio = value != 0;
+    }
   } else if (n == "dipole_solver") {
     if (value < 0 || value > 2) {
       set_error("ccp_context_set_option: dipole_solver must be 0 (Jacobi), 1 (PCG, the "
@@ -1460,6 +1474,8 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_pdl;
   } else if (n == "fs3_fp32_passes") {
     *value = ctx->opt_fs3_low;
+  } else if (n == "fs3_high_priority") {
+    *value = ctx->opt_fs3_prio;
   } else if (n == "cell_list_active") {
     *value = ctx->cells_active ? 1 : 0;
   } else if (n == "dipole_solver_pcg_active") {
