@@ -402,6 +402,8 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
      "fs3_fp32_passes" 1 (default): in the CCP_MIXED form FS3's ik and jk gradient passes run
                      in FP32; 0: they run in FP64 as in CCP_FP64 (the rest of the mixed form
                      unchanged);
+     "fs3_high_priority" 0 (default): FS3's side stream at the low priority (1: at the
+                     Ewald/induction chain's high priority);
      "pdl"           1 (default): the two kernels of a dipole step are launched with
                      programmatic dependent launch (each starts while its predecessor drains);
      "cell_list"     1 (default): the neighbour lists come from a cell list when the box holds
