@@ -28,7 +28,7 @@ using namespace ccpd;
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;  // small blocks fit beside two FS3 blocks on an SM (see the step kernels)
 
 // Programmatic dependent launch (sm_90+): `launch_dependents` lets the next kernel in the
 // stream (launched with programmatic stream serialization) start its blocks once every block

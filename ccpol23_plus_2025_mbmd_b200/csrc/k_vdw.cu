@@ -19,13 +19,15 @@ constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 
 // Tang-Toennies f_N(delta r) and its derivative (utility.f90:89-125) from one exponential.
+// The series' divisions by i are products with the reciprocals 1/i (compile-time constants):
+// FP64 divisions would dominate the kernel.
 template <int N>
 __device__ __forceinline__ void tt_both(double delta, double r, double &f, double &df) {
   const double dr = delta * r, ex = exp(-dr);
   double term = 1.0, sum = 1.0;
 #pragma unroll
   for (int i = 1; i <= N; i++) {
-    term = term * dr / (double)i;
+    term = term * dr * (1.0 / (double)i);
     sum += term;
   }
   f = 1.0 - ex * sum;
@@ -73,6 +75,7 @@ __global__ void __launch_bounds__(kThreads)
         const double rsx = c.x + sxi - sxj, rsy = c.y + syi - syj, rsz = c.z + szi - szj;
         const double rssq = rsx * rsx + rsy * rsy + rsz * rsz;
         const double sqr = sqrt(rssq);
+        const double ir = 1.0 / sqr, ir2 = ir * ir;  // one division serves every 1/r^n
         // exchange-repulsion with the short-range damping
         const double eks = exp(-beta * sqr);
         const double poly = c0 + c1 * sqr + c2 * sqr * sqr + c3 * sqr * sqr * sqr;
@@ -88,30 +91,30 @@ __global__ void __launch_bounds__(kThreads)
         if (qab != 0.0) {
           double f1, df1;
           tt_both<1>(d1, sqr, f1, df1);
-          u += kR4pie0 * (f1 - 1.0) * qab / sqr;
-          du += -kR4pie0 * qab * ((f1 - 1.0) / rssq - df1 / sqr);
+          u += kR4pie0 * (f1 - 1.0) * qab * ir;
+          du += -kR4pie0 * qab * ((f1 - 1.0) * ir2 - df1 * ir);
         }
-        const double r6 = rssq * rssq * rssq, r8 = rssq * r6, r10 = rssq * r8;
+        const double ir6 = ir2 * ir2 * ir2, ir8 = ir2 * ir6, ir10 = ir2 * ir8;
         if (c6 != 0.0) {
           double f6, df6;
           tt_both<6>(d6, sqr, f6, df6);
-          u += -f6 * c6 / r6;
-          du += -df6 * c6 / r6 + 6.0 * f6 * c6 / (r6 * sqr);
+          u += -f6 * c6 * ir6;
+          du += -df6 * c6 * ir6 + 6.0 * f6 * c6 * ir6 * ir;
         }
         if (c8 != 0.0) {
           double f8, df8;
           tt_both<8>(d8, sqr, f8, df8);
-          u += -f8 * c8 / r8;
-          du += -df8 * c8 / r8 + 8.0 * f8 * c8 / (r8 * sqr);
+          u += -f8 * c8 * ir8;
+          du += -df8 * c8 * ir8 + 8.0 * f8 * c8 * ir8 * ir;
         }
         if (c10 != 0.0) {
           double f10, df10;
           tt_both<10>(d10, sqr, f10, df10);
-          u += -f10 * c10 / r10;
-          du += -df10 * c10 / r10 + 10.0 * f10 * c10 / (r10 * sqr);
+          u += -f10 * c10 * ir10;
+          du += -df10 * c10 * ir10 + 10.0 * f10 * c10 * ir10 * ir;
         }
         e += u;
-        const double vf = -du / sqr;
+        const double vf = -du * ir;
         gx = rsx * vf;
         gy = rsy * vf;
         gz = rsz * vf;
