@@ -91,3 +91,31 @@ def test_fs3_table_reuse_matches_single_triple_blocks(box, precision):
     assert e8["vir"] == pytest.approx(e1["vir"], rel=1e-12)
     assert rel(f8, f1) <= 1e-12
     assert rel(c8, c1) <= 1e-12
+
+
+@pytest.mark.parametrize("opt,values", [("pdl", (1, 0)), ("fs3_high_priority", (1, 0)),
+                                        ("graph_loop", (1, 0))])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_launch_options_give_the_same_results(box, opt, values, precision):
+    """Programmatic dependent launch of the dipole steps, FS3's stream priority and the graph
+    against the host-driven loop change how the work is launched, not what it computes."""
+    m, b = box
+    nm, ld = b.xs.shape
+    out = []
+    for v in values:
+        args = [_dev(a) for a in (b.x, b.y, b.z, b.xs, b.ys, b.zs)]
+        f = [_zeros((nm, ld)) for _ in range(3)]
+        mu = [_zeros((nm, ld)) for _ in range(3)]
+        with Context(m, nm, b.box, precision=precision) as c:
+            c.set_option(opt, v)
+            assert c.get_option(opt) == v
+            e = c.terms_device(_lib.TERM_HOT, *args, b.box, *f, None, None, None, None, None,
+                               None, *mu)
+        out.append((e, np.stack([t.cpu().numpy() for t in f]),
+                    np.stack([t.cpu().numpy() for t in mu])))
+    (e1, f1, m1), (e0, f0, m0) = out
+    assert e1["ind_iters"] == e0["ind_iters"]
+    for k in ENERGIES:
+        assert e1[k] == pytest.approx(e0[k], rel=1e-12), k
+    assert rel(f1, f0) <= 1e-12
+    assert rel(m1, m0) <= 1e-12
