@@ -56,6 +56,7 @@ cudaError_t dalloc(T **p, size_t n) {
 
 struct ccp_context {
   int device = 0, precision = CCP_FP64, nm = 0, ns = 0, npol = 0, nsm = 148;
+  size_t l2_bytes = size_t(126) << 20;  // the device's L2 size
   cudaStream_t own = nullptr, stream = nullptr;
   // model-derived constants
   SiteSets S{};
@@ -164,6 +165,13 @@ struct ccp_context {
   double2 *d_P = nullptr;
   size_t P_cap = 0;
   bool use_P = false;
+  // with the factor tables, the full phase matrix [site][k] of the polarisable sites when it
+  // fits full_phase_budget (k_iter.cu, launch_phase_matrix)
+  double2 *d_PM = nullptr;
+  size_t PM_cap = 0;
+  bool use_PM = false;
+  int opt_pm = 1;  // the full phase matrix when it fits (1) or never (0)
+  int opt_sum_sites = 32, opt_gather_sites = 4;  // block shapes of the dipole step (IterArgs)
   // options (ccp_context_set_option)
   int opt_graph = 1;  // Jacobi loop as a conditional graph (1) or driven from the host (0)
   int opt_phase = 1;  // phase-factor tables when they fit (1) or never (0)
@@ -223,6 +231,7 @@ void free_ctx(ccp_context *c) {
   if (c->d_ticket) cudaFree(c->d_ticket);
   if (c->h_md) cudaFreeHost(c->h_md);
   if (c->d_P) cudaFree(c->d_P);
+  if (c->d_PM) cudaFree(c->d_PM);
   if (c->h_istate) cudaFreeHost(c->h_istate);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   if (c->s_fs3) cudaStreamDestroy(c->s_fs3);
@@ -371,6 +380,11 @@ struct EvalOut {
 // Largest phase-factor tables kept for the dipole iteration (nlm + nz complex numbers per
 // polarisable site: 5 MB at 512 waters, 46 MB at 2048).
 constexpr size_t kPhaseBudget = size_t(1) << 30;
+// The full phase matrix (16 bytes per polarisable site and k-vector: 38 MB at 512 waters,
+// 568 MB at 2048) pays only while it stays in L2, which it is read from twice per step: it
+// is used when it fits in half of the L2.  Streamed from HBM (2048 waters) it made the dipole
+// step slower than the factor tables and evicted the concurrent kernels' working sets.
+size_t full_phase_budget(const ccp_context *c) { return c->l2_bytes / 2; }
 
 constexpr double kIndThr = 1.0e-20;  // iteridm convergence threshold on sum |dmu|^2
 constexpr double kDebyePerEA = 4.80320471;  // Debye per e*Angstrom (dipoles are in e*A)
@@ -412,6 +426,7 @@ IterArgs make_iter_args(ccp_context *c, cudaGraphConditionalHandle handle, int u
   A.nz = 2 * c->kmax[2] + 1;
   A.XY = c->d_P;
   A.Z = c->d_P ? c->d_P + (size_t)A.nw * A.nlm : nullptr;
+  A.PM = c->use_PM ? c->d_PM : nullptr;
   A.sk = c->d_skj;
   A.par = par;
   A.scal = c->d_scal;
@@ -419,6 +434,8 @@ IterArgs make_iter_args(ccp_context *c, cudaGraphConditionalHandle handle, int u
   A.ticket = c->d_ticket;
   A.thr = ind_threshold(c);
   A.pdl = c->opt_pdl;
+  A.sum_sites = c->opt_sum_sites;
+  A.gather_sites = c->opt_gather_sites;
   if (pcg_solver(c)) {
     const size_t np3 = (size_t)A.nw * 3;
     A.cu = c->d_pcg;
@@ -472,9 +489,9 @@ int ensure_ind_graph(ccp_context *c) {
       (long long)c->d_kv,  (long long)c->d_tab,  (long long)c->d_skj, (long long)c->d_eik,
       (long long)c->d_kg,
       (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
-      (long long)c->use_P, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit,
+      (long long)c->use_P, (long long)c->d_PM, (long long)c->use_PM, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit,
       (long long)pcg_solver(c), (long long)c->opt_solver, (long long)c->d_pcg,
-      (long long)c->opt_pdl};
+      (long long)c->opt_pdl, c->opt_sum_sites, c->opt_gather_sites};
   double thr = ind_threshold(c);
   long long thr_bits;
   std::memcpy(&thr_bits, &thr, sizeof thr_bits);
@@ -574,12 +591,22 @@ int ensure_phase_matrix(ccp_context *c) {
   // the gather records pack the phase-table row of n in 8 bits
   c->use_P = c->opt_phase && c->nk > 0 && n * sizeof(double2) <= kPhaseBudget &&
              2 * c->kmax[2] + 1 <= 255;
-  if (!c->use_P || n <= c->P_cap) return CCP_OK;
-  if (c->d_P) cudaFree(c->d_P);
-  c->d_P = nullptr;
-  c->P_cap = 0;
-  CK(dalloc(&c->d_P, n));
-  c->P_cap = n;
+  const size_t npm = (size_t)c->nm * c->S.np * (size_t)c->nk;
+  c->use_PM = c->use_P && c->opt_pm && npm * sizeof(double2) <= full_phase_budget(c);
+  if (c->use_P && n > c->P_cap) {
+    if (c->d_P) cudaFree(c->d_P);
+    c->d_P = nullptr;
+    c->P_cap = 0;
+    CK(dalloc(&c->d_P, n));
+    c->P_cap = n;
+  }
+  if (c->use_PM && npm > c->PM_cap) {
+    if (c->d_PM) cudaFree(c->d_PM);
+    c->d_PM = nullptr;
+    c->PM_cap = 0;
+    CK(dalloc(&c->d_PM, npm));
+    c->PM_cap = npm;
+  }
   return CCP_OK;
 }
 
@@ -789,10 +816,13 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                               c->kmax[2], c->d_mu, c->d_sk, sk));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
                               c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, fk, sk));
-      if (c->use_P)
-        LK(launch_phase_factors(c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2], c->d_P,
-                                c->d_P + (size_t)nm * S.np * (c->kmax[0] + 1) * (2 * c->kmax[1] + 1),
-                                sk));
+      if (c->use_P) {
+        const int nlm = (c->kmax[0] + 1) * (2 * c->kmax[1] + 1), nz = 2 * c->kmax[2] + 1;
+        double2 *XY = c->d_P, *Z = c->d_P + (size_t)nm * S.np * nlm;
+        LK(launch_phase_factors(c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2], XY, Z, sk));
+        if (c->use_PM)
+          LK(launch_phase_matrix(c->d_kg, c->nk, nm * S.np, nlm, nz, XY, Z, c->d_PM, sk));
+      }
       if (kfork) CK(cudaEventRecord(c->ev_k1, sk));
       if ((mask & T_KSPACE) && ewald_late) {
         LK(launch_kspace_energy(0, c->d_kv, c->nk, c->d_sk, c->alpha, c->d_scal, sk));
@@ -1160,7 +1190,10 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
     return CCP_ERR_CUDA;
   }
   cudaDeviceProp prop;
-  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) c->nsm = prop.multiProcessorCount;
+  if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) {
+    c->nsm = prop.multiProcessorCount;
+    if (prop.l2CacheSize > 0) c->l2_bytes = (size_t)prop.l2CacheSize;
+  }
   // site sets from the model's charges and polarisabilities
   SiteSets &S = c->S;
   std::memset(&S, 0, sizeof(S));
@@ -1406,6 +1439,20 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_graph = value != 0;
   } else if (n == "phase_matrix") {
     ctx->opt_phase = value != 0;
+  } else if (n == "phase_matrix_full") {
+    ctx->opt_pm = value != 0;
+  } else if (n == "dipole_sum_sites") {
+    if (value < 1 || value > 128) {
+      set_error("ccp_context_set_option: dipole_sum_sites must be 1..128");
+      return CCP_ERR_BAD_INPUT;
+    }
+    ctx->opt_sum_sites = value;
+  } else if (n == "dipole_gather_sites") {
+    if (value != 4 && value != 8) {
+      set_error("ccp_context_set_option: dipole_gather_sites must be 4 or 8");
+      return CCP_ERR_BAD_INPUT;
+    }
+    ctx->opt_gather_sites = value;
   } else if (n == "cell_list") {
     ctx->opt_cells = value != 0;
   } else if (n == "pdl") {
@@ -1464,6 +1511,14 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_phase;
   } else if (n == "phase_matrix_active") {
     *value = ctx->use_P ? 1 : 0;
+  } else if (n == "phase_matrix_full") {
+    *value = ctx->opt_pm;
+  } else if (n == "dipole_sum_sites") {
+    *value = ctx->opt_sum_sites;
+  } else if (n == "dipole_gather_sites") {
+    *value = ctx->opt_gather_sites;
+  } else if (n == "phase_matrix_full_active") {
+    *value = ctx->use_PM ? 1 : 0;
   } else if (n == "dipole_solver") {
     *value = ctx->opt_solver;
   } else if (n == "cell_list") {

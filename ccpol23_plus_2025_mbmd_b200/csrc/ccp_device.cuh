@@ -167,6 +167,10 @@ struct IterArgs {
   const double2 *XY;  // [nw][nlm] exp(i(l x + m y)), lm = l (2 mmax + 1) + m + mmax
   const double2 *Z;   // [nw][nz] exp(i n z) (conjugated for n < 0), nz = 2 nmax + 1
   int nlm, nz, mmax, nmax;
+  // [nw][nk] the phase of every (polarisable site, k-vector) pair, XY[lm] * Z[n] formed once
+  // per evaluation (launch_phase_matrix), or null: the step kernels then form each phase
+  // from the factor rows
+  const double2 *PM;
   // sk[k] holds two S(k) buffers, (re, im) of steps of parity 0 and 1: a step accumulates
   // into its own and clears the other, which the previous step's gather has finished with
   double *sk, *scal, *state;  // state: see IterStateSlot
@@ -182,6 +186,9 @@ struct IterArgs {
   // launch the two kernels of a step with programmatic dependent launch: each lets the next
   // kernel's blocks launch early and waits for its predecessor's results itself
   int pdl;
+  // block shapes: polarisable sites per structure-factor block (1..128) and per gather and
+  // update block (4 or 8)
+  int sum_sites, gather_sites;
 };
 
 // Slots of the dipole solve's state array (doubles).
@@ -285,6 +292,9 @@ cudaError_t launch_phase_factors(const double2 *tab, int nm, SiteSets S, int kl,
 cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np, const double4 *T4,
                        const double *TB, const double4 *S4, const double *SB, const double *mu,
                        double *eim, cudaStream_t st);
+cudaError_t launch_phase_matrix(const KGather *kg, int nk, int nw, int nlm, int nz,
+                                const double2 *XY, const double2 *Z, double2 *PM,
+                                cudaStream_t st);
 cudaError_t launch_dip_first(const IterArgs &A, cudaStream_t st);
 // Start of the PCG form of the solve (A.cu.. set): x = 0, u = alpha E0, state cleared.
 cudaError_t launch_pcg_first(const IterArgs &A, cudaStream_t st);

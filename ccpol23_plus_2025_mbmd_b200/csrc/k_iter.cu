@@ -39,8 +39,8 @@ __device__ __forceinline__ void pdl_launch_dependents() {
 }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 constexpr int kWarps = kThreads / 32;
-constexpr int kSumSites = 32;     // polarisable sites per structure-factor block
-constexpr int kGatherSites = 4;  // polarisable sites per gather/update block
+constexpr int kSumSitesMax = 128;  // polarisable sites per structure-factor block (A.sum_sites)
+// polarisable sites per gather/update block: a template argument, 4 or 8 (A.gather_sites)
 
 // Phase factors of polarisable site w from the per-axis tables tab[axis][l][site] (ewald.f90:
 // 960-1010): XY[w][l][m] = exp(i l x) exp(+-i |m| y) in the reference's product order, and
@@ -83,6 +83,26 @@ __device__ __forceinline__ double2 kphase(const double2 *__restrict__ xyw,
                                           const double2 *__restrict__ zw, int lm, int ni) {
   const double2 a = xyw[lm], b = zw[ni];
   return make_double2(a.x * b.x - a.y * b.y, a.y * b.x + a.x * b.y);
+}
+
+// Phase of k-vector k (rows lm, ni of the factor tables) at polarisable site w: with the
+// phase matrix one coalesced load of row w, else the product of the two factor entries.
+template <bool PM>
+__device__ __forceinline__ double2 site_phase(const IterArgs &A, int w, int k, int lm, int ni) {
+  if constexpr (PM) return A.PM[(size_t)w * A.nk + k];
+  return kphase(A.XY + (size_t)w * A.nlm, A.Z + (size_t)w * A.nz, lm, ni);
+}
+
+// The phase matrix PM[w][k] = XY[w][lm(k)] * Z[w][n(k)] (kphase, the same product the step
+// kernels form without it), one coalesced row of nk phases per polarisable site.
+__global__ void k_phase_matrix(const KGather *__restrict__ kg, int nk, int nw, int nlm, int nz,
+                               const double2 *__restrict__ XY, const double2 *__restrict__ Z,
+                               double2 *PM) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
+  const int lmni = kg[k].lmni, lm = lmni >> 8, ni = lmni & 255;
+  for (int w = blockIdx.y; w < nw; w += gridDim.y)
+    PM[(size_t)w * nk + k] = kphase(XY + (size_t)w * nlm, Z + (size_t)w * nz, lm, ni);
 }
 
 // The vector a T.mu product reads: the dipoles themselves (Jacobi).
@@ -210,7 +230,7 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-template <bool PCG>
+template <bool PCG, bool PM>
 __global__ void __launch_bounds__(kThreads)
     k_iter_a(IterArgs A) {
   // no test of the finished flag here: a step after the finish only rewrites the T.mu
@@ -244,11 +264,11 @@ __global__ void __launch_bounds__(kThreads)
     return;
   }
   // structure factors: block b covers k-vectors [kt*256, kt*256+256) and sites of chunk sc
-  __shared__ double smu[kSumSites * 3];
+  extern __shared__ double smu[];  // A.sum_sites x 3 dipole components
   const int b = blockIdx.x - nA;
   const int nkt = (A.nk + kThreads - 1) / kThreads;
   const int kt = b % nkt, sc = b / nkt;
-  const int s0 = sc * kSumSites, cnt = min(kSumSites, A.nw - s0);
+  const int s0 = sc * A.sum_sites, cnt = min(A.sum_sites, A.nw - s0);
   for (int u = threadIdx.x; u < cnt * 3; u += kThreads) {
     if constexpr (PCG) {
       const int site = s0 + u / 3;
@@ -265,7 +285,7 @@ __global__ void __launch_bounds__(kThreads)
   double a0 = 0.0, a1 = 0.0;
 #pragma unroll 4
   for (int s = 0; s < cnt; s++) {
-    const double2 ph = kphase(A.XY + (size_t)(s0 + s) * A.nlm, A.Z + (size_t)(s0 + s) * A.nz, lm, ni);
+    const double2 ph = site_phase<PM>(A, s0 + s, k, lm, ni);
     const double dk = K.rl * smu[3 * s] + K.rm * smu[3 * s + 1] + K.rn * smu[3 * s + 2];
     a0 += dk * ph.x;
     a1 += dk * ph.y;
@@ -277,13 +297,14 @@ __global__ void __launch_bounds__(kThreads)
   atomicAdd(&A.sk[(size_t)k * 4 + 2 * A.par + 1], g * a1);
 }
 
-// The PCG step's update for the kGatherSites sites of a block, after the reciprocal field of
+// The PCG step's update for the GS sites of a block, after the reciprocal field of
 // u is in `part`: the vectors of the step (s, p, x, u, w = A u) in place, the partial sums
 // of (u, M u), (w, u), |u|^2 and the energy -1/2 x.E0 (the reference's energy expression at
 // the iterate), and in the last block to finish the step's scalars and the convergence test
 // on sum |u|^2, the Jacobi update's norm at the iterate.
+template <int GS>
 __device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk,
-                                           const double (*part)[kGatherSites * 3]) {
+                                           const double (*part)[GS * 3]) {
   double gam = 0.0, del = 0.0, ch = 0.0, en = 0.0;
   if ((int)threadIdx.x < ns_blk) {
     const int g = threadIdx.x, w = w0 + g;
@@ -355,19 +376,19 @@ __device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk
   }
 }
 
-template <bool PCG>
+template <bool PCG, bool PM, int GS>
 __global__ void __launch_bounds__(kThreads)
     k_iter_b(IterArgs A) {
-  // kGatherSites polarisable sites per block; the 8 warps split the k-vectors, so every
+  // GS polarisable sites per block; the warps split the k-vectors, so every
   // k-vector's weights are loaded once per block and reused for all its sites
   pdl_wait();  // T.mu, S(k) and the step scalars of this step's first kernel
   if (A.state[kIterFinished] != 0.0) return;  // finished in an earlier step of this pass
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int w0 = blockIdx.x * kGatherSites;
-  const int ns_blk = min(kGatherSites, A.nw - w0);
-  double acc[kGatherSites][3];
+  const int w0 = blockIdx.x * GS;
+  const int ns_blk = min(GS, A.nw - w0);
+  double acc[GS][3];
 #pragma unroll
-  for (int g = 0; g < kGatherSites; g++) acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
+  for (int g = 0; g < GS; g++) acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
   const double2 *skp = reinterpret_cast<const double2 *>(A.sk) + A.par;
 #pragma unroll 2
   for (int k = threadIdx.x; k < A.nk; k += kThreads) {
@@ -377,10 +398,9 @@ __global__ void __launch_bounds__(kThreads)
     const double2 f = skp[2 * (size_t)k];
     const double f0 = f.x, f1 = f.y;
 #pragma unroll
-    for (int g = 0; g < kGatherSites; g++) {
+    for (int g = 0; g < GS; g++) {
       if (g < ns_blk) {
-        const double2 ph = kphase(A.XY + (size_t)(w0 + g) * A.nlm, A.Z + (size_t)(w0 + g) * A.nz,
-                                  lm, ni);
+        const double2 ph = site_phase<PM>(A, w0 + g, k, lm, ni);
         const double t = ph.x * f0 + ph.y * f1;
         acc[g][0] += K.rl * t;
         acc[g][1] += K.rm * t;
@@ -389,9 +409,9 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   pdl_launch_dependents();  // the gather, the bulk of the kernel, is done
-  __shared__ double part[kWarps][kGatherSites * 3];
+  __shared__ double part[kWarps][GS * 3];
 #pragma unroll
-  for (int g = 0; g < kGatherSites; g++)
+  for (int g = 0; g < GS; g++)
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       const double v = warp_sum(acc[g][c]);
@@ -399,7 +419,7 @@ __global__ void __launch_bounds__(kThreads)
     }
   __syncthreads();
   if constexpr (PCG) {
-    pcg_update(A, w0, ns_blk, part);
+    pcg_update<GS>(A, w0, ns_blk, part);
     return;
   }
   double ch = 0.0, en = 0.0;
@@ -549,11 +569,12 @@ cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np,
 
 // Launches a step kernel, with programmatic stream serialization when A.pdl is set.
 template <typename Kernel>
-cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream_t st) {
+cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream_t st,
+                        size_t smem = 0) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -564,14 +585,39 @@ cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream
 }
 
 cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st) {
+  if (A.sum_sites < 1 || A.sum_sites > kSumSitesMax) return cudaErrorInvalidValue;
+  const size_t smem = sizeof(double) * 3 * A.sum_sites;
   const int nA = (A.nw + kWarps - 1) / kWarps;
   const int nkt = (A.nk + kThreads - 1) / kThreads;
-  const int nsc = (A.nw + kSumSites - 1) / kSumSites;
-  return A.cu ? launch_step(k_iter_a<true>, nA + nkt * nsc, A, st)
-              : launch_step(k_iter_a<false>, nA + nkt * nsc, A, st);
+  const int nsc = (A.nw + A.sum_sites - 1) / A.sum_sites;
+  const int nb = nA + nkt * nsc;
+  if (A.PM)
+    return A.cu ? launch_step(k_iter_a<true, true>, nb, A, st, smem)
+                : launch_step(k_iter_a<false, true>, nb, A, st, smem);
+  return A.cu ? launch_step(k_iter_a<true, false>, nb, A, st, smem)
+              : launch_step(k_iter_a<false, false>, nb, A, st, smem);
+}
+
+template <int GS>
+cudaError_t launch_iter_b_gs(const IterArgs &A, cudaStream_t st) {
+  const int nb = (A.nw + GS - 1) / GS;
+  if (A.PM)
+    return A.cu ? launch_step(k_iter_b<true, true, GS>, nb, A, st)
+                : launch_step(k_iter_b<false, true, GS>, nb, A, st);
+  return A.cu ? launch_step(k_iter_b<true, false, GS>, nb, A, st)
+              : launch_step(k_iter_b<false, false, GS>, nb, A, st);
 }
 
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
-  const int nb = (A.nw + kGatherSites - 1) / kGatherSites;
-  return A.cu ? launch_step(k_iter_b<true>, nb, A, st) : launch_step(k_iter_b<false>, nb, A, st);
+  if (A.gather_sites != 4 && A.gather_sites != 8) return cudaErrorInvalidValue;
+  return A.gather_sites == 8 ? launch_iter_b_gs<8>(A, st) : launch_iter_b_gs<4>(A, st);
+}
+
+cudaError_t launch_phase_matrix(const KGather *kg, int nk, int nw, int nlm, int nz,
+                                const double2 *XY, const double2 *Z, double2 *PM,
+                                cudaStream_t st) {
+  if (nk <= 0 || nw <= 0) return cudaSuccess;
+  const dim3 grid((nk + 127) / 128, nw < 1024 ? nw : 1024);
+  k_phase_matrix<<<grid, 128, 0, st>>>(kg, nk, nw, nlm, nz, XY, Z, PM);
+  return cudaGetLastError();
 }
