@@ -41,10 +41,12 @@ CONFIG = "c2_512"
 # representation), as the reference computes it: ~130 FLOP + 15 MUFU-class operations
 # (6 exp, 3 sqrt, 6 reciprocals).  Counted as 145 floating-point operations.
 FS3_FLOP_PER_SITE_TRIPLE = 145.0
-# Precision forms the bench can time: context precision and options.  "mixed_fs3fp64" is the
-# mixed form with FS3's gradient passes in FP64 (PCG dipoles and FP32 FS2 terms only).
+# Precision forms the bench can time: context precision and options.  "mixed" is the
+# library's mixed form (PCG dipoles, FP32 FS2 terms, FP64 FS3); "mixed_fs3fp32" adds FS3's ik
+# and jk gradient passes in FP32, which meets the 1e-5 force bar at 512 waters but not at
+# 2048 (the headline is taken only among the forms that meet it on the box timed).
 FORMS = {"fp64": ("fp64", {}), "mixed": ("mixed", {}),
-         "mixed_fs3fp64": ("mixed", {"fs3_fp32_passes": 0})}
+         "mixed_fs3fp32": ("mixed", {"fs3_fp32_passes": 1})}
 
 
 def open_context(model, box, device, form):
@@ -336,6 +338,55 @@ def run_single(which, host_loop=False):
                               "n_fs2_triples": e["n_fs2_triples"]}), flush=True)
 
 
+def run_floor(config, steps, warmup):
+    """The critical-path floor of the evaluation, per form (one JSON line each): the
+    Ewald/induction chain alone (self, real, reciprocal, induction), its dipole loop within
+    that, the three-body terms alone, FS3 alone, the whole step with the terms overlapping
+    (with the loop's and FS3's own durations there) and with them in order on one stream.
+    CUDA events on torch's current stream around each evaluation, L2 flushed before each,
+    means over `steps` evaluations after `warmup`."""
+    import torch
+    from ccpol23_plus_2025_mbmd_b200 import _lib
+    model, box, cfg = build_inputs(0, config)
+    dev = torch.device("cuda", 0)
+    T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
+    args = [T(a) for a in (box.x, box.y, box.z, box.xs, box.ys, box.zs)]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    chain = _lib.TERM_SELF | _lib.TERM_RSPACE | _lib.TERM_KSPACE | _lib.TERM_INDUCTION
+    three = _lib.TERM_FS2 | _lib.TERM_FS3
+
+    def timed(ctx, terms):
+        ms, ph = [], []
+        for it in range(warmup + steps):
+            flush.add_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            ctx.terms_device(terms, *args, box.box)
+            e1.record()
+            torch.cuda.synchronize()
+            if it >= warmup:
+                ms.append(e0.elapsed_time(e1))
+                ph.append(ctx.phase_ms())
+        return float(np.mean(ms)), np.mean(ph, axis=0)
+
+    for form in ("fp64", "mixed"):
+        with open_context(model, box, 0, form) as ctx:
+            ctx.set_stream(torch.cuda.current_stream().cuda_stream)
+            ctx.set_timing(True)
+            r = {"box": config, "nm": box.nm, "form": form}
+            r["chain_alone_ms"], ph = timed(ctx, chain)
+            r["loop_alone_ms"] = float(ph[4])
+            r["three_body_alone_ms"], _ = timed(ctx, three)
+            r["fs3_alone_ms"], _ = timed(ctx, _lib.TERM_FS3)
+            r["step_overlapped_ms"], ph = timed(ctx, _lib.TERM_HOT)
+            r["loop_overlapped_ms"], r["fs3_overlapped_ms"] = float(ph[4]), float(ph[8])
+            ctx.set_option("overlap", 0)
+            r["step_serial_ms"], _ = timed(ctx, _lib.TERM_HOT)
+            print(json.dumps({k: round(v, 4) if isinstance(v, float) else v
+                              for k, v in r.items()}), flush=True)
+
+
 def equilibrate(ctx, box, nsteps, temp=298.0, every=20):
     """Velocity-rescaled MD from the synthetic start (its jittered lattice is far from
     equilibrium): every `every` steps the COM velocities and angular momenta are scaled to
@@ -512,6 +563,9 @@ def main():
     ap.add_argument("--fort401", action="store_true",
                     help="time the reference's own published case (256 waters, npt_b, one MD "
                          "step) on the device and on 1 and all host threads, and print that line")
+    ap.add_argument("--floor", action="store_true",
+                    help="print the critical-path floor table (chain, dipole loop, three-body "
+                         "terms and FS3 alone, overlapped and in order) per form instead")
     ap.add_argument("--host-loop", action="store_true",
                     help="with --single: drive the dipole iteration from the host, so that "
                          "profilers see its kernels")
@@ -521,6 +575,9 @@ def main():
         return
     if args.single:
         run_single(args.single, args.host_loop)
+        return
+    if args.floor:
+        run_floor(args.config, args.steps, args.warmup)
         return
     if args.nve:
         run_nve(args.nve, args.nve_equil)
@@ -543,7 +600,7 @@ def main():
 
     model, box, cfg = build_inputs(rank, args.config)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
-    forms = ["fp64", "mixed"] + (["mixed_fs3fp64"] if args.config != CONFIG else [])
+    forms = ["fp64", "mixed", "mixed_fs3fp32"]
     results = {}
     with ClockSampler(local) as clk:
         for prec in forms:
@@ -626,9 +683,9 @@ def main():
     site_triples = (e["n_fs3_triples"] + e["n_fs3_blend"]) * 17 ** 3
     fs3_s = H["fs3_ms"] * 1e-3
     achieved = FS3_FLOP_PER_SITE_TRIPLE * site_triples / fs3_s / 1e12
-    # both forms against the FP64 pipe: the mixed kernel keeps the site-pair tables, the
-    # energy pass, the force weights and the site forces in FP64 and runs two of the three
-    # gradient passes in FP32, so the FP64 peak bounds it except for that FP32 share
+    # every form against the FP64 pipe: FS3 is FP64 except, in mixed_fs3fp32, two of its three
+    # gradient passes (the site-pair tables, the energy pass, the force weights and the site
+    # forces stay FP64), so the FP64 peak bounds it except for that FP32 share
     peak = peak64
     iso_s = results[head]["fs3_isolated_ms"] * 1e-3
     iso = FS3_FLOP_PER_SITE_TRIPLE * site_triples / iso_s / 1e12
@@ -637,7 +694,7 @@ def main():
         "value": out[head]["ns_day"], "unit": "ns/day", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": H["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32+f64" if head == "mixed" else "f64",  # mixed_fs3fp64: FP32 only in FS2
+        "dtype": "f64" if head == "fp64" else "f32+f64",
         "data": "synthetic (seeded jittered-lattice water box, 298 K)",
         "config": {"workload": f"{box.nm} H2O FS2+FS3 hot-path force evaluation (Ewald self/real/"
                                "recip + induced-dipole solve + induction forces + FS2 + FS3)",
@@ -662,7 +719,7 @@ def main():
         "e2e": {"value": H["e2e_ns_day"], "unit": "ns/day",
                 "h2d_bytes_per_step": results[head]["h2d"], "d2h_bytes_per_step": results[head]["d2h"]},
         "roofline": {"bound": "fp64_pipe",
-                     "kernel": "k_fs3<float>" if head == "mixed" else "k_fs3<double>",
+                     "kernel": "k_fs3<float>" if head == "mixed_fs3fp32" else "k_fs3<double>",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                      "peak_source": "measured in this run by an FMA-chain microbenchmark "
                                     "(MEASURED_PEAKS.json has no FP32/FP64 figure)",
@@ -672,15 +729,19 @@ def main():
                      "note": "achieved uses the kernel's duration in the timed steps, where it "
                              "shares the GPU with the Ewald/induction kernels; 'isolated' is the "
                              "same kernel with the three-body terms not overlapped"
-                             + ("; the mixed kernel runs two of its three gradient passes in "
-                                "FP32, the rest in FP64" if head == "mixed" else ""),
+                             + ("; this kernel runs two of its three gradient passes in "
+                                "FP32, the rest in FP64" if head == "mixed_fs3fp32" else ""),
                      "isolated": {"duration_ms": iso_s * 1e3, "achieved": iso,
                                   "frac": iso / peak},
                      # DRAM bytes (read + write) of one launch of each form, from an ncu
-                     # capture of the third launch: the triple records only, the tables and
-                     # sites stay in L2 / shared memory
-                     "traffic": 5.29e6 if head == "mixed" else 5.25e6,
-                     "traffic_unit": "bytes per launch"},
+                     # capture of the third launch on the 512-water box (31417 triples): the
+                     # triple records only, the tables and sites stay in L2 / shared memory;
+                     # on another box scaled by its triple count
+                     "traffic": (5.24e6 if head == "mixed_fs3fp32" else 5.22e6)
+                                * e["n_fs3_triples"] / 31417.0,
+                     "traffic_unit": "bytes per launch"
+                                     + ("" if args.config == CONFIG else
+                                        " (ncu capture at 512 waters scaled by the triple count)")},
         "gpu_launches": int(results[head]["launches"]),
         "clocks": clocks,
         "peaks_tflops": {"fp64_fma": peak64, "fp32_fma": peak32, "mufu_exp_tops": peak_mufu},

@@ -36,11 +36,11 @@ extern "C" {
 
 /* precision forms of a context */
 #define CCP_FP64 0   /* plain FP64 everywhere */
-#define CCP_MIXED 1  /* FP32 for two of the three FS3 gradient passes (the ik and jk
-                        pair families) and for FS2's spectator terms; the induced dipoles
-                        by preconditioned conjugate gradients in FP64 to 1e-8 D RMS (option
-                        "dipole_solver"); FP64 for the FS3 site-pair tables and energy pass,
-                        Ewald, the induction fields and forces, and all sums */
+#define CCP_MIXED 1  /* FP32 for FS2's spectator terms (and, with option
+                        "fs3_fp32_passes", for two of the three FS3 gradient passes); the
+                        induced dipoles by preconditioned conjugate gradients in FP64 to
+                        1e-8 D RMS (option "dipole_solver"); FP64 for FS3, Ewald, the
+                        induction fields and forces, and all sums */
 
 typedef struct ccp_model ccp_model;
 typedef struct ccp_context ccp_context;
@@ -399,9 +399,10 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
                      update at the iterate) to the same criterion; 2 (CCP_MIXED default): PCG
                      to an RMS update of 1e-8 D per polarisable site.  PCG needs the phase
                      table; without it the solve is Jacobi.  ind_iters then counts PCG steps;
-     "fs3_fp32_passes" 1 (default): in the CCP_MIXED form FS3's ik and jk gradient passes run
-                     in FP32; 0: they run in FP64 as in CCP_FP64 (the rest of the mixed form
-                     unchanged);
+     "fs3_fp32_passes" 0 (default): FS3 in FP64 in both forms; 1: in the CCP_MIXED form FS3's
+                     ik and jk gradient passes run in FP32 (about 3 % faster FS3; site forces
+                     within 2e-6 of FP64, but per-molecule forces 1.45e-5 off at 2048
+                     waters, above the mixed form's 1e-5 bar);
      "fs3_high_priority" 0 (default): FS3's side stream at the low priority (1: at the
                      Ewald/induction chain's high priority);
      "pdl"           1 (default): the two kernels of a dipole step are launched with

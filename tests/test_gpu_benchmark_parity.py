@@ -189,13 +189,13 @@ def test_256_frame_parameter_gradient_finite_differences(c4_frame):
 
 
 def test_2048_mixed_form_within_force_bar(product):
-    """At 2048 waters the mixed form with FS3's ik/jk passes in FP64 (PCG dipoles, FP32 FS2
-    terms) meets the 1e-5 bar; with those passes in FP32 the per-molecule forces are
-    1.45e-5 off (site forces 2.0e-6, torques 2.8e-6), which the bound below records, so that
-    form is not the large box's headline."""
+    """At 2048 waters the mixed form (PCG dipoles, FP32 FS2 terms, FS3 in FP64) meets the
+    1e-5 bar; with FS3's ik/jk passes in FP32 (option fs3_fp32_passes) the per-molecule forces
+    are 1.45e-5 off (site forces 2.0e-6, torques 2.8e-6), which the bound below records, which
+    is why those passes are not the mixed form's default."""
     m, b, cfg = _box("c5_2048")
     out = {}
-    for form, opt in (("fp64", None), ("mixed", None), ("mixed_fs3fp64", 0)):
+    for form, opt in (("fp64", None), ("mixed", None), ("mixed_fs3fp32", 1)):
         with Context(m, b.nm, b.box, precision="fp64" if form == "fp64" else "mixed") as c:
             if opt is not None:
                 c.set_option("fs3_fp32_passes", opt)
@@ -208,8 +208,8 @@ def test_2048_mixed_form_within_force_bar(product):
         return F, T, Q
 
     names = ("site force", "molecule force", "torque")
-    for name, a, ref in zip(names, parts(out["mixed_fs3fp64"]), parts(out["fp64"])):
+    for name, a, ref in zip(names, parts(out["mixed"]), parts(out["fp64"])):
         assert rel(a, ref) <= MIXED_FTOL, (name, rel(a, ref))
-    for name, a, ref, bound in zip(names, parts(out["mixed"]), parts(out["fp64"]),
+    for name, a, ref, bound in zip(names, parts(out["mixed_fs3fp32"]), parts(out["fp64"]),
                                    (MIXED_FTOL, 2e-5, MIXED_FTOL)):
         assert rel(a, ref) <= bound, (name, rel(a, ref))

@@ -4,11 +4,13 @@
   1e-8 D RMS): at the reference's own criterion it reproduces the oracle's Jacobi solution;
   its graph and host-driven loops agree; it reports non-convergence at maxit like Jacobi.
 - FS2 with FP32 spectator terms: energy, site forces and COM forces against the FP64 form.
+- FS3 with its ik/jk gradient passes in FP32 (an option, off by default): against the FP64
+  kernel.
 """
 import numpy as np
 import pytest
 
-from ccpol23_plus_2025_mbmd_b200 import CcpError, Context, Model, data_dir
+from ccpol23_plus_2025_mbmd_b200 import CcpError, Context, Model, _lib, data_dir
 from ccpol23_plus_2025_mbmd_b200.generator import CONFIGS, water_box
 
 from conftest import rel
@@ -136,3 +138,30 @@ def test_mixed_fs2_against_fp64(product, name):
     assert rel(Cmx, C64) <= 1e-5, rel(Cmx, C64)
     assert rel(Fmx, F64) <= 1e-5, rel(Fmx, F64)
     assert abs(vmx - v64) <= 1e-5 * abs(v64), (vmx, v64)
+
+
+def test_fs3_fp32_passes_against_fp64(product):
+    """FS3 alone with its ik/jk gradient passes in FP32 (option fs3_fp32_passes) against the
+    FP64 kernel at 512 waters: the energy comes from the FP64 family-0 pass and the COM forces
+    from the energy (both within 1e-12), the site forces within 1e-5 (about 2e-6 measured)."""
+    import torch
+    cfg = CONFIGS["c2_512"]
+    m = Model(data_dir(cfg["variant"]))
+    b = water_box(m, cfg["nm"], cfg["box"], cfg["seed"])
+    dev = torch.device("cuda:0")
+    out = {}
+    for opt in (0, 1):
+        args = [torch.as_tensor(np.ascontiguousarray(a), device=dev)
+                for a in (b.x, b.y, b.z, b.xs, b.ys, b.zs)]
+        f = [torch.zeros(b.xs.shape, dtype=torch.float64, device=dev) for _ in range(3)]
+        c3 = [torch.zeros(b.nm, dtype=torch.float64, device=dev) for _ in range(3)]
+        with Context(m, b.nm, b.box, precision="mixed") as c:
+            assert c.get_option("fs3_fp32_passes") == 0
+            c.set_option("fs3_fp32_passes", opt)
+            e = c.terms_device(_lib.TERM_FS3, *args, b.box, *f, None, None, None, *c3)
+        out[opt] = (e, np.stack([t.cpu().numpy() for t in f]),
+                    np.stack([t.cpu().numpy() for t in c3]))
+    (e0, f0, c0), (e1, f1, c1) = out[0], out[1]
+    assert e1["fs3pe"] == pytest.approx(e0["fs3pe"], rel=1e-12)
+    assert rel(c1, c0) <= 1e-12
+    assert 0.0 < rel(f1, f0) <= 1e-5

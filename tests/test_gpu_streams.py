@@ -73,8 +73,8 @@ def test_kspace_with_fs3_equals_separate_terms(box):
     assert rel(c3b, c33) <= 1e-12
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_fs3_table_reuse_matches_single_triple_blocks(box, precision):
+@pytest.mark.parametrize("precision,fp32_passes", [("fp64", 0), ("mixed", 0), ("mixed", 1)])
+def test_fs3_table_reuse_matches_single_triple_blocks(box, precision, fp32_passes):
     m, b = box
     nm, ld = b.xs.shape
     out = []
@@ -84,6 +84,7 @@ def test_fs3_table_reuse_matches_single_triple_blocks(box, precision):
         c3 = [_zeros(nm) for _ in range(3)]
         with Context(m, nm, b.box, precision=precision) as c:
             c.set_option("fs3_triples_per_block", tpb)
+            c.set_option("fs3_fp32_passes", fp32_passes)
             e = c.terms_device(_lib.TERM_FS3, *args, b.box, *f, None, None, None, *c3)
         out.append((e, np.stack([t.cpu().numpy() for t in f]), np.stack([t.cpu().numpy() for t in c3])))
     (e8, f8, c8), (e1, f1, c1) = out
