@@ -390,12 +390,24 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
   for (int g = 0; g < GS; g++) acc[g][0] = acc[g][1] = acc[g][2] = 0.0;
   const double2 *skp = reinterpret_cast<const double2 *>(A.sk) + A.par;
+  // the next k-vector's record and S(k) are loaded one iteration ahead, so that an iteration
+  // waits for its phase loads only, not for the record that indexes them first
+  KGather Kn{};
+  double2 fn = make_double2(0.0, 0.0);
+  if ((int)threadIdx.x < A.nk) {
+    Kn = A.kg[threadIdx.x];
+    fn = skp[2 * (size_t)threadIdx.x];
+  }
 #pragma unroll 2
   for (int k = threadIdx.x; k < A.nk; k += kThreads) {
-    const KGather K = A.kg[k];
+    const KGather K = Kn;
+    const double2 f = fn;
+    if (k + kThreads < A.nk) {
+      Kn = A.kg[k + kThreads];
+      fn = skp[2 * (size_t)(k + kThreads)];
+    }
     const int lm = K.lmni >> 8, ni = K.lmni & 255;
     // kspace_efield_idm gather (nb_induction_model.f90:2560-2600): g = -4 a_k (c S_re + s S_im)
-    const double2 f = skp[2 * (size_t)k];
     const double f0 = f.x, f1 = f.y;
 #pragma unroll
     for (int g = 0; g < GS; g++) {
