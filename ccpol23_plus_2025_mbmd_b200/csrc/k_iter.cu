@@ -39,6 +39,13 @@ __device__ __forceinline__ void pdl_launch_dependents() {
 }
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 constexpr int kWarps = kThreads / 32;
+// threads of a gather/update block (k_iter_b): they split the k-vectors, so the block's
+// serial chain of dependent loads is nk / kGatherThreads iterations long
+#ifndef CCP_GATHER_THREADS
+#define CCP_GATHER_THREADS 128
+#endif
+constexpr int kGatherThreads = CCP_GATHER_THREADS;
+constexpr int kGatherWarps = kGatherThreads / 32;
 constexpr int kSumSitesMax = 128;  // polarisable sites per structure-factor block (A.sum_sites)
 // polarisable sites per gather/update block: a template argument, 4 or 8 (A.gather_sites)
 
@@ -309,7 +316,7 @@ __device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk
   if ((int)threadIdx.x < ns_blk) {
     const int g = threadIdx.x, w = w0 + g;
     double ek[3] = {0.0, 0.0, 0.0};
-    for (int u = 0; u < kWarps; u++)
+    for (int u = 0; u < kGatherWarps; u++)
       for (int c = 0; c < 3; c++) ek[c] += part[u][g * 3 + c];
     const double ap = A.S.apol[w % A.np];
     const double ca = A.state[kIterAlpha], cb = A.state[kIterBeta];
@@ -377,7 +384,7 @@ __device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk
 }
 
 template <bool PCG, bool PM, int GS>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kGatherThreads)
     k_iter_b(IterArgs A) {
   // GS polarisable sites per block; the warps split the k-vectors, so every
   // k-vector's weights are loaded once per block and reused for all its sites
@@ -399,12 +406,12 @@ __global__ void __launch_bounds__(kThreads)
     fn = skp[2 * (size_t)threadIdx.x];
   }
 #pragma unroll 2
-  for (int k = threadIdx.x; k < A.nk; k += kThreads) {
+  for (int k = threadIdx.x; k < A.nk; k += kGatherThreads) {
     const KGather K = Kn;
     const double2 f = fn;
-    if (k + kThreads < A.nk) {
-      Kn = A.kg[k + kThreads];
-      fn = skp[2 * (size_t)(k + kThreads)];
+    if (k + kGatherThreads < A.nk) {
+      Kn = A.kg[k + kGatherThreads];
+      fn = skp[2 * (size_t)(k + kGatherThreads)];
     }
     const int lm = K.lmni >> 8, ni = K.lmni & 255;
     // kspace_efield_idm gather (nb_induction_model.f90:2560-2600): g = -4 a_k (c S_re + s S_im)
@@ -421,7 +428,7 @@ __global__ void __launch_bounds__(kThreads)
     }
   }
   pdl_launch_dependents();  // the gather, the bulk of the kernel, is done
-  __shared__ double part[kWarps][GS * 3];
+  __shared__ double part[kGatherWarps][GS * 3];
 #pragma unroll
   for (int g = 0; g < GS; g++)
 #pragma unroll
@@ -439,7 +446,7 @@ __global__ void __launch_bounds__(kThreads)
     // Jacobi update (nb_induction_model.f90:1317-1359), as k_dip_update
     const int g = threadIdx.x, w = w0 + g;
     double ek[3] = {0.0, 0.0, 0.0};
-    for (int u = 0; u < kWarps; u++)
+    for (int u = 0; u < kGatherWarps; u++)
       for (int c = 0; c < 3; c++) ek[c] += part[u][g * 3 + c];
     const double polr = A.S.apol[w % A.np];
     double Et[3], E0[3];
@@ -582,10 +589,10 @@ cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np,
 // Launches a step kernel, with programmatic stream serialization when A.pdl is set.
 template <typename Kernel>
 cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream_t st,
-                        size_t smem = 0) {
+                        size_t smem = 0, int threads = kThreads) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(blocks);
-  cfg.blockDim = dim3(kThreads);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
@@ -613,11 +620,12 @@ cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st) {
 template <int GS>
 cudaError_t launch_iter_b_gs(const IterArgs &A, cudaStream_t st) {
   const int nb = (A.nw + GS - 1) / GS;
+  constexpr int T = kGatherThreads;
   if (A.PM)
-    return A.cu ? launch_step(k_iter_b<true, true, GS>, nb, A, st)
-                : launch_step(k_iter_b<false, true, GS>, nb, A, st);
-  return A.cu ? launch_step(k_iter_b<true, false, GS>, nb, A, st)
-              : launch_step(k_iter_b<false, false, GS>, nb, A, st);
+    return A.cu ? launch_step(k_iter_b<true, true, GS>, nb, A, st, 0, T)
+                : launch_step(k_iter_b<false, true, GS>, nb, A, st, 0, T);
+  return A.cu ? launch_step(k_iter_b<true, false, GS>, nb, A, st, 0, T)
+              : launch_step(k_iter_b<false, false, GS>, nb, A, st, 0, T);
 }
 
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {

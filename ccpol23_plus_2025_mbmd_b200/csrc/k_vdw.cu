@@ -6,16 +6,19 @@
 //     + r4pie0 (f1(d1 r) - 1) q_a q_b / r
 //     - f6(d6 r) c6 / r^6 - f8(d8 r) c8 / r^8 - f10(d10 r) c10 / r^10,
 // f_n the Tang-Toennies damping, gamma = 20/bohr2a, r0 = 1.4 bohr2a.  One block per molecule
-// i handles its neighbours j > i: warp w takes the sites js = w, w + 8, ... of j, lane = site
-// is of i, so j's site forces are warp reductions (3 atomics per site) and i's accumulate in
-// registers.  Each exponential is evaluated once and serves the damping and its derivative.
+// i handles half of its neighbour pairs: the pair (i, j) goes to i when i < j and i + j is odd
+// or i > j and i + j is even, so that every block has about half its neighbours (with j > i
+// alone the low-numbered molecules carried twice the average and the launch ran in two
+// waves).  Warp w takes the sites js = w, w + 4, ... of j, lane = site is of i, so j's site
+// forces are warp reductions (3 atomics per site) and i's accumulate in registers.  Each
+// exponential is evaluated once and serves the damping and its derivative.
 #include "ccp_device.cuh"
 
 using namespace ccpd;
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 128;  // four blocks per SM: the molecules' blocks run in one wave
 constexpr int kWarps = kThreads / 32;
 
 // Tang-Toennies f_N(delta r) and its derivative (utility.f90:89-125) from one exponential.
@@ -58,7 +61,7 @@ __global__ void __launch_bounds__(kThreads)
   const size_t nfs = (size_t)nm * ns;
   for (int n = 0; n < cnt; n++) {
     const int j = nbr[(size_t)i * cap + n];
-    if (j <= i) continue;
+    if (j == i || (j > i) != (((i + j) & 1) != 0)) continue;  // the pair is j's
     const double4 c = nbrv[(size_t)i * cap + n];
     if (!(c.w < rcutsd)) continue;
     for (int jv = wid; jv < nv; jv += kWarps) {
