@@ -316,10 +316,10 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_single(which, host_loop=False):
+def run_single(which, host_loop=False, config=CONFIG):
     import torch
     from ccpol23_plus_2025_mbmd_b200 import Context
-    model, box, cfg = build_inputs(0)
+    model, box, cfg = build_inputs(0, config)
     dev = torch.device("cuda", 0)
     T = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)
     args = [T(a) for a in (box.x, box.y, box.z, box.xs, box.ys, box.zs)]
@@ -441,7 +441,7 @@ def run_batch(nframes, steps, warmup):
         for fuse in (1, 0):
             with Batch(model, nm, L, slots=slots) as b:
                 b.set_option("fuse_fs3", fuse)
-                out[f"batch_slots{slots}" + ("" if fuse else "_unfused")] = timed(
+                out[f"batch_slots{slots}_" + ("fs3_fused" if fuse else "fs3_per_frame")] = timed(
                     lambda: b.terms_device(terms, L, x, y, z, xs, ys, zs, *f))
     line = {"metric": f"batch of {nframes} x {nm}-water FS3 frames, three-body + induction",
             "unit": "ms per batch", "steps": steps, "warmup": warmup,
@@ -574,7 +574,7 @@ def main():
         run_reference(args)
         return
     if args.single:
-        run_single(args.single, args.host_loop)
+        run_single(args.single, args.host_loop, args.config)
         return
     if args.floor:
         run_floor(args.config, args.steps, args.warmup)

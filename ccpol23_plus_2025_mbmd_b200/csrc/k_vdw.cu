@@ -5,11 +5,11 @@
 //   u = e^{-beta r} (c0 + c1 r + c2 r^2 + c3 r^3) / (1 + e^{-gamma (r - r0)})
 //     + r4pie0 (f1(d1 r) - 1) q_a q_b / r
 //     - f6(d6 r) c6 / r^6 - f8(d8 r) c8 / r^8 - f10(d10 r) c10 / r^10,
-// f_n the Tang-Toennies damping, gamma = 20/bohr2a, r0 = 1.4 bohr2a.  One block per molecule
-// i handles half of its neighbour pairs: the pair (i, j) goes to i when i < j and i + j is odd
-// or i > j and i + j is even, so that every block has about half its neighbours (with j > i
-// alone the low-numbered molecules carried twice the average and the launch ran in two
-// waves).  Warp w takes the sites js = w, w + 4, ... of j, lane = site is of i, so j's site
+// f_n the Tang-Toennies damping, gamma = 20/bohr2a, r0 = 1.4 bohr2a.  Molecule i handles half
+// of its neighbour pairs: the pair (i, j) goes to i when i < j and i + j is odd or i > j and
+// i + j is even, so that every molecule has about half its neighbours (with j > i alone the
+// low-numbered molecules carried twice the average and the launch ran in two waves); kSplit
+// blocks share a molecule's pairs.  Warp w takes the sites js = w, w + 4, ... of j, lane = site is of i, so j's site
 // forces are warp reductions (3 atomics per site) and i's accumulate in registers.  Each
 // exponential is evaluated once and serves the damping and its derivative.
 #include "ccp_device.cuh"
@@ -18,7 +18,14 @@ using namespace ccpd;
 
 namespace {
 
-constexpr int kThreads = 128;  // four blocks per SM: the molecules' blocks run in one wave
+constexpr int kThreads = 128;
+// blocks per molecule: each takes every kSplit-th pair of the molecule's share, so that more
+// warps are in flight (a molecule's pairs are independent; its site forces are added
+// atomically)
+#ifndef CCP_VDW_SPLIT
+#define CCP_VDW_SPLIT 4
+#endif
+constexpr int kSplit = CCP_VDW_SPLIT;
 constexpr int kWarps = kThreads / 32;
 
 // Tang-Toennies f_N(delta r) and its derivative (utility.f90:89-125) from one exponential.
@@ -47,7 +54,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ double P[kVdwMaxRows * kVdwPar];
   __shared__ double fi[kWarps][32][3];
   __shared__ double red[2][kWarps];
-  const int i = blockIdx.x;
+  const int i = blockIdx.x / kSplit, part = blockIdx.x % kSplit;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int u = threadIdx.x; u < nrows * kVdwPar; u += kThreads) P[u] = par[u];
   __syncthreads();
@@ -59,7 +66,7 @@ __global__ void __launch_bounds__(kThreads)
   double fx = 0.0, fy = 0.0, fz = 0.0, e = 0.0, v = 0.0;
   const int cnt = ncnt[i];
   const size_t nfs = (size_t)nm * ns;
-  for (int n = 0; n < cnt; n++) {
+  for (int n = part; n < cnt; n += kSplit) {
     const int j = nbr[(size_t)i * cap + n];
     if (j == i || (j > i) != (((i + j) & 1) != 0)) continue;  // the pair is j's
     const double4 c = nbrv[(size_t)i * cap + n];
@@ -178,7 +185,7 @@ cudaError_t launch_vdw(const double *xs, const double *ys, const double *zs, int
                        const double *par, int nrows, const int *vsite, int nv, double *f,
                        double *scal, cudaStream_t st) {
   if (nv < 1 || nv > 32 || nrows < 1 || nrows > kVdwMaxRows) return cudaErrorInvalidValue;
-  k_vdw<<<nm, kThreads, 0, st>>>(xs, ys, zs, ld, nbr, nbrv, ncnt, cap, ns, rcutsd, row, qq, par,
+  k_vdw<<<nm * kSplit, kThreads, 0, st>>>(xs, ys, zs, ld, nbr, nbrv, ncnt, cap, ns, rcutsd, row, qq, par,
                                  nrows, vsite, nv, f, scal, nm);
   return cudaGetLastError();
 }

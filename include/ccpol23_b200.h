@@ -273,6 +273,12 @@ int ccp_batch_destroy(ccp_batch *b);
 int ccp_batch_slots(const ccp_batch *b, int *slots);
 /* the context of one slot (options, FS3 parameters, diagnostics of its last frame) */
 int ccp_batch_context(ccp_batch *b, int slot, ccp_context **ctx);
+/* Sets a context option (ccp_context_set_option) on every slot, or the batch's own option
+     "fuse_fs3" 0 (default): each frame's FS3 runs in its own evaluation; 1: when the frames
+                share one box length, FS3 runs once for all frames (one neighbour search,
+                triple list and FS3 launch on the batch's own stream) while the slots
+                evaluate the other terms.  The results are the same; fused was 7 % slower at
+                32 frames of 256 waters. */
 int ccp_batch_set_option(ccp_batch *b, const char *name, int value);
 int ccp_batch_set_fs3_params(ccp_batch *b, const double *cs_sr, const double *cs_lr, int ncoef,
                              const double *bgr_sr, const double *bgr_lr);
