@@ -1450,8 +1450,8 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     }
     ctx->opt_sum_sites = value;
   } else if (n == "dipole_gather_sites") {
-    if (value != 4 && value != 8) {
-      set_error("ccp_context_set_option: dipole_gather_sites must be 4 or 8");
+    if (value != 2 && value != 3 && value != 4 && value != 6 && value != 8) {
+      set_error("ccp_context_set_option: dipole_gather_sites must be 2, 3, 4, 6 or 8");
       return CCP_ERR_BAD_INPUT;
     }
     ctx->opt_gather_sites = value;

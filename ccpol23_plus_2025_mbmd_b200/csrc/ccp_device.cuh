@@ -187,7 +187,7 @@ struct IterArgs {
   // kernel's blocks launch early and waits for its predecessor's results itself
   int pdl;
   // block shapes: polarisable sites per structure-factor block (1..128) and per gather and
-  // update block (4 or 8)
+  // update block (2, 3, 4, 6 or 8)
   int sum_sites, gather_sites;
 };
 

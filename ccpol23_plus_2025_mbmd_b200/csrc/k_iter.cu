@@ -47,7 +47,7 @@ constexpr int kWarps = kThreads / 32;
 constexpr int kGatherThreads = CCP_GATHER_THREADS;
 constexpr int kGatherWarps = kGatherThreads / 32;
 constexpr int kSumSitesMax = 128;  // polarisable sites per structure-factor block (A.sum_sites)
-// polarisable sites per gather/update block: a template argument, 4 or 8 (A.gather_sites)
+// polarisable sites per gather/update block: a template argument, 2, 3, 4, 6 or 8 (A.gather_sites)
 
 // Phase factors of polarisable site w from the per-axis tables tab[axis][l][site] (ewald.f90:
 // 960-1010): XY[w][l][m] = exp(i l x) exp(+-i |m| y) in the reference's product order, and
@@ -629,8 +629,14 @@ cudaError_t launch_iter_b_gs(const IterArgs &A, cudaStream_t st) {
 }
 
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
-  if (A.gather_sites != 4 && A.gather_sites != 8) return cudaErrorInvalidValue;
-  return A.gather_sites == 8 ? launch_iter_b_gs<8>(A, st) : launch_iter_b_gs<4>(A, st);
+  switch (A.gather_sites) {
+    case 2: return launch_iter_b_gs<2>(A, st);
+    case 3: return launch_iter_b_gs<3>(A, st);
+    case 4: return launch_iter_b_gs<4>(A, st);
+    case 6: return launch_iter_b_gs<6>(A, st);
+    case 8: return launch_iter_b_gs<8>(A, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_phase_matrix(const KGather *kg, int nk, int nw, int nlm, int nz,

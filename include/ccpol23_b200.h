@@ -399,6 +399,14 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
                      evaluation as exp(i(l x + m y)) and exp(i n z) factors (when they take at
                      most 1 GiB), so a (site, k) phase is one complex product; 0: never (the
                      tiled on-the-fly reciprocal kernels run every iteration);
+     "phase_matrix_full" 1 (default): with the factor tables, the full (site, k-vector)
+                     phase matrix is formed once per evaluation when it fits in half of the L2
+                     (38 MB at 512 waters), and the dipole steps read one phase per pair;
+                     0: never.  Query "phase_matrix_full_active" tells whether it was used;
+     "dipole_sum_sites" 1..128 (default 32): polarisable sites per structure-factor block of
+                     a dipole step (a tuning option; results unchanged);
+     "dipole_gather_sites" 2, 3, 4 (default), 6 or 8: polarisable sites per reciprocal-field
+                     block of a dipole step (a tuning option; results unchanged);
      "dipole_solver" 0 (CCP_FP64 default): the reference's Jacobi iteration and criterion
                      (sum |dmu|^2 < 1e-20 e^2 A^2); 1: preconditioned conjugate gradients
                      (preconditioner diag(alpha), so the convergence quantity is the Jacobi
