@@ -95,11 +95,15 @@ def test_fs3_table_reuse_matches_single_triple_blocks(box, precision, fp32_passe
 
 
 @pytest.mark.parametrize("opt,values", [("pdl", (1, 0)), ("fs3_high_priority", (1, 0)),
-                                        ("graph_loop", (1, 0))])
+                                        ("graph_loop", (1, 0)), ("phase_matrix_full", (1, 0)),
+                                        ("dipole_gather_sites", (4, 3)),
+                                        ("dipole_gather_sites", (4, 8)),
+                                        ("dipole_sum_sites", (32, 100))])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_launch_options_give_the_same_results(box, opt, values, precision):
-    """Programmatic dependent launch of the dipole steps, FS3's stream priority and the graph
-    against the host-driven loop change how the work is launched, not what it computes."""
+    """Programmatic dependent launch of the dipole steps, FS3's stream priority, the graph
+    against the host-driven loop, the full phase matrix against the factor tables and the
+    dipole step's block shapes change how the work is done, not what it computes."""
     m, b = box
     nm, ld = b.xs.shape
     out = []
@@ -112,6 +116,8 @@ def test_launch_options_give_the_same_results(box, opt, values, precision):
             assert c.get_option(opt) == v
             e = c.terms_device(_lib.TERM_HOT, *args, b.box, *f, None, None, None, None, None,
                                None, *mu)
+            if opt == "phase_matrix_full":  # this box's matrix fits in L2: the option decides
+                assert c.get_option("phase_matrix_full_active") == v
         out.append((e, np.stack([t.cpu().numpy() for t in f]),
                     np.stack([t.cpu().numpy() for t in mu])))
     (e1, f1, m1), (e0, f0, m0) = out
