@@ -7,9 +7,15 @@
 - One 256-water FS3 frame (L = 19.71 A, seed 4004; a frame of the 32-frame batch): the
   autograd position gradient against the oracle's forces at 1e-10, central finite differences
   of positions (h = 1e-5 A) and of FS3 parameters (relative step 1e-6).
-- 2048 waters FS2+FS3 (L = 39.40 A, seed 5005): the mixed form against the FP64 form, site
-  forces, per-molecule forces and torques within 1e-5 (the oracle takes minutes there).
+- 2048 waters FS2+FS3 (L = 39.40 A, seed 5005): the FP64 form against the oracle's hot path
+  stored in tests/golden/c5_2048 (the oracle takes minutes there; the fixture's script
+  regenerates it) at 1e-10 -- energies, virial, iteration count, the norms of the site-force,
+  COM-force and dipole arrays and those of every 32nd molecule; the mixed form against the
+  FP64 form, site forces, per-molecule forces and torques within 1e-5.
 """
+import sys
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -213,3 +219,32 @@ def test_2048_mixed_form_within_force_bar(product):
     for name, a, ref, bound in zip(names, parts(out["mixed_fs3fp32"]), parts(out["fp64"]),
                                    (MIXED_FTOL, 2e-5, MIXED_FTOL)):
         assert rel(a, ref) <= bound, (name, rel(a, ref))
+
+
+GOLDEN_C5 = Path(__file__).parent / "golden" / "c5_2048"
+
+
+def test_2048_fp64_hot_path_matches_oracle_fixture(product):
+    sys.path.insert(0, str(GOLDEN_C5))
+    from make_fixture import fingerprint
+    g = np.load(GOLDEN_C5 / "oracle_hot_path.npz")
+    m, b, cfg = _box("c5_2048")
+    fp = fingerprint(b)
+    assert np.allclose(fp, g["fingerprint"], rtol=1e-12, atol=0.0), "inputs differ from the fixture's"
+    with Context(m, b.nm, b.box, precision="fp64") as c:
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    e = r.energies
+    for k, v in zip(g["energy_keys"], g["energies"]):
+        assert abs(e[str(k)] - v) <= TOL * abs(v), (str(k), e[str(k)], v)
+    assert e["ind_iters"] == int(g["ind_iters"])
+    F = np.stack([r.fxs, r.fys, r.fzs])
+    C2 = np.stack([r.fxfs2, r.fyfs2, r.fzfs2])
+    C3 = np.stack([r.fxfs3, r.fyfs3, r.fzfs3])
+    D = np.stack([r.idmx, r.idmy, r.idmz])
+    for a, n in zip((F, C2, C3, D), g["norms"]):
+        assert abs(np.linalg.norm(a) - n) <= TOL * n, (np.linalg.norm(a), n)
+    sel = g["sel"]
+    assert rel(F[:, sel], g["site_forces"]) <= TOL
+    assert rel(C2[:, sel], g["com_fs2"]) <= TOL
+    assert rel(C3[:, sel], g["com_fs3"]) <= TOL
+    assert rel(D[:, sel], g["dipoles"]) <= TOL
