@@ -1163,8 +1163,9 @@ extern "C" {
 
 int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int precision,
                        ccp_context **out) {
-  if (!m || !out || nm < 3 || !(box0 > 0.0) || (precision != CCP_FP64 && precision != CCP_MIXED)) {
-    set_error("ccp_context_create: bad argument");
+  if (!m || !out || nm < 1 || !(box0 > 0.0) || (precision != CCP_FP64 && precision != CCP_MIXED)) {
+    set_error("ccp_context_create: bad argument (null model or output, nm < 1, box0 <= 0 or an "
+              "unknown precision)");
     return CCP_ERR_BAD_INPUT;
   }
   *out = nullptr;
@@ -1889,7 +1890,8 @@ int md_alloc(ccp_context *c) {
   CK(dalloc(&c->d_md_q, 4 * nm));
   CK(dalloc(&c->d_md_j, 3 * nm));
   CK(dalloc(&c->d_md_red, (size_t)9));
-  CK(cudaMallocHost((void **)&c->h_md, sizeof(double) * 13 * nm));
+  // 13 doubles per molecule for the state, and at least 32 for the per-step scalar slots
+  CK(cudaMallocHost((void **)&c->h_md, sizeof(double) * std::max<size_t>(13 * nm, 40)));
   return CCP_OK;
 }
 
@@ -2184,7 +2186,7 @@ int md_steps(ccp_context *ctx, int kind, int nsteps, double dt, ccp_md_stats *st
       pend = -1;
     }
     if (kind == CCP_MD_NVE && ctx->md_eq_left == 0) {
-      double *slot = ctx->h_md + 16 + 8 * (k & 1);  // h_md holds >= 39 doubles (nm >= 3)
+      double *slot = ctx->h_md + 16 + 8 * (k & 1);  // h_md holds >= 40 doubles
       CK(cudaMemcpyAsync(slot, ctx->d_md_red, 6 * sizeof(double), cudaMemcpyDeviceToHost, st));
       pend = k;
       pend_e = ctx->md_e;
@@ -2474,7 +2476,7 @@ int batch_fs3_launch(ccp_context *c, BatchFs3 &B, int nframes, double box, const
   }
   cudaStream_t st = static_cast<cudaStream_t>(B.stream);
   const int nm = c->nm, nt = nframes * nm;
-  int cap = std::max(B.cap, std::min(nm - 1, c->cap));
+  int cap = std::max(B.cap, std::max(1, std::min(nm - 1, c->cap)));
   int tri_cap = std::max(B.tri_cap, c->tri_cap * nframes);
   const double rl = 6.3 + 0.05;  // FS3's cut-off and the list margin of an evaluation
   const Fs3Params F3 = fs3_params(c, box);

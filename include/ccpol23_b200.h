@@ -92,7 +92,7 @@ int ccp_ewald_setup(double ewps, double rcut, double box, double *alp, int *k1, 
                     int *k3);
 
 /* --------------------------------------------------------------------- context */
-/* Allocates device-resident state for boxes of nm molecules on `device` (ordinal),
+/* Allocates device-resident state for boxes of nm >= 1 molecules on `device` (ordinal),
    precision CCP_FP64 or CCP_MIXED.  Ewald alpha/k-max default to
    ccp_ewald_setup(1e-6, rcut, box0). */
 int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int precision,

@@ -166,6 +166,44 @@ def test_hot_path(oracle, boxes, key):
     assert rel(np.stack([r.fxfs3, r.fyfs3, r.fzfs3]), np.stack([st.fxfs3, st.fyfs3, st.fzfs3])) <= TOL
 
 
+@pytest.mark.parametrize("nm", [1, 2, 3])
+def test_tiny_systems_match_oracle(product, oracle, nm):
+    """One, two and three molecules in a 20 A box: empty neighbour and triple lists, one pair
+    and one close triple (centres 3 A apart), through the whole hot path against the oracle;
+    terms that vanish must vanish on both sides."""
+    O = oracle
+    m = Model(data_dir("fs2fs3"))
+    L = 20.0
+    b = water_box(m, nm, L, 11)
+    b.x[:] = [0.0, 3.0, 1.5][:nm]
+    b.y[:] = [0.0, 0.0, 2.6][:nm]
+    b.z[:] = [0.0, 0.2, -0.3][:nm]
+    M = O.make_model(O.read_inputs(data_dir("fs2fs3")), nm, L)
+    eo, st = O.hot_path(M, b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    with _ctx(m, b) as c:
+        r = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    e = r.energies
+    for k in ("scpe", "rcpe", "kcpe", "indpe", "fs2pe", "fs3pe", "vir"):
+        if eo[k] == 0.0:
+            assert e[k] == 0.0, (k, e[k])
+        else:
+            assert abs(e[k] - eo[k]) <= TOL * abs(eo[k]), (k, e[k], eo[k])
+    if nm < 3:
+        assert eo["fs3pe"] == 0.0 and e["n_fs3_triples"] == 0
+    else:
+        assert e["n_fs3_triples"] == 1 and eo["fs3pe"] != 0.0
+    assert e["ind_iters"] == eo["ind_iters"]
+    for a, ao in ((np.stack([r.fxs, r.fys, r.fzs]), np.stack([st.fxs, st.fys, st.fzs])),
+                  (np.stack([r.idmx, r.idmy, r.idmz]), np.stack([st.idmx, st.idmy, st.idmz])),
+                  (np.stack([r.fxfs2, r.fyfs2, r.fzfs2]), np.stack([st.fxfs2, st.fyfs2, st.fzfs2])),
+                  (np.stack([r.fxfs3, r.fyfs3, r.fzfs3]), np.stack([st.fxfs3, st.fyfs3, st.fzfs3]))):
+        assert rel(a, ao) <= TOL
+    # the mixed form (PCG dipoles on as few as three polarisable sites) within its force bar
+    with _ctx(m, b, "mixed") as c:
+        rm = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box)
+    assert rel(np.stack([rm.fxs, rm.fys, rm.fzs]), np.stack([st.fxs, st.fys, st.fzs])) <= MIXED_FTOL
+
+
 def test_hot_path_device_matches_host(product, boxes):
     import torch
     m, b, M = boxes["fs2fs3_128"]
