@@ -886,9 +886,14 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                            cudaMemcpyDeviceToHost, st));
     }
     CK(cudaMemcpyAsync(c->h_scal, c->d_scal, sizeof(double) * S_COUNT, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(c->h_icnt, c->d_icnt, sizeof(int) * C_COUNT, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(c->h_icnt, c->d_icnt, sizeof(int) * C_ALLOC, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     const int *ic = c->h_icnt;
+    if (ic[C_NONFINITE] > 0) {
+      CK(cudaMemset(c->d_icnt + C_NONFINITE, 0, sizeof(int)));
+      set_error("non-finite coordinates (NaN or infinite) in the positions or site offsets");
+      return CCP_ERR_BAD_INPUT;
+    }
     bool grow = false;
     int ncap = c->cap, ntcap = c->tri_cap, npcap = c->pair_cap;
     if (ic[C_OVERFLOW] > 0) {
@@ -1287,7 +1292,7 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
             dalloc(&c->d_s17, n * kNs3) == cudaSuccess && dalloc(&c->d_f, 6 * nsi) == cudaSuccess &&
             dalloc(&c->d_fc2, 3 * n) == cudaSuccess && dalloc(&c->d_fc3, 3 * n) == cudaSuccess &&
             dalloc(&c->d_scal, (size_t)S_COUNT) == cudaSuccess &&
-            dalloc(&c->d_icnt, (size_t)C_COUNT) == cudaSuccess &&
+            dalloc(&c->d_icnt, (size_t)C_ALLOC) == cudaSuccess &&
             dalloc(&c->d_mu, np3) == cudaSuccess && dalloc(&c->d_e0r, np3) == cudaSuccess &&
             dalloc(&c->d_e0k, np3) == cudaSuccess && dalloc(&c->d_e0slf, np3) == cudaSuccess &&
             dalloc(&c->d_e0s, np3) == cudaSuccess && dalloc(&c->d_eir, std::max(np3, 3 * nsi)) == cudaSuccess &&
@@ -1302,8 +1307,9 @@ int ccp_context_create(const ccp_model *m, int nm, double box0, int device, int 
   c->d_z = c->d_y + n;
   if (cudaMemset(c->d_e0s, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
   if (cudaMemset(c->d_mu, 0, np3 * sizeof(double)) != cudaSuccess) return fail("memset");
+  if (cudaMemset(c->d_icnt, 0, C_ALLOC * sizeof(int)) != cudaSuccess) return fail("memset");
   if (cudaMallocHost((void **)&c->h_scal, sizeof(double) * S_COUNT) != cudaSuccess ||
-      cudaMallocHost((void **)&c->h_icnt, sizeof(int) * C_COUNT) != cudaSuccess)
+      cudaMallocHost((void **)&c->h_icnt, sizeof(int) * C_ALLOC) != cudaSuccess)
     return fail("pinned allocation");
   if (ensure_inputs(c, m->ns) != CCP_OK) return fail("inputs");
   const int cap0 = std::min(nm - 1, 192);

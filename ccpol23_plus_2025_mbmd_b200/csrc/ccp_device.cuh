@@ -109,6 +109,9 @@ enum CountSlot {
   C_OVERFLOW,
   C_COUNT
 };
+// One more slot past those k_prep clears: set by k_prep when an input coordinate is not
+// finite, read back with the counters and cleared by the host when it reports the error.
+enum { C_NONFINITE = C_COUNT, C_ALLOC };
 
 // Model constants the kernels need, passed by value.
 struct SiteSets {

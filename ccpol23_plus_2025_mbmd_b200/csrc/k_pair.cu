@@ -25,7 +25,9 @@ __global__ void k_prep(const double *__restrict__ x, const double *__restrict__ 
   int stride = gridDim.x * blockDim.x;
   // one thread per molecule, per (molecule, active site) and per (molecule, FS site): the
   // conversions to bohr are divisions, as the reference forms them
+  bool bad = false;  // a coordinate that is not finite (NaN or infinite)
   for (int i = t; i < nm; i += stride) {
+    bad |= !(isfinite(x[i]) && isfinite(y[i]) && isfinite(z[i]));
     com[i] = make_double4(x[i], y[i], z[i], 0.0);
     comb[i] = make_double4(x[i] / kBohr2a, y[i] / kBohr2a, z[i] / kBohr2a, 0.0);
     fc2[i] = fc2[nm + i] = fc2[2 * nm + i] = 0.0;
@@ -34,13 +36,16 @@ __global__ void k_prep(const double *__restrict__ x, const double *__restrict__ 
   for (int u = t; u < nm * S.na; u += stride) {
     const int i = u / S.na, a = u - i * S.na;
     const size_t o = (size_t)i * ld + S.asite[a];
+    bad |= !(isfinite(xs[o]) && isfinite(ys[o]) && isfinite(zs[o]));
     act[u] = make_double4(xs[o], ys[o], zs[o], S.q[a]);
   }
   for (int u = t; u < nm * ns3; u += stride) {
     const int i = u / ns3, s = u - i * ns3;
     const size_t o = (size_t)i * ld + s;
+    bad |= !(isfinite(xs[o]) && isfinite(ys[o]) && isfinite(zs[o]));
     s17[(size_t)i * kNs3 + s] = make_double4(xs[o] / kBohr2a, ys[o] / kBohr2a, zs[o] / kBohr2a, 0.0);
   }
+  if (bad) atomicAdd(&icnt[C_NONFINITE], 1);
   for (int k = t; k < nf; k += stride) f[k] = 0.0;
   if (t < S_COUNT) scal[t] = 0.0;
   if (t < C_COUNT) icnt[t] = 0;

@@ -26,7 +26,11 @@ extern "C" {
 
 /* ------------------------------------------------------------------ status codes */
 #define CCP_OK 0
-#define CCP_ERR_BAD_INPUT 1      /* null pointer, nm/ld out of range, bad file contents */
+#define CCP_ERR_BAD_INPUT 1      /* null pointer, nm/ld out of range, bad file contents;
+                                    from a context's evaluations also a NaN or infinite
+                                    coordinate or site offset (found on the device as the
+                                    inputs are read, reported at the evaluation's end; the
+                                    outputs of that call are then undefined) */
 #define CCP_ERR_NOT_CONVERGED 2  /* dipole iteration hit maxit (reference: `stop`,
                                     nb_induction_model.f90:1374-1379) */
 #define CCP_ERR_CUDA 3           /* a CUDA runtime call failed; see ccp_last_error() */

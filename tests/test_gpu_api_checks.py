@@ -1,10 +1,11 @@
 """Argument checks and stream ordering of the torch-facing API on the GPU: tensors of the
-wrong dtype, layout, size or device are refused before the library runs; the autograd
-forward runs after work that torch has queued ahead of it on its current stream."""
+wrong dtype, layout, size or device are refused before the library runs; non-finite
+coordinates are refused by the evaluation itself, which stays usable; the autograd forward
+runs after work that torch has queued ahead of it on its current stream."""
 import numpy as np
 import pytest
 
-from ccpol23_plus_2025_mbmd_b200 import Context, Model, _lib, data_dir
+from ccpol23_plus_2025_mbmd_b200 import CcpError, Context, Model, _lib, data_dir
 from ccpol23_plus_2025_mbmd_b200.generator import water_box
 
 from conftest import rel
@@ -40,6 +41,28 @@ def test_terms_device_refuses_wrong_tensors(setup):
                                                           dtype=torch.float64))
         e = c.terms_device(_lib.TERM_FS3, *args, b.box)  # the context stays usable
         assert e["fs3pe"] != 0.0
+
+
+@pytest.mark.parametrize("where,value", [("x", np.nan), ("zs", np.inf), ("ys", -np.inf)])
+def test_non_finite_coordinates_are_refused(setup, where, value):
+    """A NaN or infinite COM coordinate or site offset, through the host-buffer and the
+    device entry points: CCP_ERR_BAD_INPUT naming the cause; the next valid call works."""
+    m, b, args = setup
+    bad = {k: getattr(b, k).copy() for k in ("x", "y", "z", "xs", "ys", "zs")}
+    bad[where].flat[5] = value
+    with Context(m, b.nm, b.box) as c:
+        good = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box).energies
+        with pytest.raises(CcpError, match="non-finite"):
+            c.hot_path(*(bad[k] for k in ("x", "y", "z", "xs", "ys", "zs")), b.box)
+        again = c.hot_path(b.x, b.y, b.z, b.xs, b.ys, b.zs, b.box).energies
+        assert again["fs3pe"] == pytest.approx(good["fs3pe"], rel=1e-12)
+        import torch
+        dev_bad = [torch.as_tensor(np.ascontiguousarray(bad[k]), device="cuda:0")
+                   for k in ("x", "y", "z", "xs", "ys", "zs")]
+        with pytest.raises(CcpError, match="non-finite"):
+            c.terms_device(_lib.TERM_HOT, *dev_bad, b.box)
+        e = c.terms_device(_lib.TERM_HOT, *args, b.box)
+        assert e["indpe"] == pytest.approx(good["indpe"], rel=1e-12)
 
 
 def test_autograd_forward_waits_for_queued_torch_work(setup):
