@@ -345,13 +345,14 @@ def run_single(which, host_loop=False, config=CONFIG):
                               "n_fs2_triples": e["n_fs2_triples"]}), flush=True)
 
 
-def run_floor(config, steps, warmup):
+def run_floor(config, steps, warmup, opts=()):
     """The critical-path floor of the evaluation, per form (one JSON line each): the
     Ewald/induction chain alone (self, real, reciprocal, induction), its dipole loop within
     that, the three-body terms alone, FS3 alone, the whole step with the terms overlapping
     (with the loop's and FS3's own durations there) and with them in order on one stream.
     CUDA events on torch's current stream around each evaluation, L2 flushed before each,
-    means over `steps` evaluations after `warmup`."""
+    means over `steps` evaluations after `warmup`.  `opts` are (name, value) context options
+    set on both forms."""
     import torch
     from ccpol23_plus_2025_mbmd_b200 import _lib
     model, box, cfg = build_inputs(0, config)
@@ -381,7 +382,9 @@ def run_floor(config, steps, warmup):
         with open_context(model, box, 0, form) as ctx:
             ctx.set_stream(torch.cuda.current_stream().cuda_stream)
             ctx.set_timing(True)
-            r = {"box": config, "nm": box.nm, "form": form}
+            for k, v in opts:
+                ctx.set_option(k, v)
+            r = {"box": config, "nm": box.nm, "form": form, "options": dict(opts)}
             r["chain_alone_ms"], ph = timed(ctx, chain)
             r["loop_alone_ms"] = float(ph[4])
             r["three_body_alone_ms"], _ = timed(ctx, three)
@@ -573,6 +576,8 @@ def main():
     ap.add_argument("--floor", action="store_true",
                     help="print the critical-path floor table (chain, dipole loop, three-body "
                          "terms and FS3 alone, overlapped and in order) per form instead")
+    ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
+                    help="with --floor: a context option set on both forms (repeatable)")
     ap.add_argument("--host-loop", action="store_true",
                     help="with --single: drive the dipole iteration from the host, so that "
                          "profilers see its kernels")
@@ -584,7 +589,8 @@ def main():
         run_single(args.single, args.host_loop, args.config)
         return
     if args.floor:
-        run_floor(args.config, args.steps, args.warmup)
+        opts = [(kv.split("=", 1)[0], int(kv.split("=", 1)[1])) for kv in args.opt]
+        run_floor(args.config, args.steps, args.warmup, opts)
         return
     if args.nve:
         run_nve(args.nve, args.nve_equil)
