@@ -102,6 +102,11 @@ struct ccp_context {
   KVec *d_kv = nullptr;
   KGather *d_kg = nullptr;
   int nk = 0, nk_cap = 0;
+  // the rows of the k-vector list by decreasing length (KRow) and 2 pi n / L by n, for the
+  // row form of the dipole step
+  KRow *d_rows = nullptr;
+  double *d_rn = nullptr;
+  int nrow = 0, nrow_cap = 0, nrn_cap = 0, row_span = 0;
   double kv_box = -1, kv_alpha = -1;
   int kv_kmax[3] = {-1, -1, -1};
   double2 *d_tab = nullptr;
@@ -171,6 +176,10 @@ struct ccp_context {
   size_t PM_cap = 0;
   bool use_PM = false;
   int opt_pm = 1;  // the full phase matrix when it fits (1) or never (0)
+  // without the full phase matrix, the row form of the dipole step (1) or the factor-table
+  // kernels (0)
+  int opt_rows = 1;
+  bool use_rows = false;
   int opt_sum_sites = 32, opt_gather_sites = 4;  // block shapes of the dipole step (IterArgs)
   // options (ccp_context_set_option)
   int opt_graph = 1;  // Jacobi loop as a conditional graph (1) or driven from the host (0)
@@ -234,6 +243,8 @@ void free_ctx(ccp_context *c) {
   if (c->h_md) cudaFreeHost(c->h_md);
   if (c->d_P) cudaFree(c->d_P);
   if (c->d_PM) cudaFree(c->d_PM);
+  if (c->d_rows) cudaFree(c->d_rows);
+  if (c->d_rn) cudaFree(c->d_rn);
   if (c->h_istate) cudaFreeHost(c->h_istate);
   if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
   if (c->s_fs3) cudaStreamDestroy(c->s_fs3);
@@ -321,6 +332,24 @@ std::vector<KVec> build_kvecs(int lmax, int mmax, int nmax, double alp, double b
   return out;
 }
 
+// The rows of a k-vector list in the order build_kvecs makes it (n innermost): one per run
+// of one (l, m), sorted by decreasing length (ties in list order), for the row form of the
+// dipole step (k_iter.cu).
+std::vector<KRow> build_krows(const std::vector<KVec> &kv, int mmax) {
+  std::vector<KRow> rows;
+  for (int k = 0; k < (int)kv.size(); k++) {
+    const KVec &K = kv[k];
+    if (k > 0 && K.l == kv[k - 1].l && K.m == kv[k - 1].m) {
+      rows.back().len++;
+      continue;
+    }
+    rows.push_back({K.rl, K.rm, k, 1, K.n, K.l * (2 * mmax + 1) + K.m + mmax});
+  }
+  std::stable_sort(rows.begin(), rows.end(),
+                   [](const KRow &a, const KRow &b) { return a.len > b.len; });
+  return rows;
+}
+
 int ensure_kspace(ccp_context *c, double box) {
   if (box == c->kv_box && c->alpha == c->kv_alpha && c->kmax[0] == c->kv_kmax[0] &&
       c->kmax[1] == c->kv_kmax[1] && c->kmax[2] == c->kv_kmax[2])
@@ -348,6 +377,41 @@ int ensure_kspace(ccp_context *c, double box) {
   if (c->nk)
     CK(cudaMemcpyAsync(c->d_kg, kg.data(), sizeof(KGather) * c->nk, cudaMemcpyHostToDevice,
                        c->stream));
+  {
+    std::vector<KRow> rows = build_krows(kv, c->kmax[1]);
+    c->nrow = (int)rows.size();
+    c->row_span = 0;
+    for (int t = 0; t < c->nrow; t += kRowTile) {
+      int nb = rows[t].nlo, ne = nb + rows[t].len;
+      for (int r = t + 1; r < std::min(c->nrow, t + kRowTile); r++) {
+        nb = std::min(nb, rows[r].nlo);
+        ne = std::max(ne, rows[r].nlo + rows[r].len);
+      }
+      c->row_span = std::max(c->row_span, ne - nb);
+    }
+    if (c->nrow > c->nrow_cap) {
+      if (c->d_rows) cudaFree(c->d_rows);
+      c->d_rows = nullptr;
+      c->nrow_cap = 0;
+      CK(dalloc(&c->d_rows, (size_t)c->nrow));
+      c->nrow_cap = c->nrow;
+    }
+    const int nz = 2 * c->kmax[2] + 1;
+    std::vector<double> rn(nz);
+    for (int n = -c->kmax[2]; n <= c->kmax[2]; n++) rn[n + c->kmax[2]] = 2.0 * kPi * n / box;
+    if (nz > c->nrn_cap) {
+      if (c->d_rn) cudaFree(c->d_rn);
+      c->d_rn = nullptr;
+      c->nrn_cap = 0;
+      CK(dalloc(&c->d_rn, (size_t)nz));
+      c->nrn_cap = nz;
+    }
+    if (c->nrow)
+      CK(cudaMemcpyAsync(c->d_rows, rows.data(), sizeof(KRow) * c->nrow, cudaMemcpyHostToDevice,
+                         c->stream));
+    CK(cudaMemcpyAsync(c->d_rn, rn.data(), sizeof(double) * nz, cudaMemcpyHostToDevice,
+                       c->stream));
+  }
   int k1 = std::max(c->kmax[0], std::max(c->kmax[1], c->kmax[2])) + 1;
   k1 = std::max(k1, 2);
   const size_t tab = (size_t)3 * k1 * c->nm * c->S.na;
@@ -429,6 +493,16 @@ IterArgs make_iter_args(ccp_context *c, cudaGraphConditionalHandle handle, int u
   A.XY = c->d_P;
   A.Z = c->d_P ? c->d_P + (size_t)A.nw * A.nlm : nullptr;
   A.PM = c->use_PM ? c->d_PM : nullptr;
+  if (c->use_rows) {
+    A.XY = nullptr;
+    A.rows = c->d_rows;
+    A.nrow = c->nrow;
+    A.row_span = c->row_span;
+    A.XYr = c->d_P;
+    A.Z = c->d_P + (size_t)c->nrow * A.nw;
+    A.ZT = A.Z + (size_t)A.nz * A.nw;
+    A.rn = c->d_rn;
+  }
   A.sk = c->d_skj;
   A.par = par;
   A.scal = c->d_scal;
@@ -493,7 +567,8 @@ int ensure_ind_graph(ccp_context *c) {
       (long long)c->d_e0tot, (long long)c->d_scal, (long long)c->d_istate, (long long)c->d_P,
       (long long)c->use_P, (long long)c->d_PM, (long long)c->use_PM, c->cap, c->nm, c->nk, c->kmax[0], c->kmax[1], c->kmax[2], c->maxit,
       (long long)pcg_solver(c), (long long)c->opt_solver, (long long)c->d_pcg,
-      (long long)c->opt_pdl, c->opt_sum_sites, c->opt_gather_sites};
+      (long long)c->opt_pdl, c->opt_sum_sites, c->opt_gather_sites, (long long)c->use_rows,
+      (long long)c->d_rows, c->nrow, c->row_span, (long long)c->d_rn};
   double thr = ind_threshold(c);
   long long thr_bits;
   std::memcpy(&thr_bits, &thr, sizeof thr_bits);
@@ -588,13 +663,17 @@ int run_dipole_loop(ccp_context *c, cudaStream_t st) {
 
 // Allocates the phase-factor tables when the dipole iteration can use them.
 int ensure_phase_matrix(ccp_context *c) {
-  const size_t n = (size_t)c->nm * c->S.np *
-                   ((size_t)(c->kmax[0] + 1) * (2 * c->kmax[1] + 1) + 2 * c->kmax[2] + 1);
+  const size_t nw = (size_t)c->nm * c->S.np, nz = 2 * (size_t)c->kmax[2] + 1;
+  // XY[site][l][m] and Z[site][n], or in the row form XYr[row][site], Z and ZT[n][site]
+  const size_t n = nw * std::max((size_t)(c->kmax[0] + 1) * (2 * c->kmax[1] + 1) + nz,
+                                 (size_t)c->nrow + 2 * nz);
   // the gather records pack the phase-table row of n in 8 bits
   c->use_P = c->opt_phase && c->nk > 0 && n * sizeof(double2) <= kPhaseBudget &&
              2 * c->kmax[2] + 1 <= 255;
   const size_t npm = (size_t)c->nm * c->S.np * (size_t)c->nk;
   c->use_PM = c->use_P && c->opt_pm && npm * sizeof(double2) <= full_phase_budget(c);
+  c->use_rows = c->use_P && !c->use_PM && c->opt_rows &&
+                iter_rows_fit(c->opt_sum_sites, 2 * c->kmax[2] + 1, c->row_span);
   if (c->use_P && n > c->P_cap) {
     if (c->d_P) cudaFree(c->d_P);
     c->d_P = nullptr;
@@ -818,7 +897,12 @@ int evaluate_impl(ccp_context *c, const double *px, const double *py, const doub
                               c->kmax[2], c->d_mu, c->d_sk, sk));
       LK(launch_kspace_gather(1, c->d_kv, c->nk, c->d_tab, nm, S, c->kmax[0], c->kmax[1],
                               c->kmax[2], c->d_mu, c->d_sk, c->d_e0k, fk, sk));
-      if (c->use_P) {
+      if (c->use_rows) {
+        const size_t nw = (size_t)nm * S.np, nz = 2 * c->kmax[2] + 1;
+        double2 *XYr = c->d_P, *Z = XYr + (size_t)c->nrow * nw, *ZT = Z + nz * nw;
+        LK(launch_phase_rows(c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2], c->d_rows,
+                             c->nrow, XYr, Z, ZT, sk));
+      } else if (c->use_P) {
         const int nlm = (c->kmax[0] + 1) * (2 * c->kmax[1] + 1), nz = 2 * c->kmax[2] + 1;
         double2 *XY = c->d_P, *Z = c->d_P + (size_t)nm * S.np * nlm;
         LK(launch_phase_factors(c->d_tab, nm, S, c->kmax[0], c->kmax[1], c->kmax[2], XY, Z, sk));
@@ -1450,6 +1534,8 @@ int ccp_context_set_option(ccp_context *ctx, const char *name, int value) {
     ctx->opt_phase = value != 0;
   } else if (n == "phase_matrix_full") {
     ctx->opt_pm = value != 0;
+  } else if (n == "dipole_row_form") {
+    ctx->opt_rows = value != 0;
   } else if (n == "dipole_sum_sites") {
     if (value < 1 || value > 128) {
       set_error("ccp_context_set_option: dipole_sum_sites must be 1..128");
@@ -1528,6 +1614,10 @@ int ccp_context_get_option(const ccp_context *ctx, const char *name, int *value)
     *value = ctx->opt_gather_sites;
   } else if (n == "phase_matrix_full_active") {
     *value = ctx->use_PM ? 1 : 0;
+  } else if (n == "dipole_row_form") {
+    *value = ctx->opt_rows;
+  } else if (n == "dipole_row_form_active") {
+    *value = ctx->use_rows ? 1 : 0;
   } else if (n == "dipole_solver") {
     *value = ctx->opt_solver;
   } else if (n == "cell_list") {

@@ -153,6 +153,16 @@ struct KGather {
   int lmni, pad;
 };
 
+// One row of the k-vector list: the k-vectors of one (l, m), n = nlo .. nlo + len - 1 at list
+// positions kbeg .. kbeg + len - 1 (the list runs over n innermost, ewald.f90:933-1082), with
+// their 2 pi l / L, 2 pi m / L and the row of (l, m) in the XY factor table.  The row kernels
+// of the dipole step take the rows in decreasing length (32 bytes, one L2 sector).
+struct KRow {
+  double rl, rm;
+  int kbeg, len, nlo, lm;
+};
+constexpr int kRowTile = 16;  // rows per structure-factor block of the row form
+
 // Arguments of one step of the dipole solve with the phase matrix (k_iter.cu): a Jacobi step,
 // or with cu.. set a preconditioned-conjugate-gradient step.
 struct IterArgs {
@@ -174,6 +184,14 @@ struct IterArgs {
   // per evaluation (launch_phase_matrix), or null: the step kernels then form each phase
   // from the factor rows
   const double2 *PM;
+  // the row form (PM null, rows set): the k-vector rows by decreasing length, the factor
+  // tables XYr[r][w] = exp(i(l x + m y)) of row r and site w, Z[w][n] as above and its
+  // transpose ZT[n][w], and rn[n + nmax] = 2 pi n / L
+  const KRow *rows;
+  int nrow;
+  int row_span;  // the largest n range of a tile of kRowTile consecutive rows
+  const double2 *XYr, *ZT;
+  const double *rn;
   // sk[k] holds two S(k) buffers, (re, im) of steps of parity 0 and 1: a step accumulates
   // into its own and clears the other, which the previous step's gather has finished with
   double *sk, *scal, *state;  // state: see IterStateSlot
@@ -295,6 +313,12 @@ cudaError_t launch_phase_factors(const double2 *tab, int nm, SiteSets S, int kl,
 cudaError_t launch_tmu(const int *nbr, const int *ncnt, int cap, int nm, int np, const double4 *T4,
                        const double *TB, const double4 *S4, const double *SB, const double *mu,
                        double *eim, cudaStream_t st);
+size_t iter_rows_smem_a(int sum_sites, int row_span);
+size_t iter_rows_smem_b(int nz, int row_span);
+bool iter_rows_fit(int sum_sites, int nz, int row_span);
+cudaError_t launch_phase_rows(const double2 *tab, int nm, SiteSets S, int kl, int km, int kn,
+                              const KRow *rows, int nrow, double2 *XYr, double2 *Z,
+                              double2 *ZT, cudaStream_t st);
 cudaError_t launch_phase_matrix(const KGather *kg, int nk, int nw, int nlm, int nz,
                                 const double2 *XY, const double2 *Z, double2 *PM,
                                 cudaStream_t st);

@@ -22,6 +22,8 @@
 //      of a graph body that unrolls several steps then returns at once) and, inside the
 //      graph, sets the WHILE node's condition.  S(k) alternates between two buffers by step
 //      parity, so no block has to clear it after the gather.
+#include <climits>
+
 #include "ccp_device.cuh"
 
 using namespace ccpd;
@@ -81,6 +83,49 @@ __global__ void k_phase_factors(const double2 *__restrict__ tab, int nm, SiteSet
       const int n = u - nlm - nmax;
       const double2 en = tab[(size_t)(2 * k1 + (n < 0 ? -n : n)) * N + st];
       Z[(size_t)w * nz + (u - nlm)] = make_double2(en.x, n < 0 ? -en.y : en.y);
+    }
+  }
+}
+
+// The factor tables of the row form: XYr[r][w] for the k-vector rows (KRow, lm = l (2 mmax +
+// 1) + m + mmax), formed as k_phase_factors forms XY, and Z both as Z[w][n] and as its
+// transpose ZT[n][w].  Site-fastest order, so the row-major writes and the per-axis table
+// reads coalesce.
+__global__ void k_phase_rows(const double2 *__restrict__ tab, int nm, SiteSets S, int k1,
+                             int mmax, int nmax, const KRow *__restrict__ rows, int nrow,
+                             double2 *XYr, double2 *Z, double2 *ZT) {
+  const int nw = nm * S.np;
+  const int M = 2 * mmax + 1, nz = 2 * nmax + 1;
+  const size_t N = (size_t)nm * S.na;
+  const size_t nxy = (size_t)nrow * nw, total = nxy + (size_t)nz * nw;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
+       t += (size_t)gridDim.x * blockDim.x) {
+    if (t < nxy) {
+      const int r = (int)(t / nw), w = (int)(t - (size_t)r * nw);
+      const int i = w / S.np, p = w % S.np;
+      const size_t st = (size_t)i * S.na + S.a_of_p[p];
+      const int lm = rows[r].lm, l = lm / M, m = lm % M - mmax;
+      const double2 el = tab[(size_t)(0 * k1 + l) * N + st];
+      const double2 em = tab[(size_t)(1 * k1 + (m < 0 ? -m : m)) * N + st];
+      double clm, slm;
+      if (m >= 0) {
+        clm = el.x * em.x - el.y * em.y;
+        slm = el.y * em.x + em.y * el.x;
+      } else {
+        clm = el.x * em.x + el.y * em.y;
+        slm = el.y * em.x - em.y * el.x;
+      }
+      XYr[t] = make_double2(clm, slm);
+    } else {
+      const size_t u = t - nxy;
+      const int ni = (int)(u / nw), w = (int)(u - (size_t)ni * nw);
+      const int i = w / S.np, p = w % S.np;
+      const size_t st = (size_t)i * S.na + S.a_of_p[p];
+      const int n = ni - nmax;
+      const double2 en = tab[(size_t)(2 * k1 + (n < 0 ? -n : n)) * N + st];
+      const double2 z = make_double2(en.x, n < 0 ? -en.y : en.y);
+      ZT[u] = z;
+      Z[(size_t)w * nz + ni] = z;
     }
   }
 }
@@ -237,6 +282,33 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Blocks [0, nA) of a step's first kernel: T.mu, one warp per polarisable site; they also
+// clear the S(k) buffer of the other step parity, whose last reader, the previous step's
+// gather, has finished.
+template <bool PCG>
+__device__ __forceinline__ void iter_a_tmu(const IterArgs &A, const PcgIn &pin, int nA) {
+  double2 *other = reinterpret_cast<double2 *>(A.sk) + (A.par ^ 1);
+  for (int k = blockIdx.x * kThreads + threadIdx.x; k < A.nk; k += nA * kThreads)
+    other[2 * (size_t)k] = make_double2(0.0, 0.0);
+  const int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (w >= A.nw) return;
+  double ex, ey, ez;
+  if constexpr (PCG)
+    tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, pin, ex, ey, ez);
+  else
+    tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, MuIn{A.mu}, ex, ey,
+             ez);
+  // the next kernel may launch once every block is this far: late enough that its blocks
+  // do not hold SM slots (which concurrent kernels could use) for long while they wait
+  pdl_launch_dependents();
+  if (lane == 0) {
+    A.eim[(size_t)w * 3 + 0] = ex;
+    A.eim[(size_t)w * 3 + 1] = ey;
+    A.eim[(size_t)w * 3 + 2] = ez;
+  }
+}
+
 template <bool PCG, bool PM>
 __global__ void __launch_bounds__(kThreads)
     k_iter_a(IterArgs A) {
@@ -247,27 +319,7 @@ __global__ void __launch_bounds__(kThreads)
   PcgIn pin;
   if constexpr (PCG) pin = pcg_in(A);
   if ((int)blockIdx.x < nA) {
-    // the other parity's buffer: its last reader, the previous step's gather, has finished
-    double2 *other = reinterpret_cast<double2 *>(A.sk) + (A.par ^ 1);
-    for (int k = blockIdx.x * kThreads + threadIdx.x; k < A.nk; k += nA * kThreads)
-      other[2 * (size_t)k] = make_double2(0.0, 0.0);
-    const int w = blockIdx.x * kWarps + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (w >= A.nw) return;
-    double ex, ey, ez;
-    if constexpr (PCG)
-      tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, pin, ex, ey, ez);
-    else
-      tmu_warp(w, lane, A.nbr, A.ncnt, A.cap, A.np, A.T4, A.TB, A.S4, A.SB, MuIn{A.mu}, ex, ey,
-               ez);
-    // the next kernel may launch once every block is this far: late enough that its blocks
-    // do not hold SM slots (which concurrent kernels could use) for long while they wait
-    pdl_launch_dependents();
-    if (lane == 0) {
-      A.eim[(size_t)w * 3 + 0] = ex;
-      A.eim[(size_t)w * 3 + 1] = ey;
-      A.eim[(size_t)w * 3 + 2] = ez;
-    }
+    iter_a_tmu<PCG>(A, pin, nA);
     return;
   }
   // structure factors: block b covers k-vectors [kt*256, kt*256+256) and sites of chunk sc
@@ -309,15 +361,15 @@ __global__ void __launch_bounds__(kThreads)
 // of (u, M u), (w, u), |u|^2 and the energy -1/2 x.E0 (the reference's energy expression at
 // the iterate), and in the last block to finish the step's scalars and the convergence test
 // on sum |u|^2, the Jacobi update's norm at the iterate.
-template <int GS>
-__device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk,
-                                           const double (*part)[GS * 3]) {
+// ek(g, c) gives component c of the reciprocal field at the block's site g; the updating
+// threads (one per site) are all in warp 0.
+template <typename EK>
+__device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk, const EK &ekf) {
   double gam = 0.0, del = 0.0, ch = 0.0, en = 0.0;
   if ((int)threadIdx.x < ns_blk) {
     const int g = threadIdx.x, w = w0 + g;
-    double ek[3] = {0.0, 0.0, 0.0};
-    for (int u = 0; u < kGatherWarps; u++)
-      for (int c = 0; c < 3; c++) ek[c] += part[u][g * 3 + c];
+    double ek[3];
+    for (int c = 0; c < 3; c++) ek[c] = ekf(g, c);
     const double ap = A.S.apol[w % A.np];
     const double ca = A.state[kIterAlpha], cb = A.state[kIterBeta];
     for (int c = 0; c < 3; c++) {
@@ -383,6 +435,60 @@ __device__ __forceinline__ void pcg_update(const IterArgs &A, int w0, int ns_blk
   }
 }
 
+// The Jacobi update of the block's sites (nb_induction_model.f90:1317-1359) from their
+// reciprocal field ek(g, c), the change and energy sums, and in the last block to finish the
+// step's close (iteration count, convergence test, the graph's condition).  The updating
+// threads (one per site) are all in warp 0.
+template <typename EK>
+__device__ __forceinline__ void jacobi_update(const IterArgs &A, int w0, int ns_blk,
+                                              const EK &ekf) {
+  double ch = 0.0, en = 0.0;
+  if ((int)threadIdx.x < ns_blk) {
+    const int g = threadIdx.x, w = w0 + g;
+    double ek[3];
+    for (int c = 0; c < 3; c++) ek[c] = ekf(g, c);
+    const double polr = A.S.apol[w % A.np];
+    double Et[3], E0[3];
+    for (int c = 0; c < 3; c++) {
+      const size_t o = (size_t)w * 3 + c;
+      E0[c] = A.e0[o];
+      Et[c] = (A.eim[o] + ek[c]) + E0[c];
+      const double m = polr * Et[c];
+      const double d = A.mu[o] - m;
+      ch += d * d;
+      A.mu[o] = m;
+    }
+    en = -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
+  }
+  ch = warp_sum(ch);  // the updating threads are all in warp 0
+  en = warp_sum(en);
+  __shared__ bool last;
+  if (threadIdx.x == 0) {
+    atomicAdd(&A.scal[S_IND_CHANGE], ch);
+    atomicAdd(&A.scal[S_IND_ENERGY], en);
+    __threadfence();
+    last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  // every other block has added its sums
+  __threadfence();
+  if (threadIdx.x == 0) {
+    const double chg = atomicAdd(&A.scal[S_IND_CHANGE], 0.0);
+    const double ene = atomicAdd(&A.scal[S_IND_ENERGY], 0.0);
+    const int it = (int)A.state[kIterIters] + 1;
+    A.state[kIterIters] = (double)it;
+    A.state[kIterChange] = chg;
+    A.state[kIterEnergy] = ene;
+    A.scal[S_IND_CHANGE] = 0.0;
+    A.scal[S_IND_ENERGY] = 0.0;
+    *A.ticket = 0u;
+    const bool more = chg > A.thr && it < A.maxit;
+    if (!more) A.state[kIterFinished] = 1.0;
+    if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
+  }
+}
+
 template <bool PCG, bool PM, int GS>
 __global__ void __launch_bounds__(kGatherThreads)
     k_iter_b(IterArgs A) {
@@ -437,57 +543,270 @@ __global__ void __launch_bounds__(kGatherThreads)
       if (lane == 0) part[wid][g * 3 + c] = v;
     }
   __syncthreads();
-  if constexpr (PCG) {
-    pcg_update<GS>(A, w0, ns_blk, part);
+  const auto ek = [&](int g, int c) {
+    double v = 0.0;
+    for (int u = 0; u < kGatherWarps; u++) v += part[u][g * 3 + c];
+    return v;
+  };
+  if constexpr (PCG)
+    pcg_update(A, w0, ns_blk, ek);
+  else
+    jacobi_update(A, w0, ns_blk, ek);
+}
+
+// ------------------------------------------------------------------ the row form
+// For boxes whose phase matrix does not fit in L2 the step kernels above form each (site,
+// k-vector) phase from two factor-table loads, and both passes then run at the L1 load rate,
+// far below the FP64 rate.  The row form regroups the same sums by the rows of the k-vector
+// list (one (l, m), a run of n), so that every loaded value serves many products:
+//   structure factors  S(k) = sum_w Z(w, n) (B(w, r) + k_n C(w, r)),
+//                      B = XY(w, r) (k_l mu_x + k_m mu_y),  C = XY(w, r) mu_z;
+//   gather             E(w) = sum_r Re[XY(w, r) (k_l Q, k_m Q, Q_z)],
+//                      Q = sum_n Z(w, n) conj F(k),  Q_z = sum_n k_n Z(w, n) conj F(k),
+// F(k) the weighted S(k) of the step.  These are k_iter_a's and k_iter_b's sums with the
+// products reassociated (equal to rounding).
+constexpr int kRowLanes = 8;  // n lanes per row of a structure-factor block: n = nb + lane + 8 j
+// gather blocks: sites per block (8, 16 or 32), rows per thread, warps per block
+#ifndef CCP_ROW_SITES
+#define CCP_ROW_SITES 16
+#endif
+#ifndef CCP_ROW_R
+#define CCP_ROW_R 4
+#endif
+#ifndef CCP_ROW_WARPS
+#define CCP_ROW_WARPS 4
+#endif
+constexpr int kRowSites = CCP_ROW_SITES, kRowR = CCP_ROW_R, kRowWarps = CCP_ROW_WARPS;
+static_assert(kRowSites == 8 || kRowSites == 16 || kRowSites == 32, "sites per gather block");
+
+// Structure factors of the row form: block b (after the T.mu blocks) covers tile b % ntile
+// (kRowTile consecutive rows of the length-sorted list, n in [nb, ne) of their union) and the
+// sites of chunk b / ntile.  A thread takes one row and the n = nb + lane + 8 j (j < J) of it;
+// the partial sums are merged with FP64 atomics as in k_iter_a.  The chunk's XY factors of
+// the tile's rows and its Z factors of the tile's n range are staged in shared memory before
+// the wait for the previous step (the tables are fixed during the solve), so the site loop
+// reads only shared memory.
+template <bool PCG, int J>
+__global__ void __launch_bounds__(kThreads) k_iter_a_rows(IterArgs A) {
+  const int nA = (A.nw + kWarps - 1) / kWarps;
+  if ((int)blockIdx.x < nA) {
+    pdl_wait();  // the previous step's dipoles (and its gather's last use of the S(k) buffer)
+    PcgIn pin;
+    if constexpr (PCG) pin = pcg_in(A);
+    iter_a_tmu<PCG>(A, pin, nA);
     return;
   }
-  double ch = 0.0, en = 0.0;
-  if (threadIdx.x < ns_blk) {
-    // Jacobi update (nb_induction_model.f90:1317-1359), as k_dip_update
-    const int g = threadIdx.x, w = w0 + g;
-    double ek[3] = {0.0, 0.0, 0.0};
-    for (int u = 0; u < kGatherWarps; u++)
-      for (int c = 0; c < 3; c++) ek[c] += part[u][g * 3 + c];
-    const double polr = A.S.apol[w % A.np];
-    double Et[3], E0[3];
-    for (int c = 0; c < 3; c++) {
-      const size_t o = (size_t)w * 3 + c;
-      E0[c] = A.e0[o];
-      Et[c] = (A.eim[o] + ek[c]) + E0[c];
-      const double m = polr * Et[c];
-      const double d = A.mu[o] - m;
-      ch += d * d;
-      A.mu[o] = m;
-    }
-    en = -0.5 * polr * (Et[0] * E0[0] + Et[1] * E0[1] + Et[2] * E0[2]);
-  }
-  ch = warp_sum(ch);  // the updating threads are all in warp 0
-  en = warp_sum(en);
-  __shared__ bool last;
+  // sum_sites x 3 dipole components, the XY factors [site][row] of the tile's rows and the
+  // Z factors [site][n - nb] of its n range (row stride row_span)
+  extern __shared__ double smu[];
+  constexpr int kXs = kRowTile + 1;  // site stride of the staged XY: no bank conflicts
+  double2 *bxy = reinterpret_cast<double2 *>(smu + ((3 * A.sum_sites + 1) & ~1));
+  double2 *zs = bxy + (size_t)A.sum_sites * kXs;
+  __shared__ int s_nb, s_ne;
+  const int b = blockIdx.x - nA;
+  const int ntile = (A.nrow + kRowTile - 1) / kRowTile;
+  const int rt = b % ntile, sc = b / ntile;
+  const int s0 = sc * A.sum_sites, cnt = min(A.sum_sites, A.nw - s0);
+  const int r0 = rt * kRowTile, nr = min(kRowTile, A.nrow - r0);
   if (threadIdx.x == 0) {
-    atomicAdd(&A.scal[S_IND_CHANGE], ch);
-    atomicAdd(&A.scal[S_IND_ENERGY], en);
-    __threadfence();
-    last = atomicAdd(A.ticket, 1u) == gridDim.x - 1;
+    int nb = A.rows[r0].nlo, ne = nb + A.rows[r0].len;
+    for (int r = 1; r < nr; r++) {
+      const int lo = A.rows[r0 + r].nlo;
+      nb = min(nb, lo);
+      ne = max(ne, lo + A.rows[r0 + r].len);
+    }
+    s_nb = nb;
+    s_ne = ne;
+  }
+  for (int u = threadIdx.x; u < nr * cnt; u += kThreads) {
+    const int r = u / cnt, s = u - r * cnt;
+    bxy[s * kXs + r] = A.XYr[(size_t)(r0 + r) * A.nw + s0 + s];
   }
   __syncthreads();
-  if (!last) return;
-  // every other block has added its sums
-  __threadfence();
-  if (threadIdx.x == 0) {
-    const double chg = atomicAdd(&A.scal[S_IND_CHANGE], 0.0);
-    const double ene = atomicAdd(&A.scal[S_IND_ENERGY], 0.0);
-    const int it = (int)A.state[kIterIters] + 1;
-    A.state[kIterIters] = (double)it;
-    A.state[kIterChange] = chg;
-    A.state[kIterEnergy] = ene;
-    A.scal[S_IND_CHANGE] = 0.0;
-    A.scal[S_IND_ENERGY] = 0.0;
-    *A.ticket = 0u;
-    const bool more = chg > A.thr && it < A.maxit;
-    if (!more) A.state[kIterFinished] = 1.0;
-    if (A.use_graph) cudaGraphSetConditional(A.handle, more ? 1u : 0u);
+  const int nb = s_nb, nn = s_ne - nb;  // nn <= row_span
+  for (int u = threadIdx.x; u < cnt * nn; u += kThreads) {
+    const int s = u / nn, j = u - s * nn;
+    zs[s * A.row_span + j] = A.Z[(size_t)(s0 + s) * A.nz + nb + j + A.nmax];
   }
+  pdl_wait();  // the previous step's dipoles (and its gather's last use of the S(k) buffer)
+  PcgIn pin;
+  if constexpr (PCG) pin = pcg_in(A);
+  for (int u = threadIdx.x; u < cnt * 3; u += kThreads) {
+    if constexpr (PCG) {
+      const int site = s0 + u / 3;
+      smu[u] = pin.comp((size_t)s0 * 3 + u, pin.apol(site % A.np));
+    } else {
+      smu[u] = A.mu[(size_t)s0 * 3 + u];
+    }
+  }
+  __syncthreads();
+  const int rs = threadIdx.x / kRowLanes, c = threadIdx.x % kRowLanes;
+  if (rs >= nr) return;
+  const KRow R = A.rows[r0 + rs];
+  const int jt = (nn + kRowLanes - 1) / kRowLanes;  // jt <= J: row_span
+  // the k-vector, k_n and staged Z column of each n; an n outside this row (past the tile's
+  // range for the last j, or outside a shorter row) reads column 0 and its sum is not stored
+  int kj[J], col[J];
+  double rnj[J];
+  bool ok[J];
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    const int n = nb + c + kRowLanes * j;
+    ok[j] = j < jt && n >= R.nlo && n < R.nlo + R.len;
+    kj[j] = ok[j] ? R.kbeg + (n - R.nlo) : 0;
+    col[j] = ok[j] ? n - nb : 0;
+    rnj[j] = ok[j] ? A.rn[n + A.nmax] : 0.0;
+  }
+  double ax[J], ay[J];
+#pragma unroll
+  for (int j = 0; j < J; j++) ax[j] = ay[j] = 0.0;
+#pragma unroll 2
+  for (int s = 0; s < cnt; s++) {
+    const double mx = smu[3 * s], my = smu[3 * s + 1], mz = smu[3 * s + 2];
+    const double2 xy = bxy[s * kXs + rs];
+    const double a = R.rl * mx + R.rm * my;
+    const double bx = xy.x * a, by = xy.y * a, cx = xy.x * mz, cy = xy.y * mz;
+    const double2 *zw = zs + s * A.row_span;
+#pragma unroll
+    for (int j = 0; j < J; j++) {
+      if (j < jt) {
+        const double2 z = zw[col[j]];
+        const double tx = rnj[j] * cx + bx, ty = rnj[j] * cy + by;
+        ax[j] += z.x * tx - z.y * ty;
+        ay[j] += z.x * ty + z.y * tx;
+      }
+    }
+  }
+  pdl_launch_dependents();
+#pragma unroll
+  for (int j = 0; j < J; j++) {
+    if (ok[j]) {
+      // kspace_efield_idm's weight (nb_induction_model.f90:2560-2600), applied before the merge
+      const double g = -4.0 * A.kv[kj[j]].ak;
+      atomicAdd(&A.sk[(size_t)kj[j] * 4 + 2 * A.par], g * ax[j]);
+      atomicAdd(&A.sk[(size_t)kj[j] * 4 + 2 * A.par + 1], g * ay[j]);
+    }
+  }
+}
+
+// Gather and update of the row form: a block takes kRowSites sites and its warps take the
+// groups of rows in turn (kRowR rows per thread, 32 / kRowSites threads per site, so a warp
+// covers 32 / kRowSites x kRowR consecutive rows of the length-sorted list, whose n ranges are
+// close).  The block's Z factors are staged in shared memory before the wait for the step's
+// first kernel (they are fixed during the solve), and each warp stages the F(k) of a group's
+// rows before running over its n range, so that the loop reads only shared memory.  The
+// update is k_iter_b's.
+template <bool PCG>
+__global__ void __launch_bounds__(kRowWarps * 32) k_iter_b_rows(IterArgs A) {
+  constexpr int kSB = kRowSites, kRL = 32 / kRowSites, kG = kRL * kRowR;
+  // Z [n][site] of the block's sites (nz rows), then per warp the F(k) [row][n - nlo] of its
+  // group's kG rows (row stride row_span)
+  extern __shared__ double2 zsh[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int si = lane % kSB, h = lane / kSB;
+  const int w0 = blockIdx.x * kSB;
+  const int ns_blk = min(kSB, A.nw - w0);
+  for (int u = threadIdx.x; u < A.nz * kSB; u += kRowWarps * 32) {
+    const int ni = u / kSB, s = u - ni * kSB;
+    zsh[u] = s < ns_blk ? A.ZT[(size_t)ni * A.nw + w0 + s] : make_double2(0.0, 0.0);
+  }
+  double2 *fsh = zsh + (size_t)A.nz * kSB + (size_t)wid * kG * A.row_span;
+  pdl_wait();  // T.mu, S(k) and the step scalars of this step's first kernel
+  __syncthreads();  // the staged Z
+  if (A.state[kIterFinished] != 0.0) return;  // finished in an earlier step of this pass
+  const int wc = w0 + (si < ns_blk ? si : 0);  // the site whose XY this lane reads
+  const double2 *skp = reinterpret_cast<const double2 *>(A.sk) + A.par;
+  const double2 *xyr = A.XYr + wc;
+  const double2 *zl = zsh + si + A.nmax * kSB;  // Z of n at zl[n * kSB]
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  const int ng = (A.nrow + kG - 1) / kG;
+  for (int g = wid; g < ng; g += kRowWarps) {
+    // the warp's rows g kG .. g kG + kG - 1: stage their F(k), then this lane's kRowR of them
+    const int gb = g * kG, gn = min(kG, A.nrow - gb);
+    __syncwarp();  // the previous group's reads of the staging buffer are done
+    for (int u = lane; u < gn * A.row_span; u += 32) {
+      const int r = u / A.row_span, j = u - r * A.row_span;
+      const KRow &K = A.rows[gb + r];
+      if (j < K.len) fsh[u] = skp[2 * (size_t)(K.kbeg + j)];
+    }
+    __syncwarp();
+    const int rb = gb + h * kRowR;  // this lane's rows rb .. rb + kRowR - 1
+    int nlo[kRowR], len[kRowR];
+    int nb = INT_MAX, ne = INT_MIN;
+#pragma unroll
+    for (int r = 0; r < kRowR; r++) {
+      nlo[r] = len[r] = 0;
+      if (rb + r < A.nrow) {
+        const KRow &K = A.rows[rb + r];
+        nlo[r] = K.nlo;
+        len[r] = K.len;
+        nb = min(nb, nlo[r]);
+        ne = max(ne, nlo[r] + len[r]);
+      }
+    }
+    // the warp runs the n range of all its rows
+#pragma unroll
+    for (int o = kSB; o < 32; o <<= 1) {
+      nb = min(nb, __shfl_xor_sync(0xffffffffu, nb, o));
+      ne = max(ne, __shfl_xor_sync(0xffffffffu, ne, o));
+    }
+    const double2 *fl = fsh + (size_t)h * kRowR * A.row_span;
+    double qx[kRowR], qy[kRowR], zx[kRowR], zy[kRowR];
+#pragma unroll
+    for (int r = 0; r < kRowR; r++) qx[r] = qy[r] = zx[r] = zy[r] = 0.0;
+#pragma unroll 2
+    for (int n = nb; n < ne; n++) {
+      const double2 z = zl[n * kSB];
+      const double rn = A.rn[n + A.nmax];
+#pragma unroll
+      for (int r = 0; r < kRowR; r++) {
+        if ((unsigned)(n - nlo[r]) < (unsigned)len[r]) {
+          // kspace_efield_idm gather (nb_induction_model.f90:2560-2600): the phase times the
+          // conjugate of the weighted S(k), summed over the row
+          const double2 f = fl[r * A.row_span + (n - nlo[r])];
+          const double px = z.x * f.x + z.y * f.y, py = z.y * f.x - z.x * f.y;
+          qx[r] += px;
+          qy[r] += py;
+          zx[r] += rn * px;
+          zy[r] += rn * py;
+        }
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kRowR; r++) {
+      if (len[r] > 0) {
+        const KRow &K = A.rows[rb + r];
+        const double2 xy = xyr[(size_t)(rb + r) * A.nw];
+        const double a = xy.x * qx[r] - xy.y * qy[r];
+        ex += K.rl * a;
+        ey += K.rm * a;
+        ez += xy.x * zx[r] - xy.y * zy[r];
+      }
+    }
+  }
+  pdl_launch_dependents();  // the gather, the bulk of the kernel, is done
+#pragma unroll
+  for (int o = kSB; o < 32; o <<= 1) {
+    ex += __shfl_xor_sync(0xffffffffu, ex, o);
+    ey += __shfl_xor_sync(0xffffffffu, ey, o);
+    ez += __shfl_xor_sync(0xffffffffu, ez, o);
+  }
+  __shared__ double part[kRowWarps][3][kSB];
+  if (h == 0) {
+    part[wid][0][si] = ex;
+    part[wid][1][si] = ey;
+    part[wid][2][si] = ez;
+  }
+  __syncthreads();
+  const auto ek = [&](int g, int c) {
+    double v = 0.0;
+    for (int u = 0; u < kRowWarps; u++) v += part[u][c][g];
+    return v;
+  };
+  if constexpr (PCG)
+    pcg_update(A, w0, ns_blk, ek);
+  else
+    jacobi_update(A, w0, ns_blk, ek);
 }
 
 // The first Jacobi step from mu = 0 (nb_induction_model.f90:1317-1359), where T.mu and the
@@ -603,12 +922,45 @@ cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream
   return cudaLaunchKernelEx(&cfg, kernel, A);
 }
 
+// Dynamic shared memory of the row form's two kernels; the row form runs only where both fit
+// the default 48 KB per block (less the static arrays).
+size_t iter_rows_smem_a(int sum_sites, int row_span) {
+  return sizeof(double) * (size_t)((3 * sum_sites + 1) & ~1) +
+         sizeof(double2) * (size_t)sum_sites * (kRowTile + 1 + row_span);
+}
+size_t iter_rows_smem_b(int nz, int row_span) {
+  return sizeof(double2) *
+         ((size_t)nz * kRowSites + (size_t)kRowWarps * 32 / kRowSites * kRowR * row_span);
+}
+bool iter_rows_fit(int sum_sites, int nz, int row_span) {
+  constexpr size_t kDefault = 48 * 1024 - 2048;  // room for the static shared arrays
+  return iter_rows_smem_a(sum_sites, row_span) <= kDefault &&
+         iter_rows_smem_b(nz, row_span) <= kDefault;
+}
+
+template <int J>
+cudaError_t launch_iter_a_rows(const IterArgs &A, int nb, size_t smem, cudaStream_t st) {
+  return A.cu ? launch_step(k_iter_a_rows<true, J>, nb, A, st, smem)
+              : launch_step(k_iter_a_rows<false, J>, nb, A, st, smem);
+}
+
 cudaError_t launch_iter_a(const IterArgs &A, cudaStream_t st) {
   if (A.sum_sites < 1 || A.sum_sites > kSumSitesMax) return cudaErrorInvalidValue;
-  const size_t smem = sizeof(double) * 3 * A.sum_sites;
   const int nA = (A.nw + kWarps - 1) / kWarps;
-  const int nkt = (A.nk + kThreads - 1) / kThreads;
   const int nsc = (A.nw + A.sum_sites - 1) / A.sum_sites;
+  if (A.rows) {
+    if (!iter_rows_fit(A.sum_sites, A.nz, A.row_span)) return cudaErrorInvalidValue;
+    const int ntile = (A.nrow + kRowTile - 1) / kRowTile;
+    const size_t smem = iter_rows_smem_a(A.sum_sites, A.row_span);
+    const int nb = nA + ntile * nsc;
+    const int j = (A.row_span + kRowLanes - 1) / kRowLanes;
+    if (j <= 2) return launch_iter_a_rows<2>(A, nb, smem, st);
+    if (j <= 4) return launch_iter_a_rows<4>(A, nb, smem, st);
+    if (j <= 8) return launch_iter_a_rows<8>(A, nb, smem, st);
+    return cudaErrorInvalidValue;
+  }
+  const size_t smem = sizeof(double) * 3 * A.sum_sites;
+  const int nkt = (A.nk + kThreads - 1) / kThreads;
   const int nb = nA + nkt * nsc;
   if (A.PM)
     return A.cu ? launch_step(k_iter_a<true, true>, nb, A, st, smem)
@@ -629,6 +981,13 @@ cudaError_t launch_iter_b_gs(const IterArgs &A, cudaStream_t st) {
 }
 
 cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
+  if (A.rows) {
+    if (!iter_rows_fit(A.sum_sites, A.nz, A.row_span)) return cudaErrorInvalidValue;
+    const int nb = (A.nw + kRowSites - 1) / kRowSites;
+    const size_t smem = iter_rows_smem_b(A.nz, A.row_span);
+    return A.cu ? launch_step(k_iter_b_rows<true>, nb, A, st, smem, kRowWarps * 32)
+                : launch_step(k_iter_b_rows<false>, nb, A, st, smem, kRowWarps * 32);
+  }
   switch (A.gather_sites) {
     case 2: return launch_iter_b_gs<2>(A, st);
     case 3: return launch_iter_b_gs<3>(A, st);
@@ -637,6 +996,20 @@ cudaError_t launch_iter_b(const IterArgs &A, cudaStream_t st) {
     case 8: return launch_iter_b_gs<8>(A, st);
     default: return cudaErrorInvalidValue;
   }
+}
+
+cudaError_t launch_phase_rows(const double2 *tab, int nm, SiteSets S, int kl, int km, int kn,
+                              const KRow *rows, int nrow, double2 *XYr, double2 *Z,
+                              double2 *ZT, cudaStream_t st) {
+  int k1 = kl > km ? kl : km;
+  k1 = (k1 > kn ? k1 : kn) + 1;
+  if (k1 < 2) k1 = 2;
+  const size_t total = (size_t)nm * S.np * ((size_t)nrow + 2 * kn + 1);
+  if (total == 0) return cudaSuccess;
+  size_t blocks = (total + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  k_phase_rows<<<(unsigned)blocks, 256, 0, st>>>(tab, nm, S, k1, km, kn, rows, nrow, XYr, Z, ZT);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_phase_matrix(const KGather *kg, int nk, int nw, int nlm, int nz,

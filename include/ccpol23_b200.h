@@ -407,6 +407,11 @@ int ccp_context_phase_ms(const ccp_context *ctx, double *ms, int n);
                      phase matrix is formed once per evaluation when it fits in half of the L2
                      (38 MB at 512 waters), and the dipole steps read one phase per pair;
                      0: never.  Query "phase_matrix_full_active" tells whether it was used;
+     "dipole_row_form" 1 (default): without the full phase matrix, the dipole steps take the
+                     reciprocal sums row by row of the k-vector list (one (l, m), a run of n),
+                     so each loaded factor serves many products; 0: one phase per (site,
+                     k-vector) product from the factor tables.  The same sums to rounding.
+                     Query "dipole_row_form_active" tells whether it was used;
      "dipole_sum_sites" 1..128 (default 32): polarisable sites per structure-factor block of
                      a dipole step (a tuning option; results unchanged);
      "dipole_gather_sites" 2, 3, 4 (default), 6 or 8: polarisable sites per reciprocal-field

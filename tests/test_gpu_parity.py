@@ -104,22 +104,28 @@ def test_nb_induction(oracle, boxes, key):
     assert abs(vir[0] - st.vir.value) <= TOL * abs(st.vir.value)
 
 
-@pytest.mark.parametrize("graph_loop,phase_matrix", [(1, 0), (0, 1), (0, 0)])
-def test_nb_induction_loop_forms(oracle, boxes, graph_loop, phase_matrix):
+@pytest.mark.parametrize("key,graph_loop,phase_matrix,full,rows",
+                         [("c1", 1, 0, 1, 1), ("c1", 0, 1, 1, 1), ("c1", 0, 0, 1, 1),
+                          ("c1", 1, 1, 0, 1), ("ragged_37", 1, 1, 0, 1), ("c1", 1, 1, 0, 0)])
+def test_nb_induction_loop_forms(oracle, boxes, key, graph_loop, phase_matrix, full, rows):
     """The dipole solve's other execution forms (host-driven loop; tiled on-the-fly
-    reciprocal kernels instead of the phase matrix) give the same results."""
+    reciprocal kernels instead of the phase tables; without the full phase matrix, the row
+    form or the factor-table kernels) give the same results."""
     O = oracle
-    m, b, M = boxes["c1"]
+    m, b, M = boxes[key]
     args = (b.x, b.y, b.z, b.xs, b.ys, b.zs)
     st = _state(O, b.nm, b.xs.shape[1])
     eo, status, it_o = O.nb_induction(M, *args, b.box, st)
     with _ctx(m, b) as c:
         c.set_option("graph_loop", graph_loop)
         c.set_option("phase_matrix", phase_matrix)
+        c.set_option("phase_matrix_full", full)
+        c.set_option("dipole_row_form", rows)
         fx, fy, fz, mx, my, mz = (np.zeros_like(b.xs) for _ in range(6))
         vir = np.zeros(1)
         eg, it_g = c.nb_induction(*args, b.box, mx, my, mz, fx, fy, fz, vir)
         assert c.get_option("phase_matrix_active") == phase_matrix
+        assert c.get_option("dipole_row_form_active") == (phase_matrix and not full and rows)
     assert it_g == it_o
     assert abs(eg - eo) <= TOL * abs(eo), (eg, eo)
     assert rel(np.stack([mx, my, mz]), np.stack([st.idmx, st.idmy, st.idmz])) <= TOL

@@ -94,16 +94,50 @@ def test_fs3_table_reuse_matches_single_triple_blocks(box, precision, fp32_passe
     assert rel(c8, c1) <= 1e-12
 
 
+@pytest.mark.parametrize("sum_sites", [32, 7])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_row_form_matches_factor_tables(box, precision, sum_sites):
+    """Without the full phase matrix the dipole step runs in its row form (the reciprocal sums
+    regrouped by k-vector rows) or on the factor tables: the same step to rounding, with the
+    same iteration count.  A chunk of 7 sites leaves ragged chunks and tiles."""
+    m, b = box
+    nm, ld = b.xs.shape
+    out = []
+    for rows in (1, 0):
+        args = [_dev(a) for a in (b.x, b.y, b.z, b.xs, b.ys, b.zs)]
+        f = [_zeros((nm, ld)) for _ in range(3)]
+        mu = [_zeros((nm, ld)) for _ in range(3)]
+        with Context(m, nm, b.box, precision=precision) as c:
+            c.set_option("phase_matrix_full", 0)
+            c.set_option("dipole_row_form", rows)
+            c.set_option("dipole_sum_sites", sum_sites)
+            e = c.terms_device(_lib.TERM_HOT, *args, b.box, *f, None, None, None, None, None,
+                               None, *mu)
+            assert c.get_option("phase_matrix_full_active") == 0
+            assert c.get_option("dipole_row_form_active") == rows
+        out.append((e, np.stack([t.cpu().numpy() for t in f]),
+                    np.stack([t.cpu().numpy() for t in mu])))
+    (e1, f1, m1), (e0, f0, m0) = out
+    assert e1["ind_iters"] == e0["ind_iters"]
+    for k in ENERGIES:
+        assert e1[k] == pytest.approx(e0[k], rel=1e-12), k
+    assert rel(f1, f0) <= 1e-12
+    assert rel(m1, m0) <= 1e-12
+
+
 @pytest.mark.parametrize("opt,values", [("pdl", (1, 0)), ("fs3_high_priority", (1, 0)),
                                         ("graph_loop", (1, 0)), ("phase_matrix_full", (1, 0)),
+                                        ("dipole_row_form", (1, 0)),
                                         ("dipole_gather_sites", (4, 3)),
                                         ("dipole_gather_sites", (4, 8)),
                                         ("dipole_sum_sites", (32, 100))])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_launch_options_give_the_same_results(box, opt, values, precision):
     """Programmatic dependent launch of the dipole steps, FS3's stream priority, the graph
-    against the host-driven loop, the full phase matrix against the factor tables and the
-    dipole step's block shapes change how the work is done, not what it computes."""
+    against the host-driven loop, the full phase matrix against the row form of the dipole
+    step, and the dipole step's block shapes change how the work is done, not what it
+    computes.  (This box's phase matrix fits in L2, so `dipole_row_form` alone changes
+    nothing here; the row form's own test turns the matrix off.)"""
     m, b = box
     nm, ld = b.xs.shape
     out = []
