@@ -161,7 +161,7 @@ struct KRow {
   double rl, rm;
   int kbeg, len, nlo, lm;
 };
-constexpr int kRowTile = 16;  // rows per structure-factor block of the row form
+constexpr int kRowTile = 32;  // rows per structure-factor block of the row form
 
 // Arguments of one step of the dipole solve with the phase matrix (k_iter.cu): a Jacobi step,
 // or with cu.. set a preconditioned-conjugate-gradient step.

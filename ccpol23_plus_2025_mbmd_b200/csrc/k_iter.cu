@@ -574,18 +574,20 @@ constexpr int kRowLanes = 8;  // n lanes per row of a structure-factor block: n 
 #define CCP_ROW_R 4
 #endif
 #ifndef CCP_ROW_WARPS
-#define CCP_ROW_WARPS 4
+#define CCP_ROW_WARPS 8
 #endif
 constexpr int kRowSites = CCP_ROW_SITES, kRowR = CCP_ROW_R, kRowWarps = CCP_ROW_WARPS;
 static_assert(kRowSites == 8 || kRowSites == 16 || kRowSites == 32, "sites per gather block");
+static_assert(kThreads / kRowLanes * 2 == kRowTile, "a structure-factor block takes two rows per thread");
 
 // Structure factors of the row form: block b (after the T.mu blocks) covers tile b % ntile
 // (kRowTile consecutive rows of the length-sorted list, n in [nb, ne) of their union) and the
-// sites of chunk b / ntile.  A thread takes one row and the n = nb + lane + 8 j (j < J) of it;
-// the partial sums are merged with FP64 atomics as in k_iter_a.  The chunk's XY factors of
-// the tile's rows and its Z factors of the tile's n range are staged in shared memory before
-// the wait for the previous step (the tables are fixed during the solve), so the site loop
-// reads only shared memory.
+// sites of chunk b / ntile.  A thread takes two adjacent rows of the tile and the n = nb +
+// lane + 8 j (j < J) of them, so that each Z factor it loads serves both; the partial sums are
+// merged with FP64 atomics as in k_iter_a.  The chunk's XY factors of the tile's rows and its
+// Z factors of the tile's n range are staged in shared memory before the wait for the
+// previous step (the tables are fixed during the solve), so the site loop reads only shared
+// memory.
 template <bool PCG, int J>
 __global__ void __launch_bounds__(kThreads) k_iter_a_rows(IterArgs A) {
   const int nA = (A.nw + kWarps - 1) / kWarps;
@@ -596,11 +598,11 @@ __global__ void __launch_bounds__(kThreads) k_iter_a_rows(IterArgs A) {
     iter_a_tmu<PCG>(A, pin, nA);
     return;
   }
-  // sum_sites x 3 dipole components, the XY factors [site][row] of the tile's rows and the
-  // Z factors [site][n - nb] of its n range (row stride row_span)
-  extern __shared__ double smu[];
+  // the chunk's dipoles [site] (x, y, z, 0), the XY factors [site][row] of the tile's rows and
+  // the Z factors [site][n - nb] of its n range (row stride row_span)
+  extern __shared__ double4 smu4[];
   constexpr int kXs = kRowTile + 1;  // site stride of the staged XY: no bank conflicts
-  double2 *bxy = reinterpret_cast<double2 *>(smu + ((3 * A.sum_sites + 1) & ~1));
+  double2 *bxy = reinterpret_cast<double2 *>(smu4 + A.sum_sites);
   double2 *zs = bxy + (size_t)A.sum_sites * kXs;
   __shared__ int s_nb, s_ne;
   const int b = blockIdx.x - nA;
@@ -631,60 +633,76 @@ __global__ void __launch_bounds__(kThreads) k_iter_a_rows(IterArgs A) {
   pdl_wait();  // the previous step's dipoles (and its gather's last use of the S(k) buffer)
   PcgIn pin;
   if constexpr (PCG) pin = pcg_in(A);
-  for (int u = threadIdx.x; u < cnt * 3; u += kThreads) {
+  for (int u = threadIdx.x; u < cnt; u += kThreads) {
+    const size_t o = (size_t)(s0 + u) * 3;
     if constexpr (PCG) {
-      const int site = s0 + u / 3;
-      smu[u] = pin.comp((size_t)s0 * 3 + u, pin.apol(site % A.np));
+      const double ap = pin.apol((s0 + u) % A.np);
+      smu4[u] = make_double4(pin.comp(o, ap), pin.comp(o + 1, ap), pin.comp(o + 2, ap), 0.0);
     } else {
-      smu[u] = A.mu[(size_t)s0 * 3 + u];
+      smu4[u] = make_double4(A.mu[o], A.mu[o + 1], A.mu[o + 2], 0.0);
     }
   }
   __syncthreads();
-  const int rs = threadIdx.x / kRowLanes, c = threadIdx.x % kRowLanes;
-  if (rs >= nr) return;
-  const KRow R = A.rows[r0 + rs];
+  const int ra = 2 * (threadIdx.x / kRowLanes), c = threadIdx.x % kRowLanes;
+  if (ra >= nr) return;
+  // this thread's rows ra and ra + 1 of the tile (the second empty past the tile's end)
+  const KRow R0 = A.rows[r0 + ra];
+  KRow R1 = R0;
+  if (ra + 1 < nr)
+    R1 = A.rows[r0 + ra + 1];
+  else
+    R1.len = 0;
+  const int rb1 = ra + 1 < nr ? ra + 1 : ra;
   const int jt = (nn + kRowLanes - 1) / kRowLanes;  // jt <= J: row_span
-  // the k-vector, k_n and staged Z column of each n; an n outside this row (past the tile's
-  // range for the last j, or outside a shorter row) reads column 0 and its sum is not stored
-  int kj[J], col[J];
+  // per n = nb + c + 8 j: the staged Z column (clamped to the range, so idle lanes read a
+  // column another lane reads), k_n, and the k-vector of each row that holds that n
+  int col[J], k0[J], k1[J];
   double rnj[J];
-  bool ok[J];
 #pragma unroll
   for (int j = 0; j < J; j++) {
-    const int n = nb + c + kRowLanes * j;
-    ok[j] = j < jt && n >= R.nlo && n < R.nlo + R.len;
-    kj[j] = ok[j] ? R.kbeg + (n - R.nlo) : 0;
-    col[j] = ok[j] ? n - nb : 0;
-    rnj[j] = ok[j] ? A.rn[n + A.nmax] : 0.0;
+    const int d = c + kRowLanes * j, n = nb + d;
+    col[j] = min(d, nn - 1);
+    rnj[j] = d < nn ? A.rn[n + A.nmax] : 0.0;
+    k0[j] = j < jt && n >= R0.nlo && n < R0.nlo + R0.len ? R0.kbeg + (n - R0.nlo) : -1;
+    k1[j] = j < jt && n >= R1.nlo && n < R1.nlo + R1.len ? R1.kbeg + (n - R1.nlo) : -1;
   }
-  double ax[J], ay[J];
+  double ax[J], ay[J], bx_[J], by_[J];
 #pragma unroll
-  for (int j = 0; j < J; j++) ax[j] = ay[j] = 0.0;
+  for (int j = 0; j < J; j++) ax[j] = ay[j] = bx_[j] = by_[j] = 0.0;
 #pragma unroll 2
   for (int s = 0; s < cnt; s++) {
-    const double mx = smu[3 * s], my = smu[3 * s + 1], mz = smu[3 * s + 2];
-    const double2 xy = bxy[s * kXs + rs];
-    const double a = R.rl * mx + R.rm * my;
-    const double bx = xy.x * a, by = xy.y * a, cx = xy.x * mz, cy = xy.y * mz;
+    const double4 m = smu4[s];
+    const double2 xy0 = bxy[s * kXs + ra], xy1 = bxy[s * kXs + rb1];
+    const double a0 = R0.rl * m.x + R0.rm * m.y, a1 = R1.rl * m.x + R1.rm * m.y;
+    const double b0x = xy0.x * a0, b0y = xy0.y * a0, c0x = xy0.x * m.z, c0y = xy0.y * m.z;
+    const double b1x = xy1.x * a1, b1y = xy1.y * a1, c1x = xy1.x * m.z, c1y = xy1.y * m.z;
     const double2 *zw = zs + s * A.row_span;
 #pragma unroll
     for (int j = 0; j < J; j++) {
       if (j < jt) {
         const double2 z = zw[col[j]];
-        const double tx = rnj[j] * cx + bx, ty = rnj[j] * cy + by;
-        ax[j] += z.x * tx - z.y * ty;
-        ay[j] += z.x * ty + z.y * tx;
+        const double t0x = rnj[j] * c0x + b0x, t0y = rnj[j] * c0y + b0y;
+        const double t1x = rnj[j] * c1x + b1x, t1y = rnj[j] * c1y + b1y;
+        ax[j] += z.x * t0x - z.y * t0y;
+        ay[j] += z.x * t0y + z.y * t0x;
+        bx_[j] += z.x * t1x - z.y * t1y;
+        by_[j] += z.x * t1y + z.y * t1x;
       }
     }
   }
   pdl_launch_dependents();
 #pragma unroll
   for (int j = 0; j < J; j++) {
-    if (ok[j]) {
-      // kspace_efield_idm's weight (nb_induction_model.f90:2560-2600), applied before the merge
-      const double g = -4.0 * A.kv[kj[j]].ak;
-      atomicAdd(&A.sk[(size_t)kj[j] * 4 + 2 * A.par], g * ax[j]);
-      atomicAdd(&A.sk[(size_t)kj[j] * 4 + 2 * A.par + 1], g * ay[j]);
+    // kspace_efield_idm's weight (nb_induction_model.f90:2560-2600), applied before the merge
+    if (k0[j] >= 0) {
+      const double g = -4.0 * A.kv[k0[j]].ak;
+      atomicAdd(&A.sk[(size_t)k0[j] * 4 + 2 * A.par], g * ax[j]);
+      atomicAdd(&A.sk[(size_t)k0[j] * 4 + 2 * A.par + 1], g * ay[j]);
+    }
+    if (k1[j] >= 0) {
+      const double g = -4.0 * A.kv[k1[j]].ak;
+      atomicAdd(&A.sk[(size_t)k1[j] * 4 + 2 * A.par], g * bx_[j]);
+      atomicAdd(&A.sk[(size_t)k1[j] * 4 + 2 * A.par + 1], g * by_[j]);
     }
   }
 }
@@ -697,7 +715,7 @@ __global__ void __launch_bounds__(kThreads) k_iter_a_rows(IterArgs A) {
 // rows before running over its n range, so that the loop reads only shared memory.  The
 // update is k_iter_b's.
 template <bool PCG>
-__global__ void __launch_bounds__(kRowWarps * 32) k_iter_b_rows(IterArgs A) {
+__global__ void __launch_bounds__(kRowWarps * 32, 768 / (kRowWarps * 32)) k_iter_b_rows(IterArgs A) {
   constexpr int kSB = kRowSites, kRL = 32 / kRowSites, kG = kRL * kRowR;
   // Z [n][site] of the block's sites (nz rows), then per warp the F(k) [row][n - nlo] of its
   // group's kG rows (row stride row_span)
@@ -710,7 +728,9 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_iter_b_rows(IterArgs A) {
     const int ni = u / kSB, s = u - ni * kSB;
     zsh[u] = s < ns_blk ? A.ZT[(size_t)ni * A.nw + w0 + s] : make_double2(0.0, 0.0);
   }
-  double2 *fsh = zsh + (size_t)A.nz * kSB + (size_t)wid * kG * A.row_span;
+  double *rns = reinterpret_cast<double *>(zsh + (size_t)A.nz * kSB);  // k_n by n + nmax
+  for (int u = threadIdx.x; u < A.nz; u += kRowWarps * 32) rns[u] = A.rn[u];
+  double2 *fsh = zsh + (size_t)A.nz * kSB + (A.nz + 1) / 2 + (size_t)wid * kG * A.row_span;
   pdl_wait();  // T.mu, S(k) and the step scalars of this step's first kernel
   __syncthreads();  // the staged Z
   if (A.state[kIterFinished] != 0.0) return;  // finished in an earlier step of this pass
@@ -751,13 +771,18 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_iter_b_rows(IterArgs A) {
       ne = max(ne, __shfl_xor_sync(0xffffffffu, ne, o));
     }
     const double2 *fl = fsh + (size_t)h * kRowR * A.row_span;
+    // this lane's XY factors of its rows, loaded now so that their latency overlaps the sums
+    double2 xy[kRowR];
+#pragma unroll
+    for (int r = 0; r < kRowR; r++)
+      xy[r] = len[r] > 0 ? xyr[(size_t)(rb + r) * A.nw] : make_double2(0.0, 0.0);
     double qx[kRowR], qy[kRowR], zx[kRowR], zy[kRowR];
 #pragma unroll
     for (int r = 0; r < kRowR; r++) qx[r] = qy[r] = zx[r] = zy[r] = 0.0;
 #pragma unroll 2
     for (int n = nb; n < ne; n++) {
       const double2 z = zl[n * kSB];
-      const double rn = A.rn[n + A.nmax];
+      const double rn = rns[n + A.nmax];
 #pragma unroll
       for (int r = 0; r < kRowR; r++) {
         if ((unsigned)(n - nlo[r]) < (unsigned)len[r]) {
@@ -776,11 +801,10 @@ __global__ void __launch_bounds__(kRowWarps * 32) k_iter_b_rows(IterArgs A) {
     for (int r = 0; r < kRowR; r++) {
       if (len[r] > 0) {
         const KRow &K = A.rows[rb + r];
-        const double2 xy = xyr[(size_t)(rb + r) * A.nw];
-        const double a = xy.x * qx[r] - xy.y * qy[r];
+        const double a = xy[r].x * qx[r] - xy[r].y * qy[r];
         ex += K.rl * a;
         ey += K.rm * a;
-        ez += xy.x * zx[r] - xy.y * zy[r];
+        ez += xy[r].x * zx[r] - xy[r].y * zy[r];
       }
     }
   }
@@ -925,12 +949,12 @@ cudaError_t launch_step(Kernel kernel, int blocks, const IterArgs &A, cudaStream
 // Dynamic shared memory of the row form's two kernels; the row form runs only where both fit
 // the default 48 KB per block (less the static arrays).
 size_t iter_rows_smem_a(int sum_sites, int row_span) {
-  return sizeof(double) * (size_t)((3 * sum_sites + 1) & ~1) +
+  return sizeof(double4) * (size_t)sum_sites +
          sizeof(double2) * (size_t)sum_sites * (kRowTile + 1 + row_span);
 }
 size_t iter_rows_smem_b(int nz, int row_span) {
-  return sizeof(double2) *
-         ((size_t)nz * kRowSites + (size_t)kRowWarps * 32 / kRowSites * kRowR * row_span);
+  return sizeof(double2) * ((size_t)nz * kRowSites + (nz + 1) / 2 +
+                            (size_t)kRowWarps * 32 / kRowSites * kRowR * row_span);
 }
 bool iter_rows_fit(int sum_sites, int nz, int row_span) {
   constexpr size_t kDefault = 48 * 1024 - 2048;  // room for the static shared arrays
