@@ -323,7 +323,7 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_single(which, host_loop=False, config=CONFIG):
+def run_single(which, host_loop=False, config=CONFIG, opts=()):
     import torch
     from ccpol23_plus_2025_mbmd_b200 import Context
     model, box, cfg = build_inputs(0, config)
@@ -335,6 +335,8 @@ def run_single(which, host_loop=False, config=CONFIG):
             ctx.set_timing(True)
             if host_loop:
                 ctx.set_option("graph_loop", 0)
+            for k, v in opts:
+                ctx.set_option(k, v)
             f = [torch.zeros_like(args[3]) for _ in range(3)]
             for _ in range(3):  # the first call sizes lists and builds the dipole-loop graph
                 e = ctx.hot_path_device(*args, box.box, *f)
@@ -577,7 +579,7 @@ def main():
                     help="print the critical-path floor table (chain, dipole loop, three-body "
                          "terms and FS3 alone, overlapped and in order) per form instead")
     ap.add_argument("--opt", action="append", default=[], metavar="NAME=VALUE",
-                    help="with --floor: a context option set on both forms (repeatable)")
+                    help="with --floor or --single: a context option set on every form (repeatable)")
     ap.add_argument("--host-loop", action="store_true",
                     help="with --single: drive the dipole iteration from the host, so that "
                          "profilers see its kernels")
@@ -585,11 +587,11 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    opts = [(kv.split("=", 1)[0], int(kv.split("=", 1)[1])) for kv in args.opt]
     if args.single:
-        run_single(args.single, args.host_loop, args.config)
+        run_single(args.single, args.host_loop, args.config, opts)
         return
     if args.floor:
-        opts = [(kv.split("=", 1)[0], int(kv.split("=", 1)[1])) for kv in args.opt]
         run_floor(args.config, args.steps, args.warmup, opts)
         return
     if args.nve:
