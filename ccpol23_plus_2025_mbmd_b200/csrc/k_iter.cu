@@ -22,6 +22,10 @@
 //      of a graph body that unrolls several steps then returns at once) and, inside the
 //      graph, sets the WHILE node's condition.  S(k) alternates between two buffers by step
 //      parity, so no block has to clear it after the gather.
+// When the full phase matrix [site][k] fits in L2 both passes read one phase per pair from
+// it; otherwise the row form (k_iter_a_rows, k_iter_b_rows below) takes the sums row by row
+// of the k-vector list from factors staged in shared memory.  The same step can also run on
+// the factor tables alone (k_iter_a/k_iter_b without the matrix).
 #include <climits>
 
 #include "ccp_device.cuh"
@@ -576,7 +580,12 @@ constexpr int kRowLanes = 8;  // n lanes per row of a structure-factor block: n 
 #ifndef CCP_ROW_WARPS
 #define CCP_ROW_WARPS 8
 #endif
+// structure-factor blocks resident per SM that the register allocation targets
+#ifndef CCP_ROW_SUM_BLOCKS
+#define CCP_ROW_SUM_BLOCKS 1
+#endif
 constexpr int kRowSites = CCP_ROW_SITES, kRowR = CCP_ROW_R, kRowWarps = CCP_ROW_WARPS;
+constexpr int kRowSumBlocks = CCP_ROW_SUM_BLOCKS;
 static_assert(kRowSites == 8 || kRowSites == 16 || kRowSites == 32, "sites per gather block");
 static_assert(kThreads / kRowLanes * 2 == kRowTile, "a structure-factor block takes two rows per thread");
 
@@ -589,7 +598,7 @@ static_assert(kThreads / kRowLanes * 2 == kRowTile, "a structure-factor block ta
 // previous step (the tables are fixed during the solve), so the site loop reads only shared
 // memory.
 template <bool PCG, int J>
-__global__ void __launch_bounds__(kThreads) k_iter_a_rows(IterArgs A) {
+__global__ void __launch_bounds__(kThreads, kRowSumBlocks) k_iter_a_rows(IterArgs A) {
   const int nA = (A.nw + kWarps - 1) / kWarps;
   if ((int)blockIdx.x < nA) {
     pdl_wait();  // the previous step's dipoles (and its gather's last use of the S(k) buffer)
