@@ -20,7 +20,9 @@ namespace {
 constexpr int kKT = 64;     // k-vectors per tile
 constexpr int kST = 64;     // sites per tile
 constexpr int kThreads = 256;
-constexpr int kParts = kThreads / 64;  // lanes sharing one k (sums) or one site (gather)
+constexpr int kParts = kThreads / kST;  // gathers: warps over a site tile, each a k quarter
+constexpr int kSumLanes = 2 * kThreads / kKT;  // sums: lanes over the sites of one k-vector
+static_assert(kSumLanes == 8 && kParts * kST == kThreads, "tile shapes");
 
 __global__ void k_ktab(const double4 *__restrict__ com, const double4 *__restrict__ act, int nm,
                        int na, double box, int k1, double2 *tab) {
@@ -64,20 +66,19 @@ __device__ __forceinline__ int tgt_slot(int mode, const SiteSets &S, int r) {
 }
 
 // exp(i k.r) of the staged site `ls` (tables [axis][l][site] in shared memory), in the
-// reference's product order.
-__device__ __forceinline__ void phase(const double2 *__restrict__ T, int k1, int ls, int l, int m,
-                                      int n, double &c, double &s) {
+// reference's product order: exp(i(l x + m y)) first (phase_lm), then times exp(i n z)
+// (phase_n), so that k-vectors of one (l, m) can share the first product.
+__device__ __forceinline__ double2 phase_lm(const double2 *__restrict__ T, int k1, int ls, int l,
+                                            int m) {
   const double2 el = T[(0 * k1 + l) * kST + ls];
   const double2 em = T[(1 * k1 + (m < 0 ? -m : m)) * kST + ls];
+  if (m >= 0) return make_double2(el.x * em.x - el.y * em.y, el.y * em.x + em.y * el.x);
+  return make_double2(el.x * em.x + el.y * em.y, el.y * em.x - em.y * el.x);
+}
+__device__ __forceinline__ void phase_n(const double2 *__restrict__ T, int k1, int ls,
+                                        double2 lm, int n, double &c, double &s) {
   const double2 en = T[(2 * k1 + (n < 0 ? -n : n)) * kST + ls];
-  double clm, slm;
-  if (m >= 0) {
-    clm = el.x * em.x - el.y * em.y;
-    slm = el.y * em.x + em.y * el.x;
-  } else {
-    clm = el.x * em.x + el.y * em.y;
-    slm = el.y * em.x - em.y * el.x;
-  }
+  const double clm = lm.x, slm = lm.y;
   if (n >= 0) {
     c = clm * en.x - slm * en.y;
     s = slm * en.x + clm * en.y;
@@ -136,47 +137,58 @@ __global__ void __launch_bounds__(kThreads)
   for (int u = threadIdx.x; u < kKT; u += blockDim.x)
     if (k0 + u < nk) K[u] = kv[k0 + u];
   __syncthreads();
-  const int kk = threadIdx.x / kParts, part = threadIdx.x % kParts;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  if (k0 + kk < nk) {
-    const KVec k = K[kk];
-    for (int ls = part; ls < cnt; ls += kParts) {
-      double c, s;
-      phase(T, k1, ls, k.l, k.m, k.n, c, s);
+  // kSumLanes lanes per k-vector over the sites, each thread two k-vectors (kk and kk +
+  // kKT / 2): a quarter-warp reads one table row at consecutive sites, and the site weights
+  // are loaded once for both k-vectors.  (Adjacent k-vectors sharing exp(i(l x + m y)) here
+  // cost registers and occupancy: k_ksums<3> took 548 against 443 us at 2048 waters.)
+  const int kk = threadIdx.x / kSumLanes, part = threadIdx.x % kSumLanes;
+  double a[2][4] = {{0.0, 0.0, 0.0, 0.0}, {0.0, 0.0, 0.0, 0.0}};
+  const bool on0 = k0 + kk < nk, on1 = k0 + kk + kKT / 2 < nk;
+  if (on0) {
+    const KVec ka = K[kk], kb = on1 ? K[kk + kKT / 2] : K[kk];
+    for (int ls = part; ls < cnt; ls += kSumLanes) {
       const double4 w = W[ls];
-      if (MODE <= 1) {
-        a0 += w.w * c;
-        a1 += w.w * s;
-      } else {
-        const double dk = k.rl * w.x + k.rm * w.y + k.rn * w.z;
-        if (MODE == 2) {
-          a0 += dk * c;
-          a1 += dk * s;
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const KVec &k = h == 0 ? ka : kb;
+        double c, s;
+        phase_n(T, k1, ls, phase_lm(T, k1, ls, k.l, k.m), k.n, c, s);
+        if (MODE <= 1) {
+          a[h][0] += w.w * c;
+          a[h][1] += w.w * s;
         } else {
-          a0 += w.w * c;
-          a1 += w.w * s;
-          a2 += dk * c;
-          a3 += dk * s;
+          const double dk = k.rl * w.x + k.rm * w.y + k.rn * w.z;
+          if (MODE == 2) {
+            a[h][0] += dk * c;
+            a[h][1] += dk * s;
+          } else {
+            a[h][0] += w.w * c;
+            a[h][1] += w.w * s;
+            a[h][2] += dk * c;
+            a[h][3] += dk * s;
+          }
         }
       }
     }
   }
 #pragma unroll
-  for (int off = 1; off < kParts; off <<= 1) {
-    a0 += __shfl_xor_sync(0xffffffffu, a0, off);
-    a1 += __shfl_xor_sync(0xffffffffu, a1, off);
-    if (MODE == 3) {
-      a2 += __shfl_xor_sync(0xffffffffu, a2, off);
-      a3 += __shfl_xor_sync(0xffffffffu, a3, off);
-    }
-  }
-  if (part == 0 && k0 + kk < nk) {
-    double *o = sk + (size_t)(k0 + kk) * 4;
-    atomicAdd(o, a0);
-    atomicAdd(o + 1, a1);
-    if (MODE == 3) {
-      atomicAdd(o + 2, a2);
-      atomicAdd(o + 3, a3);
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int off = 1; off < kSumLanes; off <<= 1)
+#pragma unroll
+      for (int c = 0; c < (MODE == 3 ? 4 : 2); c++)
+        a[h][c] += __shfl_xor_sync(0xffffffffu, a[h][c], off);
+  if (part == 0) {
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      if (h == 0 ? !on0 : !on1) continue;
+      double *o = sk + (size_t)(k0 + kk + h * (kKT / 2)) * 4;
+      atomicAdd(o, a[h][0]);
+      atomicAdd(o + 1, a[h][1]);
+      if (MODE == 3) {
+        atomicAdd(o + 2, a[h][2]);
+        atomicAdd(o + 3, a[h][3]);
+      }
     }
   }
 }
@@ -232,16 +244,27 @@ __global__ void __launch_bounds__(kThreads)
     A[u] = make_double4(s[0], s[1], s[2], s[3]);
   }
   __syncthreads();
-  const int ls = threadIdx.x / kParts, part = threadIdx.x % kParts;
+  // site-major lanes: a warp takes 32 consecutive sites of the tile and one contiguous
+  // quarter of its k-vectors, so its table loads are contiguous rows, its k-vector loads
+  // broadcasts, and consecutive k-vectors of one (l, m) share exp(i(l x + m y))
+  const int ls = threadIdx.x % kST, part = threadIdx.x / kST;
   double ax = 0.0, ay = 0.0, az = 0.0;
   if (ls < cnt) {
     const double4 w = W[ls];
     const double q = w.w;
-    for (int u = part; u < nkt; u += kParts) {
+    const int ub = part * (kKT / kParts), ue = min(ub + kKT / kParts, nkt);
+    int pl = -1, pm = 0;
+    double2 lm = make_double2(0.0, 0.0);
+    for (int u = ub; u < ue; u++) {
       const KVec k = K[u];
       const double4 a = A[u];
+      if (k.l != pl || k.m != pm) {  // warp-uniform: the warp's lanes share u
+        lm = phase_lm(T, k1, ls, k.l, k.m);
+        pl = k.l;
+        pm = k.m;
+      }
       double c, s;
-      phase(T, k1, ls, k.l, k.m, k.n, c, s);
+      phase_n(T, k1, ls, lm, k.n, c, s);
       double g;
       if (MODE == 0) {
         g = 4.0 * kR4pie0 * k.ak * ((q * s) * a.x - (q * c) * a.y);
@@ -261,11 +284,18 @@ __global__ void __launch_bounds__(kThreads)
       az += k.rn * g;
     }
   }
-#pragma unroll
-  for (int off = 1; off < kParts; off <<= 1) {
-    ax += __shfl_xor_sync(0xffffffffu, ax, off);
-    ay += __shfl_xor_sync(0xffffffffu, ay, off);
-    az += __shfl_xor_sync(0xffffffffu, az, off);
+  // the quarters' partial sums of each site, added in shared memory
+  double *red = reinterpret_cast<double *>(A + kKT);
+  red[(part * 3 + 0) * kST + ls] = ax;
+  red[(part * 3 + 1) * kST + ls] = ay;
+  red[(part * 3 + 2) * kST + ls] = az;
+  __syncthreads();
+  if (part == 0) {
+    for (int p = 1; p < kParts; p++) {
+      ax += red[(p * 3 + 0) * kST + ls];
+      ay += red[(p * 3 + 1) * kST + ls];
+      az += red[(p * 3 + 2) * kST + ls];
+    }
   }
   if (part == 0 && ls < cnt) {
     const int per = tgt_count(MODE, S);
@@ -337,7 +367,7 @@ inline int k1_of(int kl, int km, int kn) {
 
 inline size_t tile_smem(int k1, bool gather) {
   return sizeof(double2) * 3 * (size_t)k1 * kST + sizeof(double4) * kST + sizeof(KVec) * kKT +
-         (gather ? sizeof(double4) * kKT : 0);
+         (gather ? sizeof(double4) * kKT + sizeof(double) * 3 * kParts * kST : 0);
 }
 
 template <typename F>
