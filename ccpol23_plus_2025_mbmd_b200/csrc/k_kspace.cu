@@ -238,10 +238,31 @@ __global__ void __launch_bounds__(kThreads)
   const int k0 = blockIdx.x * kKT, s0 = blockIdx.y * kST;
   const int cnt = stage_sites<MODE == 3>(MODE, false, tab, nm, S, k1, mu, s0, T, W);
   const int nkt = min(kKT, nk - k0);
+  // each k-vector's gather weights, the mode's factor times its sums, so that a (site, k)
+  // pair's weight g is two or four products of the phase (cos, sin):
+  //   0: g = q (s W0 + c W1), W = 4 r4pie0 a(k) (S_re, -S_im)
+  //   1: g = s W0 + c W1,     W = 4 a(k) (S_re, -S_im)
+  //   2: g = c W0 + s W1,     W = -4 a(k) (S_re, S_im)
+  //   3: g = q (c W0 + s W1) + (mu.k)(c W2 + s W3), with f = -4 a(k) and the charge and dipole
+  //      sums (S, D): W = (f D_re, f D_im, f (D_im - S_re), -f (S_im + D_re))
+  // (nb_induction_model.f90:4171-4839 for mode 3: mufac, qfac and mufaci regrouped)
   for (int u = threadIdx.x; u < nkt; u += blockDim.x) {
-    K[u] = kv[k0 + u];
+    const KVec kq = kv[k0 + u];
+    K[u] = kq;
     const double *s = sk + (size_t)(k0 + u) * 4;
-    A[u] = make_double4(s[0], s[1], s[2], s[3]);
+    if (MODE == 0) {
+      const double f = 4.0 * kR4pie0 * kq.ak;
+      A[u] = make_double4(f * s[0], -f * s[1], 0.0, 0.0);
+    } else if (MODE == 1) {
+      const double f = 4.0 * kq.ak;
+      A[u] = make_double4(f * s[0], -f * s[1], 0.0, 0.0);
+    } else if (MODE == 2) {
+      const double f = -4.0 * kq.ak;
+      A[u] = make_double4(f * s[0], f * s[1], 0.0, 0.0);
+    } else {
+      const double f = -4.0 * kq.ak;
+      A[u] = make_double4(f * s[2], f * s[3], f * (s[3] - s[0]), -f * (s[1] + s[2]));
+    }
   }
   __syncthreads();
   // site-major lanes: a warp takes 32 consecutive sites of the tile and one contiguous
@@ -267,17 +288,14 @@ __global__ void __launch_bounds__(kThreads)
       phase_n(T, k1, ls, lm, k.n, c, s);
       double g;
       if (MODE == 0) {
-        g = 4.0 * kR4pie0 * k.ak * ((q * s) * a.x - (q * c) * a.y);
+        g = q * (s * a.x + c * a.y);
       } else if (MODE == 1) {
-        g = 4.0 * k.ak * (s * a.x - c * a.y);
+        g = s * a.x + c * a.y;
       } else if (MODE == 2) {
-        g = -4.0 * k.ak * (c * a.x + s * a.y);
+        g = c * a.x + s * a.y;
       } else {
-        const double mufac = -4.0 * k.ak * (c * a.z + s * a.w);
-        const double qfac = -4.0 * k.ak * (-c * a.x - s * a.y);
-        const double mufaci = -4.0 * k.ak * (c * a.w - s * a.z);
         const double mk = w.x * k.rl + w.y * k.rm + w.z * k.rn;
-        g = q * mufac + mk * (qfac + mufaci);
+        g = q * (c * a.x + s * a.y) + mk * (c * a.z + s * a.w);
       }
       ax += k.rl * g;
       ay += k.rm * g;
