@@ -10,8 +10,8 @@
 //
 // FS3, the costliest term of a frame, can be fused across the frames when they share one box
 // length (option "fuse_fs3", off by default: beside one long FS3 launch every frame's
-// Ewald/induction chain slows down, and 32 frames of 256 waters took 36.7 ms fused against
-// 34.2 ms with FS3 per frame, 8 slots): the batch then packs every frame's molecules one
+// Ewald/induction chain slows down, and 32 frames of 256 waters took 35.8 ms fused against
+// 33.7 ms with FS3 per frame, 8 slots): the batch then packs every frame's molecules one
 // frame after another and runs one neighbour search, one triple enumeration and one FS3
 // launch for all of them on its own stream (batch_fs3_launch), while the slots evaluate the
 // other terms; the FS3 forces, energies and parameter gradients are then added per frame
